@@ -1,0 +1,130 @@
+/*
+ * simtrack_b200 C ABI.
+ *
+ * The drop-in boundary for SimTrack's tracking path: plain C types, pointers
+ * and sizes only.  Every entry point returns a status code (STB_OK or a
+ * negative STB_E* value) and never terminates the process; the message of the
+ * last failure on the calling thread is available from stb_last_error().
+ * Each declaration names the reference interface it replaces
+ * (simtrack.h / simtrack.cpp, file:line).
+ *
+ * Threading: the element and line objects are not synchronised; a table may
+ * be used by one host thread at a time.  Device-pointer entry points take an
+ * explicit cudaStream_t passed as void*.
+ */
+#ifndef SIMTRACK_B200_H
+#define SIMTRACK_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define STB_OK 0
+#define STB_EINVAL (-1)
+#define STB_ENOMEM (-2)
+#define STB_ECUDA (-3)
+#define STB_ETIMEOUT (-4)
+#define STB_EABORTED (-5)
+#define STB_EUNSUPPORTED (-6)
+
+typedef struct stb_element stb_element; /* Element*  (simtrack.h:373-396) */
+typedef struct stb_line stb_line;       /* Line      (simtrack.h:1067-1100) */
+typedef struct stb_table stb_table;     /* flattened device element table (no reference counterpart) */
+
+/* Message of the last failed call on this thread ("" if none). */
+const char *stb_last_error(void);
+/* Library version as major*10000 + minor*100 + patch. */
+int stb_version(void);
+
+/* ---- reference particle: GlobalVariables GP (simtrack.h:28-68) ---- */
+/* Set_RefPartEnergy(gamma, E0, Q, A)  simtrack.cpp:87-108 */
+int stb_set_ref_energy(double gamma, double E0, double Q, double A);
+/* Set_Spin_G(g)  simtrack.cpp:110-115 */
+int stb_set_spin_g(double g);
+/* GP.H_expand, GP.quad_fringe  simtrack.h:62-66 (GP.radiate is not supported) */
+int stb_set_flags(int h_expand, int quad_fringe);
+/* out[0..7] = GP.gamma, GP.beta, GP.energy, GP.brho, GP.Q, GP.energy0, GP.G, GP.p */
+int stb_get_ref(double *out8);
+
+/* ---- elements: `new TYPE(name, args...)`  simtrack.h:399-1059 ----
+ * type: "DRIFT","MARKER","SBEND","GSBEND","QUAD","SKEWQ","SEXT","OCT","MULT","GMULT",
+ *       "SBENDMULT","KICKER","HKICKER","VKICKER","RFCAV","CRABRF","CCMULT","LBT","ILBT",
+ *       "BEAMBEAM".
+ * args: the constructor arguments after `name`, in constructor order; MULT takes
+ *       L, KNL[11], KNSL[11] (23 values); GMULT/SBENDMULT take L, ANGLE, E1, E2,
+ *       KNL[11], KNSL[11] (26 values); BEAMBEAM takes TREATMENT, NP, BBSCALE, SIGMAL,
+ *       NSLICE, EMITX, BETAX, ALFAX, EMITY, BETAY, ALFAY. */
+int stb_element_new(const char *type, const char *name, const double *args, int nargs, stb_element **out);
+/* delete of an element that is not owned by a line */
+int stb_element_free(stb_element *e);
+/* Element::SetP / Element::GetP  (e.g. QUAD simtrack.cpp:8645-8685) */
+int stb_element_setp(stb_element *e, const char *pname, double value);
+int stb_element_getp(const stb_element *e, const char *pname, double *value);
+/* public fields DX, DY, DS, DTHETA, DPHI, DPSI  (simtrack.h:388-389) */
+int stb_element_set_misalign(stb_element *e, double dx, double dy, double ds, double dtheta, double dphi,
+                             double dpsi);
+/* public fields APx, APy  (simtrack.h:394; default 1 m, simtrack.cpp:8394-8395) */
+int stb_element_set_aperture(stb_element *e, double apx, double apy);
+/* writes TYPE into buf (NUL-terminated, truncated to cap) */
+int stb_element_type(const stb_element *e, char *buf, int cap);
+
+/* ---- Line (simtrack.cpp:12341-12431); the line owns appended elements ---- */
+int stb_line_new(stb_line **out);
+int stb_line_free(stb_line *l);                       /* ~Line -> Empty() */
+int stb_line_append(stb_line *l, stb_element *e);     /* Line::Append */
+int stb_line_insert(stb_line *l, long i, stb_element *e); /* Line::Insert */
+int stb_line_delete(stb_line *l, long i);             /* Line::Delete */
+int stb_line_replace(stb_line *l, long i, stb_element *e); /* Line::Replace */
+int stb_line_rewind(stb_line *l, long i);             /* Line::Rewind */
+int stb_line_invert(stb_line *l);                     /* Line::Invert */
+long stb_line_ncell(const stb_line *l);               /* Line::Ncell */
+double stb_line_length(const stb_line *l);            /* Line::Length */
+int stb_line_cell(stb_line *l, long i, stb_element **out); /* Line::Cell[i] (borrowed) */
+
+/* ---- flattening: Line -> device element table ----
+ * No reference counterpart: the reference dispatches Element::Pass virtually
+ * per particle per element (simtrack.cpp:20801).  The table snapshots GP and
+ * every element parameter; rebuild it after editing the line. */
+int stb_table_create(const stb_line *l, int device, stb_table **out);
+int stb_table_free(stb_table *t);
+/* info[0] = elements, [1] = pool doubles, [2] = algorithmic FP64 ops per particle-turn,
+ * [3] = 1 if the table is staged in shared memory, [4] = shared-memory bytes per CTA */
+int stb_table_info(const stb_table *t, double *info5);
+
+/* ---- tracking ----
+ * Track()  simtrack.cpp:20791-20814, batched.  Coordinates are SoA device
+ * arrays of n doubles each (x, px, y, py, z=-c*dt, pt=dE/P0c; simtrack.cpp:12-21),
+ * updated in place.  lost_turn[i] < 0 marks a live particle on entry and exit;
+ * a lost particle gets the turn (turn0-based global index) and the element
+ * index after which it was lost, and keeps its coordinates at that point, as
+ * in the reference.  turn0 == 0 applies Track()'s entry check
+ * (|x| or |y| > 0.1 m -> lost at turn 0, element 0).  aperture_radius > 0 adds
+ * the circular loss test x^2 + y^2 > R^2 after every element.
+ * stream: a cudaStream_t, or NULL for the default stream.  Asynchronous. */
+int stb_track_device(stb_table *t, double *x, double *px, double *y, double *py, double *z, double *pt, long n,
+                     int turn0, int nturn, double aperture_radius, int32_t *lost_turn, int32_t *lost_elem,
+                     void *stream);
+
+/* Host-buffer form with Track()'s outputs: x is AoS n*6 (x[6] per particle as in
+ * Track), stable[i] on entry is Track()'s input flag (0 -> lost immediately);
+ * on exit stable/lost_turn/lost_post hold Track()'s outputs.  Copies in and
+ * out, synchronous. */
+int stb_track_host(stb_table *t, double *x, long n, int nturn, double aperture_radius, int *stable,
+                   int *lost_turn, int *lost_post);
+
+/* Per-element probe: as stb_track_host, and additionally writes the six
+ * coordinates after every element to dump[((i*nturn + turn)*ncell + j)*6 + k]
+ * (host buffer of n*nturn*ncell*6 doubles; entries after a particle's loss are
+ * left as passed in).  This is the commented-out per-element output of
+ * Track(), simtrack.cpp:20806-20812, made available for parity checks and
+ * diagnostics.  Intended for small n. */
+int stb_track_probe(stb_table *t, double *x, long n, int nturn, double aperture_radius, double *dump, int *stable,
+                    int *lost_turn, int *lost_post);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,245 @@
+// simtrack_b200 C++ host API: the beamline construction and tracking
+// interface of SimTrack (simtrack.h), with tracking executed on a B200 GPU.
+//
+// A driver written against the reference builds a Line with `new QUAD(...)`,
+// `SetP("Nint", 4)`, `Line::Append(...)` and calls `Track(...)`.  The same
+// driver compiles against this header after `using namespace stb;`.  The
+// classes here hold element parameters only; every Pass runs inside the
+// CUDA tracking kernel after the Line is flattened into a device table.
+//
+// Deviations from the reference, all deliberate:
+//   * errors throw stb::Error (derived from std::runtime_error) instead of
+//     printing and calling exit() (e.g. SetP on an unknown name,
+//     simtrack.cpp:8653-8685);
+//   * there is no CPU Pass: an element type without a GPU implementation is
+//     rejected when the Line is flattened.
+#pragma once
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace stb {
+
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string &m) : std::runtime_error(m), code(c) {}
+};
+
+// Reference-particle state, GlobalVariables (simtrack.h:28-68).  Only the
+// fields the tracking path reads are kept.
+struct GlobalVariables {
+  int A = 1, Q = 1, turn = 0;
+  double m0 = 1.6726216e-27, m = 1.6726216e-27, q = 1.6021765e-19;
+  double energy0 = 938.27201, energy = 99456.8, p = 1., cp = 1.;
+  double gamma = 106., beta = 0.999955, brho = 331.738;
+  double G = 1.7928474, Gr = 191.079706193;
+  bool H_expand = false, radiate = false, quad_fringe = false;
+};
+extern GlobalVariables GP;
+
+// Set_RefPartEnergy (simtrack.cpp:87-108) and Set_Spin_G (simtrack.cpp:110-115).
+void Set_RefPartEnergy(double gamma, double E0, double Q, double A);
+void Set_Spin_G(double g);
+
+// Default integration slice lengths (simtrack.cpp:45-47).
+extern double BLslice, QLslice, GLslice;
+
+// Abstract element (simtrack.h:373-396).  Named parameters are reached through
+// SetP/GetP exactly as in the reference; geometry and aperture are public
+// fields.
+class Element {
+ public:
+  explicit Element(std::string name);
+  virtual ~Element() = default;
+  void SetP(const char *name, double value);
+  double GetP(const char *name) const;
+
+  std::string NAME, TYPE, GROUP;
+  double S = 0., L = 0.;
+  double DX = 0., DY = 0., DS = 0.;
+  double DTHETA = 0., DPHI = 0., DPSI = 0.;
+  double APx = 1., APy = 1.;
+
+  // Parameter access for the flattener (names as accepted by SetP).
+  double P(const char *name) const { return GetP(name); }
+  const double *KNL() const { return knl_; }
+  const double *KNSL() const { return knsl_; }
+
+ protected:
+  void add_param(const char *name, double *slot, bool integer = false);
+  void add_multipoles();
+  virtual void on_setp(const char *name) { (void)name; }
+  double knl_[11] = {0};
+  double knsl_[11] = {0};
+
+ private:
+  struct Param {
+    const char *name;
+    double *slot;
+    bool integer;
+  };
+  std::vector<Param> params_;
+};
+
+class DRIFT : public Element { public: DRIFT(std::string name, double l); };
+class MARKER : public Element { public: MARKER(std::string name, double l); };
+class SBEND : public Element {
+ public:
+  SBEND(std::string name, double l, double angle, double e1, double e2);
+ private:
+  double ANGLE, E1, E2, Nint;
+};
+class GSBEND : public Element {
+ public:
+  GSBEND(std::string name, double l, double angle, double k0l, double e1, double e2);
+ private:
+  double ANGLE, K0L, E1, E2, Nint;
+};
+class QUAD : public Element {
+ public:
+  QUAD(std::string name, double l, double k1l, double k1sl);
+ private:
+  double K1L, K1SL, Nint;
+};
+class SKEWQ : public Element {
+ public:
+  SKEWQ(std::string name, double l, double k1sl);
+ private:
+  double K1SL, Nint;
+};
+class SEXT : public Element {
+ public:
+  SEXT(std::string name, double l, double k2l, double k2sl);
+ private:
+  double K2L, K2SL, Nint;
+};
+class OCT : public Element {
+ public:
+  OCT(std::string name, double l, double k3l, double k3sl);
+ private:
+  double K3L, K3SL, Nint;
+};
+class MULT : public Element {
+ public:
+  MULT(std::string name, double l, const double knl[11], const double knsl[11]);
+ private:
+  double Nint, Norder;
+};
+class GMULT : public Element {
+ public:
+  GMULT(std::string name, double l, double angle, double e1, double e2, const double knl[11],
+        const double knsl[11]);
+ private:
+  double ANGLE, E1, E2, Nint, Norder;
+};
+class SBENDMULT : public Element {
+ public:
+  SBENDMULT(std::string name, double l, double angle, double e1, double e2, const double knl[11],
+            const double knsl[11]);
+ private:
+  double ANGLE, E1, E2, Nint, Norder;
+};
+class KICKER : public Element {
+ public:
+  KICKER(std::string name, double l, double hkick, double vkick);
+ private:
+  double HKICK, VKICK;
+};
+class HKICKER : public Element {
+ public:
+  HKICKER(std::string name, double l, double hkick);
+ private:
+  double HKICK;
+};
+class VKICKER : public Element {
+ public:
+  VKICKER(std::string name, double l, double vkick);
+ private:
+  double VKICK;
+};
+class RFCAV : public Element {
+ public:
+  RFCAV(std::string name, double l, double vrf, double frf, double phase0);
+ private:
+  double VRF, FRF, PHASE0;
+};
+class CRABRF : public Element {
+ public:
+  CRABRF(std::string name, double l, double vrf, double frf, double phase0);
+ private:
+  double VRF, FRF, PHASE0;
+};
+class CCMULT : public Element {
+ public:
+  CCMULT(std::string name, double l, double vrf, double frf, double phase0, double b1, double a1,
+         double b2, double a2, double b3, double a3, double b4, double a4);
+ private:
+  double VRF, FRF, PHASE0, B1, A1, B2, A2, B3, A3, B4, A4;
+};
+class LBT : public Element {
+ public:
+  LBT(std::string name, double theta);
+ private:
+  double THETA;
+};
+class ILBT : public Element {
+ public:
+  ILBT(std::string name, double theta);
+ private:
+  double THETA;
+};
+class BEAMBEAM : public Element {
+ public:
+  BEAMBEAM(std::string name, int treatment, double np, double bbscale, double sigmal, int nslice,
+           double emitx, double betax, double alfax, double emity, double betay, double alfay);
+ protected:
+  void on_setp(const char *name) override;
+ private:
+  double TREATMENT, NP, BBSCALE, SIGMAL, NSLICE, EMITX, BETAX, ALFAX, EMITY, BETAY, ALFAY;
+};
+
+// Line container (simtrack.h:1067-1100).  Owns its elements, like the
+// reference: Delete/Replace/Empty and the destructor delete them.
+class Line {
+ public:
+  Line() = default;
+  ~Line();
+  Line(const Line &) = delete;
+  Line &operator=(const Line &) = delete;
+
+  void Update();
+  void Append(Element *x);
+  void Delete(int i);
+  void Insert(int i, Element *temp);
+  void Replace(int i, Element *temp);
+  void Rewind(int i);
+  void Invert();
+  void Empty();
+
+  std::vector<Element *> Cell;
+  double Length = 0.;
+  long Ncell = 0;
+  double frev0 = 0.;
+};
+
+// Options that have no counterpart in Track()'s signature.
+struct TrackOptions {
+  double aperture_radius = 0.;  // circular aperture checked after every element; <= 0 disables
+  int device = 0;
+};
+
+// Track() drop-in (simtrack.cpp:20791-20814): one particle, x[6] updated in
+// place; stable/lost_turn/lost_post as in the reference.  Runs on the GPU.
+void Track(Line &line, double x[], int nturn, int &stable, int &lost_turn, int &lost_post);
+
+// Batched Track over n particles in AoS x[n*6] (the per-particle loop of the
+// DA drivers, simtrack.cpp:21389-21441, moved onto the GPU in one launch).
+void Track_Batch(Line &line, double *x, long n, int nturn, int *stable, int *lost_turn,
+                 int *lost_post, const TrackOptions &opt = TrackOptions());
+
+// Track_Spin() drop-in (simtrack.cpp:21766-21789): x[9] = orbit + spin.
+void Track_Spin(Line &line, double x[], int nturn, int &stable, int &lost_turn, int &lost_post);
+
+}  // namespace stb

@@ -1,0 +1,202 @@
+// Reference oracle harness.  TEST INFRASTRUCTURE ONLY.
+//
+// Compiled together with the unmodified SimTrack source (simtrack.cpp) into
+// oracle/_ref/libsimtrack_ref.so by oracle/Makefile.  It exposes a C ABI that
+// pytest loads through ctypes to build a Line with the reference's own element
+// constructors (simtrack.h:399-1059) and to run the reference's own tracking
+// entry points:
+//   ref_track       -> Track()       simtrack.cpp:20791-20814 (called as is)
+//   ref_track_spin  -> Track_Spin()  simtrack.cpp:21766-21789 (called as is)
+//   ref_track_circ  -> the Track() loop with one extra loss predicate, a
+//                      circular aperture x^2+y^2 > R^2, evaluated after the
+//                      reference's own rectangular/NaN check.
+//   ref_track_dump  -> the Track() loop that also records all six
+//                      coordinates after every element (the per-element
+//                      parity probe).
+// Nothing in the product links or loads this file.
+#include "simtrack.h"
+
+#include <cstring>
+#include <cmath>
+
+extern GlobalVariables GP;
+
+namespace {
+
+void copy11(const double *src, double *dst) {
+  for (int i = 0; i < 11; i++) dst[i] = src[i];
+}
+
+Element *make_element(const char *type, const char *name, const double *p, int np) {
+  std::string nm(name ? name : "");
+  std::string t(type);
+  auto need = [&](int k) { return np >= k; };
+  if (t == "DRIFT" && need(1)) return new DRIFT(nm, p[0]);
+  if (t == "MARKER" && need(1)) return new MARKER(nm, p[0]);
+  if (t == "SBEND" && need(4)) return new SBEND(nm, p[0], p[1], p[2], p[3]);
+  if (t == "GSBEND" && need(5)) return new GSBEND(nm, p[0], p[1], p[2], p[3], p[4]);
+  if (t == "QUAD" && need(3)) return new QUAD(nm, p[0], p[1], p[2]);
+  if (t == "SKEWQ" && need(2)) return new SKEWQ(nm, p[0], p[1]);
+  if (t == "SEXT" && need(3)) return new SEXT(nm, p[0], p[1], p[2]);
+  if (t == "OCT" && need(3)) return new OCT(nm, p[0], p[1], p[2]);
+  if (t == "MULT" && need(23)) {
+    double knl[11], knsl[11];
+    copy11(p + 1, knl);
+    copy11(p + 12, knsl);
+    return new MULT(nm, p[0], knl, knsl);
+  }
+  if ((t == "GMULT" || t == "SBENDMULT") && need(26)) {
+    double knl[11], knsl[11];
+    copy11(p + 4, knl);
+    copy11(p + 15, knsl);
+    if (t == "GMULT") return new GMULT(nm, p[0], p[1], p[2], p[3], knl, knsl);
+    return new SBENDMULT(nm, p[0], p[1], p[2], p[3], knl, knsl);
+  }
+  if (t == "KICKER" && need(3)) return new KICKER(nm, p[0], p[1], p[2]);
+  if (t == "HKICKER" && need(2)) return new HKICKER(nm, p[0], p[1]);
+  if (t == "VKICKER" && need(2)) return new VKICKER(nm, p[0], p[1]);
+  if (t == "RFCAV" && need(4)) return new RFCAV(nm, p[0], p[1], p[2], p[3]);
+  if (t == "CRABRF" && need(4)) return new CRABRF(nm, p[0], p[1], p[2], p[3]);
+  if (t == "CCMULT" && need(12))
+    return new CCMULT(nm, p[0], p[1], p[2], p[3], p[4], p[5], p[6], p[7], p[8], p[9], p[10], p[11]);
+  if (t == "LBT" && need(1)) return new LBT(nm, p[0]);
+  if (t == "ILBT" && need(1)) return new ILBT(nm, p[0]);
+  if (t == "BEAMBEAM" && need(11))
+    return new BEAMBEAM(nm, int(p[0]), p[1], p[2], p[3], int(p[4]), p[5], p[6], p[7], p[8], p[9], p[10]);
+  return nullptr;
+}
+
+inline bool circ_lost(const double *x, double r2) {
+  return r2 > 0.0 && x[0] * x[0] + x[2] * x[2] > r2;
+}
+
+}  // namespace
+
+extern "C" {
+
+void ref_set_ref_energy(double gamma, double E0, double Q, double A) {
+  Set_RefPartEnergy(gamma, E0, Q, A);
+}
+
+void ref_set_spin_g(double g) { Set_Spin_G(g); }
+
+void ref_set_flags(int h_expand, int quad_fringe) {
+  GP.H_expand = h_expand != 0;
+  GP.quad_fringe = quad_fringe != 0;
+  GP.radiate = false;
+}
+
+// gamma, beta, energy, brho, Q, energy0, G
+void ref_get_gp(double *out) {
+  out[0] = GP.gamma;
+  out[1] = GP.beta;
+  out[2] = GP.energy;
+  out[3] = GP.brho;
+  out[4] = GP.Q;
+  out[5] = GP.energy0;
+  out[6] = GP.G;
+}
+
+void *ref_line_new(void) { return new Line(); }
+void ref_line_free(void *line) { delete static_cast<Line *>(line); }
+long ref_line_ncell(void *line) { return static_cast<Line *>(line)->Ncell; }
+double ref_line_length(void *line) { return static_cast<Line *>(line)->Length; }
+
+int ref_line_append(void *line, const char *type, const char *name, const double *p, int np) {
+  Element *e = make_element(type, name, p, np);
+  if (!e) return -1;
+  static_cast<Line *>(line)->Append(e);
+  return 0;
+}
+
+void ref_line_setp(void *line, long idx, const char *pname, double v) {
+  static_cast<Line *>(line)->Cell[idx]->SetP(pname, v);
+}
+
+double ref_line_getp(void *line, long idx, const char *pname) {
+  return static_cast<Line *>(line)->Cell[idx]->GetP(pname);
+}
+
+void ref_line_set_misalign(void *line, long idx, double dx, double dy, double ds, double dtheta,
+                           double dphi, double dpsi) {
+  Element *e = static_cast<Line *>(line)->Cell[idx];
+  e->DX = dx; e->DY = dy; e->DS = ds;
+  e->DTHETA = dtheta; e->DPHI = dphi; e->DPSI = dpsi;
+}
+
+void ref_line_set_aperture(void *line, long idx, double apx, double apy) {
+  Element *e = static_cast<Line *>(line)->Cell[idx];
+  e->APx = apx;
+  e->APy = apy;
+}
+
+void ref_pass(void *line, long idx, double *x) { static_cast<Line *>(line)->Cell[idx]->Pass(x); }
+
+// n particles, AoS x[n*6], through the reference Track(); stable[] is read as
+// the caller's input flag (Track's own convention) and overwritten.
+void ref_track(void *line, double *x, long n, int nturn, int *stable, int *lost_turn, int *lost_post) {
+  Line &l = *static_cast<Line *>(line);
+  for (long i = 0; i < n; i++) {
+    int st = stable[i], lt = 0, lp = 0;
+    Track(l, x + 6 * i, nturn, st, lt, lp);
+    stable[i] = st; lost_turn[i] = lt; lost_post[i] = lp;
+  }
+}
+
+void ref_track_spin(void *line, double *x9, long n, int nturn, int *stable, int *lost_turn,
+                    int *lost_post) {
+  Line &l = *static_cast<Line *>(line);
+  for (long i = 0; i < n; i++) {
+    int st = stable[i], lt = 0, lp = 0;
+    Track_Spin(l, x9 + 9 * i, nturn, st, lt, lp);
+    stable[i] = st; lost_turn[i] = lt; lost_post[i] = lp;
+  }
+}
+
+// Track() loop plus a circular aperture of radius R (R <= 0 disables it).
+void ref_track_circ(void *line, double *x, long n, int nturn, double radius, int *stable,
+                    int *lost_turn, int *lost_post) {
+  Line &l = *static_cast<Line *>(line);
+  const double r2 = radius > 0.0 ? radius * radius : 0.0;
+  for (long i = 0; i < n; i++) {
+    double *xi = x + 6 * i;
+    stable[i] = 1; lost_turn[i] = 0; lost_post[i] = 0;
+    if (std::abs(xi[0]) > 0.1 || std::abs(xi[2]) > 0.1) { stable[i] = 0; continue; }
+    bool lost = false;
+    for (GP.turn = 0; GP.turn < nturn && !lost; GP.turn++) {
+      for (long j = 0; j < l.Ncell; j++) {
+        l.Cell[j]->Pass(xi);
+        if (std::abs(xi[0]) > l.Cell[j]->APx || std::abs(xi[2]) > l.Cell[j]->APy ||
+            std::isnan(xi[0]) || std::isnan(xi[2]) || circ_lost(xi, r2)) {
+          stable[i] = 0; lost_turn[i] = GP.turn; lost_post[i] = (int)j; lost = true;
+          break;
+        }
+      }
+    }
+  }
+}
+
+// One particle; dump[(turn*ncell + j)*6 + k] = x[k] after element j of turn.
+// Entries after a loss are left untouched.
+void ref_track_dump(void *line, double *x, int nturn, double radius, double *dump, int *stable,
+                    int *lost_turn, int *lost_post) {
+  Line &l = *static_cast<Line *>(line);
+  const double r2 = radius > 0.0 ? radius * radius : 0.0;
+  *stable = 1; *lost_turn = 0; *lost_post = 0;
+  if (std::abs(x[0]) > 0.1 || std::abs(x[2]) > 0.1) { *stable = 0; return; }
+  for (GP.turn = 0; GP.turn < nturn; GP.turn++) {
+    for (long j = 0; j < l.Ncell; j++) {
+      l.Cell[j]->Pass(x);
+      std::memcpy(dump + ((long)GP.turn * l.Ncell + j) * 6, x, 6 * sizeof(double));
+      if (std::abs(x[0]) > l.Cell[j]->APx || std::abs(x[2]) > l.Cell[j]->APy || std::isnan(x[0]) ||
+          std::isnan(x[2]) || circ_lost(x, r2)) {
+        *stable = 0; *lost_turn = GP.turn; *lost_post = (int)j;
+        return;
+      }
+    }
+  }
+}
+
+double ref_pinv(double p) { return gsl_cdf_ugaussian_Pinv(p); }
+
+}  // extern "C"

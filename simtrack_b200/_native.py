@@ -1,0 +1,92 @@
+"""ctypes binding of the C ABI in include/simtrack_b200.h.
+
+The shared library is built in-tree (simtrack_b200/_lib/libsimtrack_b200.so,
+see simtrack_b200/build.py).  There is no fallback: if the library is missing
+or a CUDA call fails, the error surfaces as SimTrackError.
+"""
+from __future__ import annotations
+
+import ctypes
+from ctypes import POINTER, c_char_p, c_double, c_int, c_int32, c_long, c_void_p
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "_lib" / "libsimtrack_b200.so"
+
+STB_OK = 0
+STB_EINVAL = -1
+STB_ENOMEM = -2
+STB_ECUDA = -3
+STB_ETIMEOUT = -4
+STB_EABORTED = -5
+STB_EUNSUPPORTED = -6
+
+_CODES = {STB_EINVAL: "EINVAL", STB_ENOMEM: "ENOMEM", STB_ECUDA: "ECUDA", STB_ETIMEOUT: "ETIMEOUT",
+          STB_EABORTED: "EABORTED", STB_EUNSUPPORTED: "EUNSUPPORTED"}
+
+
+class SimTrackError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{_CODES.get(code, code)}: {msg}")
+        self.code = code
+
+
+# (name, restype, argtypes) for every exported entry point.
+SIGNATURES = [
+    ("stb_last_error", c_char_p, []),
+    ("stb_version", c_int, []),
+    ("stb_set_ref_energy", c_int, [c_double, c_double, c_double, c_double]),
+    ("stb_set_spin_g", c_int, [c_double]),
+    ("stb_set_flags", c_int, [c_int, c_int]),
+    ("stb_get_ref", c_int, [POINTER(c_double)]),
+    ("stb_element_new", c_int, [c_char_p, c_char_p, POINTER(c_double), c_int, POINTER(c_void_p)]),
+    ("stb_element_free", c_int, [c_void_p]),
+    ("stb_element_setp", c_int, [c_void_p, c_char_p, c_double]),
+    ("stb_element_getp", c_int, [c_void_p, c_char_p, POINTER(c_double)]),
+    ("stb_element_set_misalign", c_int, [c_void_p] + [c_double] * 6),
+    ("stb_element_set_aperture", c_int, [c_void_p, c_double, c_double]),
+    ("stb_element_type", c_int, [c_void_p, c_char_p, c_int]),
+    ("stb_line_new", c_int, [POINTER(c_void_p)]),
+    ("stb_line_free", c_int, [c_void_p]),
+    ("stb_line_append", c_int, [c_void_p, c_void_p]),
+    ("stb_line_insert", c_int, [c_void_p, c_long, c_void_p]),
+    ("stb_line_delete", c_int, [c_void_p, c_long]),
+    ("stb_line_replace", c_int, [c_void_p, c_long, c_void_p]),
+    ("stb_line_rewind", c_int, [c_void_p, c_long]),
+    ("stb_line_invert", c_int, [c_void_p]),
+    ("stb_line_ncell", c_long, [c_void_p]),
+    ("stb_line_length", c_double, [c_void_p]),
+    ("stb_line_cell", c_int, [c_void_p, c_long, POINTER(c_void_p)]),
+    ("stb_table_create", c_int, [c_void_p, c_int, POINTER(c_void_p)]),
+    ("stb_table_free", c_int, [c_void_p]),
+    ("stb_table_info", c_int, [c_void_p, POINTER(c_double)]),
+    ("stb_track_device", c_int, [c_void_p] + [c_void_p] * 6 + [c_long, c_int, c_int, c_double, c_void_p,
+                                                                c_void_p, c_void_p]),
+    ("stb_track_host", c_int, [c_void_p, POINTER(c_double), c_long, c_int, c_double, POINTER(c_int),
+                               POINTER(c_int), POINTER(c_int)]),
+    ("stb_track_probe", c_int, [c_void_p, POINTER(c_double), c_long, c_int, c_double, POINTER(c_double),
+                                POINTER(c_int), POINTER(c_int), POINTER(c_int)]),
+]
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """Loads the in-tree native library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise SimTrackError(STB_EINVAL, f"native library not built: {LIB_PATH} "
+                                            "(run python -m simtrack_b200.build)")
+        L = ctypes.CDLL(str(LIB_PATH))
+        for name, res, args in SIGNATURES:
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(rc: int) -> None:
+    if rc != STB_OK:
+        msg = lib().stb_last_error()
+        raise SimTrackError(rc, msg.decode() if msg else "")

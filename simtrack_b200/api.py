@@ -1,0 +1,277 @@
+"""Python mirror of SimTrack's construction and tracking interface.
+
+Names, argument order and meaning follow simtrack.h: element classes are
+created as ``QUAD(name, L, K1L, K1SL)``, tuned with ``SetP``, appended to a
+``Line`` and tracked with ``Track``.  Everything runs through the C ABI of
+the native library; tracking executes on the GPU.  Errors raise
+SimTrackError instead of terminating the process (the reference prints and
+calls exit(), e.g. simtrack.cpp:8653-8685).
+"""
+from __future__ import annotations
+
+import ctypes
+from ctypes import POINTER, byref, c_double, c_int, c_void_p
+from typing import Sequence
+
+import numpy as np
+
+from ._native import SimTrackError, check, lib
+
+__all__ = [
+    "Set_RefPartEnergy", "Set_Spin_G", "Set_Flags", "GP", "Element", "Line", "Table", "Track", "Track_Batch",
+    "DRIFT", "MARKER", "SBEND", "GSBEND", "QUAD", "SKEWQ", "SEXT", "OCT", "MULT", "GMULT", "SBENDMULT",
+    "KICKER", "HKICKER", "VKICKER", "RFCAV", "CRABRF", "CCMULT", "LBT", "ILBT", "BEAMBEAM",
+]
+
+
+def Set_RefPartEnergy(gamma: float, E0: float, Q: float, A: float) -> None:
+    """Set_RefPartEnergy (simtrack.cpp:87-108): reference particle gamma, rest energy [MeV], charge, nucleons."""
+    check(lib().stb_set_ref_energy(gamma, E0, Q, A))
+
+
+def Set_Spin_G(g: float) -> None:
+    """Set_Spin_G (simtrack.cpp:110-115)."""
+    check(lib().stb_set_spin_g(g))
+
+
+def Set_Flags(h_expand: bool = False, quad_fringe: bool = False) -> None:
+    """GP.H_expand / GP.quad_fringe (simtrack.h:62-66)."""
+    check(lib().stb_set_flags(int(h_expand), int(quad_fringe)))
+
+
+def GP() -> dict:
+    """Snapshot of the reference-particle globals."""
+    out = (c_double * 8)()
+    check(lib().stb_get_ref(out))
+    keys = ["gamma", "beta", "energy", "brho", "Q", "energy0", "G", "p"]
+    return dict(zip(keys, list(out)))
+
+
+class Element:
+    """An element handle.  Owned by the Python object until appended to a Line."""
+
+    def __init__(self, type_: str, name: str, args: Sequence[float]):
+        arr = (c_double * max(len(args), 1))(*[float(a) for a in args])
+        h = c_void_p()
+        check(lib().stb_element_new(type_.encode(), name.encode(), arr, len(args), byref(h)))
+        self._h = h
+        self._owned = True
+        self.NAME = name
+
+    @classmethod
+    def _borrow(cls, handle: c_void_p) -> "Element":
+        e = cls.__new__(cls)
+        e._h = handle
+        e._owned = False
+        e.NAME = ""
+        return e
+
+    @property
+    def TYPE(self) -> str:
+        buf = ctypes.create_string_buffer(32)
+        check(lib().stb_element_type(self._h, buf, 32))
+        return buf.value.decode()
+
+    def SetP(self, name: str, value: float) -> None:
+        check(lib().stb_element_setp(self._h, name.encode(), float(value)))
+
+    def GetP(self, name: str) -> float:
+        v = c_double()
+        check(lib().stb_element_getp(self._h, name.encode(), byref(v)))
+        return v.value
+
+    def set_misalignment(self, dx=0., dy=0., ds=0., dtheta=0., dphi=0., dpsi=0.) -> None:
+        """Element::DX/DY/DS/DTHETA/DPHI/DPSI (simtrack.h:388-389)."""
+        check(lib().stb_element_set_misalign(self._h, dx, dy, ds, dtheta, dphi, dpsi))
+
+    def set_aperture(self, apx: float, apy: float) -> None:
+        """Element::APx/APy (simtrack.h:394)."""
+        check(lib().stb_element_set_aperture(self._h, apx, apy))
+
+    def __del__(self):
+        try:
+            if getattr(self, "_owned", False) and self._h:
+                lib().stb_element_free(self._h)
+        except Exception:
+            pass
+
+
+def _mk(type_):
+    def ctor(name, *args):
+        return Element(type_, name, args)
+    ctor.__name__ = type_
+    ctor.__doc__ = f"new {type_}(name, ...) (simtrack.h element class {type_})"
+    return ctor
+
+
+DRIFT = _mk("DRIFT")
+MARKER = _mk("MARKER")
+SBEND = _mk("SBEND")
+GSBEND = _mk("GSBEND")
+QUAD = _mk("QUAD")
+SKEWQ = _mk("SKEWQ")
+SEXT = _mk("SEXT")
+OCT = _mk("OCT")
+KICKER = _mk("KICKER")
+HKICKER = _mk("HKICKER")
+VKICKER = _mk("VKICKER")
+RFCAV = _mk("RFCAV")
+CRABRF = _mk("CRABRF")
+CCMULT = _mk("CCMULT")
+LBT = _mk("LBT")
+ILBT = _mk("ILBT")
+
+
+def MULT(name, L, knl, knsl):
+    """new MULT(name, L, KNL[11], KNSL[11]) (simtrack.h:527-538)."""
+    return Element("MULT", name, [L, *_pad11(knl), *_pad11(knsl)])
+
+
+def GMULT(name, L, angle, e1, e2, knl, knsl):
+    return Element("GMULT", name, [L, angle, e1, e2, *_pad11(knl), *_pad11(knsl)])
+
+
+def SBENDMULT(name, L, angle, e1, e2, knl, knsl):
+    return Element("SBENDMULT", name, [L, angle, e1, e2, *_pad11(knl), *_pad11(knsl)])
+
+
+def BEAMBEAM(name, treatment, np_, bbscale, sigmal, nslice, emitx, betax, alfax, emity, betay, alfay):
+    """new BEAMBEAM(...) (simtrack.h:842-855); emittances are un-normalised rms."""
+    return Element("BEAMBEAM", name, [treatment, np_, bbscale, sigmal, nslice, emitx, betax, alfax,
+                                      emity, betay, alfay])
+
+
+def _pad11(v):
+    v = [float(a) for a in v]
+    if len(v) > 11:
+        raise SimTrackError(-1, "at most 11 multipole coefficients")
+    return v + [0.0] * (11 - len(v))
+
+
+class Line:
+    """Line (simtrack.h:1067-1100).  Appended elements become owned by the line."""
+
+    def __init__(self):
+        h = c_void_p()
+        check(lib().stb_line_new(byref(h)))
+        self._h = h
+
+    def Append(self, e: Element) -> None:
+        check(lib().stb_line_append(self._h, e._h))
+        e._owned = False
+
+    def Insert(self, i: int, e: Element) -> None:
+        check(lib().stb_line_insert(self._h, i, e._h))
+        e._owned = False
+
+    def Delete(self, i: int) -> None:
+        check(lib().stb_line_delete(self._h, i))
+
+    def Replace(self, i: int, e: Element) -> None:
+        check(lib().stb_line_replace(self._h, i, e._h))
+        e._owned = False
+
+    def Rewind(self, i: int) -> None:
+        check(lib().stb_line_rewind(self._h, i))
+
+    def Invert(self) -> None:
+        check(lib().stb_line_invert(self._h))
+
+    @property
+    def Ncell(self) -> int:
+        return int(lib().stb_line_ncell(self._h))
+
+    @property
+    def Length(self) -> float:
+        return float(lib().stb_line_length(self._h))
+
+    def Cell(self, i: int) -> Element:
+        h = c_void_p()
+        check(lib().stb_line_cell(self._h, i, byref(h)))
+        return Element._borrow(h)
+
+    def __len__(self):
+        return self.Ncell
+
+    def __del__(self):
+        try:
+            if self._h:
+                lib().stb_line_free(self._h)
+        except Exception:
+            pass
+
+
+class Table:
+    """Flattened device element table of a Line (rebuild after editing the line)."""
+
+    def __init__(self, line: Line, device: int = 0):
+        h = c_void_p()
+        check(lib().stb_table_create(line._h, device, byref(h)))
+        self._h = h
+        self.device = device
+
+    def info(self) -> dict:
+        out = (c_double * 5)()
+        check(lib().stb_table_info(self._h, out))
+        return {"elements": int(out[0]), "pool_doubles": int(out[1]), "flops_per_turn": out[2],
+                "smem": bool(out[3]), "smem_bytes": int(out[4])}
+
+    def track_host(self, x: np.ndarray, nturn: int, aperture_radius: float = 0.0, stable=None):
+        """Track() over AoS host coordinates x[n,6] (updated in place); returns (stable, lost_turn, lost_post)."""
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        if x.ndim != 2 or x.shape[1] != 6:
+            raise SimTrackError(-1, "x must have shape (n, 6)")
+        n = x.shape[0]
+        st = np.ones(n, dtype=np.int32) if stable is None else np.ascontiguousarray(stable, dtype=np.int32)
+        lt = np.zeros(n, dtype=np.int32)
+        lp = np.zeros(n, dtype=np.int32)
+        check(lib().stb_track_host(self._h, x.ctypes.data_as(POINTER(c_double)), n, nturn, aperture_radius,
+                                   st.ctypes.data_as(POINTER(c_int)), lt.ctypes.data_as(POINTER(c_int)),
+                                   lp.ctypes.data_as(POINTER(c_int))))
+        return x, st, lt, lp
+
+    def track_probe(self, x: np.ndarray, nturn: int, aperture_radius: float = 0.0):
+        """Per-element probe: returns (x, stable, lost_turn, lost_post, dump[n, nturn, ncell, 6])."""
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        n = x.shape[0]
+        ne = self.info()["elements"]
+        dump = np.full((n, nturn, ne, 6), np.nan)
+        st = np.ones(n, dtype=np.int32)
+        lt = np.zeros(n, dtype=np.int32)
+        lp = np.zeros(n, dtype=np.int32)
+        check(lib().stb_track_probe(self._h, x.ctypes.data_as(POINTER(c_double)), n, nturn, aperture_radius,
+                                    dump.ctypes.data_as(POINTER(c_double)), st.ctypes.data_as(POINTER(c_int)),
+                                    lt.ctypes.data_as(POINTER(c_int)), lp.ctypes.data_as(POINTER(c_int))))
+        return x, st, lt, lp, dump
+
+    def track_device(self, coords, lost_turn, lost_elem, turn0: int, nturn: int, aperture_radius: float = 0.0,
+                     stream=None) -> None:
+        """Track SoA device tensors in place (coords: 6 CUDA float64 tensors; lost_*: int32 tensors)."""
+        ptrs = [c.data_ptr() for c in coords]
+        n = coords[0].numel()
+        s = None if stream is None else c_void_p(stream)
+        check(lib().stb_track_device(self._h, *[c_void_p(p) for p in ptrs], n, turn0, nturn, aperture_radius,
+                                     c_void_p(lost_turn.data_ptr()), c_void_p(lost_elem.data_ptr()), s))
+
+    def __del__(self):
+        try:
+            if self._h:
+                lib().stb_table_free(self._h)
+        except Exception:
+            pass
+
+
+def Track_Batch(line: Line, x: np.ndarray, nturn: int, aperture_radius: float = 0.0, stable=None, device: int = 0):
+    """Track() for many particles at once: x[n,6] AoS, updated in place."""
+    return Table(line, device).track_host(x, nturn, aperture_radius, stable)[1:]
+
+
+def Track(line: Line, x, nturn: int, stable: int = 1):
+    """Track (simtrack.cpp:20791-20814) for one particle x[6] (list or array, updated in place).
+
+    Returns (stable, lost_turn, lost_post)."""
+    arr = np.asarray(x, dtype=np.float64).reshape(1, 6).copy()
+    _, st, lt, lp = Table(line).track_host(arr, nturn, 0.0, np.array([stable], dtype=np.int32))
+    for k in range(6):
+        x[k] = arr[0, k]
+    return int(st[0]), int(lt[0]), int(lp[0])

@@ -1,0 +1,460 @@
+// C ABI and C++ Track entry points over the element classes, the flattener
+// and the CUDA kernels.  Exceptions never cross the C boundary: every entry
+// point converts them into a status code plus a thread-local message.
+#include "simtrack_b200.h"
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "simtrack_b200.hpp"
+#include "stb_flatten.hpp"
+#include "stb_kernels.hpp"
+#include "stb_status.hpp"
+
+struct stb_table {
+  int device = 0;
+  stb::HostTable host;
+  stb::ElemHeader *d_hdr = nullptr;
+  double *d_pool = nullptr;
+  int npool_padded = 0;
+  bool use_smem = false;
+  int *d_status = nullptr;
+  int num_sms = 0;
+};
+
+namespace stb {
+
+namespace {
+thread_local std::string g_last_error;
+}
+
+void set_last_error(const std::string &msg) { g_last_error = msg; }
+const char *last_error() { return g_last_error.c_str(); }
+
+namespace {
+
+// Runs f(), mapping exceptions and CUDA failures onto status codes.
+template <class F>
+int guarded(F &&f) {
+  try {
+    int rc = f();
+    if (rc == STB_OK) g_last_error.clear();
+    return rc;
+  } catch (const Error &e) {
+    set_last_error(e.what());
+    return e.code;
+  } catch (const std::bad_alloc &) {
+    set_last_error("host allocation failed");
+    return STB_ENOMEM;
+  } catch (const std::exception &e) {
+    set_last_error(e.what());
+    return STB_EINVAL;
+  }
+}
+
+void cuda_check(cudaError_t e, const char *what) {
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    throw Error(e == cudaErrorMemoryAllocation ? STB_ENOMEM : STB_ECUDA,
+                std::string(what) + ": " + cudaGetErrorString(e));
+  }
+}
+
+// Restores the caller's current device on scope exit.
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cuda_check(cudaGetDevice(&prev), "cudaGetDevice");
+    if (prev != dev) cuda_check(cudaSetDevice(dev), "cudaSetDevice");
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    if (cudaGetDevice(&cur) == cudaSuccess && cur != prev && prev >= 0) cudaSetDevice(prev);
+  }
+};
+
+Element *make_element(const char *type, const char *name, const double *a, int n) {
+  if (!type) throw Error(STB_EINVAL, "element type is NULL");
+  const std::string t(type), nm(name ? name : "");
+  auto need = [&](int k) {
+    if (n < k || (k > 0 && !a))
+      throw Error(STB_EINVAL, t + " needs " + std::to_string(k) + " constructor arguments, got " + std::to_string(n));
+  };
+  if (t == "DRIFT") { need(1); return new DRIFT(nm, a[0]); }
+  if (t == "MARKER") { need(1); return new MARKER(nm, a[0]); }
+  if (t == "SBEND") { need(4); return new SBEND(nm, a[0], a[1], a[2], a[3]); }
+  if (t == "GSBEND") { need(5); return new GSBEND(nm, a[0], a[1], a[2], a[3], a[4]); }
+  if (t == "QUAD") { need(3); return new QUAD(nm, a[0], a[1], a[2]); }
+  if (t == "SKEWQ") { need(2); return new SKEWQ(nm, a[0], a[1]); }
+  if (t == "SEXT") { need(3); return new SEXT(nm, a[0], a[1], a[2]); }
+  if (t == "OCT") { need(3); return new OCT(nm, a[0], a[1], a[2]); }
+  if (t == "MULT") { need(23); return new MULT(nm, a[0], a + 1, a + 12); }
+  if (t == "GMULT") { need(26); return new GMULT(nm, a[0], a[1], a[2], a[3], a + 4, a + 15); }
+  if (t == "SBENDMULT") { need(26); return new SBENDMULT(nm, a[0], a[1], a[2], a[3], a + 4, a + 15); }
+  if (t == "KICKER") { need(3); return new KICKER(nm, a[0], a[1], a[2]); }
+  if (t == "HKICKER") { need(2); return new HKICKER(nm, a[0], a[1]); }
+  if (t == "VKICKER") { need(2); return new VKICKER(nm, a[0], a[1]); }
+  if (t == "RFCAV") { need(4); return new RFCAV(nm, a[0], a[1], a[2], a[3]); }
+  if (t == "CRABRF") { need(4); return new CRABRF(nm, a[0], a[1], a[2], a[3]); }
+  if (t == "CCMULT") {
+    need(12);
+    return new CCMULT(nm, a[0], a[1], a[2], a[3], a[4], a[5], a[6], a[7], a[8], a[9], a[10], a[11]);
+  }
+  if (t == "LBT") { need(1); return new LBT(nm, a[0]); }
+  if (t == "ILBT") { need(1); return new ILBT(nm, a[0]); }
+  if (t == "BEAMBEAM") {
+    need(11);
+    const int treatment = (int)a[0];
+    if (treatment != 4 && treatment != 6) throw Error(STB_EINVAL, "Error: beambeam treatment only can be 4 or 6");
+    return new BEAMBEAM(nm, treatment, a[1], a[2], a[3], (int)a[4], a[5], a[6], a[7], a[8], a[9], a[10]);
+  }
+  throw Error(STB_EUNSUPPORTED, "element type " + t + " is not supported");
+}
+
+Element *E(stb_element *e) { return reinterpret_cast<Element *>(e); }
+const Element *E(const stb_element *e) { return reinterpret_cast<const Element *>(e); }
+Line *Lp(stb_line *l) { return reinterpret_cast<Line *>(l); }
+const Line *Lp(const stb_line *l) { return reinterpret_cast<const Line *>(l); }
+
+void table_destroy(stb_table *t) {
+  if (!t) return;
+  int prev = -1;
+  cudaGetDevice(&prev);
+  cudaSetDevice(t->device);
+  if (t->d_hdr) cudaFree(t->d_hdr);
+  if (t->d_pool) cudaFree(t->d_pool);
+  if (t->d_status) cudaFree(t->d_status);
+  if (prev >= 0) cudaSetDevice(prev);
+  delete t;
+}
+
+stb_table *table_build(const Line &line, int device) {
+  std::unique_ptr<stb_table, void (*)(stb_table *)> t(new stb_table(), table_destroy);
+  t->device = device;
+  t->host = flatten(line);
+  if (t->host.hdr.empty()) throw Error(STB_EINVAL, "line has no elements");
+  DeviceGuard g(device);
+  std::vector<double> pool = t->host.pool;
+  pool.resize((pool.size() + 1) & ~size_t(1), 0.0);  // 16-byte multiple for the bulk copy
+  if (pool.empty()) pool.assign(2, 0.0);
+  t->npool_padded = (int)pool.size();
+  const size_t hb = t->host.hdr.size() * sizeof(ElemHeader), pb = pool.size() * sizeof(double);
+  cuda_check(cudaMalloc(&t->d_hdr, hb), "cudaMalloc(element headers)");
+  cuda_check(cudaMalloc(&t->d_pool, pb), "cudaMalloc(parameter pool)");
+  cuda_check(cudaMalloc(&t->d_status, sizeof(int)), "cudaMalloc(status)");
+  cuda_check(cudaMemcpy(t->d_hdr, t->host.hdr.data(), hb, cudaMemcpyHostToDevice), "upload headers");
+  cuda_check(cudaMemcpy(t->d_pool, pool.data(), pb, cudaMemcpyHostToDevice), "upload pool");
+  cuda_check(cudaMemset(t->d_status, 0, sizeof(int)), "clear status");
+  cuda_check(cudaDeviceGetAttribute(&t->num_sms, cudaDevAttrMultiProcessorCount, device), "SM count");
+  const size_t need = track_smem_bytes((int)t->host.hdr.size(), t->npool_padded);
+  t->use_smem = (long)need <= (long)track_smem_limit(device);
+  return t.release();
+}
+
+TrackArgs make_args(stb_table *t) {
+  TrackArgs a{};
+  a.hdr = t->d_hdr;
+  a.pool = t->d_pool;
+  a.nelem = (int)t->host.hdr.size();
+  a.npool_padded = t->npool_padded;
+  a.ref = t->host.ref;
+  a.status = t->d_status;
+  return a;
+}
+
+int track_device(stb_table *t, double *x, double *px, double *y, double *py, double *z, double *pt, long n,
+                 int turn0, int nturn, double radius, int32_t *lost_turn, int32_t *lost_elem, cudaStream_t s,
+                 double *dump = nullptr) {
+  if (!t) throw Error(STB_EINVAL, "table is NULL");
+  if (n < 0 || nturn < 0 || turn0 < 0) throw Error(STB_EINVAL, "negative particle count or turn");
+  if (n == 0 || nturn == 0) return STB_OK;
+  if (!x || !px || !y || !py || !z || !pt || !lost_turn || !lost_elem)
+    throw Error(STB_EINVAL, "coordinate or loss array is NULL");
+  DeviceGuard g(t->device);
+  TrackArgs a = make_args(t);
+  a.x = x; a.px = px; a.y = y; a.py = py; a.z = z; a.pt = pt;
+  a.n = n;
+  a.turn0 = turn0;
+  a.nturn = nturn;
+  a.r2 = radius > 0.0 ? radius * radius : 0.0;
+  a.lost_turn = lost_turn;
+  a.lost_elem = lost_elem;
+  a.dump = dump;
+  cuda_check(launch_track(a, t->num_sms, t->use_smem, s), "track kernel launch");
+  return STB_OK;
+}
+
+// Host AoS -> device SoA, track, back; Track()'s stable/lost_turn/lost_post outputs.
+int track_host(stb_table *t, double *xa, long n, int nturn, double radius, int *stable, int *lost_turn,
+               int *lost_post, double *dump_host = nullptr) {
+  if (!t) throw Error(STB_EINVAL, "table is NULL");
+  if (n < 0 || nturn < 0) throw Error(STB_EINVAL, "negative particle count or turn count");
+  if (n == 0) return STB_OK;
+  if (!xa || !stable || !lost_turn || !lost_post) throw Error(STB_EINVAL, "NULL host buffer");
+  DeviceGuard g(t->device);
+  std::vector<double> soa((size_t)n * 6);
+  std::vector<int32_t> lt((size_t)n), le((size_t)n, 0);
+  for (long i = 0; i < n; i++) {
+    for (int k = 0; k < 6; k++) soa[(size_t)k * n + i] = xa[6 * i + k];
+    lt[i] = stable[i] == 0 ? 0 : -1;  // Track(): stable == 0 on entry -> lost at turn 0, post 0
+  }
+  double *d = nullptr;
+  int32_t *dl = nullptr;
+  cuda_check(cudaMalloc(&d, sizeof(double) * 6 * n), "cudaMalloc(coordinates)");
+  struct Free {
+    void *p;
+    ~Free() { if (p) cudaFree(p); }
+  } f1{d};
+  cuda_check(cudaMalloc(&dl, sizeof(int32_t) * 2 * n), "cudaMalloc(loss arrays)");
+  Free f2{dl};
+  cuda_check(cudaMemcpy(d, soa.data(), sizeof(double) * 6 * n, cudaMemcpyHostToDevice), "upload coordinates");
+  cuda_check(cudaMemcpy(dl, lt.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice), "upload loss state");
+  cuda_check(cudaMemcpy(dl + n, le.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice), "upload loss state");
+  cuda_check(cudaMemset(t->d_status, 0, sizeof(int)), "clear status");
+  double *dd = nullptr;
+  const size_t dump_n = dump_host ? (size_t)n * nturn * t->host.hdr.size() * 6 : 0;
+  if (dump_host) {
+    cuda_check(cudaMalloc(&dd, sizeof(double) * dump_n), "cudaMalloc(probe)");
+    // Entries after a loss keep their previous content, as in the oracle probe.
+    cuda_check(cudaMemcpy(dd, dump_host, sizeof(double) * dump_n, cudaMemcpyHostToDevice), "upload probe");
+  }
+  Free f3{dd};
+  if (nturn > 0)
+    track_device(t, d, d + n, d + 2 * n, d + 3 * n, d + 4 * n, d + 5 * n, n, 0, nturn, radius, dl, dl + n, 0, dd);
+  cuda_check(cudaDeviceSynchronize(), "track kernel");
+  if (dump_host)
+    cuda_check(cudaMemcpy(dump_host, dd, sizeof(double) * dump_n, cudaMemcpyDeviceToHost), "download probe");
+  int st = 0;
+  cuda_check(cudaMemcpy(&st, t->d_status, sizeof(int), cudaMemcpyDeviceToHost), "read status");
+  if (st != 0) throw Error(st, "tracking kernel reported status " + std::to_string(st));
+  cuda_check(cudaMemcpy(soa.data(), d, sizeof(double) * 6 * n, cudaMemcpyDeviceToHost), "download coordinates");
+  cuda_check(cudaMemcpy(lt.data(), dl, sizeof(int32_t) * n, cudaMemcpyDeviceToHost), "download loss state");
+  cuda_check(cudaMemcpy(le.data(), dl + n, sizeof(int32_t) * n, cudaMemcpyDeviceToHost), "download loss state");
+  for (long i = 0; i < n; i++) {
+    for (int k = 0; k < 6; k++) xa[6 * i + k] = soa[(size_t)k * n + i];
+    if (lt[i] < 0) {
+      stable[i] = 1; lost_turn[i] = 0; lost_post[i] = 0;
+    } else {
+      stable[i] = 0; lost_turn[i] = lt[i]; lost_post[i] = le[i];
+    }
+  }
+  return STB_OK;
+}
+
+}  // namespace
+
+// ---- C++ Track entry points ----
+void Track_Batch(Line &line, double *x, long n, int nturn, int *stable, int *lost_turn, int *lost_post,
+                 const TrackOptions &opt) {
+  std::unique_ptr<stb_table, void (*)(stb_table *)> t(table_build(line, opt.device), table_destroy);
+  int rc = track_host(t.get(), x, n, nturn, opt.aperture_radius, stable, lost_turn, lost_post);
+  if (rc != STB_OK) throw Error(rc, last_error());
+}
+
+void Track(Line &line, double x[], int nturn, int &stable, int &lost_turn, int &lost_post) {
+  Track_Batch(line, x, 1, nturn, &stable, &lost_turn, &lost_post);
+}
+
+void Track_Spin(Line &line, double x[], int nturn, int &stable, int &lost_turn, int &lost_post) {
+  (void)line; (void)x; (void)nturn; (void)stable; (void)lost_turn; (void)lost_post;
+  throw Error(STB_EUNSUPPORTED, "spin tracking is not available in this build");
+}
+
+}  // namespace stb
+
+using namespace stb;
+
+extern "C" {
+
+const char *stb_last_error(void) { return stb::last_error(); }
+int stb_version(void) { return 100; }
+
+int stb_set_ref_energy(double gamma, double E0, double Q, double A) {
+  return guarded([&] {
+    if (!(gamma >= 1.0)) throw Error(STB_EINVAL, "gamma must be >= 1");
+    Set_RefPartEnergy(gamma, E0, Q, A);
+    return STB_OK;
+  });
+}
+int stb_set_spin_g(double g) {
+  return guarded([&] { Set_Spin_G(g); return STB_OK; });
+}
+int stb_set_flags(int h_expand, int quad_fringe) {
+  return guarded([&] {
+    GP.H_expand = h_expand != 0;
+    GP.quad_fringe = quad_fringe != 0;
+    return STB_OK;
+  });
+}
+int stb_get_ref(double *o) {
+  return guarded([&] {
+    if (!o) throw Error(STB_EINVAL, "NULL output");
+    o[0] = GP.gamma; o[1] = GP.beta; o[2] = GP.energy; o[3] = GP.brho;
+    o[4] = GP.Q; o[5] = GP.energy0; o[6] = GP.G; o[7] = GP.p;
+    return STB_OK;
+  });
+}
+
+int stb_element_new(const char *type, const char *name, const double *args, int nargs, stb_element **out) {
+  return guarded([&] {
+    if (!out) throw Error(STB_EINVAL, "NULL output");
+    *out = reinterpret_cast<stb_element *>(make_element(type, name, args, nargs));
+    return STB_OK;
+  });
+}
+int stb_element_free(stb_element *e) {
+  return guarded([&] { delete E(e); return STB_OK; });
+}
+int stb_element_setp(stb_element *e, const char *pname, double value) {
+  return guarded([&] {
+    if (!e || !pname) throw Error(STB_EINVAL, "NULL element or name");
+    E(e)->SetP(pname, value);
+    return STB_OK;
+  });
+}
+int stb_element_getp(const stb_element *e, const char *pname, double *value) {
+  return guarded([&] {
+    if (!e || !pname || !value) throw Error(STB_EINVAL, "NULL argument");
+    *value = E(e)->GetP(pname);
+    return STB_OK;
+  });
+}
+int stb_element_set_misalign(stb_element *e, double dx, double dy, double ds, double dtheta, double dphi,
+                             double dpsi) {
+  return guarded([&] {
+    if (!e) throw Error(STB_EINVAL, "NULL element");
+    Element *p = E(e);
+    p->DX = dx; p->DY = dy; p->DS = ds; p->DTHETA = dtheta; p->DPHI = dphi; p->DPSI = dpsi;
+    return STB_OK;
+  });
+}
+int stb_element_set_aperture(stb_element *e, double apx, double apy) {
+  return guarded([&] {
+    if (!e) throw Error(STB_EINVAL, "NULL element");
+    E(e)->APx = apx;
+    E(e)->APy = apy;
+    return STB_OK;
+  });
+}
+int stb_element_type(const stb_element *e, char *buf, int cap) {
+  return guarded([&] {
+    if (!e || !buf || cap <= 0) throw Error(STB_EINVAL, "NULL argument");
+    std::strncpy(buf, E(e)->TYPE.c_str(), (size_t)cap - 1);
+    buf[cap - 1] = 0;
+    return STB_OK;
+  });
+}
+
+int stb_line_new(stb_line **out) {
+  return guarded([&] {
+    if (!out) throw Error(STB_EINVAL, "NULL output");
+    *out = reinterpret_cast<stb_line *>(new Line());
+    return STB_OK;
+  });
+}
+int stb_line_free(stb_line *l) {
+  return guarded([&] { delete Lp(l); return STB_OK; });
+}
+int stb_line_append(stb_line *l, stb_element *e) {
+  return guarded([&] {
+    if (!l || !e) throw Error(STB_EINVAL, "NULL line or element");
+    Lp(l)->Append(E(e));
+    return STB_OK;
+  });
+}
+int stb_line_insert(stb_line *l, long i, stb_element *e) {
+  return guarded([&] {
+    if (!l || !e) throw Error(STB_EINVAL, "NULL line or element");
+    Lp(l)->Insert((int)i, E(e));
+    return STB_OK;
+  });
+}
+int stb_line_delete(stb_line *l, long i) {
+  return guarded([&] {
+    if (!l) throw Error(STB_EINVAL, "NULL line");
+    Lp(l)->Delete((int)i);
+    return STB_OK;
+  });
+}
+int stb_line_replace(stb_line *l, long i, stb_element *e) {
+  return guarded([&] {
+    if (!l || !e) throw Error(STB_EINVAL, "NULL line or element");
+    Lp(l)->Replace((int)i, E(e));
+    return STB_OK;
+  });
+}
+int stb_line_rewind(stb_line *l, long i) {
+  return guarded([&] {
+    if (!l) throw Error(STB_EINVAL, "NULL line");
+    Lp(l)->Rewind((int)i);
+    return STB_OK;
+  });
+}
+int stb_line_invert(stb_line *l) {
+  return guarded([&] {
+    if (!l) throw Error(STB_EINVAL, "NULL line");
+    Lp(l)->Invert();
+    return STB_OK;
+  });
+}
+long stb_line_ncell(const stb_line *l) { return l ? Lp(l)->Ncell : -1; }
+double stb_line_length(const stb_line *l) { return l ? Lp(l)->Length : NAN; }
+int stb_line_cell(stb_line *l, long i, stb_element **out) {
+  return guarded([&] {
+    if (!l || !out) throw Error(STB_EINVAL, "NULL argument");
+    if (i < 0 || i >= (long)Lp(l)->Cell.size()) throw Error(STB_EINVAL, "cell index out of range");
+    *out = reinterpret_cast<stb_element *>(Lp(l)->Cell[(size_t)i]);
+    return STB_OK;
+  });
+}
+
+int stb_table_create(const stb_line *l, int device, stb_table **out) {
+  return guarded([&] {
+    if (!l || !out) throw Error(STB_EINVAL, "NULL argument");
+    *out = table_build(*Lp(l), device);
+    return STB_OK;
+  });
+}
+int stb_table_free(stb_table *t) {
+  return guarded([&] { table_destroy(t); return STB_OK; });
+}
+int stb_table_info(const stb_table *t, double *info) {
+  return guarded([&] {
+    if (!t || !info) throw Error(STB_EINVAL, "NULL argument");
+    info[0] = (double)t->host.hdr.size();
+    info[1] = (double)t->host.pool.size();
+    info[2] = t->host.flops_per_turn;
+    info[3] = t->use_smem ? 1.0 : 0.0;
+    info[4] = (double)track_smem_bytes((int)t->host.hdr.size(), t->npool_padded);
+    return STB_OK;
+  });
+}
+
+int stb_track_device(stb_table *t, double *x, double *px, double *y, double *py, double *z, double *pt, long n,
+                     int turn0, int nturn, double aperture_radius, int32_t *lost_turn, int32_t *lost_elem,
+                     void *stream) {
+  return guarded([&] {
+    return track_device(t, x, px, y, py, z, pt, n, turn0, nturn, aperture_radius, lost_turn, lost_elem,
+                        (cudaStream_t)stream);
+  });
+}
+
+int stb_track_host(stb_table *t, double *x, long n, int nturn, double aperture_radius, int *stable,
+                   int *lost_turn, int *lost_post) {
+  return guarded([&] { return track_host(t, x, n, nturn, aperture_radius, stable, lost_turn, lost_post); });
+}
+
+int stb_track_probe(stb_table *t, double *x, long n, int nturn, double aperture_radius, double *dump, int *stable,
+                    int *lost_turn, int *lost_post) {
+  return guarded([&] {
+    if (!dump) throw Error(STB_EINVAL, "NULL probe buffer");
+    return track_host(t, x, n, nturn, aperture_radius, stable, lost_turn, lost_post, dump);
+  });
+}
+
+}  // extern "C"

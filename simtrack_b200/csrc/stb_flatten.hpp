@@ -1,0 +1,38 @@
+// Line -> device element table (host side).
+#pragma once
+#include <vector>
+
+#include "simtrack_b200.hpp"
+#include "stb_table.hpp"
+
+namespace stb {
+
+struct HostTable {
+  std::vector<ElemHeader> hdr;
+  std::vector<double> pool;
+  RefConsts ref{};
+  // Algorithmic FP64 operations per particle per turn (add/sub/mul/div/sqrt
+  // count 1, each transcendental counts 1), for the element sequence as the
+  // kernel executes it (pt-only invariants evaluated once per refresh).
+  double flops_per_turn = 0.;
+  // Number of per-turn refreshes of the pt-only cache (elements that change pt).
+  int pt_refreshes = 0;
+};
+
+// Flatten `line` against the current reference-particle state GP.
+// Throws stb::Error(STB_EUNSUPPORTED) for element types or settings that
+// the GPU kernel does not implement (radiation, H_expand, pitch/yaw).
+HostTable flatten(const Line &line);
+
+// Yoshida coefficients Fdrift1/Fdrift2/Fkick1/Fkick2 (simtrack.cpp:29-32),
+// computed with the same expressions as the reference.
+struct Yoshida {
+  double d1, d2, k1, k2;
+};
+Yoshida yoshida();
+
+// Inverse standard-normal CDF (Wichura's AS241), used for the strong-bunch
+// slice centroids that the reference obtains from GSL (simtrack.cpp:6614).
+double inverse_normal_cdf(double p);
+
+}  // namespace stb

@@ -1,0 +1,40 @@
+// Kernel launch interfaces shared by the host runtime and the .cu files.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+
+#include "stb_status.hpp"
+#include "stb_table.hpp"
+
+namespace stb {
+
+// CTA sizes of the two kernel variants (table in shared memory / in global memory).
+constexpr int kTrackBlockSmem = 512;
+constexpr int kTrackBlockGlobal = 256;
+
+struct TrackArgs {
+  const ElemHeader *hdr;  // device
+  const double *pool;     // device, padded to a multiple of 2 doubles
+  int nelem;
+  int npool_padded;
+  RefConsts ref;
+  double *x, *px, *y, *py, *z, *pt;  // SoA, n entries
+  long n;
+  int turn0;   // global index of the first turn of this block
+  int nturn;   // turns in this block
+  double r2;   // circular aperture radius squared; 0 disables
+  int32_t *lost_turn;  // < 0 while alive
+  int32_t *lost_elem;
+  int *status;  // device status word (STB_OK or an error code)
+  // Optional per-element probe: when non-NULL, coordinates after every element
+  // are written to dump[((i * nturn + t) * nelem + e) * 6 + k].
+  double *dump;
+};
+
+size_t track_smem_bytes(int nelem, int npool_padded);
+int track_smem_limit(int device);
+cudaError_t launch_track(const TrackArgs &a, int num_sms, bool use_smem, cudaStream_t stream);
+
+}  // namespace stb

@@ -1,0 +1,390 @@
+// Per-element particle maps executed by the tracking kernel.
+//
+// Each map restates one reference pass function (simtrack.cpp line cited per
+// function) with the particle held in registers.  Operand order matches the
+// reference expression by expression and this translation unit is compiled
+// with -fmad=false, so every +, -, *, / and sqrt rounds exactly as in the
+// reference's x86-64 build; only the transcendentals (asin, sin, cos, exp,
+// pow) come from CUDA's library instead of glibc.
+//
+// Quantities that depend only on pt (delta, gamma, beta of the particle) are
+// held in a PtCache and recomputed only when an element changes pt (RF,
+// crab cavities, beam-beam, Lorentz boosts).  The reference recomputes them
+// inside every DRIFT_Pass; the values are identical because kicks and drifts
+// never modify pt.
+#pragma once
+#include <cstdint>
+
+#include "stb_table.hpp"
+
+namespace stb {
+
+struct Particle {
+  double x, px, y, py, z, pt;
+};
+
+struct PtCache {
+  double opd;    // 1.0 + delta1
+  double opd2;   // (1.0 + delta1) * (1.0 + delta1)
+  double beta1;  // particle velocity / c
+};
+
+// delta1/gamma1/beta1 exactly as DRIFT_Pass computes them (simtrack.cpp:3755-3757).
+__device__ __forceinline__ void pt_refresh(const RefConsts &R, double pt, PtCache &c) {
+  const double delta1 = sqrt(1.0 + 2 * pt / R.beta + pt * pt) - 1.0;
+  const double gamma1 = R.gamma + R.sqrt_g2m1 * pt;
+  c.beta1 = sqrt(1.0 - 1.0 / gamma1 / gamma1);
+  c.opd = 1.0 + delta1;
+  c.opd2 = c.opd * c.opd;
+}
+
+// DRIFT_Pass exact branch, simtrack.cpp:3759-3764.  L and Lb = L/GP.beta.
+__device__ __forceinline__ void drift(Particle &p, const PtCache &c, double L, double Lb) {
+  const double pz = sqrt(c.opd2 - p.px * p.px - p.py * p.py);
+  const double betaz = pz * c.beta1 / c.opd;
+  p.x = p.x + p.px * L / pz;
+  p.y = p.y + p.py * L / pz;
+  p.z = p.z - (L / betaz - Lb);
+}
+
+// sbend_exact_pass, simtrack.cpp:3833-3858.  B = [L, L/beta, href, 1/href, cosA, sinA].
+__device__ __forceinline__ void bend_exact(Particle &p, const PtCache &c, const double *B) {
+  const double L = B[0], Lb = B[1], href = B[2], invh = B[3], cosA = B[4], sinA = B[5];
+  const double x0 = p.x, px0 = p.px, py0 = p.py;
+  const double pz0 = sqrt(c.opd2 - px0 * px0 - py0 * py0);
+  const double npx = px0 * cosA + (pz0 - 1. - href * x0) * sinA;
+  const double pz1 = sqrt(c.opd2 - npx * npx - py0 * py0);
+  const double der = (-px0) * sinA * href + (pz0 - 1. - x0 * href) * cosA * href;
+  p.x = pz1 / href - der / href / href - invh;
+  const double temp = sqrt(c.opd2 - py0 * py0);
+  const double as1 = asin(px0 / temp);
+  const double as2 = asin(npx / temp);
+  const double das = as1 - as2;
+  p.y = p.y + py0 * L + py0 * das / href;
+  const double t2 = c.opd * L + c.opd * das / href;
+  p.z = p.z - (t2 / c.beta1 - Lb);
+  p.px = npx;
+}
+
+// general_sbend_exact_pass, simtrack.cpp:3974-4010.
+// G = [L, L/beta, rhoc, b0, b0*rhoc, cosA, sinA]
+__device__ __forceinline__ void gbend_exact(Particle &p, const PtCache &c, const double *G) {
+  const double L = G[0], Lb = G[1], rhoc = G[2], b0 = G[3], b0r = G[4], cosA = G[5], sinA = G[6];
+  const double x0 = p.x, px0 = p.px, py0 = p.py;
+  const double pz0 = sqrt(c.opd2 - px0 * px0 - py0 * py0);
+  const double w = pz0 - b0r - b0 * x0;
+  const double npx = px0 * cosA + w * sinA;
+  const double pz1 = sqrt(c.opd2 - npx * npx - py0 * py0);
+  const double der = (-px0) * sinA / rhoc + w * cosA / rhoc;
+  p.x = pz1 / b0 - der * rhoc / b0 - rhoc;
+  const double temp = sqrt(c.opd2 - py0 * py0);
+  const double as1 = asin(px0 / temp);
+  const double as2 = asin(npx / temp);
+  const double das = as1 - as2;
+  p.y = p.y + py0 * L / b0 / rhoc + py0 * das / b0;
+  const double t2 = c.opd * L / b0 / rhoc + c.opd * das / b0;
+  p.z = p.z - (t2 / c.beta1 - Lb);
+  p.px = npx;
+}
+
+// quad_kick_pass, simtrack.cpp:4046-4058
+__device__ __forceinline__ void quad_kick(Particle &p, double kl, double ksl) {
+  const double Bx = ksl * p.x + kl * p.y;
+  const double By = kl * p.x - ksl * p.y;
+  p.px = p.px - By;
+  p.py = p.py + Bx;
+}
+
+// sext_kick_pass, simtrack.cpp:4060-4071
+__device__ __forceinline__ void sext_kick(Particle &p, double kl, double ksl) {
+  const double pr = p.x * p.x - p.y * p.y;
+  const double pi = 2. * p.x * p.y;
+  const double Bx = (ksl * pr + kl * pi) / 2.;
+  const double By = (kl * pr - ksl * pi) / 2.;
+  p.px = p.px - By;
+  p.py = p.py + Bx;
+}
+
+// oct_kick_pass, simtrack.cpp:4073-4084
+__device__ __forceinline__ void oct_kick(Particle &p, double kl, double ksl) {
+  const double pr = p.x * p.x * p.x - 3 * p.x * p.y * p.y;
+  const double pi = 3 * p.x * p.x * p.y - p.y * p.y * p.y;
+  const double Bx = (ksl * pr + kl * pi) / 6.;
+  const double By = (kl * pr - ksl * pi) / 6.;
+  p.px = p.px - By;
+  p.py = p.py + Bx;
+}
+
+// mult_kick_pass, simtrack.cpp:4086-4111.  K = [KNL0, KNSL0, (KNLi, KNSLi) i=1..norder]
+__device__ __forceinline__ void mult_kick(Particle &p, int norder, const double *K) {
+  double Xn = 1., Yn = 0.;
+  double By = K[0], Bx = K[1];
+  int fac = 1;
+  for (int i = 1; i <= norder; i++) {
+    const double Xn0 = Xn, Yn0 = Yn;
+    Xn = Xn0 * p.x - Yn0 * p.y;
+    Yn = Xn0 * p.y + Yn0 * p.x;
+    fac = fac * i;
+    const double kn = K[2 * i], ks = K[2 * i + 1];
+    if (kn != 0. || ks != 0.) {
+      const double f = (double)fac;
+      By = By + (kn * Xn - ks * Yn) / f;
+      Bx = Bx + (kn * Yn + ks * Xn) / f;
+    }
+  }
+  p.px = p.px - By;
+  p.py = p.py + Bx;
+}
+
+// Hard-edge quadrupole fringe maps, simtrack.cpp:4906-4920 (entry) and 4948-4956 (exit).
+__device__ __noinline__ void quad_fringe(Particle &p, double k, bool entry) {
+  const double x0 = p.x, px0 = p.px, y0 = p.y, py0 = p.py, z0 = p.z, d0 = p.pt;
+  const double a = k * (x0 * x0 * x0 + 3 * x0 * y0 * y0) / 12 / (1 + d0);
+  const double b = k * ((x0 * x0 + y0 * y0) * px0 - 2 * x0 * y0 * py0) / 4 / (1 + d0);
+  const double cc = k * (3 * x0 * x0 * y0 + y0 * y0 * y0) / 12 / (1 + d0);
+  const double d = k * ((x0 * x0 + y0 * y0) * py0 - 2 * x0 * y0 * px0) / 4 / (1 + d0);
+  const double e = k * (y0 * y0 * y0 * py0 - x0 * x0 * x0 * px0 + 3 * x0 * x0 * y0 * py0 - 3 * y0 * y0 * x0 * px0) /
+                   12 / (1 + d0) / (1 + d0);
+  if (entry) {
+    p.x = x0 + a; p.px = px0 - b; p.y = y0 - cc; p.py = py0 + d; p.z = z0 + e;
+  } else {
+    p.x = x0 - a; p.px = px0 + b; p.y = y0 + cc; p.py = py0 - d; p.z = z0 - e;
+  }
+}
+
+// GtoL1 / LtoG1, simtrack.cpp:3443-3481.  M = [dx, dy, cos(dpsi), sin(dpsi)]
+__device__ __forceinline__ void gtol1(Particle &p, const double *M, int flags) {
+  if (flags & EF_MISALIGN_OFFSET) {
+    p.x = p.x - M[0];
+    p.y = p.y - M[1];
+  }
+  if (flags & EF_MISALIGN_ROLL) {
+    const double c = M[2], s = M[3];
+    const double t0 = p.x, t1 = p.px, t2 = p.y, t3 = p.py;
+    p.x = c * t0 + s * t2;
+    p.px = c * t1 + s * t3;
+    p.y = c * t2 - s * t0;
+    p.py = c * t3 - s * t1;
+  }
+}
+__device__ __forceinline__ void ltog1(Particle &p, const double *M, int flags) {
+  if (flags & EF_MISALIGN_ROLL) {
+    const double c = M[2], s = M[3];
+    const double t0 = p.x, t1 = p.px, t2 = p.y, t3 = p.py;
+    p.x = c * t0 - s * t2;
+    p.px = c * t1 - s * t3;
+    p.y = s * t0 + c * t2;
+    p.py = s * t1 + c * t3;
+  }
+  if (flags & EF_MISALIGN_OFFSET) {
+    p.x = p.x + M[0];
+    p.y = p.y + M[1];
+  }
+}
+
+// cerrf (Faddeeva w(z)), simtrack.cpp:6258-6323.  The reference fills
+// rx[n], ry[n] for n = nu..1 and then consumes them for n = nc..1 with
+// nc < nu; both loops run downwards, so the two are fused here and the
+// arrays are not materialised.  Values are unchanged.
+__device__ __noinline__ void cerrf_dev(double xx, double yy, double &wx, double &wy) {
+  const double cc = 1.12837916709551, xlim = 5.33, ylim = 4.29, fac1 = 3.2, fac2 = 23, fac3 = 21;
+  const double x = fabs(xx), y = fabs(yy);
+  if (y < ylim && x < xlim) {
+    const double q = (1. - y / ylim) * sqrt(1. - (x / xlim) * (x / xlim));
+    const double h = 1. / (fac1 * q);
+    const int nc = 7 + int(fac2 * q);
+    double xl = pow(h, (double)(1 - nc));
+    const double xh = y + .5 / h;
+    const double yh = x;
+    const int nu = 10 + int(fac3 * q);
+    double rxn = 0., ryn = 0., sx = 0., sy = 0.;
+    for (int n = nu; n >= 1; n--) {
+      const double tx = xh + n * rxn;
+      const double ty = yh - n * ryn;
+      const double tn = tx * tx + ty * ty;
+      rxn = .5 * tx / tn;
+      ryn = .5 * ty / tn;
+      if (n <= nc) {
+        const double saux = sx + xl;
+        sx = rxn * saux - ryn * sy;
+        sy = rxn * sy + ryn * saux;
+        xl = h * xl;
+      }
+    }
+    wx = cc * sx;
+    wy = cc * sy;
+  } else {
+    const double xh = y, yh = x;
+    double rx = 0., ry = 0.;
+    for (int n = 9; n >= 1; n--) {
+      const double tx = xh + n * rx;
+      const double ty = yh - n * ry;
+      const double tn = tx * tx + ty * ty;
+      rx = .5 * tx / tn;
+      ry = .5 * ty / tn;
+    }
+    wx = cc * rx;
+    wy = cc * ry;
+  }
+  if (yy < 0.) {
+    wx = 2. * exp(y * y - x * x) * cos(2. * x * y) - wx;
+    wy = -2. * exp(y * y - x * x) * sin(2. * x * y) - wy;
+    if (xx > 0.) wy = -wy;
+  } else {
+    if (xx < 0.) wy = -wy;
+  }
+}
+
+// BB4D (x, y, gamma, N, sigmax, sigmay) overload, simtrack.cpp:6325-6377.
+// c4 = 2*N*rp/gamma (the constant prefix of temp1).
+__device__ __forceinline__ void bb4d(double x, double y, double c4, double sigmax, double sigmay, double &Dpx,
+                                     double &Dpy) {
+  const double PI = 3.14159265358979323;
+  const double signx = (x >= 0.0) ? 1. : -1.;
+  const double signy = (y >= 0.0) ? 1. : -1.;
+  if (x == 0. && y == 0.) {
+    Dpx = 0.;
+    Dpy = 0.;
+  } else if (fabs(sigmax - sigmay) / sigmax < 1.0e-6) {
+    const double r2 = x * x + y * y;
+    const double temp1 = c4 / r2;
+    const double temp2 = 1 - exp(-r2 / 2 / sigmax / sigmax);
+    Dpx = temp1 * x * temp2;
+    Dpy = temp1 * y * temp2;
+  } else if (sigmax > sigmay) {
+    const double temp1 = c4 * sqrt(PI / 2. / (sigmax * sigmax - sigmay * sigmay));
+    const double temp2 = exp(-x * x / 2. / sigmax / sigmax - y * y / 2. / sigmay / sigmay);
+    const double temp3 = sqrt(2. * (sigmax * sigmax - sigmay * sigmay));
+    double w1r, w1i, w2r, w2i;
+    const double x1 = fabs(x) / temp3, y1 = fabs(y) / temp3;
+    const double x2 = fabs(x) * sigmay / sigmax / temp3, y2 = fabs(y) * sigmax / sigmay / temp3;
+    cerrf_dev(x1, y1, w1r, w1i);
+    cerrf_dev(x2, y2, w2r, w2i);
+    Dpy = temp1 * (w1r - temp2 * w2r) * signy;
+    Dpx = temp1 * (w1i - temp2 * w2i) * signx;
+  } else if (sigmax < sigmay) {
+    const double temp1 = c4 * sqrt(PI / 2 / (sigmay * sigmay - sigmax * sigmax));
+    const double temp2 = exp(-x * x / 2 / sigmax / sigmax - y * y / 2 / sigmay / sigmay);
+    const double temp3 = sqrt(2 * (sigmay * sigmay - sigmax * sigmax));
+    double w1r, w1i, w2r, w2i;
+    const double x1 = fabs(x) / temp3, y1 = fabs(y) / temp3;
+    const double x2 = fabs(x) * sigmay / sigmax / temp3, y2 = fabs(y) * sigmax / sigmay / temp3;
+    cerrf_dev(y1, x1, w1r, w1i);
+    cerrf_dev(y2, x2, w2r, w2i);
+    Dpy = temp1 * (w1i - temp2 * w2i) * signy;
+    Dpx = temp1 * (w1r - temp2 * w2r) * signx;
+  } else {
+    // sigmax or sigmay is NaN: the reference leaves Dpx/Dpy unset; NaN marks the particle lost.
+    Dpx = __longlong_as_double(0x7ff8000000000000LL);
+    Dpy = Dpx;
+  }
+}
+
+// BB6D, simtrack.cpp:6622-6677 (slice loop).  P layout (built by the flattener):
+// [bbscale, emitx, emity, betax*, alfx*, betay*, alfy*, gx*, gy*, 2*emitx, 2*emity,
+//  temp3, c4, z_star[0..N-1]]
+__device__ __noinline__ void bb6d(Particle &p, const double *P, int nslice) {
+  const double bbscale = P[0], emitx = P[1], emity = P[2];
+  const double betax_s = P[3], alfx_s = P[4], betay_s = P[5], alfy_s = P[6];
+  const double gx = P[7], gy = P[8], e2x = P[9], e2y = P[10], t3 = P[11], c4 = P[12];
+  const double *zs = P + 13;
+  for (int i = 0; i < nslice; i++) {
+    const Particle q = p;
+    const double S = (q.z - zs[i]) / 2.0;
+    const double betax = betax_s + 2 * S * alfx_s + S * S * gx;
+    const double betay = betay_s + 2 * S * alfy_s + S * S * gy;
+    const double sigmax = sqrt(emitx * betax);
+    const double sigmay = sqrt(emity * betay);
+    const double dsx = e2x * (alfx_s + S * gx);
+    const double dsy = e2y * (alfy_s + S * gy);
+    const double X = q.x + q.px * S;
+    const double Y = q.y + q.py * S;
+    double Dpx, Dpy;
+    bb4d(X, Y, c4, sigmax, sigmay, Dpx, Dpy);
+    const double temp1 = 1.0 / 2. / (sigmax * sigmax - sigmay * sigmay);
+    const double temp2 = X * Dpx + Y * Dpy;
+    const double temp4 = exp(-X * X / 2. / sigmax / sigmax - Y * Y / 2. / sigmay / sigmay);
+    p.x = q.x - S * Dpx * bbscale;
+    p.px = q.px + Dpx * bbscale;
+    p.y = q.y - S * Dpy * bbscale;
+    p.py = q.py + Dpy * bbscale;
+    const double kx = 0.5 * Dpx * bbscale * (q.px + 0.5 * Dpx * bbscale);
+    const double ky = 0.5 * Dpy * bbscale * (q.py + 0.5 * Dpy * bbscale);
+    if (fabs(sigmax - sigmay) / sigmax < 1.0e-6) {
+      p.pt = q.pt + kx + ky + (1.0 / sigmax / sigmax) * dsx * (t3 * bbscale / 4.) * temp4;
+    } else {
+      const double dUx = temp1 * bbscale * (temp2 + t3 * (sigmay / sigmax * temp4 - 1.));
+      const double dUy = -temp1 * bbscale * (temp2 + t3 * (sigmax / sigmay * temp4 - 1.));
+      p.pt = q.pt + kx + ky - (0.5 * dsx * dUx + 0.5 * dsy * dUy);
+    }
+  }
+}
+
+// LBT_Pass, simtrack.cpp:6069-6093.  P = [sin, cos, tan]
+__device__ __noinline__ void lbt(Particle &p, const double *P) {
+  const double st = P[0], ct = P[1], tt = P[2];
+  const double x0 = p.x, px0 = p.px, y0 = p.y, py0 = p.py, z0 = p.z, pz0 = p.pt;
+  const double ps0 = sqrt((1 + pz0) * (1 + pz0) - px0 * px0 - py0 * py0);
+  const double h0 = (1 + pz0) - ps0;
+  const double pxs = (px0 - tt * h0) / ct;
+  const double pys = py0 / ct;
+  const double pzs = pz0 - tt * px0 + tt * tt * h0;
+  const double pss = sqrt((1 + pzs) * (1 + pzs) - pxs * pxs - pys * pys);
+  const double hs = (1 + pzs) - pss;
+  p.x = tt * z0 + (1 + (pxs / pss) * st) * x0;
+  p.y = y0 + st * (pys / pss) * x0;
+  p.z = z0 / ct + (-hs / pss) * st * x0;
+  p.px = pxs;
+  p.py = pys;
+  p.pt = pzs;
+}
+
+// ILBT_Pass, simtrack.cpp:6095-6123.  P = [sin, cos]
+__device__ __noinline__ void ilbt(Particle &p, const double *P) {
+  const double st = P[0], ct = P[1];
+  const double xs = p.x, pxs = p.px, ys = p.y, pys = p.py, zs = p.z, pzs = p.pt;
+  const double pss = sqrt((1 + pzs) * (1 + pzs) - pxs * pxs - pys * pys);
+  const double hs = 1 + pzs - pss;
+  const double hxs = pxs / pss, hys = pys / pss, hzs = -hs / pss;
+  const double px0 = (pxs + hs * st) * ct;
+  const double py0 = pys * ct;
+  const double pz0 = pzs + pxs * st;
+  const double x0 = (xs - zs * st) / (1 + hxs * st - hzs * st * st);
+  const double z0 = (zs - hzs * st * x0) * ct;
+  const double y0 = ys - st * hys * x0;
+  p.x = x0; p.px = px0; p.y = y0; p.py = py0; p.z = z0; p.pt = pz0;
+}
+
+// CCMULT_Pass kick part, simtrack.cpp:6037-6064.
+// P = [kf, PHASE0, scale, brho, B2, A2, B3, A3, B4, A4, B5, A5]
+__device__ __noinline__ void ccmult_kick(Particle &p, const double *P) {
+  const double kf = P[0], PHASE0 = P[1], scale = P[2], brho = P[3];
+  const double B2 = P[4], A2 = P[5], B3 = P[6], A3 = P[7], B4 = P[8], A4 = P[9], B5 = P[10], A5 = P[11];
+  const double arg = kf * p.z / 2.99792458e8 + PHASE0;
+  const double sinangle = sin(arg);
+  const double cosangle = cos(arg);
+  const double X = p.x, Y = p.y;
+  const double x2 = X * X, x3 = x2 * X, x4 = x3 * X, x5 = x4 * X;
+  const double y2 = Y * Y, y3 = y2 * Y, y4 = y3 * Y, y5 = y4 * Y;
+  const double xy = X * Y, x2y = x2 * Y, xy2 = X * y2, x2y2 = X * xy2;
+  const double x3y = Y * x3, xy3 = X * y3;
+  const double x2y3 = x2y2 * Y, x3y2 = x2y2 * X, x4y = x4 * Y, xy4 = y4 * X;
+  double px = p.px, py = p.py, pt = p.pt;
+  px = px + (B2 * X + A2 * Y) * cosangle / brho;
+  py = py + (A2 * X - B2 * Y) * cosangle / brho;
+  pt = pt + (B2 * (x2 - y2) * sinangle + A2 * xy * sinangle) * scale;
+  px = px + (B3 * (x2 - y2) + 2 * A3 * xy) * cosangle / brho;
+  py = py + (2 * B3 * xy + A3 * (x2 - y2)) * cosangle / brho;
+  pt = pt + (B3 * (x3 - 3 * xy2) * sinangle + A3 * (3 * x2y - y3) * sinangle) * scale / 3.;
+  px = px + (B4 * (x3 - 3 * xy2) - A4 * (y3 - 3 * x2y)) * cosangle / brho;
+  py = py + (B4 * (y3 - 3 * x2y) + A4 * (x3 - 3 * xy2)) * cosangle / brho;
+  pt = pt + (B4 * (x4 - 6 * x2 * y2 + y4) * sinangle + A4 * (4 * x3y - 4 * xy3) * sinangle) * scale / 4.;
+  px = px + (B5 * (x4 - 6 * x2y2 + y4) + A5 * (4 * x3y - 4 * xy3)) * cosangle / brho;
+  py = py + (B5 * (4 * xy3 - 4 * x3y) + A5 * (x4 - 6 * x2y2 + y4)) * cosangle / brho;
+  pt = pt + (B5 * (x5 - 10 * x3y2 + 5 * xy4) * sinangle + A5 * (5 * x4y - 10 * x2y3 + y5) * sinangle) * scale / 5.;
+  p.px = px;
+  p.py = py;
+  p.pt = pt;
+}
+
+}  // namespace stb

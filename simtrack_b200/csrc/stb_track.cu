@@ -1,0 +1,370 @@
+// FP64 element-by-element tracking kernel for sm_100a.
+//
+// One thread carries one particle through a block of turns with its six
+// coordinates and pt-only cache in registers; particles are stored as SoA
+// FP64 arrays so every load/store of a warp is one coalesced 256-byte
+// transaction per coordinate.  All lanes of a warp walk the same element
+// sequence, so element dispatch is warp-uniform; a lane whose particle is
+// lost leaves the loops and idles until the compaction pass (stb_compact.cu)
+// removes it between turn blocks.
+//
+// The element table (headers + parameter pool, built by stb_flatten.cpp) is
+// staged into shared memory once per CTA with bulk TMA copies
+// (cp.async.bulk, completion on an mbarrier, bounded wait) when it fits the
+// shared-memory budget; otherwise the kernel reads it through the read-only
+// data cache.  The Track() loss convention (simtrack.cpp:20791-20814) is
+// applied after every element: |x| > APx, |y| > APy, isnan(x), isnan(y),
+// plus an optional circular aperture.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "stb_kernels.hpp"
+#include "stb_physics.cuh"
+
+namespace stb {
+
+namespace {
+
+constexpr double kPI = 3.14159265358979323;
+constexpr double kC = 2.99792458e8;
+
+// Bulk copy of `bytes` (multiple of 16, both addresses 16-byte aligned) from
+// global to shared memory, completing on `bar`.
+__device__ __forceinline__ void bulk_g2s(void *smem_dst, const void *gsrc, uint32_t bytes, uint64_t *bar) {
+  const uint32_t d = (uint32_t)__cvta_generic_to_shared(smem_dst);
+  const uint32_t b = (uint32_t)__cvta_generic_to_shared(bar);
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(d),
+               "l"(gsrc), "r"(bytes), "r"(b)
+               : "memory");
+}
+
+// Stage headers + pool into shared memory.  Returns false if the bounded
+// wait ran out (the caller then records STB_ETIMEOUT and returns).
+__device__ bool stage_table(const TrackArgs &a, unsigned char *smem, uint64_t *bar) {
+  const uint32_t hbytes = (uint32_t)a.nelem * (uint32_t)sizeof(ElemHeader);
+  const uint32_t pbytes = (uint32_t)a.npool_padded * 8u;
+  const uint32_t total = hbytes + pbytes;
+  const uint32_t b = (uint32_t)__cvta_generic_to_shared(bar);
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(b) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(b), "r"(total) : "memory");
+    constexpr uint32_t kChunk = 32768;
+    for (uint32_t off = 0; off < hbytes; off += kChunk) {
+      const uint32_t n = (hbytes - off) < kChunk ? (hbytes - off) : kChunk;
+      bulk_g2s(smem + off, (const unsigned char *)a.hdr + off, n, bar);
+    }
+    for (uint32_t off = 0; off < pbytes; off += kChunk) {
+      const uint32_t n = (pbytes - off) < kChunk ? (pbytes - off) : kChunk;
+      bulk_g2s(smem + hbytes + off, (const unsigned char *)a.pool + off, n, bar);
+    }
+  }
+  // Bounded wait on phase 0 of the barrier.
+  uint32_t done = 0;
+  for (int iter = 0; iter < (1 << 22); iter++) {
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(b)
+        : "memory");
+    if (done) break;
+  }
+  return done != 0;
+}
+
+__device__ __forceinline__ bool is_lost(const Particle &p, double apx, double apy, double r2) {
+  return fabs(p.x) > apx || fabs(p.y) > apy || isnan(p.x) || isnan(p.y) || (r2 > 0.0 && p.x * p.x + p.y * p.y > r2);
+}
+
+// Runs one element on one particle.  Returns nothing; the caller checks loss.
+__device__ __forceinline__ void apply_element(const ElemHeader &h, const double *P, Particle &p, PtCache &c,
+                                              const RefConsts &R) {
+  const double *M = P;
+  if (h.flags & (EF_MISALIGN_OFFSET | EF_MISALIGN_ROLL)) {
+    gtol1(p, M, h.flags);
+    P += kMisalignParams;
+  }
+  switch (h.op) {
+    case OP_DRIFT:
+      drift(p, c, P[0], P[1]);
+      break;
+    case OP_SBEND:
+      if (h.flags & EF_EDGE1) {
+        p.px = p.px + P[0] * p.x;
+        p.py = p.py - P[0] * p.y;
+      }
+      bend_exact(p, c, P + 2);
+      if (h.flags & EF_EDGE2) {
+        p.px = p.px + P[1] * p.x;
+        p.py = p.py - P[1] * p.y;
+      }
+      break;
+    case OP_GSBEND:
+      if (h.flags & EF_EDGE1) {
+        p.px = p.px + P[0] * p.x;
+        p.py = p.py - P[0] * p.y;
+      }
+      gbend_exact(p, c, P + 2);
+      if (h.flags & EF_EDGE2) {
+        p.px = p.px + P[1] * p.x;
+        p.py = p.py - P[1] * p.y;
+      }
+      break;
+    case OP_QUAD_THICK: {
+      const double d1 = P[0], d1b = P[1], d2 = P[2], d2b = P[3];
+      const double a1 = P[4], s1 = P[5], a2 = P[6], s2 = P[7];
+      if (h.flags & EF_FRINGE) quad_fringe(p, P[8], true);
+      for (int s = 0; s < h.nint; s++) {
+        drift(p, c, d1, d1b);
+        quad_kick(p, a1, s1);
+        drift(p, c, d2, d2b);
+        quad_kick(p, a2, s2);
+        drift(p, c, d2, d2b);
+        quad_kick(p, a1, s1);
+        drift(p, c, d1, d1b);
+      }
+      if (h.flags & EF_FRINGE) quad_fringe(p, P[8], false);
+      break;
+    }
+    case OP_SEXT_THICK: {
+      const double d1 = P[0], d1b = P[1], d2 = P[2], d2b = P[3];
+      const double a1 = P[4], s1 = P[5], a2 = P[6], s2 = P[7];
+      for (int s = 0; s < h.nint; s++) {
+        drift(p, c, d1, d1b);
+        sext_kick(p, a1, s1);
+        drift(p, c, d2, d2b);
+        sext_kick(p, a2, s2);
+        drift(p, c, d2, d2b);
+        sext_kick(p, a1, s1);
+        drift(p, c, d1, d1b);
+      }
+      break;
+    }
+    case OP_OCT_THICK: {
+      const double d1 = P[0], d1b = P[1], d2 = P[2], d2b = P[3];
+      const double a1 = P[4], s1 = P[5], a2 = P[6], s2 = P[7];
+      for (int s = 0; s < h.nint; s++) {
+        drift(p, c, d1, d1b);
+        oct_kick(p, a1, s1);
+        drift(p, c, d2, d2b);
+        oct_kick(p, a2, s2);
+        drift(p, c, d2, d2b);
+        oct_kick(p, a1, s1);
+        drift(p, c, d1, d1b);
+      }
+      break;
+    }
+    case OP_MULT_THICK: {
+      const double d1 = P[0], d1b = P[1], d2 = P[2], d2b = P[3];
+      const int no = h.aux;
+      const double *K1 = P + 4;
+      const double *K2 = K1 + 2 + 2 * no;
+      for (int s = 0; s < h.nint; s++) {
+        drift(p, c, d1, d1b);
+        mult_kick(p, no, K1);
+        drift(p, c, d2, d2b);
+        mult_kick(p, no, K2);
+        drift(p, c, d2, d2b);
+        mult_kick(p, no, K1);
+        drift(p, c, d1, d1b);
+      }
+      break;
+    }
+    case OP_QUAD_KICK:
+      quad_kick(p, P[0], P[1]);
+      break;
+    case OP_SEXT_KICK:
+      sext_kick(p, P[0], P[1]);
+      break;
+    case OP_OCT_KICK:
+      oct_kick(p, P[0], P[1]);
+      break;
+    case OP_MULT_KICK:
+      mult_kick(p, h.aux, P);
+      break;
+    case OP_BENDMULT: {
+      const int no = h.aux;
+      const double *B1 = P + 2, *B2 = P + 8;
+      const double *K1 = P + 14;
+      const double *K2 = K1 + 2 + 2 * no;
+      p.px = p.px + P[0] * p.x;
+      p.py = p.py - P[0] * p.y;
+      for (int s = 0; s < h.nint; s++) {
+        bend_exact(p, c, B1);
+        mult_kick(p, no, K1);
+        bend_exact(p, c, B2);
+        mult_kick(p, no, K2);
+        bend_exact(p, c, B2);
+        mult_kick(p, no, K1);
+        bend_exact(p, c, B1);
+      }
+      p.px = p.px + P[1] * p.x;
+      p.py = p.py - P[1] * p.y;
+      break;
+    }
+    case OP_KICK:
+      drift(p, c, P[0], P[1]);
+      p.px = p.px + P[2];
+      p.py = p.py + P[3];
+      drift(p, c, P[0], P[1]);
+      break;
+    case OP_RFCAV: {
+      // RFCAV_Pass, simtrack.cpp:6008-6010
+      drift(p, c, P[0], P[1]);
+      const double absvq = P[2], kf = P[3], phase0 = P[4];
+      p.pt = p.pt + absvq * sin(kf * p.z / kC + kPI - phase0) / R.beta / R.energy;
+      pt_refresh(R, p.pt, c);
+      drift(p, c, P[0], P[1]);
+      break;
+    }
+    case OP_CRABRF: {
+      // CRABRF_Pass, simtrack.cpp:6020-6023
+      drift(p, c, P[0], P[1]);
+      const double vq = P[2], kf = P[3], phase0 = P[4], kk = P[5];
+      const double arg = kf * p.z / kC + phase0;
+      p.px = p.px - vq * sin(arg) / R.beta / R.energy;
+      p.pt = p.pt - vq * cos(arg) * p.x * kk / R.beta / R.energy;
+      pt_refresh(R, p.pt, c);
+      drift(p, c, P[0], P[1]);
+      break;
+    }
+    case OP_CCMULT:
+      drift(p, c, P[0], P[1]);
+      ccmult_kick(p, P + 2);
+      pt_refresh(R, p.pt, c);
+      drift(p, c, P[0], P[1]);
+      break;
+    case OP_LBT:
+      lbt(p, P);
+      pt_refresh(R, p.pt, c);
+      break;
+    case OP_ILBT:
+      ilbt(p, P);
+      pt_refresh(R, p.pt, c);
+      break;
+    case OP_BB6D:
+      bb6d(p, P, h.nint);
+      pt_refresh(R, p.pt, c);
+      break;
+    case OP_BB4D: {
+      double Dpx, Dpy;
+      bb4d(p.x, p.y, P[0], P[1], P[2], Dpx, Dpy);
+      p.px = p.px + Dpx * P[3];
+      p.py = p.py + Dpy * P[3];
+      break;
+    }
+    default:
+      break;
+  }
+  if (h.flags & (EF_MISALIGN_OFFSET | EF_MISALIGN_ROLL)) ltog1(p, M, h.flags);
+}
+
+template <bool kSmem, int kBlock, bool kDump>
+__global__ void __launch_bounds__(kBlock, 1) track_kernel(const TrackArgs a) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ __align__(8) uint64_t bar;
+  const ElemHeader *hdr = a.hdr;
+  const double *pool = a.pool;
+  if (kSmem) {
+    if (!stage_table(a, smem, &bar)) {
+      if (threadIdx.x == 0) atomicExch(a.status, STB_ETIMEOUT);
+      return;
+    }
+    hdr = reinterpret_cast<const ElemHeader *>(smem);
+    pool = reinterpret_cast<const double *>(smem + (size_t)a.nelem * sizeof(ElemHeader));
+  }
+  const RefConsts R = a.ref;
+  const long stride = (long)gridDim.x * blockDim.x;
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += stride) {
+    if (a.lost_turn[i] >= 0) continue;
+    Particle p;
+    p.x = a.x[i];
+    p.px = a.px[i];
+    p.y = a.y[i];
+    p.py = a.py[i];
+    p.z = a.z[i];
+    p.pt = a.pt[i];
+    // Track()'s entry quick check, simtrack.cpp:20795-20796
+    if (a.turn0 == 0 && (fabs(p.x) > 0.1 || fabs(p.y) > 0.1)) {
+      a.lost_turn[i] = 0;
+      a.lost_elem[i] = 0;
+      continue;
+    }
+    PtCache c;
+    pt_refresh(R, p.pt, c);
+    int lt = -1, le = 0;
+    for (int t = 0; t < a.nturn && lt < 0; t++) {
+      for (int e = 0; e < a.nelem; e++) {
+        const ElemHeader h = hdr[e];
+        apply_element(h, pool + h.poff, p, c, R);
+        if (kDump) {
+          double *d = a.dump + (((size_t)i * a.nturn + t) * a.nelem + e) * 6;
+          d[0] = p.x; d[1] = p.px; d[2] = p.y; d[3] = p.py; d[4] = p.z; d[5] = p.pt;
+        }
+        if (is_lost(p, h.apx, h.apy, a.r2)) {
+          lt = a.turn0 + t;
+          le = e;
+          break;
+        }
+      }
+    }
+    a.x[i] = p.x;
+    a.px[i] = p.px;
+    a.y[i] = p.y;
+    a.py[i] = p.py;
+    a.z[i] = p.z;
+    a.pt[i] = p.pt;
+    if (lt >= 0) {
+      a.lost_turn[i] = lt;
+      a.lost_elem[i] = le;
+    }
+  }
+}
+
+}  // namespace
+
+size_t track_smem_bytes(int nelem, int npool_padded) {
+  return (size_t)nelem * sizeof(ElemHeader) + (size_t)npool_padded * 8;
+}
+
+int track_smem_limit(int device) {
+  int v = 0;
+  if (cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, device) != cudaSuccess) return 0;
+  return v - 1024;  // static shared memory and the mbarrier
+}
+
+// Persistent grid: as many CTAs as fit on the device at once (never more
+// than the particles need); each CTA strides over the particle range.
+template <bool kSmem, int kBlock, bool kDump>
+static cudaError_t launch_variant(const TrackArgs &a, int num_sms, size_t smem, cudaStream_t stream) {
+  auto kern = track_kernel<kSmem, kBlock, kDump>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  int per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBlock, smem);
+  if (e != cudaSuccess) return e;
+  if (per_sm < 1) return cudaErrorInvalidConfiguration;
+  long need = (a.n + kBlock - 1) / kBlock;
+  long grid = (long)num_sms * per_sm;
+  if (grid > need) grid = need;
+  kern<<<(unsigned)grid, kBlock, smem, stream>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_track(const TrackArgs &a, int num_sms, bool use_smem, cudaStream_t stream) {
+  const size_t sm = track_smem_bytes(a.nelem, a.npool_padded);
+  if (a.dump) {
+    // Per-element probe (diagnostics and parity tests): small particle counts only.
+    if (use_smem) return launch_variant<true, kTrackBlockGlobal, true>(a, num_sms, sm, stream);
+    return launch_variant<false, kTrackBlockGlobal, true>(a, num_sms, 0, stream);
+  }
+  if (use_smem) return launch_variant<true, kTrackBlockSmem, false>(a, num_sms, sm, stream);
+  return launch_variant<false, kTrackBlockGlobal, false>(a, num_sms, 0, stream);
+}
+
+}  // namespace stb

@@ -1,0 +1,237 @@
+"""Test-side bridge to the CPU oracles (test infrastructure only).
+
+* RefOracle: the unmodified SimTrack source compiled with the GSL shim into
+  oracle/_ref/libsimtrack_ref.so (oracle/Makefile); Lines are built with the
+  reference's own constructors and tracked by its own Track().
+* PortOracle: the C restatement oracle/port/simtrack_port.c compiled into
+  oracle/_build/libsimtrack_port.so.
+
+Both consume the same simtrack_b200.lattices.Lattice description the product
+is built from.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+from ctypes import POINTER, c_char_p, c_double, c_int, c_long, c_void_p
+from pathlib import Path
+
+import numpy as np
+
+from simtrack_b200.lattices import Lattice
+
+ROOT = Path(__file__).resolve().parents[1]
+REF_SO = ROOT / "oracle" / "_ref" / "libsimtrack_ref.so"
+PORT_SO = ROOT / "oracle" / "_build" / "libsimtrack_port.so"
+
+PORT_TYPES = ["DRIFT", "MARKER", "SBEND", "GSBEND", "QUAD", "SKEWQ", "SEXT", "OCT", "MULT", "GMULT",
+              "SBENDMULT", "KICKER", "HKICKER", "VKICKER", "RFCAV", "CRABRF", "CCMULT", "LBT", "ILBT", "BEAMBEAM"]
+
+
+def ref_available() -> bool:
+    return REF_SO.exists()
+
+
+def port_available() -> bool:
+    return PORT_SO.exists()
+
+
+class RefOracle:
+    def __init__(self):
+        L = ctypes.CDLL(str(REF_SO))
+        L.ref_line_new.restype = c_void_p
+        L.ref_line_free.argtypes = [c_void_p]
+        L.ref_line_ncell.restype = c_long
+        L.ref_line_ncell.argtypes = [c_void_p]
+        L.ref_line_append.argtypes = [c_void_p, c_char_p, c_char_p, POINTER(c_double), c_int]
+        L.ref_line_setp.argtypes = [c_void_p, c_long, c_char_p, c_double]
+        L.ref_line_getp.argtypes = [c_void_p, c_long, c_char_p]
+        L.ref_line_getp.restype = c_double
+        L.ref_line_set_misalign.argtypes = [c_void_p, c_long] + [c_double] * 6
+        L.ref_line_set_aperture.argtypes = [c_void_p, c_long, c_double, c_double]
+        L.ref_set_ref_energy.argtypes = [c_double] * 4
+        L.ref_set_flags.argtypes = [c_int, c_int]
+        L.ref_get_gp.argtypes = [POINTER(c_double)]
+        L.ref_track.argtypes = [c_void_p, POINTER(c_double), c_long, c_int, POINTER(c_int), POINTER(c_int),
+                                POINTER(c_int)]
+        L.ref_track_circ.argtypes = [c_void_p, POINTER(c_double), c_long, c_int, c_double, POINTER(c_int),
+                                     POINTER(c_int), POINTER(c_int)]
+        L.ref_track_dump.argtypes = [c_void_p, POINTER(c_double), c_int, c_double, POINTER(c_double),
+                                     POINTER(c_int), POINTER(c_int), POINTER(c_int)]
+        L.ref_pinv.argtypes = [c_double]
+        L.ref_pinv.restype = c_double
+        L.ref_pass.argtypes = [c_void_p, c_long, POINTER(c_double)]
+        self.L = L
+        self.line = None
+        self.nelem = 0
+
+    def build(self, lat: Lattice) -> None:
+        L = self.L
+        L.ref_set_ref_energy(lat.gamma, lat.E0, lat.Q, lat.A)
+        L.ref_set_flags(0, int(lat.quad_fringe))
+        if self.line:
+            L.ref_line_free(self.line)
+        self.line = L.ref_line_new()
+        for i, e in enumerate(lat.elements):
+            args = (c_double * len(e.args))(*e.args)
+            rc = L.ref_line_append(self.line, e.type.encode(), e.name.encode(), args, len(e.args))
+            assert rc == 0, f"reference harness rejected {e.type}"
+            for k, v in e.setp.items():
+                L.ref_line_setp(self.line, i, k.encode(), float(v))
+            if e.misalign is not None:
+                L.ref_line_set_misalign(self.line, i, *e.misalign)
+            if e.aperture is not None:
+                L.ref_line_set_aperture(self.line, i, *e.aperture)
+        self.nelem = int(L.ref_line_ncell(self.line))
+        self.radius = lat.aperture_radius
+
+    def gp(self):
+        out = (c_double * 7)()
+        self.L.ref_get_gp(out)
+        return list(out)
+
+    def track(self, x: np.ndarray, nturn: int, radius: float | None = None):
+        """Returns (x_out, stable, lost_turn, lost_post); x is (n,6)."""
+        radius = self.radius if radius is None else radius
+        x = np.ascontiguousarray(x, dtype=np.float64).copy()
+        n = x.shape[0]
+        st = np.ones(n, dtype=np.int32)
+        lt = np.zeros(n, dtype=np.int32)
+        lp = np.zeros(n, dtype=np.int32)
+        P = lambda a, t: a.ctypes.data_as(POINTER(t))
+        if radius > 0:
+            self.L.ref_track_circ(self.line, P(x, c_double), n, nturn, radius, P(st, c_int), P(lt, c_int), P(lp, c_int))
+        else:
+            self.L.ref_track(self.line, P(x, c_double), n, nturn, P(st, c_int), P(lt, c_int), P(lp, c_int))
+        return x, st, lt, lp
+
+    def track_dump(self, x0, nturn: int, radius: float | None = None):
+        radius = self.radius if radius is None else radius
+        x = np.ascontiguousarray(x0, dtype=np.float64).copy()
+        dump = np.full((nturn, self.nelem, 6), np.nan)
+        st, lt, lp = c_int(), c_int(), c_int()
+        self.L.ref_track_dump(self.line, x.ctypes.data_as(POINTER(c_double)), nturn, radius,
+                              dump.ctypes.data_as(POINTER(c_double)), ctypes.byref(st), ctypes.byref(lt),
+                              ctypes.byref(lp))
+        return x, st.value, lt.value, lp.value, dump
+
+    def pinv(self, p: float) -> float:
+        return self.L.ref_pinv(p)
+
+
+class PortElem(ctypes.Structure):
+    _fields_ = [("type", c_int), ("nint", c_int), ("norder", c_int), ("nslice", c_int), ("treatment", c_int),
+                ("pad", c_int), ("L", c_double), ("p", c_double * 16), ("knl", c_double * 11),
+                ("knsl", c_double * 11), ("dx", c_double), ("dy", c_double), ("ds", c_double),
+                ("dtheta", c_double), ("dphi", c_double), ("dpsi", c_double), ("apx", c_double), ("apy", c_double)]
+
+
+class PortGP(ctypes.Structure):
+    _fields_ = [("gamma", c_double), ("beta", c_double), ("energy", c_double), ("brho", c_double),
+                ("G", c_double), ("Q", c_double), ("quad_fringe", c_int), ("pad", c_int)]
+
+
+def _norder(knl, knsl):
+    for i in range(10):
+        if knl[10 - i] != 0.0 or knsl[10 - i] != 0.0:
+            return 10 - i
+    return 1
+
+
+class PortOracle:
+    def __init__(self):
+        L = ctypes.CDLL(str(PORT_SO))
+        L.port_track.argtypes = [POINTER(PortElem), c_long, POINTER(PortGP), POINTER(c_double), c_long, c_int,
+                                 c_double, POINTER(c_int), POINTER(c_int), POINTER(c_int)]
+        L.port_track_dump.argtypes = [POINTER(PortElem), c_long, POINTER(PortGP), POINTER(c_double), c_int,
+                                      c_double, POINTER(c_double), POINTER(c_int), POINTER(c_int), POINTER(c_int)]
+        L.port_cerrf.argtypes = [c_double, c_double, POINTER(c_double), POINTER(c_double)]
+        self.L = L
+
+    def build(self, lat: Lattice) -> None:
+        # Reference particle as Set_RefPartEnergy computes it (simtrack.cpp:87-108).
+        gamma, E0, Q = lat.gamma, lat.E0, lat.Q
+        beta = math.sqrt(1.0 - 1.0 / gamma / gamma)
+        energy = gamma * E0
+        brho = 3.33564095198 * beta * (energy / 1000) / int(Q)
+        self.gp = PortGP(gamma, beta, energy, brho, 1.7928474, float(int(Q)), int(lat.quad_fringe), 0)
+        n = len(lat.elements)
+        arr = (PortElem * n)()
+        for i, e in enumerate(lat.elements):
+            pe = arr[i]
+            pe.type = PORT_TYPES.index(e.type)
+            a = list(e.args)
+            pe.apx, pe.apy = (1.0, 1.0) if e.aperture is None else e.aperture
+            if e.misalign is not None:
+                pe.dx, pe.dy, pe.ds, pe.dtheta, pe.dphi, pe.dpsi = e.misalign
+            t = e.type
+            if t in ("LBT", "ILBT"):
+                pe.L = 0.0
+                pe.p[0] = a[0]
+            elif t == "BEAMBEAM":
+                pe.L = 0.0
+                pe.treatment = int(a[0])
+                pe.nslice = int(a[4])
+                vals = [a[1], a[2], a[3], a[5], a[6], a[7], a[8], a[9], a[10]]
+                for k, v in enumerate(vals):
+                    pe.p[k] = v
+            elif t == "MULT":
+                pe.L = a[0]
+                for k in range(11):
+                    pe.knl[k] = a[1 + k]
+                    pe.knsl[k] = a[12 + k]
+                pe.norder = _norder(a[1:12], a[12:23])
+                pe.nint = int(a[0] / 0.05) + 1
+            elif t in ("GMULT", "SBENDMULT"):
+                pe.L = a[0]
+                pe.p[0], pe.p[1], pe.p[2] = a[1], a[2], a[3]
+                for k in range(11):
+                    pe.knl[k] = a[4 + k]
+                    pe.knsl[k] = a[15 + k]
+                pe.norder = _norder(a[4:15], a[15:26])
+                pe.nint = int(a[0] / 0.25) + 1
+            else:
+                pe.L = a[0]
+                for k, v in enumerate(a[1:]):
+                    pe.p[k] = v
+                if t in ("QUAD", "SKEWQ", "SEXT", "OCT"):
+                    pe.nint = int(a[0] / 0.05) + 1
+                elif t in ("SBEND", "GSBEND"):
+                    pe.nint = int(a[0] / 0.25) + 1
+            for k, v in e.setp.items():
+                if k == "Nint":
+                    pe.nint = int(v)
+                elif k == "Norder":
+                    pe.norder = int(v)
+                else:
+                    raise NotImplementedError(f"port bridge: SetP({k})")
+        self.elems = arr
+        self.nelem = n
+        self.radius = lat.aperture_radius
+
+    def track(self, x: np.ndarray, nturn: int, radius: float | None = None):
+        radius = self.radius if radius is None else radius
+        x = np.ascontiguousarray(x, dtype=np.float64).copy()
+        n = x.shape[0]
+        st = np.ones(n, dtype=np.int32)
+        lt = np.zeros(n, dtype=np.int32)
+        lp = np.zeros(n, dtype=np.int32)
+        P = lambda a, t: a.ctypes.data_as(POINTER(t))
+        self.L.port_track(self.elems, self.nelem, ctypes.byref(self.gp), P(x, c_double), n, nturn, radius,
+                          P(st, c_int), P(lt, c_int), P(lp, c_int))
+        return x, st, lt, lp
+
+    def track_dump(self, x0, nturn: int, radius: float | None = None):
+        radius = self.radius if radius is None else radius
+        x = np.ascontiguousarray(x0, dtype=np.float64).copy()
+        dump = np.full((nturn, self.nelem, 6), np.nan)
+        st, lt, lp = c_int(), c_int(), c_int()
+        self.L.port_track_dump(self.elems, self.nelem, ctypes.byref(self.gp), x.ctypes.data_as(POINTER(c_double)),
+                               nturn, radius, dump.ctypes.data_as(POINTER(c_double)), ctypes.byref(st),
+                               ctypes.byref(lt), ctypes.byref(lp))
+        return x, st.value, lt.value, lp.value, dump
+
+    def cerrf(self, x: float, y: float):
+        wx, wy = c_double(), c_double()
+        self.L.port_cerrf(x, y, ctypes.byref(wx), ctypes.byref(wy))
+        return wx.value, wy.value
