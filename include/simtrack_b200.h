@@ -123,6 +123,17 @@ int stb_track_host(stb_table *t, double *x, long n, int nturn, double aperture_r
 int stb_track_probe(stb_table *t, double *x, long n, int nturn, double aperture_radius, double *dump, int *stable,
                     int *lost_turn, int *lost_post);
 
+/* Diagnostics (no reference counterpart): evaluates the kernels' elementary
+ * functions on host buffers, on GPU `device` (device >= 0) or on the host CPU
+ * (device < 0).  fn: 0 asin, 1 exp, 2 sin, 3 cos, 4 integer power (input pairs
+ * h, m) as used by the tracking maps; 10..14 the same through CUDA's / the C
+ * library's own functions.  in has n values (2n for the power functions). */
+int stb_math_eval(int fn, const double *in, double *out, long n, int device);
+
+/* Diagnostics: measured FP64 FMA throughput of `device` in TFLOP/s (8 independent
+ * FMA chains per thread on every SM; the roofline denominator of the tracking kernel). */
+int stb_fp64_peak(int device, double *tflops);
+
 #ifdef __cplusplus
 }
 #endif

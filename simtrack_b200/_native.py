@@ -63,6 +63,8 @@ SIGNATURES = [
                                                                 c_void_p, c_void_p]),
     ("stb_track_host", c_int, [c_void_p, POINTER(c_double), c_long, c_int, c_double, POINTER(c_int),
                                POINTER(c_int), POINTER(c_int)]),
+    ("stb_fp64_peak", c_int, [c_int, POINTER(c_double)]),
+    ("stb_math_eval", c_int, [c_int, POINTER(c_double), POINTER(c_double), c_long, c_int]),
     ("stb_track_probe", c_int, [c_void_p, POINTER(c_double), c_long, c_int, c_double, POINTER(c_double),
                                 POINTER(c_int), POINTER(c_int), POINTER(c_int)]),
 ]

@@ -449,6 +449,40 @@ int stb_track_host(stb_table *t, double *x, long n, int nturn, double aperture_r
   return guarded([&] { return track_host(t, x, n, nturn, aperture_radius, stable, lost_turn, lost_post); });
 }
 
+int stb_fp64_peak(int device, double *tflops) {
+  return guarded([&] {
+    if (!tflops) throw Error(STB_EINVAL, "NULL output");
+    DeviceGuard g(device);
+    cuda_check(fp64_peak_probe(device, tflops), "fp64 peak probe");
+    return STB_OK;
+  });
+}
+
+int stb_math_eval(int fn, const double *in, double *out, long n, int device) {
+  return guarded([&] {
+    if (!math_fn_valid(fn)) throw Error(STB_EINVAL, "unknown function code");
+    if (n < 0 || (n > 0 && (!in || !out))) throw Error(STB_EINVAL, "bad buffers");
+    if (n == 0) return STB_OK;
+    const long nin = n * math_input_arity(fn);
+    if (device < 0) {
+      math_eval_host(fn, in, out, n);
+      return STB_OK;
+    }
+    DeviceGuard g(device);
+    double *d = nullptr;
+    cuda_check(cudaMalloc(&d, sizeof(double) * (nin + n)), "cudaMalloc(math eval)");
+    struct Free {
+      void *p;
+      ~Free() { if (p) cudaFree(p); }
+    } f{d};
+    cuda_check(cudaMemcpy(d, in, sizeof(double) * nin, cudaMemcpyHostToDevice), "upload");
+    cuda_check(math_eval_device(fn, d, d + nin, n, 0), "math eval launch");
+    cuda_check(cudaDeviceSynchronize(), "math eval");
+    cuda_check(cudaMemcpy(out, d + nin, sizeof(double) * n, cudaMemcpyDeviceToHost), "download");
+    return STB_OK;
+  });
+}
+
 int stb_track_probe(stb_table *t, double *x, long n, int nturn, double aperture_radius, double *dump, int *stable,
                     int *lost_turn, int *lost_post) {
   return guarded([&] {

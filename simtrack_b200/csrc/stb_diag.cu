@@ -1,0 +1,98 @@
+// Diagnostics: evaluation of the kernels' elementary functions on the GPU or
+// on the host, for accuracy tests against the host C library.
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "stb_crmath.cuh"
+#include "stb_kernels.hpp"
+
+namespace stb {
+
+namespace {
+
+__host__ __device__ inline double eval_fn(int fn, const double *in, long i) {
+  switch (fn) {
+    case 0: return cr_asin(in[i]);
+    case 1: return cr_exp(in[i]);
+    case 2: return cr_sin(in[i]);
+    case 3: return cr_cos(in[i]);
+    case 4: return cr_pown(in[2 * i], (int)in[2 * i + 1]);
+    case 10: return asin(in[i]);
+    case 11: return exp(in[i]);
+    case 12: return sin(in[i]);
+    case 13: return cos(in[i]);
+    case 14: return pow(in[2 * i], in[2 * i + 1]);
+    default: return 0.0;
+  }
+}
+
+__global__ void math_eval_kernel(int fn, const double *in, double *out, long n) {
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+    out[i] = eval_fn(fn, in, i);
+}
+
+// FP64 FMA throughput probe: 8 independent FMA chains per thread, `iters`
+// rounds, result folded into one store so nothing is dead code.
+__global__ void dfma_peak_kernel(double *out, int iters, double a, double b) {
+  double v0 = threadIdx.x * 1e-9, v1 = v0 + 1e-3, v2 = v0 + 2e-3, v3 = v0 + 3e-3;
+  double v4 = v0 + 4e-3, v5 = v0 + 5e-3, v6 = v0 + 6e-3, v7 = v0 + 7e-3;
+  for (int i = 0; i < iters; i++) {
+    v0 = fma(v0, a, b); v1 = fma(v1, a, b); v2 = fma(v2, a, b); v3 = fma(v3, a, b);
+    v4 = fma(v4, a, b); v5 = fma(v5, a, b); v6 = fma(v6, a, b); v7 = fma(v7, a, b);
+  }
+  const double s = ((v0 + v1) + (v2 + v3)) + ((v4 + v5) + (v6 + v7));
+  if (s == 12345.678) out[blockIdx.x] = s;
+}
+
+}  // namespace
+
+// Measured FP64 FMA peak of `device` in TFLOP/s (2 flops per FMA).
+cudaError_t fp64_peak_probe(int device, double *tflops) {
+  int sms = 0;
+  cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  if (e != cudaSuccess) return e;
+  double *d = nullptr;
+  const int blocks = sms * 8, threads = 256, iters = 1 << 15;
+  e = cudaMalloc(&d, sizeof(double) * blocks);
+  if (e != cudaSuccess) return e;
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  dfma_peak_kernel<<<blocks, threads>>>(d, 1024, 0.999999, 1e-7);  // warm-up
+  float best = 1e30f;
+  for (int r = 0; r < 3; r++) {
+    cudaEventRecord(a);
+    dfma_peak_kernel<<<blocks, threads>>>(d, iters, 0.999999, 1e-7);
+    cudaEventRecord(b);
+    cudaEventSynchronize(b);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, b);
+    if (ms < best) best = ms;
+  }
+  e = cudaGetLastError();
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaFree(d);
+  *tflops = 2.0 * 8.0 * (double)iters * blocks * threads / (best * 1e-3) / 1e12;
+  return e;
+}
+
+int math_input_arity(int fn) { return (fn == 4 || fn == 14) ? 2 : 1; }
+
+bool math_fn_valid(int fn) { return (fn >= 0 && fn <= 4) || (fn >= 10 && fn <= 14); }
+
+cudaError_t math_eval_device(int fn, const double *d_in, double *d_out, long n, cudaStream_t s) {
+  const int block = 256;
+  long grid = (n + block - 1) / block;
+  if (grid > 65535) grid = 65535;
+  if (grid < 1) grid = 1;
+  math_eval_kernel<<<(unsigned)grid, block, 0, s>>>(fn, d_in, d_out, n);
+  return cudaGetLastError();
+}
+
+void math_eval_host(int fn, const double *in, double *out, long n) {
+  for (long i = 0; i < n; i++) out[i] = eval_fn(fn, in, i);
+}
+
+}  // namespace stb

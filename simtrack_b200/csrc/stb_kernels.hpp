@@ -33,6 +33,13 @@ struct TrackArgs {
   double *dump;
 };
 
+// Elementary-function diagnostics (stb_diag.cu).
+int math_input_arity(int fn);
+bool math_fn_valid(int fn);
+cudaError_t math_eval_device(int fn, const double *d_in, double *d_out, long n, cudaStream_t s);
+void math_eval_host(int fn, const double *in, double *out, long n);
+cudaError_t fp64_peak_probe(int device, double *tflops);
+
 size_t track_smem_bytes(int nelem, int npool_padded);
 int track_smem_limit(int device);
 cudaError_t launch_track(const TrackArgs &a, int num_sms, bool use_smem, cudaStream_t stream);

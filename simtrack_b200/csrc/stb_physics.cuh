@@ -4,8 +4,10 @@
 // function) with the particle held in registers.  Operand order matches the
 // reference expression by expression and this translation unit is compiled
 // with -fmad=false, so every +, -, *, / and sqrt rounds exactly as in the
-// reference's x86-64 build; only the transcendentals (asin, sin, cos, exp,
-// pow) come from CUDA's library instead of glibc.
+// reference's x86-64 build.  The transcendentals (asin, sin, cos, exp, pow)
+// are the correctly rounded versions of stb_crmath.cuh, which agree with the
+// host C library's results except on rare arguments where the library itself
+// is not correctly rounded.
 //
 // Quantities that depend only on pt (delta, gamma, beta of the particle) are
 // held in a PtCache and recomputed only when an element changes pt (RF,
@@ -15,6 +17,7 @@
 #pragma once
 #include <cstdint>
 
+#include "stb_crmath.cuh"
 #include "stb_table.hpp"
 
 namespace stb {
@@ -57,8 +60,8 @@ __device__ __forceinline__ void bend_exact(Particle &p, const PtCache &c, const 
   const double der = (-px0) * sinA * href + (pz0 - 1. - x0 * href) * cosA * href;
   p.x = pz1 / href - der / href / href - invh;
   const double temp = sqrt(c.opd2 - py0 * py0);
-  const double as1 = asin(px0 / temp);
-  const double as2 = asin(npx / temp);
+  const double as1 = cr_asin(px0 / temp);
+  const double as2 = cr_asin(npx / temp);
   const double das = as1 - as2;
   p.y = p.y + py0 * L + py0 * das / href;
   const double t2 = c.opd * L + c.opd * das / href;
@@ -78,8 +81,8 @@ __device__ __forceinline__ void gbend_exact(Particle &p, const PtCache &c, const
   const double der = (-px0) * sinA / rhoc + w * cosA / rhoc;
   p.x = pz1 / b0 - der * rhoc / b0 - rhoc;
   const double temp = sqrt(c.opd2 - py0 * py0);
-  const double as1 = asin(px0 / temp);
-  const double as2 = asin(npx / temp);
+  const double as1 = cr_asin(px0 / temp);
+  const double as2 = cr_asin(npx / temp);
   const double das = as1 - as2;
   p.y = p.y + py0 * L / b0 / rhoc + py0 * das / b0;
   const double t2 = c.opd * L / b0 / rhoc + c.opd * das / b0;
@@ -193,7 +196,7 @@ __device__ __noinline__ void cerrf_dev(double xx, double yy, double &wx, double 
     const double q = (1. - y / ylim) * sqrt(1. - (x / xlim) * (x / xlim));
     const double h = 1. / (fac1 * q);
     const int nc = 7 + int(fac2 * q);
-    double xl = pow(h, (double)(1 - nc));
+    double xl = cr_pown(h, 1 - nc);
     const double xh = y + .5 / h;
     const double yh = x;
     const int nu = 10 + int(fac3 * q);
@@ -227,8 +230,8 @@ __device__ __noinline__ void cerrf_dev(double xx, double yy, double &wx, double 
     wy = cc * ry;
   }
   if (yy < 0.) {
-    wx = 2. * exp(y * y - x * x) * cos(2. * x * y) - wx;
-    wy = -2. * exp(y * y - x * x) * sin(2. * x * y) - wy;
+    wx = 2. * cr_exp(y * y - x * x) * cr_cos(2. * x * y) - wx;
+    wy = -2. * cr_exp(y * y - x * x) * cr_sin(2. * x * y) - wy;
     if (xx > 0.) wy = -wy;
   } else {
     if (xx < 0.) wy = -wy;
@@ -248,12 +251,12 @@ __device__ __forceinline__ void bb4d(double x, double y, double c4, double sigma
   } else if (fabs(sigmax - sigmay) / sigmax < 1.0e-6) {
     const double r2 = x * x + y * y;
     const double temp1 = c4 / r2;
-    const double temp2 = 1 - exp(-r2 / 2 / sigmax / sigmax);
+    const double temp2 = 1 - cr_exp(-r2 / 2 / sigmax / sigmax);
     Dpx = temp1 * x * temp2;
     Dpy = temp1 * y * temp2;
   } else if (sigmax > sigmay) {
     const double temp1 = c4 * sqrt(PI / 2. / (sigmax * sigmax - sigmay * sigmay));
-    const double temp2 = exp(-x * x / 2. / sigmax / sigmax - y * y / 2. / sigmay / sigmay);
+    const double temp2 = cr_exp(-x * x / 2. / sigmax / sigmax - y * y / 2. / sigmay / sigmay);
     const double temp3 = sqrt(2. * (sigmax * sigmax - sigmay * sigmay));
     double w1r, w1i, w2r, w2i;
     const double x1 = fabs(x) / temp3, y1 = fabs(y) / temp3;
@@ -264,7 +267,7 @@ __device__ __forceinline__ void bb4d(double x, double y, double c4, double sigma
     Dpx = temp1 * (w1i - temp2 * w2i) * signx;
   } else if (sigmax < sigmay) {
     const double temp1 = c4 * sqrt(PI / 2 / (sigmay * sigmay - sigmax * sigmax));
-    const double temp2 = exp(-x * x / 2 / sigmax / sigmax - y * y / 2 / sigmay / sigmay);
+    const double temp2 = cr_exp(-x * x / 2 / sigmax / sigmax - y * y / 2 / sigmay / sigmay);
     const double temp3 = sqrt(2 * (sigmay * sigmay - sigmax * sigmax));
     double w1r, w1i, w2r, w2i;
     const double x1 = fabs(x) / temp3, y1 = fabs(y) / temp3;
@@ -303,7 +306,7 @@ __device__ __noinline__ void bb6d(Particle &p, const double *P, int nslice) {
     bb4d(X, Y, c4, sigmax, sigmay, Dpx, Dpy);
     const double temp1 = 1.0 / 2. / (sigmax * sigmax - sigmay * sigmay);
     const double temp2 = X * Dpx + Y * Dpy;
-    const double temp4 = exp(-X * X / 2. / sigmax / sigmax - Y * Y / 2. / sigmay / sigmay);
+    const double temp4 = cr_exp(-X * X / 2. / sigmax / sigmax - Y * Y / 2. / sigmay / sigmay);
     p.x = q.x - S * Dpx * bbscale;
     p.px = q.px + Dpx * bbscale;
     p.y = q.y - S * Dpy * bbscale;
@@ -361,8 +364,8 @@ __device__ __noinline__ void ccmult_kick(Particle &p, const double *P) {
   const double kf = P[0], PHASE0 = P[1], scale = P[2], brho = P[3];
   const double B2 = P[4], A2 = P[5], B3 = P[6], A3 = P[7], B4 = P[8], A4 = P[9], B5 = P[10], A5 = P[11];
   const double arg = kf * p.z / 2.99792458e8 + PHASE0;
-  const double sinangle = sin(arg);
-  const double cosangle = cos(arg);
+  const double sinangle = cr_sin(arg);
+  const double cosangle = cr_cos(arg);
   const double X = p.x, Y = p.y;
   const double x2 = X * X, x3 = x2 * X, x4 = x3 * X, x5 = x4 * X;
   const double y2 = Y * Y, y3 = y2 * Y, y4 = y3 * Y, y5 = y4 * Y;

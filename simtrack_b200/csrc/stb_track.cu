@@ -217,7 +217,7 @@ __device__ __forceinline__ void apply_element(const ElemHeader &h, const double 
       // RFCAV_Pass, simtrack.cpp:6008-6010
       drift(p, c, P[0], P[1]);
       const double absvq = P[2], kf = P[3], phase0 = P[4];
-      p.pt = p.pt + absvq * sin(kf * p.z / kC + kPI - phase0) / R.beta / R.energy;
+      p.pt = p.pt + absvq * cr_sin(kf * p.z / kC + kPI - phase0) / R.beta / R.energy;
       pt_refresh(R, p.pt, c);
       drift(p, c, P[0], P[1]);
       break;
@@ -227,8 +227,8 @@ __device__ __forceinline__ void apply_element(const ElemHeader &h, const double 
       drift(p, c, P[0], P[1]);
       const double vq = P[2], kf = P[3], phase0 = P[4], kk = P[5];
       const double arg = kf * p.z / kC + phase0;
-      p.px = p.px - vq * sin(arg) / R.beta / R.energy;
-      p.pt = p.pt - vq * cos(arg) * p.x * kk / R.beta / R.energy;
+      p.px = p.px - vq * cr_sin(arg) / R.beta / R.energy;
+      p.pt = p.pt - vq * cr_cos(arg) * p.x * kk / R.beta / R.energy;
       pt_refresh(R, p.pt, c);
       drift(p, c, P[0], P[1]);
       break;

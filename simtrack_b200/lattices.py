@@ -113,3 +113,156 @@ def fodo_ring(ncell: int = 100, gamma: Optional[float] = None, nint: int = 4, k1
     els.append(ElementSpec("RFCAV", "rf", (0.0, vrf_mv, frf, 0.0)))
     lat.meta.update({"harmonic": harmonic, "frf": frf, "emit_norm": 2.5e-6})
     return lat
+
+
+# Strengths of the RHIC-like ring fitted by simtrack_b200.lattice_design
+# (beta* = 0.6 m at both interaction points, tunes 50.31 / 48.32, linear
+# chromaticity +1 / +1 from the arc sextupoles).  K1L in m^-1, K2L in m^-2.
+RHIC_LIKE_STRENGTHS = dict(
+    kf=0.1746771083134425, kd=-0.17162657379211274,
+    q1=0.2940698212888416, q2=-0.1821646680742746, q3=-0.08577597512541496, q4=0.16666371327006477,
+    ua=-0.05966870432529879, ub=0.030478182687441402,
+    k2f=0.6497955572120756, k2d=-1.323393027511492,
+)
+RHIC_BETA_STAR = 0.6
+RHIC_GAMMA = 100000.0 / PROTON_MASS_MEV  # 100 GeV protons
+
+
+def triplet_errors(seed: int, nquad: int = 12, rms: float = 1e-4) -> "np.ndarray":
+    """Gaussian b3..b10 / a3..a10 coefficients (units of 1e-4 at the reference
+    radius are folded into `rms`) for `nquad` triplet quadrupoles: shape
+    (nquad, 2, 8), [:, 0] normal, [:, 1] skew."""
+    import numpy as np
+    return np.random.default_rng(seed).standard_normal((nquad, 2, 8)) * rms
+
+
+def rhic_like_ring(seed: Optional[int] = None, nint_arc: int = 4, nint_triplet: int = 8, bb: bool = True,
+                   aperture_radius: float = 0.03, r_ref: float = 0.031) -> Lattice:
+    """Synthetic RHIC-like ring, 3,834 m, ~1,800 elements.
+
+    Six arcs of 36 FODO cells (thick sector dipoles L = 5.8 m, thick
+    quadrupoles L = 1.1 m, thin chromatic sextupoles), two low-beta
+    interaction regions (beta* = 0.6 m) whose thick triplet quadrupoles are
+    MULT elements carrying random normal/skew errors b3..b10, a3..a10 of rms
+    1e-4 relative at r_ref = 31 mm drawn from `seed` (no errors when seed is
+    None), with the convention knl[n] = K1L * r_ref * 1e-4 * g * n! / r_ref^n of
+    the reference's error assignment (Example2/DA_cal.cpp:284-290, Gaussian g
+    instead of flat), four utility straights, RF at 28 MHz (h = 360) and
+    197 MHz (h = 2520), and the weak-strong 6D beam-beam map at both IPs
+    (2e11 protons, round sigma* = 0.12 mm, sigma_z = 0.3 m, 5 slices).
+    Protons at 100 GeV; circular aperture of `aperture_radius`."""
+    from . import lattice_design as D
+    S = RHIC_LIKE_STRENGTHS
+    err = triplet_errors(seed) if seed is not None else None
+    a, b, c, d = D.ir_drifts()
+    ua, ub, uc = D.util_drifts()
+    els: List[ElementSpec] = []
+    tq = [0]
+
+    def triplet(name, L, k1l):
+        knl = [0.0, k1l] + [0.0] * 9
+        knsl = [0.0] * 11
+        if err is not None:
+            e = err[tq[0]]
+            fac = 1.0
+            for n in range(2, 10):
+                fac *= n
+                knl[n] = k1l * r_ref * 1e-4 * (e[0, n - 2] / 1e-4) * fac / r_ref ** n
+                knsl[n] = k1l * r_ref * 1e-4 * (e[1, n - 2] / 1e-4) * fac / r_ref ** n
+        tq[0] += 1
+        return ElementSpec("MULT", name, mult_args(L, knl, knsl), {"Nint": nint_triplet})
+
+    def half_ir(tag, reverse):
+        h = [ElementSpec("DRIFT", f"dstar_{tag}", (D.L_STAR,)),
+             triplet(f"q1_{tag}", D.LQ1, S["q1"]),
+             ElementSpec("DRIFT", f"d12_{tag}", (d,)),
+             triplet(f"q2_{tag}", D.LQ2, S["q2"]),
+             ElementSpec("DRIFT", f"d23_{tag}", (c,)),
+             triplet(f"q3_{tag}", D.LQ3, S["q3"]),
+             ElementSpec("DRIFT", f"d34_{tag}", (b,)),
+             ElementSpec("QUAD", f"q4_{tag}", (D.LQ4, S["q4"], 0.0), {"Nint": nint_arc}),
+             ElementSpec("DRIFT", f"dir_{tag}", (a,))]
+        return h[::-1] if reverse else h
+
+    def half_util(tag, reverse):
+        h = [ElementSpec("QUAD", f"qub_{tag}", (D.LQU, S["ub"], 0.0), {"Nint": nint_arc}),
+             ElementSpec("DRIFT", f"dub_{tag}", (ub,)),
+             ElementSpec("QUAD", f"qua_{tag}", (D.LQU, S["ua"], 0.0), {"Nint": nint_arc}),
+             ElementSpec("DRIFT", f"dua_{tag}", (ua,))]
+        return h[::-1] if reverse else h
+
+    def bb_elem(tag):
+        emit = 0.12e-3 ** 2 / RHIC_BETA_STAR
+        return ElementSpec("BEAMBEAM", f"bb_{tag}", (6, 2e11, 1.0, 0.3, 5, emit, RHIC_BETA_STAR, 0.0, emit,
+                                                     RHIC_BETA_STAR, 0.0))
+
+    def arc(k):
+        s = [ElementSpec("QUAD", f"qfh_{k}_0", (D.LQ / 2, S["kf"] / 2, 0.0), {"Nint": nint_arc})]
+        for i in range(D.CELLS_PER_ARC):
+            last = i == D.CELLS_PER_ARC - 1
+            s += [ElementSpec("SEXT", f"sf_{k}_{i}", (0.0, S["k2f"], 0.0)),
+                  ElementSpec("DRIFT", f"da_{k}_{i}", (D.LD,)),
+                  ElementSpec("SBEND", f"ba_{k}_{i}", (D.LB, D.ANGLE, 0.0, 0.0)),
+                  ElementSpec("QUAD", f"qd_{k}_{i}", (D.LQ, S["kd"], 0.0), {"Nint": nint_arc}),
+                  ElementSpec("SEXT", f"sd_{k}_{i}", (0.0, S["k2d"], 0.0)),
+                  ElementSpec("DRIFT", f"db_{k}_{i}", (D.LD,)),
+                  ElementSpec("SBEND", f"bb_{k}_{i}", (D.LB, D.ANGLE, 0.0, 0.0)),
+                  ElementSpec("QUAD", f"qf_{k}_{i}", ((D.LQ / 2, S["kf"] / 2, 0.0) if last else
+                                                      (D.LQ, S["kf"], 0.0)), {"Nint": nint_arc})]
+        return s
+
+    gamma = RHIC_GAMMA
+    beta = math.sqrt(1.0 - 1.0 / gamma / gamma)
+    frev = beta * 299792458.0 / D.CIRC
+    for k in range(D.N_ARC):
+        if k == 0:
+            if bb:
+                els.append(bb_elem("ip1"))
+            els += half_ir("ip1r", False)
+        elif k == 3:
+            els += half_ir("ip2l", True)
+            if bb:
+                els.append(bb_elem("ip2"))
+            els += half_ir("ip2r", False)
+        else:
+            els += half_util(f"u{k}l", True)
+            els.append(ElementSpec("DRIFT", f"duc_{k}", (2 * uc,)))
+            if k == 1:
+                els.append(ElementSpec("RFCAV", "rf28", (0.0, 0.3, 360 * frev, 0.0)))
+                els.append(ElementSpec("RFCAV", "rf197", (0.0, 3.0, 2520 * frev, 0.0)))
+            els += half_util(f"u{k}r", False)
+        els += arc(k)
+    els += half_ir("ip1l", True)
+    lat = Lattice("rhic_like" + ("" if seed is None else f"_s{seed}"), els, gamma, aperture_radius=aperture_radius)
+    lat.meta.update({"seed": seed, "beta_star": RHIC_BETA_STAR, "emit_norm": 2.5e-6, "frev": frev,
+                     "sigma_ip": math.sqrt(2.5e-6 * RHIC_BETA_STAR / (beta * gamma))})
+    return lat
+
+
+def da_grid(lat: Lattice, namp: int, amax: float, nang: int, deltas: Sequence[float]) -> "np.ndarray":
+    """Initial conditions of a DA scan at element 0: amplitudes 0..amax sigma
+    (inclusive) x angles 90 deg*(i+1)/(nang+1) in x-y x momentum offsets (pt),
+    px = py = z = 0, as Track_DA sets them (simtrack.cpp:21410-21416).
+    Returned as (ndelta*nang*namp, 6), amplitude fastest."""
+    import numpy as np
+    sig = lat.meta["sigma_ip"]
+    amps = np.linspace(0.0, amax, namp)
+    out = []
+    for dp in deltas:
+        for i in range(nang):
+            th = (90.0 / (nang + 1)) * (i + 1) * math.pi / 180
+            for a in amps:
+                out.append([a * math.cos(th) * sig, 0.0, a * math.sin(th) * sig, 0.0, 0.0, dp])
+    return np.array(out)
+
+
+def gaussian_beam(lat: Lattice, n: int, seed: int = 12345, sigma_z: float = 0.1, sigma_pt: float = 3e-4) -> "np.ndarray":
+    """6D Gaussian distribution at element 0, Twiss-matched transversely
+    (alpha* = 0 at the interaction point): sigma_x = sqrt(eps beta*),
+    sigma_px = sqrt(eps / beta*); longitudinal sigma_z, sigma_pt as given."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    sx = lat.meta["sigma_ip"]
+    spx = sx / lat.meta["beta_star"]
+    g = rng.standard_normal((n, 6))
+    return g * np.array([sx, spx, sx, spx, sigma_z, sigma_pt])
