@@ -234,6 +234,9 @@ def run_ours(a):
     le_ = torch.zeros(n, dtype=torch.int32, device=dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
 
+    tune = tab.autotune(coords, nturn=1, aperture_radius=lat.aperture_radius)
+    info = tab.info()
+
     peak = ctypes.c_double()
     rc = lib().stb_fp64_peak(local, ctypes.byref(peak))
     fp64_peak = peak.value if rc == 0 else None
@@ -302,7 +305,9 @@ def run_ours(a):
                     "vs_baseline": None, "dtype": "f64", "data": "synthetic",
                     "config": {"workload": WORKLOAD, "particles_per_gpu": n, "turns_per_step": T,
                                "elements": info["elements"], "l2": "256 MiB flush between timed steps",
-                               "parallelism": f"particle shards x{world}, no exchange"},
+                               "parallelism": f"particle shards x{world}, no exchange",
+                               "kernel_variant": info["variant_name"],
+                               "autotune_ms_1turn": {k: round(v, 3) for k, v in tune["ms"].items()}},
                     "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": a.steps,
                     "clocks": clk.summary(), "alive": [alive0, alive1]}
         print(json.dumps(line_out), flush=True)

@@ -90,8 +90,21 @@ int stb_line_cell(stb_line *l, long i, stb_element **out); /* Line::Cell[i] (bor
 int stb_table_create(const stb_line *l, int device, stb_table **out);
 int stb_table_free(stb_table *t);
 /* info[0] = elements, [1] = pool doubles, [2] = algorithmic FP64 ops per particle-turn,
- * [3] = 1 if the table is staged in shared memory, [4] = shared-memory bytes per CTA */
-int stb_table_info(const stb_table *t, double *info5);
+ * [3] = 1 if the current launch variant stages the table in shared memory,
+ * [4] = table bytes (shared memory per CTA when staged), [5] = launch variant */
+int stb_table_info(const stb_table *t, double *info6);
+
+/* Autotuner (no reference counterpart): times every launch variant of the
+ * tracking kernel (CTA size, registers per thread, table in shared memory or
+ * L1) on a device-side copy of the n given particles for nturn turns and keeps
+ * the fastest for this table.  The inputs are not modified.  timings_ms
+ * (optional) receives up to ntimings per-variant times (< 0: not runnable). */
+int stb_table_autotune(stb_table *t, const double *x, const double *px, const double *y, const double *py,
+                       const double *z, const double *pt, long n, int nturn, double aperture_radius, int *chosen,
+                       double *timings_ms, int ntimings);
+int stb_table_set_variant(stb_table *t, int variant);
+/* name (NUL-terminated, truncated to cap), CTA size and shared-memory flag of a launch variant */
+int stb_track_variant_info(int variant, char *name, int cap, int *block, int *smem);
 
 /* ---- tracking ----
  * Track()  simtrack.cpp:20791-20814, batched.  Coordinates are SoA device
@@ -126,8 +139,10 @@ int stb_track_probe(stb_table *t, double *x, long n, int nturn, double aperture_
 /* Diagnostics (no reference counterpart): evaluates the kernels' elementary
  * functions on host buffers, on GPU `device` (device >= 0) or on the host CPU
  * (device < 0).  fn: 0 asin, 1 exp, 2 sin, 3 cos, 4 integer power (input pairs
- * h, m) as used by the tracking maps; 10..14 the same through CUDA's / the C
- * library's own functions.  in has n values (2n for the power functions). */
+ * h, m), 5 quotient a/b through the shared-reciprocal correction (pairs a, b;
+ * IEEE division on the host) as used by the tracking maps; 10..15 the same
+ * through CUDA's / the C library's own functions and the IEEE division.
+ * in has n values (2n for the two-argument functions). */
 int stb_math_eval(int fn, const double *in, double *out, long n, int device);
 
 /* Diagnostics: measured FP64 FMA throughput of `device` in TFLOP/s (8 independent

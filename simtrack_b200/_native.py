@@ -59,6 +59,10 @@ SIGNATURES = [
     ("stb_table_create", c_int, [c_void_p, c_int, POINTER(c_void_p)]),
     ("stb_table_free", c_int, [c_void_p]),
     ("stb_table_info", c_int, [c_void_p, POINTER(c_double)]),
+    ("stb_table_autotune", c_int, [c_void_p] + [c_void_p] * 6 + [c_long, c_int, c_double, POINTER(c_int),
+                                                                  POINTER(c_double), c_int]),
+    ("stb_table_set_variant", c_int, [c_void_p, c_int]),
+    ("stb_track_variant_info", c_int, [c_int, c_char_p, c_int, POINTER(c_int), POINTER(c_int)]),
     ("stb_track_device", c_int, [c_void_p] + [c_void_p] * 6 + [c_long, c_int, c_int, c_double, c_void_p,
                                                                 c_void_p, c_void_p]),
     ("stb_track_host", c_int, [c_void_p, POINTER(c_double), c_long, c_int, c_double, POINTER(c_int),

@@ -201,6 +201,16 @@ class Line:
             pass
 
 
+NUM_VARIANTS = 6
+
+
+def variant_name(v: int) -> str:
+    buf = ctypes.create_string_buffer(64)
+    b, sm = c_int(), c_int()
+    check(lib().stb_track_variant_info(v, buf, 64, byref(b), byref(sm)))
+    return buf.value.decode()
+
+
 class Table:
     """Flattened device element table of a Line (rebuild after editing the line)."""
 
@@ -211,10 +221,25 @@ class Table:
         self.device = device
 
     def info(self) -> dict:
-        out = (c_double * 5)()
+        out = (c_double * 6)()
         check(lib().stb_table_info(self._h, out))
         return {"elements": int(out[0]), "pool_doubles": int(out[1]), "flops_per_turn": out[2],
-                "smem": bool(out[3]), "smem_bytes": int(out[4])}
+                "smem": bool(out[3]), "table_bytes": int(out[4]), "variant": int(out[5]),
+                "variant_name": variant_name(int(out[5]))}
+
+    def autotune(self, coords, nturn: int = 1, aperture_radius: float = 0.0) -> dict:
+        """Times every kernel launch variant on a copy of `coords` (6 CUDA float64
+        tensors, not modified) and keeps the fastest; returns {name: ms}."""
+        chosen = c_int()
+        t = (c_double * 16)()
+        n = coords[0].numel()
+        check(lib().stb_table_autotune(self._h, *[c_void_p(c.data_ptr()) for c in coords], n, nturn,
+                                       aperture_radius, byref(chosen), t, 16))
+        return {"chosen": variant_name(chosen.value),
+                "ms": {variant_name(v): t[v] for v in range(NUM_VARIANTS)}}
+
+    def set_variant(self, v: int) -> None:
+        check(lib().stb_table_set_variant(self._h, v))
 
     def track_host(self, x: np.ndarray, nturn: int, aperture_radius: float = 0.0, stable=None):
         """Track() over AoS host coordinates x[n,6] (updated in place); returns (stable, lost_turn, lost_post)."""

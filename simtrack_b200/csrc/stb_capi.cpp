@@ -22,7 +22,8 @@ struct stb_table {
   stb::ElemHeader *d_hdr = nullptr;
   double *d_pool = nullptr;
   int npool_padded = 0;
-  bool use_smem = false;
+  bool use_smem = false;  // the table fits the shared-memory variants
+  int variant = 2;        // launch variant (stb::kVariants), set by the autotuner
   int *d_status = nullptr;
   int num_sms = 0;
 };
@@ -153,6 +154,7 @@ stb_table *table_build(const Line &line, int device) {
   cuda_check(cudaDeviceGetAttribute(&t->num_sms, cudaDevAttrMultiProcessorCount, device), "SM count");
   const size_t need = track_smem_bytes((int)t->host.hdr.size(), t->npool_padded);
   t->use_smem = (long)need <= (long)track_smem_limit(device);
+  t->variant = t->use_smem ? 0 : 2;
   return t.release();
 }
 
@@ -185,7 +187,72 @@ int track_device(stb_table *t, double *x, double *px, double *y, double *py, dou
   a.lost_turn = lost_turn;
   a.lost_elem = lost_elem;
   a.dump = dump;
-  cuda_check(launch_track(a, t->num_sms, t->use_smem, s), "track kernel launch");
+  cuda_check(launch_track(a, t->num_sms, t->variant, s), "track kernel launch");
+  return STB_OK;
+}
+
+// Times every launch variant on a scratch copy of up to `nsample` particles
+// and keeps the fastest for this table.
+int autotune(stb_table *t, const double *const in[6], long n, int nturn, double radius, int *chosen,
+             double *timings, int ntimings) {
+  if (!t) throw Error(STB_EINVAL, "table is NULL");
+  for (int k = 0; k < 6; k++)
+    if (!in[k]) throw Error(STB_EINVAL, "NULL coordinate array");
+  if (n <= 0 || nturn <= 0) throw Error(STB_EINVAL, "autotune needs particles and turns");
+  DeviceGuard g(t->device);
+  const long m = n;
+  double *buf = nullptr;
+  int32_t *lost = nullptr;
+  cuda_check(cudaMalloc(&buf, sizeof(double) * 6 * m), "cudaMalloc(autotune)");
+  struct Free {
+    void *p;
+    ~Free() { if (p) cudaFree(p); }
+  } f1{buf};
+  cuda_check(cudaMalloc(&lost, sizeof(int32_t) * 2 * m), "cudaMalloc(autotune)");
+  Free f2{lost};
+  cudaEvent_t e0, e1;
+  cuda_check(cudaEventCreate(&e0), "event");
+  cuda_check(cudaEventCreate(&e1), "event");
+  const int saved = t->variant;
+  int best = -1;
+  float best_ms = 0.f;
+  for (int v = 0; v < kNumTrackVariants; v++) {
+    float ms = -1.f;
+    if (!kVariants[v].smem || t->use_smem) {
+      t->variant = v;
+      float runs[2] = {0.f, 0.f};
+      bool ok = true;
+      for (int r = 0; r < 2 && ok; r++) {
+        for (int k = 0; k < 6; k++)
+          cuda_check(cudaMemcpy(buf + k * m, in[k], sizeof(double) * m, cudaMemcpyDeviceToDevice), "copy");
+        cuda_check(cudaMemset(lost, 0xff, sizeof(int32_t) * m), "reset");
+        cuda_check(cudaMemset(lost + m, 0, sizeof(int32_t) * m), "reset");
+        cuda_check(cudaEventRecord(e0), "event");
+        TrackArgs a = make_args(t);
+        a.x = buf; a.px = buf + m; a.y = buf + 2 * m; a.py = buf + 3 * m; a.z = buf + 4 * m; a.pt = buf + 5 * m;
+        a.n = m; a.turn0 = 1; a.nturn = nturn; a.r2 = radius > 0 ? radius * radius : 0.0;
+        a.lost_turn = lost; a.lost_elem = lost + m; a.dump = nullptr;
+        if (launch_track(a, t->num_sms, v, 0) != cudaSuccess) {
+          cudaGetLastError();
+          ok = false;
+          break;
+        }
+        cuda_check(cudaEventRecord(e1), "event");
+        cuda_check(cudaEventSynchronize(e1), "autotune run");
+        cuda_check(cudaEventElapsedTime(&runs[r], e0, e1), "event time");
+      }
+      if (ok) ms = runs[1];
+    }
+    if (timings && v < ntimings) timings[v] = ms;
+    if (ms > 0.f && (best < 0 || ms < best_ms)) {
+      best = v;
+      best_ms = ms;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  t->variant = best >= 0 ? best : saved;
+  if (chosen) *chosen = t->variant;
   return STB_OK;
 }
 
@@ -429,8 +496,9 @@ int stb_table_info(const stb_table *t, double *info) {
     info[0] = (double)t->host.hdr.size();
     info[1] = (double)t->host.pool.size();
     info[2] = t->host.flops_per_turn;
-    info[3] = t->use_smem ? 1.0 : 0.0;
+    info[3] = stb::kVariants[t->variant].smem ? 1.0 : 0.0;
     info[4] = (double)track_smem_bytes((int)t->host.hdr.size(), t->npool_padded);
+    info[5] = (double)t->variant;
     return STB_OK;
   });
 }
@@ -447,6 +515,38 @@ int stb_track_device(stb_table *t, double *x, double *px, double *y, double *py,
 int stb_track_host(stb_table *t, double *x, long n, int nturn, double aperture_radius, int *stable,
                    int *lost_turn, int *lost_post) {
   return guarded([&] { return track_host(t, x, n, nturn, aperture_radius, stable, lost_turn, lost_post); });
+}
+
+int stb_table_autotune(stb_table *t, const double *x, const double *px, const double *y, const double *py,
+                       const double *z, const double *pt, long n, int nturn, double aperture_radius, int *chosen,
+                       double *timings_ms, int ntimings) {
+  return guarded([&] {
+    const double *in[6] = {x, px, y, py, z, pt};
+    return autotune(t, in, n, nturn, aperture_radius, chosen, timings_ms, ntimings);
+  });
+}
+
+int stb_table_set_variant(stb_table *t, int variant) {
+  return guarded([&] {
+    if (!t) throw Error(STB_EINVAL, "table is NULL");
+    if (variant < 0 || variant >= kNumTrackVariants) throw Error(STB_EINVAL, "variant out of range");
+    if (kVariants[variant].smem && !t->use_smem) throw Error(STB_EINVAL, "table does not fit shared memory");
+    t->variant = variant;
+    return STB_OK;
+  });
+}
+
+int stb_track_variant_info(int variant, char *name, int cap, int *block, int *smem) {
+  return guarded([&] {
+    if (variant < 0 || variant >= kNumTrackVariants) throw Error(STB_EINVAL, "variant out of range");
+    if (name && cap > 0) {
+      std::strncpy(name, kVariants[variant].name, (size_t)cap - 1);
+      name[cap - 1] = 0;
+    }
+    if (block) *block = kVariants[variant].block;
+    if (smem) *smem = kVariants[variant].smem ? 1 : 0;
+    return STB_OK;
+  });
 }
 
 int stb_fp64_peak(int device, double *tflops) {

@@ -94,7 +94,7 @@ __host__ __device__ inline double cr_asin(double x) {
 
 // exp: x = k ln2 + r (double-double reduction), exp(r) = (exp(r/16))^16 with
 // exp(r/16) from its Taylor series in double-double Horner form.
-__host__ __device__ inline double cr_exp(double x) {
+static __host__ __device__ __noinline__ double cr_exp(double x) {
   if (x != x) return x;
   if (x > 709.7) return exp(x);
   if (x < -708.3) return exp(x);  // subnormal or zero results
@@ -117,7 +117,7 @@ __host__ __device__ inline double cr_exp(double x) {
 
 // sin/cos: x = k pi/2 + r with pi/2 split in three parts, then the Taylor
 // series of sin(r) and cos(r), |r| <= pi/4, in double-double.
-__host__ __device__ inline void cr_sincos_reduced(double x, dd &sr, dd &cr, int &quad) {
+static __host__ __device__ __noinline__ void cr_sincos_reduced(double x, dd &sr, dd &cr, int &quad) {
   const double P1 = 1.5707963267948966192;     // pi/2 rounded to double
   const double P2 = 6.123233995736766036e-17;  // next part of pi/2
   const double P3 = -1.4973849048591698e-33;   // remainder
@@ -170,7 +170,7 @@ __host__ __device__ inline double cr_cos(double x) {
 
 // h^m for an integer m (|m| <= 64): binary powering in double-double, one
 // final rounding.
-__host__ __device__ inline double cr_pown(double h, int m) {
+static __host__ __device__ __noinline__ double cr_pown(double h, int m) {
   if (m == 0) return 1.0;
   if (!(h > 0.0) || !(h < 1e150) || !(h > 1e-150)) return pow(h, (double)m);
   int e = m < 0 ? -m : m;

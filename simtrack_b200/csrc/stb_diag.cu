@@ -6,6 +6,7 @@
 
 #include "stb_crmath.cuh"
 #include "stb_kernels.hpp"
+#include "stb_physics.cuh"
 
 namespace stb {
 
@@ -18,11 +19,17 @@ __host__ __device__ inline double eval_fn(int fn, const double *in, long i) {
     case 2: return cr_sin(in[i]);
     case 3: return cr_cos(in[i]);
     case 4: return cr_pown(in[2 * i], (int)in[2 * i + 1]);
+#ifdef __CUDA_ARCH__
+    case 5: return qdiv(in[2 * i], in[2 * i + 1], 1.0 / in[2 * i + 1]);
+#else
+    case 5: return in[2 * i] / in[2 * i + 1];
+#endif
     case 10: return asin(in[i]);
     case 11: return exp(in[i]);
     case 12: return sin(in[i]);
     case 13: return cos(in[i]);
     case 14: return pow(in[2 * i], in[2 * i + 1]);
+    case 15: return in[2 * i] / in[2 * i + 1];
     default: return 0.0;
   }
 }
@@ -78,9 +85,9 @@ cudaError_t fp64_peak_probe(int device, double *tflops) {
   return e;
 }
 
-int math_input_arity(int fn) { return (fn == 4 || fn == 14) ? 2 : 1; }
+int math_input_arity(int fn) { return (fn == 4 || fn == 5 || fn == 14 || fn == 15) ? 2 : 1; }
 
-bool math_fn_valid(int fn) { return (fn >= 0 && fn <= 4) || (fn >= 10 && fn <= 14); }
+bool math_fn_valid(int fn) { return (fn >= 0 && fn <= 5) || (fn >= 10 && fn <= 15); }
 
 cudaError_t math_eval_device(int fn, const double *d_in, double *d_out, long n, cudaStream_t s) {
   const int block = 256;

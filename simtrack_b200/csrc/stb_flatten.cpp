@@ -46,13 +46,17 @@ struct Builder {
     push(cosA);
     push(sinA);
   }
-  // Kick coefficient block for mult_kick_pass: [KNL[0], KNSL[0], (KNL[i], KNSL[i]) i=1..Norder]
+  // Kick coefficient block for mult_kick_pass:
+  // [KNL[0], KNSL[0], (KNL[i], KNSL[i], RN(1/i!)) i=1..Norder]
   void mult_block(int norder, const double *knl, const double *knsl) {
     push(knl[0]);
     push(knsl[0]);
+    double fac = 1.0;
     for (int i = 1; i <= norder; i++) {
+      fac *= i;
       push(knl[i]);
       push(knsl[i]);
+      push(1.0 / fac);
     }
   }
 };
@@ -146,6 +150,8 @@ HostTable flatten(const Line &line) {
   t.ref.brho = GP.brho;
   t.ref.sqrt_g2m1 = std::sqrt(GP.gamma * GP.gamma - 1.);
   t.ref.G = GP.G;
+  t.ref.ibeta = 1.0 / GP.beta;
+  t.ref.ienergy = 1.0 / GP.energy;
   t.flops_per_turn = kFlPtRefresh;  // turn-start evaluation of the pt cache
   const Yoshida &Y = B.y;
 
@@ -222,6 +228,8 @@ HostTable flatten(const Line &line) {
         B.push(b0 * rhoc);
         B.push(std::cos(Angle));
         B.push(std::sin(Angle));
+        B.push(1.0 / rhoc);
+        B.push(1.0 / b0);
         if (E1 != 0.) { h.flags |= EF_EDGE1; fl += kFlEdge; }
         if (E2 != 0.) { h.flags |= EF_EDGE2; fl += kFlEdge; }
         fl += kFlBend + 4;

@@ -10,9 +10,15 @@
 
 namespace stb {
 
-// CTA sizes of the two kernel variants (table in shared memory / in global memory).
-constexpr int kTrackBlockSmem = 512;
-constexpr int kTrackBlockGlobal = 256;
+// One compiled launch configuration of the tracking kernel.
+struct TrackVariant {
+  bool smem;       // element table staged in shared memory (else read through L1)
+  int block;       // threads per CTA
+  int min_blocks;  // __launch_bounds__ minimum resident CTAs per SM
+  const char *name;
+};
+constexpr int kNumTrackVariants = 6;
+extern const TrackVariant kVariants[kNumTrackVariants];
 
 struct TrackArgs {
   const ElemHeader *hdr;  // device
@@ -42,6 +48,6 @@ cudaError_t fp64_peak_probe(int device, double *tflops);
 
 size_t track_smem_bytes(int nelem, int npool_padded);
 int track_smem_limit(int device);
-cudaError_t launch_track(const TrackArgs &a, int num_sms, bool use_smem, cudaStream_t stream);
+cudaError_t launch_track(const TrackArgs &a, int num_sms, int variant, cudaStream_t stream);
 
 }  // namespace stb

@@ -14,6 +14,16 @@
 // crab cavities, beam-beam, Lorentz boosts).  The reference recomputes them
 // inside every DRIFT_Pass; the values are identical because kicks and drifts
 // never modify pt.
+//
+// Divisions.  A quotient a/b whose divisor b is reused (an element constant,
+// a pt-only quantity, or a value shared by several quotients of one map) is
+// formed from y = RN(1/b), computed once by an IEEE division, as
+//   q0 = RN(a*y),  r = a - b*q0 (exact, one FMA),  q = RN(q0 + r*y),
+// Markstein's correction step (P. Markstein, IBM J. Res. Dev. 34 (1990) 111).
+// q is the correctly rounded a/b unless a/b lies within about 2^-52 ulp of a
+// rounding midpoint (probability ~2^-50 per quotient), so it reproduces the
+// reference's IEEE division while costing one multiply and two FMAs instead
+// of a full division sequence.  Operands stay far from overflow/underflow.
 #pragma once
 #include <cstdint>
 
@@ -27,10 +37,19 @@ struct Particle {
 };
 
 struct PtCache {
-  double opd;    // 1.0 + delta1
-  double opd2;   // (1.0 + delta1) * (1.0 + delta1)
-  double beta1;  // particle velocity / c
+  double opd;     // 1.0 + delta1
+  double opd2;    // (1.0 + delta1) * (1.0 + delta1)
+  double beta1;   // particle velocity / c
+  double iopd;    // RN(1 / opd)
+  double ibeta1;  // RN(1 / beta1)
 };
+
+// a / b given y = RN(1/b) (see the division note above).
+__device__ __forceinline__ double qdiv(double a, double b, double y) {
+  const double q0 = __dmul_rn(a, y);
+  const double r = fma(-q0, b, a);
+  return fma(r, y, q0);
+}
 
 // delta1/gamma1/beta1 exactly as DRIFT_Pass computes them (simtrack.cpp:3755-3757).
 __device__ __forceinline__ void pt_refresh(const RefConsts &R, double pt, PtCache &c) {
@@ -39,18 +58,25 @@ __device__ __forceinline__ void pt_refresh(const RefConsts &R, double pt, PtCach
   c.beta1 = sqrt(1.0 - 1.0 / gamma1 / gamma1);
   c.opd = 1.0 + delta1;
   c.opd2 = c.opd * c.opd;
+  c.iopd = 1.0 / c.opd;
+  c.ibeta1 = 1.0 / c.beta1;
 }
 
 // DRIFT_Pass exact branch, simtrack.cpp:3759-3764.  L and Lb = L/GP.beta.
+// The two quotients by pz share one reciprocal; (pz*beta1)/(1+delta1) uses
+// the cached reciprocal of 1+delta1.
 __device__ __forceinline__ void drift(Particle &p, const PtCache &c, double L, double Lb) {
   const double pz = sqrt(c.opd2 - p.px * p.px - p.py * p.py);
-  const double betaz = pz * c.beta1 / c.opd;
-  p.x = p.x + p.px * L / pz;
-  p.y = p.y + p.py * L / pz;
+  const double ipz = 1.0 / pz;
+  const double betaz = qdiv(pz * c.beta1, c.opd, c.iopd);
+  p.x = p.x + qdiv(p.px * L, pz, ipz);
+  p.y = p.y + qdiv(p.py * L, pz, ipz);
   p.z = p.z - (L / betaz - Lb);
 }
 
 // sbend_exact_pass, simtrack.cpp:3833-3858.  B = [L, L/beta, href, 1/href, cosA, sinA].
+// Every quotient by href uses the element's RN(1/href); the two arcsine
+// arguments share RN(1/temp); temp/beta uses the cached RN(1/beta1).
 __device__ __forceinline__ void bend_exact(Particle &p, const PtCache &c, const double *B) {
   const double L = B[0], Lb = B[1], href = B[2], invh = B[3], cosA = B[4], sinA = B[5];
   const double x0 = p.x, px0 = p.px, py0 = p.py;
@@ -58,35 +84,38 @@ __device__ __forceinline__ void bend_exact(Particle &p, const PtCache &c, const 
   const double npx = px0 * cosA + (pz0 - 1. - href * x0) * sinA;
   const double pz1 = sqrt(c.opd2 - npx * npx - py0 * py0);
   const double der = (-px0) * sinA * href + (pz0 - 1. - x0 * href) * cosA * href;
-  p.x = pz1 / href - der / href / href - invh;
+  p.x = qdiv(pz1, href, invh) - qdiv(qdiv(der, href, invh), href, invh) - invh;
   const double temp = sqrt(c.opd2 - py0 * py0);
-  const double as1 = cr_asin(px0 / temp);
-  const double as2 = cr_asin(npx / temp);
+  const double itemp = 1.0 / temp;
+  const double as1 = cr_asin(qdiv(px0, temp, itemp));
+  const double as2 = cr_asin(qdiv(npx, temp, itemp));
   const double das = as1 - as2;
-  p.y = p.y + py0 * L + py0 * das / href;
-  const double t2 = c.opd * L + c.opd * das / href;
-  p.z = p.z - (t2 / c.beta1 - Lb);
+  p.y = p.y + py0 * L + qdiv(py0 * das, href, invh);
+  const double t2 = c.opd * L + qdiv(c.opd * das, href, invh);
+  p.z = p.z - (qdiv(t2, c.beta1, c.ibeta1) - Lb);
   p.px = npx;
 }
 
 // general_sbend_exact_pass, simtrack.cpp:3974-4010.
-// G = [L, L/beta, rhoc, b0, b0*rhoc, cosA, sinA]
-__device__ __forceinline__ void gbend_exact(Particle &p, const PtCache &c, const double *G) {
+// G = [L, L/beta, rhoc, b0, b0*rhoc, cosA, sinA, 1/rhoc, 1/b0]
+static __device__ __noinline__ void gbend_exact(Particle &p, const PtCache &c, const double *G) {
   const double L = G[0], Lb = G[1], rhoc = G[2], b0 = G[3], b0r = G[4], cosA = G[5], sinA = G[6];
+  const double irhoc = G[7], ib0 = G[8];
   const double x0 = p.x, px0 = p.px, py0 = p.py;
   const double pz0 = sqrt(c.opd2 - px0 * px0 - py0 * py0);
   const double w = pz0 - b0r - b0 * x0;
   const double npx = px0 * cosA + w * sinA;
   const double pz1 = sqrt(c.opd2 - npx * npx - py0 * py0);
-  const double der = (-px0) * sinA / rhoc + w * cosA / rhoc;
-  p.x = pz1 / b0 - der * rhoc / b0 - rhoc;
+  const double der = qdiv((-px0) * sinA, rhoc, irhoc) + qdiv(w * cosA, rhoc, irhoc);
+  p.x = qdiv(pz1, b0, ib0) - qdiv(der * rhoc, b0, ib0) - rhoc;
   const double temp = sqrt(c.opd2 - py0 * py0);
-  const double as1 = cr_asin(px0 / temp);
-  const double as2 = cr_asin(npx / temp);
+  const double itemp = 1.0 / temp;
+  const double as1 = cr_asin(qdiv(px0, temp, itemp));
+  const double as2 = cr_asin(qdiv(npx, temp, itemp));
   const double das = as1 - as2;
-  p.y = p.y + py0 * L / b0 / rhoc + py0 * das / b0;
-  const double t2 = c.opd * L / b0 / rhoc + c.opd * das / b0;
-  p.z = p.z - (t2 / c.beta1 - Lb);
+  p.y = p.y + qdiv(qdiv(py0 * L, b0, ib0), rhoc, irhoc) + qdiv(py0 * das, b0, ib0);
+  const double t2 = qdiv(qdiv(c.opd * L, b0, ib0), rhoc, irhoc) + qdiv(c.opd * das, b0, ib0);
+  p.z = p.z - (qdiv(t2, c.beta1, c.ibeta1) - Lb);
   p.px = npx;
 }
 
@@ -112,27 +141,27 @@ __device__ __forceinline__ void sext_kick(Particle &p, double kl, double ksl) {
 __device__ __forceinline__ void oct_kick(Particle &p, double kl, double ksl) {
   const double pr = p.x * p.x * p.x - 3 * p.x * p.y * p.y;
   const double pi = 3 * p.x * p.x * p.y - p.y * p.y * p.y;
-  const double Bx = (ksl * pr + kl * pi) / 6.;
-  const double By = (kl * pr - ksl * pi) / 6.;
+  const double Bx = qdiv(ksl * pr + kl * pi, 6., 1. / 6.);
+  const double By = qdiv(kl * pr - ksl * pi, 6., 1. / 6.);
   p.px = p.px - By;
   p.py = p.py + Bx;
 }
 
-// mult_kick_pass, simtrack.cpp:4086-4111.  K = [KNL0, KNSL0, (KNLi, KNSLi) i=1..norder]
+// mult_kick_pass, simtrack.cpp:4086-4111.  K = [KNL0, KNSL0, (KNLi, KNSLi, 1/i!) i=1..norder]
 __device__ __forceinline__ void mult_kick(Particle &p, int norder, const double *K) {
   double Xn = 1., Yn = 0.;
   double By = K[0], Bx = K[1];
-  int fac = 1;
+  double fac = 1.;
+#pragma unroll 1
   for (int i = 1; i <= norder; i++) {
     const double Xn0 = Xn, Yn0 = Yn;
     Xn = Xn0 * p.x - Yn0 * p.y;
     Yn = Xn0 * p.y + Yn0 * p.x;
-    fac = fac * i;
-    const double kn = K[2 * i], ks = K[2 * i + 1];
+    fac = fac * (double)i;
+    const double kn = K[3 * i - 1], ks = K[3 * i], ifac = K[3 * i + 1];
     if (kn != 0. || ks != 0.) {
-      const double f = (double)fac;
-      By = By + (kn * Xn - ks * Yn) / f;
-      Bx = Bx + (kn * Yn + ks * Xn) / f;
+      By = By + qdiv(kn * Xn - ks * Yn, fac, ifac);
+      Bx = Bx + qdiv(kn * Yn + ks * Xn, fac, ifac);
     }
   }
   p.px = p.px - By;
@@ -140,7 +169,7 @@ __device__ __forceinline__ void mult_kick(Particle &p, int norder, const double 
 }
 
 // Hard-edge quadrupole fringe maps, simtrack.cpp:4906-4920 (entry) and 4948-4956 (exit).
-__device__ __noinline__ void quad_fringe(Particle &p, double k, bool entry) {
+static __device__ __noinline__ void quad_fringe(Particle &p, double k, bool entry) {
   const double x0 = p.x, px0 = p.px, y0 = p.y, py0 = p.py, z0 = p.z, d0 = p.pt;
   const double a = k * (x0 * x0 * x0 + 3 * x0 * y0 * y0) / 12 / (1 + d0);
   const double b = k * ((x0 * x0 + y0 * y0) * px0 - 2 * x0 * y0 * py0) / 4 / (1 + d0);
@@ -189,7 +218,7 @@ __device__ __forceinline__ void ltog1(Particle &p, const double *M, int flags) {
 // rx[n], ry[n] for n = nu..1 and then consumes them for n = nc..1 with
 // nc < nu; both loops run downwards, so the two are fused here and the
 // arrays are not materialised.  Values are unchanged.
-__device__ __noinline__ void cerrf_dev(double xx, double yy, double &wx, double &wy) {
+static __device__ __noinline__ void cerrf_dev(double xx, double yy, double &wx, double &wy) {
   const double cc = 1.12837916709551, xlim = 5.33, ylim = 4.29, fac1 = 3.2, fac2 = 23, fac3 = 21;
   const double x = fabs(xx), y = fabs(yy);
   if (y < ylim && x < xlim) {
@@ -286,7 +315,7 @@ __device__ __forceinline__ void bb4d(double x, double y, double c4, double sigma
 // BB6D, simtrack.cpp:6622-6677 (slice loop).  P layout (built by the flattener):
 // [bbscale, emitx, emity, betax*, alfx*, betay*, alfy*, gx*, gy*, 2*emitx, 2*emity,
 //  temp3, c4, z_star[0..N-1]]
-__device__ __noinline__ void bb6d(Particle &p, const double *P, int nslice) {
+static __device__ __noinline__ void bb6d(Particle &p, const double *P, int nslice) {
   const double bbscale = P[0], emitx = P[1], emity = P[2];
   const double betax_s = P[3], alfx_s = P[4], betay_s = P[5], alfy_s = P[6];
   const double gx = P[7], gy = P[8], e2x = P[9], e2y = P[10], t3 = P[11], c4 = P[12];
@@ -324,7 +353,7 @@ __device__ __noinline__ void bb6d(Particle &p, const double *P, int nslice) {
 }
 
 // LBT_Pass, simtrack.cpp:6069-6093.  P = [sin, cos, tan]
-__device__ __noinline__ void lbt(Particle &p, const double *P) {
+static __device__ __noinline__ void lbt(Particle &p, const double *P) {
   const double st = P[0], ct = P[1], tt = P[2];
   const double x0 = p.x, px0 = p.px, y0 = p.y, py0 = p.py, z0 = p.z, pz0 = p.pt;
   const double ps0 = sqrt((1 + pz0) * (1 + pz0) - px0 * px0 - py0 * py0);
@@ -343,7 +372,7 @@ __device__ __noinline__ void lbt(Particle &p, const double *P) {
 }
 
 // ILBT_Pass, simtrack.cpp:6095-6123.  P = [sin, cos]
-__device__ __noinline__ void ilbt(Particle &p, const double *P) {
+static __device__ __noinline__ void ilbt(Particle &p, const double *P) {
   const double st = P[0], ct = P[1];
   const double xs = p.x, pxs = p.px, ys = p.y, pys = p.py, zs = p.z, pzs = p.pt;
   const double pss = sqrt((1 + pzs) * (1 + pzs) - pxs * pxs - pys * pys);
@@ -360,7 +389,7 @@ __device__ __noinline__ void ilbt(Particle &p, const double *P) {
 
 // CCMULT_Pass kick part, simtrack.cpp:6037-6064.
 // P = [kf, PHASE0, scale, brho, B2, A2, B3, A3, B4, A4, B5, A5]
-__device__ __noinline__ void ccmult_kick(Particle &p, const double *P) {
+static __device__ __noinline__ void ccmult_kick(Particle &p, const double *P) {
   const double kf = P[0], PHASE0 = P[1], scale = P[2], brho = P[3];
   const double B2 = P[4], A2 = P[5], B3 = P[6], A3 = P[7], B4 = P[8], A4 = P[9], B5 = P[10], A5 = P[11];
   const double arg = kf * p.z / 2.99792458e8 + PHASE0;

@@ -64,6 +64,8 @@ struct RefConsts {
   double gamma, beta, energy, brho;
   double sqrt_g2m1;  // sqrt(GP.gamma*GP.gamma-1.)
   double G;          // spin G
+  double ibeta;      // RN(1/GP.beta)
+  double ienergy;    // RN(1/GP.energy)
 };
 
 // Misalignment parameters sit in front of the element parameters when an

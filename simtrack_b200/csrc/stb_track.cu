@@ -81,132 +81,86 @@ __device__ __forceinline__ bool is_lost(const Particle &p, double apx, double ap
   return fabs(p.x) > apx || fabs(p.y) > apy || isnan(p.x) || isnan(p.y) || (r2 > 0.0 && p.x * p.x + p.y * p.y > r2);
 }
 
-// Runs one element on one particle.  Returns nothing; the caller checks loss.
-__device__ __forceinline__ void apply_element(const ElemHeader &h, const double *P, Particle &p, PtCache &c,
-                                              const RefConsts &R) {
-  const double *M = P;
-  if (h.flags & (EF_MISALIGN_OFFSET | EF_MISALIGN_ROLL)) {
-    gtol1(p, M, h.flags);
-    P += kMisalignParams;
+// Rarely executed element maps are kept out of line so the hot loop (drift,
+// bend, quadrupole and thin kicks) stays small in the instruction cache and
+// in registers.  They take the particle by reference (spilled around the
+// call, a few times per turn).
+
+__device__ __noinline__ void op_gsbend(const ElemHeader &h, const double *P, Particle &p, const PtCache &c) {
+  if (h.flags & EF_EDGE1) {
+    p.px = p.px + P[0] * p.x;
+    p.py = p.py - P[0] * p.y;
   }
+  gbend_exact(p, c, P + 2);
+  if (h.flags & EF_EDGE2) {
+    p.px = p.px + P[1] * p.x;
+    p.py = p.py - P[1] * p.y;
+  }
+}
+
+template <int kOrder>
+__device__ __noinline__ void op_thick_sext_oct(const ElemHeader &h, const double *P, Particle &p, const PtCache &c) {
+  const double d1 = P[0], d1b = P[1], d2 = P[2], d2b = P[3];
+  const double a1 = P[4], s1 = P[5], a2 = P[6], s2 = P[7];
+#pragma unroll 1
+  for (int s = 0; s < h.nint; s++) {
+    drift(p, c, d1, d1b);
+    if (kOrder == 2) sext_kick(p, a1, s1); else oct_kick(p, a1, s1);
+    drift(p, c, d2, d2b);
+    if (kOrder == 2) sext_kick(p, a2, s2); else oct_kick(p, a2, s2);
+    drift(p, c, d2, d2b);
+    if (kOrder == 2) sext_kick(p, a1, s1); else oct_kick(p, a1, s1);
+    drift(p, c, d1, d1b);
+  }
+}
+
+__device__ __noinline__ void op_mult_thick(const ElemHeader &h, const double *P, Particle &p, const PtCache &c) {
+  const double d1 = P[0], d1b = P[1], d2 = P[2], d2b = P[3];
+  const int no = h.aux;
+  const double *K1 = P + 4;
+  const double *K2 = K1 + 2 + 3 * no;
+#pragma unroll 1
+  for (int s = 0; s < h.nint; s++) {
+    drift(p, c, d1, d1b);
+    mult_kick(p, no, K1);
+    drift(p, c, d2, d2b);
+    mult_kick(p, no, K2);
+    drift(p, c, d2, d2b);
+    mult_kick(p, no, K1);
+    drift(p, c, d1, d1b);
+  }
+}
+
+__device__ __noinline__ void op_bendmult(const ElemHeader &h, const double *P, Particle &p, const PtCache &c) {
+  const int no = h.aux;
+  const double *B1 = P + 2, *B2 = P + 8;
+  const double *K1 = P + 14;
+  const double *K2 = K1 + 2 + 3 * no;
+  p.px = p.px + P[0] * p.x;
+  p.py = p.py - P[0] * p.y;
+#pragma unroll 1
+  for (int s = 0; s < h.nint; s++) {
+    bend_exact(p, c, B1);
+    mult_kick(p, no, K1);
+    bend_exact(p, c, B2);
+    mult_kick(p, no, K2);
+    bend_exact(p, c, B2);
+    mult_kick(p, no, K1);
+    bend_exact(p, c, B1);
+  }
+  p.px = p.px + P[1] * p.x;
+  p.py = p.py - P[1] * p.y;
+}
+
+__device__ __noinline__ void op_misc(const ElemHeader &h, const double *P, Particle &p, PtCache &c,
+                                     const RefConsts &R) {
   switch (h.op) {
-    case OP_DRIFT:
-      drift(p, c, P[0], P[1]);
-      break;
-    case OP_SBEND:
-      if (h.flags & EF_EDGE1) {
-        p.px = p.px + P[0] * p.x;
-        p.py = p.py - P[0] * p.y;
-      }
-      bend_exact(p, c, P + 2);
-      if (h.flags & EF_EDGE2) {
-        p.px = p.px + P[1] * p.x;
-        p.py = p.py - P[1] * p.y;
-      }
-      break;
-    case OP_GSBEND:
-      if (h.flags & EF_EDGE1) {
-        p.px = p.px + P[0] * p.x;
-        p.py = p.py - P[0] * p.y;
-      }
-      gbend_exact(p, c, P + 2);
-      if (h.flags & EF_EDGE2) {
-        p.px = p.px + P[1] * p.x;
-        p.py = p.py - P[1] * p.y;
-      }
-      break;
-    case OP_QUAD_THICK: {
-      const double d1 = P[0], d1b = P[1], d2 = P[2], d2b = P[3];
-      const double a1 = P[4], s1 = P[5], a2 = P[6], s2 = P[7];
-      if (h.flags & EF_FRINGE) quad_fringe(p, P[8], true);
-      for (int s = 0; s < h.nint; s++) {
-        drift(p, c, d1, d1b);
-        quad_kick(p, a1, s1);
-        drift(p, c, d2, d2b);
-        quad_kick(p, a2, s2);
-        drift(p, c, d2, d2b);
-        quad_kick(p, a1, s1);
-        drift(p, c, d1, d1b);
-      }
-      if (h.flags & EF_FRINGE) quad_fringe(p, P[8], false);
-      break;
-    }
-    case OP_SEXT_THICK: {
-      const double d1 = P[0], d1b = P[1], d2 = P[2], d2b = P[3];
-      const double a1 = P[4], s1 = P[5], a2 = P[6], s2 = P[7];
-      for (int s = 0; s < h.nint; s++) {
-        drift(p, c, d1, d1b);
-        sext_kick(p, a1, s1);
-        drift(p, c, d2, d2b);
-        sext_kick(p, a2, s2);
-        drift(p, c, d2, d2b);
-        sext_kick(p, a1, s1);
-        drift(p, c, d1, d1b);
-      }
-      break;
-    }
-    case OP_OCT_THICK: {
-      const double d1 = P[0], d1b = P[1], d2 = P[2], d2b = P[3];
-      const double a1 = P[4], s1 = P[5], a2 = P[6], s2 = P[7];
-      for (int s = 0; s < h.nint; s++) {
-        drift(p, c, d1, d1b);
-        oct_kick(p, a1, s1);
-        drift(p, c, d2, d2b);
-        oct_kick(p, a2, s2);
-        drift(p, c, d2, d2b);
-        oct_kick(p, a1, s1);
-        drift(p, c, d1, d1b);
-      }
-      break;
-    }
-    case OP_MULT_THICK: {
-      const double d1 = P[0], d1b = P[1], d2 = P[2], d2b = P[3];
-      const int no = h.aux;
-      const double *K1 = P + 4;
-      const double *K2 = K1 + 2 + 2 * no;
-      for (int s = 0; s < h.nint; s++) {
-        drift(p, c, d1, d1b);
-        mult_kick(p, no, K1);
-        drift(p, c, d2, d2b);
-        mult_kick(p, no, K2);
-        drift(p, c, d2, d2b);
-        mult_kick(p, no, K1);
-        drift(p, c, d1, d1b);
-      }
-      break;
-    }
-    case OP_QUAD_KICK:
-      quad_kick(p, P[0], P[1]);
-      break;
-    case OP_SEXT_KICK:
-      sext_kick(p, P[0], P[1]);
-      break;
     case OP_OCT_KICK:
       oct_kick(p, P[0], P[1]);
       break;
     case OP_MULT_KICK:
       mult_kick(p, h.aux, P);
       break;
-    case OP_BENDMULT: {
-      const int no = h.aux;
-      const double *B1 = P + 2, *B2 = P + 8;
-      const double *K1 = P + 14;
-      const double *K2 = K1 + 2 + 2 * no;
-      p.px = p.px + P[0] * p.x;
-      p.py = p.py - P[0] * p.y;
-      for (int s = 0; s < h.nint; s++) {
-        bend_exact(p, c, B1);
-        mult_kick(p, no, K1);
-        bend_exact(p, c, B2);
-        mult_kick(p, no, K2);
-        bend_exact(p, c, B2);
-        mult_kick(p, no, K1);
-        bend_exact(p, c, B1);
-      }
-      p.px = p.px + P[1] * p.x;
-      p.py = p.py - P[1] * p.y;
-      break;
-    }
     case OP_KICK:
       drift(p, c, P[0], P[1]);
       p.px = p.px + P[2];
@@ -258,14 +212,81 @@ __device__ __forceinline__ void apply_element(const ElemHeader &h, const double 
       p.py = p.py + Dpy * P[3];
       break;
     }
+    default:  // OP_IDENTITY
+      break;
+  }
+}
+
+// Runs one element on one particle; the caller checks loss.
+__device__ __forceinline__ void apply_element(const ElemHeader &h, const double *P, Particle &p, PtCache &c,
+                                              const RefConsts &R) {
+  const double *M = P;
+  if (h.flags & (EF_MISALIGN_OFFSET | EF_MISALIGN_ROLL)) {
+    gtol1(p, M, h.flags);
+    P += kMisalignParams;
+  }
+  switch (h.op) {
+    case OP_DRIFT:
+      drift(p, c, P[0], P[1]);
+      break;
+    case OP_SBEND:
+      if (h.flags & EF_EDGE1) {
+        p.px = p.px + P[0] * p.x;
+        p.py = p.py - P[0] * p.y;
+      }
+      bend_exact(p, c, P + 2);
+      if (h.flags & EF_EDGE2) {
+        p.px = p.px + P[1] * p.x;
+        p.py = p.py - P[1] * p.y;
+      }
+      break;
+    case OP_QUAD_THICK: {
+      const double d1 = P[0], d1b = P[1], d2 = P[2], d2b = P[3];
+      const double a1 = P[4], s1 = P[5], a2 = P[6], s2 = P[7];
+      if (h.flags & EF_FRINGE) quad_fringe(p, P[8], true);
+#pragma unroll 1
+      for (int s = 0; s < h.nint; s++) {
+        drift(p, c, d1, d1b);
+        quad_kick(p, a1, s1);
+        drift(p, c, d2, d2b);
+        quad_kick(p, a2, s2);
+        drift(p, c, d2, d2b);
+        quad_kick(p, a1, s1);
+        drift(p, c, d1, d1b);
+      }
+      if (h.flags & EF_FRINGE) quad_fringe(p, P[8], false);
+      break;
+    }
+    case OP_QUAD_KICK:
+      quad_kick(p, P[0], P[1]);
+      break;
+    case OP_SEXT_KICK:
+      sext_kick(p, P[0], P[1]);
+      break;
+    case OP_GSBEND:
+      op_gsbend(h, P, p, c);
+      break;
+    case OP_SEXT_THICK:
+      op_thick_sext_oct<2>(h, P, p, c);
+      break;
+    case OP_OCT_THICK:
+      op_thick_sext_oct<3>(h, P, p, c);
+      break;
+    case OP_MULT_THICK:
+      op_mult_thick(h, P, p, c);
+      break;
+    case OP_BENDMULT:
+      op_bendmult(h, P, p, c);
+      break;
     default:
+      op_misc(h, P, p, c, R);
       break;
   }
   if (h.flags & (EF_MISALIGN_OFFSET | EF_MISALIGN_ROLL)) ltog1(p, M, h.flags);
 }
 
-template <bool kSmem, int kBlock, bool kDump>
-__global__ void __launch_bounds__(kBlock, 1) track_kernel(const TrackArgs a) {
+template <bool kSmem, int kBlock, int kMinBlocks, bool kDump>
+__global__ void __launch_bounds__(kBlock, kMinBlocks) track_kernel(const TrackArgs a) {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ __align__(8) uint64_t bar;
   const ElemHeader *hdr = a.hdr;
@@ -340,9 +361,9 @@ int track_smem_limit(int device) {
 
 // Persistent grid: as many CTAs as fit on the device at once (never more
 // than the particles need); each CTA strides over the particle range.
-template <bool kSmem, int kBlock, bool kDump>
+template <bool kSmem, int kBlock, int kMinBlocks, bool kDump>
 static cudaError_t launch_variant(const TrackArgs &a, int num_sms, size_t smem, cudaStream_t stream) {
-  auto kern = track_kernel<kSmem, kBlock, kDump>;
+  auto kern = track_kernel<kSmem, kBlock, kMinBlocks, kDump>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   int per_sm = 0;
@@ -356,15 +377,29 @@ static cudaError_t launch_variant(const TrackArgs &a, int num_sms, size_t smem, 
   return cudaGetLastError();
 }
 
-cudaError_t launch_track(const TrackArgs &a, int num_sms, bool use_smem, cudaStream_t stream) {
+// Launch variants the autotuner chooses from: element table in shared
+// memory or read through L1, CTA size, and minimum resident CTAs per SM (which
+// caps registers per thread: 65536 / (block * min_blocks)).
+const TrackVariant kVariants[kNumTrackVariants] = {
+    {true, 512, 1, "smem_b512_r128"},   {true, 1024, 1, "smem_b1024_r64"},  {false, 256, 2, "l1_b256_r128"},
+    {false, 256, 3, "l1_b256_r80"},     {false, 256, 4, "l1_b256_r64"},     {false, 128, 6, "l1_b128_r80"},
+};
+
+cudaError_t launch_track(const TrackArgs &a, int num_sms, int variant, cudaStream_t stream) {
   const size_t sm = track_smem_bytes(a.nelem, a.npool_padded);
   if (a.dump) {
     // Per-element probe (diagnostics and parity tests): small particle counts only.
-    if (use_smem) return launch_variant<true, kTrackBlockGlobal, true>(a, num_sms, sm, stream);
-    return launch_variant<false, kTrackBlockGlobal, true>(a, num_sms, 0, stream);
+    return launch_variant<false, 256, 1, true>(a, num_sms, 0, stream);
   }
-  if (use_smem) return launch_variant<true, kTrackBlockSmem, false>(a, num_sms, sm, stream);
-  return launch_variant<false, kTrackBlockGlobal, false>(a, num_sms, 0, stream);
+  switch (variant) {
+    case 0: return launch_variant<true, 512, 1, false>(a, num_sms, sm, stream);
+    case 1: return launch_variant<true, 1024, 1, false>(a, num_sms, sm, stream);
+    case 2: return launch_variant<false, 256, 2, false>(a, num_sms, 0, stream);
+    case 3: return launch_variant<false, 256, 3, false>(a, num_sms, 0, stream);
+    case 4: return launch_variant<false, 256, 4, false>(a, num_sms, 0, stream);
+    case 5: return launch_variant<false, 128, 6, false>(a, num_sms, 0, stream);
+    default: return cudaErrorInvalidValue;
+  }
 }
 
 }  // namespace stb

@@ -75,3 +75,19 @@ def test_device_power_equals_host(native_lib):
     rng = np.random.default_rng(3)
     hm = np.stack([rng.random(20000) * 3 + 0.05, -rng.integers(6, 30, 20000).astype(np.float64)], 1).ravel()
     assert np.array_equal(ev(native_lib, 4, hm, 0), ev(native_lib, 4, hm, -1))
+
+
+@pytest.mark.gpu
+def test_shared_reciprocal_quotient_equals_ieee_division(native_lib):
+    """qdiv(a, b, RN(1/b)) (Markstein correction) against the IEEE quotient,
+    over random operands spanning many binades and significands near 1 and 2."""
+    rng = np.random.default_rng(11)
+    n = 2_000_000
+    a = rng.standard_normal(n) * 10.0 ** rng.integers(-12, 6, n)
+    b = (1.0 + rng.random(n)) * 2.0 ** rng.integers(-40, 20, n)
+    b[: n // 8] = np.nextafter(2.0, 0.0) * 2.0 ** rng.integers(-10, 10, n // 8)  # significand 1.11..1
+    a[n // 8: n // 4] = np.nextafter(1.0, 2.0) * rng.integers(1, 1000, n // 8)
+    ab = np.stack([a, b], 1).ravel()
+    q = ev(native_lib, 5, ab, 0)
+    assert np.array_equal(q, a / b)
+    assert np.array_equal(ev(native_lib, 15, ab, 0), a / b)
