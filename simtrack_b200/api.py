@@ -201,7 +201,7 @@ class Line:
             pass
 
 
-NUM_VARIANTS = 6
+NUM_VARIANTS = 9
 
 
 def variant_name(v: int) -> str:

@@ -15,9 +15,10 @@ struct TrackVariant {
   bool smem;       // element table staged in shared memory (else read through L1)
   int block;       // threads per CTA
   int min_blocks;  // __launch_bounds__ minimum resident CTAs per SM
+  int ppt;         // particles per thread
   const char *name;
 };
-constexpr int kNumTrackVariants = 6;
+constexpr int kNumTrackVariants = 9;
 extern const TrackVariant kVariants[kNumTrackVariants];
 
 struct TrackArgs {

@@ -217,75 +217,115 @@ __device__ __noinline__ void op_misc(const ElemHeader &h, const double *P, Parti
   }
 }
 
-// Runs one element on one particle; the caller checks loss.
-__device__ __forceinline__ void apply_element(const ElemHeader &h, const double *P, Particle &p, PtCache &c,
-                                              const RefConsts &R) {
+// Runs one element on the kPPT particles of this thread; the caller checks
+// loss.  For the hot element types the per-particle maps are issued back to
+// back, so their independent FP64 dependency chains interleave in the
+// instruction stream (latency hiding without more resident warps).
+template <int kPPT>
+__device__ __forceinline__ void apply_element(const ElemHeader &h, const double *P, Particle (&p)[kPPT],
+                                              PtCache (&c)[kPPT], const RefConsts &R) {
   const double *M = P;
-  if (h.flags & (EF_MISALIGN_OFFSET | EF_MISALIGN_ROLL)) {
-    gtol1(p, M, h.flags);
+  const bool mis = (h.flags & (EF_MISALIGN_OFFSET | EF_MISALIGN_ROLL)) != 0;
+  if (mis) {
+#pragma unroll
+    for (int k = 0; k < kPPT; k++) gtol1(p[k], M, h.flags);
     P += kMisalignParams;
   }
   switch (h.op) {
-    case OP_DRIFT:
-      drift(p, c, P[0], P[1]);
+    case OP_DRIFT: {
+      const double L = P[0], Lb = P[1];
+#pragma unroll
+      for (int k = 0; k < kPPT; k++) drift(p[k], c[k], L, Lb);
       break;
+    }
     case OP_SBEND:
-      if (h.flags & EF_EDGE1) {
-        p.px = p.px + P[0] * p.x;
-        p.py = p.py - P[0] * p.y;
-      }
-      bend_exact(p, c, P + 2);
-      if (h.flags & EF_EDGE2) {
-        p.px = p.px + P[1] * p.x;
-        p.py = p.py - P[1] * p.y;
+#pragma unroll
+      for (int k = 0; k < kPPT; k++) {
+        if (h.flags & EF_EDGE1) {
+          p[k].px = p[k].px + P[0] * p[k].x;
+          p[k].py = p[k].py - P[0] * p[k].y;
+        }
+        bend_exact(p[k], c[k], P + 2);
+        if (h.flags & EF_EDGE2) {
+          p[k].px = p[k].px + P[1] * p[k].x;
+          p[k].py = p[k].py - P[1] * p[k].y;
+        }
       }
       break;
     case OP_QUAD_THICK: {
       const double d1 = P[0], d1b = P[1], d2 = P[2], d2b = P[3];
       const double a1 = P[4], s1 = P[5], a2 = P[6], s2 = P[7];
-      if (h.flags & EF_FRINGE) quad_fringe(p, P[8], true);
+      if (h.flags & EF_FRINGE)
+        for (int k = 0; k < kPPT; k++) quad_fringe(p[k], P[8], true);
 #pragma unroll 1
       for (int s = 0; s < h.nint; s++) {
-        drift(p, c, d1, d1b);
-        quad_kick(p, a1, s1);
-        drift(p, c, d2, d2b);
-        quad_kick(p, a2, s2);
-        drift(p, c, d2, d2b);
-        quad_kick(p, a1, s1);
-        drift(p, c, d1, d1b);
+#pragma unroll
+        for (int k = 0; k < kPPT; k++) drift(p[k], c[k], d1, d1b);
+#pragma unroll
+        for (int k = 0; k < kPPT; k++) quad_kick(p[k], a1, s1);
+#pragma unroll
+        for (int k = 0; k < kPPT; k++) drift(p[k], c[k], d2, d2b);
+#pragma unroll
+        for (int k = 0; k < kPPT; k++) quad_kick(p[k], a2, s2);
+#pragma unroll
+        for (int k = 0; k < kPPT; k++) drift(p[k], c[k], d2, d2b);
+#pragma unroll
+        for (int k = 0; k < kPPT; k++) quad_kick(p[k], a1, s1);
+#pragma unroll
+        for (int k = 0; k < kPPT; k++) drift(p[k], c[k], d1, d1b);
       }
-      if (h.flags & EF_FRINGE) quad_fringe(p, P[8], false);
+      if (h.flags & EF_FRINGE)
+        for (int k = 0; k < kPPT; k++) quad_fringe(p[k], P[8], false);
       break;
     }
     case OP_QUAD_KICK:
-      quad_kick(p, P[0], P[1]);
+#pragma unroll
+      for (int k = 0; k < kPPT; k++) quad_kick(p[k], P[0], P[1]);
       break;
     case OP_SEXT_KICK:
-      sext_kick(p, P[0], P[1]);
+#pragma unroll
+      for (int k = 0; k < kPPT; k++) sext_kick(p[k], P[0], P[1]);
       break;
     case OP_GSBEND:
-      op_gsbend(h, P, p, c);
+      for (int k = 0; k < kPPT; k++) op_gsbend(h, P, p[k], c[k]);
       break;
     case OP_SEXT_THICK:
-      op_thick_sext_oct<2>(h, P, p, c);
+      for (int k = 0; k < kPPT; k++) op_thick_sext_oct<2>(h, P, p[k], c[k]);
       break;
     case OP_OCT_THICK:
-      op_thick_sext_oct<3>(h, P, p, c);
+      for (int k = 0; k < kPPT; k++) op_thick_sext_oct<3>(h, P, p[k], c[k]);
       break;
     case OP_MULT_THICK:
-      op_mult_thick(h, P, p, c);
+      for (int k = 0; k < kPPT; k++) op_mult_thick(h, P, p[k], c[k]);
       break;
     case OP_BENDMULT:
-      op_bendmult(h, P, p, c);
+      for (int k = 0; k < kPPT; k++) op_bendmult(h, P, p[k], c[k]);
       break;
     default:
-      op_misc(h, P, p, c, R);
+      for (int k = 0; k < kPPT; k++) op_misc(h, P, p[k], c[k], R);
       break;
   }
-  if (h.flags & (EF_MISALIGN_OFFSET | EF_MISALIGN_ROLL)) ltog1(p, M, h.flags);
+  if (mis) {
+#pragma unroll
+    for (int k = 0; k < kPPT; k++) ltog1(p[k], M, h.flags);
+  }
 }
 
-template <bool kSmem, int kBlock, int kMinBlocks, bool kDump>
+__device__ __forceinline__ void store_particle(const TrackArgs &a, long i, const Particle &p) {
+  a.x[i] = p.x;
+  a.px[i] = p.px;
+  a.y[i] = p.y;
+  a.py[i] = p.py;
+  a.z[i] = p.z;
+  a.pt[i] = p.pt;
+}
+
+// kPPT particles per thread: particle base + k*kBlock for k < kPPT, so every
+// load and store of a warp stays coalesced.  A particle that is lost has its
+// coordinates and loss record stored at once; its slot is then reset to the
+// reference orbit so the remaining particles of the thread keep running on
+// benign operands.
+template <bool kSmem, int kBlock, int kMinBlocks, int kPPT, bool kDump>
 __global__ void __launch_bounds__(kBlock, kMinBlocks) track_kernel(const TrackArgs a) {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ __align__(8) uint64_t bar;
@@ -300,50 +340,64 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) track_kernel(const TrackAr
     pool = reinterpret_cast<const double *>(smem + (size_t)a.nelem * sizeof(ElemHeader));
   }
   const RefConsts R = a.ref;
-  const long stride = (long)gridDim.x * blockDim.x;
-  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += stride) {
-    if (a.lost_turn[i] >= 0) continue;
-    Particle p;
-    p.x = a.x[i];
-    p.px = a.px[i];
-    p.y = a.y[i];
-    p.py = a.py[i];
-    p.z = a.z[i];
-    p.pt = a.pt[i];
-    // Track()'s entry quick check, simtrack.cpp:20795-20796
-    if (a.turn0 == 0 && (fabs(p.x) > 0.1 || fabs(p.y) > 0.1)) {
-      a.lost_turn[i] = 0;
-      a.lost_elem[i] = 0;
-      continue;
-    }
-    PtCache c;
-    pt_refresh(R, p.pt, c);
-    int lt = -1, le = 0;
-    for (int t = 0; t < a.nturn && lt < 0; t++) {
-      for (int e = 0; e < a.nelem; e++) {
-        const ElemHeader h = hdr[e];
-        apply_element(h, pool + h.poff, p, c, R);
-        if (kDump) {
-          double *d = a.dump + (((size_t)i * a.nturn + t) * a.nelem + e) * 6;
-          d[0] = p.x; d[1] = p.px; d[2] = p.y; d[3] = p.py; d[4] = p.z; d[5] = p.pt;
-        }
-        if (is_lost(p, h.apx, h.apy, a.r2)) {
-          lt = a.turn0 + t;
-          le = e;
-          break;
+  const long chunk = (long)kBlock * kPPT;
+  const long stride = (long)gridDim.x * chunk;
+  for (long base = (long)blockIdx.x * chunk + threadIdx.x; base < a.n; base += stride) {
+    Particle p[kPPT];
+    PtCache c[kPPT];
+    bool alive[kPPT];
+    int nalive = 0;
+#pragma unroll
+    for (int k = 0; k < kPPT; k++) {
+      const long i = base + (long)k * kBlock;
+      alive[k] = i < a.n && a.lost_turn[i] < 0;
+      p[k] = Particle{0., 0., 0., 0., 0., 0.};
+      if (alive[k]) {
+        p[k].x = a.x[i];
+        p[k].px = a.px[i];
+        p[k].y = a.y[i];
+        p[k].py = a.py[i];
+        p[k].z = a.z[i];
+        p[k].pt = a.pt[i];
+        // Track()'s entry quick check, simtrack.cpp:20795-20796
+        if (a.turn0 == 0 && (fabs(p[k].x) > 0.1 || fabs(p[k].y) > 0.1)) {
+          a.lost_turn[i] = 0;
+          a.lost_elem[i] = 0;
+          alive[k] = false;
+          p[k] = Particle{0., 0., 0., 0., 0., 0.};
         }
       }
+      pt_refresh(R, p[k].pt, c[k]);
+      nalive += alive[k] ? 1 : 0;
     }
-    a.x[i] = p.x;
-    a.px[i] = p.px;
-    a.y[i] = p.y;
-    a.py[i] = p.py;
-    a.z[i] = p.z;
-    a.pt[i] = p.pt;
-    if (lt >= 0) {
-      a.lost_turn[i] = lt;
-      a.lost_elem[i] = le;
+    for (int t = 0; t < a.nturn && nalive > 0; t++) {
+      for (int e = 0; e < a.nelem; e++) {
+        const ElemHeader h = hdr[e];
+        apply_element<kPPT>(h, pool + h.poff, p, c, R);
+#pragma unroll
+        for (int k = 0; k < kPPT; k++) {
+          if (!alive[k]) continue;
+          const long i = base + (long)k * kBlock;
+          if (kDump) {
+            double *d = a.dump + (((size_t)i * a.nturn + t) * a.nelem + e) * 6;
+            d[0] = p[k].x; d[1] = p[k].px; d[2] = p[k].y; d[3] = p[k].py; d[4] = p[k].z; d[5] = p[k].pt;
+          }
+          if (is_lost(p[k], h.apx, h.apy, a.r2)) {
+            store_particle(a, i, p[k]);
+            a.lost_turn[i] = a.turn0 + t;
+            a.lost_elem[i] = e;
+            alive[k] = false;
+            nalive--;
+            p[k] = Particle{0., 0., 0., 0., 0., 0.};
+            pt_refresh(R, 0.0, c[k]);
+          }
+        }
+        if (nalive == 0) break;
+      }
     }
+#pragma unroll
+    for (int k = 0; k < kPPT; k++)
+      if (alive[k]) store_particle(a, base + (long)k * kBlock, p[k]);
   }
 }
 
@@ -361,16 +415,17 @@ int track_smem_limit(int device) {
 
 // Persistent grid: as many CTAs as fit on the device at once (never more
 // than the particles need); each CTA strides over the particle range.
-template <bool kSmem, int kBlock, int kMinBlocks, bool kDump>
+template <bool kSmem, int kBlock, int kMinBlocks, int kPPT, bool kDump>
 static cudaError_t launch_variant(const TrackArgs &a, int num_sms, size_t smem, cudaStream_t stream) {
-  auto kern = track_kernel<kSmem, kBlock, kMinBlocks, kDump>;
+  auto kern = track_kernel<kSmem, kBlock, kMinBlocks, kPPT, kDump>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   int per_sm = 0;
   e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBlock, smem);
   if (e != cudaSuccess) return e;
   if (per_sm < 1) return cudaErrorInvalidConfiguration;
-  long need = (a.n + kBlock - 1) / kBlock;
+  const long chunk = (long)kBlock * kPPT;
+  long need = (a.n + chunk - 1) / chunk;
   long grid = (long)num_sms * per_sm;
   if (grid > need) grid = need;
   kern<<<(unsigned)grid, kBlock, smem, stream>>>(a);
@@ -378,26 +433,33 @@ static cudaError_t launch_variant(const TrackArgs &a, int num_sms, size_t smem, 
 }
 
 // Launch variants the autotuner chooses from: element table in shared
-// memory or read through L1, CTA size, and minimum resident CTAs per SM (which
-// caps registers per thread: 65536 / (block * min_blocks)).
+// memory or read through L1, CTA size, minimum resident CTAs per SM (which
+// caps registers per thread at 65536 / (block * min_blocks)) and particles
+// per thread.
 const TrackVariant kVariants[kNumTrackVariants] = {
-    {true, 512, 1, "smem_b512_r128"},   {true, 1024, 1, "smem_b1024_r64"},  {false, 256, 2, "l1_b256_r128"},
-    {false, 256, 3, "l1_b256_r80"},     {false, 256, 4, "l1_b256_r64"},     {false, 128, 6, "l1_b128_r80"},
+    {true, 512, 1, 1, "smem_b512_r128"},       {true, 1024, 1, 1, "smem_b1024_r64"},
+    {false, 256, 2, 1, "l1_b256_r128"},        {false, 256, 3, 1, "l1_b256_r80"},
+    {false, 256, 4, 1, "l1_b256_r64"},         {false, 128, 6, 1, "l1_b128_r80"},
+    {true, 512, 1, 2, "smem_b512_r128_ppt2"},  {false, 256, 2, 2, "l1_b256_r128_ppt2"},
+    {false, 128, 3, 2, "l1_b128_r168_ppt2"},
 };
 
 cudaError_t launch_track(const TrackArgs &a, int num_sms, int variant, cudaStream_t stream) {
   const size_t sm = track_smem_bytes(a.nelem, a.npool_padded);
   if (a.dump) {
     // Per-element probe (diagnostics and parity tests): small particle counts only.
-    return launch_variant<false, 256, 1, true>(a, num_sms, 0, stream);
+    return launch_variant<false, 256, 1, 1, true>(a, num_sms, 0, stream);
   }
   switch (variant) {
-    case 0: return launch_variant<true, 512, 1, false>(a, num_sms, sm, stream);
-    case 1: return launch_variant<true, 1024, 1, false>(a, num_sms, sm, stream);
-    case 2: return launch_variant<false, 256, 2, false>(a, num_sms, 0, stream);
-    case 3: return launch_variant<false, 256, 3, false>(a, num_sms, 0, stream);
-    case 4: return launch_variant<false, 256, 4, false>(a, num_sms, 0, stream);
-    case 5: return launch_variant<false, 128, 6, false>(a, num_sms, 0, stream);
+    case 0: return launch_variant<true, 512, 1, 1, false>(a, num_sms, sm, stream);
+    case 1: return launch_variant<true, 1024, 1, 1, false>(a, num_sms, sm, stream);
+    case 2: return launch_variant<false, 256, 2, 1, false>(a, num_sms, 0, stream);
+    case 3: return launch_variant<false, 256, 3, 1, false>(a, num_sms, 0, stream);
+    case 4: return launch_variant<false, 256, 4, 1, false>(a, num_sms, 0, stream);
+    case 5: return launch_variant<false, 128, 6, 1, false>(a, num_sms, 0, stream);
+    case 6: return launch_variant<true, 512, 1, 2, false>(a, num_sms, sm, stream);
+    case 7: return launch_variant<false, 256, 2, 2, false>(a, num_sms, 0, stream);
+    case 8: return launch_variant<false, 128, 3, 2, false>(a, num_sms, 0, stream);
     default: return cudaErrorInvalidValue;
   }
 }
