@@ -51,6 +51,7 @@ def parse():
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-procs", type=int, default=0)
+    ap.add_argument("--variant", type=int, default=-1, help="force a kernel launch variant (skips the autotuner)")
     return ap.parse_args()
 
 
@@ -234,7 +235,11 @@ def run_ours(a):
     le_ = torch.zeros(n, dtype=torch.int32, device=dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
 
-    tune = tab.autotune(coords, nturn=1, aperture_radius=lat.aperture_radius)
+    if a.variant >= 0:
+        tab.set_variant(a.variant)
+        tune = {"ms": {}}
+    else:
+        tune = tab.autotune(coords, nturn=1, aperture_radius=lat.aperture_radius)
     info = tab.info()
 
     peak = ctypes.c_double()

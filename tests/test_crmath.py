@@ -16,7 +16,7 @@ import pytest
 
 def ev(native_lib, fn, x, device):
     x = np.ascontiguousarray(x, dtype=np.float64)
-    n = x.size // (2 if fn in (4, 14) else 1)
+    n = x.size // (2 if fn in (4, 5, 14, 15) else 1)
     out = np.empty(n)
     rc = native_lib.stb_math_eval(fn, x.ctypes.data_as(POINTER(c_double)), out.ctypes.data_as(POINTER(c_double)),
                                   n, device)
