@@ -311,7 +311,7 @@ def run_ours(a):
                     "config": {"workload": WORKLOAD, "particles_per_gpu": n, "turns_per_step": T,
                                "elements": info["elements"], "l2": "256 MiB flush between timed steps",
                                "parallelism": f"particle shards x{world}, no exchange",
-                               "kernel_variant": info["variant_name"],
+                               "kernel_variant": info["variant_name"], "kernel_variant_index": info["variant"],
                                "autotune_ms_1turn": {k: round(v, 3) for k, v in tune["ms"].items()}},
                     "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": a.steps,
                     "clocks": clk.summary(), "alive": [alive0, alive1]}

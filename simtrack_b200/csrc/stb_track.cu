@@ -115,19 +115,19 @@ __device__ __noinline__ void op_thick_sext_oct(const ElemHeader &h, const double
 }
 
 __device__ __noinline__ void op_mult_thick(const ElemHeader &h, const double *P, Particle &p, const PtCache &c) {
-  const double d1 = P[0], d1b = P[1], d2 = P[2], d2b = P[3];
+  const volatile double *V = P;
   const int no = h.aux;
   const double *K1 = P + 4;
   const double *K2 = K1 + 2 + 3 * no;
 #pragma unroll 1
   for (int s = 0; s < h.nint; s++) {
-    drift(p, c, d1, d1b);
+    drift(p, c, V[0], V[1]);
     mult_kick(p, no, K1);
-    drift(p, c, d2, d2b);
+    drift(p, c, V[2], V[3]);
     mult_kick(p, no, K2);
-    drift(p, c, d2, d2b);
+    drift(p, c, V[2], V[3]);
     mult_kick(p, no, K1);
-    drift(p, c, d1, d1b);
+    drift(p, c, V[0], V[1]);
   }
 }
 
@@ -253,26 +253,27 @@ __device__ __forceinline__ void apply_element(const ElemHeader &h, const double 
       }
       break;
     case OP_QUAD_THICK: {
-      const double d1 = P[0], d1b = P[1], d2 = P[2], d2b = P[3];
-      const double a1 = P[4], s1 = P[5], a2 = P[6], s2 = P[7];
+      // Slice constants are re-read from the table at each use (volatile view)
+      // instead of being hoisted into eight live register pairs.
+      const volatile double *V = P;
       if (h.flags & EF_FRINGE)
         for (int k = 0; k < kPPT; k++) quad_fringe(p[k], P[8], true);
 #pragma unroll 1
       for (int s = 0; s < h.nint; s++) {
 #pragma unroll
-        for (int k = 0; k < kPPT; k++) drift(p[k], c[k], d1, d1b);
+        for (int k = 0; k < kPPT; k++) drift(p[k], c[k], V[0], V[1]);
 #pragma unroll
-        for (int k = 0; k < kPPT; k++) quad_kick(p[k], a1, s1);
+        for (int k = 0; k < kPPT; k++) quad_kick(p[k], V[4], V[5]);
 #pragma unroll
-        for (int k = 0; k < kPPT; k++) drift(p[k], c[k], d2, d2b);
+        for (int k = 0; k < kPPT; k++) drift(p[k], c[k], V[2], V[3]);
 #pragma unroll
-        for (int k = 0; k < kPPT; k++) quad_kick(p[k], a2, s2);
+        for (int k = 0; k < kPPT; k++) quad_kick(p[k], V[6], V[7]);
 #pragma unroll
-        for (int k = 0; k < kPPT; k++) drift(p[k], c[k], d2, d2b);
+        for (int k = 0; k < kPPT; k++) drift(p[k], c[k], V[2], V[3]);
 #pragma unroll
-        for (int k = 0; k < kPPT; k++) quad_kick(p[k], a1, s1);
+        for (int k = 0; k < kPPT; k++) quad_kick(p[k], V[4], V[5]);
 #pragma unroll
-        for (int k = 0; k < kPPT; k++) drift(p[k], c[k], d1, d1b);
+        for (int k = 0; k < kPPT; k++) drift(p[k], c[k], V[0], V[1]);
       }
       if (h.flags & EF_FRINGE)
         for (int k = 0; k < kPPT; k++) quad_fringe(p[k], P[8], false);
@@ -326,7 +327,7 @@ __device__ __forceinline__ void store_particle(const TrackArgs &a, long i, const
 // reference orbit so the remaining particles of the thread keep running on
 // benign operands.
 template <bool kSmem, int kBlock, int kMinBlocks, int kPPT, bool kDump>
-__global__ void __launch_bounds__(kBlock, kMinBlocks) track_kernel(const TrackArgs a) {
+__global__ void __launch_bounds__(kBlock, kMinBlocks) track_kernel(const __grid_constant__ TrackArgs a) {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ __align__(8) uint64_t bar;
   const ElemHeader *hdr = a.hdr;
@@ -339,7 +340,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) track_kernel(const TrackAr
     hdr = reinterpret_cast<const ElemHeader *>(smem);
     pool = reinterpret_cast<const double *>(smem + (size_t)a.nelem * sizeof(ElemHeader));
   }
-  const RefConsts R = a.ref;
+  const RefConsts &R = a.ref;
   const long chunk = (long)kBlock * kPPT;
   const long stride = (long)gridDim.x * chunk;
   for (long base = (long)blockIdx.x * chunk + threadIdx.x; base < a.n; base += stride) {
@@ -438,9 +439,9 @@ static cudaError_t launch_variant(const TrackArgs &a, int num_sms, size_t smem, 
 // per thread.
 const TrackVariant kVariants[kNumTrackVariants] = {
     {true, 512, 1, 1, "smem_b512_r128"},       {true, 1024, 1, 1, "smem_b1024_r64"},
-    {false, 256, 2, 1, "l1_b256_r128"},        {false, 256, 3, 1, "l1_b256_r80"},
-    {false, 256, 4, 1, "l1_b256_r64"},         {false, 128, 6, 1, "l1_b128_r80"},
-    {true, 512, 1, 2, "smem_b512_r128_ppt2"},  {false, 256, 2, 2, "l1_b256_r128_ppt2"},
+    {true, 768, 1, 1, "smem_b768_r85"},        {false, 256, 2, 1, "l1_b256_r128"},
+    {false, 256, 3, 1, "l1_b256_r80"},         {false, 256, 4, 1, "l1_b256_r64"},
+    {false, 384, 2, 1, "l1_b384_r85"},         {true, 512, 1, 2, "smem_b512_r128_ppt2"},
     {false, 128, 3, 2, "l1_b128_r168_ppt2"},
 };
 
@@ -453,12 +454,12 @@ cudaError_t launch_track(const TrackArgs &a, int num_sms, int variant, cudaStrea
   switch (variant) {
     case 0: return launch_variant<true, 512, 1, 1, false>(a, num_sms, sm, stream);
     case 1: return launch_variant<true, 1024, 1, 1, false>(a, num_sms, sm, stream);
-    case 2: return launch_variant<false, 256, 2, 1, false>(a, num_sms, 0, stream);
-    case 3: return launch_variant<false, 256, 3, 1, false>(a, num_sms, 0, stream);
-    case 4: return launch_variant<false, 256, 4, 1, false>(a, num_sms, 0, stream);
-    case 5: return launch_variant<false, 128, 6, 1, false>(a, num_sms, 0, stream);
-    case 6: return launch_variant<true, 512, 1, 2, false>(a, num_sms, sm, stream);
-    case 7: return launch_variant<false, 256, 2, 2, false>(a, num_sms, 0, stream);
+    case 2: return launch_variant<true, 768, 1, 1, false>(a, num_sms, sm, stream);
+    case 3: return launch_variant<false, 256, 2, 1, false>(a, num_sms, 0, stream);
+    case 4: return launch_variant<false, 256, 3, 1, false>(a, num_sms, 0, stream);
+    case 5: return launch_variant<false, 256, 4, 1, false>(a, num_sms, 0, stream);
+    case 6: return launch_variant<false, 384, 2, 1, false>(a, num_sms, 0, stream);
+    case 7: return launch_variant<true, 512, 1, 2, false>(a, num_sms, sm, stream);
     case 8: return launch_variant<false, 128, 3, 2, false>(a, num_sms, 0, stream);
     default: return cudaErrorInvalidValue;
   }
