@@ -32,6 +32,7 @@ extern "C" {
 typedef struct stb_element stb_element; /* Element*  (simtrack.h:373-396) */
 typedef struct stb_line stb_line;       /* Line      (simtrack.h:1067-1100) */
 typedef struct stb_table stb_table;     /* flattened device element table (no reference counterpart) */
+typedef struct stb_scan stb_scan;       /* batched dynamic-aperture scan (replaces the Track_DA* loops) */
 
 /* Message of the last failed call on this thread ("" if none). */
 const char *stb_last_error(void);
@@ -135,6 +136,32 @@ int stb_track_host(stb_table *t, double *x, long n, int nturn, double aperture_r
  * diagnostics.  Intended for small n. */
 int stb_track_probe(stb_table *t, double *x, long n, int nturn, double aperture_radius, double *dump, int *stable,
                     int *lost_turn, int *lost_post);
+
+/* ---- batched dynamic-aperture scan ----
+ * Replaces the per-particle loops of the DA drivers (Track_DA, simtrack.cpp:21389-21441;
+ * Track_DA_Radial_Uniform, 21736-21764), which call Track() once per initial
+ * condition: nseed lattices (one table per field-error seed, all flattened for
+ * the same reference particle, all on `device`) x n_per_seed[s] initial
+ * conditions each, given as one host AoS array x0 (seed 0's particles first).
+ * The tables must outlive the scan.  Particles are tracked in turn blocks of
+ * work list / tracking / compaction; Track()'s loss convention and entry
+ * check apply, plus the circular aperture when aperture_radius > 0. */
+int stb_scan_create(stb_table **tables, int nseed, const double *x0, const long *n_per_seed, double aperture_radius,
+                    int device, stb_scan **out);
+int stb_scan_free(stb_scan *s);
+/* Launch variant of the scan's tracking kernel (< 0 keeps the current one) and
+ * particles per work item (<= 0 keeps the current one; multiple of 32, >= 64). */
+int stb_scan_configure(stb_scan *s, int variant, int chunk);
+/* Advances all live particles by nturn turns (stops early when none is left),
+ * turns_per_block turns between compactions; use_graph != 0 replays the turn
+ * blocks from a captured CUDA graph.  Synchronous. */
+int stb_scan_run(stb_scan *s, int nturn, int turns_per_block, int use_graph);
+/* Per original particle (in x0 order): Track()'s lost turn (-1: still alive),
+ * element index of the loss, and the coordinates (AoS, at the loss or now).
+ * Any output pointer may be NULL. */
+int stb_scan_results(stb_scan *s, int32_t *lost_turn, int32_t *lost_elem, double *x_aos);
+/* st[0] turns done, [1] device milliseconds, [2] turn blocks, [3] variant, [4] chunk, [5] particles */
+int stb_scan_stats(const stb_scan *s, double *st6);
 
 /* Diagnostics (no reference counterpart): evaluates the kernels' elementary
  * functions on host buffers, on GPU `device` (device >= 0) or on the host CPU

@@ -300,3 +300,50 @@ def Track(line: Line, x, nturn: int, stable: int = 1):
     for k in range(6):
         x[k] = arr[0, k]
     return int(st[0]), int(lt[0]), int(lp[0])
+
+
+class Scan:
+    """Batched dynamic-aperture scan over several seed tables (stb_scan_*)."""
+
+    def __init__(self, tables, x0_per_seed, aperture_radius: float = 0.0, device: int = 0):
+        self._tables = list(tables)  # keep the tables alive for the scan's lifetime
+        xs = [np.ascontiguousarray(x, dtype=np.float64).reshape(-1, 6) for x in x0_per_seed]
+        if len(xs) != len(self._tables):
+            raise SimTrackError(-1, "one particle array per table")
+        self.n_per_seed = np.array([len(x) for x in xs], dtype=np.int64)
+        x0 = np.ascontiguousarray(np.concatenate(xs, axis=0))
+        arr = (c_void_p * len(self._tables))(*[t._h for t in self._tables])
+        nps = (ctypes.c_long * len(xs))(*[int(v) for v in self.n_per_seed])
+        h = c_void_p()
+        check(lib().stb_scan_create(arr, len(xs), x0.ctypes.data_as(POINTER(c_double)), nps, aperture_radius,
+                                    device, byref(h)))
+        self._h = h
+        self.n = int(self.n_per_seed.sum())
+
+    def configure(self, variant: int = -1, chunk: int = 0) -> None:
+        check(lib().stb_scan_configure(self._h, variant, chunk))
+
+    def run(self, nturn: int, turns_per_block: int = 256, use_graph: bool = True) -> None:
+        check(lib().stb_scan_run(self._h, nturn, turns_per_block, int(use_graph)))
+
+    def results(self):
+        """(lost_turn[n] (-1 alive), lost_elem[n], x[n, 6]) in input order."""
+        lt = np.empty(self.n, dtype=np.int32)
+        le = np.empty(self.n, dtype=np.int32)
+        x = np.empty((self.n, 6))
+        check(lib().stb_scan_results(self._h, c_void_p(lt.ctypes.data), c_void_p(le.ctypes.data),
+                                     c_void_p(x.ctypes.data)))
+        return lt, le, x
+
+    def stats(self) -> dict:
+        st = (c_double * 6)()
+        check(lib().stb_scan_stats(self._h, st))
+        return {"turns": int(st[0]), "device_ms": st[1], "blocks": int(st[2]), "variant": int(st[3]),
+                "chunk": int(st[4]), "particles": int(st[5])}
+
+    def __del__(self):
+        try:
+            if self._h:
+                lib().stb_scan_free(self._h)
+        except Exception:
+            pass

@@ -1,0 +1,75 @@
+// Internal runtime pieces shared by the C ABI translation units: the table
+// object, status-code plumbing and CUDA error handling.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "simtrack_b200.hpp"
+#include "stb_flatten.hpp"
+#include "stb_kernels.hpp"
+#include "stb_status.hpp"
+
+struct stb_table {
+  int device = 0;
+  stb::HostTable host;
+  stb::ElemHeader *d_hdr = nullptr;
+  double *d_pool = nullptr;
+  int npool_padded = 0;
+  bool use_smem = false;  // the table fits the shared-memory variants
+  int variant = 2;        // launch variant (stb::kVariants), set by the autotuner
+  int *d_status = nullptr;
+  int num_sms = 0;
+};
+
+namespace stb {
+
+// Runs f(), mapping exceptions onto status codes and the thread's message.
+template <class F>
+int guarded(F &&f) {
+  try {
+    int rc = f();
+    if (rc == STB_OK) set_last_error("");
+    return rc;
+  } catch (const Error &e) {
+    set_last_error(e.what());
+    return e.code;
+  } catch (const std::bad_alloc &) {
+    set_last_error("host allocation failed");
+    return STB_ENOMEM;
+  } catch (const std::exception &e) {
+    set_last_error(e.what());
+    return STB_EINVAL;
+  }
+}
+
+inline void cuda_check(cudaError_t e, const char *what) {
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    throw Error(e == cudaErrorMemoryAllocation ? STB_ENOMEM : STB_ECUDA,
+                std::string(what) + ": " + cudaGetErrorString(e));
+  }
+}
+
+// Restores the caller's current device on scope exit.
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cuda_check(cudaGetDevice(&prev), "cudaGetDevice");
+    if (prev != dev) cuda_check(cudaSetDevice(dev), "cudaSetDevice");
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    if (cudaGetDevice(&cur) == cudaSuccess && cur != prev && prev >= 0) cudaSetDevice(prev);
+  }
+};
+
+// cudaFree on scope exit.
+struct DevFree {
+  void *p;
+  ~DevFree() {
+    if (p) cudaFree(p);
+  }
+};
+
+}  // namespace stb

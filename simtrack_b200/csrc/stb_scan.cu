@@ -1,0 +1,284 @@
+// Batched dynamic-aperture scan: many lattices (one per field-error seed) x
+// per-seed particle grids, tracked turn block by turn block on one GPU.
+//
+// Per turn block (all device-side, so a block of them is captured once in a
+// CUDA graph and replayed):
+//   1. scan_worklist_kernel  builds the work list: for every seed, its live
+//      particles (always the first live[s] slots of the seed's range) are cut
+//      into chunks of `chunk` particles; items are (seed, first slot).
+//   2. scan_track_kernel     persistent CTAs pull items from an atomic
+//      counter, stage that seed's element table into shared memory when it
+//      differs from the one already staged (bulk TMA copies), and track the
+//      item's particles for `nturn` turns starting at the device turn counter.
+//   3. scan_compact_kernel   one CTA per seed stably compacts the seed's live
+//      particles to the front of its range (warp ballots + a block prefix
+//      sum), writes the final state of every particle lost in this block to
+//      the outputs (indexed by original particle id) and advances the turn
+//      counter.
+// Dead lanes therefore stop costing cycles at the next turn-block boundary,
+// and the work list shrinks with the uneven survival of the seeds.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "stb_scan.hpp"
+#include "stb_track_impl.cuh"
+
+namespace stb {
+
+namespace {
+
+constexpr int kCompactBlock = 1024;
+
+__global__ void scan_worklist_kernel(ScanArgs a) {
+  __shared__ int pre[kMaxScanSeeds + 1];
+  const int s = threadIdx.x;
+  int n = 0;
+  if (s < a.nseed) n = (a.live[s] + a.chunk - 1) / a.chunk;
+  // Exclusive prefix sum over the (<= 1024) seeds.
+  pre[s + 1] = n;
+  if (s == 0) pre[0] = 0;
+  __syncthreads();
+  for (int off = 1; off <= a.nseed; off <<= 1) {
+    int v = 0;
+    if (s + 1 > off && s < a.nseed) v = pre[s + 1 - off];
+    __syncthreads();
+    if (s < a.nseed) pre[s + 1] += v;
+    __syncthreads();
+  }
+  if (s < a.nseed) {
+    const int base = pre[s + 1] - n;
+    for (int k = 0; k < n; k++) {
+      a.items[2 * (base + k)] = s;
+      a.items[2 * (base + k) + 1] = k * a.chunk;
+    }
+  }
+  if (s == 0) {
+    *a.n_items = pre[a.nseed];
+    *a.next_item = 0;
+  }
+}
+
+template <bool kSmem, int kBlock, int kMinBlocks>
+__global__ void __launch_bounds__(kBlock, kMinBlocks) scan_track_kernel(const __grid_constant__ ScanArgs a) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ int item_s;
+  const RefConsts &R = a.ref;
+  const int turn0 = *a.turn0;
+  const int n_items = *a.n_items;
+  int staged = -1;
+  uint32_t phase = 0;
+  for (;;) {
+    if (threadIdx.x == 0) item_s = atomicAdd(a.next_item, 1);
+    __syncthreads();
+    const int item = item_s;
+    __syncthreads();
+    if (item >= n_items) break;
+    const int s = a.items[2 * item];
+    const int first = a.items[2 * item + 1];
+    const ScanSeed sd = a.seeds[s];
+    const ElemHeader *hdr = sd.hdr;
+    const double *pool = sd.pool;
+    if (kSmem) {
+      if (s != staged) {
+        if (!stage_table_ptr(sd.hdr, sd.nelem, sd.pool, sd.npool_padded, smem, &bar, phase, staged < 0)) {
+          if (threadIdx.x == 0) atomicExch(a.status, STB_ETIMEOUT);
+          return;
+        }
+        phase ^= 1u;
+        staged = s;
+      }
+      hdr = reinterpret_cast<const ElemHeader *>(smem);
+      pool = reinterpret_cast<const double *>(smem + (size_t)sd.nelem * sizeof(ElemHeader));
+    }
+    const int live = a.live[s];
+    for (int j = threadIdx.x; j < a.chunk; j += kBlock) {
+      const int slot_in_seed = first + j;
+      if (slot_in_seed >= live) continue;
+      const long i = sd.off + slot_in_seed;
+      if (a.lost_turn[i] >= 0) continue;
+      Particle p[1];
+      PtCache c[1];
+      p[0].x = a.x[i];
+      p[0].px = a.px[i];
+      p[0].y = a.y[i];
+      p[0].py = a.py[i];
+      p[0].z = a.z[i];
+      p[0].pt = a.pt[i];
+      // Track()'s entry quick check, simtrack.cpp:20795-20796
+      if (turn0 == 0 && (fabs(p[0].x) > 0.1 || fabs(p[0].y) > 0.1)) {
+        a.lost_turn[i] = 0;
+        a.lost_elem[i] = 0;
+        continue;
+      }
+      pt_refresh(R, p[0].pt, c[0]);
+      int lt = -1, le = 0;
+      for (int t = 0; t < a.nturn && lt < 0; t++) {
+        for (int e = 0; e < sd.nelem; e++) {
+          const ElemHeader h = hdr[e];
+          apply_element<1>(h, pool + h.poff, p, c, R);
+          if (is_lost(p[0], h.apx, h.apy, a.r2)) {
+            lt = turn0 + t;
+            le = e;
+            break;
+          }
+        }
+      }
+      a.x[i] = p[0].x;
+      a.px[i] = p[0].px;
+      a.y[i] = p[0].y;
+      a.py[i] = p[0].py;
+      a.z[i] = p[0].z;
+      a.pt[i] = p[0].pt;
+      if (lt >= 0) {
+        a.lost_turn[i] = lt;
+        a.lost_elem[i] = le;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+__device__ __forceinline__ void write_output(const ScanArgs &a, long slot, int lt, int le) {
+  const long o = a.id[slot];
+  a.out_lost_turn[o] = lt;
+  a.out_lost_elem[o] = le;
+  double *x = a.out_x + 6 * o;
+  x[0] = a.x[slot];
+  x[1] = a.px[slot];
+  x[2] = a.y[slot];
+  x[3] = a.py[slot];
+  x[4] = a.z[slot];
+  x[5] = a.pt[slot];
+}
+
+// One CTA per seed: stable in-place compaction of [off, off + live).  Each
+// pass reads one CTA-sized window into registers, ranks the live particles
+// with warp ballots and a block prefix sum, synchronises, then writes; a
+// destination never exceeds its source, and all reads of a window precede
+// its writes, so the in-place moves are safe.
+__global__ void __launch_bounds__(kCompactBlock) scan_compact_kernel(ScanArgs a) {
+  constexpr int kWarps = kCompactBlock / 32;
+  __shared__ int warp_off[kWarps];
+  __shared__ int window_total;
+  const int s = blockIdx.x;
+  const ScanSeed sd = a.seeds[s];
+  const int live = a.live[s];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int base = 0;
+  for (int w0 = 0; w0 < live; w0 += kCompactBlock) {
+    const int j = w0 + threadIdx.x;
+    const bool in = j < live;
+    const long src = sd.off + j;
+    int lt = -1, idv = 0;
+    double v[6] = {0, 0, 0, 0, 0, 0};
+    if (in) {
+      lt = a.lost_turn[src];
+      idv = a.id[src];
+      v[0] = a.x[src]; v[1] = a.px[src]; v[2] = a.y[src];
+      v[3] = a.py[src]; v[4] = a.z[src]; v[5] = a.pt[src];
+      if (lt >= 0) write_output(a, src, lt, a.lost_elem[src]);
+    }
+    const bool keep = in && lt < 0;
+    const unsigned m = __ballot_sync(0xffffffffu, keep);
+    if (lane == 0) warp_off[warp] = __popc(m);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int acc = 0;
+      for (int w = 0; w < kWarps; w++) {
+        const int c = warp_off[w];
+        warp_off[w] = acc;
+        acc += c;
+      }
+      window_total = acc;
+    }
+    __syncthreads();
+    if (keep) {
+      const long dst = sd.off + base + warp_off[warp] + __popc(m & ((1u << lane) - 1u));
+      a.x[dst] = v[0]; a.px[dst] = v[1]; a.y[dst] = v[2];
+      a.py[dst] = v[3]; a.z[dst] = v[4]; a.pt[dst] = v[5];
+      a.id[dst] = idv;
+      a.lost_turn[dst] = -1;
+      a.lost_elem[dst] = 0;
+    }
+    base += window_total;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    a.live[s] = base;
+    if (s == 0) *a.turn0 += a.nturn;
+  }
+}
+
+// Particles still alive at the end of the run: outputs with lost_turn = -1.
+__global__ void scan_finalize_kernel(ScanArgs a) {
+  const int s = blockIdx.y;
+  const ScanSeed sd = a.seeds[s];
+  const int live = a.live[s];
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < live; j += gridDim.x * blockDim.x)
+    write_output(a, sd.off + j, -1, 0);
+}
+
+template <bool kSmem, int kBlock, int kMinBlocks>
+cudaError_t prepare_scan_variant(int num_sms, size_t smem, int *grid) {
+  auto kern = scan_track_kernel<kSmem, kBlock, kMinBlocks>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  int per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBlock, smem);
+  if (e != cudaSuccess) return e;
+  if (per_sm < 1) return cudaErrorInvalidConfiguration;
+  *grid = num_sms * per_sm;
+  return cudaSuccess;
+}
+
+}  // namespace
+
+const ScanVariant kScanVariants[kNumScanVariants] = {
+    {true, 1024, 1, "smem_b1024_r64"}, {true, 512, 1, "smem_b512_r128"}, {false, 256, 4, "l1_b256_r64"},
+    {false, 256, 3, "l1_b256_r80"},    {false, 128, 8, "l1_b128_r64"},
+};
+
+cudaError_t prepare_scan(int variant, int num_sms, size_t smem, int *grid) {
+  switch (variant) {
+    case 0: return prepare_scan_variant<true, 1024, 1>(num_sms, smem, grid);
+    case 1: return prepare_scan_variant<true, 512, 1>(num_sms, smem, grid);
+    case 2: return prepare_scan_variant<false, 256, 4>(num_sms, 0, grid);
+    case 3: return prepare_scan_variant<false, 256, 3>(num_sms, 0, grid);
+    case 4: return prepare_scan_variant<false, 128, 8>(num_sms, 0, grid);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+// Only kernel launches: safe inside stream capture (prepare_scan ran before).
+cudaError_t launch_scan_block(const ScanArgs &a, int variant, int grid, size_t smem, cudaStream_t st) {
+  scan_worklist_kernel<<<1, 1024, 0, st>>>(a);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  switch (variant) {
+    case 0: scan_track_kernel<true, 1024, 1><<<grid, 1024, smem, st>>>(a); break;
+    case 1: scan_track_kernel<true, 512, 1><<<grid, 512, smem, st>>>(a); break;
+    case 2: scan_track_kernel<false, 256, 4><<<grid, 256, 0, st>>>(a); break;
+    case 3: scan_track_kernel<false, 256, 3><<<grid, 256, 0, st>>>(a); break;
+    case 4: scan_track_kernel<false, 128, 8><<<grid, 128, 0, st>>>(a); break;
+    default: return cudaErrorInvalidValue;
+  }
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  scan_compact_kernel<<<a.nseed, kCompactBlock, 0, st>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_scan_finalize(const ScanArgs &a, long max_per_seed, cudaStream_t st) {
+  dim3 grid((unsigned)std::max<long>(1, std::min<long>((max_per_seed + 255) / 256, 64)), (unsigned)a.nseed);
+  scan_finalize_kernel<<<grid, 256, 0, st>>>(a);
+  return cudaGetLastError();
+}
+
+}  // namespace stb

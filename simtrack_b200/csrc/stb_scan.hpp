@@ -1,0 +1,60 @@
+// Batched dynamic-aperture scan: device argument block and launch interface.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "stb_table.hpp"
+
+namespace stb {
+
+constexpr int kMaxScanSeeds = 1024;
+
+// One seed: its element table and its particle range in the flat arrays.
+struct ScanSeed {
+  const ElemHeader *hdr;
+  const double *pool;
+  int nelem;
+  int npool_padded;
+  long off;  // first slot of this seed
+  int cap;   // particles of this seed
+  int pad;
+};
+
+struct ScanArgs {
+  const ScanSeed *seeds;
+  int nseed;
+  int chunk;  // particles per work item
+  RefConsts ref;
+  double *x, *px, *y, *py, *z, *pt;  // flat slot arrays
+  int32_t *id;                       // original particle index of each slot
+  int32_t *lost_turn, *lost_elem;    // per slot (-1: alive)
+  int32_t *live;                     // per seed: live particles occupy slots [off, off+live)
+  int32_t *items;                    // work list: (seed, first slot) pairs
+  int32_t *n_items, *next_item;
+  int32_t *turn0;                    // device turn counter
+  int nturn;                         // turns per block
+  double r2;
+  int *status;
+  int32_t *out_lost_turn, *out_lost_elem;  // by original index
+  double *out_x;                           // AoS by original index
+};
+
+struct ScanVariant {
+  bool smem;
+  int block;
+  int min_blocks;
+  const char *name;
+};
+constexpr int kNumScanVariants = 5;
+extern const ScanVariant kScanVariants[kNumScanVariants];
+
+// Sets the kernel attributes of a variant and returns its persistent grid size
+// (call outside stream capture).
+cudaError_t prepare_scan(int variant, int num_sms, size_t smem, int *grid);
+// Work list + tracking + compaction of one turn block (stream-ordered, capturable).
+cudaError_t launch_scan_block(const ScanArgs &a, int variant, int grid, size_t smem, cudaStream_t st);
+// Outputs for the particles still alive.
+cudaError_t launch_scan_finalize(const ScanArgs &a, long max_per_seed, cudaStream_t st);
+
+}  // namespace stb

@@ -1,0 +1,338 @@
+// Host side of the batched dynamic-aperture scan (C ABI stb_scan_*).
+//
+// The scan owns the flat particle state of all seeds on one device and
+// drives turn blocks of (work list, tracking, compaction).  Turn blocks are
+// captured into a CUDA graph once and replayed; the device turn counter makes
+// every replay identical.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "simtrack_b200.h"
+#include "stb_runtime.hpp"
+#include "stb_scan.hpp"
+
+struct stb_scan {
+  int device = 0;
+  int num_sms = 0;
+  int nseed = 0;
+  long ntot = 0;
+  long max_per_seed = 0;
+  std::vector<long> n_per_seed;
+  bool smem_ok = false;
+  size_t smem = 0;
+  int variant = 2;
+  int grid = 0;  // persistent grid of the current variant
+  int chunk = 1024;
+  stb::ScanArgs args{};
+  // device buffers
+  stb::ScanSeed *d_seeds = nullptr;
+  double *d_coords = nullptr;
+  int32_t *d_i32 = nullptr;  // id, lost_turn, lost_elem, out_lost_turn, out_lost_elem
+  int32_t *d_live = nullptr, *d_items = nullptr, *d_ctr = nullptr;
+  double *d_out_x = nullptr;
+  int *d_status = nullptr;
+  long max_items = 0;
+  cudaStream_t stream = nullptr;
+  cudaGraphExec_t graph = nullptr;
+  int graph_blocks = 0, graph_tpb = 0, graph_variant = -1, graph_chunk = -1;
+  int turns_done = 0;
+  double device_ms = 0.0;
+  long blocks_run = 0;
+};
+
+namespace stb {
+namespace {
+
+void scan_destroy(stb_scan *s) {
+  if (!s) return;
+  int prev = -1;
+  cudaGetDevice(&prev);
+  cudaSetDevice(s->device);
+  if (s->graph) cudaGraphExecDestroy(s->graph);
+  if (s->stream) cudaStreamDestroy(s->stream);
+  for (void *p : {(void *)s->d_seeds, (void *)s->d_coords, (void *)s->d_i32, (void *)s->d_live, (void *)s->d_items,
+                  (void *)s->d_ctr, (void *)s->d_out_x, (void *)s->d_status})
+    if (p) cudaFree(p);
+  if (prev >= 0) cudaSetDevice(prev);
+  delete s;
+}
+
+void set_chunk(stb_scan *s, int chunk) {
+  s->chunk = chunk;
+  long items = 0;
+  for (long n : s->n_per_seed) items += (n + chunk - 1) / chunk;
+  if (items > s->max_items) throw Error(STB_EINVAL, "work list capacity exceeded (chunk too small)");
+  s->args.chunk = chunk;
+}
+
+stb_scan *scan_build(stb_table **tables, int nseed, const double *x0, const long *n_per_seed, double radius,
+                     int device) {
+  if (!tables || !x0 || !n_per_seed) throw Error(STB_EINVAL, "NULL argument");
+  if (nseed < 1 || nseed > kMaxScanSeeds) throw Error(STB_EINVAL, "seed count out of range");
+  std::unique_ptr<stb_scan, void (*)(stb_scan *)> s(new stb_scan(), scan_destroy);
+  s->device = device;
+  s->nseed = nseed;
+  DeviceGuard g(device);
+  cuda_check(cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, device), "SM count");
+  std::vector<ScanSeed> seeds(nseed);
+  long off = 0;
+  s->smem_ok = true;
+  for (int i = 0; i < nseed; i++) {
+    stb_table *t = tables[i];
+    if (!t) throw Error(STB_EINVAL, "NULL table");
+    if (t->device != device) throw Error(STB_EINVAL, "all tables must live on the scan's device");
+    if (std::memcmp(&t->host.ref, &tables[0]->host.ref, sizeof(RefConsts)) != 0)
+      throw Error(STB_EINVAL, "all tables must be flattened for the same reference particle");
+    if (n_per_seed[i] < 0 || n_per_seed[i] > (1L << 30)) throw Error(STB_EINVAL, "bad particle count");
+    seeds[i] = ScanSeed{t->d_hdr, t->d_pool, (int)t->host.hdr.size(), t->npool_padded, off, (int)n_per_seed[i], 0};
+    s->n_per_seed.push_back(n_per_seed[i]);
+    off += n_per_seed[i];
+    s->max_per_seed = std::max(s->max_per_seed, n_per_seed[i]);
+    s->smem = std::max(s->smem, track_smem_bytes((int)t->host.hdr.size(), t->npool_padded));
+    s->smem_ok = s->smem_ok && t->use_smem;
+  }
+  s->ntot = off;
+  if (s->ntot == 0) throw Error(STB_EINVAL, "no particles");
+  if (s->ntot > (1L << 31) - 1) throw Error(STB_EINVAL, "too many particles for 32-bit ids");
+  const long n = s->ntot;
+  s->max_items = 0;
+  for (long v : s->n_per_seed) s->max_items += (v + 63) / 64;  // smallest chunk supported: 64
+  cuda_check(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "stream");
+  cuda_check(cudaMalloc(&s->d_seeds, sizeof(ScanSeed) * nseed), "cudaMalloc(seeds)");
+  cuda_check(cudaMalloc(&s->d_coords, sizeof(double) * 6 * n), "cudaMalloc(coordinates)");
+  cuda_check(cudaMalloc(&s->d_i32, sizeof(int32_t) * 5 * n), "cudaMalloc(particle state)");
+  cuda_check(cudaMalloc(&s->d_live, sizeof(int32_t) * nseed), "cudaMalloc(live)");
+  cuda_check(cudaMalloc(&s->d_items, sizeof(int32_t) * 2 * std::max<long>(1, s->max_items)), "cudaMalloc(items)");
+  cuda_check(cudaMalloc(&s->d_ctr, sizeof(int32_t) * 4), "cudaMalloc(counters)");
+  cuda_check(cudaMalloc(&s->d_out_x, sizeof(double) * 6 * n), "cudaMalloc(outputs)");
+  cuda_check(cudaMalloc(&s->d_status, sizeof(int)), "cudaMalloc(status)");
+  // initial state: AoS host -> SoA device; id = original index; all alive
+  std::vector<double> soa((size_t)6 * n);
+  for (long i = 0; i < n; i++)
+    for (int k = 0; k < 6; k++) soa[(size_t)k * n + i] = x0[6 * i + k];
+  std::vector<int32_t> i32((size_t)5 * n);
+  for (long i = 0; i < n; i++) {
+    i32[i] = (int32_t)i;
+    i32[n + i] = -1;
+    i32[2 * n + i] = 0;
+    i32[3 * n + i] = -1;
+    i32[4 * n + i] = 0;
+  }
+  std::vector<int32_t> live(nseed);
+  for (int i = 0; i < nseed; i++) live[i] = (int32_t)s->n_per_seed[i];
+  cuda_check(cudaMemcpy(s->d_seeds, seeds.data(), sizeof(ScanSeed) * nseed, cudaMemcpyHostToDevice), "upload");
+  cuda_check(cudaMemcpy(s->d_coords, soa.data(), sizeof(double) * 6 * n, cudaMemcpyHostToDevice), "upload");
+  cuda_check(cudaMemcpy(s->d_i32, i32.data(), sizeof(int32_t) * 5 * n, cudaMemcpyHostToDevice), "upload");
+  cuda_check(cudaMemcpy(s->d_live, live.data(), sizeof(int32_t) * nseed, cudaMemcpyHostToDevice), "upload");
+  cuda_check(cudaMemset(s->d_ctr, 0, sizeof(int32_t) * 4), "reset counters");
+  cuda_check(cudaMemset(s->d_status, 0, sizeof(int)), "reset status");
+  cuda_check(cudaMemcpy(s->d_out_x, x0, sizeof(double) * 6 * n, cudaMemcpyHostToDevice), "upload");
+  ScanArgs &a = s->args;
+  a.seeds = s->d_seeds;
+  a.nseed = nseed;
+  a.ref = tables[0]->host.ref;
+  a.x = s->d_coords;
+  a.px = a.x + n;
+  a.y = a.x + 2 * n;
+  a.py = a.x + 3 * n;
+  a.z = a.x + 4 * n;
+  a.pt = a.x + 5 * n;
+  a.id = s->d_i32;
+  a.lost_turn = s->d_i32 + n;
+  a.lost_elem = s->d_i32 + 2 * n;
+  a.out_lost_turn = s->d_i32 + 3 * n;
+  a.out_lost_elem = s->d_i32 + 4 * n;
+  a.out_x = s->d_out_x;
+  a.live = s->d_live;
+  a.items = s->d_items;
+  a.n_items = s->d_ctr;
+  a.next_item = s->d_ctr + 1;
+  a.turn0 = s->d_ctr + 2;
+  a.r2 = radius > 0.0 ? radius * radius : 0.0;
+  a.status = s->d_status;
+  s->variant = s->smem_ok ? 0 : 2;
+  cuda_check(prepare_scan(s->variant, s->num_sms, s->smem, &s->grid), "scan kernel setup");
+  set_chunk(s.get(), kScanVariants[s->variant].block);
+  return s.release();
+}
+
+long total_live(stb_scan *s) {
+  std::vector<int32_t> live(s->nseed);
+  cuda_check(cudaMemcpyAsync(live.data(), s->d_live, sizeof(int32_t) * s->nseed, cudaMemcpyDeviceToHost, s->stream),
+             "read live counts");
+  cuda_check(cudaStreamSynchronize(s->stream), "scan");
+  long t = 0;
+  for (int v : live) t += v;
+  return t;
+}
+
+void check_status(stb_scan *s) {
+  int st = 0;
+  cuda_check(cudaMemcpy(&st, s->d_status, sizeof(int), cudaMemcpyDeviceToHost), "read status");
+  if (st != 0) throw Error(st, "scan kernel reported status " + std::to_string(st));
+}
+
+void run_blocks_direct(stb_scan *s, int nblocks, int tpb) {
+  ScanArgs a = s->args;
+  a.nturn = tpb;
+  for (int b = 0; b < nblocks; b++)
+    cuda_check(launch_scan_block(a, s->variant, s->grid, s->smem, s->stream), "scan block launch");
+}
+
+void ensure_graph(stb_scan *s, int blocks, int tpb) {
+  if (s->graph && s->graph_blocks == blocks && s->graph_tpb == tpb && s->graph_variant == s->variant &&
+      s->graph_chunk == s->chunk)
+    return;
+  if (s->graph) {
+    cudaGraphExecDestroy(s->graph);
+    s->graph = nullptr;
+  }
+  cudaGraph_t graph = nullptr;
+  cuda_check(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+  ScanArgs a = s->args;
+  a.nturn = tpb;
+  cudaError_t le = cudaSuccess;
+  for (int b = 0; b < blocks && le == cudaSuccess; b++) le = launch_scan_block(a, s->variant, s->grid, s->smem, s->stream);
+  cudaError_t ce = cudaStreamEndCapture(s->stream, &graph);
+  cuda_check(le, "scan block capture");
+  cuda_check(ce, "end capture");
+  cudaError_t ie = cudaGraphInstantiate(&s->graph, graph, 0);
+  cudaGraphDestroy(graph);
+  cuda_check(ie, "graph instantiate");
+  s->graph_blocks = blocks;
+  s->graph_tpb = tpb;
+  s->graph_variant = s->variant;
+  s->graph_chunk = s->chunk;
+}
+
+// Advances every live particle by nturn turns (fewer if all are lost).
+void scan_run(stb_scan *s, int nturn, int tpb, int use_graph) {
+  if (nturn < 0 || tpb <= 0) throw Error(STB_EINVAL, "bad turn counts");
+  DeviceGuard g(s->device);
+  cudaEvent_t e0, e1;
+  cuda_check(cudaEventCreate(&e0), "event");
+  cuda_check(cudaEventCreate(&e1), "event");
+  const int nblocks = nturn / tpb, rem = nturn % tpb;
+  const int per_graph = std::max(1, std::min(nblocks, 16));
+  int done_blocks = 0;
+  float ms_total = 0.f;
+  auto timed = [&](auto &&fn) {
+    cuda_check(cudaEventRecord(e0, s->stream), "event");
+    fn();
+    cuda_check(cudaEventRecord(e1, s->stream), "event");
+    cuda_check(cudaEventSynchronize(e1), "scan");
+    float ms = 0.f;
+    cuda_check(cudaEventElapsedTime(&ms, e0, e1), "event time");
+    ms_total += ms;
+  };
+  while (done_blocks < nblocks) {
+    const int todo = std::min(per_graph, nblocks - done_blocks);
+    if (use_graph && todo == per_graph) {
+      ensure_graph(s, per_graph, tpb);
+      timed([&] { cuda_check(cudaGraphLaunch(s->graph, s->stream), "graph launch"); });
+    } else {
+      timed([&] { run_blocks_direct(s, todo, tpb); });
+    }
+    done_blocks += todo;
+    s->blocks_run += todo;
+    s->turns_done += todo * tpb;
+    check_status(s);
+    if (total_live(s) == 0) break;
+  }
+  if (rem > 0 && total_live(s) > 0) {
+    timed([&] { run_blocks_direct(s, 1, rem); });
+    s->blocks_run += 1;
+    s->turns_done += rem;
+    check_status(s);
+  }
+  cuda_check(launch_scan_finalize(s->args, s->max_per_seed, s->stream), "finalize");
+  cuda_check(cudaStreamSynchronize(s->stream), "finalize");
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  s->device_ms += ms_total;
+}
+
+}  // namespace
+}  // namespace stb
+
+using namespace stb;
+
+extern "C" {
+
+int stb_scan_create(stb_table **tables, int nseed, const double *x0, const long *n_per_seed, double aperture_radius,
+                    int device, stb_scan **out) {
+  return guarded([&] {
+    if (!out) throw Error(STB_EINVAL, "NULL output");
+    *out = scan_build(tables, nseed, x0, n_per_seed, aperture_radius, device);
+    return STB_OK;
+  });
+}
+
+int stb_scan_free(stb_scan *s) {
+  return guarded([&] {
+    scan_destroy(s);
+    return STB_OK;
+  });
+}
+
+int stb_scan_configure(stb_scan *s, int variant, int chunk) {
+  return guarded([&] {
+    if (!s) throw Error(STB_EINVAL, "NULL scan");
+    if (variant >= 0) {
+      if (variant >= kNumScanVariants) throw Error(STB_EINVAL, "variant out of range");
+      if (kScanVariants[variant].smem && !s->smem_ok) throw Error(STB_EINVAL, "tables do not fit shared memory");
+      DeviceGuard g(s->device);
+      int grid = 0;
+      cuda_check(prepare_scan(variant, s->num_sms, s->smem, &grid), "scan kernel setup");
+      s->variant = variant;
+      s->grid = grid;
+    }
+    if (chunk > 0) {
+      if (chunk < 64 || chunk % 32) throw Error(STB_EINVAL, "chunk must be a multiple of 32, >= 64");
+      set_chunk(s, chunk);
+    }
+    return STB_OK;
+  });
+}
+
+int stb_scan_run(stb_scan *s, int nturn, int turns_per_block, int use_graph) {
+  return guarded([&] {
+    if (!s) throw Error(STB_EINVAL, "NULL scan");
+    scan_run(s, nturn, turns_per_block, use_graph);
+    return STB_OK;
+  });
+}
+
+int stb_scan_results(stb_scan *s, int32_t *lost_turn, int32_t *lost_elem, double *x_aos) {
+  return guarded([&] {
+    if (!s) throw Error(STB_EINVAL, "NULL scan");
+    DeviceGuard g(s->device);
+    const long n = s->ntot;
+    if (lost_turn)
+      cuda_check(cudaMemcpy(lost_turn, s->args.out_lost_turn, sizeof(int32_t) * n, cudaMemcpyDeviceToHost), "download");
+    if (lost_elem)
+      cuda_check(cudaMemcpy(lost_elem, s->args.out_lost_elem, sizeof(int32_t) * n, cudaMemcpyDeviceToHost), "download");
+    if (x_aos) cuda_check(cudaMemcpy(x_aos, s->d_out_x, sizeof(double) * 6 * n, cudaMemcpyDeviceToHost), "download");
+    return STB_OK;
+  });
+}
+
+int stb_scan_stats(const stb_scan *s, double *st) {
+  return guarded([&] {
+    if (!s || !st) throw Error(STB_EINVAL, "NULL argument");
+    st[0] = (double)s->turns_done;
+    st[1] = s->device_ms;
+    st[2] = (double)s->blocks_run;
+    st[3] = (double)s->variant;
+    st[4] = (double)s->chunk;
+    st[5] = (double)s->ntot;
+    return STB_OK;
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,427 @@
+// Device code of the element-by-element tracking kernels, shared by the
+// single-lattice tracker (stb_track.cu) and the batched scan (stb_scan.cu).
+// Included by exactly those two translation units; everything here has
+// internal linkage.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "stb_kernels.hpp"
+#include "stb_physics.cuh"
+
+namespace stb {
+namespace {
+
+constexpr double kPI = 3.14159265358979323;
+constexpr double kC = 2.99792458e8;
+
+// Bulk copy of `bytes` (multiple of 16, both addresses 16-byte aligned) from
+// global to shared memory, completing on `bar`.
+__device__ __forceinline__ void bulk_g2s(void *smem_dst, const void *gsrc, uint32_t bytes, uint64_t *bar) {
+  const uint32_t d = (uint32_t)__cvta_generic_to_shared(smem_dst);
+  const uint32_t b = (uint32_t)__cvta_generic_to_shared(bar);
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(d),
+               "l"(gsrc), "r"(bytes), "r"(b)
+               : "memory");
+}
+
+// Stage an element table (headers then pool) into shared memory with bulk
+// copies completing on `bar`.  `phase` is the barrier phase this staging
+// completes (0 for the first use of a freshly initialised barrier, then
+// alternating).  Returns false if the bounded wait ran out (the caller then
+// records STB_ETIMEOUT and returns).  Must be called by all threads of the CTA.
+__device__ bool stage_table_ptr(const ElemHeader *ghdr, int nelem, const double *gpool, int npool_padded,
+                                unsigned char *smem, uint64_t *bar, uint32_t phase, bool init) {
+  const uint32_t hbytes = (uint32_t)nelem * (uint32_t)sizeof(ElemHeader);
+  const uint32_t pbytes = (uint32_t)npool_padded * 8u;
+  const uint32_t total = hbytes + pbytes;
+  const uint32_t b = (uint32_t)__cvta_generic_to_shared(bar);
+  if (init && threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(b) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    // Order earlier generic-proxy accesses of the buffer before the async copies.
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(b), "r"(total) : "memory");
+    constexpr uint32_t kChunk = 32768;
+    for (uint32_t off = 0; off < hbytes; off += kChunk) {
+      const uint32_t n = (hbytes - off) < kChunk ? (hbytes - off) : kChunk;
+      bulk_g2s(smem + off, (const unsigned char *)ghdr + off, n, bar);
+    }
+    for (uint32_t off = 0; off < pbytes; off += kChunk) {
+      const uint32_t n = (pbytes - off) < kChunk ? (pbytes - off) : kChunk;
+      bulk_g2s(smem + hbytes + off, (const unsigned char *)gpool + off, n, bar);
+    }
+  }
+  // Bounded wait on the barrier phase; the CTA agrees on the outcome.
+  uint32_t done = 0;
+  for (int iter = 0; iter < (1 << 22); iter++) {
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(b), "r"(phase & 1u)
+        : "memory");
+    if (done) break;
+  }
+  return __syncthreads_and((int)done) != 0;
+}
+
+__device__ bool stage_table(const TrackArgs &a, unsigned char *smem, uint64_t *bar) {
+  return stage_table_ptr(a.hdr, a.nelem, a.pool, a.npool_padded, smem, bar, 0, true);
+}
+
+__device__ __forceinline__ bool is_lost(const Particle &p, double apx, double apy, double r2) {
+  return fabs(p.x) > apx || fabs(p.y) > apy || isnan(p.x) || isnan(p.y) || (r2 > 0.0 && p.x * p.x + p.y * p.y > r2);
+}
+
+// Rarely executed element maps are kept out of line so the hot loop (drift,
+// bend, quadrupole and thin kicks) stays small in the instruction cache and
+// in registers.  They take the particle by reference (spilled around the
+// call, a few times per turn).
+
+__device__ __noinline__ void op_gsbend(const ElemHeader &h, const double *P, Particle &p, const PtCache &c) {
+  if (h.flags & EF_EDGE1) {
+    p.px = p.px + P[0] * p.x;
+    p.py = p.py - P[0] * p.y;
+  }
+  gbend_exact(p, c, P + 2);
+  if (h.flags & EF_EDGE2) {
+    p.px = p.px + P[1] * p.x;
+    p.py = p.py - P[1] * p.y;
+  }
+}
+
+template <int kOrder>
+__device__ __noinline__ void op_thick_sext_oct(const ElemHeader &h, const double *P, Particle &p, const PtCache &c) {
+  const double d1 = P[0], d1b = P[1], d2 = P[2], d2b = P[3];
+  const double a1 = P[4], s1 = P[5], a2 = P[6], s2 = P[7];
+#pragma unroll 1
+  for (int s = 0; s < h.nint; s++) {
+    drift(p, c, d1, d1b);
+    if (kOrder == 2) sext_kick(p, a1, s1); else oct_kick(p, a1, s1);
+    drift(p, c, d2, d2b);
+    if (kOrder == 2) sext_kick(p, a2, s2); else oct_kick(p, a2, s2);
+    drift(p, c, d2, d2b);
+    if (kOrder == 2) sext_kick(p, a1, s1); else oct_kick(p, a1, s1);
+    drift(p, c, d1, d1b);
+  }
+}
+
+__device__ __noinline__ void op_mult_thick(const ElemHeader &h, const double *P, Particle &p, const PtCache &c) {
+  const volatile double *V = P;
+  const int no = h.aux;
+  const double *K1 = P + 4;
+  const double *K2 = K1 + 2 + 3 * no;
+#pragma unroll 1
+  for (int s = 0; s < h.nint; s++) {
+    drift(p, c, V[0], V[1]);
+    mult_kick(p, no, K1);
+    drift(p, c, V[2], V[3]);
+    mult_kick(p, no, K2);
+    drift(p, c, V[2], V[3]);
+    mult_kick(p, no, K1);
+    drift(p, c, V[0], V[1]);
+  }
+}
+
+__device__ __noinline__ void op_bendmult(const ElemHeader &h, const double *P, Particle &p, const PtCache &c) {
+  const int no = h.aux;
+  const double *B1 = P + 2, *B2 = P + 8;
+  const double *K1 = P + 14;
+  const double *K2 = K1 + 2 + 3 * no;
+  p.px = p.px + P[0] * p.x;
+  p.py = p.py - P[0] * p.y;
+#pragma unroll 1
+  for (int s = 0; s < h.nint; s++) {
+    bend_exact(p, c, B1);
+    mult_kick(p, no, K1);
+    bend_exact(p, c, B2);
+    mult_kick(p, no, K2);
+    bend_exact(p, c, B2);
+    mult_kick(p, no, K1);
+    bend_exact(p, c, B1);
+  }
+  p.px = p.px + P[1] * p.x;
+  p.py = p.py - P[1] * p.y;
+}
+
+__device__ __noinline__ void op_misc(const ElemHeader &h, const double *P, Particle &p, PtCache &c,
+                                     const RefConsts &R) {
+  switch (h.op) {
+    case OP_OCT_KICK:
+      oct_kick(p, P[0], P[1]);
+      break;
+    case OP_MULT_KICK:
+      mult_kick(p, h.aux, P);
+      break;
+    case OP_KICK:
+      drift(p, c, P[0], P[1]);
+      p.px = p.px + P[2];
+      p.py = p.py + P[3];
+      drift(p, c, P[0], P[1]);
+      break;
+    case OP_RFCAV: {
+      // RFCAV_Pass, simtrack.cpp:6008-6010
+      drift(p, c, P[0], P[1]);
+      const double absvq = P[2], kf = P[3], phase0 = P[4];
+      p.pt = p.pt + absvq * cr_sin(kf * p.z / kC + kPI - phase0) / R.beta / R.energy;
+      pt_refresh(R, p.pt, c);
+      drift(p, c, P[0], P[1]);
+      break;
+    }
+    case OP_CRABRF: {
+      // CRABRF_Pass, simtrack.cpp:6020-6023
+      drift(p, c, P[0], P[1]);
+      const double vq = P[2], kf = P[3], phase0 = P[4], kk = P[5];
+      const double arg = kf * p.z / kC + phase0;
+      p.px = p.px - vq * cr_sin(arg) / R.beta / R.energy;
+      p.pt = p.pt - vq * cr_cos(arg) * p.x * kk / R.beta / R.energy;
+      pt_refresh(R, p.pt, c);
+      drift(p, c, P[0], P[1]);
+      break;
+    }
+    case OP_CCMULT:
+      drift(p, c, P[0], P[1]);
+      ccmult_kick(p, P + 2);
+      pt_refresh(R, p.pt, c);
+      drift(p, c, P[0], P[1]);
+      break;
+    case OP_LBT:
+      lbt(p, P);
+      pt_refresh(R, p.pt, c);
+      break;
+    case OP_ILBT:
+      ilbt(p, P);
+      pt_refresh(R, p.pt, c);
+      break;
+    case OP_BB6D:
+      bb6d(p, P, h.nint);
+      pt_refresh(R, p.pt, c);
+      break;
+    case OP_BB4D: {
+      double Dpx, Dpy;
+      bb4d(p.x, p.y, P[0], P[1], P[2], Dpx, Dpy);
+      p.px = p.px + Dpx * P[3];
+      p.py = p.py + Dpy * P[3];
+      break;
+    }
+    default:  // OP_IDENTITY
+      break;
+  }
+}
+
+// Uniform signature wrappers for the out-of-line maps.
+__device__ __noinline__ void op_gsbend_w(const ElemHeader &h, const double *P, Particle &p, PtCache &c,
+                                         const RefConsts &) { op_gsbend(h, P, p, c); }
+__device__ __noinline__ void op_sext_w(const ElemHeader &h, const double *P, Particle &p, PtCache &c,
+                                       const RefConsts &) { op_thick_sext_oct<2>(h, P, p, c); }
+__device__ __noinline__ void op_oct_w(const ElemHeader &h, const double *P, Particle &p, PtCache &c,
+                                      const RefConsts &) { op_thick_sext_oct<3>(h, P, p, c); }
+__device__ __noinline__ void op_mult_w(const ElemHeader &h, const double *P, Particle &p, PtCache &c,
+                                       const RefConsts &) { op_mult_thick(h, P, p, c); }
+__device__ __noinline__ void op_bendmult_w(const ElemHeader &h, const double *P, Particle &p, PtCache &c,
+                                           const RefConsts &) { op_bendmult(h, P, p, c); }
+
+// Calls an out-of-line map on copies of the particle state, so the address
+// of the register-resident state never escapes (taking it would pin the hot
+// loop's particle in the stack frame).
+template <class F>
+__device__ __forceinline__ void call_out_of_line(const ElemHeader &h, const double *P, Particle &p, PtCache &c,
+                                                 const RefConsts &R, F f) {
+  Particle q = p;
+  PtCache cc = c;
+  f(h, P, q, cc, R);
+  p = q;
+  c = cc;
+}
+
+// Runs one element on the kPPT particles of this thread; the caller checks
+// loss.  For the hot element types the per-particle maps are issued back to
+// back, so their independent FP64 dependency chains interleave in the
+// instruction stream (latency hiding without more resident warps).
+template <int kPPT>
+__device__ __forceinline__ void apply_element(const ElemHeader &h, const double *P, Particle (&p)[kPPT],
+                                              PtCache (&c)[kPPT], const RefConsts &R) {
+  const double *M = P;
+  const bool mis = (h.flags & (EF_MISALIGN_OFFSET | EF_MISALIGN_ROLL)) != 0;
+  if (mis) {
+#pragma unroll
+    for (int k = 0; k < kPPT; k++) gtol1(p[k], M, h.flags);
+    P += kMisalignParams;
+  }
+  switch (h.op) {
+    case OP_DRIFT: {
+      const double L = P[0], Lb = P[1];
+#pragma unroll
+      for (int k = 0; k < kPPT; k++) drift(p[k], c[k], L, Lb);
+      break;
+    }
+    case OP_SBEND:
+#pragma unroll
+      for (int k = 0; k < kPPT; k++) {
+        if (h.flags & EF_EDGE1) {
+          p[k].px = p[k].px + P[0] * p[k].x;
+          p[k].py = p[k].py - P[0] * p[k].y;
+        }
+        bend_exact(p[k], c[k], P + 2);
+        if (h.flags & EF_EDGE2) {
+          p[k].px = p[k].px + P[1] * p[k].x;
+          p[k].py = p[k].py - P[1] * p[k].y;
+        }
+      }
+      break;
+    case OP_QUAD_THICK: {
+      // Slice constants are re-read from the table at each use (volatile view)
+      // instead of being hoisted into eight live register pairs.
+      const volatile double *V = P;
+      if (h.flags & EF_FRINGE)
+        for (int k = 0; k < kPPT; k++) quad_fringe(p[k], P[8], true);
+#pragma unroll 1
+      for (int s = 0; s < h.nint; s++) {
+#pragma unroll
+        for (int k = 0; k < kPPT; k++) drift(p[k], c[k], V[0], V[1]);
+#pragma unroll
+        for (int k = 0; k < kPPT; k++) quad_kick(p[k], V[4], V[5]);
+#pragma unroll
+        for (int k = 0; k < kPPT; k++) drift(p[k], c[k], V[2], V[3]);
+#pragma unroll
+        for (int k = 0; k < kPPT; k++) quad_kick(p[k], V[6], V[7]);
+#pragma unroll
+        for (int k = 0; k < kPPT; k++) drift(p[k], c[k], V[2], V[3]);
+#pragma unroll
+        for (int k = 0; k < kPPT; k++) quad_kick(p[k], V[4], V[5]);
+#pragma unroll
+        for (int k = 0; k < kPPT; k++) drift(p[k], c[k], V[0], V[1]);
+      }
+      if (h.flags & EF_FRINGE)
+        for (int k = 0; k < kPPT; k++) quad_fringe(p[k], P[8], false);
+      break;
+    }
+    case OP_QUAD_KICK:
+#pragma unroll
+      for (int k = 0; k < kPPT; k++) quad_kick(p[k], P[0], P[1]);
+      break;
+    case OP_SEXT_KICK:
+#pragma unroll
+      for (int k = 0; k < kPPT; k++) sext_kick(p[k], P[0], P[1]);
+      break;
+    case OP_GSBEND:
+      for (int k = 0; k < kPPT; k++) call_out_of_line(h, P, p[k], c[k], R, op_gsbend_w);
+      break;
+    case OP_SEXT_THICK:
+      for (int k = 0; k < kPPT; k++) call_out_of_line(h, P, p[k], c[k], R, op_sext_w);
+      break;
+    case OP_OCT_THICK:
+      for (int k = 0; k < kPPT; k++) call_out_of_line(h, P, p[k], c[k], R, op_oct_w);
+      break;
+    case OP_MULT_THICK:
+      for (int k = 0; k < kPPT; k++) call_out_of_line(h, P, p[k], c[k], R, op_mult_w);
+      break;
+    case OP_BENDMULT:
+      for (int k = 0; k < kPPT; k++) call_out_of_line(h, P, p[k], c[k], R, op_bendmult_w);
+      break;
+    default:
+      for (int k = 0; k < kPPT; k++) call_out_of_line(h, P, p[k], c[k], R, op_misc);
+      break;
+  }
+  if (mis) {
+#pragma unroll
+    for (int k = 0; k < kPPT; k++) ltog1(p[k], M, h.flags);
+  }
+}
+
+__device__ __forceinline__ void store_particle(const TrackArgs &a, long i, const Particle &p) {
+  a.x[i] = p.x;
+  a.px[i] = p.px;
+  a.y[i] = p.y;
+  a.py[i] = p.py;
+  a.z[i] = p.z;
+  a.pt[i] = p.pt;
+}
+
+// kPPT particles per thread: particle base + k*kBlock for k < kPPT, so every
+// load and store of a warp stays coalesced.  A particle that is lost has its
+// coordinates and loss record stored at once; its slot is then reset to the
+// reference orbit so the remaining particles of the thread keep running on
+// benign operands.
+template <bool kSmem, int kBlock, int kMinBlocks, int kPPT, bool kDump>
+__global__ void __launch_bounds__(kBlock, kMinBlocks) track_kernel(const __grid_constant__ TrackArgs a) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ __align__(8) uint64_t bar;
+  const ElemHeader *hdr = a.hdr;
+  const double *pool = a.pool;
+  if (kSmem) {
+    if (!stage_table(a, smem, &bar)) {
+      if (threadIdx.x == 0) atomicExch(a.status, STB_ETIMEOUT);
+      return;
+    }
+    hdr = reinterpret_cast<const ElemHeader *>(smem);
+    pool = reinterpret_cast<const double *>(smem + (size_t)a.nelem * sizeof(ElemHeader));
+  }
+  const RefConsts &R = a.ref;
+  const long chunk = (long)kBlock * kPPT;
+  const long stride = (long)gridDim.x * chunk;
+  for (long base = (long)blockIdx.x * chunk + threadIdx.x; base < a.n; base += stride) {
+    Particle p[kPPT];
+    PtCache c[kPPT];
+    bool alive[kPPT];
+    int nalive = 0;
+#pragma unroll
+    for (int k = 0; k < kPPT; k++) {
+      const long i = base + (long)k * kBlock;
+      alive[k] = i < a.n && a.lost_turn[i] < 0;
+      p[k] = Particle{0., 0., 0., 0., 0., 0.};
+      if (alive[k]) {
+        p[k].x = a.x[i];
+        p[k].px = a.px[i];
+        p[k].y = a.y[i];
+        p[k].py = a.py[i];
+        p[k].z = a.z[i];
+        p[k].pt = a.pt[i];
+        // Track()'s entry quick check, simtrack.cpp:20795-20796
+        if (a.turn0 == 0 && (fabs(p[k].x) > 0.1 || fabs(p[k].y) > 0.1)) {
+          a.lost_turn[i] = 0;
+          a.lost_elem[i] = 0;
+          alive[k] = false;
+          p[k] = Particle{0., 0., 0., 0., 0., 0.};
+        }
+      }
+      pt_refresh(R, p[k].pt, c[k]);
+      nalive += alive[k] ? 1 : 0;
+    }
+    for (int t = 0; t < a.nturn && nalive > 0; t++) {
+      for (int e = 0; e < a.nelem; e++) {
+        const ElemHeader h = hdr[e];
+        apply_element<kPPT>(h, pool + h.poff, p, c, R);
+#pragma unroll
+        for (int k = 0; k < kPPT; k++) {
+          if (!alive[k]) continue;
+          const long i = base + (long)k * kBlock;
+          if (kDump) {
+            double *d = a.dump + (((size_t)i * a.nturn + t) * a.nelem + e) * 6;
+            d[0] = p[k].x; d[1] = p[k].px; d[2] = p[k].y; d[3] = p[k].py; d[4] = p[k].z; d[5] = p[k].pt;
+          }
+          if (is_lost(p[k], h.apx, h.apy, a.r2)) {
+            store_particle(a, i, p[k]);
+            a.lost_turn[i] = a.turn0 + t;
+            a.lost_elem[i] = e;
+            alive[k] = false;
+            nalive--;
+            p[k] = Particle{0., 0., 0., 0., 0., 0.};
+            pt_refresh(R, 0.0, c[k]);
+          }
+        }
+        if (nalive == 0) break;
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < kPPT; k++)
+      if (alive[k]) store_particle(a, base + (long)k * kBlock, p[k]);
+  }
+}
+
+}  // namespace
+}  // namespace stb
