@@ -160,6 +160,11 @@ int stb_scan_run(stb_scan *s, int nturn, int turns_per_block, int use_graph);
  * element index of the loss, and the coordinates (AoS, at the loss or now).
  * Any output pointer may be NULL. */
 int stb_scan_results(stb_scan *s, int32_t *lost_turn, int32_t *lost_elem, double *x_aos);
+/* Autotuner: times one turn block of nturn turns for every launch variant of
+ * the scan's tracking kernel on a snapshot of the current state (restored
+ * after each trial, so the scan does not advance) and keeps the fastest.
+ * timings_ms (optional) receives up to ntimings times (< 0: not runnable). */
+int stb_scan_autotune(stb_scan *s, int nturn, int *chosen, double *timings_ms, int ntimings);
 /* st[0] turns done, [1] device milliseconds, [2] turn blocks, [3] variant, [4] chunk, [5] particles */
 int stb_scan_stats(const stb_scan *s, double *st6);
 

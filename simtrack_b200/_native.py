@@ -74,6 +74,7 @@ SIGNATURES = [
     ("stb_scan_run", c_int, [c_void_p, c_int, c_int, c_int]),
     ("stb_scan_results", c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
     ("stb_scan_stats", c_int, [c_void_p, POINTER(c_double)]),
+    ("stb_scan_autotune", c_int, [c_void_p, c_int, POINTER(c_int), POINTER(c_double), c_int]),
     ("stb_fp64_peak", c_int, [c_int, POINTER(c_double)]),
     ("stb_math_eval", c_int, [c_int, POINTER(c_double), POINTER(c_double), c_long, c_int]),
     ("stb_track_probe", c_int, [c_void_p, POINTER(c_double), c_long, c_int, c_double, POINTER(c_double),

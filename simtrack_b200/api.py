@@ -323,6 +323,13 @@ class Scan:
     def configure(self, variant: int = -1, chunk: int = 0) -> None:
         check(lib().stb_scan_configure(self._h, variant, chunk))
 
+    def autotune(self, nturn: int = 16) -> dict:
+        """Picks the fastest tracking-kernel variant on a snapshot of the current state."""
+        ch = c_int()
+        t = (c_double * 8)()
+        check(lib().stb_scan_autotune(self._h, nturn, byref(ch), t, 8))
+        return {"chosen": ch.value, "ms": [t[i] for i in range(5)]}
+
     def run(self, nturn: int, turns_per_block: int = 256, use_graph: bool = True) -> None:
         check(lib().stb_scan_run(self._h, nturn, turns_per_block, int(use_graph)))
 

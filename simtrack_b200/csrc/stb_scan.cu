@@ -35,14 +35,38 @@ namespace {
 
 constexpr int kCompactBlock = 1024;
 
+// Work-item size adapts to the live population: with few survivors the items
+// shrink (down to one warp) so that they still spread over every resident
+// CTA; with many they grow up to the configured chunk.
 __global__ void scan_worklist_kernel(ScanArgs a) {
   __shared__ int pre[kMaxScanSeeds + 1];
+  __shared__ int chunk_s;
   const int s = threadIdx.x;
-  int n = 0;
-  if (s < a.nseed) n = (a.live[s] + a.chunk - 1) / a.chunk;
-  // Exclusive prefix sum over the (<= 1024) seeds.
-  pre[s + 1] = n;
+  const int lv = s < a.nseed ? a.live[s] : 0;
+  // total live particles (block reduction through the prefix array)
+  pre[s + 1] = lv;
   if (s == 0) pre[0] = 0;
+  __syncthreads();
+  for (int off = 1; off <= a.nseed; off <<= 1) {
+    int v = 0;
+    if (s + 1 > off && s < a.nseed) v = pre[s + 1 - off];
+    __syncthreads();
+    if (s < a.nseed) pre[s + 1] += v;
+    __syncthreads();
+  }
+  if (s == 0) {
+    const long total = pre[a.nseed];
+    long c = (total + a.grid - 1) / (a.grid > 0 ? a.grid : 1);
+    c = ((c + 31) / 32) * 32;
+    if (c < 32) c = 32;
+    if (c > a.chunk) c = a.chunk;
+    chunk_s = (int)c;
+  }
+  __syncthreads();
+  const int chunk = chunk_s;
+  const int n = s < a.nseed ? (lv + chunk - 1) / chunk : 0;
+  __syncthreads();
+  pre[s + 1] = n;
   __syncthreads();
   for (int off = 1; off <= a.nseed; off <<= 1) {
     int v = 0;
@@ -55,12 +79,13 @@ __global__ void scan_worklist_kernel(ScanArgs a) {
     const int base = pre[s + 1] - n;
     for (int k = 0; k < n; k++) {
       a.items[2 * (base + k)] = s;
-      a.items[2 * (base + k) + 1] = k * a.chunk;
+      a.items[2 * (base + k) + 1] = k * chunk;
     }
   }
   if (s == 0) {
     *a.n_items = pre[a.nseed];
     *a.next_item = 0;
+    *a.item_chunk = chunk;
   }
 }
 
@@ -72,6 +97,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) scan_track_kernel(const __
   const RefConsts &R = a.ref;
   const int turn0 = *a.turn0;
   const int n_items = *a.n_items;
+  const int chunk = *a.item_chunk;
   int staged = -1;
   uint32_t phase = 0;
   for (;;) {
@@ -98,7 +124,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) scan_track_kernel(const __
       pool = reinterpret_cast<const double *>(smem + (size_t)sd.nelem * sizeof(ElemHeader));
     }
     const int live = a.live[s];
-    for (int j = threadIdx.x; j < a.chunk; j += kBlock) {
+    for (int j = threadIdx.x; j < chunk; j += kBlock) {
       const int slot_in_seed = first + j;
       if (slot_in_seed >= live) continue;
       const long i = sd.off + slot_in_seed;

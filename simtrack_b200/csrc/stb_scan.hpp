@@ -24,14 +24,15 @@ struct ScanSeed {
 struct ScanArgs {
   const ScanSeed *seeds;
   int nseed;
-  int chunk;  // particles per work item
+  int chunk;  // largest work item (particles); the work list may use smaller ones
+  int grid;   // resident CTAs of the tracking kernel
   RefConsts ref;
   double *x, *px, *y, *py, *z, *pt;  // flat slot arrays
   int32_t *id;                       // original particle index of each slot
   int32_t *lost_turn, *lost_elem;    // per slot (-1: alive)
   int32_t *live;                     // per seed: live particles occupy slots [off, off+live)
   int32_t *items;                    // work list: (seed, first slot) pairs
-  int32_t *n_items, *next_item;
+  int32_t *n_items, *next_item, *item_chunk;
   int32_t *turn0;                    // device turn counter
   int nturn;                         // turns per block
   double r2;

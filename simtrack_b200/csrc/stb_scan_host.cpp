@@ -101,7 +101,7 @@ stb_scan *scan_build(stb_table **tables, int nseed, const double *x0, const long
   if (s->ntot > (1L << 31) - 1) throw Error(STB_EINVAL, "too many particles for 32-bit ids");
   const long n = s->ntot;
   s->max_items = 0;
-  for (long v : s->n_per_seed) s->max_items += (v + 63) / 64;  // smallest chunk supported: 64
+  for (long v : s->n_per_seed) s->max_items += (v + 31) / 32;  // smallest work item: one warp
   cuda_check(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "stream");
   cuda_check(cudaMalloc(&s->d_seeds, sizeof(ScanSeed) * nseed), "cudaMalloc(seeds)");
   cuda_check(cudaMalloc(&s->d_coords, sizeof(double) * 6 * n), "cudaMalloc(coordinates)");
@@ -153,10 +153,12 @@ stb_scan *scan_build(stb_table **tables, int nseed, const double *x0, const long
   a.n_items = s->d_ctr;
   a.next_item = s->d_ctr + 1;
   a.turn0 = s->d_ctr + 2;
+  a.item_chunk = s->d_ctr + 3;
   a.r2 = radius > 0.0 ? radius * radius : 0.0;
   a.status = s->d_status;
   s->variant = s->smem_ok ? 0 : 2;
   cuda_check(prepare_scan(s->variant, s->num_sms, s->smem, &s->grid), "scan kernel setup");
+  a.grid = s->grid;
   set_chunk(s.get(), kScanVariants[s->variant].block);
   return s.release();
 }
@@ -257,6 +259,70 @@ void scan_run(stb_scan *s, int nturn, int tpb, int use_graph) {
   s->device_ms += ms_total;
 }
 
+// Times one turn block of `nturn` turns per launch variant on a snapshot of
+// the current state (restored after every trial) and keeps the fastest.
+int scan_autotune(stb_scan *s, int nturn, double *timings, int ntimings) {
+  DeviceGuard g(s->device);
+  const long n = s->ntot;
+  const size_t bc = sizeof(double) * 6 * n, bi = sizeof(int32_t) * 5 * n, bl = sizeof(int32_t) * s->nseed,
+               bk = sizeof(int32_t) * 4;
+  char *snap = nullptr;
+  cuda_check(cudaMalloc(&snap, bc + bi + bl + bk), "cudaMalloc(autotune snapshot)");
+  DevFree f{snap};
+  auto save = [&](bool restore) {
+    void *dst[4] = {snap, snap + bc, snap + bc + bi, snap + bc + bi + bl};
+    void *src[4] = {s->d_coords, s->d_i32, s->d_live, s->d_ctr};
+    size_t sz[4] = {bc, bi, bl, bk};
+    for (int k = 0; k < 4; k++)
+      cuda_check(cudaMemcpyAsync(restore ? src[k] : dst[k], restore ? dst[k] : src[k], sz[k], cudaMemcpyDeviceToDevice,
+                                 s->stream), "autotune snapshot");
+  };
+  save(false);
+  cudaEvent_t e0, e1;
+  cuda_check(cudaEventCreate(&e0), "event");
+  cuda_check(cudaEventCreate(&e1), "event");
+  const int saved_v = s->variant, saved_grid = s->grid;
+  int best = -1;
+  float best_ms = 0.f;
+  for (int v = 0; v < kNumScanVariants; v++) {
+    float ms = -1.f;
+    int grid = 0;
+    if ((!kScanVariants[v].smem || s->smem_ok) && prepare_scan(v, s->num_sms, s->smem, &grid) == cudaSuccess) {
+      ScanArgs a = s->args;
+      a.nturn = nturn;
+      a.grid = grid;
+      a.chunk = kScanVariants[v].block;
+      cuda_check(cudaEventRecord(e0, s->stream), "event");
+      cudaError_t le = launch_scan_block(a, v, grid, s->smem, s->stream);
+      cuda_check(cudaEventRecord(e1, s->stream), "event");
+      cuda_check(cudaEventSynchronize(e1), "autotune trial");
+      if (le == cudaSuccess) cuda_check(cudaEventElapsedTime(&ms, e0, e1), "event time");
+      else cudaGetLastError();
+      save(true);
+      cuda_check(cudaStreamSynchronize(s->stream), "autotune restore");
+    } else {
+      cudaGetLastError();
+    }
+    if (timings && v < ntimings) timings[v] = ms;
+    if (ms > 0.f && (best < 0 || ms < best_ms)) {
+      best = v;
+      best_ms = ms;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (best < 0) {
+    s->variant = saved_v;
+    s->grid = saved_grid;
+  } else {
+    s->variant = best;
+    cuda_check(prepare_scan(best, s->num_sms, s->smem, &s->grid), "scan kernel setup");
+    set_chunk(s, kScanVariants[best].block);
+  }
+  s->args.grid = s->grid;
+  return s->variant;
+}
+
 }  // namespace
 }  // namespace stb
 
@@ -291,9 +357,10 @@ int stb_scan_configure(stb_scan *s, int variant, int chunk) {
       cuda_check(prepare_scan(variant, s->num_sms, s->smem, &grid), "scan kernel setup");
       s->variant = variant;
       s->grid = grid;
+      s->args.grid = grid;
     }
     if (chunk > 0) {
-      if (chunk < 64 || chunk % 32) throw Error(STB_EINVAL, "chunk must be a multiple of 32, >= 64");
+      if (chunk < 32 || chunk % 32) throw Error(STB_EINVAL, "chunk must be a positive multiple of 32");
       set_chunk(s, chunk);
     }
     return STB_OK;
@@ -318,6 +385,15 @@ int stb_scan_results(stb_scan *s, int32_t *lost_turn, int32_t *lost_elem, double
     if (lost_elem)
       cuda_check(cudaMemcpy(lost_elem, s->args.out_lost_elem, sizeof(int32_t) * n, cudaMemcpyDeviceToHost), "download");
     if (x_aos) cuda_check(cudaMemcpy(x_aos, s->d_out_x, sizeof(double) * 6 * n, cudaMemcpyDeviceToHost), "download");
+    return STB_OK;
+  });
+}
+
+int stb_scan_autotune(stb_scan *s, int nturn, int *chosen, double *timings_ms, int ntimings) {
+  return guarded([&] {
+    if (!s || nturn <= 0) throw Error(STB_EINVAL, "bad arguments");
+    const int v = scan_autotune(s, nturn, timings_ms, ntimings);
+    if (chosen) *chosen = v;
     return STB_OK;
   });
 }

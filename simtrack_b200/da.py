@@ -75,6 +75,8 @@ def rhic_da_scan(nseed: int = 64, namp: int = 64, amax: float = 12.0, nang: int 
     sc = Scan(tables, grids, aperture_radius=lats[0].aperture_radius, device=device)
     if variant >= 0 or chunk > 0:
         sc.configure(variant, chunk)
+    else:
+        sc.autotune(nturn=min(16, max(1, nturn)))
     sc.run(nturn, turns_per_block, use_graph)
     lt, le, x = sc.results()
     wall = time.perf_counter() - t0
