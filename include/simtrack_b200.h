@@ -33,6 +33,7 @@ typedef struct stb_element stb_element; /* Element*  (simtrack.h:373-396) */
 typedef struct stb_line stb_line;       /* Line      (simtrack.h:1067-1100) */
 typedef struct stb_table stb_table;     /* flattened device element table (no reference counterpart) */
 typedef struct stb_scan stb_scan;       /* batched dynamic-aperture scan (replaces the Track_DA* loops) */
+typedef struct stb_mlp stb_mlp;         /* loss-prediction surrogate network (no reference counterpart) */
 
 /* Message of the last failed call on this thread ("" if none). */
 const char *stb_last_error(void);
@@ -167,6 +168,32 @@ int stb_scan_results(stb_scan *s, int32_t *lost_turn, int32_t *lost_elem, double
 int stb_scan_autotune(stb_scan *s, int nturn, int *chosen, double *timings_ms, int ntimings);
 /* st[0] turns done, [1] device milliseconds, [2] turn blocks, [3] variant, [4] chunk, [5] particles */
 int stb_scan_stats(const stb_scan *s, double *st6);
+
+/* ---- loss-prediction surrogate (no reference counterpart) ----
+ * MLP nin -> hidden -> hidden -> hidden -> nout (GELU, softmax cross-entropy)
+ * with FP32 master parameters, bf16 operands and FP32 accumulation on the
+ * tcgen05 tensor cores.  nin, nout <= 16; hidden a multiple of 16, <= 256;
+ * batches are multiples of 16 up to max_batch.  x, labels, weights and probs
+ * are device pointers (x: [B x nin] FP32 row-major; labels: int32 class ids;
+ * weights: optional per-sample FP32 weights; probs: [B x nout]).
+ * Parameter layout (stb_mlp_get_params/set_params, FP32): for each layer l,
+ * W_l [out x in] row-major then b_l [out]. */
+int stb_mlp_create(int nin, int hidden, int nout, int max_batch, unsigned long long seed, int device, stb_mlp **out);
+int stb_mlp_free(stb_mlp *m);
+long stb_mlp_param_count(const stb_mlp *m);
+/* which = 0: parameters, 1: gradients of the last stb_mlp_gradients/train_step */
+int stb_mlp_get_params(stb_mlp *m, float *host, int which);
+int stb_mlp_set_params(stb_mlp *m, const float *host);
+int stb_mlp_set_adamw(stb_mlp *m, float lr, float beta1, float beta2, float eps, float weight_decay);
+int stb_mlp_forward(stb_mlp *m, const float *x, int B, float *probs);
+/* Loss (host, may be NULL) and gradients of the weighted mean cross-entropy, no update. */
+int stb_mlp_gradients(stb_mlp *m, const float *x, const int32_t *labels, const float *weights, int B, float *loss);
+/* Gradients, then one AdamW step (decoupled weight decay, bias-corrected moments). */
+int stb_mlp_train_step(stb_mlp *m, const float *x, const int32_t *labels, const float *weights, int B, float *loss);
+/* Diagnostics: C[M x N] (FP32, row stride ldc) = A[M x K] * B[N x K]^T for bf16 device
+ * matrices through the tcgen05 GEMM kernel (N a multiple of 16 <= 256, K of 16). */
+int stb_mlp_gemm_test(const void *A, int lda, const void *B, int ldb, int M, int N, int K, float *C, int ldc,
+                      int device);
 
 /* Diagnostics (no reference counterpart): evaluates the kernels' elementary
  * functions on host buffers, on GPU `device` (device >= 0) or on the host CPU

@@ -7,7 +7,7 @@ or a CUDA call fails, the error surfaces as SimTrackError.
 from __future__ import annotations
 
 import ctypes
-from ctypes import POINTER, c_char_p, c_double, c_int, c_int32, c_long, c_void_p
+from ctypes import POINTER, c_char_p, c_double, c_float, c_int, c_int32, c_long, c_ulonglong, c_void_p
 from pathlib import Path
 
 LIB_PATH = Path(__file__).resolve().parent / "_lib" / "libsimtrack_b200.so"
@@ -75,6 +75,16 @@ SIGNATURES = [
     ("stb_scan_results", c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
     ("stb_scan_stats", c_int, [c_void_p, POINTER(c_double)]),
     ("stb_scan_autotune", c_int, [c_void_p, c_int, POINTER(c_int), POINTER(c_double), c_int]),
+    ("stb_mlp_create", c_int, [c_int, c_int, c_int, c_int, c_ulonglong, c_int, POINTER(c_void_p)]),
+    ("stb_mlp_free", c_int, [c_void_p]),
+    ("stb_mlp_param_count", c_long, [c_void_p]),
+    ("stb_mlp_get_params", c_int, [c_void_p, POINTER(c_float), c_int]),
+    ("stb_mlp_set_params", c_int, [c_void_p, POINTER(c_float)]),
+    ("stb_mlp_set_adamw", c_int, [c_void_p, c_float, c_float, c_float, c_float, c_float]),
+    ("stb_mlp_forward", c_int, [c_void_p, c_void_p, c_int, c_void_p]),
+    ("stb_mlp_gradients", c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, POINTER(c_float)]),
+    ("stb_mlp_train_step", c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, POINTER(c_float)]),
+    ("stb_mlp_gemm_test", c_int, [c_void_p, c_int, c_void_p, c_int, c_int, c_int, c_int, c_void_p, c_int, c_int]),
     ("stb_fp64_peak", c_int, [c_int, POINTER(c_double)]),
     ("stb_math_eval", c_int, [c_int, POINTER(c_double), POINTER(c_double), c_long, c_int]),
     ("stb_track_probe", c_int, [c_void_p, POINTER(c_double), c_long, c_int, c_double, POINTER(c_double),

@@ -354,3 +354,55 @@ class Scan:
                 lib().stb_scan_free(self._h)
         except Exception:
             pass
+
+
+class MLP:
+    """The loss-prediction surrogate network on the tensor cores (stb_mlp_*)."""
+
+    def __init__(self, nin: int = 12, hidden: int = 256, nout: int = 2, max_batch: int = 4096, seed: int = 0,
+                 device: int = 0):
+        h = c_void_p()
+        check(lib().stb_mlp_create(nin, hidden, nout, max_batch, seed, device, byref(h)))
+        self._h = h
+        self.nin, self.hidden, self.nout, self.max_batch = nin, hidden, nout, max_batch
+
+    @property
+    def nparams(self) -> int:
+        return int(lib().stb_mlp_param_count(self._h))
+
+    def get_params(self, which: int = 0) -> np.ndarray:
+        out = np.empty(self.nparams, dtype=np.float32)
+        check(lib().stb_mlp_get_params(self._h, out.ctypes.data_as(POINTER(ctypes.c_float)), which))
+        return out
+
+    def set_params(self, p: np.ndarray) -> None:
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        check(lib().stb_mlp_set_params(self._h, p.ctypes.data_as(POINTER(ctypes.c_float))))
+
+    def set_adamw(self, lr=1e-3, beta1=0.9, beta2=0.999, eps=1e-8, weight_decay=1e-2) -> None:
+        check(lib().stb_mlp_set_adamw(self._h, lr, beta1, beta2, eps, weight_decay))
+
+    def forward(self, x, probs) -> None:
+        """x: CUDA float32 tensor [B, nin]; probs: CUDA float32 tensor [B, nout] (written)."""
+        check(lib().stb_mlp_forward(self._h, c_void_p(x.data_ptr()), x.shape[0], c_void_p(probs.data_ptr())))
+
+    def gradients(self, x, labels, weights=None) -> float:
+        loss = ctypes.c_float()
+        check(lib().stb_mlp_gradients(self._h, c_void_p(x.data_ptr()), c_void_p(labels.data_ptr()),
+                                      None if weights is None else c_void_p(weights.data_ptr()), x.shape[0],
+                                      byref(loss)))
+        return loss.value
+
+    def train_step(self, x, labels, weights=None) -> float:
+        loss = ctypes.c_float()
+        check(lib().stb_mlp_train_step(self._h, c_void_p(x.data_ptr()), c_void_p(labels.data_ptr()),
+                                       None if weights is None else c_void_p(weights.data_ptr()), x.shape[0],
+                                       byref(loss)))
+        return loss.value
+
+    def __del__(self):
+        try:
+            if self._h:
+                lib().stb_mlp_free(self._h)
+        except Exception:
+            pass
