@@ -168,6 +168,41 @@ int stb_scan_results(stb_scan *s, int32_t *lost_turn, int32_t *lost_elem, double
 int stb_scan_autotune(stb_scan *s, int nturn, int *chosen, double *timings_ms, int ntimings);
 /* st[0] turns done, [1] device milliseconds, [2] turn blocks, [3] variant, [4] chunk, [5] particles */
 int stb_scan_stats(const stb_scan *s, double *st6);
+/* Turn-by-turn record at the start of the line, as Track_tbt (simtrack.cpp:20841)
+ * keeps it, for all particles at once: after global turn t < nturns the scan
+ * writes x, px, y, py of particle i (x0 order) to tbt[(t*4 + k)*n + i], n the
+ * scan's particle count; tbt is a device buffer of nturns*4*n doubles owned by
+ * the caller (entries of lost particles stop at their loss).  nturns = 0
+ * switches recording off. */
+int stb_scan_set_tbt(stb_scan *s, double *tbt, int nturns);
+/* Removes the live particles with mask[i] != 0 (host array of n bytes, x0
+ * order) from further tracking; their result is lost_turn = STB_RETIRED with
+ * the coordinates at retirement.  Used by the surrogate to stop tracking the
+ * particles it has classified. */
+#define STB_RETIRED 0x40000000
+int stb_scan_retire(stb_scan *s, const uint8_t *mask);
+
+/* ---- turn-by-turn diagnostics ----
+ * FineTuneFinder (simtrack.cpp:2288-2319; with px != NULL the x/px form,
+ * 2321-2352) for nsig signals at once: sample i of signal j is
+ * x[i*stride + j] (device arrays; stride >= nsig when nsig > 1), n <= 4096
+ * samples; the same coarse 1e-3 scan over [tune_lower, tune_upper) and
+ * ten-fold zooms down to a 1e-12 step.  tune: device array [nsig].
+ * Asynchronous on `stream`. */
+int stb_fine_tune(const double *x, const double *px, int n, long nsig, long stride, double tune_lower,
+                  double tune_upper, double *tune, int device, void *stream);
+/* Early-turn features of the loss-prediction surrogate (no reference
+ * counterpart; built from Track_tbt_FMA's ingredients, simtrack.cpp:21179-21241):
+ * per particle i, from tbt[(t*4 + k)*ntot + i] (t < nturn; x, px, y, py),
+ * the initial coordinates x0[k*ntot + i] (k < 6) and the window tunes
+ * tunes[w*ntot + i] (Qx, Qy of the first window, Qx, Qy of the second):
+ * features[i*12 + f] = amplitude_x, amplitude_y (sigma units), 1e3*pt,
+ * atan2(amp_y, amp_x), the four tunes, log10|dQx|, log10|dQy|, log10 of the
+ * action spread over the record relative to the initial action, and the
+ * largest amplitude reached.  twiss6 (host) = beta_x, alpha_x, beta_y,
+ * alpha_y, emit_x, emit_y at the record point.  Asynchronous on `stream`. */
+int stb_tbt_features(const double *tbt, long ntot, int nturn, const double *x0, const double *tunes,
+                     const double *twiss6, float *features, int device, void *stream);
 
 /* ---- loss-prediction surrogate (no reference counterpart) ----
  * MLP nin -> hidden -> hidden -> hidden -> nout (GELU, softmax cross-entropy)

@@ -800,3 +800,46 @@ void port_track_dump(const port_elem *e, long ne, const port_gp *gp, double *x, 
     }
   }
 }
+
+/* DFT power of the samples at one tune; the phase argument and the sums are
+ * formed in the reference's order (simtrack.cpp:2302-2306, 2335-2339). */
+static double dft_power(int n, const double *x, const double *px, double tune)
+{
+  const double pi_ref = 3.14159265358979323; /* PI, simtrack.cpp:23 */
+  double re = 0.0, im = 0.0;
+  int i;
+  for (i = 0; i < n; i++) {
+    const double arg = -2 * pi_ref * i * tune;
+    const double c = cos(arg), s = sin(arg);
+    if (px) {
+      re = re + x[i] * c - px[i] * s;
+      im = im + x[i] * s + px[i] * c;
+    } else {
+      re = re + x[i] * c;
+      im = im + x[i] * s;
+    }
+  }
+  return re * re + im * im;
+}
+
+/* Coarse scan with step 1e-3 over [lower, upper), then repeated zooms to
+ * [peak - step, peak + step) with a ten times finer step, until the step is
+ * no longer above 1e-12; the first strict maximum of each scan wins. */
+double port_fine_tune(int n, const double *x, const double *px, double tune_lower, double tune_upper)
+{
+  double step = 0.001, lo = tune_lower, hi = tune_upper, peak = tune_lower;
+  for (;;) {
+    double best = 0.0, t = lo;
+    peak = lo;
+    do {
+      const double p = dft_power(n, x, px, t);
+      if (p > best) { best = p; peak = t; }
+      t = t + step;
+    } while (t < hi);
+    lo = peak - step;
+    hi = peak + step;
+    step = step / 10.;
+    if (!(step > 1.0e-12)) break;
+  }
+  return peak;
+}

@@ -61,6 +61,10 @@ int port_pass(const port_elem *e, const port_gp *gp, double *x);
 /* Faddeeva function w(z) (cerrf, simtrack.cpp:6258-6323). */
 void port_cerrf(double xx, double yy, double *wx, double *wy);
 
+/* Peak-DFT tune of n samples (FineTuneFinder, simtrack.cpp:2288-2319; with
+ * px != NULL the x/px form of simtrack.cpp:2321-2352). */
+double port_fine_tune(int n, const double *x, const double *px, double tune_lower, double tune_upper);
+
 #ifdef __cplusplus
 }
 #endif

@@ -17,6 +17,7 @@
 #include "simtrack.h"
 
 #include <cstring>
+#include <vector>
 #include <cmath>
 
 extern GlobalVariables GP;
@@ -198,5 +199,18 @@ void ref_track_dump(void *line, double *x, int nturn, double radius, double *dum
 }
 
 double ref_pinv(double p) { return gsl_cdf_ugaussian_Pinv(p); }
+
+// FineTuneFinder, both overloads (simtrack.cpp:2288, 2321).
+double ref_fine_tune(int n, const double *x, const double *px, double lo, double hi) {
+  std::vector<double> a(x, x + n);
+  double tune = 0.0;
+  if (px) {
+    std::vector<double> b(px, px + n);
+    FineTuneFinder(n, a.data(), b.data(), lo, hi, tune);
+  } else {
+    FineTuneFinder(n, a.data(), lo, hi, tune);
+  }
+  return tune;
+}
 
 }  // extern "C"

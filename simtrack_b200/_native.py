@@ -75,6 +75,12 @@ SIGNATURES = [
     ("stb_scan_results", c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
     ("stb_scan_stats", c_int, [c_void_p, POINTER(c_double)]),
     ("stb_scan_autotune", c_int, [c_void_p, c_int, POINTER(c_int), POINTER(c_double), c_int]),
+    ("stb_scan_set_tbt", c_int, [c_void_p, c_void_p, c_int]),
+    ("stb_fine_tune", c_int, [c_void_p, c_void_p, c_int, c_long, c_long, c_double, c_double, c_void_p, c_int,
+                              c_void_p]),
+    ("stb_tbt_features", c_int, [c_void_p, c_long, c_int, c_void_p, c_void_p, POINTER(c_double), c_void_p, c_int,
+                                 c_void_p]),
+    ("stb_scan_retire", c_int, [c_void_p, c_void_p]),
     ("stb_mlp_create", c_int, [c_int, c_int, c_int, c_int, c_ulonglong, c_int, POINTER(c_void_p)]),
     ("stb_mlp_free", c_int, [c_void_p]),
     ("stb_mlp_param_count", c_long, [c_void_p]),

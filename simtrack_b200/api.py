@@ -342,6 +342,25 @@ class Scan:
                                      c_void_p(x.ctypes.data)))
         return lt, le, x
 
+    def set_tbt(self, tbt, nturns: int) -> None:
+        """Records x, px, y, py of every particle after each of the first nturns
+        turns into the CUDA float64 tensor tbt[nturns, 4, n] (None: stop)."""
+        if tbt is None or nturns == 0:
+            check(lib().stb_scan_set_tbt(self._h, None, 0))
+            self._tbt = None
+            return
+        if tuple(tbt.shape) != (nturns, 4, self.n) or not tbt.is_contiguous():
+            raise SimTrackError(-1, "tbt must be a contiguous [nturns, 4, n] tensor")
+        self._tbt = tbt  # keep the buffer alive while the scan writes it
+        check(lib().stb_scan_set_tbt(self._h, c_void_p(tbt.data_ptr()), nturns))
+
+    def retire(self, mask) -> None:
+        """Stops tracking the live particles with mask[i] true (x0 order)."""
+        m = np.ascontiguousarray(np.asarray(mask, dtype=np.uint8).reshape(-1))
+        if m.size != self.n:
+            raise SimTrackError(-1, "mask must have one entry per particle")
+        check(lib().stb_scan_retire(self._h, c_void_p(m.ctypes.data)))
+
     def stats(self) -> dict:
         st = (c_double * 6)()
         check(lib().stb_scan_stats(self._h, st))
@@ -354,6 +373,38 @@ class Scan:
                 lib().stb_scan_free(self._h)
         except Exception:
             pass
+
+
+RETIRED = 0x40000000  # lost_turn of particles removed by Scan.retire
+
+
+def fine_tune(x, n: int, nsig: int, stride: int, tune_lower: float, tune_upper: float, out, px=None,
+              offset: int = 0, device: int = 0, stream=None) -> None:
+    """FineTuneFinder (simtrack.cpp:2288 / 2321) for nsig signals at once on
+    the GPU: sample i of signal j is x.flat[offset + i * stride + j] (CUDA
+    float64 tensors; px optional, same layout); out: CUDA float64 [nsig]."""
+    esz = 8
+    xp = c_void_p(x.data_ptr() + offset * esz)
+    pp = None if px is None else c_void_p(px.data_ptr() + offset * esz)
+    check(lib().stb_fine_tune(xp, pp, n, nsig, stride, tune_lower, tune_upper, c_void_p(out.data_ptr()), device,
+                              None if stream is None else c_void_p(stream)))
+
+
+NUM_FEATURES = 12
+FEATURE_NAMES = ["amp_x", "amp_y", "delta_1e3", "angle", "qx_w1", "qy_w1", "qx_w2", "qy_w2",
+                 "log10_dqx", "log10_dqy", "log10_action_spread", "max_amp"]
+
+
+def tbt_features(tbt, x0, tunes, twiss6, out, device: int = 0, stream=None) -> None:
+    """Surrogate features from a turn-by-turn record tbt[nturn, 4, n], initial
+    coordinates x0[6, n] and window tunes[4, n] (all CUDA float64) into
+    out[n, 12] (CUDA float32).  twiss6 = (beta_x, alpha_x, beta_y, alpha_y,
+    emit_x, emit_y) at the record point."""
+    nturn, _, n = tbt.shape
+    tw = (c_double * 6)(*[float(v) for v in twiss6])
+    check(lib().stb_tbt_features(c_void_p(tbt.data_ptr()), n, nturn, c_void_p(x0.data_ptr()),
+                                 c_void_p(tunes.data_ptr()), tw, c_void_p(out.data_ptr()), device,
+                                 None if stream is None else c_void_p(stream)))
 
 
 class MLP:

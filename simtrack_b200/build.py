@@ -22,10 +22,11 @@ CSRC = PKG / "csrc"
 LIBDIR = PKG / "_lib"
 LIB = LIBDIR / "libsimtrack_b200.so"
 
-CUDA_SOURCES = ["stb_track.cu", "stb_scan.cu", "stb_diag.cu", "stb_mlp.cu", "stb_mlp_ops.cu"]
-CXX_SOURCES = ["stb_elements.cpp", "stb_flatten.cpp", "stb_capi.cpp", "stb_scan_host.cpp", "stb_mlp_host.cpp"]
+CUDA_SOURCES = ["stb_track.cu", "stb_scan.cu", "stb_tune.cu", "stb_diag.cu", "stb_mlp.cu", "stb_mlp_ops.cu"]
+CXX_SOURCES = ["stb_elements.cpp", "stb_flatten.cpp", "stb_capi.cpp", "stb_scan_host.cpp", "stb_mlp_host.cpp",
+               "stb_tune_host.cpp"]
 HEADERS = ["stb_table.hpp", "stb_physics.cuh", "stb_crmath.cuh", "stb_kernels.hpp", "stb_status.hpp", "stb_flatten.hpp",
-           "stb_track_impl.cuh", "stb_scan.hpp", "stb_runtime.hpp", "stb_mlp.hpp"]
+           "stb_track_impl.cuh", "stb_scan.hpp", "stb_runtime.hpp", "stb_mlp.hpp", "stb_tune.hpp"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off",

@@ -145,6 +145,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) scan_track_kernel(const __
       }
       pt_refresh(R, p[0].pt, c[0]);
       int lt = -1, le = 0;
+      const long id = a.tbt ? (long)a.id[i] : 0;
       for (int t = 0; t < a.nturn && lt < 0; t++) {
         for (int e = 0; e < sd.nelem; e++) {
           const ElemHeader h = hdr[e];
@@ -154,6 +155,14 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) scan_track_kernel(const __
             le = e;
             break;
           }
+        }
+        const int tg = turn0 + t;
+        if (a.tbt && lt < 0 && tg < a.tbt_turns) {
+          double *d = a.tbt + (size_t)tg * 4 * a.ntot + id;
+          d[0] = p[0].x;
+          d[a.ntot] = p[0].px;
+          d[2 * a.ntot] = p[0].y;
+          d[3 * a.ntot] = p[0].py;
         }
       }
       a.x[i] = p[0].x;
@@ -242,6 +251,19 @@ __global__ void __launch_bounds__(kCompactBlock) scan_compact_kernel(ScanArgs a)
   }
 }
 
+__global__ void scan_retire_kernel(ScanArgs a, const uint8_t *mask) {
+  const int s = blockIdx.y;
+  const ScanSeed sd = a.seeds[s];
+  const int live = a.live[s];
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < live; j += gridDim.x * blockDim.x) {
+    const long i = sd.off + j;
+    if (a.lost_turn[i] < 0 && mask[a.id[i]]) {
+      a.lost_turn[i] = kRetiredCode;
+      a.lost_elem[i] = 0;
+    }
+  }
+}
+
 // Particles still alive at the end of the run: outputs with lost_turn = -1.
 __global__ void scan_finalize_kernel(ScanArgs a) {
   const int s = blockIdx.y;
@@ -298,6 +320,17 @@ cudaError_t launch_scan_block(const ScanArgs &a, int variant, int grid, size_t s
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   scan_compact_kernel<<<a.nseed, kCompactBlock, 0, st>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_scan_compact_only(const ScanArgs &a, cudaStream_t st) {
+  scan_compact_kernel<<<a.nseed, kCompactBlock, 0, st>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_scan_retire(const ScanArgs &a, const uint8_t *mask, long max_per_seed, cudaStream_t st) {
+  dim3 grid((unsigned)std::max<long>(1, std::min<long>((max_per_seed + 255) / 256, 64)), (unsigned)a.nseed);
+  scan_retire_kernel<<<grid, 256, 0, st>>>(a, mask);
   return cudaGetLastError();
 }
 

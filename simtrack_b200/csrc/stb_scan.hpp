@@ -39,7 +39,16 @@ struct ScanArgs {
   int *status;
   int32_t *out_lost_turn, *out_lost_elem;  // by original index
   double *out_x;                           // AoS by original index
+  // Optional turn-by-turn record at the start of the line: after turn t
+  // (global index, t < tbt_turns) x, px, y, py of particle `id` go to
+  // tbt[(t * 4 + k) * ntot + id].
+  double *tbt;
+  int tbt_turns;
+  long ntot;
 };
+
+// Loss code written for particles removed by stb_scan_retire (never a turn).
+constexpr int32_t kRetiredCode = 0x40000000;
 
 struct ScanVariant {
   bool smem;
@@ -57,5 +66,10 @@ cudaError_t prepare_scan(int variant, int num_sms, size_t smem, int *grid);
 cudaError_t launch_scan_block(const ScanArgs &a, int variant, int grid, size_t smem, cudaStream_t st);
 // Outputs for the particles still alive.
 cudaError_t launch_scan_finalize(const ScanArgs &a, long max_per_seed, cudaStream_t st);
+// Marks the live particles whose original index has mask[id] != 0 as retired
+// (removed at the next compaction, output lost_turn = kRetiredCode).
+cudaError_t launch_scan_retire(const ScanArgs &a, const uint8_t *mask, long max_per_seed, cudaStream_t st);
+// One compaction pass (advances the turn counter by a.nturn).
+cudaError_t launch_scan_compact_only(const ScanArgs &a, cudaStream_t st);
 
 }  // namespace stb

@@ -156,6 +156,9 @@ stb_scan *scan_build(stb_table **tables, int nseed, const double *x0, const long
   a.item_chunk = s->d_ctr + 3;
   a.r2 = radius > 0.0 ? radius * radius : 0.0;
   a.status = s->d_status;
+  a.tbt = nullptr;
+  a.tbt_turns = 0;
+  a.ntot = n;
   s->variant = s->smem_ok ? 0 : 2;
   cuda_check(prepare_scan(s->variant, s->num_sms, s->smem, &s->grid), "scan kernel setup");
   a.grid = s->grid;
@@ -394,6 +397,39 @@ int stb_scan_autotune(stb_scan *s, int nturn, int *chosen, double *timings_ms, i
     if (!s || nturn <= 0) throw Error(STB_EINVAL, "bad arguments");
     const int v = scan_autotune(s, nturn, timings_ms, ntimings);
     if (chosen) *chosen = v;
+    return STB_OK;
+  });
+}
+
+int stb_scan_set_tbt(stb_scan *s, double *tbt, int nturns) {
+  return guarded([&] {
+    if (!s) throw Error(STB_EINVAL, "NULL scan");
+    if (nturns < 0 || (nturns > 0 && !tbt)) throw Error(STB_EINVAL, "bad turn-by-turn buffer");
+    s->args.tbt = nturns > 0 ? tbt : nullptr;
+    s->args.tbt_turns = nturns;
+    if (s->graph) {  // captured launches embed the old arguments
+      cudaGraphExecDestroy(s->graph);
+      s->graph = nullptr;
+    }
+    return STB_OK;
+  });
+}
+
+int stb_scan_retire(stb_scan *s, const uint8_t *mask) {
+  return guarded([&] {
+    if (!s || !mask) throw Error(STB_EINVAL, "NULL argument");
+    DeviceGuard g(s->device);
+    uint8_t *d = nullptr;
+    cuda_check(cudaMalloc(&d, (size_t)s->ntot), "cudaMalloc(retire mask)");
+    DevFree f{d};
+    cuda_check(cudaMemcpy(d, mask, (size_t)s->ntot, cudaMemcpyHostToDevice), "upload mask");
+    cuda_check(launch_scan_retire(s->args, d, s->max_per_seed, s->stream), "retire");
+    // compact now so the retired particles leave the work list immediately
+    ScanArgs a = s->args;
+    a.nturn = 0;
+    cuda_check(stb::launch_scan_compact_only(a, s->stream), "compaction");
+    cuda_check(launch_scan_finalize(s->args, s->max_per_seed, s->stream), "finalize");
+    cuda_check(cudaStreamSynchronize(s->stream), "retire");
     return STB_OK;
   });
 }

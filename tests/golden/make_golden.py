@@ -40,9 +40,40 @@ CASES = {
 }
 
 
+def tune_signals(n: int = 512, count: int = 12, seed: int = 7):
+    """Turn-by-turn-like test signals: a betatron line with random tune,
+    phase and amplitude, a weaker second line, slow amplitude modulation and
+    noise; px is the matching conjugate signal."""
+    rng = np.random.default_rng(seed)
+    i = np.arange(n)
+    xs, pxs = [], []
+    for k in range(count):
+        q1 = rng.uniform(0.21, 0.44)
+        q2 = rng.uniform(0.05, 0.48)
+        a1 = rng.uniform(1e-4, 1e-2)
+        ph = rng.uniform(0, 2 * np.pi)
+        mod = 1.0 + 0.05 * np.sin(2 * np.pi * i * rng.uniform(0.001, 0.01))
+        x = a1 * mod * np.cos(2 * np.pi * q1 * i + ph) + 0.1 * a1 * np.cos(2 * np.pi * q2 * i)
+        px = -a1 * mod * np.sin(2 * np.pi * q1 * i + ph)
+        x = x + rng.normal(0, 1e-3 * a1, n)
+        xs.append(x)
+        pxs.append(px)
+    return np.array(xs), np.array(pxs)
+
+
+# tune windows of the fixture: (lower, upper, with px)
+TUNE_WINDOWS = [(0.2, 0.45, False), (0.0, 0.5, False), (0.0, 1.0, True)]
+
+
 def main():
     from oracle_bridge import RefOracle
     ref = RefOracle()
+    xs, pxs = tune_signals()
+    tunes = np.array([[ref.fine_tune(x, px if w else None, lo, hi) for lo, hi, w in TUNE_WINDOWS]
+                      for x, px in zip(xs, pxs)])
+    np.savez_compressed(HERE / "fine_tune.npz", x=xs, px=pxs, windows=np.array(TUNE_WINDOWS, dtype=np.float64),
+                        tunes=tunes)
+    print("wrote fine_tune")
     for name, c in CASES.items():
         ref.build(lattice_for(name))
         dumps, loss = [], []

@@ -61,6 +61,8 @@ class RefOracle:
         L.ref_pinv.argtypes = [c_double]
         L.ref_pinv.restype = c_double
         L.ref_pass.argtypes = [c_void_p, c_long, POINTER(c_double)]
+        L.ref_fine_tune.argtypes = [c_int, POINTER(c_double), POINTER(c_double), c_double, c_double]
+        L.ref_fine_tune.restype = c_double
         self.L = L
         self.line = None
         self.nelem = 0
@@ -115,6 +117,13 @@ class RefOracle:
                               ctypes.byref(lp))
         return x, st.value, lt.value, lp.value, dump
 
+    def fine_tune(self, x, px=None, lo: float = 0.0, hi: float = 0.5) -> float:
+        """FineTuneFinder (x-only, or the x/px overload when px is given)."""
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        p = None if px is None else np.ascontiguousarray(px, dtype=np.float64)
+        return self.L.ref_fine_tune(len(x), x.ctypes.data_as(POINTER(c_double)),
+                                    None if p is None else p.ctypes.data_as(POINTER(c_double)), lo, hi)
+
     def pinv(self, p: float) -> float:
         return self.L.ref_pinv(p)
 
@@ -146,6 +155,8 @@ class PortOracle:
         L.port_track_dump.argtypes = [POINTER(PortElem), c_long, POINTER(PortGP), POINTER(c_double), c_int,
                                       c_double, POINTER(c_double), POINTER(c_int), POINTER(c_int), POINTER(c_int)]
         L.port_cerrf.argtypes = [c_double, c_double, POINTER(c_double), POINTER(c_double)]
+        L.port_fine_tune.argtypes = [c_int, POINTER(c_double), POINTER(c_double), c_double, c_double]
+        L.port_fine_tune.restype = c_double
         self.L = L
 
     def build(self, lat: Lattice) -> None:
@@ -230,6 +241,12 @@ class PortOracle:
                                nturn, radius, dump.ctypes.data_as(POINTER(c_double)), ctypes.byref(st),
                                ctypes.byref(lt), ctypes.byref(lp))
         return x, st.value, lt.value, lp.value, dump
+
+    def fine_tune(self, x, px=None, lo: float = 0.0, hi: float = 0.5) -> float:
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        p = None if px is None else np.ascontiguousarray(px, dtype=np.float64)
+        return self.L.port_fine_tune(len(x), x.ctypes.data_as(POINTER(c_double)),
+                                     None if p is None else p.ctypes.data_as(POINTER(c_double)), lo, hi)
 
     def cerrf(self, x: float, y: float):
         wx, wy = c_double(), c_double()

@@ -60,3 +60,53 @@ def test_scan_variants_agree():
         else:
             for a, b in zip(ref, res):
                 assert np.array_equal(a, b)
+
+
+def test_scan_turn_by_turn_record_and_retire():
+    import torch
+
+    from simtrack_b200.api import RETIRED
+
+    tabs, xs, lats = seed_setup(2, namp=12, nang=3)
+    sc = Scan(tabs, xs, aperture_radius=0.03)
+    n = sc.n
+    nrec = 24
+    tbt = torch.full((nrec, 4, n), float("nan"), dtype=torch.float64, device="cuda:0")
+    sc.set_tbt(tbt, nrec)
+    sc.run(10, turns_per_block=5)
+    # retire every third particle (x0 order) after 10 turns
+    mask = np.zeros(n, dtype=bool)
+    mask[::3] = True
+    lt10, _, _ = sc.results()
+    sc.retire(mask)
+    sc.run(30, turns_per_block=8)
+    lt_s, le_s, x_s = sc.results()
+    rec = tbt.cpu().numpy()
+    # reference: per-seed single-table tracking one turn at a time
+    off = 0
+    for s in range(2):
+        m = len(xs[s])
+        coords = torch.tensor(xs[s].T.copy(), dtype=torch.float64, device="cuda:0").contiguous()
+        lost = torch.full((m,), -1, dtype=torch.int32, device="cuda:0")
+        le = torch.zeros(m, dtype=torch.int32, device="cuda:0")
+        for t in range(nrec):
+            tabs[s].track_device([coords[k] for k in range(6)], lost, le, t, 1, 0.03)
+            c = coords.cpu().numpy()
+            l = lost.cpu().numpy()
+            live = l < 0
+            if t >= 10:
+                live &= ~mask[off:off + m]
+            for k, row in enumerate((0, 1, 2, 3)):
+                got = rec[t, k, off:off + m]
+                assert np.array_equal(got[live], c[row][live]), f"seed {s} turn {t} coord {k}"
+        off += m
+    retired = (lt10 < 0) & mask
+    assert retired.any()
+    assert np.all(lt_s[retired] == RETIRED)
+    # the others follow the plain scan exactly
+    plain = Scan(tabs, xs, aperture_radius=0.03)
+    plain.run(40, turns_per_block=8)
+    lt_p, le_p, x_p = plain.results()
+    keep = ~retired
+    assert np.array_equal(lt_s[keep], lt_p[keep])
+    assert np.array_equal(x_s[keep], x_p[keep])

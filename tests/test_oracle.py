@@ -80,9 +80,9 @@ def test_port_matches_reference_every_element(which, ref_oracle, port_oracle):
 
 def test_port_matches_golden(port_oracle):
     """Bit-level agreement with outputs of the reference itself, run here."""
-    files = sorted(GOLDEN.glob("*.npz"))
-    assert files, "golden fixtures missing"
-    from golden.make_golden import lattice_for
+    from golden.make_golden import CASES, lattice_for
+    files = [GOLDEN / f"{name}.npz" for name in CASES]
+    assert all(f.exists() for f in files), "golden fixtures missing"
     for f in files:
         g = np.load(f)
         lat = lattice_for(str(g["lattice"]))
