@@ -129,6 +129,27 @@ int stb_track_device(stb_table *t, double *x, double *px, double *y, double *py,
 int stb_track_host(stb_table *t, double *x, long n, int nturn, double aperture_radius, int *stable,
                    int *lost_turn, int *lost_post);
 
+/* Seed-batched tracking that allocates nothing (no counterpart in the
+ * reference).  Same semantics as stb_track_device applied to each table in
+ * turn: nseed tables (one device, one reference particle), seed s owning
+ * n_per_seed[s] consecutive particles of the SoA device arrays x..pt,
+ * lost_turn, lost_elem; particles with lost_turn >= 0 on entry are skipped.
+ * Its work list, counters and status word live in a fixed static device
+ * array sized for at most STB_STATIC_MAX_SEEDS seeds and
+ * STB_STATIC_MAX_PARTICLES particles in total (larger requests fail with
+ * STB_EINVAL): for callers whose device memory belongs to another allocator's
+ * pool, or which must not call cudaMalloc/cudaFree (they synchronise the
+ * device) between their own kernels.  Each call rewrites the whole scratch
+ * before use.  The first call on a device looks the scratch up
+ * (cudaGetSymbolAddress); make it before any stream capture begins on that
+ * device.  Calls that overlap in time on one device race on the shared
+ * scratch.  Waits for `stream` before returning. */
+#define STB_STATIC_MAX_SEEDS 64
+#define STB_STATIC_MAX_PARTICLES 1048576
+int stb_track_seeds_static(stb_table *const *tables, int nseed, const long *n_per_seed, double *x, double *px,
+                           double *y, double *py, double *z, double *pt, int32_t *lost_turn, int32_t *lost_elem,
+                           int turn0, int nturn, double aperture_radius, void *stream);
+
 /* Per-element probe: as stb_track_host, and additionally writes the six
  * coordinates after every element to dump[((i*nturn + turn)*ncell + j)*6 + k]
  * (host buffer of n*nturn*ncell*6 doubles; entries after a particle's loss are

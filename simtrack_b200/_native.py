@@ -81,6 +81,8 @@ SIGNATURES = [
     ("stb_tbt_features", c_int, [c_void_p, c_long, c_int, c_void_p, c_void_p, POINTER(c_double), c_void_p, c_int,
                                  c_void_p]),
     ("stb_scan_retire", c_int, [c_void_p, c_void_p]),
+    ("stb_track_seeds_static", c_int, [POINTER(c_void_p), c_int, POINTER(c_long)] + [c_void_p] * 8 +
+     [c_int, c_int, c_double, c_void_p]),
     ("stb_mlp_create", c_int, [c_int, c_int, c_int, c_int, c_ulonglong, c_int, POINTER(c_void_p)]),
     ("stb_mlp_free", c_int, [c_void_p]),
     ("stb_mlp_param_count", c_long, [c_void_p]),

@@ -378,6 +378,20 @@ class Scan:
 RETIRED = 0x40000000  # lost_turn of particles removed by Scan.retire
 
 
+def track_seeds_static(tables, n_per_seed, coords, lost_turn, lost_elem, turn0: int, nturn: int,
+                       aperture_radius: float = 0.0, stream=None) -> None:
+    """stb_track_seeds_static: tracks several seed tables' particles in one
+    work-list launch without allocating device memory.  coords: CUDA float64
+    tensor [6, n] (x, px, y, py, z, pt rows; seed 0's particles first);
+    lost_turn, lost_elem: CUDA int32 tensors [n]."""
+    arr = (c_void_p * len(tables))(*[t._h for t in tables])
+    nps = (ctypes.c_long * len(tables))(*[int(v) for v in n_per_seed])
+    ptrs = [c_void_p(coords[k].data_ptr()) for k in range(6)]
+    st = None if stream is None else c_void_p(stream)
+    check(lib().stb_track_seeds_static(arr, len(tables), nps, *ptrs, c_void_p(lost_turn.data_ptr()),
+                                       c_void_p(lost_elem.data_ptr()), turn0, nturn, aperture_radius, st))
+
+
 def fine_tune(x, n: int, nsig: int, stride: int, tune_lower: float, tune_upper: float, out, px=None,
               offset: int = 0, device: int = 0, stream=None) -> None:
     """FineTuneFinder (simtrack.cpp:2288 / 2321) for nsig signals at once on

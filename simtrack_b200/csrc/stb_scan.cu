@@ -328,6 +328,18 @@ cudaError_t launch_scan_compact_only(const ScanArgs &a, cudaStream_t st) {
   return cudaGetLastError();
 }
 
+cudaError_t launch_scan_track_only(const ScanArgs &a, int variant, int grid, size_t smem, cudaStream_t st) {
+  scan_worklist_kernel<<<1, 1024, 0, st>>>(a);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  switch (variant) {
+    case 0: scan_track_kernel<true, 1024, 1><<<grid, 1024, smem, st>>>(a); break;
+    case 2: scan_track_kernel<false, 256, 4><<<grid, 256, 0, st>>>(a); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
 cudaError_t launch_scan_retire(const ScanArgs &a, const uint8_t *mask, long max_per_seed, cudaStream_t st) {
   dim3 grid((unsigned)std::max<long>(1, std::min<long>((max_per_seed + 255) / 256, 64)), (unsigned)a.nseed);
   scan_retire_kernel<<<grid, 256, 0, st>>>(a, mask);

@@ -71,5 +71,8 @@ cudaError_t launch_scan_finalize(const ScanArgs &a, long max_per_seed, cudaStrea
 cudaError_t launch_scan_retire(const ScanArgs &a, const uint8_t *mask, long max_per_seed, cudaStream_t st);
 // One compaction pass (advances the turn counter by a.nturn).
 cudaError_t launch_scan_compact_only(const ScanArgs &a, cudaStream_t st);
+// Work list + tracking without compaction (variants 0 and 2 only): particles
+// keep their slots, lost ones are skipped by their lost_turn.
+cudaError_t launch_scan_track_only(const ScanArgs &a, int variant, int grid, size_t smem, cudaStream_t st);
 
 }  // namespace stb
