@@ -217,6 +217,7 @@ def run_ours(a):
 
     from simtrack_b200 import lattices
     from simtrack_b200.api import Table
+    from simtrack_b200.parallel import reduce_scalar
     from simtrack_b200._native import lib
     import ctypes
 
@@ -270,31 +271,28 @@ def run_ours(a):
     # particle-turns actually tracked: particles lost inside the timed region count
     # only up to their loss turn; approximate with the mean of alive counts.
     pt_rank = 0.5 * (alive0 + alive1) * T * a.steps
-    if dist:
-        t = torch.tensor([ms, pt_rank], dtype=torch.float64, device=dev)
-        tmax = t.clone()
-        dist.all_reduce(tmax[0:1], op=dist.ReduceOp.MAX)
-        dist.all_reduce(t[1:2], op=dist.ReduceOp.SUM)
-        ms, pt_total = float(tmax[0]), float(t[1])
-    else:
-        pt_total = pt_rank
+    # device time: max over ranks; particle-turns: sum over ranks
+    ms = reduce_scalar(ms, "max")
+    pt_total = reduce_scalar(pt_rank, "sum")
     value = pt_total / (ms * 1e-3)
 
-    # e2e through the host-buffer C ABI (copies and host layout conversion inside the region)
-    e2e = None
-    if rank == 0:
-        xh = X.copy()
-        st = np.ones(n, dtype=np.int32)
-        tab.track_host(xh.copy(), 1, lat.aperture_radius)  # warm-up
-        reps = max(2, min(a.steps, 4))
-        t0 = time.perf_counter()
-        for _ in range(reps):
-            xr, st_o, ltn, lp = tab.track_host(xh, T, lat.aperture_radius, st.copy())
-        t1 = time.perf_counter()
-        e2e_pt = n * T * reps
-        e2e = {"value": e2e_pt / (t1 - t0), "unit": UNIT, "h2d_bytes_per_step": n * 6 * 8 + n * 4 * 2,
-               "d2h_bytes_per_step": n * 6 * 8 + n * 4 * 2,
-               "note": "stb_track_host: AoS host x[n*6] in, Track() outputs out, one call per step"}
+    # e2e through the host-buffer C ABI (copies and host layout conversion
+    # inside the region), on every rank; whole-job rate = all ranks'
+    # particle-turns over the slowest rank's time
+    xh = X.copy()
+    st = np.ones(n, dtype=np.int32)
+    tab.track_host(xh.copy(), 1, lat.aperture_radius)  # warm-up
+    reps = max(2, min(a.steps, 4))
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        xr, st_o, ltn, lp = tab.track_host(xh, T, lat.aperture_radius, st.copy())
+    e2e_s = reduce_scalar(time.perf_counter() - t0, "max")
+    e2e_pt = reduce_scalar(n * T * reps, "sum")
+    e2e = {"value": e2e_pt / e2e_s, "unit": UNIT, "h2d_bytes_per_step": world * (n * 6 * 8 + n * 4 * 2),
+           "d2h_bytes_per_step": world * (n * 6 * 8 + n * 4 * 2),
+           "note": "stb_track_host per rank: AoS host x[n*6] in, Track() outputs out, one call per step"}
 
     if rank == 0:
         kernel_ms = ms / a.steps
