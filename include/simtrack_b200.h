@@ -53,7 +53,7 @@ int stb_get_ref(double *out8);
 /* ---- elements: `new TYPE(name, args...)`  simtrack.h:399-1059 ----
  * type: "DRIFT","MARKER","SBEND","GSBEND","QUAD","SKEWQ","SEXT","OCT","MULT","GMULT",
  *       "SBENDMULT","KICKER","HKICKER","VKICKER","RFCAV","CRABRF","CCMULT","LBT","ILBT",
- *       "BEAMBEAM".
+ *       "BEAMBEAM","BPM","HBPM","VBPM".
  * args: the constructor arguments after `name`, in constructor order; MULT takes
  *       L, KNL[11], KNSL[11] (23 values); GMULT/SBENDMULT take L, ANGLE, E1, E2,
  *       KNL[11], KNSL[11] (26 values); BEAMBEAM takes TREATMENT, NP, BBSCALE, SIGMAL,
@@ -69,6 +69,10 @@ int stb_element_set_misalign(stb_element *e, double dx, double dy, double ds, do
                              double dpsi);
 /* public fields APx, APy  (simtrack.h:394; default 1 m, simtrack.cpp:8394-8395) */
 int stb_element_set_aperture(stb_element *e, double apx, double apy);
+/* writes NAME into buf (NUL-terminated, truncated to cap) */
+int stb_element_name(const stb_element *e, char *buf, int cap);
+/* out[0..9] = public fields L, S, DX, DY, DS, DTHETA, DPHI, DPSI, APx, APy (simtrack.h:384-394) */
+int stb_element_geometry(const stb_element *e, double *out10);
 /* writes TYPE into buf (NUL-terminated, truncated to cap) */
 int stb_element_type(const stb_element *e, char *buf, int cap);
 
@@ -84,6 +88,9 @@ int stb_line_invert(stb_line *l);                     /* Line::Invert */
 long stb_line_ncell(const stb_line *l);               /* Line::Ncell */
 double stb_line_length(const stb_line *l);            /* Line::Length */
 int stb_line_cell(stb_line *l, long i, stb_element **out); /* Line::Cell[i] (borrowed) */
+/* Read_MADX_Lattice(line, filename), simtrack.cpp:13591-13791: appends the
+ * elements of a MAD-X TFS twiss table (see include/simtrack_b200.hpp). */
+int stb_line_read_madx(stb_line *l, const char *path);
 
 /* ---- flattening: Line -> device element table ----
  * No reference counterpart: the reference dispatches Element::Pass virtually
@@ -149,6 +156,43 @@ int stb_track_host(stb_table *t, double *x, long n, int nturn, double aperture_r
 int stb_track_seeds_static(stb_table *const *tables, int nseed, const long *n_per_seed, double *x, double *px,
                            double *y, double *py, double *z, double *pt, int32_t *lost_turn, int32_t *lost_elem,
                            int turn0, int nturn, double aperture_radius, void *stream);
+
+/* ---- Track_Radial (simtrack.cpp:21641-21680) ----
+ * As stb_track_device / stb_track_host, with z corrected after every element
+ * j by the path-length change of the on-momentum reference particle through
+ * j (x04[j], from a particle started at zero with z and pt reset before each
+ * element, simtrack.cpp:21652-21657).  The first call on a table computes
+ * x04 on the device (allocation and a synchronisation); later calls reuse it. */
+int stb_track_radial_device(stb_table *t, double *x, double *px, double *y, double *py, double *z, double *pt,
+                            long n, int turn0, int nturn, double aperture_radius, int32_t *lost_turn,
+                            int32_t *lost_elem, void *stream);
+int stb_track_radial_host(stb_table *t, double *x, long n, int nturn, double aperture_radius, int *stable,
+                          int *lost_turn, int *lost_post);
+/* Per-element probe of Track_Radial (layout as stb_track_probe). */
+int stb_track_radial_probe(stb_table *t, double *x, long n, int nturn, double aperture_radius, double *dump,
+                           int *stable, int *lost_turn, int *lost_post);
+
+/* ---- spin tracking: Track_Spin (simtrack.cpp:21766-21789) ----
+ * A spin table is flattened with Element::sPass semantics: orbit slices
+ * interleaved with the Thomas-BMT rotation spin() (4574-4630) of
+ * SBEND/QUAD/SKEWQ/SEXT/OCT/MULT/SBENDMULT/KICKER (7486-8208); CRABRF acts as
+ * a drift and RF/CCMULT/LBT/ILBT/BEAMBEAM leave the spin unchanged, as the
+ * reference's sPass does.  GSBEND and GMULT are rejected (STB_EUNSUPPORTED).
+ * The spin G is the one set by stb_set_spin_g before the table is created.
+ * Spin tables work only with the stb_track_spin_* entry points. */
+int stb_table_create_spin(const stb_line *l, int device, stb_table **out);
+/* Device SoA form: orbit arrays as stb_track_device plus the spin unit
+ * vector (x[6], x[7], x[8] of the reference) in sx, sy, sz.  Asynchronous. */
+int stb_track_spin_device(stb_table *t, double *x, double *px, double *y, double *py, double *z, double *pt,
+                          double *sx, double *sy, double *sz, long n, int turn0, int nturn, double aperture_radius,
+                          int32_t *lost_turn, int32_t *lost_elem, void *stream);
+/* Host AoS x[n*9] form with Track_Spin()'s outputs.  Synchronous. */
+int stb_track_spin_host(stb_table *t, double *x9, long n, int nturn, double aperture_radius, int *stable,
+                        int *lost_turn, int *lost_post);
+/* As stb_track_spin_host, also writing the nine coordinates after every
+ * element to dump9[((i*nturn + turn)*ncell + j)*9 + k] (small n). */
+int stb_track_spin_probe(stb_table *t, double *x9, long n, int nturn, double aperture_radius, double *dump9,
+                         int *stable, int *lost_turn, int *lost_post);
 
 /* Per-element probe: as stb_track_host, and additionally writes the six
  * coordinates after every element to dump[((i*nturn + turn)*ncell + j)*6 + k]

@@ -85,6 +85,10 @@ class Element {
 
 class DRIFT : public Element { public: DRIFT(std::string name, double l); };
 class MARKER : public Element { public: MARKER(std::string name, double l); };
+// Beam position monitors (simtrack.cpp:10470-10600): drifts for tracking.
+class BPM : public Element { public: BPM(std::string name, double l); };
+class HBPM : public Element { public: HBPM(std::string name, double l); };
+class VBPM : public Element { public: VBPM(std::string name, double l); };
 class SBEND : public Element {
  public:
   SBEND(std::string name, double l, double angle, double e1, double e2);
@@ -238,6 +242,18 @@ void Track(Line &line, double x[], int nturn, int &stable, int &lost_turn, int &
 // DA drivers, simtrack.cpp:21389-21441, moved onto the GPU in one launch).
 void Track_Batch(Line &line, double *x, long n, int nturn, int *stable, int *lost_turn,
                  int *lost_post, const TrackOptions &opt = TrackOptions());
+
+// Read_MADX_Lattice (simtrack.cpp:13591-13791): appends the elements of a
+// MAD-X TFS twiss table (columns NAME KEYWORD S L ANGLE E1 E2 TILT K0L K0SL
+// ... K10L K10SL KS) to `line`, mapping keywords to element types as the
+// reference does.  Throws Error(STB_EUNSUPPORTED) for a solenoid with KS != 0
+// or an electron lens (not implemented on the GPU path) and
+// Error(STB_EINVAL) for an unreadable file.
+void Read_MADX_Lattice(Line &line, const char *filename);
+
+// Track_Radial() drop-in (simtrack.cpp:21641-21680): Track() with z taken
+// relative to the on-momentum reference particle after every element.
+void Track_Radial(Line &line, double x[], int nturn, int &stable, int &lost_turn, int &lost_post);
 
 // Track_Spin() drop-in (simtrack.cpp:21766-21789): x[9] = orbit + spin.
 void Track_Spin(Line &line, double x[], int nturn, int &stable, int &lost_turn, int &lost_post);

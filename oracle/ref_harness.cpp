@@ -7,6 +7,9 @@
 // entry points:
 //   ref_track       -> Track()       simtrack.cpp:20791-20814 (called as is)
 //   ref_track_spin  -> Track_Spin()  simtrack.cpp:21766-21789 (called as is)
+//   ref_track_radial -> Track_Radial()  simtrack.cpp:21641-21680 (called as is)
+//   ref_track_spin_dump -> the Track_Spin() loop recording x[9] after every
+//                      element.
 //   ref_track_circ  -> the Track() loop with one extra loss predicate, a
 //                      circular aperture x^2+y^2 > R^2, evaluated after the
 //                      reference's own rectangular/NaN check.
@@ -16,6 +19,7 @@
 // Nothing in the product links or loads this file.
 #include "simtrack.h"
 
+#include <cstdio>
 #include <cstring>
 #include <vector>
 #include <cmath>
@@ -34,6 +38,9 @@ Element *make_element(const char *type, const char *name, const double *p, int n
   auto need = [&](int k) { return np >= k; };
   if (t == "DRIFT" && need(1)) return new DRIFT(nm, p[0]);
   if (t == "MARKER" && need(1)) return new MARKER(nm, p[0]);
+  if (t == "BPM" && need(1)) return new BPM(nm, p[0]);
+  if (t == "HBPM" && need(1)) return new HBPM(nm, p[0]);
+  if (t == "VBPM" && need(1)) return new VBPM(nm, p[0]);
   if (t == "SBEND" && need(4)) return new SBEND(nm, p[0], p[1], p[2], p[3]);
   if (t == "GSBEND" && need(5)) return new GSBEND(nm, p[0], p[1], p[2], p[3], p[4]);
   if (t == "QUAD" && need(3)) return new QUAD(nm, p[0], p[1], p[2]);
@@ -133,6 +140,23 @@ void ref_line_set_aperture(void *line, long idx, double apx, double apy) {
 
 void ref_pass(void *line, long idx, double *x) { static_cast<Line *>(line)->Cell[idx]->Pass(x); }
 
+// Read_MADX_Lattice (simtrack.cpp:13591) into a new Line.  The reference
+// exits the process on a missing file: callers check the path first.
+void *ref_line_read_madx(const char *path) {
+  Line *l = new Line();
+  Read_MADX_Lattice(*l, path);
+  return l;
+}
+
+// TYPE, NAME and the public geometry fields of element idx.
+void ref_line_elem(void *line, long idx, char *type, char *name, int cap, double *geom10) {
+  Element *e = static_cast<Line *>(line)->Cell[idx];
+  std::snprintf(type, (size_t)cap, "%s", e->TYPE.c_str());
+  std::snprintf(name, (size_t)cap, "%s", e->NAME.c_str());
+  const double v[10] = {e->L, e->S, e->DX, e->DY, e->DS, e->DTHETA, e->DPHI, e->DPSI, e->APx, e->APy};
+  for (int k = 0; k < 10; k++) geom10[k] = v[k];
+}
+
 // n particles, AoS x[n*6], through the reference Track(); stable[] is read as
 // the caller's input flag (Track's own convention) and overwritten.
 void ref_track(void *line, double *x, long n, int nturn, int *stable, int *lost_turn, int *lost_post) {
@@ -144,6 +168,16 @@ void ref_track(void *line, double *x, long n, int nturn, int *stable, int *lost_
   }
 }
 
+// n particles through the reference Track_Radial() (simtrack.cpp:21641-21680).
+void ref_track_radial(void *line, double *x, long n, int nturn, int *stable, int *lost_turn, int *lost_post) {
+  Line &l = *static_cast<Line *>(line);
+  for (long i = 0; i < n; i++) {
+    int st = stable[i], lt = 0, lp = 0;
+    Track_Radial(l, x + 6 * i, nturn, st, lt, lp);
+    stable[i] = st; lost_turn[i] = lt; lost_post[i] = lp;
+  }
+}
+
 void ref_track_spin(void *line, double *x9, long n, int nturn, int *stable, int *lost_turn,
                     int *lost_post) {
   Line &l = *static_cast<Line *>(line);
@@ -151,6 +185,27 @@ void ref_track_spin(void *line, double *x9, long n, int nturn, int *stable, int 
     int st = stable[i], lt = 0, lp = 0;
     Track_Spin(l, x9 + 9 * i, nturn, st, lt, lp);
     stable[i] = st; lost_turn[i] = lt; lost_post[i] = lp;
+  }
+}
+
+// One particle through the Track_Spin() loop (simtrack.cpp:21766-21789) with
+// dump[(turn*ncell + j)*9 + k] = x[k] after element j of turn (the
+// per-element probe of the spin path; entries after a loss are untouched).
+void ref_track_spin_dump(void *line, double *x9, int nturn, double *dump, int *stable, int *lost_turn,
+                         int *lost_post) {
+  Line &l = *static_cast<Line *>(line);
+  *stable = 1; *lost_turn = 0; *lost_post = 0;
+  if (std::abs(x9[0]) > 0.1 || std::abs(x9[2]) > 0.1) { *stable = 0; return; }
+  for (GP.turn = 0; GP.turn < nturn; GP.turn++) {
+    for (long j = 0; j < l.Ncell; j++) {
+      l.Cell[j]->sPass(x9);
+      std::memcpy(dump + ((long)GP.turn * l.Ncell + j) * 9, x9, 9 * sizeof(double));
+      if (std::abs(x9[0]) > l.Cell[j]->APx || std::abs(x9[2]) > l.Cell[j]->APy || std::isnan(x9[0]) ||
+          std::isnan(x9[2])) {
+        *stable = 0; *lost_turn = GP.turn; *lost_post = (int)j;
+        return;
+      }
+    }
   }
 }
 

@@ -76,6 +76,22 @@ SIGNATURES = [
     ("stb_scan_stats", c_int, [c_void_p, POINTER(c_double)]),
     ("stb_scan_autotune", c_int, [c_void_p, c_int, POINTER(c_int), POINTER(c_double), c_int]),
     ("stb_scan_set_tbt", c_int, [c_void_p, c_void_p, c_int]),
+    ("stb_table_create_spin", c_int, [c_void_p, c_int, POINTER(c_void_p)]),
+    ("stb_element_name", c_int, [c_void_p, c_char_p, c_int]),
+    ("stb_element_geometry", c_int, [c_void_p, POINTER(c_double)]),
+    ("stb_line_read_madx", c_int, [c_void_p, c_char_p]),
+    ("stb_track_radial_device", c_int, [c_void_p] + [c_void_p] * 6 + [c_long, c_int, c_int, c_double, c_void_p,
+                                                                       c_void_p, c_void_p]),
+    ("stb_track_radial_host", c_int, [c_void_p, POINTER(c_double), c_long, c_int, c_double, POINTER(c_int),
+                                      POINTER(c_int), POINTER(c_int)]),
+    ("stb_track_radial_probe", c_int, [c_void_p, POINTER(c_double), c_long, c_int, c_double, POINTER(c_double),
+                                       POINTER(c_int), POINTER(c_int), POINTER(c_int)]),
+    ("stb_track_spin_device", c_int, [c_void_p] + [c_void_p] * 9 + [c_long, c_int, c_int, c_double, c_void_p,
+                                                                     c_void_p, c_void_p]),
+    ("stb_track_spin_host", c_int, [c_void_p, POINTER(c_double), c_long, c_int, c_double, POINTER(c_int),
+                                    POINTER(c_int), POINTER(c_int)]),
+    ("stb_track_spin_probe", c_int, [c_void_p, POINTER(c_double), c_long, c_int, c_double, POINTER(c_double),
+                                     POINTER(c_int), POINTER(c_int), POINTER(c_int)]),
     ("stb_fine_tune", c_int, [c_void_p, c_void_p, c_int, c_long, c_long, c_double, c_double, c_void_p, c_int,
                               c_void_p]),
     ("stb_tbt_features", c_int, [c_void_p, c_long, c_int, c_void_p, c_void_p, POINTER(c_double), c_void_p, c_int,

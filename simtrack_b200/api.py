@@ -56,14 +56,12 @@ class Element:
         check(lib().stb_element_new(type_.encode(), name.encode(), arr, len(args), byref(h)))
         self._h = h
         self._owned = True
-        self.NAME = name
 
     @classmethod
     def _borrow(cls, handle: c_void_p) -> "Element":
         e = cls.__new__(cls)
         e._h = handle
         e._owned = False
-        e.NAME = ""
         return e
 
     @property
@@ -79,6 +77,19 @@ class Element:
         v = c_double()
         check(lib().stb_element_getp(self._h, name.encode(), byref(v)))
         return v.value
+
+    @property
+    def NAME(self) -> str:
+        buf = ctypes.create_string_buffer(256)
+        check(lib().stb_element_name(self._h, buf, 256))
+        return buf.value.decode()
+
+    def geometry(self) -> dict:
+        """Public fields L, S, DX, DY, DS, DTHETA, DPHI, DPSI, APx, APy."""
+        out = (c_double * 10)()
+        check(lib().stb_element_geometry(self._h, out))
+        keys = ("L", "S", "DX", "DY", "DS", "DTHETA", "DPHI", "DPSI", "APx", "APy")
+        return {k: out[i] for i, k in enumerate(keys)}
 
     def set_misalignment(self, dx=0., dy=0., ds=0., dtheta=0., dphi=0., dpsi=0.) -> None:
         """Element::DX/DY/DS/DTHETA/DPHI/DPSI (simtrack.h:388-389)."""
@@ -185,6 +196,10 @@ class Line:
     def Length(self) -> float:
         return float(lib().stb_line_length(self._h))
 
+    def read_madx(self, path: str) -> None:
+        """Read_MADX_Lattice (simtrack.cpp:13591-13791): appends the elements of a MAD-X TFS table."""
+        check(lib().stb_line_read_madx(self._h, str(path).encode()))
+
     def Cell(self, i: int) -> Element:
         h = c_void_p()
         check(lib().stb_line_cell(self._h, i, byref(h)))
@@ -255,6 +270,26 @@ class Table:
                                    lp.ctypes.data_as(POINTER(c_int))))
         return x, st, lt, lp
 
+    def track_radial_host(self, x: np.ndarray, nturn: int, aperture_radius: float = 0.0, stable=None):
+        """Track_Radial (simtrack.cpp:21641-21680) over AoS host x[n, 6] (updated in place)."""
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        n = x.shape[0]
+        st = np.ones(n, dtype=np.int32) if stable is None else np.ascontiguousarray(stable, dtype=np.int32)
+        lt = np.zeros(n, dtype=np.int32)
+        lp = np.zeros(n, dtype=np.int32)
+        check(lib().stb_track_radial_host(self._h, x.ctypes.data_as(POINTER(c_double)), n, nturn, aperture_radius,
+                                          st.ctypes.data_as(POINTER(c_int)), lt.ctypes.data_as(POINTER(c_int)),
+                                          lp.ctypes.data_as(POINTER(c_int))))
+        return x, st, lt, lp
+
+    def track_radial_device(self, coords, lost_turn, lost_elem, turn0: int, nturn: int,
+                            aperture_radius: float = 0.0, stream=None) -> None:
+        n = coords[0].numel()
+        s = None if stream is None else c_void_p(stream)
+        check(lib().stb_track_radial_device(self._h, *[c_void_p(c.data_ptr()) for c in coords], n, turn0, nturn,
+                                            aperture_radius, c_void_p(lost_turn.data_ptr()),
+                                            c_void_p(lost_elem.data_ptr()), s))
+
     def track_probe(self, x: np.ndarray, nturn: int, aperture_radius: float = 0.0):
         """Per-element probe: returns (x, stable, lost_turn, lost_post, dump[n, nturn, ncell, 6])."""
         x = np.ascontiguousarray(x, dtype=np.float64)
@@ -284,6 +319,85 @@ class Table:
                 lib().stb_table_free(self._h)
         except Exception:
             pass
+
+
+class SpinTable:
+    """Element table flattened for spin tracking (Track_Spin, Element::sPass)."""
+
+    def __init__(self, line: Line, device: int = 0):
+        h = c_void_p()
+        check(lib().stb_table_create_spin(line._h, device, byref(h)))
+        self._h = h
+        self.device = device
+
+    def info(self) -> dict:
+        out = (c_double * 6)()
+        check(lib().stb_table_info(self._h, out))
+        return {"elements": int(out[0]), "pool_doubles": int(out[1]), "flops_per_turn": out[2]}
+
+    def track_host(self, x: np.ndarray, nturn: int, aperture_radius: float = 0.0, stable=None):
+        """Track_Spin over AoS host x[n, 9] (updated in place); returns (x, stable, lost_turn, lost_post)."""
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        if x.ndim != 2 or x.shape[1] != 9:
+            raise SimTrackError(-1, "x must have shape (n, 9)")
+        n = x.shape[0]
+        st = np.ones(n, dtype=np.int32) if stable is None else np.ascontiguousarray(stable, dtype=np.int32)
+        lt = np.zeros(n, dtype=np.int32)
+        lp = np.zeros(n, dtype=np.int32)
+        check(lib().stb_track_spin_host(self._h, x.ctypes.data_as(POINTER(c_double)), n, nturn, aperture_radius,
+                                        st.ctypes.data_as(POINTER(c_int)), lt.ctypes.data_as(POINTER(c_int)),
+                                        lp.ctypes.data_as(POINTER(c_int))))
+        return x, st, lt, lp
+
+    def track_probe(self, x: np.ndarray, nturn: int, aperture_radius: float = 0.0):
+        """Per-element probe: returns (x, stable, lost_turn, lost_post, dump[n, nturn, ncell, 9])."""
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        n = x.shape[0]
+        ne = self.info()["elements"]
+        dump = np.full((n, nturn, ne, 9), np.nan)
+        st = np.ones(n, dtype=np.int32)
+        lt = np.zeros(n, dtype=np.int32)
+        lp = np.zeros(n, dtype=np.int32)
+        check(lib().stb_track_spin_probe(self._h, x.ctypes.data_as(POINTER(c_double)), n, nturn, aperture_radius,
+                                         dump.ctypes.data_as(POINTER(c_double)), st.ctypes.data_as(POINTER(c_int)),
+                                         lt.ctypes.data_as(POINTER(c_int)), lp.ctypes.data_as(POINTER(c_int))))
+        return x, st, lt, lp, dump
+
+    def track_device(self, coords, lost_turn, lost_elem, turn0: int, nturn: int, aperture_radius: float = 0.0,
+                     stream=None) -> None:
+        """coords: 9 CUDA float64 tensors (x, px, y, py, z, pt, sx, sy, sz), updated in place."""
+        n = coords[0].numel()
+        s = None if stream is None else c_void_p(stream)
+        check(lib().stb_track_spin_device(self._h, *[c_void_p(c.data_ptr()) for c in coords], n, turn0, nturn,
+                                          aperture_radius, c_void_p(lost_turn.data_ptr()),
+                                          c_void_p(lost_elem.data_ptr()), s))
+
+    def __del__(self):
+        try:
+            if self._h:
+                lib().stb_table_free(self._h)
+        except Exception:
+            pass
+
+
+def Track_Radial(line: Line, x, nturn: int, stable: int = 1):
+    """Track_Radial (simtrack.cpp:21641-21680) for one particle x[6] (updated in place).
+
+    Returns (stable, lost_turn, lost_post)."""
+    arr = np.asarray(x, dtype=np.float64).reshape(1, 6).copy()
+    _, st, lt, lp = Table(line).track_radial_host(arr, nturn, 0.0, np.array([stable], dtype=np.int32))
+    x[:] = arr[0]
+    return int(st[0]), int(lt[0]), int(lp[0])
+
+
+def Track_Spin(line: Line, x, nturn: int, stable: int = 1):
+    """Track_Spin (simtrack.cpp:21766-21789) for one particle x[9] (updated in place).
+
+    Returns (stable, lost_turn, lost_post)."""
+    arr = np.asarray(x, dtype=np.float64).reshape(1, 9).copy()
+    _, st, lt, lp = SpinTable(line).track_host(arr, nturn, 0.0, np.array([stable], dtype=np.int32))
+    x[:] = arr[0]
+    return int(st[0]), int(lt[0]), int(lp[0])
 
 
 def Track_Batch(line: Line, x: np.ndarray, nturn: int, aperture_radius: float = 0.0, stable=None, device: int = 0):

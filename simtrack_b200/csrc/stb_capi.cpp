@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -37,6 +38,9 @@ Element *make_element(const char *type, const char *name, const double *a, int n
   };
   if (t == "DRIFT") { need(1); return new DRIFT(nm, a[0]); }
   if (t == "MARKER") { need(1); return new MARKER(nm, a[0]); }
+  if (t == "BPM") { need(1); return new BPM(nm, a[0]); }
+  if (t == "HBPM") { need(1); return new HBPM(nm, a[0]); }
+  if (t == "VBPM") { need(1); return new VBPM(nm, a[0]); }
   if (t == "SBEND") { need(4); return new SBEND(nm, a[0], a[1], a[2], a[3]); }
   if (t == "GSBEND") { need(5); return new GSBEND(nm, a[0], a[1], a[2], a[3], a[4]); }
   if (t == "QUAD") { need(3); return new QUAD(nm, a[0], a[1], a[2]); }
@@ -79,14 +83,15 @@ void table_destroy(stb_table *t) {
   if (t->d_hdr) cudaFree(t->d_hdr);
   if (t->d_pool) cudaFree(t->d_pool);
   if (t->d_status) cudaFree(t->d_status);
+  if (t->d_zsub) cudaFree(t->d_zsub);
   if (prev >= 0) cudaSetDevice(prev);
   delete t;
 }
 
-stb_table *table_build(const Line &line, int device) {
+stb_table *table_build(const Line &line, int device, bool spin = false) {
   std::unique_ptr<stb_table, void (*)(stb_table *)> t(new stb_table(), table_destroy);
   t->device = device;
-  t->host = flatten(line);
+  t->host = spin ? flatten_spin(line) : flatten(line);
   if (t->host.hdr.empty()) throw Error(STB_EINVAL, "line has no elements");
   DeviceGuard g(device);
   std::vector<double> pool = t->host.pool;
@@ -122,6 +127,7 @@ int track_device(stb_table *t, double *x, double *px, double *y, double *py, dou
                  int turn0, int nturn, double radius, int32_t *lost_turn, int32_t *lost_elem, cudaStream_t s,
                  double *dump = nullptr) {
   if (!t) throw Error(STB_EINVAL, "table is NULL");
+  if (t->host.spin) throw Error(STB_EINVAL, "table is flattened for spin tracking (use stb_track_spin_*)");
   if (n < 0 || nturn < 0 || turn0 < 0) throw Error(STB_EINVAL, "negative particle count or turn");
   if (n == 0 || nturn == 0) return STB_OK;
   if (!x || !px || !y || !py || !z || !pt || !lost_turn || !lost_elem)
@@ -145,6 +151,7 @@ int track_device(stb_table *t, double *x, double *px, double *y, double *py, dou
 int autotune(stb_table *t, const double *const in[6], long n, int nturn, double radius, int *chosen,
              double *timings, int ntimings) {
   if (!t) throw Error(STB_EINVAL, "table is NULL");
+  if (t->host.spin) throw Error(STB_EINVAL, "table is flattened for spin tracking");
   for (int k = 0; k < 6; k++)
     if (!in[k]) throw Error(STB_EINVAL, "NULL coordinate array");
   if (n <= 0 || nturn <= 0) throw Error(STB_EINVAL, "autotune needs particles and turns");
@@ -262,6 +269,175 @@ int track_host(stb_table *t, double *xa, long n, int nturn, double radius, int *
   return STB_OK;
 }
 
+// Track_Radial on device SoA arrays, asynchronous after the first call on a
+// table (which computes the reference particle's per-element z).
+int radial_device(stb_table *t, double *x, double *px, double *y, double *py, double *z, double *pt, long n,
+                  int turn0, int nturn, double radius, int32_t *lost_turn, int32_t *lost_elem, cudaStream_t s,
+                  double *dump = nullptr) {
+  if (!t) throw Error(STB_EINVAL, "table is NULL");
+  if (t->host.spin) throw Error(STB_EINVAL, "table is flattened for spin tracking");
+  if (n < 0 || nturn < 0 || turn0 < 0) throw Error(STB_EINVAL, "negative particle count or turn");
+  if (n == 0 || nturn == 0) return STB_OK;
+  if (!x || !px || !y || !py || !z || !pt || !lost_turn || !lost_elem)
+    throw Error(STB_EINVAL, "coordinate or loss array is NULL");
+  DeviceGuard g(t->device);
+  TrackArgs a = make_args(t);
+  if (!t->d_zsub) {
+    double *zs = nullptr;
+    cuda_check(cudaMalloc(&zs, sizeof(double) * t->host.hdr.size()), "cudaMalloc(radial reference)");
+    cudaError_t e = launch_radial_reference(a, zs, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+      cudaFree(zs);
+      cuda_check(e, "radial reference pass");
+    }
+    t->d_zsub = zs;
+  }
+  a.x = x; a.px = px; a.y = y; a.py = py; a.z = z; a.pt = pt;
+  a.n = n;
+  a.turn0 = turn0;
+  a.nturn = nturn;
+  a.r2 = radius > 0.0 ? radius * radius : 0.0;
+  a.lost_turn = lost_turn;
+  a.lost_elem = lost_elem;
+  a.dump = dump;
+  cuda_check(launch_radial(a, t->d_zsub, t->num_sms, t->use_smem, s), "radial kernel launch");
+  return STB_OK;
+}
+
+int radial_host(stb_table *t, double *xa, long n, int nturn, double radius, int *stable, int *lost_turn,
+                int *lost_post, double *dump_host = nullptr) {
+  if (!t) throw Error(STB_EINVAL, "table is NULL");
+  if (n < 0 || nturn < 0) throw Error(STB_EINVAL, "negative particle count or turn count");
+  if (n == 0) return STB_OK;
+  if (!xa || !stable || !lost_turn || !lost_post) throw Error(STB_EINVAL, "NULL host buffer");
+  DeviceGuard g(t->device);
+  std::vector<double> soa((size_t)n * 6);
+  std::vector<int32_t> lt((size_t)n), le((size_t)n, 0);
+  for (long i = 0; i < n; i++) {
+    for (int k = 0; k < 6; k++) soa[(size_t)k * n + i] = xa[6 * i + k];
+    lt[i] = stable[i] == 0 ? 0 : -1;
+  }
+  double *d = nullptr;
+  int32_t *dl = nullptr;
+  cuda_check(cudaMalloc(&d, sizeof(double) * 6 * n), "cudaMalloc(coordinates)");
+  DevFree f1{d};
+  cuda_check(cudaMalloc(&dl, sizeof(int32_t) * 2 * n), "cudaMalloc(loss arrays)");
+  DevFree f2{dl};
+  cuda_check(cudaMemcpy(d, soa.data(), sizeof(double) * 6 * n, cudaMemcpyHostToDevice), "upload coordinates");
+  cuda_check(cudaMemcpy(dl, lt.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice), "upload loss state");
+  cuda_check(cudaMemcpy(dl + n, le.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice), "upload loss state");
+  cuda_check(cudaMemset(t->d_status, 0, sizeof(int)), "clear status");
+  double *dd = nullptr;
+  const size_t dump_n = dump_host ? (size_t)n * nturn * t->host.hdr.size() * 6 : 0;
+  if (dump_host) {
+    cuda_check(cudaMalloc(&dd, sizeof(double) * dump_n), "cudaMalloc(probe)");
+    cuda_check(cudaMemcpy(dd, dump_host, sizeof(double) * dump_n, cudaMemcpyHostToDevice), "upload probe");
+  }
+  DevFree f3{dd};
+  if (nturn > 0)
+    radial_device(t, d, d + n, d + 2 * n, d + 3 * n, d + 4 * n, d + 5 * n, n, 0, nturn, radius, dl, dl + n, 0, dd);
+  cuda_check(cudaDeviceSynchronize(), "radial kernel");
+  if (dump_host)
+    cuda_check(cudaMemcpy(dump_host, dd, sizeof(double) * dump_n, cudaMemcpyDeviceToHost), "download probe");
+  int st = 0;
+  cuda_check(cudaMemcpy(&st, t->d_status, sizeof(int), cudaMemcpyDeviceToHost), "read status");
+  if (st != 0) throw Error(st, "radial kernel reported status " + std::to_string(st));
+  cuda_check(cudaMemcpy(soa.data(), d, sizeof(double) * 6 * n, cudaMemcpyDeviceToHost), "download coordinates");
+  cuda_check(cudaMemcpy(lt.data(), dl, sizeof(int32_t) * n, cudaMemcpyDeviceToHost), "download loss state");
+  cuda_check(cudaMemcpy(le.data(), dl + n, sizeof(int32_t) * n, cudaMemcpyDeviceToHost), "download loss state");
+  for (long i = 0; i < n; i++) {
+    for (int k = 0; k < 6; k++) xa[6 * i + k] = soa[(size_t)k * n + i];
+    if (lt[i] < 0) {
+      stable[i] = 1; lost_turn[i] = 0; lost_post[i] = 0;
+    } else {
+      stable[i] = 0; lost_turn[i] = lt[i]; lost_post[i] = le[i];
+    }
+  }
+  return STB_OK;
+}
+
+// Track_Spin on device SoA arrays (orbit + spin unit vector), asynchronous.
+int spin_device(stb_table *t, double *const xs[9], long n, int turn0, int nturn, double radius, int32_t *lost_turn,
+                int32_t *lost_elem, cudaStream_t s, double *dump = nullptr) {
+  if (!t) throw Error(STB_EINVAL, "table is NULL");
+  if (!t->host.spin) throw Error(STB_EINVAL, "table is not flattened for spin tracking (use stb_table_create_spin)");
+  if (n < 0 || nturn < 0 || turn0 < 0) throw Error(STB_EINVAL, "negative particle count or turn");
+  if (n == 0 || nturn == 0) return STB_OK;
+  for (int k = 0; k < 9; k++)
+    if (!xs[k]) throw Error(STB_EINVAL, "coordinate or spin array is NULL");
+  if (!lost_turn || !lost_elem) throw Error(STB_EINVAL, "loss array is NULL");
+  DeviceGuard g(t->device);
+  SpinArgs a{};
+  a.t = make_args(t);
+  a.t.x = xs[0]; a.t.px = xs[1]; a.t.y = xs[2]; a.t.py = xs[3]; a.t.z = xs[4]; a.t.pt = xs[5];
+  a.sx = xs[6]; a.sy = xs[7]; a.sz = xs[8];
+  a.t.n = n;
+  a.t.turn0 = turn0;
+  a.t.nturn = nturn;
+  a.t.r2 = radius > 0.0 ? radius * radius : 0.0;
+  a.t.lost_turn = lost_turn;
+  a.t.lost_elem = lost_elem;
+  a.dump = dump;
+  cuda_check(launch_spin(a, t->num_sms, t->use_smem, s), "spin kernel launch");
+  return STB_OK;
+}
+
+// Host AoS x[n*9] -> device SoA, Track_Spin, back; optional per-element probe.
+int spin_host(stb_table *t, double *xa, long n, int nturn, double radius, int *stable, int *lost_turn,
+              int *lost_post, double *dump_host = nullptr) {
+  if (!t) throw Error(STB_EINVAL, "table is NULL");
+  if (n < 0 || nturn < 0) throw Error(STB_EINVAL, "negative particle count or turn count");
+  if (n == 0) return STB_OK;
+  if (!xa || !stable || !lost_turn || !lost_post) throw Error(STB_EINVAL, "NULL host buffer");
+  if (!t->host.spin) throw Error(STB_EINVAL, "table is not flattened for spin tracking (use stb_table_create_spin)");
+  DeviceGuard g(t->device);
+  std::vector<double> soa((size_t)n * 9);
+  std::vector<int32_t> lt((size_t)n), le((size_t)n, 0);
+  for (long i = 0; i < n; i++) {
+    for (int k = 0; k < 9; k++) soa[(size_t)k * n + i] = xa[9 * i + k];
+    lt[i] = stable[i] == 0 ? 0 : -1;  // Track_Spin(): stable == 0 on entry -> lost at turn 0, post 0
+  }
+  double *d = nullptr;
+  int32_t *dl = nullptr;
+  cuda_check(cudaMalloc(&d, sizeof(double) * 9 * n), "cudaMalloc(coordinates)");
+  DevFree f1{d};
+  cuda_check(cudaMalloc(&dl, sizeof(int32_t) * 2 * n), "cudaMalloc(loss arrays)");
+  DevFree f2{dl};
+  cuda_check(cudaMemcpy(d, soa.data(), sizeof(double) * 9 * n, cudaMemcpyHostToDevice), "upload coordinates");
+  cuda_check(cudaMemcpy(dl, lt.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice), "upload loss state");
+  cuda_check(cudaMemcpy(dl + n, le.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice), "upload loss state");
+  cuda_check(cudaMemset(t->d_status, 0, sizeof(int)), "clear status");
+  double *dd = nullptr;
+  const size_t dump_n = dump_host ? (size_t)n * nturn * t->host.hdr.size() * 9 : 0;
+  if (dump_host) {
+    cuda_check(cudaMalloc(&dd, sizeof(double) * dump_n), "cudaMalloc(probe)");
+    cuda_check(cudaMemcpy(dd, dump_host, sizeof(double) * dump_n, cudaMemcpyHostToDevice), "upload probe");
+  }
+  DevFree f3{dd};
+  double *xs[9];
+  for (int k = 0; k < 9; k++) xs[k] = d + (size_t)k * n;
+  if (nturn > 0) spin_device(t, xs, n, 0, nturn, radius, dl, dl + n, 0, dd);
+  cuda_check(cudaDeviceSynchronize(), "spin kernel");
+  if (dump_host)
+    cuda_check(cudaMemcpy(dump_host, dd, sizeof(double) * dump_n, cudaMemcpyDeviceToHost), "download probe");
+  int st = 0;
+  cuda_check(cudaMemcpy(&st, t->d_status, sizeof(int), cudaMemcpyDeviceToHost), "read status");
+  if (st != 0) throw Error(st, "spin kernel reported status " + std::to_string(st));
+  cuda_check(cudaMemcpy(soa.data(), d, sizeof(double) * 9 * n, cudaMemcpyDeviceToHost), "download coordinates");
+  cuda_check(cudaMemcpy(lt.data(), dl, sizeof(int32_t) * n, cudaMemcpyDeviceToHost), "download loss state");
+  cuda_check(cudaMemcpy(le.data(), dl + n, sizeof(int32_t) * n, cudaMemcpyDeviceToHost), "download loss state");
+  for (long i = 0; i < n; i++) {
+    for (int k = 0; k < 9; k++) xa[9 * i + k] = soa[(size_t)k * n + i];
+    if (lt[i] < 0) {
+      stable[i] = 1; lost_turn[i] = 0; lost_post[i] = 0;
+    } else {
+      stable[i] = 0; lost_turn[i] = lt[i]; lost_post[i] = le[i];
+    }
+  }
+  return STB_OK;
+}
+
 }  // namespace
 
 // ---- C++ Track entry points ----
@@ -276,9 +452,16 @@ void Track(Line &line, double x[], int nturn, int &stable, int &lost_turn, int &
   Track_Batch(line, x, 1, nturn, &stable, &lost_turn, &lost_post);
 }
 
+void Track_Radial(Line &line, double x[], int nturn, int &stable, int &lost_turn, int &lost_post) {
+  std::unique_ptr<stb_table, void (*)(stb_table *)> t(table_build(line, 0), table_destroy);
+  int rc = radial_host(t.get(), x, 1, nturn, 0.0, &stable, &lost_turn, &lost_post);
+  if (rc != STB_OK) throw Error(rc, last_error());
+}
+
 void Track_Spin(Line &line, double x[], int nturn, int &stable, int &lost_turn, int &lost_post) {
-  (void)line; (void)x; (void)nturn; (void)stable; (void)lost_turn; (void)lost_post;
-  throw Error(STB_EUNSUPPORTED, "spin tracking is not available in this build");
+  std::unique_ptr<stb_table, void (*)(stb_table *)> t(table_build(line, 0, true), table_destroy);
+  int rc = spin_host(t.get(), x, 1, nturn, 0.0, &stable, &lost_turn, &lost_post);
+  if (rc != STB_OK) throw Error(rc, last_error());
 }
 
 }  // namespace stb
@@ -354,6 +537,29 @@ int stb_element_set_aperture(stb_element *e, double apx, double apy) {
     if (!e) throw Error(STB_EINVAL, "NULL element");
     E(e)->APx = apx;
     E(e)->APy = apy;
+    return STB_OK;
+  });
+}
+int stb_element_name(const stb_element *e, char *buf, int cap) {
+  return guarded([&] {
+    if (!e || !buf || cap <= 0) throw Error(STB_EINVAL, "NULL argument");
+    std::snprintf(buf, (size_t)cap, "%s", E(e)->NAME.c_str());
+    return STB_OK;
+  });
+}
+int stb_element_geometry(const stb_element *e, double *out10) {
+  return guarded([&] {
+    if (!e || !out10) throw Error(STB_EINVAL, "NULL argument");
+    const Element *x = E(e);
+    const double v[10] = {x->L, x->S, x->DX, x->DY, x->DS, x->DTHETA, x->DPHI, x->DPSI, x->APx, x->APy};
+    for (int k = 0; k < 10; k++) out10[k] = v[k];
+    return STB_OK;
+  });
+}
+int stb_line_read_madx(stb_line *l, const char *path) {
+  return guarded([&] {
+    if (!l || !path) throw Error(STB_EINVAL, "NULL argument");
+    Read_MADX_Lattice(*Lp(l), path);
     return STB_OK;
   });
 }
@@ -433,6 +639,13 @@ int stb_table_create(const stb_line *l, int device, stb_table **out) {
   return guarded([&] {
     if (!l || !out) throw Error(STB_EINVAL, "NULL argument");
     *out = table_build(*Lp(l), device);
+    return STB_OK;
+  });
+}
+int stb_table_create_spin(const stb_line *l, int device, stb_table **out) {
+  return guarded([&] {
+    if (!l || !out) throw Error(STB_EINVAL, "NULL argument");
+    *out = table_build(*Lp(l), device, true);
     return STB_OK;
   });
 }
@@ -537,6 +750,50 @@ int stb_track_probe(stb_table *t, double *x, long n, int nturn, double aperture_
   return guarded([&] {
     if (!dump) throw Error(STB_EINVAL, "NULL probe buffer");
     return track_host(t, x, n, nturn, aperture_radius, stable, lost_turn, lost_post, dump);
+  });
+}
+
+int stb_track_radial_device(stb_table *t, double *x, double *px, double *y, double *py, double *z, double *pt,
+                            long n, int turn0, int nturn, double aperture_radius, int32_t *lost_turn,
+                            int32_t *lost_elem, void *stream) {
+  return guarded([&] {
+    return radial_device(t, x, px, y, py, z, pt, n, turn0, nturn, aperture_radius, lost_turn, lost_elem,
+                         (cudaStream_t)stream);
+  });
+}
+
+int stb_track_radial_host(stb_table *t, double *x, long n, int nturn, double aperture_radius, int *stable,
+                          int *lost_turn, int *lost_post) {
+  return guarded([&] { return radial_host(t, x, n, nturn, aperture_radius, stable, lost_turn, lost_post); });
+}
+
+int stb_track_radial_probe(stb_table *t, double *x, long n, int nturn, double aperture_radius, double *dump,
+                           int *stable, int *lost_turn, int *lost_post) {
+  return guarded([&] {
+    if (!dump) throw Error(STB_EINVAL, "NULL probe buffer");
+    return radial_host(t, x, n, nturn, aperture_radius, stable, lost_turn, lost_post, dump);
+  });
+}
+
+int stb_track_spin_device(stb_table *t, double *x, double *px, double *y, double *py, double *z, double *pt,
+                          double *sx, double *sy, double *sz, long n, int turn0, int nturn, double aperture_radius,
+                          int32_t *lost_turn, int32_t *lost_elem, void *stream) {
+  return guarded([&] {
+    double *xs[9] = {x, px, y, py, z, pt, sx, sy, sz};
+    return spin_device(t, xs, n, turn0, nturn, aperture_radius, lost_turn, lost_elem, (cudaStream_t)stream);
+  });
+}
+
+int stb_track_spin_host(stb_table *t, double *x9, long n, int nturn, double aperture_radius, int *stable,
+                        int *lost_turn, int *lost_post) {
+  return guarded([&] { return spin_host(t, x9, n, nturn, aperture_radius, stable, lost_turn, lost_post); });
+}
+
+int stb_track_spin_probe(stb_table *t, double *x9, long n, int nturn, double aperture_radius, double *dump9,
+                         int *stable, int *lost_turn, int *lost_post) {
+  return guarded([&] {
+    if (!dump9) throw Error(STB_EINVAL, "NULL probe buffer");
+    return spin_host(t, x9, n, nturn, aperture_radius, stable, lost_turn, lost_post, dump9);
   });
 }
 

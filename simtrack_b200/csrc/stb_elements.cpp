@@ -96,6 +96,23 @@ MARKER::MARKER(std::string name, double l) : Element(std::move(name)) {
   L = l;
 }
 
+// BPM / HBPM / VBPM, simtrack.cpp:10470-10600 (Pass = DRIFT_Pass)
+BPM::BPM(std::string name, double l) : Element(std::move(name)) {
+  require(l >= 0, "Error: BPM length should be non-negative.");
+  TYPE = "BPM";
+  L = l;
+}
+HBPM::HBPM(std::string name, double l) : Element(std::move(name)) {
+  require(l >= 0, "Error: HBPM length should be non-negative.");
+  TYPE = "HBPM";
+  L = l;
+}
+VBPM::VBPM(std::string name, double l) : Element(std::move(name)) {
+  require(l >= 0, "Error: VBPM length should be non-negative.");
+  TYPE = "VBPM";
+  L = l;
+}
+
 // SBEND, simtrack.cpp:8441-8458
 SBEND::SBEND(std::string name, double l, double angle, double e1, double e2)
     : Element(std::move(name)), ANGLE(angle), E1(e1), E2(e2) {

@@ -139,7 +139,178 @@ double inverse_normal_cdf(double p) {
   return p < 0.5 ? -(u / v) : (u / v);
 }
 
-HostTable flatten(const Line &line) {
+namespace {
+
+// Spin-tracking flop estimate of one spin() call (simtrack.cpp:4574-4630):
+// direction vector, field terms, rotation matrix and product, cos + sin.
+const double kFlSpin = 110;
+
+// Element::sPass forms that differ from Pass (simtrack.cpp:8436-11213).
+// Returns false when the element's sPass is its Pass (the caller then emits
+// the orbit form).  Parameter layouts are documented in stb_spin.cuh.
+bool spin_form(Builder &B, const Element &E, ElemHeader &h, double &fl) {
+  const std::string &T = E.TYPE;
+  const Yoshida &Y = B.y;
+  auto as_drift = [&](double L) {
+    h.op = OP_DRIFT;
+    B.drift_params(L);
+    fl += kFlDrift;
+  };
+  if (T == "GSBEND" || T == "GMULT")
+    throw Error(STB_EUNSUPPORTED, "element " + E.NAME + ": spin tracking of " + T + " is not implemented");
+  if (T == "CRABRF") {
+    as_drift(E.L);  // CRABRF::sPass 10808-10812: a drift inside GtoL/LtoG
+    return true;
+  }
+  if (T == "SBEND") {
+    // SBEND_sPass 7486-7536: Nint exact sub-bends, spin() after each
+    const double L = E.L, Angle = E.GetP("ANGLE"), E1 = E.GetP("E1"), E2 = E.GetP("E2");
+    const int Nint = (int)E.GetP("Nint");
+    if (Angle == 0.) {
+      as_drift(L);
+      return true;
+    }
+    if (Nint <= 0) throw Error(STB_EINVAL, "element " + E.NAME + ": Nint must be positive");
+    const double href = Angle / L, Lint = L / Nint, an = Angle / Nint;
+    h.op = OP_S_SBEND;
+    h.nint = Nint;
+    B.push(std::tan(E1) * href);
+    B.push(std::tan(E2) * href);
+    B.bend_params(Lint, an, std::cos(an), std::sin(an));
+    B.push(an);
+    B.push(href);
+    fl += 2 * kFlEdge + Nint * (kFlBend + kFlSpin);
+    return true;
+  }
+  if (T == "QUAD" || T == "SKEWQ" || T == "SEXT" || T == "OCT") {
+    // QUAD_sPass 7538-7590 (SKEWQ::sPass 8766: K1L = 0), SEXT_sPass 7592-7644, OCT_sPass 7646-7698
+    const int order = (T == "SEXT") ? 2 : (T == "OCT") ? 3 : 1;
+    double kl, ksl;
+    if (T == "QUAD") { kl = E.GetP("K1L"); ksl = E.GetP("K1SL"); }
+    else if (T == "SKEWQ") { kl = 0.; ksl = E.GetP("K1SL"); }
+    else if (T == "SEXT") { kl = E.GetP("K2L"); ksl = E.GetP("K2SL"); }
+    else { kl = E.GetP("K3L"); ksl = E.GetP("K3SL"); }
+    const int Nint = (int)E.GetP("Nint");
+    const double L = E.L;
+    const double kick_fl = order == 1 ? kFlQuadKick : order == 2 ? kFlSextKick : kFlOctKick;
+    h.aux = order;
+    if (kl == 0. && ksl == 0.) {
+      as_drift(L);
+    } else if (L == 0.) {
+      h.op = OP_S_MPOLE_KICK;
+      B.push(kl);
+      B.push(ksl);
+      B.push((double)Nint);
+      fl += kick_fl + 10 + kFlSpin;
+    } else {
+      if (Nint <= 0) throw Error(STB_EINVAL, "element " + E.NAME + ": Nint must be positive");
+      h.op = OP_S_MPOLE_THICK;
+      h.nint = Nint;
+      const double Lint = L / Nint;
+      B.drift_params(Y.d1 * Lint);
+      B.drift_params(Y.d2 * Lint);
+      B.push(Y.k1 * kl / Nint);
+      B.push(Y.k1 * ksl / Nint);
+      B.push(Y.k2 * kl / Nint);
+      B.push(Y.k2 * ksl / Nint);
+      B.push(kl);
+      B.push(ksl);
+      B.push((double)Nint);
+      fl += Nint * (4 * kFlDrift + 3 * kick_fl + 12 + kFlSpin);
+    }
+    return true;
+  }
+  if (T == "MULT") {
+    // MULT_sPass 7700-7740
+    const int Nint = (int)E.GetP("Nint"), Norder = (int)E.GetP("Norder");
+    if (Norder < 0 || Norder > kMaxOrder) throw Error(STB_EINVAL, "element " + E.NAME + ": Norder out of range");
+    const double *knl = E.KNL(), *knsl = E.KNSL();
+    h.aux = Norder;
+    if (E.L == 0.) {
+      h.op = OP_S_MULT_KICK;
+      B.mult_block(Norder, knl, knsl);
+      fl += 2 * mult_kick_flops(Norder, knl, knsl) + 3 + kFlSpin;
+    } else {
+      if (Nint <= 0) throw Error(STB_EINVAL, "element " + E.NAME + ": Nint must be positive");
+      h.op = OP_S_MULT_THICK;
+      h.nint = Nint;
+      const double Lint = E.L / Nint;
+      double k1[11], s1[11], k2[11], s2[11];
+      for (int i = 0; i < 11; i++) {
+        k1[i] = Y.k1 * knl[i] / Nint;
+        s1[i] = Y.k1 * knsl[i] / Nint;
+        k2[i] = Y.k2 * knl[i] / Nint;
+        s2[i] = Y.k2 * knsl[i] / Nint;
+      }
+      B.drift_params(Y.d1 * Lint);
+      B.drift_params(Y.d2 * Lint);
+      B.mult_block(Norder, k1, s1);
+      B.mult_block(Norder, k2, s2);
+      B.mult_block(Norder, knl, knsl);
+      B.push((double)Nint);
+      fl += Nint * (4 * kFlDrift + 2 * mult_kick_flops(Norder, k1, s1) + mult_kick_flops(Norder, k2, s2) +
+                    mult_kick_flops(Norder, knl, knsl) + 7 + kFlSpin);
+    }
+    return true;
+  }
+  if (T == "SBENDMULT") {
+    // SBENDMULT_sPass 7836-7928, exact (non-H_expand) branch
+    const int Nint = (int)E.GetP("Nint"), Norder = (int)E.GetP("Norder");
+    if (Norder < 0 || Norder > kMaxOrder) throw Error(STB_EINVAL, "element " + E.NAME + ": Norder out of range");
+    const double *knl = E.KNL(), *knsl = E.KNSL();
+    const double Angle = E.GetP("ANGLE");
+    h.aux = Norder;
+    if (E.L == 0.) {
+      h.op = OP_S_BENDMULT_KICK;
+      B.mult_block(Norder, knl, knsl);
+      B.push(Angle);
+      fl += 2 * mult_kick_flops(Norder, knl, knsl) + 5 + kFlSpin;
+    } else {
+      if (Nint <= 0) throw Error(STB_EINVAL, "element " + E.NAME + ": Nint must be positive");
+      const double L = E.L, E1 = E.GetP("E1"), E2 = E.GetP("E2");
+      const double href = Angle / L, Lint = L / Nint;
+      h.op = OP_S_BENDMULT;
+      h.nint = Nint;
+      B.push(std::tan(E1) * href);
+      B.push(std::tan(E2) * href);
+      double k1[11], s1[11], k2[11], s2[11];
+      for (int i = 0; i < 11; i++) {
+        k1[i] = Y.k1 * knl[i] / Nint;
+        s1[i] = Y.k1 * knsl[i] / Nint;
+        k2[i] = Y.k2 * knl[i] / Nint;
+        s2[i] = Y.k2 * knsl[i] / Nint;
+      }
+      B.bend_params(Y.d1 * Lint, Y.d1 * Angle / Nint, std::cos(Y.d1 * Angle / Nint), std::sin(Y.d1 * Angle / Nint));
+      B.bend_params(Y.d2 * Lint, Y.d2 * Angle / Nint, std::cos(Y.d2 * Angle / Nint), std::sin(Y.d2 * Angle / Nint));
+      B.mult_block(Norder, k1, s1);
+      B.mult_block(Norder, k2, s2);
+      B.mult_block(Norder, knl, knsl);
+      B.push(Angle / Nint);
+      B.push(href);
+      B.push(Angle);
+      B.push((double)Nint);
+      fl += 2 * kFlEdge + Nint * (4 * kFlBend + 2 * mult_kick_flops(Norder, k1, s1) +
+                                  mult_kick_flops(Norder, k2, s2) + mult_kick_flops(Norder, knl, knsl) + 8 +
+                                  kFlSpin);
+    }
+    return true;
+  }
+  if (T == "KICKER" || T == "HKICKER" || T == "VKICKER") {
+    // KICK_sPass 8193-8208
+    double hk = 0., vk = 0.;
+    if (T != "VKICKER") hk = E.GetP("HKICK");
+    if (T != "HKICKER") vk = E.GetP("VKICK");
+    h.op = OP_S_KICK;
+    B.drift_params(E.L / 2.0);
+    B.push(hk);
+    B.push(vk);
+    fl += 2 * kFlDrift + 2 + kFlSpin;
+    return true;
+  }
+  return false;
+}
+
+HostTable flatten_impl(const Line &line, bool spin) {
   if (GP.H_expand) throw Error(STB_EUNSUPPORTED, "GP.H_expand == true is not implemented on the GPU path");
   if (GP.radiate) throw Error(STB_EUNSUPPORTED, "GP.radiate == true is not implemented on the GPU path");
   Builder B;
@@ -153,6 +324,7 @@ HostTable flatten(const Line &line) {
   t.ref.ibeta = 1.0 / GP.beta;
   t.ref.ienergy = 1.0 / GP.energy;
   t.flops_per_turn = kFlPtRefresh;  // turn-start evaluation of the pt cache
+  t.spin = spin;
   const Yoshida &Y = B.y;
 
   for (size_t idx = 0; idx < line.Cell.size(); idx++) {
@@ -163,9 +335,11 @@ HostTable flatten(const Line &line) {
     h.apy = E.APy;
     double fl = 0;
 
-    // GtoL dispatch (simtrack.cpp:3701-3741).  DRIFT and MARKER never call it.
-    const bool straight_drift = (T == "DRIFT" || T == "MARKER");
-    if (!straight_drift) {
+    // GtoL dispatch (simtrack.cpp:3701-3741).  DRIFT and MARKER never call it,
+    // nor do LBT::sPass and ILBT::sPass (11004, 11053) in spin tracking.
+    const bool straight_drift = (T == "DRIFT" || T == "MARKER" || T == "BPM" || T == "HBPM" || T == "VBPM");
+    const bool no_gtol = straight_drift || (spin && (T == "LBT" || T == "ILBT"));
+    if (!no_gtol) {
       double s = std::fabs(E.DX) + std::fabs(E.DY) + std::fabs(E.DS) + std::fabs(E.DTHETA) +
                  std::fabs(E.DPHI) + std::fabs(E.DPSI);
       if (!(s < 1.0e-9)) {
@@ -193,7 +367,9 @@ HostTable flatten(const Line &line) {
     };
 
     if (straight_drift) {
-      as_drift(E.L);  // DRIFT::Pass 8426, MARKER::Pass 10617
+      as_drift(E.L);  // DRIFT::Pass 8426, MARKER::Pass 10617, BPM/HBPM/VBPM::Pass 10497-10579
+    } else if (spin && spin_form(B, E, h, fl)) {
+      // Element::sPass form emitted by spin_form
     } else if (T == "SBEND") {
       // SBEND_Pass, simtrack.cpp:4693-4752
       const double L = E.L, Angle = E.GetP("ANGLE"), E1 = E.GetP("E1"), E2 = E.GetP("E2");
@@ -481,5 +657,10 @@ HostTable flatten(const Line &line) {
   }
   return t;
 }
+
+}  // namespace
+
+HostTable flatten(const Line &line) { return flatten_impl(line, false); }
+HostTable flatten_spin(const Line &line) { return flatten_impl(line, true); }
 
 }  // namespace stb

@@ -17,12 +17,18 @@ struct HostTable {
   double flops_per_turn = 0.;
   // Number of per-turn refreshes of the pt-only cache (elements that change pt).
   int pt_refreshes = 0;
+  // Flattened for spin tracking (Element::sPass semantics).
+  bool spin = false;
 };
 
 // Flatten `line` against the current reference-particle state GP.
 // Throws stb::Error(STB_EUNSUPPORTED) for element types or settings that
 // the GPU kernel does not implement (radiation, H_expand, pitch/yaw).
 HostTable flatten(const Line &line);
+// Flatten for Track_Spin (simtrack.cpp:21766-21789): the orbit maps of
+// Element::sPass plus the Thomas-BMT rotation of spin() after every slice.
+// GSBEND and GMULT are not available in this form (STB_EUNSUPPORTED).
+HostTable flatten_spin(const Line &line);
 
 // Yoshida coefficients Fdrift1/Fdrift2/Fkick1/Fkick2 (simtrack.cpp:29-32),
 // computed with the same expressions as the reference.

@@ -40,6 +40,22 @@ struct TrackArgs {
   double *dump;
 };
 
+// Spin tracking (stb_spin.cu): the orbit arguments plus the spin unit vector
+// (x[6..8] of the reference's x[9]) as three SoA arrays, updated in place.
+struct SpinArgs {
+  TrackArgs t;  // t.dump is unused
+  double *sx, *sy, *sz;
+  // Optional per-element probe: dump[((i * nturn + t) * nelem + e) * 9 + k].
+  double *dump;
+};
+cudaError_t launch_spin(const SpinArgs &a, int num_sms, bool use_smem, cudaStream_t stream);
+
+// Track_Radial (stb_radial.cu): zsub[j] = z of the on-momentum reference
+// particle after element j (one device thread), then the tracking kernel
+// that subtracts it after every element.
+cudaError_t launch_radial_reference(const TrackArgs &a, double *zsub, cudaStream_t stream);
+cudaError_t launch_radial(const TrackArgs &a, const double *zsub, int num_sms, bool use_smem, cudaStream_t stream);
+
 // Elementary-function diagnostics (stb_diag.cu).
 int math_input_arity(int fn);
 bool math_fn_valid(int fn);

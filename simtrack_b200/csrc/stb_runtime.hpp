@@ -20,6 +20,7 @@ struct stb_table {
   int variant = 2;        // launch variant (stb::kVariants), set by the autotuner
   int *d_status = nullptr;
   int num_sms = 0;
+  double *d_zsub = nullptr;  // Track_Radial's per-element on-momentum z (computed on first use)
 };
 
 namespace stb {

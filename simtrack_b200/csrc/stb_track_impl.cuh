@@ -1,7 +1,6 @@
 // Device code of the element-by-element tracking kernels, shared by the
-// single-lattice tracker (stb_track.cu) and the batched scan (stb_scan.cu).
-// Included by exactly those two translation units; everything here has
-// internal linkage.
+// single-lattice tracker (stb_track.cu), the batched scan (stb_scan.cu) and
+// the spin tracker (stb_spin.cu).  Everything here has internal linkage.
 #pragma once
 #include <cuda_runtime.h>
 

@@ -266,3 +266,156 @@ def gaussian_beam(lat: Lattice, n: int, seed: int = 12345, sigma_z: float = 0.1,
     spx = sx / lat.meta["beta_star"]
     g = rng.standard_normal((n, 6))
     return g * np.array([sx, spx, sx, spx, sigma_z, sigma_pt])
+
+
+EIC_GAMMA = 275000.0 / PROTON_MASS_MEV  # 275 GeV protons
+EIC_HALF_CROSSING = 0.0125              # half of the 25 mrad full crossing angle
+
+
+def eic_like_ring(seed: Optional[int] = None, nint_arc: int = 4, nint_triplet: int = 8,
+                  aperture_radius: float = 0.03, crab_mv=(2.0, -0.4)) -> Lattice:
+    """Synthetic EIC hadron-ring-like lattice for spin tracking, 3,834 m,
+    ~2,450 elements, 275 GeV protons.
+
+    The RHIC-like ring's optics (normalised strengths do not depend on the
+    energy) with one collision point: at IP1 a Lorentz boost for the 25 mrad
+    full crossing angle (LBT / ILBT, theta = 12.5 mrad) around the weak-strong
+    6D beam-beam map of a flat electron bunch (1.7e11 charges of opposite sign,
+    sigma_x = 95 um, sigma_y = 8.5 um, sigma_z = 7 mm, 7 slices), thin crab
+    cavities at 197 and 394 MHz on either side of it (the downstream pair
+    with opposite voltages), no beam-beam at IP2, a beam-position marker after
+    every arc quadrupole and a zero-strength orbit corrector after the
+    sextupoles of every other arc cell.  IR triplet errors as in
+    rhic_like_ring."""
+    base = rhic_like_ring(seed=seed, nint_arc=nint_arc, nint_triplet=nint_triplet, bb=False,
+                          aperture_radius=aperture_radius)
+    beta = math.sqrt(1.0 - 1.0 / EIC_GAMMA / EIC_GAMMA)
+    from . import lattice_design as D
+    frev = beta * 299792458.0 / D.CIRC
+    bx, by = 0.8, 0.072
+    bb = ElementSpec("BEAMBEAM", "bb_ip1", (6, 1.7e11, -1.0, 0.007, 7, 95e-6 ** 2 / bx, bx, 0.0, 8.5e-6 ** 2 / by,
+                                            by, 0.0))
+    v1, v2 = crab_mv
+    up = [ElementSpec("CRABRF", "crab197_u", (0.0, v1, 197e6, 0.0)),
+          ElementSpec("CRABRF", "crab394_u", (0.0, v2, 394e6, 0.0))]
+    down = [ElementSpec("CRABRF", "crab394_d", (0.0, -v2, 394e6, 0.0)),
+            ElementSpec("CRABRF", "crab197_d", (0.0, -v1, 197e6, 0.0))]
+    ip = up + [ElementSpec("LBT", "lbt_ip1", (EIC_HALF_CROSSING,)), bb,
+               ElementSpec("ILBT", "ilbt_ip1", (EIC_HALF_CROSSING,))] + down
+    els: List[ElementSpec] = list(ip)
+    cell = 0
+    for e in base.elements:
+        if e.type == "RFCAV":
+            h = 360 if "28" in e.name else 2520
+            e = ElementSpec("RFCAV", e.name, (e.args[0], e.args[1], h * frev, e.args[3]))
+        els.append(e)
+        if e.type == "QUAD" and (e.name.startswith("qd_") or e.name.startswith("qf_")):
+            els.append(ElementSpec("MARKER", "bpm_" + e.name, (0.0,)))
+        if e.type == "SEXT" and e.name.startswith("sd_"):
+            cell += 1
+            if cell % 2 == 0:
+                kind = "HKICKER" if cell % 4 == 0 else "VKICKER"
+                els.append(ElementSpec(kind, "cor_" + e.name, (0.0, 0.0)))
+    lat = Lattice("eic_like" + ("" if seed is None else f"_s{seed}"), els, EIC_GAMMA,
+                  aperture_radius=aperture_radius)
+    lat.meta.update({"seed": seed, "beta_star": RHIC_BETA_STAR, "emit_norm": 2.5e-6, "frev": frev,
+                     "sigma_ip": math.sqrt(2.5e-6 * RHIC_BETA_STAR / (beta * EIC_GAMMA)), "spin_g": 1.7928474})
+    return lat
+
+
+# ---- MAD-X TFS twiss tables (the format Read_MADX_Lattice reads) ----
+
+_TFS_KEYWORD = {"DRIFT": "DRIFT", "SBEND": "SBEND", "QUAD": "QUADRUPOLE", "SEXT": "SEXTUPOLE", "OCT": "OCTUPOLE",
+                "MULT": "MULTIPOLE", "MARKER": "MARKER", "HKICKER": "HKICKER", "VKICKER": "VKICKER",
+                "KICKER": "TKICKER", "RFCAV": "RFCAVITY", "BEAMBEAM": "BEAMBEAM", "BPM": "MONITOR",
+                "VBPM": "VMONITOR"}
+
+
+def write_madx_tfs(lat: Lattice, path: str) -> None:
+    """Writes `lat` as a MAD-X-style TFS twiss table with the columns
+    Read_MADX_Lattice (simtrack.cpp:13591) reads.  Strengths are written
+    with 17 significant digits (exact round trip).  What the format cannot
+    carry is dropped, as reading a MAD-X table would: slice counts (the
+    reader's defaults apply), corrector kicks, RF voltages and beam-beam
+    parameters."""
+    cols = ["NAME", "KEYWORD", "S", "L", "ANGLE", "E1", "E2", "TILT"]
+    for k in range(11):
+        cols += [f"K{k}L", f"K{k}SL"]
+    cols += ["KS"]
+    rows = []
+    s = 0.0
+    for e in lat.elements:
+        kw = _TFS_KEYWORD.get(e.type, "INSTRUMENT")
+        a = e.args
+        L = 0.0 if e.type in ("LBT", "ILBT", "BEAMBEAM") else float(a[0])
+        angle = e1 = e2 = 0.0
+        knl = [0.0] * 11
+        knsl = [0.0] * 11
+        if e.type == "SBEND":
+            angle, e1, e2 = a[1], a[2], a[3]
+        elif e.type in ("QUAD", "SEXT", "OCT"):
+            order = {"QUAD": 1, "SEXT": 2, "OCT": 3}[e.type]
+            knl[order], knsl[order] = a[1], a[2]
+        elif e.type == "MULT":
+            knl, knsl = list(a[1:12]), list(a[12:23])
+        tilt = e.misalign[5] if e.misalign is not None else 0.0
+        s += L
+        vals = [s, L, angle, e1, e2, tilt]
+        for k in range(11):
+            vals += [knl[k], knsl[k]]
+        vals.append(0.0)
+        rows.append(f'"{e.name.upper()}" "{kw}" ' + " ".join(repr(float(v)) for v in vals))
+    with open(path, "w") as f:
+        f.write('@ NAME             %05s "TWISS"\n')
+        f.write(f"@ LENGTH           %le {s!r}\n")
+        f.write("* " + " ".join(cols) + "\n")
+        f.write("$ %s %s " + " ".join(["%le"] * (len(cols) - 2)) + "\n")
+        f.write("\n".join(rows) + "\n")
+
+
+def specs_from_line(line: api.Line) -> List[ElementSpec]:
+    """ElementSpec list describing an existing Line (for the oracles or for
+    inspection): type, name, constructor arguments, slice counts, roll."""
+    out = []
+    mult = tuple(f"K{k}L" for k in range(11)) + tuple(f"K{k}SL" for k in range(11))
+    for i in range(line.Ncell):
+        e = line.Cell(i)
+        t, g = e.TYPE, e.geometry()
+        P = e.GetP
+        setp = {}
+        if t in ("DRIFT", "MARKER", "BPM", "HBPM", "VBPM"):
+            args = (g["L"],)
+        elif t == "SBEND":
+            args = (g["L"], P("ANGLE"), P("E1"), P("E2"))
+            setp = {"Nint": P("Nint")}
+        elif t == "GSBEND":
+            args = (g["L"], P("ANGLE"), P("K0L"), P("E1"), P("E2"))
+            setp = {"Nint": P("Nint")}
+        elif t in ("QUAD", "SEXT", "OCT"):
+            k = {"QUAD": "1", "SEXT": "2", "OCT": "3"}[t]
+            args = (g["L"], P(f"K{k}L"), P(f"K{k}SL"))
+            setp = {"Nint": P("Nint")}
+        elif t == "MULT":
+            args = (g["L"],) + tuple(P(n) for n in mult)
+            setp = {"Nint": P("Nint"), "Norder": P("Norder")}
+        elif t in ("GMULT", "SBENDMULT"):
+            args = (g["L"], P("ANGLE"), P("E1"), P("E2")) + tuple(P(n) for n in mult)
+            setp = {"Nint": P("Nint"), "Norder": P("Norder")}
+        elif t == "HKICKER":
+            args = (g["L"], P("HKICK"))
+        elif t == "VKICKER":
+            args = (g["L"], P("VKICK"))
+        elif t == "KICKER":
+            args = (g["L"], P("HKICK"), P("VKICK"))
+        elif t == "RFCAV":
+            args = (g["L"], P("VRF"), P("FRF"), P("PHASE0"))
+        elif t == "BEAMBEAM":
+            args = tuple(P(n) for n in ("TREATMENT", "NP", "BBSCALE", "SIGMAL", "NSLICE", "EMITX", "BETAX", "ALFAX",
+                                        "EMITY", "BETAY", "ALFAY"))
+        else:
+            raise ValueError(f"specs_from_line: element type {t} not handled")
+        mis = (g["DX"], g["DY"], g["DS"], g["DTHETA"], g["DPHI"], g["DPSI"])
+        out.append(ElementSpec(t, e.NAME, tuple(float(v) for v in args), setp,
+                               misalign=mis if any(v != 0.0 for v in mis) else None,
+                               aperture=(g["APx"], g["APy"]) if (g["APx"], g["APy"]) != (1.0, 1.0) else None))
+    return out

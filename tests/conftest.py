@@ -37,6 +37,13 @@ def ref_oracle():
 
 
 @pytest.fixture(scope="session")
+def ref_cr_oracle():
+    if not oracle_bridge.ref_available(cr=True):
+        pytest.skip("compiled reference oracle with correctly rounded libm (oracle/_ref) not built here")
+    return oracle_bridge.RefOracle(cr=True)
+
+
+@pytest.fixture(scope="session")
 def native_lib():
     from simtrack_b200 import _native
     if not _native.LIB_PATH.exists():

@@ -21,7 +21,7 @@ HERE = Path(__file__).resolve().parent
 sys.path.insert(0, str(HERE.parent))
 sys.path.insert(0, str(HERE.parents[1]))
 
-from lattice_zoo import zoo, zoo_particles  # noqa: E402
+from lattice_zoo import spin_particles, spin_zoo, zoo, zoo_particles  # noqa: E402
 from simtrack_b200.lattices import fodo_ring  # noqa: E402
 
 
@@ -74,6 +74,19 @@ def main():
     np.savez_compressed(HERE / "fine_tune.npz", x=xs, px=pxs, windows=np.array(TUNE_WINDOWS, dtype=np.float64),
                         tunes=tunes)
     print("wrote fine_tune")
+    # spin tracking: Track_Spin's per-element x[9] on the spin zoo
+    lat = spin_zoo()
+    ref.build(lat)
+    x9 = spin_particles()
+    nturn = lat.meta["turns"]
+    dumps, loss = [], []
+    for x0 in x9:
+        _, st, lt, lp, d = ref.track_spin_dump(x0, nturn)
+        dumps.append(d)
+        loss.append((st, lt, lp))
+    np.savez_compressed(HERE / "spin_zoo.npz", x0=x9, nturn=nturn, dump=np.array(dumps),
+                        loss=np.array(loss, dtype=np.int64))
+    print("wrote spin_zoo")
     for name, c in CASES.items():
         ref.build(lattice_for(name))
         dumps, loss = [], []

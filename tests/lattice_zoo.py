@@ -67,3 +67,30 @@ def zoo_particles():
         [1e-4, 1e-6, 1e-4, 1e-6, -0.3, 3e-4],
     ]
     return np.array(P, dtype=np.float64)
+
+
+def spin_zoo() -> Lattice:
+    """The zoo without the element types whose spin form is not implemented
+    (GSBEND, GMULT), plus thin forms that only spin tracking treats apart
+    (thin sextupole, thin bend multipole, a zero-strength kicker)."""
+    base = zoo()
+    els = [e for e in base.elements if e.type not in ("GSBEND", "GMULT")]
+    els += [
+        S("SEXT", "s_thin", (0.0, 0.8, -0.2)),
+        S("SBENDMULT", "sbm0", (0.0, 0.003, 0.0, 0.0, *([0.0, 0.0, 0.1, 0.0, 10.0] + [0.0] * 6),
+                                 *([0.0, 0.0, 0.0, 2.0] + [0.0] * 7))),
+        S("KICKER", "k0", (0.3, 0.0, 0.0)),
+        S("SBEND", "b2", (2.0, -0.015, 0.0, 0.0), {"Nint": 3}),
+    ]
+    lat = Lattice("spin_zoo", els, GAMMA_100GEV)
+    lat.meta["turns"] = 2
+    return lat
+
+
+def spin_particles():
+    """zoo_particles with a spin unit vector appended to each."""
+    import numpy as np
+    x = zoo_particles()
+    s = np.array([[0.0, 1.0, 0.0], [0.6, 0.8, 0.0], [0.0, 0.6, 0.8], [1.0, 0.0, 0.0],
+                  [0.36, 0.48, 0.8], [0.0, 1.0, 0.0], [-0.28, 0.96, 0.0]])
+    return np.concatenate([x, s], axis=1)

@@ -22,14 +22,16 @@ from simtrack_b200.lattices import Lattice
 
 ROOT = Path(__file__).resolve().parents[1]
 REF_SO = ROOT / "oracle" / "_ref" / "libsimtrack_ref.so"
+# the same reference objects with correctly rounded asin/sin/cos/exp/pow
+REF_CR_SO = ROOT / "oracle" / "_ref" / "libsimtrack_ref_cr.so"
 PORT_SO = ROOT / "oracle" / "_build" / "libsimtrack_port.so"
 
 PORT_TYPES = ["DRIFT", "MARKER", "SBEND", "GSBEND", "QUAD", "SKEWQ", "SEXT", "OCT", "MULT", "GMULT",
               "SBENDMULT", "KICKER", "HKICKER", "VKICKER", "RFCAV", "CRABRF", "CCMULT", "LBT", "ILBT", "BEAMBEAM"]
 
 
-def ref_available() -> bool:
-    return REF_SO.exists()
+def ref_available(cr: bool = False) -> bool:
+    return (REF_CR_SO if cr else REF_SO).exists()
 
 
 def port_available() -> bool:
@@ -37,8 +39,11 @@ def port_available() -> bool:
 
 
 class RefOracle:
-    def __init__(self):
-        L = ctypes.CDLL(str(REF_SO))
+    """The compiled reference.  cr=True loads the variant whose transcendentals
+    are correctly rounded (oracle/crlibm_shim.cpp)."""
+
+    def __init__(self, cr: bool = False):
+        L = ctypes.CDLL(str(REF_CR_SO if cr else REF_SO))
         L.ref_line_new.restype = c_void_p
         L.ref_line_free.argtypes = [c_void_p]
         L.ref_line_ncell.restype = c_long
@@ -61,6 +66,16 @@ class RefOracle:
         L.ref_pinv.argtypes = [c_double]
         L.ref_pinv.restype = c_double
         L.ref_pass.argtypes = [c_void_p, c_long, POINTER(c_double)]
+        L.ref_track_spin.argtypes = [c_void_p, POINTER(c_double), c_long, c_int, POINTER(c_int), POINTER(c_int),
+                                     POINTER(c_int)]
+        L.ref_line_read_madx.argtypes = [ctypes.c_char_p]
+        L.ref_line_read_madx.restype = c_void_p
+        L.ref_line_elem.argtypes = [c_void_p, c_long, ctypes.c_char_p, ctypes.c_char_p, c_int, POINTER(c_double)]
+        L.ref_track_radial.argtypes = [c_void_p, POINTER(c_double), c_long, c_int, POINTER(c_int), POINTER(c_int),
+                                       POINTER(c_int)]
+        L.ref_track_spin_dump.argtypes = [c_void_p, POINTER(c_double), c_int, POINTER(c_double), POINTER(c_int),
+                                          POINTER(c_int), POINTER(c_int)]
+        L.ref_set_spin_g.argtypes = [c_double]
         L.ref_fine_tune.argtypes = [c_int, POINTER(c_double), POINTER(c_double), c_double, c_double]
         L.ref_fine_tune.restype = c_double
         self.L = L
@@ -117,6 +132,59 @@ class RefOracle:
                               ctypes.byref(lp))
         return x, st.value, lt.value, lp.value, dump
 
+    def track_spin(self, x9: np.ndarray, nturn: int):
+        """Track_Spin over AoS x[n, 9] (copied); returns (x, stable, lost_turn, lost_post)."""
+        x = np.ascontiguousarray(x9, dtype=np.float64).copy()
+        n = x.shape[0]
+        st = np.ones(n, dtype=np.int32)
+        lt = np.zeros(n, dtype=np.int32)
+        lp = np.zeros(n, dtype=np.int32)
+        P = POINTER
+        self.L.ref_track_spin(self.line, x.ctypes.data_as(P(c_double)), n, nturn, st.ctypes.data_as(P(c_int)),
+                              lt.ctypes.data_as(P(c_int)), lp.ctypes.data_as(P(c_int)))
+        return x, st, lt, lp
+
+    def read_madx(self, path: str) -> None:
+        """Replaces the line by the reference's Read_MADX_Lattice of `path` (must exist)."""
+        if self.line:
+            self.L.ref_line_free(self.line)
+        self.line = self.L.ref_line_read_madx(str(path).encode())
+        self.nelem = int(self.L.ref_line_ncell(self.line))
+        self.radius = 0.0
+
+    def element(self, i: int):
+        """(TYPE, NAME, {L, S, DX, DY, DS, DTHETA, DPHI, DPSI, APx, APy}) of element i."""
+        t = ctypes.create_string_buffer(256)
+        nm = ctypes.create_string_buffer(256)
+        g = (c_double * 10)()
+        self.L.ref_line_elem(self.line, i, t, nm, 256, g)
+        keys = ("L", "S", "DX", "DY", "DS", "DTHETA", "DPHI", "DPSI", "APx", "APy")
+        return t.value.decode(), nm.value.decode(), {k: g[j] for j, k in enumerate(keys)}
+
+    def getp(self, i: int, name: str) -> float:
+        return self.L.ref_line_getp(self.line, i, name.encode())
+
+    def track_radial(self, x: np.ndarray, nturn: int):
+        """Track_Radial over AoS x[n, 6] (copied); returns (x, stable, lost_turn, lost_post)."""
+        x = np.ascontiguousarray(x, dtype=np.float64).copy()
+        n = x.shape[0]
+        st = np.ones(n, dtype=np.int32)
+        lt = np.zeros(n, dtype=np.int32)
+        lp = np.zeros(n, dtype=np.int32)
+        P = POINTER
+        self.L.ref_track_radial(self.line, x.ctypes.data_as(P(c_double)), n, nturn, st.ctypes.data_as(P(c_int)),
+                                lt.ctypes.data_as(P(c_int)), lp.ctypes.data_as(P(c_int)))
+        return x, st, lt, lp
+
+    def track_spin_dump(self, x0, nturn: int):
+        x = np.ascontiguousarray(x0, dtype=np.float64).copy()
+        dump = np.full((nturn, self.nelem, 9), np.nan)
+        st, lt, lp = c_int(), c_int(), c_int()
+        self.L.ref_track_spin_dump(self.line, x.ctypes.data_as(POINTER(c_double)), nturn,
+                                   dump.ctypes.data_as(POINTER(c_double)), ctypes.byref(st), ctypes.byref(lt),
+                                   ctypes.byref(lp))
+        return x, st.value, lt.value, lp.value, dump
+
     def fine_tune(self, x, px=None, lo: float = 0.0, hi: float = 0.5) -> float:
         """FineTuneFinder (x-only, or the x/px overload when px is given)."""
         x = np.ascontiguousarray(x, dtype=np.float64)
@@ -170,7 +238,8 @@ class PortOracle:
         arr = (PortElem * n)()
         for i, e in enumerate(lat.elements):
             pe = arr[i]
-            pe.type = PORT_TYPES.index(e.type)
+            # monitors track as markers: a drift without misalignment (BPM::Pass 10497)
+            pe.type = PORT_TYPES.index("MARKER" if e.type in ("BPM", "HBPM", "VBPM") else e.type)
             a = list(e.args)
             pe.apx, pe.apy = (1.0, 1.0) if e.aperture is None else e.aperture
             if e.misalign is not None:

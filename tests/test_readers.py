@@ -1,0 +1,114 @@
+"""Read_MADX_Lattice (simtrack.cpp:13591-13791): the reader against the
+reference's own reader, on the RHIC lattice shipped with the reference
+(Example1/parameters_input, 6,858 elements; read in place, CPU only) and on
+tables written by lattices.write_madx_tfs, and tracking through what was read."""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from simtrack_b200 import api
+from simtrack_b200 import lattices as lt
+
+RHIC_TFS = Path("/root/reference/Example1/parameters_input")
+
+PARAMS = {
+    "SBEND": ("ANGLE", "E1", "E2", "Nint"),
+    "GSBEND": ("ANGLE", "K0L", "E1", "E2", "Nint"),
+    "QUAD": ("K1L", "K1SL", "Nint"),
+    "SEXT": ("K2L", "K2SL", "Nint"),
+    "OCT": ("K3L", "K3SL", "Nint"),
+    "MULT": tuple(f"K{k}L" for k in range(11)) + tuple(f"K{k}SL" for k in range(11)) + ("Norder", "Nint"),
+    "HKICKER": ("HKICK",),
+    "VKICKER": ("VKICK",),
+    "KICKER": ("HKICK", "VKICK"),
+    "RFCAV": ("VRF", "FRF", "PHASE0"),
+}
+
+
+def compare_lines(line, ref):
+    assert line.Ncell == ref.nelem
+    for i in range(line.Ncell):
+        e = line.Cell(i)
+        rt, rn, rg = ref.element(i)
+        assert (e.TYPE, e.NAME) == (rt, rn), i
+        g = e.geometry()
+        for k in ("L", "S", "DX", "DY", "DPSI", "APx", "APy"):
+            assert g[k] == rg[k], (i, k, g[k], rg[k])
+        for p in PARAMS.get(rt, ()):
+            assert e.GetP(p) == ref.getp(i, p), (i, rt, p)
+
+
+@pytest.mark.skipif(not RHIC_TFS.exists(), reason="reference example lattice not present")
+def test_reader_matches_reference_on_rhic_lattice(ref_oracle, port_oracle):
+    api.Set_RefPartEnergy(100.0, 938.27201, 1, 1)
+    ref_oracle.L.ref_set_ref_energy(100.0, 938.27201, 1.0, 1.0)
+    line = api.Line()
+    line.read_madx(str(RHIC_TFS))
+    ref_oracle.read_madx(str(RHIC_TFS))
+    compare_lines(line, ref_oracle)
+    # tracking through what was read: the C restatement on our reader's line
+    # equals the reference's Track() on the reference reader's line
+    lat = lt.Lattice("rhic_tfs", lt.specs_from_line(line), 100.0)
+    port_oracle.build(lat)
+    X = np.array([[1e-3, 0, 5e-4, 0, 0, 0], [-2e-3, 1e-5, 1e-3, 0, 0.01, 3e-4]])
+    xp, sp, lp_, pp = port_oracle.track(X.copy(), 3)
+    xr = X.copy()
+    st = np.ones(2, dtype=np.int32)
+    lt_ = np.zeros(2, dtype=np.int32)
+    lp = np.zeros(2, dtype=np.int32)
+    from ctypes import POINTER, c_double, c_int
+    ref_oracle.L.ref_track(ref_oracle.line, xr.ctypes.data_as(POINTER(c_double)), 2, 3,
+                           st.ctypes.data_as(POINTER(c_int)), lt_.ctypes.data_as(POINTER(c_int)),
+                           lp.ctypes.data_as(POINTER(c_int)))
+    assert np.array_equal(sp, st) and np.array_equal(lp_, lt_)
+    assert np.array_equal(xp, xr)
+
+
+def test_written_table_reads_back(tmp_path, ref_oracle):
+    lat = lt.rhic_like_ring(seed=4)
+    # give a few elements a roll so that TILT is exercised
+    for e in lat.elements[10:400:37]:
+        if e.type in ("QUAD", "SEXT", "MULT", "SBEND"):
+            e.misalign = (0.0, 0.0, 0.0, 0.0, 0.0, 2e-3)
+    path = tmp_path / "ring.tfs"
+    lt.write_madx_tfs(lat, str(path))
+    lat.set_reference()
+    ref_oracle.L.ref_set_ref_energy(lat.gamma, lat.E0, lat.Q, lat.A)
+    line = api.Line()
+    line.read_madx(str(path))
+    ref_oracle.read_madx(str(path))
+    compare_lines(line, ref_oracle)
+    assert abs(line.Length - lat.circumference) < 1e-6
+
+
+@pytest.mark.gpu
+def test_gpu_tracking_through_read_table(tmp_path, native_lib, ref_oracle):
+    lat = lt.rhic_like_ring(seed=5)
+    for e in lat.elements[5:900:41]:
+        if e.type in ("QUAD", "SEXT", "MULT", "SBEND"):
+            e.misalign = (0.0, 0.0, 0.0, 0.0, 0.0, -1.5e-3)
+    path = tmp_path / "ring.tfs"
+    lt.write_madx_tfs(lat, str(path))
+    lat.set_reference()
+    ref_oracle.L.ref_set_ref_energy(lat.gamma, lat.E0, lat.Q, lat.A)
+    line = api.Line()
+    line.read_madx(str(path))
+    ref_oracle.read_madx(str(path))
+    tab = api.Table(line)
+    sig = lat.meta["sigma_ip"]
+    X = np.array([[a * sig, 0, 0.5 * a * sig, 0, 0.02, 2e-4] for a in (0.5, 2.0, 5.0, 9.0)])
+    nt = 20
+    xg, sg, lg, pg = tab.track_host(X.copy(), nt)
+    xr = X.copy()
+    st = np.ones(4, dtype=np.int32)
+    lt_ = np.zeros(4, dtype=np.int32)
+    lp = np.zeros(4, dtype=np.int32)
+    from ctypes import POINTER, c_double, c_int
+    ref_oracle.L.ref_track(ref_oracle.line, xr.ctypes.data_as(POINTER(c_double)), 4, nt,
+                           st.ctypes.data_as(POINTER(c_int)), lt_.ctypes.data_as(POINTER(c_int)),
+                           lp.ctypes.data_as(POINTER(c_int)))
+    assert np.array_equal(sg, st) and np.array_equal(lg, lt_) and np.array_equal(pg, lp)
+    ok = sg == 1
+    floor = np.maximum(np.sqrt(np.mean(xr[ok] ** 2, axis=0)), 1e-300)
+    assert np.all(np.abs(xg[ok] - xr[ok]) <= 1e-12 * np.maximum(np.abs(xr[ok]), floor))
