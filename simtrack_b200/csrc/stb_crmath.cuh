@@ -92,6 +92,71 @@ __host__ __device__ inline double cr_asin(double x) {
   return s.hi + (s.lo + xr.lo);
 }
 
+// Double-double reciprocals of the Taylor-series divisors: inv_n(n) = 1/n
+// (n = 1..14), inv_cos(j) = 1/((2j-1)(2j)) and inv_sin(j) = 1/((2j)(2j+1))
+// (j = 1..13), each split as the rounded value plus its rounded remainder
+// (exact rational arithmetic).  The loops below are unrolled, so every
+// lookup folds to a constant.
+// Multiplying by them in double-double keeps the ~2^-104 relative accuracy
+// of dividing by the exact integers, at a fraction of the cost.
+__host__ __device__ constexpr dd inv_n(int n) {
+  switch (n) {
+    case 1: return dd{1.0, 0.0};
+    case 2: return dd{0.5, 0.0};
+    case 3: return dd{0.3333333333333333, 1.850371707708594e-17};
+    case 4: return dd{0.25, 0.0};
+    case 5: return dd{0.2, -1.1102230246251566e-17};
+    case 6: return dd{0.16666666666666666, 9.25185853854297e-18};
+    case 7: return dd{0.14285714285714285, 7.93016446160826e-18};
+    case 8: return dd{0.125, 0.0};
+    case 9: return dd{0.1111111111111111, 6.1679056923619804e-18};
+    case 10: return dd{0.1, -5.551115123125783e-18};
+    case 11: return dd{0.09090909090909091, -2.523234146875356e-18};
+    case 12: return dd{0.08333333333333333, 4.625929269271485e-18};
+    case 13: return dd{0.07692307692307693, -4.270088556250602e-18};
+    case 14: return dd{0.07142857142857142, 3.96508223080413e-18};
+    default: return dd{0.0, 0.0};
+  }
+}
+// 1/((2j-1)(2j)), the cosine series (j = 1..13: 1/2, 1/12, ..., 1/650)
+__host__ __device__ constexpr dd inv_cos(int n) {
+  switch (n) {
+    case 1: return dd{0.5, 0.0};
+    case 2: return dd{0.08333333333333333, 4.625929269271485e-18};
+    case 3: return dd{0.03333333333333333, 4.625929269271486e-19};
+    case 4: return dd{0.017857142857142856, 9.912705577010326e-19};
+    case 5: return dd{0.011111111111111112, -4.2404351634988616e-19};
+    case 6: return dd{0.007575757575757576, -2.1026951223961299e-19};
+    case 7: return dd{0.005494505494505495, -4.2891514515910067e-19};
+    case 8: return dd{0.004166666666666667, 5.782411586589357e-20};
+    case 9: return dd{0.0032679738562091504, -9.920804192677818e-20};
+    case 10: return dd{0.002631578947368421, 5.934580312552235e-20};
+    case 11: return dd{0.0021645021645021645, 1.8774063592822588e-21};
+    case 12: return dd{0.0018115942028985507, -2.199830494898125e-20};
+    case 13: return dd{0.0015384615384615385, 1.3344026738283131e-21};
+    default: return dd{0.0, 0.0};
+  }
+}
+// 1/((2j)(2j+1)), the sine series (j = 1..13: 1/6, 1/20, ..., 1/702)
+__host__ __device__ constexpr dd inv_sin(int n) {
+  switch (n) {
+    case 1: return dd{0.16666666666666666, 9.25185853854297e-18};
+    case 2: return dd{0.05, -2.7755575615628915e-18};
+    case 3: return dd{0.023809523809523808, 1.32169407693471e-18};
+    case 4: return dd{0.013888888888888888, 7.709882115452476e-19};
+    case 5: return dd{0.00909090909090909, 4.415659757031872e-19};
+    case 6: return dd{0.00641025641025641, 2.2240044563805217e-19};
+    case 7: return dd{0.004761904761904762, -4.295505750037808e-19};
+    case 8: return dd{0.003676470588235294, 5.102127870520021e-20};
+    case 9: return dd{0.0029239766081871343, 1.6231330769373633e-19};
+    case 10: return dd{0.002380952380952381, -2.147752875018904e-19};
+    case 11: return dd{0.001976284584980237, 1.3370398332627564e-19};
+    case 12: return dd{0.0016666666666666668, -1.0697461435190311e-19};
+    case 13: return dd{0.0014245014245014246, -7.104458680104445e-20};
+    default: return dd{0.0, 0.0};
+  }
+}
+
 // exp: x = k ln2 + r (double-double reduction), exp(r) = (exp(r/16))^16 with
 // exp(r/16) from its Taylor series in double-double Horner form.
 static __host__ __device__ __noinline__ double cr_exp(double x) {
@@ -107,8 +172,9 @@ static __host__ __device__ __noinline__ double cr_exp(double x) {
   const dd s{r.hi * 0.0625, r.lo * 0.0625};
   // e = exp(s) = 1 + s(1 + s/2(1 + s/3(... (1 + s/14))))
   dd e{1.0, 0.0};
+#pragma unroll
   for (int n = 14; n >= 1; n--) {
-    e = dd_div_small(dd_mul(e, s), (double)n);
+    e = dd_mul(dd_mul(e, s), inv_n(n));  // e * s / n
     e = dd_add_d(e, 1.0);
   }
   for (int i = 0; i < 4; i++) e = dd_mul(e, e);
@@ -129,18 +195,31 @@ static __host__ __device__ __noinline__ void cr_sincos_reduced(double x, dd &sr,
   r = dd_add(r, dd{-b.hi, -b.lo});
   r = dd_add_d(r, -k * P3);
   const dd r2 = dd_mul(r, r);
+  // Terms kept: all 13 for |r| up to pi/4.  For |r| < 2^-4 the first
+  // neglected term (r^18/19! resp. r^20/20!) is below 2^-128 relative, so 8
+  // resp. 9 terms suffice; for |r| < 2^-7, 6 and 6 (first neglected term
+  // below 2^-112).
+  const double ar = fabs(r.hi);
+  const int jmax_s = ar < 0.0078125 ? 6 : ar < 0.0625 ? 8 : 13;
+  const int jmax_c = ar < 0.0078125 ? 6 : ar < 0.0625 ? 9 : 13;
   // sin r = r (1 - r^2/(2*3) (1 - r^2/(4*5) (...)))
   dd s{1.0, 0.0};
-  for (int n = 26; n >= 2; n -= 2) {
-    s = dd_div_small(dd_mul(r2, s), (double)(n * (n + 1)));
-    s = dd_add_d(dd{-s.hi, -s.lo}, 1.0);
+#pragma unroll
+  for (int j = 13; j >= 1; j--) {
+    if (j <= jmax_s) {
+      s = dd_mul(dd_mul(r2, s), inv_sin(j));
+      s = dd_add_d(dd{-s.hi, -s.lo}, 1.0);
+    }
   }
   sr = dd_mul(r, s);
   // cos r = 1 - r^2/(1*2) (1 - r^2/(3*4) (...))
   dd c{1.0, 0.0};
-  for (int n = 25; n >= 1; n -= 2) {
-    c = dd_div_small(dd_mul(r2, c), (double)(n * (n + 1)));
-    c = dd_add_d(dd{-c.hi, -c.lo}, 1.0);
+#pragma unroll
+  for (int j = 13; j >= 1; j--) {
+    if (j <= jmax_c) {
+      c = dd_mul(dd_mul(r2, c), inv_cos(j));
+      c = dd_add_d(dd{-c.hi, -c.lo}, 1.0);
+    }
   }
   cr = c;
   quad = ((int)fmod(k, 4.0) + 4) & 3;
@@ -155,6 +234,23 @@ __host__ __device__ inline double cr_sin(double x) {
   if (q == 1) return c.hi + c.lo;
   if (q == 2) return -(s.hi + s.lo);
   return -(c.hi + c.lo);
+}
+
+// sin and cos of the same argument from one reduction.
+__host__ __device__ inline void cr_sincos(double x, double &sn, double &cs) {
+  if (!(fabs(x) < 1048576.0)) {
+    sn = sin(x);
+    cs = cos(x);
+    return;
+  }
+  dd s, c;
+  int q;
+  cr_sincos_reduced(x, s, c, q);
+  const double sv = s.hi + s.lo, cv = c.hi + c.lo;
+  if (q == 0) { sn = sv; cs = cv; }
+  else if (q == 1) { sn = cv; cs = -sv; }
+  else if (q == 2) { sn = -sv; cs = -cv; }
+  else { sn = -cv; cs = sv; }
 }
 
 __host__ __device__ inline double cr_cos(double x) {

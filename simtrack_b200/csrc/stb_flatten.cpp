@@ -655,6 +655,18 @@ HostTable flatten_impl(const Line &line, bool spin) {
     t.flops_per_turn += fl;
     t.hdr.push_back(h);
   }
+  // Elements after which the loss test cannot newly fail: thin kicks (x, y
+  // unchanged) without misalignment whose aperture is no tighter than the
+  // previous element's.  The test after the previous element passed, so it
+  // passes again with the same x, y; the kernels skip it.
+  for (size_t i = 1; i < t.hdr.size(); i++) {
+    ElemHeader &h = t.hdr[i];
+    const ElemHeader &q = t.hdr[i - 1];
+    const bool kick = h.op == OP_QUAD_KICK || h.op == OP_SEXT_KICK || h.op == OP_OCT_KICK || h.op == OP_MULT_KICK ||
+                      h.op == OP_BB4D || h.op == OP_IDENTITY;
+    const bool mis = (h.flags & (EF_MISALIGN_OFFSET | EF_MISALIGN_ROLL)) != 0;
+    if (kick && !mis && h.apx >= q.apx && h.apy >= q.apy) h.flags |= EF_NO_LOSS_CHECK;
+  }
   return t;
 }
 

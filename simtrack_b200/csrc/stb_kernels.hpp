@@ -17,8 +17,9 @@ struct TrackVariant {
   int min_blocks;  // __launch_bounds__ minimum resident CTAs per SM
   int ppt;         // particles per thread
   const char *name;
+  bool prefetch;   // next element header loaded while the current element runs
 };
-constexpr int kNumTrackVariants = 9;
+constexpr int kNumTrackVariants = 11;
 extern const TrackVariant kVariants[kNumTrackVariants];
 
 struct TrackArgs {
@@ -31,7 +32,7 @@ struct TrackArgs {
   long n;
   int turn0;   // global index of the first turn of this block
   int nturn;   // turns in this block
-  double r2;   // circular aperture radius squared; 0 disables
+  double r2;   // circular aperture radius squared; +inf when there is none
   int32_t *lost_turn;  // < 0 while alive
   int32_t *lost_elem;
   int *status;  // device status word (STB_OK or an error code)

@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -155,7 +156,7 @@ stb_scan *scan_build(stb_table **tables, int nseed, const double *x0, const long
   a.next_item = s->d_ctr + 1;
   a.turn0 = s->d_ctr + 2;
   a.item_chunk = s->d_ctr + 3;
-  a.r2 = radius > 0.0 ? radius * radius : 0.0;
+  a.r2 = radius > 0.0 ? radius * radius : INFINITY;
   a.status = s->d_status;
   a.tbt = nullptr;
   a.tbt_turns = 0;

@@ -62,7 +62,8 @@ __device__ __noinline__ void spin_rotate(const Particle &x0, const PtCache &c, c
   const double Fabs = sqrt(F0 * F0 + F1 * F1 + F2 * F2);
   const double a0 = F0 / Fabs, a1 = F1 / Fabs, a2 = F2 / Fabs;
   const double theta = -Fabs;
-  const double ct = cr_cos(theta), st = cr_sin(theta);
+  double st, ct;
+  cr_sincos(theta, st, ct);
   const double r0 = a0 * a0 * (1 - ct) + ct;
   const double r1 = a0 * a1 * (1 - ct) - a2 * st;
   const double r2 = a0 * a2 * (1 - ct) + a1 * st;
@@ -327,7 +328,7 @@ __global__ void __launch_bounds__(kBlock, 1) spin_track_kernel(const __grid_cons
           d[0] = p[0].x; d[1] = p[0].px; d[2] = p[0].y; d[3] = p[0].py; d[4] = p[0].z; d[5] = p[0].pt;
           d[6] = s.x; d[7] = s.y; d[8] = s.z;
         }
-        if (is_lost(p[0], h.apx, h.apy, a.r2)) {
+        if (needs_loss_check(h) && is_lost(p[0], h.apx, h.apy, a.r2)) {
           lt = a.turn0 + t;
           le = e;
           break;

@@ -58,6 +58,10 @@ enum : int16_t {
   EF_EDGE2 = 8,            // exit edge focusing present
   EF_FRINGE = 16,          // GP.quad_fringe hard-edge maps around a thick quad
   EF_CHANGES_PT = 32,      // element modifies pt: the pt-only cache is refreshed after it
+  // The loss test after this element cannot fail when it passed after the
+  // previous one: a kick that leaves x and y untouched, no misalignment, an
+  // aperture no tighter than the previous element's.
+  EF_NO_LOSS_CHECK = 64,
 };
 
 struct ElemHeader {

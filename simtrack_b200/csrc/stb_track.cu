@@ -35,9 +35,9 @@ int track_smem_limit(int device) {
 
 // Persistent grid: as many CTAs as fit on the device at once (never more
 // than the particles need); each CTA strides over the particle range.
-template <bool kSmem, int kBlock, int kMinBlocks, int kPPT, bool kDump>
+template <bool kSmem, int kBlock, int kMinBlocks, int kPPT, bool kDump, bool kPF = false>
 static cudaError_t launch_variant(const TrackArgs &a, int num_sms, size_t smem, cudaStream_t stream) {
-  auto kern = track_kernel<kSmem, kBlock, kMinBlocks, kPPT, kDump>;
+  auto kern = track_kernel<kSmem, kBlock, kMinBlocks, kPPT, kDump, kPF>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   int per_sm = 0;
@@ -57,11 +57,12 @@ static cudaError_t launch_variant(const TrackArgs &a, int num_sms, size_t smem, 
 // caps registers per thread at 65536 / (block * min_blocks)) and particles
 // per thread.
 const TrackVariant kVariants[kNumTrackVariants] = {
-    {true, 512, 1, 1, "smem_b512_r128"},       {true, 1024, 1, 1, "smem_b1024_r64"},
-    {true, 768, 1, 1, "smem_b768_r85"},        {false, 256, 2, 1, "l1_b256_r128"},
-    {false, 256, 3, 1, "l1_b256_r80"},         {false, 256, 4, 1, "l1_b256_r64"},
-    {false, 384, 2, 1, "l1_b384_r85"},         {true, 512, 1, 2, "smem_b512_r128_ppt2"},
-    {false, 128, 3, 2, "l1_b128_r168_ppt2"},
+    {true, 512, 1, 1, "smem_b512_r128", false},       {true, 1024, 1, 1, "smem_b1024_r64", false},
+    {true, 768, 1, 1, "smem_b768_r85", false},        {false, 256, 2, 1, "l1_b256_r128", false},
+    {false, 256, 3, 1, "l1_b256_r80", false},         {false, 256, 4, 1, "l1_b256_r64", false},
+    {false, 384, 2, 1, "l1_b384_r85", false},         {true, 512, 1, 2, "smem_b512_r128_ppt2", false},
+    {false, 128, 3, 2, "l1_b128_r168_ppt2", false},   {true, 1024, 1, 1, "smem_b1024_r64_pf", true},
+    {true, 768, 1, 1, "smem_b768_r85_pf", true},
 };
 
 cudaError_t launch_track(const TrackArgs &a, int num_sms, int variant, cudaStream_t stream) {
@@ -80,6 +81,8 @@ cudaError_t launch_track(const TrackArgs &a, int num_sms, int variant, cudaStrea
     case 6: return launch_variant<false, 384, 2, 1, false>(a, num_sms, 0, stream);
     case 7: return launch_variant<true, 512, 1, 2, false>(a, num_sms, sm, stream);
     case 8: return launch_variant<false, 128, 3, 2, false>(a, num_sms, 0, stream);
+    case 9: return launch_variant<true, 1024, 1, 1, false, true>(a, num_sms, sm, stream);
+    case 10: return launch_variant<true, 768, 1, 1, false, true>(a, num_sms, sm, stream);
     default: return cudaErrorInvalidValue;
   }
 }

@@ -72,9 +72,14 @@ __device__ bool stage_table(const TrackArgs &a, unsigned char *smem, uint64_t *b
   return stage_table_ptr(a.hdr, a.nelem, a.pool, a.npool_padded, smem, bar, 0, true);
 }
 
+// Track()'s loss test (simtrack.cpp:20802): |x| > APx, |y| > APy or NaN;
+// !(|x| <= APx) is true for NaN as well.  r2 is the circular aperture radius
+// squared, +inf when there is none.
 __device__ __forceinline__ bool is_lost(const Particle &p, double apx, double apy, double r2) {
-  return fabs(p.x) > apx || fabs(p.y) > apy || isnan(p.x) || isnan(p.y) || (r2 > 0.0 && p.x * p.x + p.y * p.y > r2);
+  return !(fabs(p.x) <= apx) || !(fabs(p.y) <= apy) || p.x * p.x + p.y * p.y > r2;
 }
+
+__device__ __forceinline__ bool needs_loss_check(const ElemHeader &h) { return (h.flags & EF_NO_LOSS_CHECK) == 0; }
 
 // Rarely executed element maps are kept out of line so the hot loop (drift,
 // bend, quadrupole and thin kicks) stays small in the instruction cache and
@@ -346,7 +351,7 @@ __device__ __forceinline__ void store_particle(const TrackArgs &a, long i, const
 // coordinates and loss record stored at once; its slot is then reset to the
 // reference orbit so the remaining particles of the thread keep running on
 // benign operands.
-template <bool kSmem, int kBlock, int kMinBlocks, int kPPT, bool kDump>
+template <bool kSmem, int kBlock, int kMinBlocks, int kPPT, bool kDump, bool kPF = false>
 __global__ void __launch_bounds__(kBlock, kMinBlocks) track_kernel(const __grid_constant__ TrackArgs a) {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ __align__(8) uint64_t bar;
@@ -392,8 +397,17 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) track_kernel(const __grid_
       nalive += alive[k] ? 1 : 0;
     }
     for (int t = 0; t < a.nturn && nalive > 0; t++) {
+      ElemHeader hnext;
+      if (kPF) hnext = hdr[0];
       for (int e = 0; e < a.nelem; e++) {
-        const ElemHeader h = hdr[e];
+        ElemHeader h;
+        if (kPF) {
+          // the next header's shared-memory load overlaps this element's maps
+          h = hnext;
+          if (e + 1 < a.nelem) hnext = hdr[e + 1];
+        } else {
+          h = hdr[e];
+        }
         apply_element<kPPT>(h, pool + h.poff, p, c, R);
 #pragma unroll
         for (int k = 0; k < kPPT; k++) {
@@ -403,7 +417,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) track_kernel(const __grid_
             double *d = a.dump + (((size_t)i * a.nturn + t) * a.nelem + e) * 6;
             d[0] = p[k].x; d[1] = p[k].px; d[2] = p[k].y; d[3] = p[k].py; d[4] = p[k].z; d[5] = p[k].pt;
           }
-          if (is_lost(p[k], h.apx, h.apy, a.r2)) {
+          if (needs_loss_check(h) && is_lost(p[k], h.apx, h.apy, a.r2)) {
             store_particle(a, i, p[k]);
             a.lost_turn[i] = a.turn0 + t;
             a.lost_elem[i] = e;

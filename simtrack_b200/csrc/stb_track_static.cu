@@ -153,7 +153,7 @@ int track_seeds_static(stb_table *const *tables, int nseed, const long *n_per_se
   a.turn0 = sc->ctr + 2;
   a.item_chunk = sc->ctr + 3;
   a.nturn = nturn;
-  a.r2 = radius > 0.0 ? radius * radius : 0.0;
+  a.r2 = radius > 0.0 ? radius * radius : INFINITY;
   a.status = &sc->status;
   a.ntot = total;
   static_init_kernel<<<1, kStaticMaxSeeds, 0, stream>>>(in, sc);
