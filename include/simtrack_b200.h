@@ -157,6 +157,20 @@ int stb_track_seeds_static(stb_table *const *tables, int nseed, const long *n_pe
                            double *y, double *py, double *z, double *pt, int32_t *lost_turn, int32_t *lost_elem,
                            int turn0, int nturn, double aperture_radius, void *stream);
 
+/* Cal_Orbit_Num(line, deltap), simtrack.cpp:14947-15030: 4D closed orbit at
+ * momentum offset deltap (Newton iteration on the GPU one-turn map, RF off);
+ * stores each element's X[] and, when orbit6 is not NULL, writes the orbit
+ * after element j to orbit6[j*6 + k]. */
+int stb_cal_orbit(stb_line *l, double deltap, double *orbit6, int device);
+
+/* Track_DA(line, nturn, deltap0, sigmax0, sigmay0, filename), simtrack.cpp:21389-21441:
+ * the stable amplitude of 10 phase angles by twin-particle bisection, written
+ * to filename as the reference writes it (NULL: no file) and returned in
+ * angles10 / sigma10 (optional).  All reachable bisection midpoints are
+ * tracked in one batched launch, then the bisections are replayed. */
+int stb_track_da(stb_line *l, int nturn, double deltap0, double sigmax0, double sigmay0, const char *filename,
+                 double *angles10, double *sigma10, int device);
+
 /* ---- Track_Radial (simtrack.cpp:21641-21680) ----
  * As stb_track_device / stb_track_host, with z corrected after every element
  * j by the path-length change of the on-momentum reference particle through

@@ -61,6 +61,7 @@ class Element {
   double DX = 0., DY = 0., DS = 0.;
   double DTHETA = 0., DPHI = 0., DPSI = 0.;
   double APx = 1., APy = 1.;
+  double X[6] = {0., 0., 0., 0., 0., 0.};  // closed orbit at the element's exit (simtrack.h:389), see Cal_Orbit_Num
 
   // Parameter access for the flattener (names as accepted by SetP).
   double P(const char *name) const { return GetP(name); }
@@ -242,6 +243,22 @@ void Track(Line &line, double x[], int nturn, int &stable, int &lost_turn, int &
 // DA drivers, simtrack.cpp:21389-21441, moved onto the GPU in one launch).
 void Track_Batch(Line &line, double *x, long n, int nturn, int *stable, int *lost_turn,
                  int *lost_post, const TrackOptions &opt = TrackOptions());
+
+// Track_DA (simtrack.cpp:21389-21441): twin-particle bisection of the stable
+// amplitude at 10 phase angles between 0 and 50 sigma, written to `filename`
+// as the reference writes it ("angle sigma" per line; NULL: no file).  All
+// midpoints the bisections can visit are tracked in one GPU launch and the
+// bisections replayed on the outcomes, which reproduces the reference's file.
+// angles_out / sigma_out (optional) receive the 10 results.
+void Track_DA(Line &line, int nturn, double deltap0, double sigmax0, double sigmay0, const char *filename,
+              double *angles_out = nullptr, double *sigma_out = nullptr, int device = 0);
+
+// Cal_Orbit_Num (simtrack.cpp:14947-15030): 4D closed orbit at momentum
+// offset deltap by Newton iteration on the one-turn map (RF voltages off,
+// one-sided finite differences with step 1e-9, the reference's own matrix
+// inversion), one-turn tracks on the GPU; fills every element's X[] with the
+// orbit after it.  Throws Error(STB_EABORTED) where the reference exits.
+void Cal_Orbit_Num(Line &line, double deltap, int device = 0);
 
 // Read_MADX_Lattice (simtrack.cpp:13591-13791): appends the elements of a
 // MAD-X TFS twiss table (columns NAME KEYWORD S L ANGLE E1 E2 TILT K0L K0SL

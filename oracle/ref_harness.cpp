@@ -168,6 +168,20 @@ void ref_track(void *line, double *x, long n, int nturn, int *stable, int *lost_
   }
 }
 
+// The reference's Cal_Orbit_Num (simtrack.cpp:14947) and the orbit it stores
+// in every element's X[] (orbit6[j*6 + k]).
+void ref_cal_orbit(void *line, double deltap, double *orbit6) {
+  Line &l = *static_cast<Line *>(line);
+  Cal_Orbit_Num(l, deltap);
+  for (long j = 0; j < l.Ncell; j++)
+    for (int k = 0; k < 6; k++) orbit6[j * 6 + k] = l.Cell[j]->X[k];
+}
+
+// The reference's Track_DA (simtrack.cpp:21389-21441), writing `filename`.
+void ref_track_da(void *line, int nturn, double deltap0, double sigmax0, double sigmay0, const char *filename) {
+  Track_DA(*static_cast<Line *>(line), nturn, deltap0, sigmax0, sigmay0, filename);
+}
+
 // n particles through the reference Track_Radial() (simtrack.cpp:21641-21680).
 void ref_track_radial(void *line, double *x, long n, int nturn, int *stable, int *lost_turn, int *lost_post) {
   Line &l = *static_cast<Line *>(line);

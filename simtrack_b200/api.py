@@ -216,7 +216,7 @@ class Line:
             pass
 
 
-NUM_VARIANTS = 9
+NUM_VARIANTS = 11
 
 
 def variant_name(v: int) -> str:
@@ -378,6 +378,25 @@ class SpinTable:
                 lib().stb_table_free(self._h)
         except Exception:
             pass
+
+
+def Cal_Orbit_Num(line: Line, deltap: float = 0.0, device: int = 0) -> np.ndarray:
+    """Cal_Orbit_Num (simtrack.cpp:14947-15030): the closed orbit after every
+    element, [ncell, 6] (also stored in the elements' X fields)."""
+    out = np.empty((line.Ncell, 6))
+    check(lib().stb_cal_orbit(line._h, deltap, out.ctypes.data_as(POINTER(c_double)), device))
+    return out
+
+
+def Track_DA(line: Line, nturn: int, deltap0: float, sigmax0: float, sigmay0: float, filename=None,
+             device: int = 0):
+    """Track_DA (simtrack.cpp:21389-21441): returns (angles_deg[10], sigma[10]);
+    writes the reference's output file when `filename` is given."""
+    ang = (c_double * 10)()
+    sig = (c_double * 10)()
+    check(lib().stb_track_da(line._h, nturn, deltap0, sigmax0, sigmay0,
+                             None if filename is None else str(filename).encode(), ang, sig, device))
+    return np.array(ang[:]), np.array(sig[:])
 
 
 def Track_Radial(line: Line, x, nturn: int, stable: int = 1):

@@ -138,7 +138,7 @@ int track_device(stb_table *t, double *x, double *px, double *y, double *py, dou
   a.n = n;
   a.turn0 = turn0;
   a.nturn = nturn;
-  a.r2 = radius > 0.0 ? radius * radius : 0.0;
+  a.r2 = radius > 0.0 ? radius * radius : INFINITY;
   a.lost_turn = lost_turn;
   a.lost_elem = lost_elem;
   a.dump = dump;
@@ -186,7 +186,7 @@ int autotune(stb_table *t, const double *const in[6], long n, int nturn, double 
         cuda_check(cudaEventRecord(e0), "event");
         TrackArgs a = make_args(t);
         a.x = buf; a.px = buf + m; a.y = buf + 2 * m; a.py = buf + 3 * m; a.z = buf + 4 * m; a.pt = buf + 5 * m;
-        a.n = m; a.turn0 = 1; a.nturn = nturn; a.r2 = radius > 0 ? radius * radius : 0.0;
+        a.n = m; a.turn0 = 1; a.nturn = nturn; a.r2 = radius > 0 ? radius * radius : INFINITY;
         a.lost_turn = lost; a.lost_elem = lost + m; a.dump = nullptr;
         if (launch_track(a, t->num_sms, v, 0) != cudaSuccess) {
           cudaGetLastError();
@@ -297,7 +297,7 @@ int radial_device(stb_table *t, double *x, double *px, double *y, double *py, do
   a.n = n;
   a.turn0 = turn0;
   a.nturn = nturn;
-  a.r2 = radius > 0.0 ? radius * radius : 0.0;
+  a.r2 = radius > 0.0 ? radius * radius : INFINITY;
   a.lost_turn = lost_turn;
   a.lost_elem = lost_elem;
   a.dump = dump;
@@ -375,7 +375,7 @@ int spin_device(stb_table *t, double *const xs[9], long n, int turn0, int nturn,
   a.t.n = n;
   a.t.turn0 = turn0;
   a.t.nturn = nturn;
-  a.t.r2 = radius > 0.0 ? radius * radius : 0.0;
+  a.t.r2 = radius > 0.0 ? radius * radius : INFINITY;
   a.t.lost_turn = lost_turn;
   a.t.lost_elem = lost_elem;
   a.dump = dump;
@@ -553,6 +553,26 @@ int stb_element_geometry(const stb_element *e, double *out10) {
     const Element *x = E(e);
     const double v[10] = {x->L, x->S, x->DX, x->DY, x->DS, x->DTHETA, x->DPHI, x->DPSI, x->APx, x->APy};
     for (int k = 0; k < 10; k++) out10[k] = v[k];
+    return STB_OK;
+  });
+}
+int stb_cal_orbit(stb_line *l, double deltap, double *orbit6, int device) {
+  return guarded([&] {
+    if (!l) throw Error(STB_EINVAL, "NULL line");
+    Line &line = *Lp(l);
+    Cal_Orbit_Num(line, deltap, device);
+    if (orbit6)
+      for (size_t j = 0; j < line.Cell.size(); j++)
+        for (int i = 0; i < 6; i++) orbit6[j * 6 + i] = line.Cell[j]->X[i];
+    return STB_OK;
+  });
+}
+int stb_track_da(stb_line *l, int nturn, double deltap0, double sigmax0, double sigmay0, const char *filename,
+                 double *angles10, double *sigma10, int device) {
+  return guarded([&] {
+    if (!l) throw Error(STB_EINVAL, "NULL line");
+    if (nturn < 0) throw Error(STB_EINVAL, "negative turn count");
+    Track_DA(*Lp(l), nturn, deltap0, sigmax0, sigmay0, filename, angles10, sigma10, device);
     return STB_OK;
   });
 }

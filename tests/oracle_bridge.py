@@ -71,6 +71,8 @@ class RefOracle:
         L.ref_line_read_madx.argtypes = [ctypes.c_char_p]
         L.ref_line_read_madx.restype = c_void_p
         L.ref_line_elem.argtypes = [c_void_p, c_long, ctypes.c_char_p, ctypes.c_char_p, c_int, POINTER(c_double)]
+        L.ref_cal_orbit.argtypes = [c_void_p, c_double, POINTER(c_double)]
+        L.ref_track_da.argtypes = [c_void_p, c_int, c_double, c_double, c_double, ctypes.c_char_p]
         L.ref_track_radial.argtypes = [c_void_p, POINTER(c_double), c_long, c_int, POINTER(c_int), POINTER(c_int),
                                        POINTER(c_int)]
         L.ref_track_spin_dump.argtypes = [c_void_p, POINTER(c_double), c_int, POINTER(c_double), POINTER(c_int),
@@ -163,6 +165,14 @@ class RefOracle:
 
     def getp(self, i: int, name: str) -> float:
         return self.L.ref_line_getp(self.line, i, name.encode())
+
+    def cal_orbit(self, deltap: float) -> np.ndarray:
+        out = np.empty((self.nelem, 6))
+        self.L.ref_cal_orbit(self.line, deltap, out.ctypes.data_as(POINTER(c_double)))
+        return out
+
+    def track_da(self, nturn: int, deltap0: float, sigmax0: float, sigmay0: float, filename: str) -> None:
+        self.L.ref_track_da(self.line, nturn, deltap0, sigmax0, sigmay0, str(filename).encode())
 
     def track_radial(self, x: np.ndarray, nturn: int):
         """Track_Radial over AoS x[n, 6] (copied); returns (x, stable, lost_turn, lost_post)."""

@@ -59,3 +59,19 @@ def test_track_radial_drop_in(native_lib, ref_oracle):
     xo, so, lo, po = ref_oracle.track_radial(np.array([x]), 100)
     assert (st, ltn, lp) == (so[0], lo[0], po[0])
     assert_close(np.array([xs]), xo, "drop-in")
+
+
+def test_track_da_reproduces_reference_file(tmp_path, native_lib, ref_oracle):
+    """Track_DA's output file (10 angles, twin-particle bisection) equals the
+    reference's, byte for byte."""
+    from simtrack_b200.api import Track_DA
+    lat = lt.rhic_like_ring(seed=1)
+    line = lt.build_line(lat)
+    ref_oracle.build(lat)
+    ours, theirs = tmp_path / "da_gpu.dat", tmp_path / "da_ref.dat"
+    sig = lat.meta["sigma_ip"]
+    ang, s = Track_DA(line, 64, 5e-4, sig, sig, ours)
+    ref_oracle.track_da(64, 5e-4, sig, sig, theirs)
+    assert ours.read_text() == theirs.read_text()
+    # the bisections end inside the interval, at different amplitudes per angle
+    assert np.all(s > 1) and np.all(s < 49) and len(set(s.tolist())) > 3
