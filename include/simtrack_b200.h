@@ -53,8 +53,9 @@ int stb_get_ref(double *out8);
 /* ---- elements: `new TYPE(name, args...)`  simtrack.h:399-1059 ----
  * type: "DRIFT","MARKER","SBEND","GSBEND","QUAD","SKEWQ","SEXT","OCT","MULT","GMULT",
  *       "SBENDMULT","KICKER","HKICKER","VKICKER","RFCAV","CRABRF","CCMULT","LBT","ILBT",
- *       "BEAMBEAM","BPM","HBPM","VBPM".
- * args: the constructor arguments after `name`, in constructor order; MULT takes
+ *       "BEAMBEAM","BPM","HBPM","VBPM","SOLEN","PATCH".
+ * args: the constructor arguments after `name`, in constructor order (SOLEN: L, KS;
+ *       PATCH: DX, DY, DS, THETA, simtrack.cpp:9645, 12262); MULT takes
  *       L, KNL[11], KNSL[11] (23 values); GMULT/SBENDMULT take L, ANGLE, E1, E2,
  *       KNL[11], KNSL[11] (26 values); BEAMBEAM takes TREATMENT, NP, BBSCALE, SIGMAL,
  *       NSLICE, EMITX, BETAX, ALFAX, EMITY, BETAY, ALFAY. */
@@ -91,6 +92,9 @@ int stb_line_cell(stb_line *l, long i, stb_element **out); /* Line::Cell[i] (bor
 /* Read_MADX_Lattice(line, filename), simtrack.cpp:13591-13791: appends the
  * elements of a MAD-X TFS twiss table (see include/simtrack_b200.hpp). */
 int stb_line_read_madx(stb_line *l, const char *path);
+/* Read_BMAD_Lattice(line, filename), simtrack.cpp:14054-14244: appends the
+ * elements of a Bmad lattice table (see include/simtrack_b200.hpp). */
+int stb_line_read_bmad(stb_line *l, const char *path);
 
 /* ---- flattening: Line -> device element table ----
  * No reference counterpart: the reference dispatches Element::Pass virtually

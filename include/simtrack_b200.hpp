@@ -164,6 +164,23 @@ class VKICKER : public Element {
  private:
   double VKICK;
 };
+// Solenoid (simtrack.h:576-587): KS = Bs / (B rho) as in MAD-X; one slice.
+class SOLEN : public Element {
+ public:
+  SOLEN(std::string name, double l, double ks);
+ private:
+  double KS;
+};
+// Coordinate patch (simtrack.h:1048-1059): a translation by (DX, DY, DS)
+// followed by a rotation THETA about the y axis.  These are the patch's own
+// parameters (SetP/GetP "DX", "DY", "DS", "THETA"), not the Element
+// misalignment fields, which a patch ignores; L = DS at construction.
+class PATCH : public Element {
+ public:
+  PATCH(std::string name, double dx, double dy, double ds, double theta);
+ private:
+  double PDX, PDY, PDS, THETA;
+};
 class RFCAV : public Element {
  public:
   RFCAV(std::string name, double l, double vrf, double frf, double phase0);
@@ -263,10 +280,18 @@ void Cal_Orbit_Num(Line &line, double deltap, int device = 0);
 // Read_MADX_Lattice (simtrack.cpp:13591-13791): appends the elements of a
 // MAD-X TFS twiss table (columns NAME KEYWORD S L ANGLE E1 E2 TILT K0L K0SL
 // ... K10L K10SL KS) to `line`, mapping keywords to element types as the
-// reference does.  Throws Error(STB_EUNSUPPORTED) for a solenoid with KS != 0
-// or an electron lens (not implemented on the GPU path) and
-// Error(STB_EINVAL) for an unreadable file.
+// reference does.  Throws Error(STB_EUNSUPPORTED) for an electron lens (not
+// implemented on the GPU path) and Error(STB_EINVAL) for an unreadable file.
 void Read_MADX_Lattice(Line &line, const char *filename);
+
+// Read_BMAD_Lattice (simtrack.cpp:14054-14244): appends the elements of a
+// Bmad table (one header line, then rows NAME KEY S L ANGLE ANGLE1 E1 E2 TILT
+// X_OFFSET Z_OFFSET X_PITCH K0L K0SL ... K10L K10SL KS HKICK VKICK) to
+// `line`, mapping keys to element types as the reference does.  Rows whose
+// S column is not a number (column-name and unit lines) are skipped.  Throws
+// Error(STB_EUNSUPPORTED) for an electron lens and Error(STB_EINVAL) for an
+// unreadable file or a beam-beam element of non-zero length.
+void Read_BMAD_Lattice(Line &line, const char *filename);
 
 // Track_Radial() drop-in (simtrack.cpp:21641-21680): Track() with z taken
 // relative to the on-momentum reference particle after every element.

@@ -368,6 +368,89 @@ static void kick_pass(double *x, double L, double hk, double vk, const port_gp *
   drift(x, L / 2.0, gp);
 }
 
+/* SOLEN_Pass, simtrack.cpp:5804-5857, with the solenoid's single slice
+ * (SOLEN's constructor fixes Nint = 1, simtrack.cpp:9645-9660). */
+static void solen_pass(double *x, double L, double KS, const port_gp *gp)
+{
+  const int Nint = 1;
+  double Bz, delta1, gamma1, beta1, ps, vz, K, Lint, theta, sn, cs;
+  double m[4][4], t[4];
+  int i, j, k;
+  if (KS == 0) {
+    drift(x, L, gp);
+    return;
+  }
+  Bz = KS * gp->brho;
+  Lint = L / Nint;
+  delta1 = sqrt(1.0 + 2 * x[5] / gp->beta + x[5] * x[5]) - 1.0;
+  gamma1 = gp->gamma + sqrt(gp->gamma * gp->gamma - 1.) * x[5];
+  beta1 = sqrt(1.0 - 1.0 / gamma1 / gamma1);
+  /* (px, py) -> (x', y') */
+  ps = sqrt((1 + delta1) * (1 + delta1) - x[1] * x[1] - x[3] * x[3]);
+  x[1] = x[1] / ps;
+  x[3] = x[3] / ps;
+  vz = 2.99792458e8 * beta1 / sqrt(1.0 + x[1] * x[1] + x[3] * x[3]);
+  K = gp->q * Bz / 2.0 / gamma1 / gp->m0 / vz;
+  /* entrance fringe */
+  x[1] = x[1] + x[2] * K;
+  x[3] = x[3] - x[0] * K;
+  /* body: rotation in the transverse plane */
+  theta = -2.0 * K * L / Nint;
+  sn = sin(theta);
+  cs = cos(theta);
+  for (i = 0; i < 4; i++)
+    for (j = 0; j < 4; j++) m[i][j] = 0.;
+  m[0][0] = 1.0;
+  m[0][1] = Lint * sn / theta;
+  m[0][3] = -(1 - cs) * Lint / theta;
+  m[1][1] = cs;
+  m[1][3] = -sn;
+  m[2][1] = (1 - cs) * Lint / theta;
+  m[2][2] = 1.;
+  m[2][3] = Lint * sn / theta;
+  m[3][1] = sn;
+  m[3][3] = cs;
+  for (i = 0; i < Nint; i++) {
+    for (k = 0; k < 4; k++) t[k] = x[k];
+    for (k = 0; k < 4; k++) {
+      x[k] = 0.;
+      for (j = 0; j < 4; j++) x[k] = x[k] + m[k][j] * t[j];
+    }
+  }
+  /* exit fringe, then back to (px, py) */
+  x[1] = x[1] - x[2] * K;
+  x[3] = x[3] + x[0] * K;
+  x[1] = gamma1 * gp->m0 * x[1] * vz / gp->p;
+  x[3] = gamma1 * gp->m0 * x[3] * vz / gp->p;
+  x[4] = x[4] - 2.99792458e8 * (L / vz - L / gp->beta / 2.99792458e8);
+}
+
+/* PATCH_Pass, simtrack.cpp:6248-6256: TRANS_Pass (6140-6151), then
+ * YROTAT_Pass (6192-6217), which does nothing for |THETA| < 1e-9. */
+static void patch_pass(double *x, double DX, double DY, double DS, double THETA, const port_gp *gp)
+{
+  double x0, px0, py0, delta1, gamma1, beta1, cosT, sinT, tanT, pz, temp;
+  x[0] = x[0] - DX;
+  x[2] = x[2] - DY;
+  x[4] = x[4] - DS;
+  if (fabs(THETA) < 1.0e-9) return;
+  delta1 = sqrt(1.0 + 2 * x[5] / gp->beta + x[5] * x[5]) - 1.0;
+  gamma1 = gp->gamma + sqrt(gp->gamma * gp->gamma - 1.) * x[5];
+  beta1 = sqrt(1.0 - 1.0 / gamma1 / gamma1);
+  cosT = cos(THETA);
+  sinT = sin(THETA);
+  tanT = tan(THETA);
+  x0 = x[0];
+  px0 = x[1];
+  py0 = x[3];
+  pz = sqrt((1 + delta1) * (1 + delta1) - px0 * px0 - py0 * py0);
+  temp = 1 - px0 * tanT / pz;
+  x[0] = x0 / cosT / temp;
+  x[1] = px0 * cosT + pz * sinT;
+  x[2] = x[2] + py0 * x0 * tanT / pz / temp;
+  x[4] = x[4] - (1 + delta1) * x0 * tanT / pz / temp / beta1;
+}
+
 /* RFCAV_Pass, simtrack.cpp:6002-6012 */
 static void rfcav_pass(double *x, double L, double VRF, double FRF, double PHASE0, const port_gp *gp)
 {
@@ -712,6 +795,10 @@ int port_pass(const port_elem *e, const port_gp *gp, double *x)
     drift(x, e->L, gp);
     return 0;
   }
+  if (e->type == PORT_PATCH) { /* PATCH::Pass 12323: no GtoL */
+    patch_pass(x, e->p[0], e->p[1], e->p[2], e->p[3], gp);
+    return 0;
+  }
   mis = misaligned(e);
   if (mis < 0) return -1;
   if (mis) gtol1(x, e->dx, e->dy, e->dpsi);
@@ -739,6 +826,7 @@ int port_pass(const port_elem *e, const port_gp *gp, double *x)
   case PORT_LBT: lbt_pass(x, e->p[0]); break;
   case PORT_ILBT: ilbt_pass(x, e->p[0]); break;
   case PORT_BEAMBEAM: beambeam_pass(x, e, gp); break;
+  case PORT_SOLEN: solen_pass(x, e->L, e->p[0], gp); break;
   default: return -1;
   }
   if (mis) ltog1(x, e->dx, e->dy, e->dpsi);

@@ -19,7 +19,7 @@ extern "C" {
 enum port_type {
   PORT_DRIFT = 0, PORT_MARKER, PORT_SBEND, PORT_GSBEND, PORT_QUAD, PORT_SKEWQ, PORT_SEXT,
   PORT_OCT, PORT_MULT, PORT_GMULT, PORT_SBENDMULT, PORT_KICKER, PORT_HKICKER, PORT_VKICKER,
-  PORT_RFCAV, PORT_CRABRF, PORT_CCMULT, PORT_LBT, PORT_ILBT, PORT_BEAMBEAM
+  PORT_RFCAV, PORT_CRABRF, PORT_CCMULT, PORT_LBT, PORT_ILBT, PORT_BEAMBEAM, PORT_SOLEN, PORT_PATCH
 };
 
 /* One element in "as constructed" form: the reference constructor's
@@ -43,6 +43,7 @@ typedef struct {
   double Q;
   int quad_fringe;
   int pad;
+  double m0, q, p; /* GP.m0 [kg], GP.q [C], GP.p [kg m/s] (solenoid) */
 } port_gp;
 
 /* Track n particles (AoS x[n*6]) for nturn turns: Track() semantics

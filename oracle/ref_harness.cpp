@@ -63,6 +63,8 @@ Element *make_element(const char *type, const char *name, const double *p, int n
   if (t == "KICKER" && need(3)) return new KICKER(nm, p[0], p[1], p[2]);
   if (t == "HKICKER" && need(2)) return new HKICKER(nm, p[0], p[1]);
   if (t == "VKICKER" && need(2)) return new VKICKER(nm, p[0], p[1]);
+  if (t == "SOLEN" && need(2)) return new SOLEN(nm, p[0], p[1]);
+  if (t == "PATCH" && need(4)) return new PATCH(nm, p[0], p[1], p[2], p[3]);
   if (t == "RFCAV" && need(4)) return new RFCAV(nm, p[0], p[1], p[2], p[3]);
   if (t == "CRABRF" && need(4)) return new CRABRF(nm, p[0], p[1], p[2], p[3]);
   if (t == "CCMULT" && need(12))
@@ -145,6 +147,15 @@ void ref_pass(void *line, long idx, double *x) { static_cast<Line *>(line)->Cell
 void *ref_line_read_madx(const char *path) {
   Line *l = new Line();
   Read_MADX_Lattice(*l, path);
+  return l;
+}
+
+// Read_BMAD_Lattice (simtrack.cpp:14054) into a new Line.  The reference
+// turns a row whose S column is not a number into a drift of an
+// uninitialised length, so callers pass a table without such rows.
+void *ref_line_read_bmad(const char *path) {
+  Line *l = new Line();
+  Read_BMAD_Lattice(*l, path);
   return l;
 }
 

@@ -200,6 +200,10 @@ class Line:
         """Read_MADX_Lattice (simtrack.cpp:13591-13791): appends the elements of a MAD-X TFS table."""
         check(lib().stb_line_read_madx(self._h, str(path).encode()))
 
+    def read_bmad(self, path: str) -> None:
+        """Read_BMAD_Lattice (simtrack.cpp:14054-14244): appends the elements of a Bmad lattice table."""
+        check(lib().stb_line_read_bmad(self._h, str(path).encode()))
+
     def Cell(self, i: int) -> Element:
         h = c_void_p()
         check(lib().stb_line_cell(self._h, i, byref(h)))

@@ -53,6 +53,8 @@ Element *make_element(const char *type, const char *name, const double *a, int n
   if (t == "KICKER") { need(3); return new KICKER(nm, a[0], a[1], a[2]); }
   if (t == "HKICKER") { need(2); return new HKICKER(nm, a[0], a[1]); }
   if (t == "VKICKER") { need(2); return new VKICKER(nm, a[0], a[1]); }
+  if (t == "SOLEN") { need(2); return new SOLEN(nm, a[0], a[1]); }
+  if (t == "PATCH") { need(4); return new PATCH(nm, a[0], a[1], a[2], a[3]); }
   if (t == "RFCAV") { need(4); return new RFCAV(nm, a[0], a[1], a[2], a[3]); }
   if (t == "CRABRF") { need(4); return new CRABRF(nm, a[0], a[1], a[2], a[3]); }
   if (t == "CCMULT") {
@@ -580,6 +582,14 @@ int stb_line_read_madx(stb_line *l, const char *path) {
   return guarded([&] {
     if (!l || !path) throw Error(STB_EINVAL, "NULL argument");
     Read_MADX_Lattice(*Lp(l), path);
+    return STB_OK;
+  });
+}
+
+int stb_line_read_bmad(stb_line *l, const char *path) {
+  return guarded([&] {
+    if (!l || !path) throw Error(STB_EINVAL, "NULL argument");
+    Read_BMAD_Lattice(*Lp(l), path);
     return STB_OK;
   });
 }

@@ -247,6 +247,25 @@ SBENDMULT::SBENDMULT(std::string name, double l, double angle, double e1, double
 }
 
 // KICKER / HKICKER / VKICKER, simtrack.cpp:9912-10100
+// SOLEN, simtrack.cpp:9645-9686 (Nint fixed at 1; only KS is settable)
+SOLEN::SOLEN(std::string name, double l, double ks) : Element(std::move(name)), KS(ks) {
+  require(l > 0, "Solenoid: L must be positive. ");
+  TYPE = "SOLEN";
+  L = l;
+  add_param("KS", &KS);
+}
+
+// PATCH, simtrack.cpp:12262-12321
+PATCH::PATCH(std::string name, double dx, double dy, double ds, double theta)
+    : Element(std::move(name)), PDX(dx), PDY(dy), PDS(ds), THETA(theta) {
+  TYPE = "PATCH";
+  L = ds;
+  add_param("DX", &PDX);
+  add_param("DY", &PDY);
+  add_param("DS", &PDS);
+  add_param("THETA", &THETA);
+}
+
 KICKER::KICKER(std::string name, double l, double hkick, double vkick)
     : Element(std::move(name)), HKICK(hkick), VKICK(vkick) {
   require(l >= 0, "Error: KICKER length should be non-negative.");

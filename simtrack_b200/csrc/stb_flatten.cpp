@@ -145,6 +145,24 @@ namespace {
 // direction vector, field terms, rotation matrix and product, cos + sin.
 const double kFlSpin = 110;
 
+// One solenoid slice with its entry and exit conversions (SOLEN_Pass).
+const double kFlSolen = 76;
+
+// Parameters of SOLEN_Pass / SOLEN_sPass for KS != 0 (simtrack.cpp:5804-5857,
+// 8118-8183): Bz is KS*brho in Pass and KS*brho/L in sPass.  The solenoid's
+// slice count is fixed at 1 by its constructor (simtrack.cpp:9645-9660).
+void solen_params(Builder &B, const Element &E, double Bz, bool spin) {
+  const double L = E.L, Nint = 1.0, Lint = L / Nint;
+  B.push(GP.q * Bz / 2.0);
+  B.push(L);
+  B.push(Nint);
+  B.push(Lint);
+  B.push(L / GP.beta / 2.99792458e8);
+  B.push(GP.m0);
+  B.push(GP.p);
+  if (spin) B.push(Bz * Lint / GP.brho);
+}
+
 // Element::sPass forms that differ from Pass (simtrack.cpp:8436-11213).
 // Returns false when the element's sPass is its Pass (the caller then emits
 // the orbit form).  Parameter layouts are documented in stb_spin.cuh.
@@ -295,6 +313,16 @@ bool spin_form(Builder &B, const Element &E, ElemHeader &h, double &fl) {
     }
     return true;
   }
+  if (T == "SOLEN") {
+    // SOLEN_sPass 8118-8183; KS == 0 is DRIFT_Pass, the orbit form
+    const double KS = E.GetP("KS");
+    if (KS == 0) return false;
+    h.op = OP_S_SOLEN;
+    h.nint = 1;
+    solen_params(B, E, KS * GP.brho / E.L, true);
+    fl += kFlSolen + kFlSpin;
+    return true;
+  }
   if (T == "KICKER" || T == "HKICKER" || T == "VKICKER") {
     // KICK_sPass 8193-8208
     double hk = 0., vk = 0.;
@@ -338,7 +366,9 @@ HostTable flatten_impl(const Line &line, bool spin) {
     // GtoL dispatch (simtrack.cpp:3701-3741).  DRIFT and MARKER never call it,
     // nor do LBT::sPass and ILBT::sPass (11004, 11053) in spin tracking.
     const bool straight_drift = (T == "DRIFT" || T == "MARKER" || T == "BPM" || T == "HBPM" || T == "VBPM");
-    const bool no_gtol = straight_drift || (spin && (T == "LBT" || T == "ILBT"));
+    // PATCH::Pass/sPass (12323-12333) apply the patch alone: its DX, DY, DS
+    // are the patch's own offsets, not a misalignment.
+    const bool no_gtol = straight_drift || T == "PATCH" || (spin && (T == "LBT" || T == "ILBT"));
     if (!no_gtol) {
       double s = std::fabs(E.DX) + std::fabs(E.DY) + std::fabs(E.DS) + std::fabs(E.DTHETA) +
                  std::fabs(E.DPHI) + std::fabs(E.DPSI);
@@ -370,6 +400,32 @@ HostTable flatten_impl(const Line &line, bool spin) {
       as_drift(E.L);  // DRIFT::Pass 8426, MARKER::Pass 10617, BPM/HBPM/VBPM::Pass 10497-10579
     } else if (spin && spin_form(B, E, h, fl)) {
       // Element::sPass form emitted by spin_form
+    } else if (T == "PATCH") {
+      // PATCH_Pass, simtrack.cpp:6248-6256 (also PATCH::sPass)
+      const double th = E.GetP("THETA");
+      h.op = OP_PATCH;
+      B.push(E.GetP("DX"));
+      B.push(E.GetP("DY"));
+      B.push(E.GetP("DS"));
+      fl += 3;
+      if (!(std::fabs(th) < 1.0e-9)) {  // YROTAT_Pass returns early below 1e-9 (6195)
+        h.aux = 1;
+        B.push(std::cos(th));
+        B.push(std::sin(th));
+        B.push(std::tan(th));
+        fl += 22;
+      }
+    } else if (T == "SOLEN") {
+      // SOLEN::Pass, simtrack.cpp:9688-9692; KS == 0 is DRIFT_Pass (5811-5814)
+      const double KS = E.GetP("KS");
+      if (KS == 0) {
+        as_drift(E.L);
+      } else {
+        h.op = OP_SOLEN;
+        h.nint = 1;
+        solen_params(B, E, KS * GP.brho, false);
+        fl += kFlSolen;
+      }
     } else if (T == "SBEND") {
       // SBEND_Pass, simtrack.cpp:4693-4752
       const double L = E.L, Angle = E.GetP("ANGLE"), E1 = E.GetP("E1"), E2 = E.GetP("E2");

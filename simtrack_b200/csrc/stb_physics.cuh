@@ -419,4 +419,63 @@ static __device__ __noinline__ void ccmult_kick(Particle &p, const double *P) {
   p.pt = pt;
 }
 
+// PATCH_Pass, simtrack.cpp:6248-6256: TRANS_Pass (6140-6151) then, when
+// |THETA| >= 1e-9, YROTAT_Pass (6192-6217).  P = [DX, DY, DS, cos, sin, tan].
+__device__ __forceinline__ void patch_map(Particle &p, const PtCache &c, const double *P, bool rotate) {
+  p.x = p.x - P[0];
+  p.y = p.y - P[1];
+  p.z = p.z - P[2];
+  if (!rotate) return;
+  const double cosT = P[3], sinT = P[4], tanT = P[5];
+  const double x0 = p.x, px0 = p.px, py0 = p.py;
+  const double pz = sqrt(c.opd2 - px0 * px0 - py0 * py0);
+  const double temp = 1 - px0 * tanT / pz;
+  p.x = x0 / cosT / temp;
+  p.px = px0 * cosT + pz * sinT;
+  p.y = p.y + py0 * x0 * tanT / pz / temp;
+  p.z = p.z - c.opd * x0 * tanT / pz / temp / c.beta1;
+}
+
+// Solenoid body shared by SOLEN_Pass (simtrack.cpp:5804-5857) and
+// SOLEN_sPass (8118-8183), KS != 0: hard-edge entrance kick, Nint slices of
+// the 4x4 rotation matrix in (x, x', y, y'), exit kick, path length.
+// P = [q*Bz/2, L, Nint, L/Nint, L/beta/c, m0, p0 (, Bz*Lint/brho for spin)].
+// `slice(xt, px, py)` is called before every slice with the slice's entry
+// state and its momenta converted back to (px, py), as SOLEN_sPass feeds
+// spin().
+template <class SliceHook>
+__device__ __forceinline__ void solen_map(Particle &p, const PtCache &c, const RefConsts &R, const double *P, int nint,
+                                          SliceHook slice) {
+  const double qb2 = P[0], L = P[1], fnint = P[2], Lint = P[3], Lbc = P[4], m0 = P[5], p0 = P[6];
+  const double gamma1 = R.gamma + R.sqrt_g2m1 * p.pt;
+  const double ps = sqrt(c.opd2 - p.px * p.px - p.py * p.py);
+  double x0 = p.x, x1 = p.px / ps, x2 = p.y, x3 = p.py / ps;
+  const double vz = 2.99792458e8 * c.beta1 / sqrt(1.0 + x1 * x1 + x3 * x3);
+  const double K = qb2 / gamma1 / m0 / vz;
+  x1 = x1 + x2 * K;
+  x3 = x3 - x0 * K;
+  const double theta = -2.0 * K * L / fnint;
+  double st, ct;
+  cr_sincos(theta, st, ct);
+  const double m01 = Lint * st / theta, m03 = -(1 - ct) * Lint / theta;
+  const double m21 = (1 - ct) * Lint / theta, m23 = Lint * st / theta;
+  const double m11 = ct, m13 = -st, m31 = st, m33 = ct;
+  for (int i = 0; i < nint; i++) {
+    const double t0 = x0, t1 = x1, t2 = x2, t3 = x3;
+    slice(t0, t1, t2, t3, gamma1, vz);
+    // the reference's 4x4 product, zero and unit entries included
+    x0 = 0. + 1.0 * t0 + m01 * t1 + 0. * t2 + m03 * t3;
+    x1 = 0. + 0. * t0 + m11 * t1 + 0. * t2 + m13 * t3;
+    x2 = 0. + 0. * t0 + m21 * t1 + 1. * t2 + m23 * t3;
+    x3 = 0. + 0. * t0 + m31 * t1 + 0. * t2 + m33 * t3;
+  }
+  x1 = x1 - x2 * K;
+  x3 = x3 + x0 * K;
+  p.x = x0;
+  p.y = x2;
+  p.px = gamma1 * m0 * x1 * vz / p0;
+  p.py = gamma1 * m0 * x3 * vz / p0;
+  p.z = p.z - 2.99792458e8 * (L / vz - Lbc);
+}
+
 }  // namespace stb

@@ -20,6 +20,7 @@
 //                        Angle/Nint, Angle/L, Angle, Nint]                              aux = Norder
 //   OP_S_BENDMULT_KICK  [block(KNL), Angle]                                             aux = Norder
 //   OP_S_KICK           [L/2, L/2/b, HKICK, VKICK]
+//   OP_S_SOLEN          [q*Bz/2, L, Nint, L/Nint, L/beta/c, m0, p0, Bz*(L/Nint)/brho]  (Bz = KS*brho/L)
 // where a block is [KNL0, KNSL0, (KNLi, KNSLi, 1/i!) i = 1..Norder].
 #include <cuda_runtime.h>
 
@@ -265,6 +266,18 @@ __device__ __noinline__ void spin_element(const ElemHeader &h, const double *P, 
       p.px = p.px + P[2];
       p.py = p.py + P[3];
       drift(p, c, P[0], P[1]);
+      break;
+    }
+    case OP_S_SOLEN: {
+      // SOLEN_sPass, simtrack.cpp:8118-8183: before every slice the spin turns
+      // about the longitudinal field integrated over the slice, with the
+      // slice's entry state (momenta converted back to px, py).
+      const double m0 = P[5], p0 = P[6], B2 = P[7];
+      const double z = p.z, pt = p.pt;
+      solen_map(p, c, R, P, h.nint, [&](double t0, double t1, double t2, double t3, double gamma1, double vz) {
+        const Particle xs{t0, gamma1 * m0 * t1 * vz / p0, t2, gamma1 * m0 * t3 * vz / p0, z, pt};
+        spin_rotate(xs, c, R, 0., 0., 0., 0., B2, s);
+      });
       break;
     }
     default:

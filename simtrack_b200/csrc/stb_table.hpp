@@ -36,17 +36,20 @@ enum Op : int32_t {
   OP_BB6D = 18,      // BB6D                          simtrack.cpp:6579-6678
   OP_BB4D = 19,      // BEAMBEAM_Pass treatment 4     simtrack.cpp:7348-7353
   OP_IDENTITY = 20,  // element whose Pass is a no-op (BEAMBEAM with NP == 0)
+  OP_PATCH = 21,     // PATCH_Pass: TRANS_Pass + YROTAT_Pass simtrack.cpp:6140-6151, 6192-6217, 6248-6256
+  OP_SOLEN = 22,     // SOLEN_Pass, KS != 0           simtrack.cpp:5804-5857
   // Spin-tracking forms (Element::sPass), used only in tables flattened for
   // spin; every other element's sPass equals its Pass (or a drift).
-  OP_S_SBEND = 21,          // SBEND_sPass exact branch          simtrack.cpp:7486-7536
-  OP_S_MPOLE_THICK = 22,    // QUAD/SEXT/OCT_sPass slices (aux = order) 7538-7698
-  OP_S_MPOLE_KICK = 23,     // their L == 0 branches
-  OP_S_MULT_THICK = 24,     // MULT_sPass                        7700-7740
-  OP_S_MULT_KICK = 25,      // MULT_sPass L == 0
-  OP_S_BENDMULT = 26,       // SBENDMULT_sPass exact branch      7836-7928
-  OP_S_BENDMULT_KICK = 27,  // SBENDMULT_sPass L == 0
-  OP_S_KICK = 28,           // KICK_sPass                        8193-8208
-  OP_COUNT = 29
+  OP_S_SBEND = 23,          // SBEND_sPass exact branch          simtrack.cpp:7486-7536
+  OP_S_MPOLE_THICK = 24,    // QUAD/SEXT/OCT_sPass slices (aux = order) 7538-7698
+  OP_S_MPOLE_KICK = 25,     // their L == 0 branches
+  OP_S_MULT_THICK = 26,     // MULT_sPass                        7700-7740
+  OP_S_MULT_KICK = 27,      // MULT_sPass L == 0
+  OP_S_BENDMULT = 28,       // SBENDMULT_sPass exact branch      7836-7928
+  OP_S_BENDMULT_KICK = 29,  // SBENDMULT_sPass L == 0
+  OP_S_KICK = 30,           // KICK_sPass                        8193-8208
+  OP_S_SOLEN = 31,          // SOLEN_sPass, KS != 0              8118-8183
+  OP_COUNT = 32
 };
 constexpr int16_t OP_S_FIRST = OP_S_SBEND;
 

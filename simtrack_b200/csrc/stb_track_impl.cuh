@@ -212,6 +212,12 @@ __device__ __noinline__ void op_misc(const ElemHeader &h, const double *P, Parti
       p.py = p.py + Dpy * P[3];
       break;
     }
+    case OP_PATCH:
+      patch_map(p, c, P, h.aux != 0);
+      break;
+    case OP_SOLEN:
+      solen_map(p, c, R, P, h.nint, [](double, double, double, double, double, double) {});
+      break;
     default:  // OP_IDENTITY
       break;
   }

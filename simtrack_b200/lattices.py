@@ -51,6 +51,8 @@ class Lattice:
 def _length(e: ElementSpec) -> float:
     if e.type in ("LBT", "ILBT", "BEAMBEAM"):
         return 0.0
+    if e.type == "PATCH":
+        return float(e.args[2])  # L = DS (PATCH constructor, simtrack.cpp:12266)
     return float(e.args[0])
 
 
@@ -412,6 +414,10 @@ def specs_from_line(line: api.Line) -> List[ElementSpec]:
         elif t == "BEAMBEAM":
             args = tuple(P(n) for n in ("TREATMENT", "NP", "BBSCALE", "SIGMAL", "NSLICE", "EMITX", "BETAX", "ALFAX",
                                         "EMITY", "BETAY", "ALFAY"))
+        elif t == "SOLEN":
+            args = (g["L"], P("KS"))
+        elif t == "PATCH":
+            args = (P("DX"), P("DY"), P("DS"), P("THETA"))
         else:
             raise ValueError(f"specs_from_line: element type {t} not handled")
         mis = (g["DX"], g["DY"], g["DS"], g["DTHETA"], g["DPHI"], g["DPSI"])

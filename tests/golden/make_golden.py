@@ -6,7 +6,9 @@ reference source in place).  For each fixture lattice it records, per
 particle, Track()'s loss outputs and the six coordinates after every element
 for a few sampled turns, as produced by the reference's own element Pass
 functions.  The fixtures let the C restatement be pinned on machines where
-the reference cannot be built.
+the reference cannot be built.  It also copies the reference's Example2 HSR
+lattice table and its printed closed orbit (compressed) and records the
+reference's closed orbit for that table.
 
 Usage: python tests/golden/make_golden.py
 """
@@ -65,9 +67,51 @@ def tune_signals(n: int = 512, count: int = 12, seed: int = 7):
 TUNE_WINDOWS = [(0.2, 0.45, False), (0.0, 0.5, False), (0.0, 1.0, True)]
 
 
+# The reference's Example2 inputs: the HSR lattice as a Bmad table and the
+# closed orbit the reference printed for it (Print_Orbit after Cal_Optics).
+EXAMPLE2 = Path("/root/reference/Example2")
+HSR_ENERGY = (275000. / 938.27201, 938.27201, 1.0, 1.0)  # Set_RefPartEnergy, Example2/DA_cal.cpp:613
+
+
+def numeric_rows(text: str) -> str:
+    """The table without rows whose S column is not a number (its
+    column-name and unit lines), which the reference's reader would turn
+    into drifts of an undefined length."""
+    rows = text.splitlines(True)
+    keep = [rows[0]]
+    for r in rows[1:]:
+        t = r.split()
+        try:
+            float(t[2])
+        except (IndexError, ValueError):
+            continue
+        keep.append(r)
+    return "".join(keep)
+
+
+def hsr_fixtures(ref) -> None:
+    """Compressed copies of Example2's Bmad table and orbit0.dat, and the
+    reference's own Read_BMAD_Lattice + Cal_Orbit_Num(0) on that table."""
+    import lzma
+    import tempfile
+    tab = (EXAMPLE2 / "SimTrack_hsr_base_forIRerr.tab").read_text()
+    (HERE / "hsr_bmad.tab.xz").write_bytes(lzma.compress(tab.encode(), preset=9))
+    (HERE / "hsr_orbit0.dat.xz").write_bytes(lzma.compress((EXAMPLE2 / "orbit0.dat").read_bytes(), preset=9))
+    with tempfile.TemporaryDirectory() as d:
+        path = Path(d) / "hsr.tab"
+        path.write_text(numeric_rows(tab))
+        ref.L.ref_set_ref_energy(*HSR_ENERGY)
+        ref.L.ref_set_flags(0, 0)
+        ref.read_bmad(str(path))
+        orbit = ref.cal_orbit(0.0)
+    np.savez_compressed(HERE / "hsr_orbit_ref.npz", orbit=orbit, energy=np.array(HSR_ENERGY))
+    print("wrote hsr fixtures")
+
+
 def main():
     from oracle_bridge import RefOracle
     ref = RefOracle()
+    hsr_fixtures(ref)
     xs, pxs = tune_signals()
     tunes = np.array([[ref.fine_tune(x, px if w else None, lo, hi) for lo, hi, w in TUNE_WINDOWS]
                       for x, px in zip(xs, pxs)])

@@ -87,6 +87,30 @@ def spin_zoo() -> Lattice:
     return lat
 
 
+def patch_solen_zoo() -> Lattice:
+    """Coordinate patches and solenoids, arranged as around the detector
+    solenoid of the Bmad HSR table (rotate, solenoid, translate back, rotate
+    back), plus a solenoid with KS == 0, a misaligned one, a patch with both
+    offsets and a rotation, and one whose rotation is below YROTAT_Pass's
+    1e-9 threshold."""
+    els = [
+        S("QUAD", "q1", (1.0, 0.08, 0.0), {"Nint": 4}),
+        S("PATCH", "pb", (0.0, 0.0, 0.0, -0.025)),
+        S("SOLEN", "sol", (2.0, 0.15)),
+        S("PATCH", "pe", (-0.05, 1e-4, -6.25e-4, 0.0)),
+        S("PATCH", "pr", (0.0, 0.0, 0.0, 0.025)),
+        S("SOLEN", "sol0", (1.5, 0.0)),
+        S("SOLEN", "solm", (0.8, -0.3), misalign=(1e-4, -2e-4, 0.0, 0.0, 0.0, 2e-3)),
+        S("PATCH", "pm", (2e-4, -1e-4, 3e-4, 1e-3)),
+        S("PATCH", "ptiny", (0.0, 0.0, 0.0, 5e-10)),
+        S("DRIFT", "d1", (0.5,)),
+        S("QUAD", "q2", (1.0, -0.08, 0.0), {"Nint": 4}),
+    ]
+    lat = Lattice("patch_solen", els, 275000.0 / 938.27201)
+    lat.meta["turns"] = 3
+    return lat
+
+
 def spin_particles():
     """zoo_particles with a spin unit vector appended to each."""
     import numpy as np

@@ -27,7 +27,8 @@ REF_CR_SO = ROOT / "oracle" / "_ref" / "libsimtrack_ref_cr.so"
 PORT_SO = ROOT / "oracle" / "_build" / "libsimtrack_port.so"
 
 PORT_TYPES = ["DRIFT", "MARKER", "SBEND", "GSBEND", "QUAD", "SKEWQ", "SEXT", "OCT", "MULT", "GMULT",
-              "SBENDMULT", "KICKER", "HKICKER", "VKICKER", "RFCAV", "CRABRF", "CCMULT", "LBT", "ILBT", "BEAMBEAM"]
+              "SBENDMULT", "KICKER", "HKICKER", "VKICKER", "RFCAV", "CRABRF", "CCMULT", "LBT", "ILBT", "BEAMBEAM",
+              "SOLEN", "PATCH"]
 
 
 def ref_available(cr: bool = False) -> bool:
@@ -70,6 +71,8 @@ class RefOracle:
                                      POINTER(c_int)]
         L.ref_line_read_madx.argtypes = [ctypes.c_char_p]
         L.ref_line_read_madx.restype = c_void_p
+        L.ref_line_read_bmad.argtypes = [ctypes.c_char_p]
+        L.ref_line_read_bmad.restype = c_void_p
         L.ref_line_elem.argtypes = [c_void_p, c_long, ctypes.c_char_p, ctypes.c_char_p, c_int, POINTER(c_double)]
         L.ref_cal_orbit.argtypes = [c_void_p, c_double, POINTER(c_double)]
         L.ref_track_da.argtypes = [c_void_p, c_int, c_double, c_double, c_double, ctypes.c_char_p]
@@ -154,6 +157,15 @@ class RefOracle:
         self.nelem = int(self.L.ref_line_ncell(self.line))
         self.radius = 0.0
 
+    def read_bmad(self, path: str) -> None:
+        """Replaces the line by the reference's Read_BMAD_Lattice of `path`
+        (must exist and hold no row with a non-numeric S column)."""
+        if self.line:
+            self.L.ref_line_free(self.line)
+        self.line = self.L.ref_line_read_bmad(str(path).encode())
+        self.nelem = int(self.L.ref_line_ncell(self.line))
+        self.radius = 0.0
+
     def element(self, i: int):
         """(TYPE, NAME, {L, S, DX, DY, DS, DTHETA, DPHI, DPSI, APx, APy}) of element i."""
         t = ctypes.create_string_buffer(256)
@@ -215,7 +227,8 @@ class PortElem(ctypes.Structure):
 
 class PortGP(ctypes.Structure):
     _fields_ = [("gamma", c_double), ("beta", c_double), ("energy", c_double), ("brho", c_double),
-                ("G", c_double), ("Q", c_double), ("quad_fringe", c_int), ("pad", c_int)]
+                ("G", c_double), ("Q", c_double), ("quad_fringe", c_int), ("pad", c_int),
+                ("m0", c_double), ("q", c_double), ("p", c_double)]
 
 
 def _norder(knl, knsl):
@@ -243,7 +256,11 @@ class PortOracle:
         beta = math.sqrt(1.0 - 1.0 / gamma / gamma)
         energy = gamma * E0
         brho = 3.33564095198 * beta * (energy / 1000) / int(Q)
-        self.gp = PortGP(gamma, beta, energy, brho, 1.7928474, float(int(Q)), int(lat.quad_fringe), 0)
+        # m0, q, p as Set_RefPartEnergy computes them (the solenoid needs them)
+        m0 = E0 * 1.0e6 * 1.6021765e-19 / 299792458. / 299792458.
+        q = Q * 1.6021765e-19
+        p = energy * beta * 1.0e6 * 1.6021765e-19 / 299792458.
+        self.gp = PortGP(gamma, beta, energy, brho, 1.7928474, float(int(Q)), int(lat.quad_fringe), 0, m0, q, p)
         n = len(lat.elements)
         arr = (PortElem * n)()
         for i, e in enumerate(lat.elements):
@@ -272,6 +289,10 @@ class PortOracle:
                     pe.knsl[k] = a[12 + k]
                 pe.norder = _norder(a[1:12], a[12:23])
                 pe.nint = int(a[0] / 0.05) + 1
+            elif t == "PATCH":
+                pe.L = a[2]  # PATCH: L = DS (simtrack.cpp:12266)
+                for k, v in enumerate(a):
+                    pe.p[k] = v
             elif t in ("GMULT", "SBENDMULT"):
                 pe.L = a[0]
                 pe.p[0], pe.p[1], pe.p[2] = a[1], a[2], a[3]

@@ -14,7 +14,7 @@ from pathlib import Path
 import numpy as np
 import pytest
 
-from lattice_zoo import zoo, zoo_particles
+from lattice_zoo import patch_solen_zoo, zoo, zoo_particles
 from simtrack_b200.lattices import fodo_ring
 
 GOLDEN = Path(__file__).resolve().parent / "golden"
@@ -61,10 +61,12 @@ def _same(a, b):
     return np.array_equal(np.nan_to_num(a, nan=7.0), np.nan_to_num(b, nan=7.0))
 
 
-@pytest.mark.parametrize("which", ["zoo", "fodo"])
+@pytest.mark.parametrize("which", ["zoo", "fodo", "patch_solen"])
 def test_port_matches_reference_every_element(which, ref_oracle, port_oracle):
     if which == "zoo":
         lat, X, nturn = zoo(), zoo_particles(), 3
+    elif which == "patch_solen":
+        lat, X, nturn = patch_solen_zoo(), zoo_particles(), 3
     else:
         lat = fodo_ring()
         X = np.array([[1e-3, 0, 5e-4, 0, 0, 0], [4e-3, 1e-5, -3e-3, 0, 0.01, 5e-4]])

@@ -1,7 +1,14 @@
 """Read_MADX_Lattice (simtrack.cpp:13591-13791): the reader against the
 reference's own reader, on the RHIC lattice shipped with the reference
 (Example1/parameters_input, 6,858 elements; read in place, CPU only) and on
-tables written by lattices.write_madx_tfs, and tracking through what was read."""
+tables written by lattices.write_madx_tfs, and tracking through what was read.
+
+Read_BMAD_Lattice (simtrack.cpp:14054-14244): the reader against the
+reference's own reader on the HSR table of the reference's Example2
+(tests/golden/hsr_bmad.tab.xz, 2,836 elements with patches and solenoids),
+and against the element names and S positions of the orbit the reference
+printed for it (tests/golden/hsr_orbit0.dat.xz)."""
+import lzma
 from pathlib import Path
 
 import numpy as np
@@ -23,7 +30,30 @@ PARAMS = {
     "VKICKER": ("VKICK",),
     "KICKER": ("HKICK", "VKICK"),
     "RFCAV": ("VRF", "FRF", "PHASE0"),
+    "SOLEN": ("KS",),
+    "PATCH": ("DX", "DY", "DS", "THETA"),
 }
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+HSR_ENERGY = (275000. / 938.27201, 938.27201, 1.0, 1.0)  # Example2/DA_cal.cpp:613
+
+
+def hsr_table(tmp_path, numeric_only=False) -> Path:
+    """The Example2 Bmad table written to tmp_path (optionally without the
+    column-name and unit rows, which the reference's reader cannot take)."""
+    from golden.make_golden import numeric_rows
+    text = lzma.decompress((GOLDEN / "hsr_bmad.tab.xz").read_bytes()).decode()
+    path = tmp_path / ("hsr_numeric.tab" if numeric_only else "hsr.tab")
+    path.write_text(numeric_rows(text) if numeric_only else text)
+    return path
+
+
+def hsr_orbit0():
+    """(names, types, S, orbit[n, 6]) printed by the reference (6 digits)."""
+    rows = lzma.decompress((GOLDEN / "hsr_orbit0.dat.xz").read_bytes()).decode().splitlines()[1:]
+    t = [r.split() for r in rows]
+    return ([r[0] for r in t], [r[1] for r in t], np.array([float(r[2]) for r in t]),
+            np.array([[float(v) for v in r[3:9]] for r in t]))
 
 
 def compare_lines(line, ref):
@@ -112,3 +142,52 @@ def test_gpu_tracking_through_read_table(tmp_path, native_lib, ref_oracle):
     ok = sg == 1
     floor = np.maximum(np.sqrt(np.mean(xr[ok] ** 2, axis=0)), 1e-300)
     assert np.all(np.abs(xg[ok] - xr[ok]) <= 1e-12 * np.maximum(np.abs(xr[ok]), floor))
+
+
+def test_bmad_reader_matches_reference(tmp_path, ref_oracle):
+    api.Set_RefPartEnergy(*HSR_ENERGY)
+    ref_oracle.L.ref_set_ref_energy(*HSR_ENERGY)
+    line = api.Line()
+    line.read_bmad(str(hsr_table(tmp_path)))
+    ref_oracle.read_bmad(str(hsr_table(tmp_path, numeric_only=True)))
+    compare_lines(line, ref_oracle)
+    types = [line.Cell(i).TYPE for i in range(line.Ncell)]
+    assert types.count("PATCH") == 34 and types.count("SOLEN") == 2
+
+
+def test_bmad_reader_against_printed_orbit_table(tmp_path):
+    """Names, count and S positions of the elements equal the reference's
+    printed table (6 significant digits).  That table came from an older
+    reader: monitors and solenoids (KS = 0, a drift either way) print as
+    DRIFT there."""
+    api.Set_RefPartEnergy(*HSR_ENERGY)
+    line = api.Line()
+    line.read_bmad(str(hsr_table(tmp_path)))
+    names, types, S, _ = hsr_orbit0()
+    assert line.Ncell == len(names) == 2836
+    assert [line.Cell(i).NAME for i in range(line.Ncell)] == names
+    ours = [line.Cell(i).TYPE for i in range(line.Ncell)]
+    for a, b in zip(ours, types):
+        assert a == b or (a in ("BPM", "SOLEN") and b == "DRIFT"), (a, b)
+    s = np.array([line.Cell(i).geometry()["S"] for i in range(line.Ncell)])
+    assert np.all(np.abs(s - S) <= 5e-6 * np.abs(S) + 1e-9)
+
+
+def test_bmad_read_line_tracks_like_reference(tmp_path, ref_oracle, port_oracle):
+    """The C restatement on the line our reader built equals the reference's
+    Track() on the line the reference's reader built, through every element
+    of the HSR table (patches and solenoids included), bit for bit."""
+    api.Set_RefPartEnergy(*HSR_ENERGY)
+    line = api.Line()
+    line.read_bmad(str(hsr_table(tmp_path)))
+    lat = lt.Lattice("hsr", lt.specs_from_line(line), HSR_ENERGY[0])
+    port_oracle.build(lat)
+    ref_oracle.L.ref_set_ref_energy(*HSR_ENERGY)
+    ref_oracle.L.ref_set_flags(0, 0)
+    ref_oracle.read_bmad(str(hsr_table(tmp_path, numeric_only=True)))
+    x0 = np.load(GOLDEN / "hsr_orbit_ref.npz")["orbit"][-1]
+    for d in ([0, 0, 0, 0, 0, 0], [-3e-4, 1e-6, 2e-4, -1e-6, 0.01, 2e-4]):
+        a = ref_oracle.track_dump(x0 + np.array(d), 2)
+        b = port_oracle.track_dump(x0 + np.array(d), 2)
+        assert a[1:4] == b[1:4]
+        assert np.array_equal(a[4], b[4])
