@@ -266,7 +266,24 @@ int stb_scan_set_tbt(stb_scan *s, double *tbt, int nturns);
 int stb_scan_retire(stb_scan *s, const uint8_t *mask);
 
 /* ---- turn-by-turn diagnostics ----
- * FineTuneFinder (simtrack.cpp:2288-2319; with px != NULL the x/px form,
+ * Track_tbt (simtrack.cpp:20841-20860) for n particles on the GPU: x AoS
+ * n*6 (in/out), stable[] Track()'s input flags and outputs as in
+ * stb_track_host; x_tbt[(i*nturn + turn)*6 + k] = coordinate k of particle i
+ * at the start of each turn up to and including the turn of its loss
+ * (nothing for particles rejected by the entry check); x_tbt may be NULL. */
+int stb_track_tbt(stb_line *l, double *x, long n, int nturn, double *x_tbt, int *stable, int *lost_turn,
+                  int *lost_post, int device);
+/* Track_tbt_FMA (simtrack.cpp:21179-21241) with FineTuneFinder's window
+ * [tune_lower, tune_upper) (the reference's globals tune_low/tune_high):
+ * writes the reference's FMA-output.dat rows to `filename`; *rows = their
+ * number (may be NULL). */
+int stb_track_tbt_fma(stb_line *l, double deltap0, double sigmax0, double sigmay0, double tune_lower,
+                      double tune_upper, const char *filename, long *rows, int device);
+/* Track_tbt_Lyapunov (simtrack.cpp:21243-21306): writes the reference's
+ * Lmap-output.dat rows to `filename`; *rows = their number (may be NULL). */
+int stb_track_tbt_lyapunov(stb_line *l, double deltap0, double sigmax0, double sigmay0, const char *filename,
+                           long *rows, int device);
+/* FineTuneFinder (simtrack.cpp:2288-2319; with px != NULL the x/px form,
  * 2321-2352) for nsig signals at once: sample i of signal j is
  * x[i*stride + j] (device arrays; stride >= nsig when nsig > 1), n <= 4096
  * samples; the same coarse 1e-3 scan over [tune_lower, tune_upper) and

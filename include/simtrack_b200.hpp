@@ -293,6 +293,32 @@ void Read_MADX_Lattice(Line &line, const char *filename);
 // unreadable file or a beam-beam element of non-zero length.
 void Read_BMAD_Lattice(Line &line, const char *filename);
 
+// Track_tbt() drop-in (simtrack.cpp:20841-20860): Track() that also records
+// x[6] at the start of every turn, x_tbt[turn*6 + k], up to and including the
+// turn of the loss.  Track_tbt_Batch: n particles (AoS x[n*6], stable[] as
+// Track()'s input flags), x_tbt[(i*nturn + turn)*6 + k].
+void Track_tbt(Line &line, double x[], int nturn, double x_tbt[], int &stable, int &lost_turn, int &lost_post);
+void Track_tbt_Batch(Line &line, double *x, long n, int nturn, double *x_tbt, int *stable, int *lost_turn,
+                     int *lost_post, int device = 0);
+
+// FineTuneFinder's search window used by Track_tbt_FMA (simtrack.cpp:27).
+extern double tune_low, tune_high;
+
+// Track_tbt_FMA (simtrack.cpp:21179-21241): frequency map of a 0-6 sigma
+// quarter-disc grid (step 0.1 sigma) around the closed orbit at deltap0,
+// 2,048 turns, tunes of turns 0-1023 and 1023-2046 by FineTuneFinder in
+// [tune_low, tune_high); writes the reference's FMA-output.dat rows (to
+// `filename`) and returns their number.
+long Track_tbt_FMA(Line &line, double deltap0, double sigmax0, double sigmay0,
+                   const char *filename = "./FMA-output.dat", int device = 0);
+
+// Track_tbt_Lyapunov (simtrack.cpp:21243-21306): for a 0-6 sigma quarter-disc
+// grid (step 0.05 sigma), the growth of the distance between a particle and
+// a twin 1e-6 away over 2,048 turns, averaged over the last 25 turns; writes
+// the reference's Lmap-output.dat rows (to `filename`) and returns their number.
+long Track_tbt_Lyapunov(Line &line, double deltap0, double sigmax0, double sigmay0,
+                        const char *filename = "./Lmap-output.dat", int device = 0);
+
 // Track_Radial() drop-in (simtrack.cpp:21641-21680): Track() with z taken
 // relative to the on-momentum reference particle after every element.
 void Track_Radial(Line &line, double x[], int nturn, int &stable, int &lost_turn, int &lost_post);

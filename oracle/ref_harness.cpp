@@ -25,6 +25,7 @@
 #include <cmath>
 
 extern GlobalVariables GP;
+extern double tune_low, tune_high;
 
 namespace {
 
@@ -148,6 +149,22 @@ void *ref_line_read_madx(const char *path) {
   Line *l = new Line();
   Read_MADX_Lattice(*l, path);
   return l;
+}
+
+// Track_tbt (simtrack.cpp:20841), the overload without a BPM index.
+void ref_track_tbt(void *line, double *x, int nturn, double *x_tbt, int *stable, int *lost_turn, int *lost_post) {
+  Track_tbt(*static_cast<Line *>(line), x, nturn, x_tbt, *stable, *lost_turn, *lost_post);
+}
+
+// Track_tbt_FMA / Track_tbt_Lyapunov (simtrack.cpp:21179, 21243): write
+// ./FMA-output.dat / ./Lmap-output.dat in the current directory.
+void ref_track_tbt_fma(void *line, double deltap0, double sigmax0, double sigmay0, double lo, double hi) {
+  tune_low = lo;
+  tune_high = hi;
+  Track_tbt_FMA(*static_cast<Line *>(line), deltap0, sigmax0, sigmay0);
+}
+void ref_track_tbt_lyapunov(void *line, double deltap0, double sigmax0, double sigmay0) {
+  Track_tbt_Lyapunov(*static_cast<Line *>(line), deltap0, sigmax0, sigmay0);
 }
 
 // Read_BMAD_Lattice (simtrack.cpp:14054) into a new Line.  The reference

@@ -10,7 +10,7 @@ calls exit(), e.g. simtrack.cpp:8653-8685).
 from __future__ import annotations
 
 import ctypes
-from ctypes import POINTER, byref, c_double, c_int, c_void_p
+from ctypes import POINTER, byref, c_double, c_int, c_long, c_void_p
 from typing import Sequence
 
 import numpy as np
@@ -390,6 +390,43 @@ def Cal_Orbit_Num(line: Line, deltap: float = 0.0, device: int = 0) -> np.ndarra
     out = np.empty((line.Ncell, 6))
     check(lib().stb_cal_orbit(line._h, deltap, out.ctypes.data_as(POINTER(c_double)), device))
     return out
+
+
+def Track_tbt(line: Line, x, nturn: int, stable=None, device: int = 0):
+    """Track_tbt (simtrack.cpp:20841-20860) for particles x[n, 6] (copied):
+    returns (x, stable, lost_turn, lost_post, x_tbt[n, nturn, 6]); x_tbt holds
+    the coordinates at the start of each turn up to the turn of the loss and
+    NaN after it."""
+    x = np.ascontiguousarray(np.atleast_2d(np.asarray(x, dtype=np.float64))).copy()
+    n = x.shape[0]
+    st = np.ones(n, dtype=np.int32) if stable is None else np.ascontiguousarray(stable, dtype=np.int32).copy()
+    lt = np.zeros(n, dtype=np.int32)
+    lp = np.zeros(n, dtype=np.int32)
+    tbt = np.full((n, nturn, 6), np.nan)
+    P = lambda a, t: a.ctypes.data_as(POINTER(t))
+    check(lib().stb_track_tbt(line._h, P(x, c_double), n, nturn, P(tbt, c_double), P(st, c_int), P(lt, c_int),
+                              P(lp, c_int), device))
+    return x, st, lt, lp, tbt
+
+
+def Track_tbt_FMA(line: Line, deltap0: float, sigmax0: float, sigmay0: float, filename="./FMA-output.dat",
+                  tune_low: float = 0.660, tune_high: float = 0.70, device: int = 0) -> int:
+    """Track_tbt_FMA (simtrack.cpp:21179-21241): writes the frequency map to
+    `filename` in the reference's format; returns the number of rows."""
+    rows = c_long(0)
+    check(lib().stb_track_tbt_fma(line._h, deltap0, sigmax0, sigmay0, tune_low, tune_high, str(filename).encode(),
+                                  ctypes.byref(rows), device))
+    return rows.value
+
+
+def Track_tbt_Lyapunov(line: Line, deltap0: float, sigmax0: float, sigmay0: float, filename="./Lmap-output.dat",
+                       device: int = 0) -> int:
+    """Track_tbt_Lyapunov (simtrack.cpp:21243-21306): writes the Lyapunov map
+    to `filename` in the reference's format; returns the number of rows."""
+    rows = c_long(0)
+    check(lib().stb_track_tbt_lyapunov(line._h, deltap0, sigmax0, sigmay0, str(filename).encode(),
+                                       ctypes.byref(rows), device))
+    return rows.value
 
 
 def Track_DA(line: Line, nturn: int, deltap0: float, sigmax0: float, sigmay0: float, filename=None,

@@ -593,6 +593,42 @@ int stb_line_read_bmad(stb_line *l, const char *path) {
     return STB_OK;
   });
 }
+
+int stb_track_tbt(stb_line *l, double *x, long n, int nturn, double *x_tbt, int *stable, int *lost_turn,
+                  int *lost_post, int device) {
+  return guarded([&] {
+    if (!l) throw Error(STB_EINVAL, "line is NULL");
+    Track_tbt_Batch(*Lp(l), x, n, nturn, x_tbt, stable, lost_turn, lost_post, device);
+    return STB_OK;
+  });
+}
+
+int stb_track_tbt_fma(stb_line *l, double deltap0, double sigmax0, double sigmay0, double tune_lower,
+                      double tune_upper, const char *filename, long *rows, int device) {
+  return guarded([&] {
+    if (!l) throw Error(STB_EINVAL, "line is NULL");
+    const double lo = tune_low, hi = tune_high;
+    tune_low = tune_lower;
+    tune_high = tune_upper;
+    struct Restore {
+      double lo, hi;
+      ~Restore() { tune_low = lo; tune_high = hi; }
+    } restore{lo, hi};
+    const long r = Track_tbt_FMA(*Lp(l), deltap0, sigmax0, sigmay0, filename, device);
+    if (rows) *rows = r;
+    return STB_OK;
+  });
+}
+
+int stb_track_tbt_lyapunov(stb_line *l, double deltap0, double sigmax0, double sigmay0, const char *filename,
+                           long *rows, int device) {
+  return guarded([&] {
+    if (!l) throw Error(STB_EINVAL, "line is NULL");
+    const long r = Track_tbt_Lyapunov(*Lp(l), deltap0, sigmax0, sigmay0, filename, device);
+    if (rows) *rows = r;
+    return STB_OK;
+  });
+}
 int stb_element_type(const stb_element *e, char *buf, int cap) {
   return guarded([&] {
     if (!e || !buf || cap <= 0) throw Error(STB_EINVAL, "NULL argument");

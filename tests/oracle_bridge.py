@@ -73,6 +73,10 @@ class RefOracle:
         L.ref_line_read_madx.restype = c_void_p
         L.ref_line_read_bmad.argtypes = [ctypes.c_char_p]
         L.ref_line_read_bmad.restype = c_void_p
+        L.ref_track_tbt.argtypes = [c_void_p, POINTER(c_double), c_int, POINTER(c_double), POINTER(c_int),
+                                    POINTER(c_int), POINTER(c_int)]
+        L.ref_track_tbt_fma.argtypes = [c_void_p, c_double, c_double, c_double, c_double, c_double]
+        L.ref_track_tbt_lyapunov.argtypes = [c_void_p, c_double, c_double, c_double]
         L.ref_line_elem.argtypes = [c_void_p, c_long, ctypes.c_char_p, ctypes.c_char_p, c_int, POINTER(c_double)]
         L.ref_cal_orbit.argtypes = [c_void_p, c_double, POINTER(c_double)]
         L.ref_track_da.argtypes = [c_void_p, c_int, c_double, c_double, c_double, ctypes.c_char_p]
@@ -165,6 +169,17 @@ class RefOracle:
         self.line = self.L.ref_line_read_bmad(str(path).encode())
         self.nelem = int(self.L.ref_line_ncell(self.line))
         self.radius = 0.0
+
+    def track_tbt(self, x0, nturn: int, stable: int = 1):
+        """Track_tbt of one particle: (x, stable, lost_turn, lost_post, x_tbt[nturn, 6])
+        with NaN in the turns it did not record."""
+        x = np.ascontiguousarray(x0, dtype=np.float64).copy()
+        tbt = np.full((nturn, 6), np.nan)
+        st, lt, lp = c_int(stable), c_int(0), c_int(0)
+        self.L.ref_track_tbt(self.line, x.ctypes.data_as(POINTER(c_double)), nturn,
+                             tbt.ctypes.data_as(POINTER(c_double)), ctypes.byref(st), ctypes.byref(lt),
+                             ctypes.byref(lp))
+        return x, st.value, lt.value, lp.value, tbt
 
     def element(self, i: int):
         """(TYPE, NAME, {L, S, DX, DY, DS, DTHETA, DPHI, DPSI, APx, APy}) of element i."""
