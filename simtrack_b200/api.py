@@ -221,6 +221,7 @@ class Line:
 
 
 NUM_VARIANTS = 11
+NUM_SCAN_VARIANTS = 7
 
 
 def variant_name(v: int) -> str:
@@ -502,7 +503,7 @@ class Scan:
         ch = c_int()
         t = (c_double * 8)()
         check(lib().stb_scan_autotune(self._h, nturn, byref(ch), t, 8))
-        return {"chosen": ch.value, "ms": [t[i] for i in range(5)]}
+        return {"chosen": ch.value, "ms": [t[i] for i in range(NUM_SCAN_VARIANTS)]}
 
     def run(self, nturn: int, turns_per_block: int = 256, use_graph: bool = True) -> None:
         check(lib().stb_scan_run(self._h, nturn, turns_per_block, int(use_graph)))

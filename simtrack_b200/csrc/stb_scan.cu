@@ -290,7 +290,8 @@ cudaError_t prepare_scan_variant(int num_sms, size_t smem, int *grid) {
 
 const ScanVariant kScanVariants[kNumScanVariants] = {
     {true, 1024, 1, "smem_b1024_r64"}, {true, 512, 1, "smem_b512_r128"}, {false, 256, 4, "l1_b256_r64"},
-    {false, 256, 3, "l1_b256_r80"},    {false, 128, 8, "l1_b128_r64"},
+    {false, 256, 3, "l1_b256_r80"},    {false, 128, 8, "l1_b128_r64"},    {false, 256, 2, "l1_b256_r128"},
+    {false, 128, 2, "l1_b128_r255"},
 };
 
 cudaError_t prepare_scan(int variant, int num_sms, size_t smem, int *grid) {
@@ -300,6 +301,8 @@ cudaError_t prepare_scan(int variant, int num_sms, size_t smem, int *grid) {
     case 2: return prepare_scan_variant<false, 256, 4>(num_sms, 0, grid);
     case 3: return prepare_scan_variant<false, 256, 3>(num_sms, 0, grid);
     case 4: return prepare_scan_variant<false, 128, 8>(num_sms, 0, grid);
+    case 5: return prepare_scan_variant<false, 256, 2>(num_sms, 0, grid);
+    case 6: return prepare_scan_variant<false, 128, 2>(num_sms, 0, grid);
     default: return cudaErrorInvalidValue;
   }
 }
@@ -315,6 +318,8 @@ cudaError_t launch_scan_block(const ScanArgs &a, int variant, int grid, size_t s
     case 2: scan_track_kernel<false, 256, 4><<<grid, 256, 0, st>>>(a); break;
     case 3: scan_track_kernel<false, 256, 3><<<grid, 256, 0, st>>>(a); break;
     case 4: scan_track_kernel<false, 128, 8><<<grid, 128, 0, st>>>(a); break;
+    case 5: scan_track_kernel<false, 256, 2><<<grid, 256, 0, st>>>(a); break;
+    case 6: scan_track_kernel<false, 128, 2><<<grid, 128, 0, st>>>(a); break;
     default: return cudaErrorInvalidValue;
   }
   e = cudaGetLastError();

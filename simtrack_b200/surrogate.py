@@ -53,6 +53,7 @@ class SurrogateConfig:
     policy: str = "ray"
     band_lo: int = 2             # amplitude steps tracked below the predicted first loss of a ray
     band_hi: int = 2             # ... and above it
+    retune: bool = True          # re-choose the scan's launch variant for the survivors of retirement
 
 
 @dataclass
@@ -237,7 +238,15 @@ def pruned_scan(tables, grids, radius, twiss6, mlp: MLP, std: Standardizer, cfg:
     retire = cand & ~audit
     ep.scan.retire(retire)
     t2 = time.perf_counter()
-    ep.scan.run(cfg.nturn - cfg.nrec, cfg.turns_per_block)
+    # One turn block compacts the retired particles away; the launch variant
+    # is then chosen again for the few survivors, whose tracking is bound by
+    # the latency of one particle-turn rather than by throughput.
+    rest = cfg.nturn - cfg.nrec
+    first = min(cfg.turns_per_block, rest)
+    ep.scan.run(first, cfg.turns_per_block)
+    if cfg.retune and rest > first:
+        ep.scan.autotune(nturn=16)
+    ep.scan.run(rest - first, cfg.turns_per_block)
     lt, _, _ = ep.scan.results()
     t3 = time.perf_counter()
     survive = np.where(retire, cand_stable, (lt < 0) | (lt >= cfg.nturn))
