@@ -175,6 +175,40 @@ int stb_cal_orbit(stb_line *l, double deltap, double *orbit6, int device);
 int stb_track_da(stb_line *l, int nturn, double deltap0, double sigmax0, double sigmay0, const char *filename,
                  double *angles10, double *sigma10, int device);
 
+/* The reference's other DA drivers with their output files (see
+ * include/simtrack_b200.hpp):
+ *   STB_DA1 Track_DA1 (simtrack.cpp:21443), STB_DA2 Track_DA2 (21497),
+ *   STB_DA3 Track_DA3 (21535), STB_DA_RADIAL Track_DA_Radial (21682):
+ *     bisections; out_a / out_sigma (optional, 10 entries) receive the angle
+ *     labels [deg] and stable amplitudes, *nout their number (5 or 10);
+ *   STB_DA_UNIFORM Track_DA_Uniform (21574), STB_DA_RADIAL_UNIFORM
+ *     Track_DA_Radial_Uniform (21736): a sweep at `angle` [rad]; out_a /
+ *     out_sigma (optional, 150 entries) receive each written line's stable
+ *     flag (1.0 / 0.0) and amplitude, *nout the number of lines (up to the
+ *     first loss, where the reference ends the process).
+ * `angle` is ignored by the bisections; filename may be NULL. */
+#define STB_DA1 1
+#define STB_DA2 2
+#define STB_DA3 3
+#define STB_DA_RADIAL 4
+#define STB_DA_UNIFORM 5
+#define STB_DA_RADIAL_UNIFORM 6
+int stb_track_da_driver(stb_line *l, int which, int nturn, double deltap0, double angle, double sigmax0,
+                        double sigmay0, const char *filename, double *out_a, double *out_sigma, long *nout,
+                        int device);
+
+/* Cal_Tunes_Track (simtrack.cpp:20971-20990): x6 (in/out) tracked nturn turns
+ * with a turn-by-turn record (x[0], x[2] below 1e-9 raised by 1e-9 first);
+ * if it survives, tunes2 = FineTuneFinder of its x and y records in
+ * [tune_lower, tune_upper) and *stable = 1, else tunes2 is left alone and
+ * *stable = 0. */
+int stb_cal_tunes_track(stb_line *l, double *x6, int nturn, double tune_lower, double tune_upper, double *tunes2,
+                        int *stable, int device);
+/* Cal_Tunes_Track(line, deltap0) (simtrack.cpp:20992-21025): the tunes of the
+ * closed orbit at deltap0 over 1,024 turns (line.Tune1/Tune2; 0 if lost). */
+int stb_cal_tunes_track_orbit(stb_line *l, double deltap0, double tune_lower, double tune_upper, double *tunes2,
+                              int device);
+
 /* ---- Track_Radial (simtrack.cpp:21641-21680) ----
  * As stb_track_device / stb_track_host, with z corrected after every element
  * j by the path-length change of the on-momentum reference particle through

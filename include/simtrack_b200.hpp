@@ -244,6 +244,7 @@ class Line {
   double Length = 0.;
   long Ncell = 0;
   double frev0 = 0.;
+  double Tune1 = 0., Tune2 = 0.;  // set by Cal_Tunes_Track (simtrack.h:1085)
 };
 
 // Options that have no counterpart in Track()'s signature.
@@ -269,6 +270,42 @@ void Track_Batch(Line &line, double *x, long n, int nturn, int *stable, int *los
 // angles_out / sigma_out (optional) receive the 10 results.
 void Track_DA(Line &line, int nturn, double deltap0, double sigmax0, double sigmay0, const char *filename,
               double *angles_out = nullptr, double *sigma_out = nullptr, int device = 0);
+
+// The other bisection drivers, same method and output format:
+//   Track_DA1 (simtrack.cpp:21443-21495): twin particles, 5 angles 15..75 deg, 0-50 sigma;
+//   Track_DA2 (21497-21533): single particles, 10 angles (90/11)(i+1) deg, 0-50 sigma;
+//   Track_DA3 (21535-21572): Cal_Orbit_Num(line, 0) first, single particles, 5 angles 15..75 deg, 0-30 sigma;
+//   Track_DA_Radial (21682-21734): twin particles through Track_Radial, 10 angles, 0-15 sigma.
+void Track_DA1(Line &line, int nturn, double deltap0, double sigmax0, double sigmay0, const char *filename,
+               double *angles_out = nullptr, double *sigma_out = nullptr, int device = 0);
+void Track_DA2(Line &line, int nturn, double deltap0, double sigmax0, double sigmay0, const char *filename,
+               double *angles_out = nullptr, double *sigma_out = nullptr, int device = 0);
+void Track_DA3(Line &line, int nturn, double deltap0, double sigmax0, double sigmay0, const char *filename,
+               double *angles_out = nullptr, double *sigma_out = nullptr, int device = 0);
+void Track_DA_Radial(Line &line, int nturn, double deltap0, double sigmax0, double sigmay0, const char *filename,
+                     double *angles_out = nullptr, double *sigma_out = nullptr, int device = 0);
+
+// Track_DA_Uniform (simtrack.cpp:21574-21603) / Track_DA_Radial_Uniform
+// (21736-21764): amplitudes 1, 1.2, ..., 30.8 sigma at one angle [rad]
+// through Track / Track_Radial, one "angle sigma stable" line per amplitude
+// up to and including the first loss (where the reference ends the process;
+// here the function returns).  Returns the number of lines; sigma_out /
+// stable_out (optional, 150 entries) receive their values.
+long Track_DA_Uniform(Line &line, int nturn, double deltap0, double angle, double sigmax0, double sigmay0,
+                      const char *filename, double *sigma_out = nullptr, double *stable_out = nullptr,
+                      int device = 0);
+long Track_DA_Radial_Uniform(Line &line, int nturn, double deltap0, double angle, double sigmax0, double sigmay0,
+                             const char *filename, double *sigma_out = nullptr, double *stable_out = nullptr,
+                             int device = 0);
+
+// Cal_Tunes_Track (simtrack.cpp:20971-21025): tunes of a tracked particle by
+// FineTuneFinder over its Track_tbt record in [tune_low, tune_high).  The
+// first form tracks x (x[0], x[2] below 1e-9 are raised by 1e-9, in place)
+// for Nturn turns and leaves tune1/tune2 unchanged if it is lost; the second
+// tracks the closed orbit at deltap0 for 1,024 turns and stores the tunes in
+// line.Tune1 / line.Tune2 (0 if the particle is lost).
+void Cal_Tunes_Track(Line &line, double x[], int Nturn, double &tune1, double &tune2, int device = 0);
+void Cal_Tunes_Track(Line &line, double deltap0, int device = 0);
 
 // Cal_Orbit_Num (simtrack.cpp:14947-15030): 4D closed orbit at momentum
 // offset deltap by Newton iteration on the one-turn map (RF voltages off,

@@ -210,6 +210,18 @@ void ref_track_da(void *line, int nturn, double deltap0, double sigmax0, double 
   Track_DA(*static_cast<Line *>(line), nturn, deltap0, sigmax0, sigmay0, filename);
 }
 
+// The reference's other bisection drivers: 1 Track_DA1, 2 Track_DA2,
+// 3 Track_DA3, 4 Track_DA_Radial (simtrack.cpp:21443, 21497, 21535, 21682).
+// The uniform sweeps are not wrapped: they end the process at the first loss.
+void ref_track_da_driver(void *line, int which, int nturn, double deltap0, double sigmax0, double sigmay0,
+                         const char *filename) {
+  Line &l = *static_cast<Line *>(line);
+  if (which == 1) Track_DA1(l, nturn, deltap0, sigmax0, sigmay0, filename);
+  if (which == 2) Track_DA2(l, nturn, deltap0, sigmax0, sigmay0, filename);
+  if (which == 3) Track_DA3(l, nturn, deltap0, sigmax0, sigmay0, filename);
+  if (which == 4) Track_DA_Radial(l, nturn, deltap0, sigmax0, sigmay0, filename);
+}
+
 // n particles through the reference Track_Radial() (simtrack.cpp:21641-21680).
 void ref_track_radial(void *line, double *x, long n, int nturn, int *stable, int *lost_turn, int *lost_post) {
   Line &l = *static_cast<Line *>(line);

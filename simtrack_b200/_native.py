@@ -81,6 +81,11 @@ SIGNATURES = [
     ("stb_element_geometry", c_int, [c_void_p, POINTER(c_double)]),
     ("stb_line_read_madx", c_int, [c_void_p, c_char_p]),
     ("stb_line_read_bmad", c_int, [c_void_p, c_char_p]),
+    ("stb_track_da_driver", c_int, [c_void_p, c_int, c_int, c_double, c_double, c_double, c_double, c_char_p,
+                                    POINTER(c_double), POINTER(c_double), POINTER(c_long), c_int]),
+    ("stb_cal_tunes_track", c_int, [c_void_p, POINTER(c_double), c_int, c_double, c_double, POINTER(c_double),
+                                    POINTER(c_int), c_int]),
+    ("stb_cal_tunes_track_orbit", c_int, [c_void_p, c_double, c_double, c_double, POINTER(c_double), c_int]),
     ("stb_track_tbt", c_int, [c_void_p, POINTER(c_double), c_long, c_int, POINTER(c_double), POINTER(c_int),
                               POINTER(c_int), POINTER(c_int), c_int]),
     ("stb_track_tbt_fma", c_int, [c_void_p, c_double, c_double, c_double, c_double, c_double, c_char_p,

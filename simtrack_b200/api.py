@@ -393,6 +393,49 @@ def Cal_Orbit_Num(line: Line, deltap: float = 0.0, device: int = 0) -> np.ndarra
     return out
 
 
+DA_DRIVERS = {"Track_DA1": 1, "Track_DA2": 2, "Track_DA3": 3, "Track_DA_Radial": 4, "Track_DA_Uniform": 5,
+              "Track_DA_Radial_Uniform": 6}
+
+
+def Track_DA_driver(name: str, line: Line, nturn: int, deltap0: float, sigmax0: float, sigmay0: float,
+                    angle: float = 0.0, filename=None, device: int = 0):
+    """The reference's other DA drivers by name (Track_DA1, Track_DA2,
+    Track_DA3, Track_DA_Radial: simtrack.cpp:21443-21734; Track_DA_Uniform,
+    Track_DA_Radial_Uniform: 21574, 21736), writing the reference's file when
+    `filename` is given.  Bisections return (angle labels [deg], sigma);
+    uniform sweeps (at `angle` [rad]) return (stable flags, sigma) of the lines
+    written, up to the first loss."""
+    a = (c_double * 150)()
+    sg = (c_double * 150)()
+    n = c_long(0)
+    check(lib().stb_track_da_driver(line._h, DA_DRIVERS[name], nturn, deltap0, angle, sigmax0, sigmay0,
+                                    None if filename is None else str(filename).encode(), a, sg, ctypes.byref(n),
+                                    device))
+    return np.array(a[:n.value]), np.array(sg[:n.value])
+
+
+def Cal_Tunes_Track(line: Line, x, nturn: int, tune_low: float = 0.660, tune_high: float = 0.70,
+                    device: int = 0):
+    """Cal_Tunes_Track (simtrack.cpp:20971-20990): (tune1, tune2) of particle
+    x[6] from its turn-by-turn record, or None if it is lost; x is tracked in
+    place (a float64 numpy array of 6)."""
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    t = (c_double * 2)()
+    st = c_int(0)
+    check(lib().stb_cal_tunes_track(line._h, x.ctypes.data_as(POINTER(c_double)), nturn, tune_low, tune_high, t,
+                                    ctypes.byref(st), device))
+    return (t[0], t[1]) if st.value else None
+
+
+def Cal_Tunes_Track_orbit(line: Line, deltap0: float, tune_low: float = 0.660, tune_high: float = 0.70,
+                          device: int = 0):
+    """Cal_Tunes_Track(line, deltap0) (simtrack.cpp:20992-21025): tunes of the
+    closed orbit at deltap0 over 1,024 turns (0, 0 if it is lost)."""
+    t = (c_double * 2)()
+    check(lib().stb_cal_tunes_track_orbit(line._h, deltap0, tune_low, tune_high, t, device))
+    return t[0], t[1]
+
+
 def Track_tbt(line: Line, x, nturn: int, stable=None, device: int = 0):
     """Track_tbt (simtrack.cpp:20841-20860) for particles x[n, 6] (copied):
     returns (x, stable, lost_turn, lost_post, x_tbt[n, nturn, 6]); x_tbt holds

@@ -470,6 +470,23 @@ void Track_Spin(Line &line, double x[], int nturn, int &stable, int &lost_turn, 
 
 using namespace stb;
 
+namespace stb {
+namespace {
+// Runs f with FineTuneFinder's window set to [lo, hi), restoring it afterwards.
+template <class F>
+void with_tune_window(double lo, double hi, F f) {
+  const double lo0 = tune_low, hi0 = tune_high;
+  tune_low = lo;
+  tune_high = hi;
+  struct Restore {
+    double lo, hi;
+    ~Restore() { tune_low = lo; tune_high = hi; }
+  } restore{lo0, hi0};
+  f();
+}
+}  // namespace
+}  // namespace stb
+
 extern "C" {
 
 const char *stb_last_error(void) { return stb::last_error(); }
@@ -578,6 +595,63 @@ int stb_track_da(stb_line *l, int nturn, double deltap0, double sigmax0, double 
     return STB_OK;
   });
 }
+int stb_track_da_driver(stb_line *l, int which, int nturn, double deltap0, double angle, double sigmax0,
+                        double sigmay0, const char *filename, double *out_a, double *out_sigma, long *nout,
+                        int device) {
+  return guarded([&] {
+    if (!l) throw Error(STB_EINVAL, "NULL line");
+    Line &L = *Lp(l);
+    long n = 0;
+    switch (which) {
+      case STB_DA1: Track_DA1(L, nturn, deltap0, sigmax0, sigmay0, filename, out_a, out_sigma, device); n = 5; break;
+      case STB_DA2: Track_DA2(L, nturn, deltap0, sigmax0, sigmay0, filename, out_a, out_sigma, device); n = 10; break;
+      case STB_DA3: Track_DA3(L, nturn, deltap0, sigmax0, sigmay0, filename, out_a, out_sigma, device); n = 5; break;
+      case STB_DA_RADIAL:
+        Track_DA_Radial(L, nturn, deltap0, sigmax0, sigmay0, filename, out_a, out_sigma, device);
+        n = 10;
+        break;
+      case STB_DA_UNIFORM:
+        n = Track_DA_Uniform(L, nturn, deltap0, angle, sigmax0, sigmay0, filename, out_sigma, out_a, device);
+        break;
+      case STB_DA_RADIAL_UNIFORM:
+        n = Track_DA_Radial_Uniform(L, nturn, deltap0, angle, sigmax0, sigmay0, filename, out_sigma, out_a, device);
+        break;
+      default: throw Error(STB_EINVAL, "unknown DA driver");
+    }
+    if (nout) *nout = n;
+    return STB_OK;
+  });
+}
+
+int stb_cal_tunes_track(stb_line *l, double *x6, int nturn, double tune_lower, double tune_upper, double *tunes2,
+                        int *stable, int device) {
+  return guarded([&] {
+    if (!l || !x6 || !tunes2) throw Error(STB_EINVAL, "NULL argument");
+    double t1 = NAN, t2 = NAN;
+    with_tune_window(tune_lower, tune_upper, [&] { Cal_Tunes_Track(*Lp(l), x6, nturn, t1, t2, device); });
+    const bool ok = !std::isnan(t1);
+    if (ok) {
+      tunes2[0] = t1;
+      tunes2[1] = t2;
+    }
+    if (stable) *stable = ok ? 1 : 0;
+    return STB_OK;
+  });
+}
+
+int stb_cal_tunes_track_orbit(stb_line *l, double deltap0, double tune_lower, double tune_upper, double *tunes2,
+                              int device) {
+  return guarded([&] {
+    if (!l) throw Error(STB_EINVAL, "NULL line");
+    with_tune_window(tune_lower, tune_upper, [&] { Cal_Tunes_Track(*Lp(l), deltap0, device); });
+    if (tunes2) {
+      tunes2[0] = Lp(l)->Tune1;
+      tunes2[1] = Lp(l)->Tune2;
+    }
+    return STB_OK;
+  });
+}
+
 int stb_line_read_madx(stb_line *l, const char *path) {
   return guarded([&] {
     if (!l || !path) throw Error(STB_EINVAL, "NULL argument");
@@ -607,14 +681,8 @@ int stb_track_tbt_fma(stb_line *l, double deltap0, double sigmax0, double sigmay
                       double tune_upper, const char *filename, long *rows, int device) {
   return guarded([&] {
     if (!l) throw Error(STB_EINVAL, "line is NULL");
-    const double lo = tune_low, hi = tune_high;
-    tune_low = tune_lower;
-    tune_high = tune_upper;
-    struct Restore {
-      double lo, hi;
-      ~Restore() { tune_low = lo; tune_high = hi; }
-    } restore{lo, hi};
-    const long r = Track_tbt_FMA(*Lp(l), deltap0, sigmax0, sigmay0, filename, device);
+    long r = 0;
+    with_tune_window(tune_lower, tune_upper, [&] { r = Track_tbt_FMA(*Lp(l), deltap0, sigmax0, sigmay0, filename, device); });
     if (rows) *rows = r;
     return STB_OK;
   });

@@ -77,6 +77,7 @@ class RefOracle:
                                     POINTER(c_int), POINTER(c_int)]
         L.ref_track_tbt_fma.argtypes = [c_void_p, c_double, c_double, c_double, c_double, c_double]
         L.ref_track_tbt_lyapunov.argtypes = [c_void_p, c_double, c_double, c_double]
+        L.ref_track_da_driver.argtypes = [c_void_p, c_int, c_int, c_double, c_double, c_double, ctypes.c_char_p]
         L.ref_line_elem.argtypes = [c_void_p, c_long, ctypes.c_char_p, ctypes.c_char_p, c_int, POINTER(c_double)]
         L.ref_cal_orbit.argtypes = [c_void_p, c_double, POINTER(c_double)]
         L.ref_track_da.argtypes = [c_void_p, c_int, c_double, c_double, c_double, ctypes.c_char_p]
