@@ -307,6 +307,10 @@ int stb_scan_retire(stb_scan *s, const uint8_t *mask);
  * (nothing for particles rejected by the entry check); x_tbt may be NULL. */
 int stb_track_tbt(stb_line *l, double *x, long n, int nturn, double *x_tbt, int *stable, int *lost_turn,
                   int *lost_post, int device);
+/* Track_tbt_spin (simtrack.cpp:20863-20882): as stb_track_tbt with spin
+ * tracking (Element::sPass), x AoS n*9 and x_tbt[(i*nturn + turn)*9 + k]. */
+int stb_track_tbt_spin(stb_line *l, double *x9, long n, int nturn, double *x_tbt9, int *stable, int *lost_turn,
+                       int *lost_post, int device);
 /* Track_tbt_FMA (simtrack.cpp:21179-21241) with FineTuneFinder's window
  * [tune_lower, tune_upper) (the reference's globals tune_low/tune_high):
  * writes the reference's FMA-output.dat rows to `filename`; *rows = their

@@ -337,6 +337,12 @@ void Read_BMAD_Lattice(Line &line, const char *filename);
 void Track_tbt(Line &line, double x[], int nturn, double x_tbt[], int &stable, int &lost_turn, int &lost_post);
 void Track_tbt_Batch(Line &line, double *x, long n, int nturn, double *x_tbt, int *stable, int *lost_turn,
                      int *lost_post, int device = 0);
+// Track_tbt_spin() (simtrack.cpp:20863-20882): the same with spin tracking,
+// x[9] and x_tbt[turn*9 + k]; the batch form takes x9[n*9], x_tbt9[(i*nturn + turn)*9 + k].
+void Track_tbt_spin(Line &line, double x[], int nturn, double x_tbt[], int &stable, int &lost_turn,
+                    int &lost_post);
+void Track_tbt_spin_Batch(Line &line, double *x9, long n, int nturn, double *x_tbt9, int *stable, int *lost_turn,
+                          int *lost_post, int device = 0);
 
 // FineTuneFinder's search window used by Track_tbt_FMA (simtrack.cpp:27).
 extern double tune_low, tune_high;

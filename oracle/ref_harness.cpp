@@ -156,6 +156,12 @@ void ref_track_tbt(void *line, double *x, int nturn, double *x_tbt, int *stable,
   Track_tbt(*static_cast<Line *>(line), x, nturn, x_tbt, *stable, *lost_turn, *lost_post);
 }
 
+// Track_tbt_spin (simtrack.cpp:20863), the overload without a BPM index.
+void ref_track_tbt_spin(void *line, double *x9, int nturn, double *x_tbt9, int *stable, int *lost_turn,
+                        int *lost_post) {
+  Track_tbt_spin(*static_cast<Line *>(line), x9, nturn, x_tbt9, *stable, *lost_turn, *lost_post);
+}
+
 // Track_tbt_FMA / Track_tbt_Lyapunov (simtrack.cpp:21179, 21243): write
 // ./FMA-output.dat / ./Lmap-output.dat in the current directory.
 void ref_track_tbt_fma(void *line, double deltap0, double sigmax0, double sigmay0, double lo, double hi) {

@@ -677,6 +677,15 @@ int stb_track_tbt(stb_line *l, double *x, long n, int nturn, double *x_tbt, int 
   });
 }
 
+int stb_track_tbt_spin(stb_line *l, double *x9, long n, int nturn, double *x_tbt9, int *stable, int *lost_turn,
+                       int *lost_post, int device) {
+  return guarded([&] {
+    if (!l) throw Error(STB_EINVAL, "line is NULL");
+    Track_tbt_spin_Batch(*Lp(l), x9, n, nturn, x_tbt9, stable, lost_turn, lost_post, device);
+    return STB_OK;
+  });
+}
+
 int stb_track_tbt_fma(stb_line *l, double deltap0, double sigmax0, double sigmay0, double tune_lower,
                       double tune_upper, const char *filename, long *rows, int device) {
   return guarded([&] {

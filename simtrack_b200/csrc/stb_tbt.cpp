@@ -1,6 +1,6 @@
 // Turn-by-turn tracking and its diagnostics on the GPU: Track_tbt
-// (simtrack.cpp:20841-20860), Track_tbt_FMA (21179-21241) and
-// Track_tbt_Lyapunov (21243-21306).
+// (simtrack.cpp:20841-20860), Track_tbt_spin (20863-20882), Track_tbt_FMA
+// (21179-21241) and Track_tbt_Lyapunov (21243-21306).
 //
 // A batch of particles is tracked one turn per launch; before every turn the
 // coordinates of all particles are copied (device to device) into a record
@@ -51,16 +51,18 @@ TablePtr make_table(const Line &line, int device) {
   return TablePtr(raw, stb_table_free);
 }
 
-// Particles of one batch on the device, SoA, with Track()'s loss state.
+// Particles of one batch on the device, SoA, with Track()'s loss state:
+// nc = 6 orbit coordinates, or 9 with the spin vector (Track_Spin's x[9]).
 struct DeviceBatch {
   long n;
+  int nc;
   DevMem coords, loss;
-  DeviceBatch(const double *xa, const int *stable, long n_)
-      : n(n_), coords(sizeof(double) * 6 * (size_t)n_), loss(sizeof(int32_t) * 2 * (size_t)n_) {
-    std::vector<double> soa((size_t)n * 6);
+  DeviceBatch(const double *xa, const int *stable, long n_, int nc_ = 6)
+      : n(n_), nc(nc_), coords(sizeof(double) * nc_ * (size_t)n_), loss(sizeof(int32_t) * 2 * (size_t)n_) {
+    std::vector<double> soa((size_t)n * nc);
     std::vector<int32_t> l((size_t)n * 2, 0);
     for (long i = 0; i < n; i++) {
-      for (int k = 0; k < 6; k++) soa[(size_t)k * n + i] = xa[6 * i + k];
+      for (int k = 0; k < nc; k++) soa[(size_t)k * n + i] = xa[(size_t)nc * i + k];
       l[i] = stable[i] == 0 ? 0 : -1;  // stable == 0 on entry: lost at turn 0, post 0
     }
     cuda_check(cudaMemcpy(coords.p, soa.data(), sizeof(double) * soa.size(), cudaMemcpyHostToDevice),
@@ -73,14 +75,14 @@ struct DeviceBatch {
 
   // Final coordinates (AoS) and Track()'s outputs.
   void download(double *xa, int *stable, int *lost_turn_out, int *lost_post) const {
-    std::vector<double> soa((size_t)n * 6);
+    std::vector<double> soa((size_t)n * nc);
     std::vector<int32_t> l((size_t)n * 2);
     cuda_check(cudaMemcpy(soa.data(), coords.p, sizeof(double) * soa.size(), cudaMemcpyDeviceToHost),
                "download coordinates");
     cuda_check(cudaMemcpy(l.data(), loss.p, sizeof(int32_t) * l.size(), cudaMemcpyDeviceToHost), "download loss");
     for (long i = 0; i < n; i++) {
       if (xa)
-        for (int k = 0; k < 6; k++) xa[6 * i + k] = soa[(size_t)k * n + i];
+        for (int k = 0; k < nc; k++) xa[(size_t)nc * i + k] = soa[(size_t)k * n + i];
       const bool alive = l[i] < 0;
       stable[i] = alive ? 1 : 0;
       lost_turn_out[i] = alive ? 0 : l[i];
@@ -89,9 +91,10 @@ struct DeviceBatch {
   }
 };
 
-// nturn one-turn launches.  rec (device, [nturn - rec_from][ncoord][n])
-// gets the first ncoord coordinates (x, px, y, py, z, pt order) at the start
-// of every turn from rec_from on.
+// nturn one-turn launches (spin tracking for a 9-coordinate batch).  rec
+// (device, [nturn - rec_from][ncoord][n]) gets the first ncoord coordinates
+// (x, px, y, py, z, pt, sx, sy, sz order) at the start of every turn from
+// rec_from on.
 void track_recorded(stb_table *t, const DeviceBatch &b, int nturn, int ncoord, double *rec, int rec_from = 0) {
   const long n = b.n;
   const size_t bytes = sizeof(double) * (size_t)n;
@@ -101,10 +104,48 @@ void track_recorded(stb_table *t, const DeviceBatch &b, int nturn, int ncoord, d
         cuda_check(cudaMemcpyAsync(rec + ((size_t)(turn - rec_from) * ncoord + k) * n, b.c(k), bytes,
                                    cudaMemcpyDeviceToDevice, 0),
                    "record turn");
-    check(stb_track_device(t, b.c(0), b.c(1), b.c(2), b.c(3), b.c(4), b.c(5), n, turn, 1, 0.0, b.lost_turn(),
-                           b.lost_elem(), nullptr));
+    if (b.nc == 9)
+      check(stb_track_spin_device(t, b.c(0), b.c(1), b.c(2), b.c(3), b.c(4), b.c(5), b.c(6), b.c(7), b.c(8), n, turn,
+                                  1, 0.0, b.lost_turn(), b.lost_elem(), nullptr));
+    else
+      check(stb_track_device(t, b.c(0), b.c(1), b.c(2), b.c(3), b.c(4), b.c(5), n, turn, 1, 0.0, b.lost_turn(),
+                             b.lost_elem(), nullptr));
   }
   cuda_check(cudaDeviceSynchronize(), "turn-by-turn tracking");
+}
+
+// Track_tbt / Track_tbt_spin for n particles of nc coordinates (AoS x).
+void tbt_batch(Line &line, double *x, long n, int nc, int nturn, double *x_tbt, int *stable, int *lost_turn,
+               int *lost_post, int device) {
+  if (n < 0 || nturn < 0) throw Error(STB_EINVAL, "negative particle count or turn count");
+  if (n == 0) return;
+  if (!x || !stable || !lost_turn || !lost_post) throw Error(STB_EINVAL, "NULL host buffer");
+  // the entry check returns before anything is recorded
+  std::vector<char> rejected((size_t)n);
+  for (long i = 0; i < n; i++)
+    rejected[i] = std::fabs(x[(size_t)nc * i]) > 0.1 || std::fabs(x[(size_t)nc * i + 2]) > 0.1 || stable[i] == 0;
+  DeviceGuard g(device);
+  stb_table *raw = nullptr;
+  if (nc == 9)
+    check(stb_table_create_spin(reinterpret_cast<const stb_line *>(&line), device, &raw));
+  else
+    check(stb_table_create(reinterpret_cast<const stb_line *>(&line), device, &raw));
+  TablePtr t(raw, stb_table_free);
+  DeviceBatch b(x, stable, n, nc);
+  DevMem rec(sizeof(double) * nc * (size_t)n * (size_t)nturn);
+  track_recorded(t.get(), b, nturn, nc, rec.as<double>());
+  b.download(x, stable, lost_turn, lost_post);
+  if (!x_tbt) return;
+  std::vector<double> r((size_t)nc * n * nturn);
+  cuda_check(cudaMemcpy(r.data(), rec.p, sizeof(double) * r.size(), cudaMemcpyDeviceToHost), "download record");
+  // x_tbt[(i*nturn + turn)*nc + k] for the turns recorded: every turn up to
+  // and including the one in which the particle is lost
+  for (long i = 0; i < n; i++) {
+    const int last = rejected[i] ? 0 : stable[i] ? nturn : lost_turn[i] + 1;
+    for (int turn = 0; turn < last; turn++)
+      for (int k = 0; k < nc; k++)
+        x_tbt[((size_t)i * nturn + turn) * nc + k] = r[((size_t)turn * nc + k) * n + i];
+  }
 }
 
 // The reference's grid of amplitudes inside a quarter circle of 6 sigma.
@@ -123,29 +164,16 @@ std::vector<GridPoint> quarter_disc(int nsigma, double sigma_step) {
 
 void Track_tbt_Batch(Line &line, double *x, long n, int nturn, double *x_tbt, int *stable, int *lost_turn,
                      int *lost_post, int device) {
-  if (n < 0 || nturn < 0) throw Error(STB_EINVAL, "negative particle count or turn count");
-  if (n == 0) return;
-  if (!x || !stable || !lost_turn || !lost_post) throw Error(STB_EINVAL, "NULL host buffer");
-  // Track_tbt's entry check returns before anything is recorded
-  std::vector<char> rejected((size_t)n);
-  for (long i = 0; i < n; i++)
-    rejected[i] = std::fabs(x[6 * i]) > 0.1 || std::fabs(x[6 * i + 2]) > 0.1 || stable[i] == 0;
-  DeviceGuard g(device);
-  TablePtr t = make_table(line, device);
-  DeviceBatch b(x, stable, n);
-  DevMem rec(sizeof(double) * 6 * (size_t)n * (size_t)nturn);
-  track_recorded(t.get(), b, nturn, 6, rec.as<double>());
-  b.download(x, stable, lost_turn, lost_post);
-  if (!x_tbt) return;
-  std::vector<double> r((size_t)6 * n * nturn);
-  cuda_check(cudaMemcpy(r.data(), rec.p, sizeof(double) * r.size(), cudaMemcpyDeviceToHost), "download record");
-  // x_tbt[(i*nturn + turn)*6 + k] for the turns Track_tbt records: every turn
-  // up to and including the one in which the particle is lost
-  for (long i = 0; i < n; i++) {
-    const int last = rejected[i] ? 0 : stable[i] ? nturn : lost_turn[i] + 1;
-    for (int turn = 0; turn < last; turn++)
-      for (int k = 0; k < 6; k++) x_tbt[((size_t)i * nturn + turn) * 6 + k] = r[((size_t)turn * 6 + k) * n + i];
-  }
+  tbt_batch(line, x, n, 6, nturn, x_tbt, stable, lost_turn, lost_post, device);
+}
+
+void Track_tbt_spin_Batch(Line &line, double *x9, long n, int nturn, double *x_tbt9, int *stable, int *lost_turn,
+                          int *lost_post, int device) {
+  tbt_batch(line, x9, n, 9, nturn, x_tbt9, stable, lost_turn, lost_post, device);
+}
+
+void Track_tbt_spin(Line &line, double x[], int nturn, double x_tbt[], int &stable, int &lost_turn, int &lost_post) {
+  Track_tbt_spin_Batch(line, x, 1, nturn, x_tbt, &stable, &lost_turn, &lost_post, 0);
 }
 
 void Track_tbt(Line &line, double x[], int nturn, double x_tbt[], int &stable, int &lost_turn, int &lost_post) {

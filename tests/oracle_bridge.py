@@ -75,6 +75,8 @@ class RefOracle:
         L.ref_line_read_bmad.restype = c_void_p
         L.ref_track_tbt.argtypes = [c_void_p, POINTER(c_double), c_int, POINTER(c_double), POINTER(c_int),
                                     POINTER(c_int), POINTER(c_int)]
+        L.ref_track_tbt_spin.argtypes = [c_void_p, POINTER(c_double), c_int, POINTER(c_double), POINTER(c_int),
+                                         POINTER(c_int), POINTER(c_int)]
         L.ref_track_tbt_fma.argtypes = [c_void_p, c_double, c_double, c_double, c_double, c_double]
         L.ref_track_tbt_lyapunov.argtypes = [c_void_p, c_double, c_double, c_double]
         L.ref_track_da_driver.argtypes = [c_void_p, c_int, c_int, c_double, c_double, c_double, ctypes.c_char_p]
@@ -172,14 +174,15 @@ class RefOracle:
         self.radius = 0.0
 
     def track_tbt(self, x0, nturn: int, stable: int = 1):
-        """Track_tbt of one particle: (x, stable, lost_turn, lost_post, x_tbt[nturn, 6])
-        with NaN in the turns it did not record."""
+        """Track_tbt of one particle (Track_tbt_spin for x0 of 9): (x, stable,
+        lost_turn, lost_post, x_tbt[nturn, 6 or 9]) with NaN in the turns it did
+        not record."""
         x = np.ascontiguousarray(x0, dtype=np.float64).copy()
-        tbt = np.full((nturn, 6), np.nan)
+        tbt = np.full((nturn, len(x)), np.nan)
         st, lt, lp = c_int(stable), c_int(0), c_int(0)
-        self.L.ref_track_tbt(self.line, x.ctypes.data_as(POINTER(c_double)), nturn,
-                             tbt.ctypes.data_as(POINTER(c_double)), ctypes.byref(st), ctypes.byref(lt),
-                             ctypes.byref(lp))
+        fn = self.L.ref_track_tbt_spin if len(x) == 9 else self.L.ref_track_tbt
+        fn(self.line, x.ctypes.data_as(POINTER(c_double)), nturn, tbt.ctypes.data_as(POINTER(c_double)),
+           ctypes.byref(st), ctypes.byref(lt), ctypes.byref(lp))
         return x, st.value, lt.value, lp.value, tbt
 
     def element(self, i: int):

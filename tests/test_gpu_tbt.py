@@ -53,6 +53,21 @@ def test_track_tbt_record(which, native_lib, ref_oracle):
     assert lost > 0  # losses (entry check or in tracking) are covered
 
 
+def test_track_tbt_spin_record(native_lib, ref_oracle):
+    """Track_tbt_spin (simtrack.cpp:20863): the nine-coordinate record."""
+    from lattice_zoo import spin_particles, spin_zoo
+    lat = spin_zoo()
+    line = lt.build_line(lat)
+    X = spin_particles()
+    nt = 3
+    x, st, ltn, lp, tbt = api.Track_tbt(line, X, nt, spin=True)
+    ref_oracle.build(lat)
+    for i, x0 in enumerate(X):
+        xo, so, lo, po, to = ref_oracle.track_tbt(x0, nt)
+        assert (st[i], ltn[i], lp[i]) == (so, lo, po), f"particle {i}"
+        assert _same(tbt[i], to), f"particle {i}: record differs"
+
+
 def test_lyapunov_file_matches_reference(native_lib, ref_oracle, tmp_path, monkeypatch):
     lat = thin_fodo_ring()
     line = lt.build_line(lat)
