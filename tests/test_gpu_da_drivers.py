@@ -84,6 +84,15 @@ def test_cal_tunes_track(ring, native_lib, ref_oracle):
         assert so == 1 and got is not None
         ref = (ref_oracle.fine_tune(tbt[:, 0], None, lo, hi), ref_oracle.fine_tune(tbt[:, 2], None, lo, hi))
         assert abs(got[0] - ref[0]) < 1e-9 and abs(got[1] - ref[1]) < 1e-9, (a, got, ref)
-    # the closed-orbit form: tunes of the ring's working point (0.31 / 0.32)
+    # the closed-orbit form: a particle on the closed orbit (raised by 1e-9 in
+    # x and y) tracked 1,024 turns; its small-amplitude tunes include the
+    # beam-beam tune shift of the two interaction points
     q1, q2 = api.Cal_Tunes_Track_orbit(line, 0.0, lo, hi)
-    assert abs(q1 - 0.31) < 0.01 and abs(q2 - 0.32) < 0.01
+    x0 = np.zeros(6)
+    x0[:4] = ref_oracle.cal_orbit(0.0)[-1][:4]
+    x0[0] += 1e-9 if x0[0] < 1e-9 else 0.0
+    x0[2] += 1e-9 if x0[2] < 1e-9 else 0.0
+    _, so, _, _, tbt = ref_oracle.track_tbt(x0, 1024)
+    ref = (ref_oracle.fine_tune(tbt[:, 0], None, lo, hi), ref_oracle.fine_tune(tbt[:, 2], None, lo, hi))
+    assert so == 1 and abs(q1 - ref[0]) < 1e-9 and abs(q2 - ref[1]) < 1e-9, ((q1, q2), ref)
+    assert lo < q1 < hi and lo < q2 < hi
