@@ -307,6 +307,11 @@ int stb_scan_retire(stb_scan *s, const uint8_t *mask);
  * (nothing for particles rejected by the entry check); x_tbt may be NULL. */
 int stb_track_tbt(stb_line *l, double *x, long n, int nturn, double *x_tbt, int *stable, int *lost_turn,
                   int *lost_post, int device);
+/* Track_tbt with a BPM index (simtrack.cpp:20884-20905): as stb_track_tbt,
+ * recording x[6] after element bpm_index in every turn that reaches it; the
+ * per-element probe it runs needs n * ncell * 48 B < 4 GB (else STB_EINVAL). */
+int stb_track_tbt_bpm(stb_line *l, double *x, long n, int nturn, double *x_tbt, int bpm_index, int *stable,
+                      int *lost_turn, int *lost_post, int device);
 /* Track_tbt_spin (simtrack.cpp:20863-20882): as stb_track_tbt with spin
  * tracking (Element::sPass), x AoS n*9 and x_tbt[(i*nturn + turn)*9 + k]. */
 int stb_track_tbt_spin(stb_line *l, double *x9, long n, int nturn, double *x_tbt9, int *stable, int *lost_turn,

@@ -337,6 +337,14 @@ void Read_BMAD_Lattice(Line &line, const char *filename);
 void Track_tbt(Line &line, double x[], int nturn, double x_tbt[], int &stable, int &lost_turn, int &lost_post);
 void Track_tbt_Batch(Line &line, double *x, long n, int nturn, double *x_tbt, int *stable, int *lost_turn,
                      int *lost_post, int device = 0);
+// Track_tbt() with a BPM index (simtrack.cpp:20884-20905): records x[6] after
+// element bpm_index in every turn that reaches it (x_tbt[turn*6 + k]).  The
+// batch form runs the tracking kernel's per-element probe, so n x Ncell x
+// 48 B must stay under 4 GB.
+void Track_tbt(Line &line, double x[], int nturn, double x_tbt[], int &bpm_index, int &stable, int &lost_turn,
+               int &lost_post);
+void Track_tbt_bpm_Batch(Line &line, double *x, long n, int nturn, double *x_tbt, int bpm_index, int *stable,
+                         int *lost_turn, int *lost_post, int device = 0);
 // Track_tbt_spin() (simtrack.cpp:20863-20882): the same with spin tracking,
 // x[9] and x_tbt[turn*9 + k]; the batch form takes x9[n*9], x_tbt9[(i*nturn + turn)*9 + k].
 void Track_tbt_spin(Line &line, double x[], int nturn, double x_tbt[], int &stable, int &lost_turn,

@@ -156,6 +156,12 @@ void ref_track_tbt(void *line, double *x, int nturn, double *x_tbt, int *stable,
   Track_tbt(*static_cast<Line *>(line), x, nturn, x_tbt, *stable, *lost_turn, *lost_post);
 }
 
+// Track_tbt with a BPM index (simtrack.cpp:20884).
+void ref_track_tbt_bpm(void *line, double *x, int nturn, double *x_tbt, int bpm_index, int *stable, int *lost_turn,
+                       int *lost_post) {
+  Track_tbt(*static_cast<Line *>(line), x, nturn, x_tbt, bpm_index, *stable, *lost_turn, *lost_post);
+}
+
 // Track_tbt_spin (simtrack.cpp:20863), the overload without a BPM index.
 void ref_track_tbt_spin(void *line, double *x9, int nturn, double *x_tbt9, int *stable, int *lost_turn,
                         int *lost_post) {

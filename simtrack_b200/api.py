@@ -436,12 +436,13 @@ def Cal_Tunes_Track_orbit(line: Line, deltap0: float, tune_low: float = 0.660, t
     return t[0], t[1]
 
 
-def Track_tbt(line: Line, x, nturn: int, stable=None, device: int = 0, spin: bool = False):
+def Track_tbt(line: Line, x, nturn: int, stable=None, device: int = 0, spin: bool = False, bpm_index=None):
     """Track_tbt (simtrack.cpp:20841-20860; with spin=True Track_tbt_spin,
     20863-20882, x[n, 9]) for particles x[n, 6] (copied): returns (x, stable,
     lost_turn, lost_post, x_tbt[n, nturn, 6 or 9]); x_tbt holds the
     coordinates at the start of each turn up to the turn of the loss and NaN
-    after it."""
+    after it.  With bpm_index (20884-20905) the record is taken after that
+    element, in the turns that reach it."""
     x = np.ascontiguousarray(np.atleast_2d(np.asarray(x, dtype=np.float64))).copy()
     n, nc = x.shape
     if nc != (9 if spin else 6):
@@ -451,6 +452,12 @@ def Track_tbt(line: Line, x, nturn: int, stable=None, device: int = 0, spin: boo
     lp = np.zeros(n, dtype=np.int32)
     tbt = np.full((n, nturn, nc), np.nan)
     P = lambda a, t: a.ctypes.data_as(POINTER(t))
+    if bpm_index is not None:
+        if spin:
+            raise ValueError("the BPM form is not available with spin")
+        check(lib().stb_track_tbt_bpm(line._h, P(x, c_double), n, nturn, P(tbt, c_double), int(bpm_index),
+                                      P(st, c_int), P(lt, c_int), P(lp, c_int), device))
+        return x, st, lt, lp, tbt
     fn = lib().stb_track_tbt_spin if spin else lib().stb_track_tbt
     check(fn(line._h, P(x, c_double), n, nturn, P(tbt, c_double), P(st, c_int), P(lt, c_int), P(lp, c_int), device))
     return x, st, lt, lp, tbt

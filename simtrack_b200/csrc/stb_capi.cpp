@@ -442,6 +442,13 @@ int spin_host(stb_table *t, double *xa, long n, int nturn, double radius, int *s
 
 }  // namespace
 
+// One-turn-block launch with the per-element record (the probe variant of the
+// tracking kernel): dump[((i*nturn + turn)*nelem + j)*6 + k] after element j.
+void track_device_dump(stb_table *t, double *const c[6], long n, int turn0, int nturn, int32_t *lost_turn,
+                       int32_t *lost_elem, double *dump) {
+  track_device(t, c[0], c[1], c[2], c[3], c[4], c[5], n, turn0, nturn, 0.0, lost_turn, lost_elem, 0, dump);
+}
+
 // ---- C++ Track entry points ----
 void Track_Batch(Line &line, double *x, long n, int nturn, int *stable, int *lost_turn, int *lost_post,
                  const TrackOptions &opt) {
@@ -673,6 +680,15 @@ int stb_track_tbt(stb_line *l, double *x, long n, int nturn, double *x_tbt, int 
   return guarded([&] {
     if (!l) throw Error(STB_EINVAL, "line is NULL");
     Track_tbt_Batch(*Lp(l), x, n, nturn, x_tbt, stable, lost_turn, lost_post, device);
+    return STB_OK;
+  });
+}
+
+int stb_track_tbt_bpm(stb_line *l, double *x, long n, int nturn, double *x_tbt, int bpm_index, int *stable,
+                      int *lost_turn, int *lost_post, int device) {
+  return guarded([&] {
+    if (!l) throw Error(STB_EINVAL, "line is NULL");
+    Track_tbt_bpm_Batch(*Lp(l), x, n, nturn, x_tbt, bpm_index, stable, lost_turn, lost_post, device);
     return STB_OK;
   });
 }

@@ -52,6 +52,12 @@ inline void cuda_check(cudaError_t e, const char *what) {
   }
 }
 
+// One launch of nturn turns from turn0 on the probe variant of the tracking
+// kernel, which writes dump[((i*nturn + turn)*nelem + j)*6 + k] after every
+// element j (no circular aperture); default stream, asynchronous.
+void track_device_dump(stb_table *t, double *const c[6], long n, int turn0, int nturn, int32_t *lost_turn,
+                       int32_t *lost_elem, double *dump);
+
 // Restores the caller's current device on scope exit.
 struct DeviceGuard {
   int prev = -1;

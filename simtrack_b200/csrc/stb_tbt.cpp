@@ -1,5 +1,6 @@
 // Turn-by-turn tracking and its diagnostics on the GPU: Track_tbt
-// (simtrack.cpp:20841-20860), Track_tbt_spin (20863-20882), Track_tbt_FMA
+// (simtrack.cpp:20841-20860; with a BPM index 20884-20905), Track_tbt_spin
+// (20863-20882), Track_tbt_FMA
 // (21179-21241) and Track_tbt_Lyapunov (21243-21306).
 //
 // A batch of particles is tracked one turn per launch; before every turn the
@@ -7,7 +8,10 @@
 // rec[(t*ncoord + k)*n + i] (k in x, px, y, py, z, pt order): what Track_tbt
 // stores in x_tbt at the start of each turn.  The frequency-map tunes come from the GPU
 // FineTuneFinder (stb_fine_tune) over two 1,024-turn windows of the record;
-// the Lyapunov indicator needs only the last 25 turns of it.  The output
+// the Lyapunov indicator needs only the last 25 turns of it.  The BPM form
+// records after a given element instead: each one-turn launch runs the
+// tracking kernel's per-element probe variant and the element's slice of
+// the probe is copied into the record.  The output
 // files are written with the reference's stream formatting, including the
 // scientific/18-digit state its stream keeps after the first row.
 #include <cuda_runtime.h>
@@ -174,6 +178,58 @@ void Track_tbt_spin_Batch(Line &line, double *x9, long n, int nturn, double *x_t
 
 void Track_tbt_spin(Line &line, double x[], int nturn, double x_tbt[], int &stable, int &lost_turn, int &lost_post) {
   Track_tbt_spin_Batch(line, x, 1, nturn, x_tbt, &stable, &lost_turn, &lost_post, 0);
+}
+
+void Track_tbt_bpm_Batch(Line &line, double *x, long n, int nturn, double *x_tbt, int bpm_index, int *stable,
+                         int *lost_turn, int *lost_post, int device) {
+  if (n < 0 || nturn < 0) throw Error(STB_EINVAL, "negative particle count or turn count");
+  if (n == 0) return;
+  if (!x || !stable || !lost_turn || !lost_post) throw Error(STB_EINVAL, "NULL host buffer");
+  const long nelem = line.Ncell;
+  if (nelem < 1) throw Error(STB_EINVAL, "line has no elements");
+  // the per-element record of one turn must fit a modest device buffer
+  const double dump_bytes = 48.0 * (double)n * (double)nelem;
+  if (dump_bytes > 4.0e9)
+    throw Error(STB_EINVAL, "particles x elements too large for the element record (over 4 GB per turn)");
+  std::vector<char> rejected((size_t)n);
+  for (long i = 0; i < n; i++) rejected[i] = std::fabs(x[6 * i]) > 0.1 || std::fabs(x[6 * i + 2]) > 0.1 || stable[i] == 0;
+  const bool in_line = bpm_index >= 0 && bpm_index < nelem;
+  DeviceGuard g(device);
+  TablePtr t = make_table(line, device);
+  DeviceBatch b(x, stable, n, 6);
+  DevMem dump((size_t)dump_bytes);
+  DevMem rec(sizeof(double) * 6 * (size_t)n * (size_t)nturn);  // [turn][i][6]
+  double *const c[6] = {b.c(0), b.c(1), b.c(2), b.c(3), b.c(4), b.c(5)};
+  for (int turn = 0; turn < nturn; turn++) {
+    track_device_dump(t.get(), c, n, turn, 1, b.lost_turn(), b.lost_elem(), dump.as<double>());
+    if (in_line)
+      cuda_check(cudaMemcpy2DAsync(rec.as<double>() + (size_t)turn * n * 6, 6 * sizeof(double),
+                                   dump.as<double>() + (size_t)bpm_index * 6, (size_t)nelem * 6 * sizeof(double),
+                                   6 * sizeof(double), (size_t)n, cudaMemcpyDeviceToDevice, 0),
+                 "record element");
+  }
+  cuda_check(cudaDeviceSynchronize(), "turn-by-turn tracking");
+  int st = 0;
+  cuda_check(cudaMemcpy(&st, t->d_status, sizeof(int), cudaMemcpyDeviceToHost), "read status");
+  if (st != 0) throw Error(st, "tracking kernel reported status " + std::to_string(st));
+  b.download(x, stable, lost_turn, lost_post);
+  if (!x_tbt || !in_line) return;
+  std::vector<double> r((size_t)6 * n * nturn);
+  cuda_check(cudaMemcpy(r.data(), rec.p, sizeof(double) * r.size(), cudaMemcpyDeviceToHost), "download record");
+  // a turn is recorded when the particle passed the element in it: every turn
+  // before its loss, and the turn of the loss if it came at or after the element
+  for (long i = 0; i < n; i++) {
+    if (rejected[i]) continue;
+    int last = nturn;
+    if (!stable[i]) last = lost_post[i] >= bpm_index ? lost_turn[i] + 1 : lost_turn[i];
+    for (int turn = 0; turn < last; turn++)
+      for (int k = 0; k < 6; k++) x_tbt[((size_t)i * nturn + turn) * 6 + k] = r[((size_t)turn * n + i) * 6 + k];
+  }
+}
+
+void Track_tbt(Line &line, double x[], int nturn, double x_tbt[], int &bpm_index, int &stable, int &lost_turn,
+               int &lost_post) {
+  Track_tbt_bpm_Batch(line, x, 1, nturn, x_tbt, bpm_index, &stable, &lost_turn, &lost_post, 0);
 }
 
 void Track_tbt(Line &line, double x[], int nturn, double x_tbt[], int &stable, int &lost_turn, int &lost_post) {

@@ -75,6 +75,8 @@ class RefOracle:
         L.ref_line_read_bmad.restype = c_void_p
         L.ref_track_tbt.argtypes = [c_void_p, POINTER(c_double), c_int, POINTER(c_double), POINTER(c_int),
                                     POINTER(c_int), POINTER(c_int)]
+        L.ref_track_tbt_bpm.argtypes = [c_void_p, POINTER(c_double), c_int, POINTER(c_double), c_int, POINTER(c_int),
+                                        POINTER(c_int), POINTER(c_int)]
         L.ref_track_tbt_spin.argtypes = [c_void_p, POINTER(c_double), c_int, POINTER(c_double), POINTER(c_int),
                                          POINTER(c_int), POINTER(c_int)]
         L.ref_track_tbt_fma.argtypes = [c_void_p, c_double, c_double, c_double, c_double, c_double]
@@ -183,6 +185,16 @@ class RefOracle:
         fn = self.L.ref_track_tbt_spin if len(x) == 9 else self.L.ref_track_tbt
         fn(self.line, x.ctypes.data_as(POINTER(c_double)), nturn, tbt.ctypes.data_as(POINTER(c_double)),
            ctypes.byref(st), ctypes.byref(lt), ctypes.byref(lp))
+        return x, st.value, lt.value, lp.value, tbt
+
+    def track_tbt_bpm(self, x0, nturn: int, bpm_index: int):
+        """Track_tbt with a BPM index: (x, stable, lost_turn, lost_post, x_tbt[nturn, 6]), NaN where not recorded."""
+        x = np.ascontiguousarray(x0, dtype=np.float64).copy()
+        tbt = np.full((nturn, 6), np.nan)
+        st, lt, lp = c_int(1), c_int(0), c_int(0)
+        self.L.ref_track_tbt_bpm(self.line, x.ctypes.data_as(POINTER(c_double)), nturn,
+                                 tbt.ctypes.data_as(POINTER(c_double)), bpm_index, ctypes.byref(st), ctypes.byref(lt),
+                                 ctypes.byref(lp))
         return x, st.value, lt.value, lp.value, tbt
 
     def element(self, i: int):

@@ -53,6 +53,31 @@ def test_track_tbt_record(which, native_lib, ref_oracle):
     assert lost > 0  # losses (entry check or in tracking) are covered
 
 
+@pytest.mark.parametrize("which,bpm", [("zoo", 0), ("zoo", 17), ("fodo", 600), ("fodo", 1200)])
+def test_track_tbt_bpm_record(which, bpm, native_lib, ref_oracle):
+    """Track_tbt with a BPM index (simtrack.cpp:20884): the record after
+    element `bpm` in every turn that reaches it, losses before and after the
+    element included."""
+    if which == "zoo":
+        lat, X, nt = zoo(), zoo_particles(), 3
+    else:
+        lat = lt.fodo_ring()
+        a = np.linspace(0.0, 0.03, 12)
+        X = np.zeros((12, 6))
+        X[:, 0] = a
+        X[:, 2] = 0.5 * a
+        X[-1, 0] = 0.2
+        nt = 60
+    line = lt.build_line(lat)
+    x, st, ltn, lp, tbt = api.Track_tbt(line, X, nt, bpm_index=bpm)
+    ref_oracle.build(lat)
+    for i, x0 in enumerate(X):
+        xo, so, lo, po, to = ref_oracle.track_tbt_bpm(x0, nt, bpm)
+        assert (st[i], ltn[i], lp[i]) == (so, lo, po), f"particle {i}"
+        assert _same(tbt[i], to), f"particle {i}: record differs"
+        assert _same(x[i], xo), f"particle {i}: final coordinates differ"
+
+
 def test_track_tbt_spin_record(native_lib, ref_oracle):
     """Track_tbt_spin (simtrack.cpp:20863): the nine-coordinate record."""
     from lattice_zoo import spin_particles, spin_zoo
