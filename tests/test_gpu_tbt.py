@@ -102,7 +102,7 @@ def test_lyapunov_file_matches_reference(native_lib, ref_oracle, tmp_path, monke
     ref_oracle.L.ref_track_tbt_lyapunov(ref_oracle.line, 0.0, SIGMA, SIGMA)
     ours = (tmp_path / "gpu.dat").read_text()
     ref = (tmp_path / "Lmap-output.dat").read_text()
-    assert rows == len(ref.splitlines()) > 10000
+    assert 5000 < rows == len(ref.splitlines()) < 11425  # some twins are lost
     assert ours == ref
 
 
