@@ -375,10 +375,12 @@ def pruned_from_artifacts(path: str, cfg: Optional[SurrogateConfig] = None, devi
 
 
 def evaluate_saved(path: str, seeds: Sequence[int], cfg: Optional[SurrogateConfig] = None, device: int = 0,
-                   log=print) -> dict:
+                   log=print, plain: bool = True) -> dict:
     """Plain and pruned scans of `seeds` (e.g. seeds neither trained nor used
     to choose the retirement policy) with the network saved by
-    experiment(artifacts=...)."""
+    experiment(artifacts=...).  With plain=False only the pruned scan runs
+    (its wall time and tracking work, e.g. for a seed count whose plain scan
+    is measured elsewhere)."""
     a = np.load(path)
     cfg = cfg or SurrogateConfig()
     cfg.nturn, cfg.nrec, cfg.hidden = int(a["nturn"]), int(a["nrec"]), int(a["hidden"])
@@ -390,12 +392,20 @@ def evaluate_saved(path: str, seeds: Sequence[int], cfg: Optional[SurrogateConfi
     std.mean, std.std = a["std_mean"], a["std_std"]
     lats, tables, grids = ring_setup(seeds, namp, amax, nang, deltas, device)
     radius = lats[0].aperture_radius
+    out = {"eval_seeds": list(seeds), "config": asdict(cfg), "model_from": path,
+           "grid": {"namp": namp, "amax_sigma": amax, "nang": nang, "deltas": list(deltas)}}
+    if not plain:
+        res = pruned_scan(tables, grids, radius, tuple(a["twiss6"]), mlp, std, cfg, namp, device)
+        log(f"pruned scan: {res.seconds['total']:.1f} s {res.seconds}")
+        out["pruned"] = {"wall_s": res.seconds["total"], "seconds": res.seconds,
+                         "particle_turns": res.particle_turns, "retired": int(res.retired.sum()),
+                         "audited": int(res.audited.sum()),
+                         "tracked_to_end": int((~res.retired & ~res.lost_early).sum())}
+        return out
     lt_plain, wall_plain, pt_plain = plain_scan(tables, grids, radius, cfg, device)
     log(f"plain scan: {wall_plain:.1f} s")
     res = pruned_scan(tables, grids, radius, tuple(a["twiss6"]), mlp, std, cfg, namp, device)
     log(f"pruned scan: {res.seconds['total']:.1f} s {res.seconds}")
-    out = {"eval_seeds": list(seeds), "config": asdict(cfg), "model_from": path,
-           "grid": {"namp": namp, "amax_sigma": amax, "nang": nang, "deltas": list(deltas)}}
     out.update(compare(res, lt_plain, wall_plain, pt_plain, len(seeds), len(deltas), nang, namp, amax, cfg))
     return out
 
@@ -440,6 +450,7 @@ def main(argv=None):
     ap.add_argument("--replay", action="store_true", help="offline policy replay on --artifacts (no GPU)")
     ap.add_argument("--eval-seeds", type=int, nargs=2, default=None, metavar=("FIRST", "COUNT"),
                     help="plain and pruned scans of new seeds with the network saved in --artifacts")
+    ap.add_argument("--no-plain", action="store_true", help="with --eval-seeds: run the pruned scan only")
     ap.add_argument("--out", default="")
     a = ap.parse_args(argv)
     cfg = SurrogateConfig(nturn=a.nturn, epochs=a.epochs, policy=a.policy, band_lo=a.band[0], band_hi=a.band[1],
@@ -449,7 +460,8 @@ def main(argv=None):
             print(json.dumps(r))
         return
     if a.eval_seeds:
-        res = evaluate_saved(a.artifacts, list(range(a.eval_seeds[0], a.eval_seeds[0] + a.eval_seeds[1])), cfg)
+        res = evaluate_saved(a.artifacts, list(range(a.eval_seeds[0], a.eval_seeds[0] + a.eval_seeds[1])), cfg,
+                             plain=not a.no_plain)
     elif a.pruned_only:
         res = pruned_from_artifacts(a.artifacts, cfg)
     else:
