@@ -208,6 +208,9 @@ int stb_cal_tunes_track(stb_line *l, double *x6, int nturn, double tune_lower, d
  * closed orbit at deltap0 over 1,024 turns (line.Tune1/Tune2; 0 if lost). */
 int stb_cal_tunes_track_orbit(stb_line *l, double deltap0, double tune_lower, double tune_upper, double *tunes2,
                               int device);
+/* Cal_Chrom_Track (simtrack.cpp:21027-21051): chroms4 = Chromx1, Chromy1,
+ * Chromx2, Chromy2 from the tracked tunes at deltap = +3e-4, -3e-4, 0. */
+int stb_cal_chrom_track(stb_line *l, double tune_lower, double tune_upper, double *chroms4, int device);
 
 /* ---- Track_Radial (simtrack.cpp:21641-21680) ----
  * As stb_track_device / stb_track_host, with z corrected after every element

@@ -245,6 +245,7 @@ class Line {
   long Ncell = 0;
   double frev0 = 0.;
   double Tune1 = 0., Tune2 = 0.;  // set by Cal_Tunes_Track (simtrack.h:1085)
+  double Chromx1 = 0., Chromy1 = 0., Chromx2 = 0., Chromy2 = 0.;  // set by Cal_Chrom_Track
 };
 
 // Options that have no counterpart in Track()'s signature.
@@ -306,6 +307,11 @@ long Track_DA_Radial_Uniform(Line &line, int nturn, double deltap0, double angle
 // line.Tune1 / line.Tune2 (0 if the particle is lost).
 void Cal_Tunes_Track(Line &line, double x[], int Nturn, double &tune1, double &tune2, int device = 0);
 void Cal_Tunes_Track(Line &line, double deltap0, int device = 0);
+
+// Cal_Chrom_Track (simtrack.cpp:21027-21051): first and second order
+// chromaticities from the tracked tunes at deltap = +3e-4, -3e-4 and 0
+// (Cal_Tunes_Track(line, deltap) each), stored in line.Chromx1 ... Chromy2.
+void Cal_Chrom_Track(Line &line, int device = 0);
 
 // Cal_Orbit_Num (simtrack.cpp:14947-15030): 4D closed orbit at momentum
 // offset deltap by Newton iteration on the one-turn map (RF voltages off,

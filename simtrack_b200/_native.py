@@ -86,6 +86,7 @@ SIGNATURES = [
     ("stb_cal_tunes_track", c_int, [c_void_p, POINTER(c_double), c_int, c_double, c_double, POINTER(c_double),
                                     POINTER(c_int), c_int]),
     ("stb_cal_tunes_track_orbit", c_int, [c_void_p, c_double, c_double, c_double, POINTER(c_double), c_int]),
+    ("stb_cal_chrom_track", c_int, [c_void_p, c_double, c_double, POINTER(c_double), c_int]),
     ("stb_track_tbt", c_int, [c_void_p, POINTER(c_double), c_long, c_int, POINTER(c_double), POINTER(c_int),
                               POINTER(c_int), POINTER(c_int), c_int]),
     ("stb_track_tbt_bpm", c_int, [c_void_p, POINTER(c_double), c_long, c_int, POINTER(c_double), c_int, POINTER(c_int),

@@ -436,6 +436,14 @@ def Cal_Tunes_Track_orbit(line: Line, deltap0: float, tune_low: float = 0.660, t
     return t[0], t[1]
 
 
+def Cal_Chrom_Track(line: Line, tune_low: float = 0.660, tune_high: float = 0.70, device: int = 0):
+    """Cal_Chrom_Track (simtrack.cpp:21027-21051): (Chromx1, Chromy1, Chromx2,
+    Chromy2) from the tracked tunes at deltap = +3e-4, -3e-4 and 0."""
+    c = (c_double * 4)()
+    check(lib().stb_cal_chrom_track(line._h, tune_low, tune_high, c, device))
+    return tuple(c[:])
+
+
 def Track_tbt(line: Line, x, nturn: int, stable=None, device: int = 0, spin: bool = False, bpm_index=None):
     """Track_tbt (simtrack.cpp:20841-20860; with spin=True Track_tbt_spin,
     20863-20882, x[n, 9]) for particles x[n, 6] (copied): returns (x, stable,

@@ -646,6 +646,19 @@ int stb_cal_tunes_track(stb_line *l, double *x6, int nturn, double tune_lower, d
   });
 }
 
+int stb_cal_chrom_track(stb_line *l, double tune_lower, double tune_upper, double *chroms4, int device) {
+  return guarded([&] {
+    if (!l || !chroms4) throw Error(STB_EINVAL, "NULL argument");
+    with_tune_window(tune_lower, tune_upper, [&] { Cal_Chrom_Track(*Lp(l), device); });
+    const Line &L = *Lp(l);
+    chroms4[0] = L.Chromx1;
+    chroms4[1] = L.Chromy1;
+    chroms4[2] = L.Chromx2;
+    chroms4[3] = L.Chromy2;
+    return STB_OK;
+  });
+}
+
 int stb_cal_tunes_track_orbit(stb_line *l, double deltap0, double tune_lower, double tune_upper, double *tunes2,
                               int device) {
   return guarded([&] {

@@ -2,7 +2,8 @@
 // files: Track_DA (simtrack.cpp:21389-21441), Track_DA1 (21443-21495),
 // Track_DA2 (21497-21533), Track_DA3 (21535-21572), Track_DA_Radial
 // (21682-21734), Track_DA_Uniform (21574-21603), Track_DA_Radial_Uniform
-// (21736-21764); and Cal_Tunes_Track (20971-21025).
+// (21736-21764); and Cal_Tunes_Track (20971-21025), Cal_Chrom_Track
+// (21027-21051).
 //
 // The bisection drivers halve the stable amplitude interval [0, sigma_max] of
 // each phase angle until it is no longer than 0.1 sigma; every step tracks
@@ -251,6 +252,19 @@ void Cal_Tunes_Track(Line &line, double deltap0, int device) {
   tbt_tunes(line, x, Nturn, 1024, t1, t2, device);
   line.Tune1 = t1;
   line.Tune2 = t2;
+}
+
+void Cal_Chrom_Track(Line &line, int device) {
+  Cal_Tunes_Track(line, 0.0003, device);
+  const double qxp = line.Tune1, qyp = line.Tune2;
+  Cal_Tunes_Track(line, -0.0003, device);
+  const double qxm = line.Tune1, qym = line.Tune2;
+  Cal_Tunes_Track(line, 0.00, device);
+  const double qx0 = line.Tune1, qy0 = line.Tune2;
+  line.Chromx1 = (qxp - qxm) / 2. / 0.0003;
+  line.Chromy1 = (qyp - qym) / 2. / 0.0003;
+  line.Chromx2 = (qxp + qxm - 2 * qx0) / 2. / 0.0003 / 0.0003;
+  line.Chromy2 = (qyp + qym - 2 * qy0) / 2. / 0.0003 / 0.0003;
 }
 
 }  // namespace stb

@@ -96,3 +96,34 @@ def test_cal_tunes_track(ring, native_lib, ref_oracle):
     ref = (ref_oracle.fine_tune(tbt[:, 0], None, lo, hi), ref_oracle.fine_tune(tbt[:, 2], None, lo, hi))
     assert so == 1 and abs(q1 - ref[0]) < 1e-9 and abs(q2 - ref[1]) < 1e-9, ((q1, q2), ref)
     assert lo < q1 < hi and lo < q2 < hi
+
+
+def test_cal_chrom_track(ring, native_lib, ref_oracle):
+    """Cal_Chrom_Track (simtrack.cpp:21027): the chromaticities are the
+    reference's finite differences of the tracked closed-orbit tunes at
+    deltap = +3e-4, -3e-4 and 0.  As in the reference, a particle started on
+    an off-momentum closed orbit with x above 1e-9 is not displaced, so its
+    horizontal "tune" is that of rounding noise; only the vertical tunes,
+    whose start is raised by 1e-9, carry a betatron line.  Checked: the
+    result equals the formula on this library's Cal_Tunes_Track, whose
+    vertical tunes agree with the reference's FineTuneFinder within 1e-9."""
+    lat, line = ring
+    lat.set_reference()
+    lo, hi = 0.2, 0.45
+    got = api.Cal_Chrom_Track(line, lo, hi)
+    qp = api.Cal_Tunes_Track_orbit(line, 0.0003, lo, hi)
+    qm = api.Cal_Tunes_Track_orbit(line, -0.0003, lo, hi)
+    q0 = api.Cal_Tunes_Track_orbit(line, 0.0, lo, hi)
+    want = ((qp[0] - qm[0]) / 2. / 0.0003, (qp[1] - qm[1]) / 2. / 0.0003,
+            (qp[0] + qm[0] - 2 * q0[0]) / 2. / 0.0003 / 0.0003, (qp[1] + qm[1] - 2 * q0[1]) / 2. / 0.0003 / 0.0003)
+    assert got == want
+    ref_oracle.build(lat)
+    for dp, q in ((0.0003, qp), (-0.0003, qm)):
+        x0 = np.zeros(6)
+        x0[:4] = ref_oracle.cal_orbit(dp)[-1][:4]
+        x0[5] = dp
+        x0[0] += 1e-9 if x0[0] < 1e-9 else 0.0
+        x0[2] += 1e-9 if x0[2] < 1e-9 else 0.0
+        _, so, _, _, tbt = ref_oracle.track_tbt(x0, 1024)
+        assert so == 1
+        assert abs(q[1] - ref_oracle.fine_tune(tbt[:, 2], None, lo, hi)) < 1e-9
