@@ -2,7 +2,8 @@
 
 * The GSL shim's inverse normal CDF reproduces the N=11 strong-bunch slice
   table that BB6D hard-codes (simtrack.cpp:6593-6604) through the general
-  centroid formula (6612-6619), and the survey's N=5 / N=7 values.
+  centroid formula (6612-6619), and N=5 / N=7 centroids computed
+  independently with Python's AS241 inverse normal CDF.
 * The C restatement (oracle/port) is bit-identical to the compiled reference
   at every element: live when oracle/_ref is built, and against the golden
   fixtures in tests/golden/ (generated from the reference by
