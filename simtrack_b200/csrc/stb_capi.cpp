@@ -720,7 +720,8 @@ int stb_track_tbt_fma(stb_line *l, double deltap0, double sigmax0, double sigmay
   return guarded([&] {
     if (!l) throw Error(STB_EINVAL, "line is NULL");
     long r = 0;
-    with_tune_window(tune_lower, tune_upper, [&] { r = Track_tbt_FMA(*Lp(l), deltap0, sigmax0, sigmay0, filename, device); });
+    with_tune_window(tune_lower, tune_upper,
+                     [&] { r = Track_tbt_FMA(*Lp(l), deltap0, sigmax0, sigmay0, filename, device); });
     if (rows) *rows = r;
     return STB_OK;
   });

@@ -192,7 +192,8 @@ void Track_tbt_bpm_Batch(Line &line, double *x, long n, int nturn, double *x_tbt
   if (dump_bytes > 4.0e9)
     throw Error(STB_EINVAL, "particles x elements too large for the element record (over 4 GB per turn)");
   std::vector<char> rejected((size_t)n);
-  for (long i = 0; i < n; i++) rejected[i] = std::fabs(x[6 * i]) > 0.1 || std::fabs(x[6 * i + 2]) > 0.1 || stable[i] == 0;
+  for (long i = 0; i < n; i++)
+    rejected[i] = std::fabs(x[6 * i]) > 0.1 || std::fabs(x[6 * i + 2]) > 0.1 || stable[i] == 0;
   const bool in_line = bpm_index >= 0 && bpm_index < nelem;
   DeviceGuard g(device);
   TablePtr t = make_table(line, device);

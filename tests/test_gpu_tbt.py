@@ -140,8 +140,8 @@ def test_fma_matches_reference(native_lib, ref_oracle, tmp_path):
         x0 = X[grid.index((i, j))]
         _, so, _, _, tbt = ref_oracle.track_tbt(x0, 2048)
         assert so == 1
-        ref_t = [ref_oracle.fine_tune(tbt[0:1024, 0], None, lo, hi), ref_oracle.fine_tune(tbt[1023:2047, 0], None, lo, hi),
-                 ref_oracle.fine_tune(tbt[0:1024, 2], None, lo, hi), ref_oracle.fine_tune(tbt[1023:2047, 2], None, lo, hi)]
+        ref_t = [ref_oracle.fine_tune(tbt[a:b, k], None, lo, hi)
+                 for k, (a, b) in ((0, (0, 1024)), (0, (1023, 2047)), (2, (0, 1024)), (2, (1023, 2047)))]
         got = vals[r, 2:6]
         assert np.max(np.abs(got - ref_t)) < 1e-9, (i, j, got, ref_t)
         assert vals[r, 6] == got[0] - got[1] and vals[r, 7] == got[2] - got[3]
