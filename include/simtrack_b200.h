@@ -319,6 +319,11 @@ int stb_track_tbt_bpm(stb_line *l, double *x, long n, int nturn, double *x_tbt, 
  * tracking (Element::sPass), x AoS n*9 and x_tbt[(i*nturn + turn)*9 + k]. */
 int stb_track_tbt_spin(stb_line *l, double *x9, long n, int nturn, double *x_tbt9, int *stable, int *lost_turn,
                        int *lost_post, int device);
+/* Track_tbt_spin with a BPM index (simtrack.cpp:20907-20927): as
+ * stb_track_tbt_bpm with spin tracking and nine coordinates (n * ncell * 72 B
+ * < 4 GB). */
+int stb_track_tbt_spin_bpm(stb_line *l, double *x9, long n, int nturn, double *x_tbt9, int bpm_index, int *stable,
+                           int *lost_turn, int *lost_post, int device);
 /* Track_tbt_FMA (simtrack.cpp:21179-21241) with FineTuneFinder's window
  * [tune_lower, tune_upper) (the reference's globals tune_low/tune_high):
  * writes the reference's FMA-output.dat rows to `filename`; *rows = their

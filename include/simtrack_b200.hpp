@@ -357,6 +357,12 @@ void Track_tbt_spin(Line &line, double x[], int nturn, double x_tbt[], int &stab
                     int &lost_post);
 void Track_tbt_spin_Batch(Line &line, double *x9, long n, int nturn, double *x_tbt9, int *stable, int *lost_turn,
                           int *lost_post, int device = 0);
+// Track_tbt_spin() with a BPM index (simtrack.cpp:20907-20927): x[9] recorded
+// after element bpm_index; n x Ncell x 72 B must stay under 4 GB.
+void Track_tbt_spin(Line &line, double x[], int nturn, double x_tbt[], int &bpm_index, int &stable, int &lost_turn,
+                    int &lost_post);
+void Track_tbt_spin_bpm_Batch(Line &line, double *x9, long n, int nturn, double *x_tbt9, int bpm_index, int *stable,
+                              int *lost_turn, int *lost_post, int device = 0);
 
 // FineTuneFinder's search window used by Track_tbt_FMA (simtrack.cpp:27).
 extern double tune_low, tune_high;

@@ -162,6 +162,12 @@ void ref_track_tbt_bpm(void *line, double *x, int nturn, double *x_tbt, int bpm_
   Track_tbt(*static_cast<Line *>(line), x, nturn, x_tbt, bpm_index, *stable, *lost_turn, *lost_post);
 }
 
+// Track_tbt_spin with a BPM index (simtrack.cpp:20907).
+void ref_track_tbt_spin_bpm(void *line, double *x9, int nturn, double *x_tbt9, int bpm_index, int *stable,
+                            int *lost_turn, int *lost_post) {
+  Track_tbt_spin(*static_cast<Line *>(line), x9, nturn, x_tbt9, bpm_index, *stable, *lost_turn, *lost_post);
+}
+
 // Track_tbt_spin (simtrack.cpp:20863), the overload without a BPM index.
 void ref_track_tbt_spin(void *line, double *x9, int nturn, double *x_tbt9, int *stable, int *lost_turn,
                         int *lost_post) {

@@ -91,6 +91,8 @@ SIGNATURES = [
                               POINTER(c_int), POINTER(c_int), c_int]),
     ("stb_track_tbt_bpm", c_int, [c_void_p, POINTER(c_double), c_long, c_int, POINTER(c_double), c_int, POINTER(c_int),
                                   POINTER(c_int), POINTER(c_int), c_int]),
+    ("stb_track_tbt_spin_bpm", c_int, [c_void_p, POINTER(c_double), c_long, c_int, POINTER(c_double), c_int,
+                                       POINTER(c_int), POINTER(c_int), POINTER(c_int), c_int]),
     ("stb_track_tbt_spin", c_int, [c_void_p, POINTER(c_double), c_long, c_int, POINTER(c_double), POINTER(c_int),
                                    POINTER(c_int), POINTER(c_int), c_int]),
     ("stb_track_tbt_fma", c_int, [c_void_p, c_double, c_double, c_double, c_double, c_double, c_char_p,

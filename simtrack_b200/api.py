@@ -461,10 +461,9 @@ def Track_tbt(line: Line, x, nturn: int, stable=None, device: int = 0, spin: boo
     tbt = np.full((n, nturn, nc), np.nan)
     P = lambda a, t: a.ctypes.data_as(POINTER(t))
     if bpm_index is not None:
-        if spin:
-            raise ValueError("the BPM form is not available with spin")
-        check(lib().stb_track_tbt_bpm(line._h, P(x, c_double), n, nturn, P(tbt, c_double), int(bpm_index),
-                                      P(st, c_int), P(lt, c_int), P(lp, c_int), device))
+        fn = lib().stb_track_tbt_spin_bpm if spin else lib().stb_track_tbt_bpm
+        check(fn(line._h, P(x, c_double), n, nturn, P(tbt, c_double), int(bpm_index), P(st, c_int), P(lt, c_int),
+                 P(lp, c_int), device))
         return x, st, lt, lp, tbt
     fn = lib().stb_track_tbt_spin if spin else lib().stb_track_tbt
     check(fn(line._h, P(x, c_double), n, nturn, P(tbt, c_double), P(st, c_int), P(lt, c_int), P(lp, c_int), device))

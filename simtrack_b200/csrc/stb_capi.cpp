@@ -442,6 +442,12 @@ int spin_host(stb_table *t, double *xa, long n, int nturn, double radius, int *s
 
 }  // namespace
 
+// The same for spin tracking: dump[((i*nturn + turn)*nelem + j)*9 + k].
+void spin_device_dump(stb_table *t, double *const c[9], long n, int turn0, int nturn, int32_t *lost_turn,
+                      int32_t *lost_elem, double *dump) {
+  spin_device(t, c, n, turn0, nturn, 0.0, lost_turn, lost_elem, 0, dump);
+}
+
 // One-turn-block launch with the per-element record (the probe variant of the
 // tracking kernel): dump[((i*nturn + turn)*nelem + j)*6 + k] after element j.
 void track_device_dump(stb_table *t, double *const c[6], long n, int turn0, int nturn, int32_t *lost_turn,
@@ -702,6 +708,15 @@ int stb_track_tbt_bpm(stb_line *l, double *x, long n, int nturn, double *x_tbt, 
   return guarded([&] {
     if (!l) throw Error(STB_EINVAL, "line is NULL");
     Track_tbt_bpm_Batch(*Lp(l), x, n, nturn, x_tbt, bpm_index, stable, lost_turn, lost_post, device);
+    return STB_OK;
+  });
+}
+
+int stb_track_tbt_spin_bpm(stb_line *l, double *x9, long n, int nturn, double *x_tbt9, int bpm_index, int *stable,
+                           int *lost_turn, int *lost_post, int device) {
+  return guarded([&] {
+    if (!l) throw Error(STB_EINVAL, "line is NULL");
+    Track_tbt_spin_bpm_Batch(*Lp(l), x9, n, nturn, x_tbt9, bpm_index, stable, lost_turn, lost_post, device);
     return STB_OK;
   });
 }

@@ -57,6 +57,9 @@ inline void cuda_check(cudaError_t e, const char *what) {
 // element j (no circular aperture); default stream, asynchronous.
 void track_device_dump(stb_table *t, double *const c[6], long n, int turn0, int nturn, int32_t *lost_turn,
                        int32_t *lost_elem, double *dump);
+// The same for spin tracking (a spin table, nine arrays, dump[...*9 + k]).
+void spin_device_dump(stb_table *t, double *const c[9], long n, int turn0, int nturn, int32_t *lost_turn,
+                      int32_t *lost_elem, double *dump);
 
 // Restores the caller's current device on scope exit.
 struct DeviceGuard {

@@ -1,6 +1,6 @@
 // Turn-by-turn tracking and its diagnostics on the GPU: Track_tbt
 // (simtrack.cpp:20841-20860; with a BPM index 20884-20905), Track_tbt_spin
-// (20863-20882), Track_tbt_FMA
+// (20863-20882; with a BPM index 20907-20927), Track_tbt_FMA
 // (21179-21241) and Track_tbt_Lyapunov (21243-21306).
 //
 // A batch of particles is tracked one turn per launch; before every turn the
@@ -180,33 +180,48 @@ void Track_tbt_spin(Line &line, double x[], int nturn, double x_tbt[], int &stab
   Track_tbt_spin_Batch(line, x, 1, nturn, x_tbt, &stable, &lost_turn, &lost_post, 0);
 }
 
-void Track_tbt_bpm_Batch(Line &line, double *x, long n, int nturn, double *x_tbt, int bpm_index, int *stable,
-                         int *lost_turn, int *lost_post, int device) {
+namespace {
+
+// Track_tbt / Track_tbt_spin with a BPM index for n particles of nc = 6 or 9
+// coordinates: one-turn launches of the probe variant, whose record of the
+// element is copied out after each turn.
+void tbt_bpm_batch(Line &line, double *x, long n, int nc, int nturn, double *x_tbt, int bpm_index, int *stable,
+                   int *lost_turn, int *lost_post, int device) {
   if (n < 0 || nturn < 0) throw Error(STB_EINVAL, "negative particle count or turn count");
   if (n == 0) return;
   if (!x || !stable || !lost_turn || !lost_post) throw Error(STB_EINVAL, "NULL host buffer");
   const long nelem = line.Ncell;
   if (nelem < 1) throw Error(STB_EINVAL, "line has no elements");
   // the per-element record of one turn must fit a modest device buffer
-  const double dump_bytes = 48.0 * (double)n * (double)nelem;
+  const double dump_bytes = 8.0 * nc * (double)n * (double)nelem;
   if (dump_bytes > 4.0e9)
     throw Error(STB_EINVAL, "particles x elements too large for the element record (over 4 GB per turn)");
   std::vector<char> rejected((size_t)n);
   for (long i = 0; i < n; i++)
-    rejected[i] = std::fabs(x[6 * i]) > 0.1 || std::fabs(x[6 * i + 2]) > 0.1 || stable[i] == 0;
+    rejected[i] = std::fabs(x[(size_t)nc * i]) > 0.1 || std::fabs(x[(size_t)nc * i + 2]) > 0.1 || stable[i] == 0;
   const bool in_line = bpm_index >= 0 && bpm_index < nelem;
   DeviceGuard g(device);
-  TablePtr t = make_table(line, device);
-  DeviceBatch b(x, stable, n, 6);
+  stb_table *raw = nullptr;
+  if (nc == 9)
+    check(stb_table_create_spin(reinterpret_cast<const stb_line *>(&line), device, &raw));
+  else
+    check(stb_table_create(reinterpret_cast<const stb_line *>(&line), device, &raw));
+  TablePtr t(raw, stb_table_free);
+  DeviceBatch b(x, stable, n, nc);
   DevMem dump((size_t)dump_bytes);
-  DevMem rec(sizeof(double) * 6 * (size_t)n * (size_t)nturn);  // [turn][i][6]
-  double *const c[6] = {b.c(0), b.c(1), b.c(2), b.c(3), b.c(4), b.c(5)};
+  DevMem rec(sizeof(double) * nc * (size_t)n * (size_t)nturn);  // [turn][i][nc]
+  double *c[9];
+  for (int k = 0; k < nc; k++) c[k] = b.c(k);
+  const size_t row = (size_t)nc * sizeof(double);
   for (int turn = 0; turn < nturn; turn++) {
-    track_device_dump(t.get(), c, n, turn, 1, b.lost_turn(), b.lost_elem(), dump.as<double>());
+    if (nc == 9)
+      spin_device_dump(t.get(), c, n, turn, 1, b.lost_turn(), b.lost_elem(), dump.as<double>());
+    else
+      track_device_dump(t.get(), c, n, turn, 1, b.lost_turn(), b.lost_elem(), dump.as<double>());
     if (in_line)
-      cuda_check(cudaMemcpy2DAsync(rec.as<double>() + (size_t)turn * n * 6, 6 * sizeof(double),
-                                   dump.as<double>() + (size_t)bpm_index * 6, (size_t)nelem * 6 * sizeof(double),
-                                   6 * sizeof(double), (size_t)n, cudaMemcpyDeviceToDevice, 0),
+      cuda_check(cudaMemcpy2DAsync(rec.as<double>() + (size_t)turn * n * nc, row,
+                                   dump.as<double>() + (size_t)bpm_index * nc, (size_t)nelem * row, row, (size_t)n,
+                                   cudaMemcpyDeviceToDevice, 0),
                  "record element");
   }
   cuda_check(cudaDeviceSynchronize(), "turn-by-turn tracking");
@@ -215,7 +230,7 @@ void Track_tbt_bpm_Batch(Line &line, double *x, long n, int nturn, double *x_tbt
   if (st != 0) throw Error(st, "tracking kernel reported status " + std::to_string(st));
   b.download(x, stable, lost_turn, lost_post);
   if (!x_tbt || !in_line) return;
-  std::vector<double> r((size_t)6 * n * nturn);
+  std::vector<double> r((size_t)nc * n * nturn);
   cuda_check(cudaMemcpy(r.data(), rec.p, sizeof(double) * r.size(), cudaMemcpyDeviceToHost), "download record");
   // a turn is recorded when the particle passed the element in it: every turn
   // before its loss, and the turn of the loss if it came at or after the element
@@ -224,8 +239,26 @@ void Track_tbt_bpm_Batch(Line &line, double *x, long n, int nturn, double *x_tbt
     int last = nturn;
     if (!stable[i]) last = lost_post[i] >= bpm_index ? lost_turn[i] + 1 : lost_turn[i];
     for (int turn = 0; turn < last; turn++)
-      for (int k = 0; k < 6; k++) x_tbt[((size_t)i * nturn + turn) * 6 + k] = r[((size_t)turn * n + i) * 6 + k];
+      for (int k = 0; k < nc; k++)
+        x_tbt[((size_t)i * nturn + turn) * nc + k] = r[((size_t)turn * n + i) * nc + k];
   }
+}
+
+}  // namespace
+
+void Track_tbt_bpm_Batch(Line &line, double *x, long n, int nturn, double *x_tbt, int bpm_index, int *stable,
+                         int *lost_turn, int *lost_post, int device) {
+  tbt_bpm_batch(line, x, n, 6, nturn, x_tbt, bpm_index, stable, lost_turn, lost_post, device);
+}
+
+void Track_tbt_spin_bpm_Batch(Line &line, double *x9, long n, int nturn, double *x_tbt9, int bpm_index, int *stable,
+                              int *lost_turn, int *lost_post, int device) {
+  tbt_bpm_batch(line, x9, n, 9, nturn, x_tbt9, bpm_index, stable, lost_turn, lost_post, device);
+}
+
+void Track_tbt_spin(Line &line, double x[], int nturn, double x_tbt[], int &bpm_index, int &stable, int &lost_turn,
+                    int &lost_post) {
+  Track_tbt_spin_bpm_Batch(line, x, 1, nturn, x_tbt, bpm_index, &stable, &lost_turn, &lost_post, 0);
 }
 
 void Track_tbt(Line &line, double x[], int nturn, double x_tbt[], int &bpm_index, int &stable, int &lost_turn,

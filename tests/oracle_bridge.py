@@ -75,6 +75,8 @@ class RefOracle:
         L.ref_line_read_bmad.restype = c_void_p
         L.ref_track_tbt.argtypes = [c_void_p, POINTER(c_double), c_int, POINTER(c_double), POINTER(c_int),
                                     POINTER(c_int), POINTER(c_int)]
+        L.ref_track_tbt_spin_bpm.argtypes = [c_void_p, POINTER(c_double), c_int, POINTER(c_double), c_int,
+                                             POINTER(c_int), POINTER(c_int), POINTER(c_int)]
         L.ref_track_tbt_bpm.argtypes = [c_void_p, POINTER(c_double), c_int, POINTER(c_double), c_int, POINTER(c_int),
                                         POINTER(c_int), POINTER(c_int)]
         L.ref_track_tbt_spin.argtypes = [c_void_p, POINTER(c_double), c_int, POINTER(c_double), POINTER(c_int),
@@ -188,13 +190,14 @@ class RefOracle:
         return x, st.value, lt.value, lp.value, tbt
 
     def track_tbt_bpm(self, x0, nturn: int, bpm_index: int):
-        """Track_tbt with a BPM index: (x, stable, lost_turn, lost_post, x_tbt[nturn, 6]), NaN where not recorded."""
+        """Track_tbt with a BPM index (Track_tbt_spin for x0 of 9): (x, stable,
+        lost_turn, lost_post, x_tbt[nturn, 6 or 9]), NaN where not recorded."""
         x = np.ascontiguousarray(x0, dtype=np.float64).copy()
-        tbt = np.full((nturn, 6), np.nan)
+        tbt = np.full((nturn, len(x)), np.nan)
         st, lt, lp = c_int(1), c_int(0), c_int(0)
-        self.L.ref_track_tbt_bpm(self.line, x.ctypes.data_as(POINTER(c_double)), nturn,
-                                 tbt.ctypes.data_as(POINTER(c_double)), bpm_index, ctypes.byref(st), ctypes.byref(lt),
-                                 ctypes.byref(lp))
+        fn = self.L.ref_track_tbt_spin_bpm if len(x) == 9 else self.L.ref_track_tbt_bpm
+        fn(self.line, x.ctypes.data_as(POINTER(c_double)), nturn, tbt.ctypes.data_as(POINTER(c_double)), bpm_index,
+           ctypes.byref(st), ctypes.byref(lt), ctypes.byref(lp))
         return x, st.value, lt.value, lp.value, tbt
 
     def element(self, i: int):

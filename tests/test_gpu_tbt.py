@@ -78,6 +78,23 @@ def test_track_tbt_bpm_record(which, bpm, native_lib, ref_oracle):
         assert _same(x[i], xo), f"particle {i}: final coordinates differ"
 
 
+@pytest.mark.parametrize("bpm", [0, 12, 33])
+def test_track_tbt_spin_bpm_record(bpm, native_lib, ref_oracle):
+    """Track_tbt_spin with a BPM index (simtrack.cpp:20907): the nine
+    coordinates after element `bpm` in every turn that reaches it."""
+    from lattice_zoo import spin_particles, spin_zoo
+    lat = spin_zoo()
+    line = lt.build_line(lat)
+    X = spin_particles()
+    nt = 3
+    x, st, ltn, lp, tbt = api.Track_tbt(line, X, nt, spin=True, bpm_index=bpm)
+    ref_oracle.build(lat)
+    for i, x0 in enumerate(X):
+        xo, so, lo, po, to = ref_oracle.track_tbt_bpm(x0, nt, bpm)
+        assert (st[i], ltn[i], lp[i]) == (so, lo, po), f"particle {i}"
+        assert _same(tbt[i], to), f"particle {i}: record differs"
+
+
 def test_track_tbt_spin_record(native_lib, ref_oracle):
     """Track_tbt_spin (simtrack.cpp:20863): the nine-coordinate record."""
     from lattice_zoo import spin_particles, spin_zoo
