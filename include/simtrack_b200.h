@@ -223,6 +223,15 @@ int stb_track_radial_device(stb_table *t, double *x, double *px, double *y, doub
                             int32_t *lost_elem, void *stream);
 int stb_track_radial_host(stb_table *t, double *x, long n, int nturn, double aperture_radius, int *stable,
                           int *lost_turn, int *lost_post);
+/* Cal_dz0_OnMomentumPart (simtrack.cpp:20929-20940): x0[6] (host, in/out)
+ * through every element with z and pt reset before each; dz0 (host, ncell)
+ * receives its z after each element. */
+int stb_cal_dz0(stb_line *l, double *x0, double *dz0, int device);
+/* Track_wrt_OnMomentumPart (simtrack.cpp:20942-20967): as stb_track_radial_host
+ * (no circular aperture) with the caller's dz0[ncell] in place of the
+ * on-momentum path. */
+int stb_track_wrt_onmom(stb_line *l, double *x, long n, const double *dz0, int nturn, int *stable, int *lost_turn,
+                        int *lost_post, int device);
 /* Per-element probe of Track_Radial (layout as stb_track_probe). */
 int stb_track_radial_probe(stb_table *t, double *x, long n, int nturn, double aperture_radius, double *dump,
                            int *stable, int *lost_turn, int *lost_post);

@@ -382,6 +382,18 @@ long Track_tbt_FMA(Line &line, double deltap0, double sigmax0, double sigmay0,
 long Track_tbt_Lyapunov(Line &line, double deltap0, double sigmax0, double sigmay0,
                         const char *filename = "./Lmap-output.dat", int device = 0);
 
+// Cal_dz0_OnMomentumPart (simtrack.cpp:20929-20940): x0[6] (in/out) passes
+// every element with z and pt reset to zero before each; dz0[j] (Ncell
+// entries) = its z after element j.  Track_wrt_OnMomentumPart (20942-20967):
+// Track() with dz0[j] subtracted from z after every element j (Track_Radial
+// with a caller-supplied path).  The batch form takes AoS x[n*6].
+void Cal_dz0_OnMomentumPart(Line &line, double x0[], double dz0[]);
+void Cal_dz0_OnMomentumPart_dev(Line &line, double x0[], double dz0[], int device);
+void Track_wrt_OnMomentumPart(Line &line, double x[], double dz0[], int nturn, int &stable, int &lost_turn,
+                              int &lost_post);
+void Track_wrt_OnMomentumPart_Batch(Line &line, double *x, long n, const double *dz0, int nturn, int *stable,
+                                    int *lost_turn, int *lost_post, int device = 0);
+
 // Track_Radial() drop-in (simtrack.cpp:21641-21680): Track() with z taken
 // relative to the on-momentum reference particle after every element.
 void Track_Radial(Line &line, double x[], int nturn, int &stable, int &lost_turn, int &lost_post);

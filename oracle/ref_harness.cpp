@@ -156,6 +156,22 @@ void ref_track_tbt(void *line, double *x, int nturn, double *x_tbt, int *stable,
   Track_tbt(*static_cast<Line *>(line), x, nturn, x_tbt, *stable, *lost_turn, *lost_post);
 }
 
+// Cal_dz0_OnMomentumPart / Track_wrt_OnMomentumPart (simtrack.cpp:20929, 20942).
+void ref_cal_dz0(void *line, double *x0, double *dz0) {
+  Cal_dz0_OnMomentumPart(*static_cast<Line *>(line), x0, dz0);
+}
+void ref_track_wrt_onmom(void *line, double *x, long n, double *dz0, int nturn, int *stable, int *lost_turn,
+                         int *lost_post) {
+  Line &l = *static_cast<Line *>(line);
+  for (long i = 0; i < n; i++) {
+    int st = 1, lt = 0, lp = 0;
+    Track_wrt_OnMomentumPart(l, x + 6 * i, dz0, nturn, st, lt, lp);
+    stable[i] = st;
+    lost_turn[i] = lt;
+    lost_post[i] = lp;
+  }
+}
+
 // Track_tbt with a BPM index (simtrack.cpp:20884).
 void ref_track_tbt_bpm(void *line, double *x, int nturn, double *x_tbt, int bpm_index, int *stable, int *lost_turn,
                        int *lost_post) {

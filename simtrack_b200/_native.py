@@ -91,6 +91,9 @@ SIGNATURES = [
                               POINTER(c_int), POINTER(c_int), c_int]),
     ("stb_track_tbt_bpm", c_int, [c_void_p, POINTER(c_double), c_long, c_int, POINTER(c_double), c_int, POINTER(c_int),
                                   POINTER(c_int), POINTER(c_int), c_int]),
+    ("stb_cal_dz0", c_int, [c_void_p, POINTER(c_double), POINTER(c_double), c_int]),
+    ("stb_track_wrt_onmom", c_int, [c_void_p, POINTER(c_double), c_long, POINTER(c_double), c_int, POINTER(c_int),
+                                    POINTER(c_int), POINTER(c_int), c_int]),
     ("stb_track_tbt_spin_bpm", c_int, [c_void_p, POINTER(c_double), c_long, c_int, POINTER(c_double), c_int,
                                        POINTER(c_int), POINTER(c_int), POINTER(c_int), c_int]),
     ("stb_track_tbt_spin", c_int, [c_void_p, POINTER(c_double), c_long, c_int, POINTER(c_double), POINTER(c_int),

@@ -436,6 +436,31 @@ def Cal_Tunes_Track_orbit(line: Line, deltap0: float, tune_low: float = 0.660, t
     return t[0], t[1]
 
 
+def Cal_dz0_OnMomentumPart(line: Line, x0, device: int = 0):
+    """Cal_dz0_OnMomentumPart (simtrack.cpp:20929-20940): returns (x0 after
+    the pass, dz0[ncell]); z and pt are reset before every element."""
+    x = np.ascontiguousarray(x0, dtype=np.float64).copy()
+    dz0 = np.empty(line.Ncell)
+    check(lib().stb_cal_dz0(line._h, x.ctypes.data_as(POINTER(c_double)), dz0.ctypes.data_as(POINTER(c_double)),
+                            device))
+    return x, dz0
+
+
+def Track_wrt_OnMomentumPart(line: Line, x, dz0, nturn: int, device: int = 0):
+    """Track_wrt_OnMomentumPart (simtrack.cpp:20942-20967) for x[n, 6]
+    (copied): returns (x, stable, lost_turn, lost_post)."""
+    x = np.ascontiguousarray(np.atleast_2d(np.asarray(x, dtype=np.float64))).copy()
+    d = np.ascontiguousarray(dz0, dtype=np.float64)
+    n = x.shape[0]
+    st = np.ones(n, dtype=np.int32)
+    lt = np.zeros(n, dtype=np.int32)
+    lp = np.zeros(n, dtype=np.int32)
+    P = lambda a, t: a.ctypes.data_as(POINTER(t))
+    check(lib().stb_track_wrt_onmom(line._h, P(x, c_double), n, P(d, c_double), nturn, P(st, c_int), P(lt, c_int),
+                                    P(lp, c_int), device))
+    return x, st, lt, lp
+
+
 def Cal_Chrom_Track(line: Line, tune_low: float = 0.660, tune_high: float = 0.70, device: int = 0):
     """Cal_Chrom_Track (simtrack.cpp:21027-21051): (Chromx1, Chromy1, Chromx2,
     Chromy2) from the tracked tunes at deltap = +3e-4, -3e-4 and 0."""

@@ -473,6 +473,42 @@ void Track_Radial(Line &line, double x[], int nturn, int &stable, int &lost_turn
   if (rc != STB_OK) throw Error(rc, last_error());
 }
 
+void Cal_dz0_OnMomentumPart_dev(Line &line, double x0[], double dz0[], int device) {
+  if (!x0 || !dz0) throw Error(STB_EINVAL, "NULL buffer");
+  std::unique_ptr<stb_table, void (*)(stb_table *)> t(table_build(line, device), table_destroy);
+  DeviceGuard g(device);
+  const size_t ne = t->host.hdr.size();
+  double *d = nullptr;
+  cuda_check(cudaMalloc(&d, sizeof(double) * (6 + ne)), "cudaMalloc(on-momentum pass)");
+  std::unique_ptr<double, cudaError_t (*)(void *)> hold(d, cudaFree);
+  cuda_check(cudaMemcpy(d, x0, sizeof(double) * 6, cudaMemcpyHostToDevice), "upload x0");
+  cuda_check(launch_onmom_dz0(make_args(t.get()), d, d + 6, 0), "on-momentum pass launch");
+  cuda_check(cudaDeviceSynchronize(), "on-momentum pass");
+  cuda_check(cudaMemcpy(x0, d, sizeof(double) * 6, cudaMemcpyDeviceToHost), "download x0");
+  cuda_check(cudaMemcpy(dz0, d + 6, sizeof(double) * ne, cudaMemcpyDeviceToHost), "download dz0");
+}
+
+void Cal_dz0_OnMomentumPart(Line &line, double x0[], double dz0[]) { Cal_dz0_OnMomentumPart_dev(line, x0, dz0, 0); }
+
+void Track_wrt_OnMomentumPart_Batch(Line &line, double *x, long n, const double *dz0, int nturn, int *stable,
+                                    int *lost_turn, int *lost_post, int device) {
+  if (!dz0) throw Error(STB_EINVAL, "NULL dz0");
+  std::unique_ptr<stb_table, void (*)(stb_table *)> t(table_build(line, device), table_destroy);
+  DeviceGuard g(device);
+  const size_t ne = t->host.hdr.size();
+  double *zs = nullptr;
+  cuda_check(cudaMalloc(&zs, sizeof(double) * ne), "cudaMalloc(dz0)");
+  t->d_zsub = zs;  // owned by the table from here on
+  cuda_check(cudaMemcpy(zs, dz0, sizeof(double) * ne, cudaMemcpyHostToDevice), "upload dz0");
+  const int rc = radial_host(t.get(), x, n, nturn, 0.0, stable, lost_turn, lost_post);
+  if (rc != STB_OK) throw Error(rc, last_error());
+}
+
+void Track_wrt_OnMomentumPart(Line &line, double x[], double dz0[], int nturn, int &stable, int &lost_turn,
+                              int &lost_post) {
+  Track_wrt_OnMomentumPart_Batch(line, x, 1, dz0, nturn, &stable, &lost_turn, &lost_post, 0);
+}
+
 void Track_Spin(Line &line, double x[], int nturn, int &stable, int &lost_turn, int &lost_post) {
   std::unique_ptr<stb_table, void (*)(stb_table *)> t(table_build(line, 0, true), table_destroy);
   int rc = spin_host(t.get(), x, 1, nturn, 0.0, &stable, &lost_turn, &lost_post);
@@ -708,6 +744,23 @@ int stb_track_tbt_bpm(stb_line *l, double *x, long n, int nturn, double *x_tbt, 
   return guarded([&] {
     if (!l) throw Error(STB_EINVAL, "line is NULL");
     Track_tbt_bpm_Batch(*Lp(l), x, n, nturn, x_tbt, bpm_index, stable, lost_turn, lost_post, device);
+    return STB_OK;
+  });
+}
+
+int stb_cal_dz0(stb_line *l, double *x0, double *dz0, int device) {
+  return guarded([&] {
+    if (!l) throw Error(STB_EINVAL, "line is NULL");
+    Cal_dz0_OnMomentumPart_dev(*Lp(l), x0, dz0, device);
+    return STB_OK;
+  });
+}
+
+int stb_track_wrt_onmom(stb_line *l, double *x, long n, const double *dz0, int nturn, int *stable, int *lost_turn,
+                        int *lost_post, int device) {
+  return guarded([&] {
+    if (!l) throw Error(STB_EINVAL, "line is NULL");
+    Track_wrt_OnMomentumPart_Batch(*Lp(l), x, n, dz0, nturn, stable, lost_turn, lost_post, device);
     return STB_OK;
   });
 }

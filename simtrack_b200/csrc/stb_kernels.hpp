@@ -56,6 +56,9 @@ cudaError_t launch_spin(const SpinArgs &a, int num_sms, bool use_smem, cudaStrea
 // that subtracts it after every element.
 cudaError_t launch_radial_reference(const TrackArgs &a, double *zsub, cudaStream_t stream);
 cudaError_t launch_radial(const TrackArgs &a, const double *zsub, int num_sms, bool use_smem, cudaStream_t stream);
+// Cal_dz0_OnMomentumPart (stb_radial.cu): x0[6] (device, in/out) through every
+// element with z and pt reset before each, dz0[j] = z after element j.
+cudaError_t launch_onmom_dz0(const TrackArgs &a, double *x0, double *dz0, cudaStream_t stream);
 
 // Elementary-function diagnostics (stb_diag.cu).
 int math_input_arity(int fn);

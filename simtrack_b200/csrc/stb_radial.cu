@@ -32,6 +32,25 @@ __global__ void radial_ref_kernel(const __grid_constant__ TrackArgs a, double *z
   }
 }
 
+// Cal_dz0_OnMomentumPart (simtrack.cpp:20929-20940): the particle x0 (six
+// coordinates, in/out) passes every element with z and pt reset to zero
+// before it; dz0[j] = its z after element j.  One device thread.
+__global__ void onmom_dz0_kernel(const __grid_constant__ TrackArgs a, double *x0, double *dz0) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  const RefConsts &R = a.ref;
+  Particle p[1] = {Particle{x0[0], x0[1], x0[2], x0[3], x0[4], x0[5]}};
+  PtCache c[1];
+  for (int j = 0; j < a.nelem; j++) {
+    p[0].z = 0.;
+    p[0].pt = 0.;
+    pt_refresh(R, 0.0, c[0]);
+    const ElemHeader h = a.hdr[j];
+    apply_element<1>(h, a.pool + h.poff, p, c, R);
+    dz0[j] = p[0].z;
+  }
+  x0[0] = p[0].x; x0[1] = p[0].px; x0[2] = p[0].y; x0[3] = p[0].py; x0[4] = p[0].z; x0[5] = p[0].pt;
+}
+
 template <bool kSmem, int kBlock, bool kDump>
 __global__ void __launch_bounds__(kBlock, 1) radial_track_kernel(const __grid_constant__ TrackArgs a,
                                                                   const double *zsub) {
@@ -112,6 +131,11 @@ cudaError_t launch_radial_variant(const TrackArgs &a, const double *zsub, int nu
 
 cudaError_t launch_radial_reference(const TrackArgs &a, double *zsub, cudaStream_t stream) {
   radial_ref_kernel<<<1, 32, 0, stream>>>(a, zsub);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_onmom_dz0(const TrackArgs &a, double *x0, double *dz0, cudaStream_t stream) {
+  onmom_dz0_kernel<<<1, 32, 0, stream>>>(a, x0, dz0);
   return cudaGetLastError();
 }
 

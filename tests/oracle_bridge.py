@@ -75,6 +75,9 @@ class RefOracle:
         L.ref_line_read_bmad.restype = c_void_p
         L.ref_track_tbt.argtypes = [c_void_p, POINTER(c_double), c_int, POINTER(c_double), POINTER(c_int),
                                     POINTER(c_int), POINTER(c_int)]
+        L.ref_cal_dz0.argtypes = [c_void_p, POINTER(c_double), POINTER(c_double)]
+        L.ref_track_wrt_onmom.argtypes = [c_void_p, POINTER(c_double), c_long, POINTER(c_double), c_int,
+                                          POINTER(c_int), POINTER(c_int), POINTER(c_int)]
         L.ref_track_tbt_spin_bpm.argtypes = [c_void_p, POINTER(c_double), c_int, POINTER(c_double), c_int,
                                              POINTER(c_int), POINTER(c_int), POINTER(c_int)]
         L.ref_track_tbt_bpm.argtypes = [c_void_p, POINTER(c_double), c_int, POINTER(c_double), c_int, POINTER(c_int),

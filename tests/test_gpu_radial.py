@@ -75,3 +75,42 @@ def test_track_da_reproduces_reference_file(tmp_path, native_lib, ref_oracle):
     assert ours.read_text() == theirs.read_text()
     # the bisections end inside the interval, at different amplitudes per angle
     assert np.all(s > 1) and np.all(s < 49) and len(set(s.tolist())) > 3
+
+
+def test_onmom_dz0_and_tracking_wrt_it(native_lib, ref_oracle):
+    """Cal_dz0_OnMomentumPart and Track_wrt_OnMomentumPart (simtrack.cpp:20929,
+    20942) on the RHIC-like ring with offset quadrupoles, started from its
+    closed orbit: dz0 and the pass's end point equal the reference's, and
+    tracking with that dz0 gives the reference's coordinates and losses."""
+    from ctypes import POINTER, c_double, c_int
+    from simtrack_b200.api import Cal_dz0_OnMomentumPart, Cal_Orbit_Num, Track_wrt_OnMomentumPart
+    lat = lt.rhic_like_ring(seed=3)
+    rng = np.random.default_rng(11)
+    for e in lat.elements:
+        if e.type == "QUAD" and rng.random() < 0.1:
+            e.misalign = (rng.normal(0, 1e-4), rng.normal(0, 1e-4), 0.0, 0.0, 0.0, 0.0)
+    line = lt.build_line(lat)
+    x0 = np.zeros(6)
+    x0[:4] = Cal_Orbit_Num(line, 0.0)[-1][:4]
+    xe, dz0 = Cal_dz0_OnMomentumPart(line, x0)
+    ref_oracle.build(lat)
+    xr = x0.copy()
+    dr = np.empty(len(lat.elements))
+    ref_oracle.L.ref_cal_dz0(ref_oracle.line, xr.ctypes.data_as(POINTER(c_double)),
+                             dr.ctypes.data_as(POINTER(c_double)))
+    assert np.max(np.abs(dz0)) > 0
+    assert_close(dz0.reshape(-1, 1), dr.reshape(-1, 1), "dz0")
+    assert_close(xe.reshape(1, 6), xr.reshape(1, 6), "end of the pass")
+    sig = lat.meta["sigma_ip"]
+    X = np.array([[a * sig, 0, 0.6 * a * sig, 0, 0.01, 3e-4] for a in (0.5, 3.0, 8.0, 20.0)])
+    nt = 40
+    xg, sg, lg, pg = Track_wrt_OnMomentumPart(line, X, dz0, nt)
+    xo = X.copy()
+    so = np.ones(len(X), dtype=np.int32)
+    lo = np.zeros(len(X), dtype=np.int32)
+    po = np.zeros(len(X), dtype=np.int32)
+    P = lambda a, t: a.ctypes.data_as(POINTER(t))
+    ref_oracle.L.ref_track_wrt_onmom(ref_oracle.line, P(xo, c_double), len(X), P(dz0, c_double), nt, P(so, c_int),
+                                     P(lo, c_int), P(po, c_int))
+    assert np.array_equal(sg, so) and np.array_equal(lg, lo) and np.array_equal(pg, po)
+    assert_close(xg, xo, "tracked with dz0")
