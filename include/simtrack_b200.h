@@ -154,7 +154,10 @@ int stb_track_host(stb_table *t, double *x, long n, int nturn, double aperture_r
  * before use.  The first call on a device looks the scratch up
  * (cudaGetSymbolAddress); make it before any stream capture begins on that
  * device.  Calls that overlap in time on one device race on the shared
- * scratch.  Waits for `stream` before returning. */
+ * scratch.  Every call reads its status word back and waits for `stream`
+ * before returning.  The looked-up address lives as long as the CUDA
+ * context: after cudaDeviceReset no handle of this library (tables, scans,
+ * this scratch) may be used again. */
 #define STB_STATIC_MAX_SEEDS 64
 #define STB_STATIC_MAX_PARTICLES 1048576
 int stb_track_seeds_static(stb_table *const *tables, int nseed, const long *n_per_seed, double *x, double *px,

@@ -224,6 +224,32 @@ NUM_VARIANTS = 11
 NUM_SCAN_VARIANTS = 7
 
 
+def _check_device_arrays(coords, lost_turn, lost_elem, n: int, device: int, ncoord: int = 6) -> None:
+    """Rejects device buffers the C entry points cannot check themselves:
+    `ncoord` contiguous CUDA float64 arrays of at least n entries and two
+    contiguous CUDA int32 arrays of at least n entries, all on `device`."""
+    import torch
+    if len(coords) != ncoord:
+        raise ValueError(f"expected {ncoord} coordinate arrays, got {len(coords)}")
+
+    def ok(t, dtype, what):
+        if not isinstance(t, torch.Tensor):
+            raise ValueError(f"{what} must be a torch tensor")
+        if t.device.type != "cuda" or t.device.index != device:
+            raise ValueError(f"{what} must be on cuda:{device}, not {t.device}")
+        if t.dtype != dtype:
+            raise ValueError(f"{what} must be {dtype}, not {t.dtype}")
+        if not t.is_contiguous():
+            raise ValueError(f"{what} must be contiguous")
+        if t.numel() < n:
+            raise ValueError(f"{what} holds {t.numel()} entries, {n} needed")
+
+    for k, c in enumerate(coords):
+        ok(c, torch.float64, f"coordinate array {k}")
+    ok(lost_turn, torch.int32, "lost_turn")
+    ok(lost_elem, torch.int32, "lost_elem")
+
+
 def variant_name(v: int) -> str:
     buf = ctypes.create_string_buffer(64)
     b, sm = c_int(), c_int()
@@ -290,6 +316,7 @@ class Table:
     def track_radial_device(self, coords, lost_turn, lost_elem, turn0: int, nturn: int,
                             aperture_radius: float = 0.0, stream=None) -> None:
         n = coords[0].numel()
+        _check_device_arrays(coords, lost_turn, lost_elem, n, self.device)
         s = None if stream is None else c_void_p(stream)
         check(lib().stb_track_radial_device(self._h, *[c_void_p(c.data_ptr()) for c in coords], n, turn0, nturn,
                                             aperture_radius, c_void_p(lost_turn.data_ptr()),
@@ -312,8 +339,9 @@ class Table:
     def track_device(self, coords, lost_turn, lost_elem, turn0: int, nturn: int, aperture_radius: float = 0.0,
                      stream=None) -> None:
         """Track SoA device tensors in place (coords: 6 CUDA float64 tensors; lost_*: int32 tensors)."""
-        ptrs = [c.data_ptr() for c in coords]
         n = coords[0].numel()
+        _check_device_arrays(coords, lost_turn, lost_elem, n, self.device)
+        ptrs = [c.data_ptr() for c in coords]
         s = None if stream is None else c_void_p(stream)
         check(lib().stb_track_device(self._h, *[c_void_p(p) for p in ptrs], n, turn0, nturn, aperture_radius,
                                      c_void_p(lost_turn.data_ptr()), c_void_p(lost_elem.data_ptr()), s))
@@ -372,6 +400,7 @@ class SpinTable:
                      stream=None) -> None:
         """coords: 9 CUDA float64 tensors (x, px, y, py, z, pt, sx, sy, sz), updated in place."""
         n = coords[0].numel()
+        _check_device_arrays(coords, lost_turn, lost_elem, n, self.device, ncoord=9)
         s = None if stream is None else c_void_p(stream)
         check(lib().stb_track_spin_device(self._h, *[c_void_p(c.data_ptr()) for c in coords], n, turn0, nturn,
                                           aperture_radius, c_void_p(lost_turn.data_ptr()),
@@ -644,6 +673,12 @@ def track_seeds_static(tables, n_per_seed, coords, lost_turn, lost_elem, turn0: 
     work-list launch without allocating device memory.  coords: CUDA float64
     tensor [6, n] (x, px, y, py, z, pt rows; seed 0's particles first);
     lost_turn, lost_elem: CUDA int32 tensors [n]."""
+    if len(tables) != len(n_per_seed) or not tables:
+        raise ValueError("one particle count per table")
+    ntot = int(sum(int(v) for v in n_per_seed))
+    if coords.dim() != 2 or coords.shape[0] != 6 or coords.shape[1] < ntot:
+        raise ValueError(f"coords must have shape [6, >= {ntot}], not {tuple(coords.shape)}")
+    _check_device_arrays([coords[k] for k in range(6)], lost_turn, lost_elem, ntot, tables[0].device)
     arr = (c_void_p * len(tables))(*[t._h for t in tables])
     nps = (ctypes.c_long * len(tables))(*[int(v) for v in n_per_seed])
     ptrs = [c_void_p(coords[k].data_ptr()) for k in range(6)]

@@ -57,15 +57,25 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     LIBDIR.mkdir(exist_ok=True)
     objdir = LIBDIR / "obj"
     objdir.mkdir(exist_ok=True)
-    objs = []
+    common_deps = deps[len(srcs):]
+    jobs = []
     for s in srcs:
         o = objdir / (s.name + ".o")
         cmd = [nvcc(), *ARCH, *COMMON, "-fmad=false", "-x", "cu" if s.suffix == ".cu" else "c++",
                "-c", str(s), "-o", str(o)]
+        if force or _stale(o, [s] + common_deps):
+            jobs.append(cmd)
+    objs = [str(objdir / (s.name + ".o")) for s in srcs]
+
+    def run(cmd):
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
-        objs.append(str(o))
+
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        for f in [ex.submit(run, c) for c in jobs]:
+            f.result()
     cmd = [nvcc(), *ARCH, "-shared", "-o", str(LIB), *objs, "-lcudart_static", "-lrt", "-lpthread", "-ldl"]
     if verbose:
         print(" ".join(cmd), flush=True)

@@ -9,6 +9,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -86,6 +87,8 @@ void table_destroy(stb_table *t) {
   if (t->d_pool) cudaFree(t->d_pool);
   if (t->d_status) cudaFree(t->d_status);
   if (t->d_zsub) cudaFree(t->d_zsub);
+  if (t->d_io) cudaFree(t->d_io);
+  if (t->io_stream) cudaStreamDestroy(t->io_stream);
   if (prev >= 0) cudaSetDevice(prev);
   delete t;
 }
@@ -214,60 +217,85 @@ int autotune(stb_table *t, const double *const in[6], long n, int nturn, double 
   return STB_OK;
 }
 
-// Host AoS -> device SoA, track, back; Track()'s stable/lost_turn/lost_post outputs.
+// Device staging of the host-buffer entry points, kept with the table and
+// grown on demand: AoS and SoA copies of up to nine coordinates per particle
+// plus five int32 arrays (input flag / stable, internal loss turn and
+// element, Track()'s lost_turn and lost_post).
+struct IoBufs {
+  double *aos, *soa;
+  int32_t *st, *lt, *le, *lt_out, *lp_out;
+};
+constexpr size_t kIoBytesPerParticle = 18 * sizeof(double) + 5 * sizeof(int32_t);
+
+IoBufs io_buffers(stb_table *t, long n) {
+  if (!t->io_stream) cuda_check(cudaStreamCreateWithFlags(&t->io_stream, cudaStreamNonBlocking), "create stream");
+  if ((size_t)n > t->io_cap) {
+    if (t->d_io) {
+      cuda_check(cudaStreamSynchronize(t->io_stream), "staging stream");
+      cudaFree(t->d_io);
+      t->d_io = nullptr;
+      t->io_cap = 0;
+    }
+    cuda_check(cudaMalloc(&t->d_io, (size_t)n * kIoBytesPerParticle), "cudaMalloc(host-buffer staging)");
+    t->io_cap = (size_t)n;
+  }
+  const size_t cap = t->io_cap;
+  IoBufs b;
+  b.aos = static_cast<double *>(t->d_io);
+  b.soa = b.aos + 9 * cap;
+  int32_t *ip = reinterpret_cast<int32_t *>(b.soa + 9 * cap);
+  b.st = ip;
+  b.lt = ip + cap;
+  b.le = ip + 2 * cap;
+  b.lt_out = ip + 3 * cap;
+  b.lp_out = ip + 4 * cap;
+  return b;
+}
+
+// Host AoS -> device SoA, track, back; Track()'s stable/lost_turn/lost_post
+// outputs.  The caller's arrays are copied as they are (pinned memory gives
+// full-speed DMA); the transposes, Track()'s entry check and the output
+// flags are computed on the device; everything runs on the table's own
+// stream, which the call waits for before returning.
 int track_host(stb_table *t, double *xa, long n, int nturn, double radius, int *stable, int *lost_turn,
                int *lost_post, double *dump_host = nullptr) {
   if (!t) throw Error(STB_EINVAL, "table is NULL");
+  if (t->host.spin) throw Error(STB_EINVAL, "table is flattened for spin tracking (use stb_track_spin_*)");
   if (n < 0 || nturn < 0) throw Error(STB_EINVAL, "negative particle count or turn count");
   if (n == 0) return STB_OK;
   if (!xa || !stable || !lost_turn || !lost_post) throw Error(STB_EINVAL, "NULL host buffer");
   DeviceGuard g(t->device);
-  std::vector<double> soa((size_t)n * 6);
-  std::vector<int32_t> lt((size_t)n), le((size_t)n, 0);
-  for (long i = 0; i < n; i++) {
-    for (int k = 0; k < 6; k++) soa[(size_t)k * n + i] = xa[6 * i + k];
-    lt[i] = stable[i] == 0 ? 0 : -1;  // Track(): stable == 0 on entry -> lost at turn 0, post 0
-  }
-  double *d = nullptr;
-  int32_t *dl = nullptr;
-  cuda_check(cudaMalloc(&d, sizeof(double) * 6 * n), "cudaMalloc(coordinates)");
-  struct Free {
-    void *p;
-    ~Free() { if (p) cudaFree(p); }
-  } f1{d};
-  cuda_check(cudaMalloc(&dl, sizeof(int32_t) * 2 * n), "cudaMalloc(loss arrays)");
-  Free f2{dl};
-  cuda_check(cudaMemcpy(d, soa.data(), sizeof(double) * 6 * n, cudaMemcpyHostToDevice), "upload coordinates");
-  cuda_check(cudaMemcpy(dl, lt.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice), "upload loss state");
-  cuda_check(cudaMemcpy(dl + n, le.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice), "upload loss state");
-  cuda_check(cudaMemset(t->d_status, 0, sizeof(int)), "clear status");
+  const IoBufs b = io_buffers(t, n);
+  cudaStream_t s = t->io_stream;
+  cuda_check(cudaMemcpyAsync(b.aos, xa, sizeof(double) * 6 * n, cudaMemcpyHostToDevice, s), "upload coordinates");
+  cuda_check(cudaMemcpyAsync(b.st, stable, sizeof(int32_t) * n, cudaMemcpyHostToDevice, s), "upload input flags");
+  cuda_check(launch_aos_to_soa(b.aos, b.st, n, 6, b.soa, b.lt, b.le, s), "AoS to SoA");
+  cuda_check(cudaMemsetAsync(t->d_status, 0, sizeof(int), s), "clear status");
   double *dd = nullptr;
   const size_t dump_n = dump_host ? (size_t)n * nturn * t->host.hdr.size() * 6 : 0;
   if (dump_host) {
     cuda_check(cudaMalloc(&dd, sizeof(double) * dump_n), "cudaMalloc(probe)");
     // Entries after a loss keep their previous content, as in the oracle probe.
-    cuda_check(cudaMemcpy(dd, dump_host, sizeof(double) * dump_n, cudaMemcpyHostToDevice), "upload probe");
+    cuda_check(cudaMemcpyAsync(dd, dump_host, sizeof(double) * dump_n, cudaMemcpyHostToDevice, s), "upload probe");
   }
-  Free f3{dd};
+  DevFree f3{dd};
+  double *c = b.soa;
   if (nturn > 0)
-    track_device(t, d, d + n, d + 2 * n, d + 3 * n, d + 4 * n, d + 5 * n, n, 0, nturn, radius, dl, dl + n, 0, dd);
-  cuda_check(cudaDeviceSynchronize(), "track kernel");
-  if (dump_host)
-    cuda_check(cudaMemcpy(dump_host, dd, sizeof(double) * dump_n, cudaMemcpyDeviceToHost), "download probe");
+    track_device(t, c, c + n, c + 2 * n, c + 3 * n, c + 4 * n, c + 5 * n, n, 0, nturn, radius, b.lt, b.le, s, dd);
+  cuda_check(launch_soa_to_aos(c, b.lt, b.le, n, 6, b.aos, b.st, b.lt_out, b.lp_out, s), "SoA to AoS");
   int st = 0;
-  cuda_check(cudaMemcpy(&st, t->d_status, sizeof(int), cudaMemcpyDeviceToHost), "read status");
+  cuda_check(cudaMemcpyAsync(&st, t->d_status, sizeof(int), cudaMemcpyDeviceToHost, s), "read status");
+  cuda_check(cudaStreamSynchronize(s), "track kernel");
   if (st != 0) throw Error(st, "tracking kernel reported status " + std::to_string(st));
-  cuda_check(cudaMemcpy(soa.data(), d, sizeof(double) * 6 * n, cudaMemcpyDeviceToHost), "download coordinates");
-  cuda_check(cudaMemcpy(lt.data(), dl, sizeof(int32_t) * n, cudaMemcpyDeviceToHost), "download loss state");
-  cuda_check(cudaMemcpy(le.data(), dl + n, sizeof(int32_t) * n, cudaMemcpyDeviceToHost), "download loss state");
-  for (long i = 0; i < n; i++) {
-    for (int k = 0; k < 6; k++) xa[6 * i + k] = soa[(size_t)k * n + i];
-    if (lt[i] < 0) {
-      stable[i] = 1; lost_turn[i] = 0; lost_post[i] = 0;
-    } else {
-      stable[i] = 0; lost_turn[i] = lt[i]; lost_post[i] = le[i];
-    }
-  }
+  if (dump_host)
+    cuda_check(cudaMemcpyAsync(dump_host, dd, sizeof(double) * dump_n, cudaMemcpyDeviceToHost, s), "download probe");
+  cuda_check(cudaMemcpyAsync(xa, b.aos, sizeof(double) * 6 * n, cudaMemcpyDeviceToHost, s), "download coordinates");
+  cuda_check(cudaMemcpyAsync(stable, b.st, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, s), "download outputs");
+  cuda_check(cudaMemcpyAsync(lost_turn, b.lt_out, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, s),
+             "download outputs");
+  cuda_check(cudaMemcpyAsync(lost_post, b.lp_out, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, s),
+             "download outputs");
+  cuda_check(cudaStreamSynchronize(s), "download");
   return STB_OK;
 }
 
@@ -318,7 +346,7 @@ int radial_host(stb_table *t, double *xa, long n, int nturn, double radius, int 
   std::vector<int32_t> lt((size_t)n), le((size_t)n, 0);
   for (long i = 0; i < n; i++) {
     for (int k = 0; k < 6; k++) soa[(size_t)k * n + i] = xa[6 * i + k];
-    lt[i] = stable[i] == 0 ? 0 : -1;
+    lt[i] = entry_rejected(xa + 6 * i, stable[i]) ? 0 : -1;  // Track_Radial's entry check, 21647-21649
   }
   double *d = nullptr;
   int32_t *dl = nullptr;
@@ -398,7 +426,7 @@ int spin_host(stb_table *t, double *xa, long n, int nturn, double radius, int *s
   std::vector<int32_t> lt((size_t)n), le((size_t)n, 0);
   for (long i = 0; i < n; i++) {
     for (int k = 0; k < 9; k++) soa[(size_t)k * n + i] = xa[9 * i + k];
-    lt[i] = stable[i] == 0 ? 0 : -1;  // Track_Spin(): stable == 0 on entry -> lost at turn 0, post 0
+    lt[i] = entry_rejected(xa + 9 * i, stable[i]) ? 0 : -1;  // Track_Spin's entry check, 21769-21771
   }
   double *d = nullptr;
   int32_t *dl = nullptr;
@@ -521,9 +549,14 @@ using namespace stb;
 
 namespace stb {
 namespace {
-// Runs f with FineTuneFinder's window set to [lo, hi), restoring it afterwards.
+// Runs f with FineTuneFinder's window set to [lo, hi), restoring it
+// afterwards.  The window is the process-wide tune_low / tune_high pair (a
+// global in the reference too, simtrack.cpp:27), so C-ABI calls that set it
+// are serialised: two host threads never see each other's window.
+std::mutex g_tune_window_mu;
 template <class F>
 void with_tune_window(double lo, double hi, F f) {
+  std::lock_guard<std::mutex> lk(g_tune_window_mu);
   const double lo0 = tune_low, hi0 = tune_high;
   tune_low = lo;
   tune_high = hi;

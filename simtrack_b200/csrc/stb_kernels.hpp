@@ -71,4 +71,16 @@ size_t track_smem_bytes(int nelem, int npool_padded);
 int track_smem_limit(int device);
 cudaError_t launch_track(const TrackArgs &a, int num_sms, int variant, cudaStream_t stream);
 
+// Host-buffer staging of Track()'s AoS interface (stb_track.cu).  aos[n*nc]
+// (nc = 6, or 9 with the spin vector) -> SoA soa[k*n + i]; lost_turn = 0 for
+// particles Track()'s entry check rejects (input flag 0, |x| or |y| > 0.1),
+// else -1; lost_elem = 0.
+cudaError_t launch_aos_to_soa(const double *aos, const int32_t *stable, long n, int nc, double *soa,
+                              int32_t *lost_turn, int32_t *lost_elem, cudaStream_t s);
+// SoA -> AoS and Track()'s outputs: stable = lost_turn < 0; lost_turn_out /
+// lost_post = the loss turn and element of lost particles, 0 for survivors.
+cudaError_t launch_soa_to_aos(const double *soa, const int32_t *lost_turn, const int32_t *lost_elem, long n, int nc,
+                              double *aos, int32_t *stable, int32_t *lost_turn_out, int32_t *lost_post,
+                              cudaStream_t s);
+
 }  // namespace stb

@@ -3,6 +3,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <string>
 
 #include "simtrack_b200.hpp"
@@ -21,6 +22,12 @@ struct stb_table {
   int *d_status = nullptr;
   int num_sms = 0;
   double *d_zsub = nullptr;  // Track_Radial's per-element on-momentum z (computed on first use)
+  // Host-buffer entry points (stb_track_host): device staging grown on
+  // demand and kept with the table, and the stream their copies and kernels
+  // run on (created on first use).
+  void *d_io = nullptr;
+  size_t io_cap = 0;  // particles d_io holds
+  cudaStream_t io_stream = nullptr;
 };
 
 namespace stb {
@@ -60,6 +67,13 @@ void track_device_dump(stb_table *t, double *const c[6], long n, int turn0, int 
 // The same for spin tracking (a spin table, nine arrays, dump[...*9 + k]).
 void spin_device_dump(stb_table *t, double *const c[9], long n, int turn0, int nturn, int32_t *lost_turn,
                       int32_t *lost_elem, double *dump);
+
+// Track()'s entry quick check (simtrack.cpp:20795-20796; the same in
+// Track_Radial and Track_Spin): a particle whose input flag is 0 or whose
+// |x| or |y| exceeds 0.1 m is lost at turn 0, element 0, whatever nturn is.
+inline bool entry_rejected(const double *x, int stable) {
+  return stable == 0 || std::fabs(x[0]) > 0.1 || std::fabs(x[2]) > 0.1;
+}
 
 // Restores the caller's current device on scope exit.
 struct DeviceGuard {

@@ -67,7 +67,8 @@ struct DeviceBatch {
     std::vector<int32_t> l((size_t)n * 2, 0);
     for (long i = 0; i < n; i++) {
       for (int k = 0; k < nc; k++) soa[(size_t)k * n + i] = xa[(size_t)nc * i + k];
-      l[i] = stable[i] == 0 ? 0 : -1;  // stable == 0 on entry: lost at turn 0, post 0
+      // Track()'s entry check: stable == 0, |x| > 0.1 or |y| > 0.1 -> lost at turn 0, post 0
+      l[i] = entry_rejected(xa + (size_t)nc * i, stable[i]) ? 0 : -1;
     }
     cuda_check(cudaMemcpy(coords.p, soa.data(), sizeof(double) * soa.size(), cudaMemcpyHostToDevice),
                "upload coordinates");

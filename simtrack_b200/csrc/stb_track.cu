@@ -87,4 +87,53 @@ cudaError_t launch_track(const TrackArgs &a, int num_sms, int variant, cudaStrea
   }
 }
 
+namespace {
+
+__global__ void aos_to_soa_kernel(const double *__restrict__ aos, const int32_t *__restrict__ stable, long n,
+                                  int nc, double *__restrict__ soa, int32_t *__restrict__ lost_turn,
+                                  int32_t *__restrict__ lost_elem) {
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    const double *q = aos + (size_t)nc * i;
+    for (int k = 0; k < nc; k++) soa[(size_t)k * n + i] = q[k];
+    // Track()'s entry quick check, simtrack.cpp:20795-20796
+    lost_turn[i] = (stable[i] == 0 || fabs(q[0]) > 0.1 || fabs(q[2]) > 0.1) ? 0 : -1;
+    lost_elem[i] = 0;
+  }
+}
+
+__global__ void soa_to_aos_kernel(const double *__restrict__ soa, const int32_t *__restrict__ lost_turn,
+                                  const int32_t *__restrict__ lost_elem, long n, int nc, double *__restrict__ aos,
+                                  int32_t *__restrict__ stable, int32_t *__restrict__ lost_turn_out,
+                                  int32_t *__restrict__ lost_post) {
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    double *q = aos + (size_t)nc * i;
+    for (int k = 0; k < nc; k++) q[k] = soa[(size_t)k * n + i];
+    const int32_t t = lost_turn[i];
+    stable[i] = t < 0 ? 1 : 0;
+    lost_turn_out[i] = t < 0 ? 0 : t;
+    lost_post[i] = t < 0 ? 0 : lost_elem[i];
+  }
+}
+
+unsigned io_grid(long n) {
+  long g = (n + 255) / 256;
+  return (unsigned)(g < 1 ? 1 : (g > 148 * 16 ? 148 * 16 : g));
+}
+
+}  // namespace
+
+cudaError_t launch_aos_to_soa(const double *aos, const int32_t *stable, long n, int nc, double *soa,
+                              int32_t *lost_turn, int32_t *lost_elem, cudaStream_t s) {
+  aos_to_soa_kernel<<<io_grid(n), 256, 0, s>>>(aos, stable, n, nc, soa, lost_turn, lost_elem);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_soa_to_aos(const double *soa, const int32_t *lost_turn, const int32_t *lost_elem, long n, int nc,
+                              double *aos, int32_t *stable, int32_t *lost_turn_out, int32_t *lost_post,
+                              cudaStream_t s) {
+  soa_to_aos_kernel<<<io_grid(n), 256, 0, s>>>(soa, lost_turn, lost_elem, n, nc, aos, stable, lost_turn_out,
+                                               lost_post);
+  return cudaGetLastError();
+}
+
 }  // namespace stb

@@ -389,3 +389,26 @@ class PortOracle:
         wx, wy = c_double(), c_double()
         self.L.port_cerrf(x, y, ctypes.byref(wx), ctypes.byref(wy))
         return wx.value, wy.value
+
+
+def _ref_track_worker(args):
+    lat, x, nturn, cr, spin = args
+    o = RefOracle(cr=cr)
+    o.build(lat)
+    return o.track_spin(x, nturn) if spin else o.track(x, nturn)
+
+
+def ref_track_parallel(lat: Lattice, x: np.ndarray, nturn: int, cr: bool = False, spin: bool = False,
+                       procs: int = 0):
+    """The compiled reference's Track() (Track_Spin for spin=True) over the
+    rows of x split into contiguous ranges, one spawned process per range
+    (processes, because the reference keeps the turn counter in a global).
+    Returns (x_out, stable, lost_turn, lost_post) in the input order."""
+    import multiprocessing as mp
+    import os
+    procs = procs or os.cpu_count() or 1
+    procs = max(1, min(procs, len(x)))
+    chunks = np.array_split(np.ascontiguousarray(x, dtype=np.float64), procs)
+    with mp.get_context("spawn").Pool(procs) as pool:
+        res = pool.map(_ref_track_worker, [(lat, c, nturn, cr, spin) for c in chunks])
+    return tuple(np.concatenate([r[k] for r in res]) for k in range(4))

@@ -2,16 +2,26 @@
 
 The reference calls the host C library's asin/exp/sin/cos/pow.  The kernels
 use correctly rounded double-double evaluations instead; these tests check
-(CPU) that they sit within 1 ulp of the C library and agree with it on all
-but a small fraction of arguments (the C library itself misrounds those,
-e.g. exp(-38.706775399911955) is off by 0.50015 ulp in glibc), and (GPU) that
-the device build returns the host build's values bit for bit.
+(CPU) that they are exactly the correctly rounded values, against mpmath at 60
+significant digits, on the sampled argument ranges of the maps and on
+near-midpoint arguments found by an extended-precision search; that they sit
+within 1 ulp of the C library and agree with it on all but a small fraction
+of arguments (the C library itself misrounds those, e.g.
+exp(-38.706775399911955) is off by 0.50015 ulp in glibc); that the oracle's
+independent correctly rounded shim (oracle/crlibm_shim.cpp: x87 extended and
+binary128 evaluations, no code shared with the tracker) passes the same
+mpmath check; and (GPU) that the device build returns the host build's values
+bit for bit.
 """
+import ctypes
 import math
 from ctypes import POINTER, c_double
 
+import mpmath
 import numpy as np
 import pytest
+
+import oracle_bridge
 
 
 def ev(native_lib, fn, x, device):
@@ -34,6 +44,47 @@ def samples(kind, n, seed=0):
 
 
 CASES = [("asin", 0, math.asin), ("exp", 1, math.exp), ("sin", 2, math.sin), ("cos", 3, math.cos)]
+MP_FN = {0: mpmath.asin, 1: mpmath.exp, 2: mpmath.sin, 3: mpmath.cos}
+NP_FN = {0: np.arcsin, 1: np.exp, 2: np.sin, 3: np.cos}
+
+
+def mp_rounded(fn, x, m=None, digits=60):
+    """The correctly rounded (nearest, ties to even) double of f(x), or of
+    x**m for fn 4, from a `digits`-digit mpmath evaluation."""
+    with mpmath.workdps(digits):
+        v = mpmath.mpf(float(x)) ** int(m) if fn == 4 else MP_FN[fn](mpmath.mpf(float(x)))
+    with mpmath.workprec(53):
+        return float(+v)
+
+
+def near_midpoint(fn, x, keep, m=None):
+    """The `keep` arguments of x whose value lies closest to a rounding
+    midpoint between two doubles, by an x87 extended-precision evaluation
+    (hard cases for a correctly rounded implementation)."""
+    xl = x.astype(np.longdouble)
+    v = xl ** m.astype(np.longdouble) if fn == 4 else NP_FN[fn](xl)
+    d = v.astype(np.float64)
+    u = np.spacing(np.abs(d)).astype(np.longdouble)
+    frac = (v - d.astype(np.longdouble)) / u
+    dist = np.abs(np.abs(frac) - 0.5)
+    idx = np.argsort(dist.astype(np.float64))[:keep]
+    return idx
+
+
+def hard_and_sampled(name, fn, seed):
+    x = samples(name, 2000, seed=seed)
+    pool = samples(name, 400000, seed=seed + 100)
+    return np.concatenate([x, pool[near_midpoint(fn, pool, 64)]])
+
+
+def pown_cases(seed):
+    rng = np.random.default_rng(seed)
+    h = np.concatenate([rng.random(1500) * 3 + 0.05, 1.0 / (3.2 * rng.random(1500) + 1e-3)])
+    m = -rng.integers(6, 30, h.size).astype(np.float64)
+    ph = rng.random(400000) * 3 + 0.05
+    pm = -rng.integers(6, 30, ph.size).astype(np.float64)
+    k = near_midpoint(4, ph, 64, pm)
+    return np.concatenate([h, ph[k]]), np.concatenate([m, pm[k]])
 
 
 @pytest.mark.parametrize("name,fn,ref", CASES)
@@ -61,6 +112,49 @@ def test_integer_power(native_lib):
     y = ev(native_lib, 4, np.stack([h, m], 1).ravel(), -1)
     r = np.array([math.pow(a, b) for a, b in zip(h, m)])
     assert np.max(np.abs(y - r) / np.abs(r)) <= 2.3e-16
+
+
+@pytest.mark.parametrize("name,fn,ref", CASES)
+def test_correctly_rounded_vs_mpmath(native_lib, name, fn, ref):
+    """The tracker's functions (host build of the device code) are the
+    correctly rounded values."""
+    x = hard_and_sampled(name, fn, seed=21)
+    y = ev(native_lib, fn, x, -1)
+    r = np.array([mp_rounded(fn, v) for v in x])
+    bad = np.flatnonzero(y != r)
+    assert bad.size == 0, f"{name}: {bad.size} misrounded, e.g. x={x[bad[0]]!r}"
+
+
+def test_pown_correctly_rounded_vs_mpmath(native_lib):
+    h, m = pown_cases(22)
+    y = ev(native_lib, 4, np.stack([h, m], 1).ravel(), -1)
+    r = np.array([mp_rounded(4, a, b) for a, b in zip(h, m)])
+    assert np.array_equal(y, r)
+
+
+def _crshim():
+    if not oracle_bridge.ref_available(cr=True):
+        pytest.skip("compiled reference oracle with correctly rounded libm (oracle/_ref) not built here")
+    lib = ctypes.CDLL(str(oracle_bridge.REF_CR_SO))
+    lib.stb_crshim_eval.restype = ctypes.c_double
+    lib.stb_crshim_eval.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double]
+    lib.stb_crshim_unresolved.restype = ctypes.c_long
+    return lib
+
+
+@pytest.mark.parametrize("name,fn,ref", CASES)
+def test_oracle_shim_correctly_rounded_vs_mpmath(name, fn, ref):
+    """The correctly rounded oracle's own functions, which share no code with
+    the tracker, are the correctly rounded values too."""
+    lib = _crshim()
+    x = hard_and_sampled(name, fn, seed=31)
+    y = np.array([lib.stb_crshim_eval(fn, float(v), 0.0) for v in x])
+    r = np.array([mp_rounded(fn, v) for v in x])
+    assert np.array_equal(y, r)
+    h, m = pown_cases(32)
+    y = np.array([lib.stb_crshim_eval(4, float(a), float(b)) for a, b in zip(h, m)])
+    assert np.array_equal(y, np.array([mp_rounded(4, a, b) for a, b in zip(h, m)]))
+    assert lib.stb_crshim_unresolved() == 0
 
 
 @pytest.mark.gpu

@@ -3,11 +3,13 @@ stb_track_device on each seed table, over two calls in a row (needs a B200).
 
 Collected last on purpose: it must pass both in a fresh process and after
 every other test has used the device."""
+import ctypes
+
 import numpy as np
 import pytest
 
 from simtrack_b200 import lattices as lt
-from simtrack_b200._native import SimTrackError
+from simtrack_b200._native import STB_EINVAL, lib
 from simtrack_b200.api import Table, track_seeds_static
 
 pytestmark = pytest.mark.gpu
@@ -65,18 +67,33 @@ def test_static_matches_track_device_two_calls():
 
 
 def test_static_rejects_oversize_requests():
+    """Through the C ABI with NULL buffers: the size limits are checked before
+    anything touches the device."""
     tabs, xs = _setup()
-    with pytest.raises(SimTrackError, match="particles"):
-        track_seeds_static(tabs[:1], [1 << 21], _Null(), _Null(), _Null(), 0, 10)
-    with pytest.raises(SimTrackError, match="seed count"):
-        track_seeds_static(tabs[:1] * 65, [1] * 65, _Null(), _Null(), _Null(), 0, 10)
+
+    def call(tables, n_per):
+        arr = (ctypes.c_void_p * len(tables))(*[t._h for t in tables])
+        nps = (ctypes.c_long * len(n_per))(*n_per)
+        return lib().stb_track_seeds_static(arr, len(tables), nps, *([None] * 8), 0, 10, 0.0, None)
+
+    assert call(tabs[:1], [1 << 21]) == STB_EINVAL
+    assert b"particles" in lib().stb_last_error()
+    assert call(tabs[:1] * 65, [1] * 65) == STB_EINVAL
+    assert b"seed count" in lib().stb_last_error()
 
 
-class _Null:
-    """Stands in for a tensor that must never be touched (size checks come first)."""
-
-    def __getitem__(self, k):
-        return self
-
-    def data_ptr(self):
-        return 0
+def test_python_wrapper_checks_buffers():
+    tabs, xs = _setup()
+    dev = torch.device("cuda:0")
+    n = 10
+    c = torch.zeros((6, n), dtype=torch.float64, device=dev)
+    lt_ = torch.full((n,), -1, dtype=torch.int32, device=dev)
+    le_ = torch.zeros(n, dtype=torch.int32, device=dev)
+    with pytest.raises(ValueError):
+        track_seeds_static(tabs[:1], [n + 1], c, lt_, le_, 0, 1)
+    with pytest.raises(ValueError):
+        track_seeds_static(tabs[:1], [n], c.float(), lt_, le_, 0, 1)
+    with pytest.raises(ValueError):
+        track_seeds_static(tabs[:1], [n], c, lt_.long(), le_, 0, 1)
+    with pytest.raises(ValueError):
+        track_seeds_static(tabs[:1], [n], c.cpu(), lt_, le_, 0, 1)
