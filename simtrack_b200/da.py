@@ -96,18 +96,21 @@ def rhic_da_scan(nseed: int = 64, namp: int = 64, amax: float = 12.0, nang: int 
                     wall_s=wall, device_ms=st["device_ms"], stats=st)
 
 
-def sharded_da_scan(nseed: int = 64, **kw) -> Optional[DAResult]:
-    """rhic_da_scan over seeds seed0..seed0+nseed-1 split across the ranks of
+def sharded_da_scan(nseed: int = 64, scan=None, **kw) -> Optional[DAResult]:
+    """A DA scan over seeds seed0..seed0+nseed-1 split across the ranks of
     the default process group (contiguous seed shares, no exchange while
-    tracking); the per-seed loss turns are gathered to every rank and the
-    full result is returned (wall time: slowest rank)."""
+    tracking); the per-seed loss turns are gathered to every rank in seed
+    order and the full result is returned (wall time: slowest rank).
+    `scan(nseed=, seed0=, **kw) -> DAResult` runs one rank's share
+    (rhic_da_scan, the batched GPU scan, by default)."""
     from .parallel import gather_concat, reduce_scalar, shard_bounds
     import torch.distributed as dist
+    scan = scan or rhic_da_scan
     world = dist.get_world_size() if dist.is_available() and dist.is_initialized() else 1
     rank = dist.get_rank() if world > 1 else 0
     seed0 = kw.pop("seed0", 1)
     lo, hi = shard_bounds(nseed, rank, world)
-    part = rhic_da_scan(nseed=hi - lo, seed0=seed0 + lo, **kw) if hi > lo else None
+    part = scan(nseed=hi - lo, seed0=seed0 + lo, **kw) if hi > lo else None
     namp = kw.get("namp", 64)
     nang = kw.get("nang", 11)
     deltas = list(kw.get("deltas", (-1e-3, -5e-4, 0.0, 5e-4, 1e-3)))

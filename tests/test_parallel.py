@@ -70,3 +70,57 @@ def test_gloo_two_ranks_reduce_and_gather():
         assert ntot == 300.0
         assert g1 == [0, 10, 20, 30, 40]
         assert g2 == [[i, 2 * i] for i in range(5)]
+
+
+def fake_scan(nseed, seed0, namp=16, nang=3, deltas=(-1e-3, 0.0, 1e-3), amax=12.0, nturn=1000):
+    """Stands in for one rank's batched GPU scan: a deterministic loss pattern
+    per (seed, momentum offset, angle, amplitude)."""
+    from simtrack_b200.da import DAResult, da_from_lost
+    nd = len(deltas)
+    lt_ = np.full((nseed, nd, nang, namp), -1, dtype=np.int64)
+    for s in range(nseed):
+        sd = seed0 + s
+        for d in range(nd):
+            for a in range(nang):
+                edge = (3 * sd + 5 * d + 7 * a) % namp
+                lt_[s, d, a, edge:] = 10 * sd + np.arange(namp - edge)
+    amps = np.linspace(0.0, amax, namp)
+    return DAResult(nseed, namp, nang, list(deltas), amax, nturn, lt_, da_from_lost(lt_, amps, nturn), wall_s=1.0 + s)
+
+
+def _scan_worker(rank, world, port, nseed, q):
+    import datetime
+
+    import torch.distributed as dist
+
+    from simtrack_b200.da import sharded_da_scan
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        r = sharded_da_scan(nseed=nseed, scan=fake_scan, seed0=5, namp=16, nang=3, deltas=(-1e-3, 0.0, 1e-3),
+                            amax=12.0, nturn=1000)
+        q.put((rank, r.lost_turn.tolist(), r.da.tolist(), r.wall_s))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world,nseed", [(2, 7), (3, 7), (3, 2)])
+def test_sharded_scan_gathers_seeds_in_order(world, nseed):
+    """Seed sharding across gloo ranks, the gather order and the DA assembly
+    equal one process scanning every seed (a rank may get no seeds)."""
+    port = _free_port()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_scan_worker, args=(r, world, port, nseed, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    out = [q.get(timeout=120) for _ in range(world)]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    whole = fake_scan(nseed, 5)
+    for rank, lt_, da, wall in out:
+        assert np.array_equal(np.array(lt_), whole.lost_turn)
+        assert np.array_equal(np.array(da), whole.da)
+        assert wall >= 1.0
