@@ -313,6 +313,26 @@ int stb_scan_set_tbt(stb_scan *s, double *tbt, int nturns);
  * particles it has classified. */
 #define STB_RETIRED 0x40000000
 int stb_scan_retire(stb_scan *s, const uint8_t *mask);
+/* Stopping and resuming long scans (the reference's Track_DA* loops have
+ * neither; a 1e5-turn scan of many seeds runs for many minutes).
+ * stb_scan_set_abort(s, 1), callable from any host thread while another one
+ * is inside stb_scan_run, sets a flag in mapped host memory that every turn
+ * block reads on the device: the blocks still queued track nothing, and
+ * stb_scan_run returns STB_EABORTED at a turn-block boundary with the state
+ * intact.  While the flag is set every stb_scan_run returns STB_EABORTED at
+ * once; stb_scan_set_abort(s, 0) re-arms the scan. */
+int stb_scan_set_abort(stb_scan *s, int value);
+/* Wall-clock budget of each stb_scan_run call in seconds (0: none), checked
+ * between groups of turn blocks; when it is spent the call returns
+ * STB_ETIMEOUT at a turn-block boundary with the state intact. */
+int stb_scan_set_budget(stb_scan *s, double max_seconds);
+/* Writes the scan's state (particle slots, ids, loss state, live counts, turn
+ * counter, outputs) to `path` (through a temporary file renamed into place);
+ * stb_scan_restore loads it into a scan created with the same tables and
+ * particle counts (STB_EINVAL otherwise).  A restored scan continues exactly
+ * as the saved one would have: results equal those of an uninterrupted run. */
+int stb_scan_checkpoint(stb_scan *s, const char *path);
+int stb_scan_restore(stb_scan *s, const char *path);
 
 /* ---- turn-by-turn diagnostics ----
  * Track_tbt (simtrack.cpp:20841-20860) for n particles on the GPU: x AoS

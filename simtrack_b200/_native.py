@@ -121,6 +121,10 @@ SIGNATURES = [
     ("stb_tbt_features", c_int, [c_void_p, c_long, c_int, c_void_p, c_void_p, POINTER(c_double), c_void_p, c_int,
                                  c_void_p]),
     ("stb_scan_retire", c_int, [c_void_p, c_void_p]),
+    ("stb_scan_set_abort", c_int, [c_void_p, c_int]),
+    ("stb_scan_set_budget", c_int, [c_void_p, c_double]),
+    ("stb_scan_checkpoint", c_int, [c_void_p, c_char_p]),
+    ("stb_scan_restore", c_int, [c_void_p, c_char_p]),
     ("stb_track_seeds_static", c_int, [POINTER(c_void_p), c_int, POINTER(c_long)] + [c_void_p] * 8 +
      [c_int, c_int, c_double, c_void_p]),
     ("stb_mlp_create", c_int, [c_int, c_int, c_int, c_int, c_ulonglong, c_int, POINTER(c_void_p)]),

@@ -650,6 +650,22 @@ class Scan:
             raise SimTrackError(-1, "mask must have one entry per particle")
         check(lib().stb_scan_retire(self._h, c_void_p(m.ctypes.data)))
 
+    def set_abort(self, value: bool = True) -> None:
+        """Asks a run in progress (in another thread) to stop at the next turn
+        block (run raises SimTrackError with STB_EABORTED); False re-arms."""
+        check(lib().stb_scan_set_abort(self._h, int(bool(value))))
+
+    def set_budget(self, seconds: float) -> None:
+        """Wall-clock budget of each run call (0: none); a spent budget raises
+        SimTrackError with STB_ETIMEOUT at a turn-block boundary."""
+        check(lib().stb_scan_set_budget(self._h, float(seconds)))
+
+    def checkpoint(self, path) -> None:
+        check(lib().stb_scan_checkpoint(self._h, str(path).encode()))
+
+    def restore(self, path) -> None:
+        check(lib().stb_scan_restore(self._h, str(path).encode()))
+
     def stats(self) -> dict:
         st = (c_double * 6)()
         check(lib().stb_scan_stats(self._h, st))

@@ -41,7 +41,21 @@ constexpr int kCompactBlock = 1024;
 __global__ void scan_worklist_kernel(ScanArgs a) {
   __shared__ int pre[kMaxScanSeeds + 1];
   __shared__ int chunk_s;
+  __shared__ int abort_s;
   const int s = threadIdx.x;
+  // The caller's abort flag is read once per turn block: a set flag empties
+  // the work list, so the block tracks nothing and (through block_skipped)
+  // leaves the turn counter where it is; the state stays resumable.
+  if (s == 0) {
+    abort_s = (a.abort && *a.abort != 0) ? 1 : 0;
+    *a.block_skipped = abort_s;
+    if (abort_s) {
+      *a.n_items = 0;
+      *a.next_item = 0;
+    }
+  }
+  __syncthreads();
+  if (abort_s) return;
   const int lv = s < a.nseed ? a.live[s] : 0;
   // total live particles (block reduction through the prefix array)
   pre[s + 1] = lv;
@@ -247,7 +261,7 @@ __global__ void __launch_bounds__(kCompactBlock) scan_compact_kernel(ScanArgs a)
   }
   if (threadIdx.x == 0) {
     a.live[s] = base;
-    if (s == 0) *a.turn0 += a.nturn;
+    if (s == 0 && *a.block_skipped == 0) *a.turn0 += a.nturn;
   }
 }
 

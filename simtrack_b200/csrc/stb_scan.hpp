@@ -45,6 +45,11 @@ struct ScanArgs {
   double *tbt;
   int tbt_turns;
   long ntot;
+  // Abort flag in mapped host memory (nonzero: every following turn block
+  // of the run tracks nothing and leaves the turn counter alone), and the
+  // device flag recording that the current block was skipped.
+  const volatile int32_t *abort;
+  int32_t *block_skipped;
 };
 
 // Loss code written for particles removed by stb_scan_retire (never a turn).

@@ -7,6 +7,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
+#include <cstdio>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -44,10 +46,15 @@ struct stb_scan {
   int turns_done = 0;
   double device_ms = 0.0;
   long blocks_run = 0;
+  int32_t *h_abort = nullptr;  // mapped host flag read by every turn block (stb_scan_set_abort)
+  double budget_s = 0.0;       // wall-clock budget of one stb_scan_run call (0: none)
 };
 
 namespace stb {
 namespace {
+
+// Device counters: n_items, next_item, turn counter, item_chunk, block_skipped.
+constexpr int kScanCounters = 5;
 
 void scan_destroy(stb_scan *s) {
   if (!s) return;
@@ -56,6 +63,7 @@ void scan_destroy(stb_scan *s) {
   cudaSetDevice(s->device);
   if (s->graph) cudaGraphExecDestroy(s->graph);
   if (s->stream) cudaStreamDestroy(s->stream);
+  if (s->h_abort) cudaFreeHost(s->h_abort);
   for (void *p : {(void *)s->d_seeds, (void *)s->d_coords, (void *)s->d_i32, (void *)s->d_live, (void *)s->d_items,
                   (void *)s->d_ctr, (void *)s->d_out_x, (void *)s->d_status})
     if (p) cudaFree(p);
@@ -110,7 +118,11 @@ stb_scan *scan_build(stb_table **tables, int nseed, const double *x0, const long
   cuda_check(cudaMalloc(&s->d_i32, sizeof(int32_t) * 5 * n), "cudaMalloc(particle state)");
   cuda_check(cudaMalloc(&s->d_live, sizeof(int32_t) * nseed), "cudaMalloc(live)");
   cuda_check(cudaMalloc(&s->d_items, sizeof(int32_t) * 2 * std::max<long>(1, s->max_items)), "cudaMalloc(items)");
-  cuda_check(cudaMalloc(&s->d_ctr, sizeof(int32_t) * 4), "cudaMalloc(counters)");
+  cuda_check(cudaMalloc(&s->d_ctr, sizeof(int32_t) * kScanCounters), "cudaMalloc(counters)");
+  cuda_check(cudaHostAlloc(&s->h_abort, sizeof(int32_t), cudaHostAllocMapped), "cudaHostAlloc(abort flag)");
+  *(volatile int32_t *)s->h_abort = 0;
+  int32_t *d_abort = nullptr;
+  cuda_check(cudaHostGetDevicePointer((void **)&d_abort, s->h_abort, 0), "abort flag mapping");
   cuda_check(cudaMalloc(&s->d_out_x, sizeof(double) * 6 * n), "cudaMalloc(outputs)");
   cuda_check(cudaMalloc(&s->d_status, sizeof(int)), "cudaMalloc(status)");
   // initial state: AoS host -> SoA device; id = original index; all alive
@@ -131,7 +143,7 @@ stb_scan *scan_build(stb_table **tables, int nseed, const double *x0, const long
   cuda_check(cudaMemcpy(s->d_coords, soa.data(), sizeof(double) * 6 * n, cudaMemcpyHostToDevice), "upload");
   cuda_check(cudaMemcpy(s->d_i32, i32.data(), sizeof(int32_t) * 5 * n, cudaMemcpyHostToDevice), "upload");
   cuda_check(cudaMemcpy(s->d_live, live.data(), sizeof(int32_t) * nseed, cudaMemcpyHostToDevice), "upload");
-  cuda_check(cudaMemset(s->d_ctr, 0, sizeof(int32_t) * 4), "reset counters");
+  cuda_check(cudaMemset(s->d_ctr, 0, sizeof(int32_t) * kScanCounters), "reset counters");
   cuda_check(cudaMemset(s->d_status, 0, sizeof(int)), "reset status");
   cuda_check(cudaMemcpy(s->d_out_x, x0, sizeof(double) * 6 * n, cudaMemcpyHostToDevice), "upload");
   ScanArgs &a = s->args;
@@ -156,6 +168,8 @@ stb_scan *scan_build(stb_table **tables, int nseed, const double *x0, const long
   a.next_item = s->d_ctr + 1;
   a.turn0 = s->d_ctr + 2;
   a.item_chunk = s->d_ctr + 3;
+  a.block_skipped = s->d_ctr + 4;
+  a.abort = d_abort;
   a.r2 = radius > 0.0 ? radius * radius : INFINITY;
   a.status = s->d_status;
   a.tbt = nullptr;
@@ -217,13 +231,32 @@ void ensure_graph(stb_scan *s, int blocks, int tpb) {
   s->graph_chunk = s->chunk;
 }
 
-// Advances every live particle by nturn turns (fewer if all are lost).
+int32_t device_turn(stb_scan *s) {
+  int32_t t = 0;
+  cuda_check(cudaMemcpyAsync(&t, s->d_ctr + 2, sizeof(int32_t), cudaMemcpyDeviceToHost, s->stream), "read turn");
+  cuda_check(cudaStreamSynchronize(s->stream), "scan");
+  return t;
+}
+
+bool abort_requested(const stb_scan *s) { return *(const volatile int32_t *)s->h_abort != 0; }
+
+// Advances every live particle by nturn turns (fewer if all are lost).  Stops
+// early, with the state consistent at a turn-block boundary (resumable by
+// another stb_scan_run or from a checkpoint), when the caller's abort flag is
+// set (STB_EABORTED; blocks still queued track nothing) or when the run's
+// wall-clock budget is spent (STB_ETIMEOUT); both are checked between groups
+// of turn blocks, the abort flag also by every block on the device.
 void scan_run(stb_scan *s, int nturn, int tpb, int use_graph) {
   if (nturn < 0 || tpb <= 0) throw Error(STB_EINVAL, "bad turn counts");
   DeviceGuard g(s->device);
   cudaEvent_t e0, e1;
   cuda_check(cudaEventCreate(&e0), "event");
   cuda_check(cudaEventCreate(&e1), "event");
+  struct Events {
+    cudaEvent_t a, b;
+    ~Events() { cudaEventDestroy(a); cudaEventDestroy(b); }
+  } ev{e0, e1};
+  const auto t_start = std::chrono::steady_clock::now();
   const int nblocks = nturn / tpb, rem = nturn % tpb;
   const int per_graph = std::max(1, std::min(nblocks, 16));
   int done_blocks = 0;
@@ -237,6 +270,25 @@ void scan_run(stb_scan *s, int nturn, int tpb, int use_graph) {
     cuda_check(cudaEventElapsedTime(&ms, e0, e1), "event time");
     ms_total += ms;
   };
+  auto stop_check = [&]() {
+    s->turns_done = device_turn(s);
+    int code = 0;
+    const char *why = nullptr;
+    if (abort_requested(s)) {
+      code = STB_EABORTED;
+      why = "scan stopped by the caller's abort flag";
+    } else if (s->budget_s > 0.0 &&
+               std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count() > s->budget_s) {
+      code = STB_ETIMEOUT;
+      why = "scan stopped: its wall-clock budget is spent";
+    }
+    if (!code) return;
+    cuda_check(launch_scan_finalize(s->args, s->max_per_seed, s->stream), "finalize");
+    cuda_check(cudaStreamSynchronize(s->stream), "finalize");
+    s->device_ms += ms_total;
+    throw Error(code, std::string(why) + " at turn " + std::to_string(s->turns_done));
+  };
+  stop_check();
   while (done_blocks < nblocks) {
     const int todo = std::min(per_graph, nblocks - done_blocks);
     if (use_graph && todo == per_graph) {
@@ -247,21 +299,115 @@ void scan_run(stb_scan *s, int nturn, int tpb, int use_graph) {
     }
     done_blocks += todo;
     s->blocks_run += todo;
-    s->turns_done += todo * tpb;
     check_status(s);
+    stop_check();
     if (total_live(s) == 0) break;
   }
   if (rem > 0 && total_live(s) > 0) {
     timed([&] { run_blocks_direct(s, 1, rem); });
     s->blocks_run += 1;
-    s->turns_done += rem;
     check_status(s);
+    stop_check();
   }
+  s->turns_done = device_turn(s);
   cuda_check(launch_scan_finalize(s->args, s->max_per_seed, s->stream), "finalize");
   cuda_check(cudaStreamSynchronize(s->stream), "finalize");
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
   s->device_ms += ms_total;
+}
+
+// Checkpoint file: a header (magic, version, seed count, particle count,
+// particles per seed, turn counter, bookkeeping) and the device state (SoA
+// slots, ids and loss state, live counts, counters, outputs).
+constexpr char kCkptMagic[8] = {'S', 'T', 'B', 'S', 'C', 'A', 'N', '1'};
+
+void scan_checkpoint(stb_scan *s, const char *path) {
+  if (!path) throw Error(STB_EINVAL, "NULL path");
+  DeviceGuard g(s->device);
+  const long n = s->ntot;
+  std::vector<double> coords((size_t)6 * n), out_x((size_t)6 * n);
+  std::vector<int32_t> i32((size_t)5 * n), live(s->nseed), ctr(kScanCounters);
+  cuda_check(cudaStreamSynchronize(s->stream), "scan");
+  cuda_check(cudaMemcpy(coords.data(), s->d_coords, sizeof(double) * coords.size(), cudaMemcpyDeviceToHost), "save");
+  cuda_check(cudaMemcpy(out_x.data(), s->d_out_x, sizeof(double) * out_x.size(), cudaMemcpyDeviceToHost), "save");
+  cuda_check(cudaMemcpy(i32.data(), s->d_i32, sizeof(int32_t) * i32.size(), cudaMemcpyDeviceToHost), "save");
+  cuda_check(cudaMemcpy(live.data(), s->d_live, sizeof(int32_t) * live.size(), cudaMemcpyDeviceToHost), "save");
+  cuda_check(cudaMemcpy(ctr.data(), s->d_ctr, sizeof(int32_t) * ctr.size(), cudaMemcpyDeviceToHost), "save");
+  const std::string tmp = std::string(path) + ".tmp";
+  std::FILE *f = std::fopen(tmp.c_str(), "wb");
+  if (!f) throw Error(STB_EINVAL, std::string("cannot write ") + tmp);
+  bool ok = true;
+  auto put = [&](const void *p, size_t bytes) { ok = ok && std::fwrite(p, 1, bytes, f) == bytes; };
+  const int32_t version = 1, nseed = s->nseed;
+  const int64_t ntot = n, blocks = s->blocks_run;
+  put(kCkptMagic, sizeof(kCkptMagic));
+  put(&version, sizeof(version));
+  put(&nseed, sizeof(nseed));
+  put(&ntot, sizeof(ntot));
+  for (long v : s->n_per_seed) {
+    const int64_t w = v;
+    put(&w, sizeof(w));
+  }
+  put(&blocks, sizeof(blocks));
+  put(&s->device_ms, sizeof(s->device_ms));
+  put(ctr.data(), sizeof(int32_t) * ctr.size());
+  put(live.data(), sizeof(int32_t) * live.size());
+  put(coords.data(), sizeof(double) * coords.size());
+  put(i32.data(), sizeof(int32_t) * i32.size());
+  put(out_x.data(), sizeof(double) * out_x.size());
+  ok = (std::fclose(f) == 0) && ok;
+  if (!ok || std::rename(tmp.c_str(), path) != 0) {
+    std::remove(tmp.c_str());
+    throw Error(STB_EINVAL, std::string("cannot write checkpoint ") + path);
+  }
+}
+
+void scan_restore(stb_scan *s, const char *path) {
+  if (!path) throw Error(STB_EINVAL, "NULL path");
+  std::FILE *f = std::fopen(path, "rb");
+  if (!f) throw Error(STB_EINVAL, std::string("cannot read ") + path);
+  struct Close {
+    std::FILE *f;
+    ~Close() { std::fclose(f); }
+  } c{f};
+  bool ok = true;
+  auto get = [&](void *p, size_t bytes) { ok = ok && std::fread(p, 1, bytes, f) == bytes; };
+  char magic[8];
+  int32_t version = 0, nseed = 0;
+  int64_t ntot = 0, blocks = 0;
+  double dev_ms = 0.0;
+  get(magic, sizeof(magic));
+  get(&version, sizeof(version));
+  get(&nseed, sizeof(nseed));
+  get(&ntot, sizeof(ntot));
+  if (!ok || std::memcmp(magic, kCkptMagic, sizeof(magic)) != 0 || version != 1)
+    throw Error(STB_EINVAL, std::string("not a scan checkpoint: ") + path);
+  if (nseed != s->nseed || ntot != s->ntot) throw Error(STB_EINVAL, "checkpoint was written by a different scan");
+  for (int i = 0; i < nseed; i++) {
+    int64_t w = 0;
+    get(&w, sizeof(w));
+    if (!ok || w != s->n_per_seed[i]) throw Error(STB_EINVAL, "checkpoint was written by a different scan");
+  }
+  const long n = s->ntot;
+  std::vector<double> coords((size_t)6 * n), out_x((size_t)6 * n);
+  std::vector<int32_t> i32((size_t)5 * n), live(nseed), ctr(kScanCounters);
+  get(&blocks, sizeof(blocks));
+  get(&dev_ms, sizeof(dev_ms));
+  get(ctr.data(), sizeof(int32_t) * ctr.size());
+  get(live.data(), sizeof(int32_t) * live.size());
+  get(coords.data(), sizeof(double) * coords.size());
+  get(i32.data(), sizeof(int32_t) * i32.size());
+  get(out_x.data(), sizeof(double) * out_x.size());
+  if (!ok || std::fgetc(f) != EOF) throw Error(STB_EINVAL, std::string("truncated or oversized checkpoint ") + path);
+  DeviceGuard g(s->device);
+  cuda_check(cudaStreamSynchronize(s->stream), "scan");
+  cuda_check(cudaMemcpy(s->d_coords, coords.data(), sizeof(double) * coords.size(), cudaMemcpyHostToDevice), "load");
+  cuda_check(cudaMemcpy(s->d_out_x, out_x.data(), sizeof(double) * out_x.size(), cudaMemcpyHostToDevice), "load");
+  cuda_check(cudaMemcpy(s->d_i32, i32.data(), sizeof(int32_t) * i32.size(), cudaMemcpyHostToDevice), "load");
+  cuda_check(cudaMemcpy(s->d_live, live.data(), sizeof(int32_t) * live.size(), cudaMemcpyHostToDevice), "load");
+  cuda_check(cudaMemcpy(s->d_ctr, ctr.data(), sizeof(int32_t) * ctr.size(), cudaMemcpyHostToDevice), "load");
+  s->turns_done = ctr[2];
+  s->blocks_run = blocks;
+  s->device_ms = dev_ms;
 }
 
 // Times one turn block of `nturn` turns per launch variant on a snapshot of
@@ -270,7 +416,7 @@ int scan_autotune(stb_scan *s, int nturn, double *timings, int ntimings) {
   DeviceGuard g(s->device);
   const long n = s->ntot;
   const size_t bc = sizeof(double) * 6 * n, bi = sizeof(int32_t) * 5 * n, bl = sizeof(int32_t) * s->nseed,
-               bk = sizeof(int32_t) * 4;
+               bk = sizeof(int32_t) * kScanCounters;
   char *snap = nullptr;
   cuda_check(cudaMalloc(&snap, bc + bi + bl + bk), "cudaMalloc(autotune snapshot)");
   DevFree f{snap};
@@ -432,6 +578,38 @@ int stb_scan_retire(stb_scan *s, const uint8_t *mask) {
     cuda_check(stb::launch_scan_compact_only(a, s->stream), "compaction");
     cuda_check(launch_scan_finalize(s->args, s->max_per_seed, s->stream), "finalize");
     cuda_check(cudaStreamSynchronize(s->stream), "retire");
+    return STB_OK;
+  });
+}
+
+int stb_scan_set_abort(stb_scan *s, int value) {
+  return guarded([&] {
+    if (!s) throw Error(STB_EINVAL, "NULL scan");
+    *(volatile int32_t *)s->h_abort = value ? 1 : 0;
+    return STB_OK;
+  });
+}
+
+int stb_scan_set_budget(stb_scan *s, double max_seconds) {
+  return guarded([&] {
+    if (!s || !(max_seconds >= 0.0)) throw Error(STB_EINVAL, "bad arguments");
+    s->budget_s = max_seconds;
+    return STB_OK;
+  });
+}
+
+int stb_scan_checkpoint(stb_scan *s, const char *path) {
+  return guarded([&] {
+    if (!s) throw Error(STB_EINVAL, "NULL scan");
+    scan_checkpoint(s, path);
+    return STB_OK;
+  });
+}
+
+int stb_scan_restore(stb_scan *s, const char *path) {
+  return guarded([&] {
+    if (!s) throw Error(STB_EINVAL, "NULL scan");
+    scan_restore(s, path);
     return STB_OK;
   });
 }

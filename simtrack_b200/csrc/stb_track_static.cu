@@ -40,7 +40,8 @@ struct StaticScratch {
   int32_t live[kStaticMaxSeeds];
   int32_t ctr[4];  // n_items, next_item, turn0, item_chunk
   int32_t status;
-  int32_t pad[3];
+  int32_t block_skipped;  // written by the work-list kernel
+  int32_t pad[2];
   int32_t items[2 * kStaticMaxItems];
 };
 
@@ -156,6 +157,8 @@ int track_seeds_static(stb_table *const *tables, int nseed, const long *n_per_se
   a.r2 = radius > 0.0 ? radius * radius : INFINITY;
   a.status = &sc->status;
   a.ntot = total;
+  a.abort = nullptr;
+  a.block_skipped = &sc->block_skipped;
   static_init_kernel<<<1, kStaticMaxSeeds, 0, stream>>>(in, sc);
   cuda_check(cudaGetLastError(), "init launch");
   cuda_check(launch_scan_track_only(a, variant, grid, smem_ok ? smem : 0, stream), "tracking launch");

@@ -1,9 +1,12 @@
 """Batched DA scan (work list + tracking + compaction + CUDA graphs) against
-per-seed single-lattice tracking (needs a B200)."""
+per-seed single-lattice tracking, and its stop/resume controls: the abort
+flag set from another host thread, the wall-clock budget, checkpoint and
+restore (needs a B200)."""
 import numpy as np
 import pytest
 
 from simtrack_b200 import lattices as lt
+from simtrack_b200._native import STB_EABORTED, STB_ETIMEOUT, SimTrackError
 from simtrack_b200.api import Scan, Table
 
 pytestmark = pytest.mark.gpu
@@ -110,3 +113,86 @@ def test_scan_turn_by_turn_record_and_retire():
     keep = ~retired
     assert np.array_equal(lt_s[keep], lt_p[keep])
     assert np.array_equal(x_s[keep], x_p[keep])
+
+
+def _small_scan(tabs, xs):
+    sc = Scan(tabs, xs, aperture_radius=0.03)
+    sc.configure(variant=2, chunk=64)
+    return sc
+
+
+def test_checkpoint_resume_equals_uninterrupted(tmp_path):
+    tabs, xs, lats = seed_setup(2, namp=12, nang=3)
+    whole = _small_scan(tabs, xs)
+    whole.run(300, turns_per_block=64)
+    ref = whole.results()
+    first = _small_scan(tabs, xs)
+    first.run(128, turns_per_block=64)
+    path = tmp_path / "scan.ckpt"
+    first.checkpoint(path)
+    second = _small_scan(tabs, xs)
+    second.restore(path)
+    assert second.stats()["turns"] == 128
+    second.run(172, turns_per_block=64)
+    got = second.results()
+    for a, b in zip(ref, got):
+        assert np.array_equal(a, b)
+    assert second.stats()["turns"] == 300
+    # a checkpoint of another scan is refused
+    other = Scan(tabs[:1], xs[:1], aperture_radius=0.03)
+    with pytest.raises(SimTrackError, match="different scan"):
+        other.restore(path)
+
+
+def test_abort_flag_stops_at_a_block_boundary_and_resumes():
+    import threading
+    import time
+    tabs, xs, lats = seed_setup(2, namp=12, nang=3)
+    whole = _small_scan(tabs, xs)
+    whole.run(400, turns_per_block=8, use_graph=True)
+    ref = whole.results()
+    sc = _small_scan(tabs, xs)
+    sc.set_abort(True)
+    with pytest.raises(SimTrackError) as e:
+        sc.run(400, turns_per_block=8)
+    assert e.value.code == STB_EABORTED and sc.stats()["turns"] == 0
+    sc.set_abort(False)
+    err = []
+
+    def worker():
+        try:
+            sc.run(400, turns_per_block=8, use_graph=True)
+        except SimTrackError as ex:
+            err.append(ex)
+
+    th = threading.Thread(target=worker)
+    th.start()
+    time.sleep(0.3)
+    sc.set_abort(True)  # from another host thread, while the run is on the device
+    th.join(timeout=300)
+    assert not th.is_alive()
+    done = sc.stats()["turns"]
+    if err:  # the run was stopped part way (it may also have finished first)
+        assert err[0].code == STB_EABORTED
+        assert done % 8 == 0 and done < 400
+    sc.set_abort(False)
+    sc.run(400 - done, turns_per_block=8)
+    for a, b in zip(ref, sc.results()):
+        assert np.array_equal(a, b)
+
+
+def test_wall_clock_budget_stops_and_resumes():
+    tabs, xs, lats = seed_setup(2, namp=12, nang=3)
+    whole = _small_scan(tabs, xs)
+    whole.run(256, turns_per_block=16)
+    sc = _small_scan(tabs, xs)
+    sc.set_budget(1e-6)
+    with pytest.raises(SimTrackError) as e:
+        sc.run(256, turns_per_block=16)
+    assert e.value.code == STB_ETIMEOUT
+    done = sc.stats()["turns"]
+    assert done % 16 == 0 and done < 256
+    sc.set_budget(0)
+    sc.run(256 - done, turns_per_block=16)
+    for a, b in zip(whole.results(), sc.results()):
+        assert np.array_equal(a, b)
