@@ -23,6 +23,7 @@ HERE = Path(__file__).resolve().parent
 sys.path.insert(0, str(HERE.parent))
 sys.path.insert(0, str(HERE.parents[1]))
 
+import oracle_bridge  # noqa: E402
 from lattice_zoo import spin_particles, spin_zoo, zoo, zoo_particles  # noqa: E402
 from simtrack_b200.lattices import fodo_ring  # noqa: E402
 
@@ -69,7 +70,8 @@ TUNE_WINDOWS = [(0.2, 0.45, False), (0.0, 0.5, False), (0.0, 1.0, True)]
 
 # The reference's Example2 inputs: the HSR lattice as a Bmad table and the
 # closed orbit the reference printed for it (Print_Orbit after Cal_Optics).
-EXAMPLE2 = Path("/root/reference/Example2")
+_REF = oracle_bridge.ref_source_dir()
+EXAMPLE2 = _REF / "Example2" if _REF else Path("/nonexistent")
 HSR_ENERGY = (275000. / 938.27201, 938.27201, 1.0, 1.0)  # Set_RefPartEnergy, Example2/DA_cal.cpp:613
 
 

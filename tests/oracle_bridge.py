@@ -31,6 +31,16 @@ PORT_TYPES = ["DRIFT", "MARKER", "SBEND", "GSBEND", "QUAD", "SKEWQ", "SEXT", "OC
               "SOLEN", "PATCH"]
 
 
+def ref_source_dir() -> Path | None:
+    """The reference source tree the compiled reference was built from
+    (recorded by oracle/Makefile), when it is still present."""
+    f = ROOT / "oracle" / "_ref" / "ref_src.txt"
+    if not f.exists():
+        return None
+    d = Path(f.read_text().strip())
+    return d if (d / "simtrack.cpp").exists() else None
+
+
 def ref_available(cr: bool = False) -> bool:
     return (REF_CR_SO if cr else REF_SO).exists()
 

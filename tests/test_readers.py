@@ -14,10 +14,12 @@ from pathlib import Path
 import numpy as np
 import pytest
 
+import oracle_bridge
 from simtrack_b200 import api
 from simtrack_b200 import lattices as lt
 
-RHIC_TFS = Path("/root/reference/Example1/parameters_input")
+_REF = oracle_bridge.ref_source_dir()
+RHIC_TFS = _REF / "Example1" / "parameters_input" if _REF else Path("/nonexistent")
 
 PARAMS = {
     "SBEND": ("ANGLE", "E1", "E2", "Nint"),
