@@ -116,6 +116,15 @@ int stb_table_autotune(stb_table *t, const double *x, const double *px, const do
                        const double *z, const double *pt, long n, int nturn, double aperture_radius, int *chosen,
                        double *timings_ms, int ntimings);
 int stb_table_set_variant(stb_table *t, int variant);
+/* Contraction policy of the table's tracking kernel (no reference
+ * counterpart).  fast = 0 (default): the strict kernel, in which every FP64
+ * add and multiply rounds separately as in the reference's x86-64 build, so
+ * results equal the reference's.  fast != 0: the same kernel compiled with
+ * FMA contraction; each contracted multiply-add rounds once, so coordinates
+ * differ from the reference's in the last bits and chaotic trajectories
+ * separate over many turns.  Applies to stb_track_device / stb_track_host
+ * and the autotuner on this table. */
+int stb_table_set_contraction(stb_table *t, int fast);
 /* name (NUL-terminated, truncated to cap), CTA size and shared-memory flag of a launch variant */
 int stb_track_variant_info(int variant, char *name, int cap, int *block, int *smem);
 

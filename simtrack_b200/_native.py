@@ -122,6 +122,7 @@ SIGNATURES = [
                                  c_void_p]),
     ("stb_scan_retire", c_int, [c_void_p, c_void_p]),
     ("stb_scan_set_abort", c_int, [c_void_p, c_int]),
+    ("stb_table_set_contraction", c_int, [c_void_p, c_int]),
     ("stb_scan_set_budget", c_int, [c_void_p, c_double]),
     ("stb_scan_checkpoint", c_int, [c_void_p, c_char_p]),
     ("stb_scan_restore", c_int, [c_void_p, c_char_p]),

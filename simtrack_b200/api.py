@@ -287,6 +287,13 @@ class Table:
     def set_variant(self, v: int) -> None:
         check(lib().stb_table_set_variant(self._h, v))
 
+    def set_contraction(self, policy: str) -> None:
+        """"strict" (default: results equal the reference's) or "fast" (the
+        kernel compiled with FMA contraction)."""
+        if policy not in ("strict", "fast"):
+            raise ValueError("policy must be 'strict' or 'fast'")
+        check(lib().stb_table_set_contraction(self._h, int(policy == "fast")))
+
     def track_host(self, x: np.ndarray, nturn: int, aperture_radius: float = 0.0, stable=None):
         """Track() over AoS host coordinates x[n,6] (updated in place); returns (stable, lost_turn, lost_post)."""
         x = np.ascontiguousarray(x, dtype=np.float64)

@@ -4,7 +4,9 @@ All CUDA code targets sm_100a only.  Device code is compiled with
 -fmad=false: the tracking maps must round every FP64 add and multiply
 separately, exactly as the reference's x86-64 build does (no fused
 multiply-add), for the per-element parity the tests enforce.  Kernels that
-intentionally use fused multiply-adds call fma() explicitly.
+intentionally use fused multiply-adds call fma() explicitly.  The one
+exception is stb_track_fast.cu, the same tracking kernel built with
+-fmad=true (the "fast" contraction policy, selected per table).
 
 Usage: python -m simtrack_b200.build [--force]
 """
@@ -22,12 +24,15 @@ CSRC = PKG / "csrc"
 LIBDIR = PKG / "_lib"
 LIB = LIBDIR / "libsimtrack_b200.so"
 
-CUDA_SOURCES = ["stb_track.cu", "stb_scan.cu", "stb_track_static.cu", "stb_tune.cu", "stb_spin.cu", "stb_radial.cu", "stb_diag.cu", "stb_mlp.cu", "stb_mlp_ops.cu"]
+CUDA_SOURCES = ["stb_track.cu", "stb_track_fast.cu", "stb_scan.cu", "stb_track_static.cu", "stb_tune.cu", "stb_spin.cu", "stb_radial.cu", "stb_diag.cu", "stb_mlp.cu", "stb_mlp_ops.cu"]
 CXX_SOURCES = ["stb_elements.cpp", "stb_flatten.cpp", "stb_capi.cpp", "stb_scan_host.cpp", "stb_mlp_host.cpp",
                "stb_tune_host.cpp", "stb_readers.cpp", "stb_da.cpp",
                "stb_orbit.cpp", "stb_tbt.cpp"]
 HEADERS = ["stb_table.hpp", "stb_physics.cuh", "stb_crmath.cuh", "stb_kernels.hpp", "stb_status.hpp", "stb_flatten.hpp",
-           "stb_track_impl.cuh", "stb_scan.hpp", "stb_runtime.hpp", "stb_mlp.hpp", "stb_tune.hpp"]
+           "stb_track_impl.cuh", "stb_track_launch.cuh", "stb_scan.hpp", "stb_runtime.hpp", "stb_mlp.hpp", "stb_tune.hpp"]
+
+# Units compiled with FMA contraction: the fast tracking kernel only.
+FMA_SOURCES = {"stb_track_fast.cu"}
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off",
@@ -61,7 +66,8 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     jobs = []
     for s in srcs:
         o = objdir / (s.name + ".o")
-        cmd = [nvcc(), *ARCH, *COMMON, "-fmad=false", "-x", "cu" if s.suffix == ".cu" else "c++",
+        fmad = "-fmad=true" if s.name in FMA_SOURCES else "-fmad=false"
+        cmd = [nvcc(), *ARCH, *COMMON, fmad, "-x", "cu" if s.suffix == ".cu" else "c++",
                "-c", str(s), "-o", str(o)]
         if force or _stale(o, [s] + common_deps):
             jobs.append(cmd)

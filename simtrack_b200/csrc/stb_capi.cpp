@@ -147,7 +147,7 @@ int track_device(stb_table *t, double *x, double *px, double *y, double *py, dou
   a.lost_turn = lost_turn;
   a.lost_elem = lost_elem;
   a.dump = dump;
-  cuda_check(launch_track(a, t->num_sms, t->variant, s), "track kernel launch");
+  cuda_check((t->fast ? launch_track_fast : launch_track)(a, t->num_sms, t->variant, s), "track kernel launch");
   return STB_OK;
 }
 
@@ -193,7 +193,7 @@ int autotune(stb_table *t, const double *const in[6], long n, int nturn, double 
         a.x = buf; a.px = buf + m; a.y = buf + 2 * m; a.py = buf + 3 * m; a.z = buf + 4 * m; a.pt = buf + 5 * m;
         a.n = m; a.turn0 = 1; a.nturn = nturn; a.r2 = radius > 0 ? radius * radius : INFINITY;
         a.lost_turn = lost; a.lost_elem = lost + m; a.dump = nullptr;
-        if (launch_track(a, t->num_sms, v, 0) != cudaSuccess) {
+        if ((t->fast ? launch_track_fast : launch_track)(a, t->num_sms, v, 0) != cudaSuccess) {
           cudaGetLastError();
           ok = false;
           break;
@@ -968,6 +968,14 @@ int stb_table_set_variant(stb_table *t, int variant) {
     if (variant < 0 || variant >= kNumTrackVariants) throw Error(STB_EINVAL, "variant out of range");
     if (kVariants[variant].smem && !t->use_smem) throw Error(STB_EINVAL, "table does not fit shared memory");
     t->variant = variant;
+    return STB_OK;
+  });
+}
+
+int stb_table_set_contraction(stb_table *t, int fast) {
+  return guarded([&] {
+    if (!t) throw Error(STB_EINVAL, "table is NULL");
+    t->fast = fast != 0;
     return STB_OK;
   });
 }

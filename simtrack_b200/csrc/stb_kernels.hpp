@@ -70,6 +70,8 @@ cudaError_t fp64_peak_probe(int device, double *tflops);
 size_t track_smem_bytes(int nelem, int npool_padded);
 int track_smem_limit(int device);
 cudaError_t launch_track(const TrackArgs &a, int num_sms, int variant, cudaStream_t stream);
+// The same kernel compiled with FMA contraction allowed (stb_track_fast.cu).
+cudaError_t launch_track_fast(const TrackArgs &a, int num_sms, int variant, cudaStream_t stream);
 
 // Host-buffer staging of Track()'s AoS interface (stb_track.cu).  aos[n*nc]
 // (nc = 6, or 9 with the spin vector) -> SoA soa[k*n + i]; lost_turn = 0 for

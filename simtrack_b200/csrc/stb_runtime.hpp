@@ -19,6 +19,7 @@ struct stb_table {
   int npool_padded = 0;
   bool use_smem = false;  // the table fits the shared-memory variants
   int variant = 2;        // launch variant (stb::kVariants), set by the autotuner
+  bool fast = false;      // FMA-contracted kernel (stb_table_set_contraction) instead of the strict one
   int *d_status = nullptr;
   int num_sms = 0;
   double *d_zsub = nullptr;  // Track_Radial's per-element on-momentum z (computed on first use)

@@ -19,7 +19,7 @@
 
 #include <cstdint>
 
-#include "stb_track_impl.cuh"
+#include "stb_track_launch.cuh"
 
 namespace stb {
 
@@ -31,25 +31,6 @@ int track_smem_limit(int device) {
   int v = 0;
   if (cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, device) != cudaSuccess) return 0;
   return v - 1024;  // static shared memory and the mbarrier
-}
-
-// Persistent grid: as many CTAs as fit on the device at once (never more
-// than the particles need); each CTA strides over the particle range.
-template <bool kSmem, int kBlock, int kMinBlocks, int kPPT, bool kDump, bool kPF = false>
-static cudaError_t launch_variant(const TrackArgs &a, int num_sms, size_t smem, cudaStream_t stream) {
-  auto kern = track_kernel<kSmem, kBlock, kMinBlocks, kPPT, kDump, kPF>;
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
-  int per_sm = 0;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBlock, smem);
-  if (e != cudaSuccess) return e;
-  if (per_sm < 1) return cudaErrorInvalidConfiguration;
-  const long chunk = (long)kBlock * kPPT;
-  long need = (a.n + chunk - 1) / chunk;
-  long grid = (long)num_sms * per_sm;
-  if (grid > need) grid = need;
-  kern<<<(unsigned)grid, kBlock, smem, stream>>>(a);
-  return cudaGetLastError();
 }
 
 // Launch variants the autotuner chooses from: element table in shared
@@ -66,25 +47,7 @@ const TrackVariant kVariants[kNumTrackVariants] = {
 };
 
 cudaError_t launch_track(const TrackArgs &a, int num_sms, int variant, cudaStream_t stream) {
-  const size_t sm = track_smem_bytes(a.nelem, a.npool_padded);
-  if (a.dump) {
-    // Per-element probe (diagnostics and parity tests): small particle counts only.
-    return launch_variant<false, 256, 1, 1, true>(a, num_sms, 0, stream);
-  }
-  switch (variant) {
-    case 0: return launch_variant<true, 512, 1, 1, false>(a, num_sms, sm, stream);
-    case 1: return launch_variant<true, 1024, 1, 1, false>(a, num_sms, sm, stream);
-    case 2: return launch_variant<true, 768, 1, 1, false>(a, num_sms, sm, stream);
-    case 3: return launch_variant<false, 256, 2, 1, false>(a, num_sms, 0, stream);
-    case 4: return launch_variant<false, 256, 3, 1, false>(a, num_sms, 0, stream);
-    case 5: return launch_variant<false, 256, 4, 1, false>(a, num_sms, 0, stream);
-    case 6: return launch_variant<false, 384, 2, 1, false>(a, num_sms, 0, stream);
-    case 7: return launch_variant<true, 512, 1, 2, false>(a, num_sms, sm, stream);
-    case 8: return launch_variant<false, 128, 3, 2, false>(a, num_sms, 0, stream);
-    case 9: return launch_variant<true, 1024, 1, 1, false, true>(a, num_sms, sm, stream);
-    case 10: return launch_variant<true, 768, 1, 1, false, true>(a, num_sms, sm, stream);
-    default: return cudaErrorInvalidValue;
-  }
+  return launch_track_variants(a, num_sms, variant, stream);
 }
 
 namespace {

@@ -5,7 +5,10 @@ the GPU) of the EIC-like ring: `nseed` error seeds x `n` particles each, all
 seeds' launches issued on their own CUDA streams and timed together with CUDA
 events; prints one JSON line.  `python -m simtrack_b200.measure radial` does
 the same for Track_Radial on the RHIC-like ring.  `python -m
-simtrack_b200.measure elements` times the tracking kernel on single-type
+simtrack_b200.measure contraction --turns 1000` compares the FMA-contracted
+kernel with the strict one on the RHIC-like ring's DA grid (divergence, DA,
+loss turns, throughput).  `python -m simtrack_b200.measure elements` times
+the tracking kernel on single-type
 lattices (400 identical drifts, thick quadrupoles, sector bends, thin
 sextupoles; 40 thick multipoles of order 9; 100 beam-beam maps; 200 RF
 cavities) over 1,048,576 particles: the per-element-type cost behind the
@@ -130,15 +133,104 @@ def element_costs(n: int = 1 << 20, device: int = 0) -> dict:
     return out
 
 
+def contraction(nturn: int = 1000, every: int = 10, n_rate: int = 1 << 20, rate_turns: int = 4, device: int = 0,
+                seed: int = 1) -> dict:
+    """The fast contraction policy (FMA-contracted kernel) against the strict
+    kernel on the DA grid of the RHIC-like ring (64 amplitudes x 11 angles x 5
+    momentum offsets): per particle the first checked turn at which any
+    coordinate differs from the strict trajectory by more than 1e-12
+    relative (rms floor per coordinate), the DA per ray of both, and the loss
+    turns away from each ray's boundary; plus both kernels' particle-turns/s
+    on n_rate Gaussian particles.  Prints one JSON line."""
+    import torch
+    from .da import da_from_lost
+    dev = torch.device("cuda", device)
+    lat = lattices.rhic_like_ring(seed=seed)
+    namp, amax, nang, deltas = 64, 12.0, 11, [-1e-3, -5e-4, 0.0, 5e-4, 1e-3]
+    X = lattices.da_grid(lat, namp, amax, nang, deltas)
+    n = len(X)
+    tabs = {}
+    for pol in ("strict", "fast"):
+        t = Table(lattices.build_line(lat), device)
+        t.set_contraction(pol)
+        tabs[pol] = t
+    st = {p: [torch.tensor(np.ascontiguousarray(X[:, k]), device=dev) for k in range(6)] for p in tabs}
+    lost = {p: (torch.full((n,), -1, dtype=torch.int32, device=dev), torch.zeros(n, dtype=torch.int32, device=dev))
+            for p in tabs}
+    first_div = torch.full((n,), -1, dtype=torch.int64, device=dev)
+    r = lat.aperture_radius
+    for t0 in range(0, nturn, every):
+        k = min(every, nturn - t0)
+        for p, t in tabs.items():
+            t.track_device(st[p], lost[p][0], lost[p][1], t0, k, r)
+        a = torch.stack(st["strict"], 1)
+        b = torch.stack(st["fast"], 1)
+        both = (lost["strict"][0] < 0) & (lost["fast"][0] < 0)
+        floor = torch.sqrt(torch.mean(a[both] ** 2, 0)) if both.any() else torch.ones(6, device=dev)
+        rel = ((a - b).abs() / torch.maximum(a.abs(), floor)).amax(1)
+        diverged = (rel > 1e-12) | (lost["strict"][0] != lost["fast"][0])
+        first_div = torch.where((first_div < 0) & diverged, torch.full_like(first_div, t0 + k), first_div)
+    torch.cuda.synchronize(dev)
+    fd = first_div.cpu().numpy()
+    lts = lost["strict"][0].cpu().numpy().reshape(len(deltas) * nang, namp)
+    ltf = lost["fast"][0].cpu().numpy().reshape(len(deltas) * nang, namp)
+    amps = np.linspace(0.0, amax, namp)
+    da_s, da_f = da_from_lost(lts, amps, nturn), da_from_lost(ltf, amps, nturn)
+    step = amps[1] - amps[0]
+
+    def first_lost(lt_):
+        lostm = (lt_ >= 0) & (lt_ < nturn)
+        return np.where(lostm.any(1), np.argmax(lostm, 1), namp)
+
+    b = first_lost(lts)
+    far = np.abs(np.arange(namp)[None, :] - b[:, None]) > 1
+    surv = lts < 0
+    out = {"measure": "contraction policy divergence", "ring": "RHIC-like", "seed": seed, "particles": n,
+           "turns": nturn, "checked_every": every,
+           "diverged_particles": int((fd >= 0).sum()),
+           "surviving_particles_strict": int(surv.sum()),
+           "first_divergence_turn_percentiles": {q: (float(np.percentile(fd[fd >= 0], q)) if (fd >= 0).any() else None)
+                                                 for q in (5, 25, 50, 75, 95)},
+           "never_diverged_survivors": int(((fd < 0) & surv.ravel()).sum()),
+           "rays": int(len(b)), "rays_da_differs": int((da_s != da_f).sum()),
+           "max_da_difference_sigma": float(np.max(np.abs(da_s - da_f))), "amplitude_step_sigma": float(step),
+           "loss_turn_mismatches_away_from_boundary": int((lts[far] != ltf[far]).sum()),
+           "particles_away_from_boundary": int(far.sum())}
+    # throughput of both kernels on the Gaussian throughput workload
+    Xg = lattices.gaussian_beam(lattices.rhic_like_ring(seed=None, bb=False), n_rate, seed=12345)
+    rates = {}
+    for pol, t in tabs.items():
+        c = [torch.tensor(np.ascontiguousarray(Xg[:, k]), device=dev) for k in range(6)]
+        tune = t.autotune(c, 1, r)
+        lt_ = torch.full((n_rate,), -1, dtype=torch.int32, device=dev)
+        le_ = torch.zeros(n_rate, dtype=torch.int32, device=dev)
+        t.track_device(c, lt_, le_, 0, 1, r)
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        t.track_device(c, lt_, le_, 1, rate_turns, r)
+        e1.record()
+        torch.cuda.synchronize(dev)
+        ms = e0.elapsed_time(e1)
+        alive = int((lt_ < 0).sum())
+        rates[pol] = {"particle_turns_per_s": alive * rate_turns / (ms * 1e-3), "variant": tune["chosen"],
+                      "flops_per_particle_turn": t.info()["flops_per_turn"]}
+    out["throughput"] = rates
+    print(json.dumps(out))
+    return out
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("kind", choices=["spin", "radial", "elements"])
+    ap.add_argument("kind", choices=["spin", "radial", "elements", "contraction"])
     ap.add_argument("--seeds", type=int, default=16)
     ap.add_argument("--particles", type=int, default=2048)
     ap.add_argument("--turns", type=int, default=200)
     a = ap.parse_args(argv)
     if a.kind == "elements":
         element_costs()
+    elif a.kind == "contraction":
+        contraction(nturn=a.turns)
     else:
         run(a.kind, a.seeds, a.particles, a.turns)
 

@@ -133,3 +133,26 @@ def test_device_turn_blocks_equal_one_launch():
     b = run([7, 13, 40])
     assert np.array_equal(a[1], b[1]) and np.array_equal(a[2], b[2])
     assert np.array_equal(np.nan_to_num(a[0]), np.nan_to_num(b[0]))
+
+
+def test_fast_contraction_policy_stays_close_and_strict_is_unchanged(port_oracle):
+    """The FMA-contracted kernel (contraction policy "fast") agrees with the
+    strict kernel to rounding level over a few turns of the FODO grid, and
+    switching back to "strict" restores bit-exact parity with the oracle."""
+    lat = lt.fodo_ring()
+    line, tab = gpu_table(lat)
+    port_oracle.build(lat)
+    amps = np.linspace(0.5, 6.0, 12)
+    X = np.array([[a * 1e-3, 0, 0.5 * a * 1e-3, 0, 0, 1e-4] for a in amps])
+    nt = 20
+    xs, ss, ls, ps = tab.track_host(X.copy(), nt)
+    tab.set_contraction("fast")
+    xf, sf, lf, pf = tab.track_host(X.copy(), nt)
+    assert np.array_equal(ss, sf)
+    scale = np.sqrt(np.mean(xs ** 2, axis=0)) + 1e-300
+    assert np.max(np.abs(xf - xs) / np.maximum(np.abs(xs), scale)) < 1e-9
+    assert not np.array_equal(xf, xs)  # contraction did change some roundings
+    tab.set_contraction("strict")
+    xg, sg, lg, pg = tab.track_host(X.copy(), nt)
+    xo, so, lo, po = port_oracle.track(X.copy(), nt)
+    assert np.array_equal(xg, xo) and np.array_equal(sg, so)
