@@ -116,6 +116,14 @@ int stb_table_autotune(stb_table *t, const double *x, const double *px, const do
                        const double *z, const double *pt, long n, int nturn, double aperture_radius, int *chosen,
                        double *timings_ms, int ntimings);
 int stb_table_set_variant(stb_table *t, int variant);
+/* The autotuner for a spin table (stb_table_create_spin): xs9 = the nine
+ * device arrays x, px, y, py, z, pt, sx, sy, sz of n particles (not
+ * modified); chooses among the spin kernel's launch variants, whose names
+ * stb_spin_variant_info gives.  stb_table_set_variant indexes the spin
+ * variants for a spin table. */
+int stb_table_autotune_spin(stb_table *t, const double *const *xs9, long n, int nturn, double aperture_radius,
+                            int *chosen, double *timings_ms, int ntimings);
+int stb_spin_variant_info(int variant, char *name, int cap, int *block, int *smem);
 /* Contraction policy of the table's tracking kernel (no reference
  * counterpart).  fast = 0 (default): the strict kernel, in which every FP64
  * add and multiply rounds separately as in the reference's x86-64 build, so

@@ -123,6 +123,9 @@ SIGNATURES = [
     ("stb_scan_retire", c_int, [c_void_p, c_void_p]),
     ("stb_scan_set_abort", c_int, [c_void_p, c_int]),
     ("stb_table_set_contraction", c_int, [c_void_p, c_int]),
+    ("stb_table_autotune_spin", c_int, [c_void_p, POINTER(c_void_p), c_long, c_int, c_double, POINTER(c_int),
+                                        POINTER(c_double), c_int]),
+    ("stb_spin_variant_info", c_int, [c_int, ctypes.c_char_p, c_int, POINTER(c_int), POINTER(c_int)]),
     ("stb_scan_set_budget", c_int, [c_void_p, c_double]),
     ("stb_scan_checkpoint", c_int, [c_void_p, c_char_p]),
     ("stb_scan_restore", c_int, [c_void_p, c_char_p]),

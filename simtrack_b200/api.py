@@ -250,6 +250,16 @@ def _check_device_arrays(coords, lost_turn, lost_elem, n: int, device: int, ncoo
     ok(lost_elem, torch.int32, "lost_elem")
 
 
+NUM_SPIN_VARIANTS = 9
+
+
+def spin_variant_name(v: int) -> str:
+    buf = ctypes.create_string_buffer(64)
+    b, sm = c_int(), c_int()
+    check(lib().stb_spin_variant_info(v, buf, 64, byref(b), byref(sm)))
+    return buf.value.decode()
+
+
 def variant_name(v: int) -> str:
     buf = ctypes.create_string_buffer(64)
     b, sm = c_int(), c_int()
@@ -373,7 +383,24 @@ class SpinTable:
     def info(self) -> dict:
         out = (c_double * 6)()
         check(lib().stb_table_info(self._h, out))
-        return {"elements": int(out[0]), "pool_doubles": int(out[1]), "flops_per_turn": out[2]}
+        return {"elements": int(out[0]), "pool_doubles": int(out[1]), "flops_per_turn": out[2],
+                "smem": bool(out[3]), "variant": int(out[5]), "variant_name": spin_variant_name(int(out[5]))}
+
+    def autotune(self, coords, nturn: int = 1, aperture_radius: float = 0.0) -> dict:
+        """Times every launch variant of the spin kernel on a copy of `coords`
+        (9 CUDA float64 tensors, not modified) and keeps the fastest."""
+        n = coords[0].numel()
+        if len(coords) != 9:
+            raise ValueError("a spin table is tuned on nine coordinate arrays")
+        arr = (c_void_p * 9)(*[c.data_ptr() for c in coords])
+        chosen = c_int()
+        t = (c_double * 16)()
+        check(lib().stb_table_autotune_spin(self._h, arr, n, nturn, aperture_radius, byref(chosen), t, 16))
+        return {"chosen": spin_variant_name(chosen.value),
+                "ms": {spin_variant_name(v): t[v] for v in range(NUM_SPIN_VARIANTS)}}
+
+    def set_variant(self, v: int) -> None:
+        check(lib().stb_table_set_variant(self._h, v))
 
     def track_host(self, x: np.ndarray, nturn: int, aperture_radius: float = 0.0, stable=None):
         """Track_Spin over AoS host x[n, 9] (updated in place); returns (x, stable, lost_turn, lost_post)."""

@@ -113,7 +113,9 @@ stb_table *table_build(const Line &line, int device, bool spin = false) {
   cuda_check(cudaDeviceGetAttribute(&t->num_sms, cudaDevAttrMultiProcessorCount, device), "SM count");
   const size_t need = track_smem_bytes((int)t->host.hdr.size(), t->npool_padded);
   t->use_smem = (long)need <= (long)track_smem_limit(device);
-  t->variant = t->use_smem ? 0 : 2;
+  // default launch variant: the first shared-memory one when the table fits,
+  // else the first L1 one (stb_track.cu kVariants, stb_spin.cu kSpinVariants)
+  t->variant = t->use_smem ? 0 : 3;
   return t.release();
 }
 
@@ -151,49 +153,60 @@ int track_device(stb_table *t, double *x, double *px, double *y, double *py, dou
   return STB_OK;
 }
 
-// Times every launch variant on a scratch copy of up to `nsample` particles
-// and keeps the fastest for this table.
-int autotune(stb_table *t, const double *const in[6], long n, int nturn, double radius, int *chosen,
+// Times every launch variant (the orbit kernel's, or the spin kernel's for a
+// spin table) on a device-side copy of the n given particles (nc = 6 or 9
+// coordinate arrays, not modified) and keeps the fastest for this table.
+int autotune(stb_table *t, const double *const *in, int nc, long n, int nturn, double radius, int *chosen,
              double *timings, int ntimings) {
   if (!t) throw Error(STB_EINVAL, "table is NULL");
-  if (t->host.spin) throw Error(STB_EINVAL, "table is flattened for spin tracking");
-  for (int k = 0; k < 6; k++)
+  if (nc != (t->host.spin ? 9 : 6))
+    throw Error(STB_EINVAL, t->host.spin ? "a spin table is tuned on nine coordinate arrays"
+                                         : "table is flattened for orbit tracking: six coordinate arrays");
+  for (int k = 0; k < nc; k++)
     if (!in[k]) throw Error(STB_EINVAL, "NULL coordinate array");
   if (n <= 0 || nturn <= 0) throw Error(STB_EINVAL, "autotune needs particles and turns");
   DeviceGuard g(t->device);
   const long m = n;
   double *buf = nullptr;
   int32_t *lost = nullptr;
-  cuda_check(cudaMalloc(&buf, sizeof(double) * 6 * m), "cudaMalloc(autotune)");
-  struct Free {
-    void *p;
-    ~Free() { if (p) cudaFree(p); }
-  } f1{buf};
+  cuda_check(cudaMalloc(&buf, sizeof(double) * nc * m), "cudaMalloc(autotune)");
+  DevFree f1{buf};
   cuda_check(cudaMalloc(&lost, sizeof(int32_t) * 2 * m), "cudaMalloc(autotune)");
-  Free f2{lost};
+  DevFree f2{lost};
   cudaEvent_t e0, e1;
   cuda_check(cudaEventCreate(&e0), "event");
   cuda_check(cudaEventCreate(&e1), "event");
   const int saved = t->variant;
+  const int nvar = t->host.spin ? kNumSpinVariants : kNumTrackVariants;
   int best = -1;
   float best_ms = 0.f;
-  for (int v = 0; v < kNumTrackVariants; v++) {
+  for (int v = 0; v < nvar; v++) {
     float ms = -1.f;
-    if (!kVariants[v].smem || t->use_smem) {
-      t->variant = v;
+    const bool smem = t->host.spin ? kSpinVariants[v].smem : kVariants[v].smem;
+    if (!smem || t->use_smem) {
       float runs[2] = {0.f, 0.f};
       bool ok = true;
       for (int r = 0; r < 2 && ok; r++) {
-        for (int k = 0; k < 6; k++)
+        for (int k = 0; k < nc; k++)
           cuda_check(cudaMemcpy(buf + k * m, in[k], sizeof(double) * m, cudaMemcpyDeviceToDevice), "copy");
         cuda_check(cudaMemset(lost, 0xff, sizeof(int32_t) * m), "reset");
         cuda_check(cudaMemset(lost + m, 0, sizeof(int32_t) * m), "reset");
-        cuda_check(cudaEventRecord(e0), "event");
         TrackArgs a = make_args(t);
         a.x = buf; a.px = buf + m; a.y = buf + 2 * m; a.py = buf + 3 * m; a.z = buf + 4 * m; a.pt = buf + 5 * m;
         a.n = m; a.turn0 = 1; a.nturn = nturn; a.r2 = radius > 0 ? radius * radius : INFINITY;
         a.lost_turn = lost; a.lost_elem = lost + m; a.dump = nullptr;
-        if ((t->fast ? launch_track_fast : launch_track)(a, t->num_sms, v, 0) != cudaSuccess) {
+        cuda_check(cudaEventRecord(e0), "event");
+        cudaError_t le;
+        if (t->host.spin) {
+          SpinArgs sa{};
+          sa.t = a;
+          sa.sx = buf + 6 * m; sa.sy = buf + 7 * m; sa.sz = buf + 8 * m;
+          sa.dump = nullptr;
+          le = launch_spin(sa, t->num_sms, v, 0);
+        } else {
+          le = (t->fast ? launch_track_fast : launch_track)(a, t->num_sms, v, 0);
+        }
+        if (le != cudaSuccess) {
           cudaGetLastError();
           ok = false;
           break;
@@ -409,7 +422,7 @@ int spin_device(stb_table *t, double *const xs[9], long n, int turn0, int nturn,
   a.t.lost_turn = lost_turn;
   a.t.lost_elem = lost_elem;
   a.dump = dump;
-  cuda_check(launch_spin(a, t->num_sms, t->use_smem, s), "spin kernel launch");
+  cuda_check(launch_spin(a, t->num_sms, t->variant, s), "spin kernel launch");
   return STB_OK;
 }
 
@@ -932,7 +945,7 @@ int stb_table_info(const stb_table *t, double *info) {
     info[0] = (double)t->host.hdr.size();
     info[1] = (double)t->host.pool.size();
     info[2] = t->host.flops_per_turn;
-    info[3] = stb::kVariants[t->variant].smem ? 1.0 : 0.0;
+    info[3] = (t->host.spin ? stb::kSpinVariants[t->variant].smem : stb::kVariants[t->variant].smem) ? 1.0 : 0.0;
     info[4] = (double)track_smem_bytes((int)t->host.hdr.size(), t->npool_padded);
     info[5] = (double)t->variant;
     return STB_OK;
@@ -958,16 +971,39 @@ int stb_table_autotune(stb_table *t, const double *x, const double *px, const do
                        double *timings_ms, int ntimings) {
   return guarded([&] {
     const double *in[6] = {x, px, y, py, z, pt};
-    return autotune(t, in, n, nturn, aperture_radius, chosen, timings_ms, ntimings);
+    return autotune(t, in, 6, n, nturn, aperture_radius, chosen, timings_ms, ntimings);
+  });
+}
+
+int stb_table_autotune_spin(stb_table *t, const double *const *xs9, long n, int nturn, double aperture_radius,
+                            int *chosen, double *timings_ms, int ntimings) {
+  return guarded([&] {
+    if (!xs9) throw Error(STB_EINVAL, "NULL coordinate array list");
+    return autotune(t, xs9, 9, n, nturn, aperture_radius, chosen, timings_ms, ntimings);
   });
 }
 
 int stb_table_set_variant(stb_table *t, int variant) {
   return guarded([&] {
     if (!t) throw Error(STB_EINVAL, "table is NULL");
-    if (variant < 0 || variant >= kNumTrackVariants) throw Error(STB_EINVAL, "variant out of range");
-    if (kVariants[variant].smem && !t->use_smem) throw Error(STB_EINVAL, "table does not fit shared memory");
+    const int nvar = t->host.spin ? kNumSpinVariants : kNumTrackVariants;
+    if (variant < 0 || variant >= nvar) throw Error(STB_EINVAL, "variant out of range");
+    const bool smem = t->host.spin ? kSpinVariants[variant].smem : kVariants[variant].smem;
+    if (smem && !t->use_smem) throw Error(STB_EINVAL, "table does not fit shared memory");
     t->variant = variant;
+    return STB_OK;
+  });
+}
+
+int stb_spin_variant_info(int variant, char *name, int cap, int *block, int *smem) {
+  return guarded([&] {
+    if (variant < 0 || variant >= kNumSpinVariants) throw Error(STB_EINVAL, "variant out of range");
+    if (name && cap > 0) {
+      std::strncpy(name, kSpinVariants[variant].name, (size_t)cap - 1);
+      name[cap - 1] = 0;
+    }
+    if (block) *block = kSpinVariants[variant].block;
+    if (smem) *smem = kSpinVariants[variant].smem ? 1 : 0;
     return STB_OK;
   });
 }

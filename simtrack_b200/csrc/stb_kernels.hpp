@@ -49,7 +49,15 @@ struct SpinArgs {
   // Optional per-element probe: dump[((i * nturn + t) * nelem + e) * 9 + k].
   double *dump;
 };
-cudaError_t launch_spin(const SpinArgs &a, int num_sms, bool use_smem, cudaStream_t stream);
+struct SpinVariant {
+  bool smem;
+  int block;
+  int min_blocks;
+  const char *name;
+};
+constexpr int kNumSpinVariants = 9;
+extern const SpinVariant kSpinVariants[kNumSpinVariants];
+cudaError_t launch_spin(const SpinArgs &a, int num_sms, int variant, cudaStream_t stream);
 
 // Track_Radial (stb_radial.cu): zsub[j] = z of the on-momentum reference
 // particle after element j (one device thread), then the tracking kernel

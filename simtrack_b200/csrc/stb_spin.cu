@@ -285,8 +285,8 @@ __device__ __noinline__ void spin_element(const ElemHeader &h, const double *P, 
   }
 }
 
-template <bool kSmem, int kBlock, bool kDump>
-__global__ void __launch_bounds__(kBlock, 1) spin_track_kernel(const __grid_constant__ SpinArgs sa) {
+template <bool kSmem, int kBlock, int kMinBlocks, bool kDump>
+__global__ void __launch_bounds__(kBlock, kMinBlocks) spin_track_kernel(const __grid_constant__ SpinArgs sa) {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ __align__(8) uint64_t bar;
   const TrackArgs &a = sa.t;
@@ -364,9 +364,9 @@ __global__ void __launch_bounds__(kBlock, 1) spin_track_kernel(const __grid_cons
   }
 }
 
-template <bool kSmem, int kBlock, bool kDump>
+template <bool kSmem, int kBlock, int kMinBlocks, bool kDump>
 cudaError_t launch_spin_variant(const SpinArgs &a, int num_sms, size_t smem, cudaStream_t stream) {
-  auto kern = spin_track_kernel<kSmem, kBlock, kDump>;
+  auto kern = spin_track_kernel<kSmem, kBlock, kMinBlocks, kDump>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   int per_sm = 0;
@@ -383,13 +383,33 @@ cudaError_t launch_spin_variant(const SpinArgs &a, int num_sms, size_t smem, cud
 
 }  // namespace
 
-cudaError_t launch_spin(const SpinArgs &a, int num_sms, bool use_smem, cudaStream_t stream) {
+// Launch variants of the spin kernel the autotuner chooses from: the element
+// table staged in shared memory (one CTA per SM) or read through L1; CTA
+// size and minimum resident CTAs (registers per thread = 65536 / (block *
+// min_blocks)).  Small CTAs spread a few thousand particles per seed over
+// every SM when several seeds run side by side on their own streams.
+const SpinVariant kSpinVariants[kNumSpinVariants] = {
+    {true, 512, 1, "smem_b512_r128"}, {true, 1024, 1, "smem_b1024_r64"}, {true, 768, 1, "smem_b768_r85"},
+    {false, 256, 2, "l1_b256_r128"},  {false, 256, 3, "l1_b256_r80"},    {false, 256, 4, "l1_b256_r64"},
+    {false, 128, 4, "l1_b128_r128"},  {false, 64, 8, "l1_b64_r128"},     {false, 64, 12, "l1_b64_r85"},
+};
+
+cudaError_t launch_spin(const SpinArgs &a, int num_sms, int variant, cudaStream_t stream) {
   if (a.t.n <= 0 || a.t.nturn <= 0) return cudaSuccess;
-  if (a.dump) return launch_spin_variant<false, 128, true>(a, num_sms, 0, stream);
-  if (use_smem)
-    return launch_spin_variant<true, 512, false>(a, num_sms, track_smem_bytes(a.t.nelem, a.t.npool_padded),
-                                                 stream);
-  return launch_spin_variant<false, 256, false>(a, num_sms, 0, stream);
+  if (a.dump) return launch_spin_variant<false, 128, 1, true>(a, num_sms, 0, stream);
+  const size_t sm = track_smem_bytes(a.t.nelem, a.t.npool_padded);
+  switch (variant) {
+    case 0: return launch_spin_variant<true, 512, 1, false>(a, num_sms, sm, stream);
+    case 1: return launch_spin_variant<true, 1024, 1, false>(a, num_sms, sm, stream);
+    case 2: return launch_spin_variant<true, 768, 1, false>(a, num_sms, sm, stream);
+    case 3: return launch_spin_variant<false, 256, 2, false>(a, num_sms, 0, stream);
+    case 4: return launch_spin_variant<false, 256, 3, false>(a, num_sms, 0, stream);
+    case 5: return launch_spin_variant<false, 256, 4, false>(a, num_sms, 0, stream);
+    case 6: return launch_spin_variant<false, 128, 4, false>(a, num_sms, 0, stream);
+    case 7: return launch_spin_variant<false, 64, 8, false>(a, num_sms, 0, stream);
+    case 8: return launch_spin_variant<false, 64, 12, false>(a, num_sms, 0, stream);
+    default: return cudaErrorInvalidValue;
+  }
 }
 
 }  // namespace stb

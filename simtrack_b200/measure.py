@@ -52,6 +52,10 @@ def run(kind: str = "spin", nseed: int = 16, n: int = 2048, nturn: int = 200, wa
                                                                                       device=dev)))
         flops = t.info()["flops_per_turn"]
     radius = lat.aperture_radius
+    chosen = []
+    if spin:  # launch variant per seed table, tuned on its own particles
+        for t, c in zip(tabs, coords):
+            chosen.append(t.autotune(c, 1, radius)["chosen"])
     streams = [torch.cuda.Stream(dev) for _ in range(nseed)]
 
     def launch(turn0, nt):
@@ -79,7 +83,8 @@ def run(kind: str = "spin", nseed: int = 16, n: int = 2048, nturn: int = 200, wa
     pt = 0.5 * (alive0 + alive1) * nturn
     line = {"measure": f"{kind} tracking", "ring": "EIC-like (spin)" if spin else "RHIC-like (Track_Radial)",
             "seeds": nseed, "particles_per_seed": n, "turns": nturn, "ms": ms, "particle_turns_per_s": pt / (ms * 1e-3),
-            "flops_per_particle_turn": flops, "tflops": pt * flops / (ms * 1e-3) / 1e12, "alive": [alive0, alive1]}
+            "flops_per_particle_turn": flops, "tflops": pt * flops / (ms * 1e-3) / 1e12, "alive": [alive0, alive1],
+            "variants": sorted(set(chosen))}
     print(json.dumps(line))
     return line
 

@@ -128,3 +128,31 @@ def test_tables_keep_to_their_mode(native_lib):
     torch.cuda.synchronize()
     xh, st, _, _ = spin_tab.track_host(spin_particles()[:3].copy(), 1)
     np.testing.assert_array_equal(x.cpu().numpy().T, xh)
+
+
+def test_spin_launch_variants_agree_and_autotune(native_lib):
+    """Every launch variant of the spin kernel gives the same bits (same maps,
+    different CTA shapes and register budgets), and the autotuner leaves the
+    inputs untouched and picks one of them."""
+    import torch
+    from simtrack_b200.api import NUM_SPIN_VARIANTS
+    lat = lt.eic_like_ring(seed=3)
+    tab = SpinTable(lt.build_line(lat))
+    X = _eic_particles(lat, n=200, seed=9)
+    coords = [torch.tensor(X[:, k].copy(), device="cuda:0") for k in range(9)]
+    tune = tab.autotune(coords, 1, 0.03)
+    assert tune["chosen"] in tune["ms"]
+    assert np.array_equal(torch.stack(coords, 1).cpu().numpy(), X)
+    ref = None
+    for v in range(NUM_SPIN_VARIANTS):
+        try:
+            tab.set_variant(v)
+        except SimTrackError:
+            continue  # a shared-memory variant the table does not fit
+        out = tab.track_host(X.copy(), 3, 0.03)
+        if ref is None:
+            ref = out
+        else:
+            for a, b in zip(ref, out):
+                assert np.array_equal(a, b), f"variant {v}"
+    assert ref is not None
