@@ -133,6 +133,17 @@ int stb_spin_variant_info(int variant, char *name, int cap, int *block, int *sme
  * separate over many turns.  Applies to stb_track_device / stb_track_host
  * and the autotuner on this table. */
 int stb_table_set_contraction(stb_table *t, int fast);
+/* Segmented staging (no reference counterpart).  An orbit table too large to
+ * sit in shared memory whole is cut into consecutive segments of at most
+ * `bytes` bytes each (element headers plus their parameters); the seg_*
+ * launch variants stage them into two shared-memory buffers with bulk copies,
+ * the next segment's copy running while the current one is tracked.  The
+ * autotuner picks the segment size; stb_table_set_segment_bytes sets it
+ * (1024 bytes to half the shared memory of a CTA; STB_EINVAL for tables that
+ * fit whole and spin tables).  stb_table_segments reports the current plan
+ * (nseg = 0: none). */
+int stb_table_set_segment_bytes(stb_table *t, long bytes);
+int stb_table_segments(const stb_table *t, int *nseg, int *seg_bytes);
 /* name (NUL-terminated, truncated to cap), CTA size and shared-memory flag of a launch variant */
 int stb_track_variant_info(int variant, char *name, int cap, int *block, int *smem);
 

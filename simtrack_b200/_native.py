@@ -123,6 +123,8 @@ SIGNATURES = [
     ("stb_scan_retire", c_int, [c_void_p, c_void_p]),
     ("stb_scan_set_abort", c_int, [c_void_p, c_int]),
     ("stb_table_set_contraction", c_int, [c_void_p, c_int]),
+    ("stb_table_set_segment_bytes", c_int, [c_void_p, c_long]),
+    ("stb_table_segments", c_int, [c_void_p, POINTER(c_int), POINTER(c_int)]),
     ("stb_table_autotune_spin", c_int, [c_void_p, POINTER(c_void_p), c_long, c_int, c_double, POINTER(c_int),
                                         POINTER(c_double), c_int]),
     ("stb_spin_variant_info", c_int, [c_int, ctypes.c_char_p, c_int, POINTER(c_int), POINTER(c_int)]),

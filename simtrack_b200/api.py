@@ -220,7 +220,7 @@ class Line:
             pass
 
 
-NUM_VARIANTS = 11
+NUM_VARIANTS = 14
 NUM_SCAN_VARIANTS = 7
 
 
@@ -296,6 +296,15 @@ class Table:
 
     def set_variant(self, v: int) -> None:
         check(lib().stb_table_set_variant(self._h, v))
+
+    def segments(self) -> dict:
+        """Segment plan of a table too large for shared memory: {"nseg", "bytes"} (nseg 0: none)."""
+        n, b = c_int(), c_int()
+        check(lib().stb_table_segments(self._h, byref(n), byref(b)))
+        return {"nseg": n.value, "bytes": b.value}
+
+    def set_segment_bytes(self, nbytes: int) -> None:
+        check(lib().stb_table_set_segment_bytes(self._h, int(nbytes)))
 
     def set_contraction(self, policy: str) -> None:
         """"strict" (default: results equal the reference's) or "fast" (the

@@ -88,9 +88,35 @@ void table_destroy(stb_table *t) {
   if (t->d_status) cudaFree(t->d_status);
   if (t->d_zsub) cudaFree(t->d_zsub);
   if (t->d_io) cudaFree(t->d_io);
+  if (t->d_segs) cudaFree(t->d_segs);
   if (t->io_stream) cudaStreamDestroy(t->io_stream);
   if (prev >= 0) cudaSetDevice(prev);
   delete t;
+}
+
+// Plans the table's segments for buffers of `budget` bytes and uploads the
+// plan (nseg = 0 when an element alone exceeds the budget).
+void set_segments(stb_table *t, size_t budget) {
+  const std::vector<SegDesc> segs =
+      plan_segments(t->host.hdr.data(), (int)t->host.hdr.size(), t->npool_padded, budget);
+  if (t->d_segs) {
+    cudaFree(t->d_segs);
+    t->d_segs = nullptr;
+  }
+  t->nseg = 0;
+  t->seg_bytes = 0;
+  if (segs.empty()) return;
+  cuda_check(cudaMalloc(&t->d_segs, sizeof(SegDesc) * segs.size()), "cudaMalloc(segments)");
+  cuda_check(cudaMemcpy(t->d_segs, segs.data(), sizeof(SegDesc) * segs.size(), cudaMemcpyHostToDevice),
+             "upload segments");
+  t->nseg = (int)segs.size();
+  t->seg_bytes = (int)budget;
+}
+
+bool variant_allowed(const stb_table *t, int v) {
+  if (t->host.spin) return !kSpinVariants[v].smem || t->use_smem;
+  if (kVariants[v].seg) return !t->use_smem && t->nseg > 1;
+  return !kVariants[v].smem || t->use_smem;
 }
 
 stb_table *table_build(const Line &line, int device, bool spin = false) {
@@ -116,6 +142,9 @@ stb_table *table_build(const Line &line, int device, bool spin = false) {
   // default launch variant: the first shared-memory one when the table fits,
   // else the first L1 one (stb_track.cu kVariants, stb_spin.cu kSpinVariants)
   t->variant = t->use_smem ? 0 : 3;
+  // tables too large for one shared-memory copy are also staged segment by
+  // segment (two buffers of half the shared memory each) by the seg_* variants
+  if (!t->use_smem && !spin) set_segments(t.get(), (size_t)track_smem_limit(device) / 2 & ~size_t(15));
   return t.release();
 }
 
@@ -127,6 +156,9 @@ TrackArgs make_args(stb_table *t) {
   a.npool_padded = t->npool_padded;
   a.ref = t->host.ref;
   a.status = t->d_status;
+  a.segs = t->d_segs;
+  a.nseg = t->nseg;
+  a.seg_bytes = t->seg_bytes;
   return a;
 }
 
@@ -180,10 +212,18 @@ int autotune(stb_table *t, const double *const *in, int nc, long n, int nturn, d
   const int nvar = t->host.spin ? kNumSpinVariants : kNumTrackVariants;
   int best = -1;
   float best_ms = 0.f;
-  for (int v = 0; v < nvar; v++) {
+  // segment length: the largest buffers (half the shared memory each) and
+  // buffers half that size; the faster plan stays with the seg_* variants
+  const size_t seg_full = (size_t)track_smem_limit(t->device) / 2 & ~size_t(15);
+  const size_t seg_budgets[2] = {seg_full, seg_full / 2 & ~size_t(15)};
+  size_t best_seg = (size_t)t->seg_bytes;
+  for (int vv = 0; vv < nvar + (t->nseg > 0 ? 3 : 0); vv++) {
+    // vv >= nvar: the seg_* variants again with the smaller segment budget
+    const int v = vv < nvar ? vv : kNumTrackVariants - 3 + (vv - nvar);
+    const bool seg_v = !t->host.spin && kVariants[v].seg;
+    if (seg_v) set_segments(t, seg_budgets[vv < nvar ? 0 : 1]);
     float ms = -1.f;
-    const bool smem = t->host.spin ? kSpinVariants[v].smem : kVariants[v].smem;
-    if (!smem || t->use_smem) {
+    if (variant_allowed(t, v)) {
       float runs[2] = {0.f, 0.f};
       bool ok = true;
       for (int r = 0; r < 2 && ok; r++) {
@@ -217,14 +257,17 @@ int autotune(stb_table *t, const double *const *in, int nc, long n, int nturn, d
       }
       if (ok) ms = runs[1];
     }
-    if (timings && v < ntimings) timings[v] = ms;
+    if (timings && v < ntimings && (vv < nvar || (ms > 0.f && (timings[v] <= 0.0 || ms < timings[v]))))
+      timings[v] = ms;
     if (ms > 0.f && (best < 0 || ms < best_ms)) {
       best = v;
       best_ms = ms;
+      if (seg_v) best_seg = (size_t)t->seg_bytes;
     }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  if (t->nseg > 0 || best_seg > 0) set_segments(t, best_seg > 0 ? best_seg : seg_full);
   t->variant = best >= 0 ? best : saved;
   if (chosen) *chosen = t->variant;
   return STB_OK;
@@ -988,8 +1031,10 @@ int stb_table_set_variant(stb_table *t, int variant) {
     if (!t) throw Error(STB_EINVAL, "table is NULL");
     const int nvar = t->host.spin ? kNumSpinVariants : kNumTrackVariants;
     if (variant < 0 || variant >= nvar) throw Error(STB_EINVAL, "variant out of range");
-    const bool smem = t->host.spin ? kSpinVariants[variant].smem : kVariants[variant].smem;
-    if (smem && !t->use_smem) throw Error(STB_EINVAL, "table does not fit shared memory");
+    if (!variant_allowed(t, variant))
+      throw Error(STB_EINVAL, !t->host.spin && kVariants[variant].seg
+                                  ? "segmented staging is for tables that do not fit shared memory whole"
+                                  : "table does not fit shared memory");
     t->variant = variant;
     return STB_OK;
   });
@@ -1004,6 +1049,28 @@ int stb_spin_variant_info(int variant, char *name, int cap, int *block, int *sme
     }
     if (block) *block = kSpinVariants[variant].block;
     if (smem) *smem = kSpinVariants[variant].smem ? 1 : 0;
+    return STB_OK;
+  });
+}
+
+int stb_table_segments(const stb_table *t, int *nseg, int *seg_bytes) {
+  return guarded([&] {
+    if (!t) throw Error(STB_EINVAL, "table is NULL");
+    if (nseg) *nseg = t->nseg;
+    if (seg_bytes) *seg_bytes = t->seg_bytes;
+    return STB_OK;
+  });
+}
+
+int stb_table_set_segment_bytes(stb_table *t, long bytes) {
+  return guarded([&] {
+    if (!t) throw Error(STB_EINVAL, "table is NULL");
+    if (t->host.spin || t->use_smem) throw Error(STB_EINVAL, "only orbit tables too large for shared memory are segmented");
+    const long limit = track_smem_limit(t->device) / 2;
+    if (bytes < 1024 || bytes > limit) throw Error(STB_EINVAL, "segment bytes out of range (1024..half the shared memory)");
+    DeviceGuard g(t->device);
+    set_segments(t, (size_t)bytes & ~size_t(15));
+    if (t->nseg == 0) throw Error(STB_EINVAL, "an element's parameters alone exceed the segment size");
     return STB_OK;
   });
 }

@@ -4,6 +4,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <vector>
 
 #include "stb_status.hpp"
 #include "stb_table.hpp"
@@ -13,13 +14,14 @@ namespace stb {
 // One compiled launch configuration of the tracking kernel.
 struct TrackVariant {
   bool smem;       // element table staged in shared memory (else read through L1)
+  bool seg;        // staged segment by segment, double-buffered (tables too large for shared memory)
   int block;       // threads per CTA
   int min_blocks;  // __launch_bounds__ minimum resident CTAs per SM
   int ppt;         // particles per thread
   const char *name;
   bool prefetch;   // next element header loaded while the current element runs
 };
-constexpr int kNumTrackVariants = 11;
+constexpr int kNumTrackVariants = 14;
 extern const TrackVariant kVariants[kNumTrackVariants];
 
 struct TrackArgs {
@@ -39,6 +41,11 @@ struct TrackArgs {
   // Optional per-element probe: when non-NULL, coordinates after every element
   // are written to dump[((i * nturn + t) * nelem + e) * 6 + k].
   double *dump;
+  // Segmented staging (launch variants with seg set): nseg segments, each
+  // staged into one of two shared-memory buffers of seg_bytes bytes.
+  const SegDesc *segs;
+  int nseg;
+  int seg_bytes;
 };
 
 // Spin tracking (stb_spin.cu): the orbit arguments plus the spin unit vector
@@ -76,6 +83,9 @@ void math_eval_host(int fn, const double *in, double *out, long n);
 cudaError_t fp64_peak_probe(int device, double *tflops);
 
 size_t track_smem_bytes(int nelem, int npool_padded);
+// Consecutive segments of at most `budget` bytes of staged table (headers plus
+// 16-byte aligned pool slice); empty if one element alone exceeds the budget.
+std::vector<SegDesc> plan_segments(const ElemHeader *hdr, int nelem, int npool_padded, size_t budget);
 int track_smem_limit(int device);
 cudaError_t launch_track(const TrackArgs &a, int num_sms, int variant, cudaStream_t stream);
 // The same kernel compiled with FMA contraction allowed (stb_track_fast.cu).

@@ -20,6 +20,11 @@ struct stb_table {
   bool use_smem = false;  // the table fits the shared-memory variants
   int variant = 2;        // launch variant (stb::kVariants), set by the autotuner
   bool fast = false;      // FMA-contracted kernel (stb_table_set_contraction) instead of the strict one
+  // Segment plan for tables that do not fit shared memory whole (seg_*
+  // launch variants): segments of at most seg_bytes bytes each.
+  stb::SegDesc *d_segs = nullptr;
+  int nseg = 0;
+  int seg_bytes = 0;
   int *d_status = nullptr;
   int num_sms = 0;
   double *d_zsub = nullptr;  // Track_Radial's per-element on-momentum z (computed on first use)

@@ -77,6 +77,15 @@ struct ElemHeader {
 };
 static_assert(sizeof(ElemHeader) == 32, "ElemHeader must stay 32 bytes");
 
+// A lattice segment for tables too large for shared memory: elements
+// [e0, e0 + ne) whose headers and pool slice [pool_lo, pool_lo + pool_n)
+// (pool_lo and pool_n even, so both bulk copies start and end on 16-byte
+// boundaries) fit one staging buffer.
+struct SegDesc {
+  int32_t e0, ne;
+  int32_t pool_lo, pool_n;
+};
+
 // Reference-particle constants snapshotted from the global state at flatten time.
 struct RefConsts {
   double gamma, beta, energy, brho;

@@ -18,6 +18,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <vector>
 
 #include "stb_track_launch.cuh"
 
@@ -38,13 +39,37 @@ int track_smem_limit(int device) {
 // caps registers per thread at 65536 / (block * min_blocks)) and particles
 // per thread.
 const TrackVariant kVariants[kNumTrackVariants] = {
-    {true, 512, 1, 1, "smem_b512_r128", false},       {true, 1024, 1, 1, "smem_b1024_r64", false},
-    {true, 768, 1, 1, "smem_b768_r85", false},        {false, 256, 2, 1, "l1_b256_r128", false},
-    {false, 256, 3, 1, "l1_b256_r80", false},         {false, 256, 4, 1, "l1_b256_r64", false},
-    {false, 384, 2, 1, "l1_b384_r85", false},         {true, 512, 1, 2, "smem_b512_r128_ppt2", false},
-    {false, 128, 3, 2, "l1_b128_r168_ppt2", false},   {true, 1024, 1, 1, "smem_b1024_r64_pf", true},
-    {true, 768, 1, 1, "smem_b768_r85_pf", true},
+    {true, false, 512, 1, 1, "smem_b512_r128", false},      {true, false, 1024, 1, 1, "smem_b1024_r64", false},
+    {true, false, 768, 1, 1, "smem_b768_r85", false},       {false, false, 256, 2, 1, "l1_b256_r128", false},
+    {false, false, 256, 3, 1, "l1_b256_r80", false},        {false, false, 256, 4, 1, "l1_b256_r64", false},
+    {false, false, 384, 2, 1, "l1_b384_r85", false},        {true, false, 512, 1, 2, "smem_b512_r128_ppt2", false},
+    {false, false, 128, 3, 2, "l1_b128_r168_ppt2", false},  {true, false, 1024, 1, 1, "smem_b1024_r64_pf", true},
+    {true, false, 768, 1, 1, "smem_b768_r85_pf", true},     {true, true, 1024, 1, 1, "seg_b1024_r64", false},
+    {true, true, 768, 1, 1, "seg_b768_r85", false},         {true, true, 512, 1, 1, "seg_b512_r128", false},
 };
+
+// Segments of at most `budget` bytes each (headers plus the 16-byte aligned
+// pool slice), in element order; empty when one element alone exceeds it.
+std::vector<SegDesc> plan_segments(const ElemHeader *hdr, int nelem, int npool_padded, size_t budget) {
+  std::vector<SegDesc> out;
+  int e0 = 0;
+  auto pool_end = [&](int e) { return e + 1 < nelem ? hdr[e + 1].poff : npool_padded; };
+  while (e0 < nelem) {
+    const int lo = hdr[e0].poff & ~1;
+    int e1 = e0;
+    while (e1 < nelem) {
+      const int hi = (pool_end(e1) + 1) & ~1;
+      const size_t b = (size_t)(e1 - e0 + 1) * sizeof(ElemHeader) + (size_t)(hi - lo) * 8;
+      if (b > budget) break;
+      e1++;
+    }
+    if (e1 == e0) return {};
+    const int hi = (pool_end(e1 - 1) + 1) & ~1;
+    out.push_back(SegDesc{e0, e1 - e0, lo, hi - lo});
+    e0 = e1;
+  }
+  return out;
+}
 
 cudaError_t launch_track(const TrackArgs &a, int num_sms, int variant, cudaStream_t stream) {
   return launch_track_variants(a, num_sms, variant, stream);

@@ -72,6 +72,40 @@ __device__ bool stage_table(const TrackArgs &a, unsigned char *smem, uint64_t *b
   return stage_table_ptr(a.hdr, a.nelem, a.pool, a.npool_padded, smem, bar, 0, true);
 }
 
+// Segmented staging.  One thread issues the bulk copies of segment `sg`
+// (its headers, then its pool slice) into `buf`, completing on `bar`.  Every
+// copy starts on a 16-byte boundary and is a multiple of 16 bytes (headers
+// are 32 bytes, pool_lo and pool_n are even).
+__device__ __forceinline__ void issue_segment(const TrackArgs &a, const SegDesc &sg, unsigned char *buf,
+                                              uint64_t *bar) {
+  const uint32_t hbytes = (uint32_t)sg.ne * (uint32_t)sizeof(ElemHeader);
+  const uint32_t pbytes = (uint32_t)sg.pool_n * 8u;
+  const uint32_t b = (uint32_t)__cvta_generic_to_shared(bar);
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(b), "r"(hbytes + pbytes) : "memory");
+  constexpr uint32_t kChunk = 32768;
+  const unsigned char *gh = (const unsigned char *)(a.hdr + sg.e0);
+  const unsigned char *gp = (const unsigned char *)(a.pool + sg.pool_lo);
+  for (uint32_t off = 0; off < hbytes; off += kChunk)
+    bulk_g2s(buf + off, gh + off, (hbytes - off) < kChunk ? (hbytes - off) : kChunk, bar);
+  for (uint32_t off = 0; off < pbytes; off += kChunk)
+    bulk_g2s(buf + hbytes + off, gp + off, (pbytes - off) < kChunk ? (pbytes - off) : kChunk, bar);
+}
+
+// Bounded wait of the calling thread for phase `phase` of `bar`.
+__device__ __forceinline__ bool wait_phase(uint64_t *bar, uint32_t phase) {
+  const uint32_t b = (uint32_t)__cvta_generic_to_shared(bar);
+  uint32_t done = 0;
+  for (int iter = 0; iter < (1 << 22) && !done; iter++) {
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(b), "r"(phase & 1u)
+        : "memory");
+  }
+  return done != 0;
+}
+
 // Track()'s loss test (simtrack.cpp:20802): |x| > APx, |y| > APy or NaN;
 // !(|x| <= APx) is true for NaN as well.  r2 is the circular aperture radius
 // squared, +inf when there is none.
@@ -352,17 +386,149 @@ __device__ __forceinline__ void store_particle(const TrackArgs &a, long i, const
   a.pt[i] = p.pt;
 }
 
+// Loads particle base + k*kBlock (k < kPPT) into registers, applying
+// Track()'s entry check at turn 0; returns how many are alive.
+template <int kBlock, int kPPT>
+__device__ __forceinline__ int load_particles(const TrackArgs &a, long base, Particle (&p)[kPPT],
+                                              PtCache (&c)[kPPT], bool (&alive)[kPPT]) {
+  int nalive = 0;
+#pragma unroll
+  for (int k = 0; k < kPPT; k++) {
+    const long i = base + (long)k * kBlock;
+    alive[k] = i < a.n && a.lost_turn[i] < 0;
+    p[k] = Particle{0., 0., 0., 0., 0., 0.};
+    if (alive[k]) {
+      p[k] = Particle{a.x[i], a.px[i], a.y[i], a.py[i], a.z[i], a.pt[i]};
+      // Track()'s entry quick check, simtrack.cpp:20795-20796
+      if (a.turn0 == 0 && (fabs(p[k].x) > 0.1 || fabs(p[k].y) > 0.1)) {
+        a.lost_turn[i] = 0;
+        a.lost_elem[i] = 0;
+        alive[k] = false;
+        p[k] = Particle{0., 0., 0., 0., 0., 0.};
+      }
+    }
+    pt_refresh(a.ref, p[k].pt, c[k]);
+    nalive += alive[k] ? 1 : 0;
+  }
+  return nalive;
+}
+
+// Loss bookkeeping after global element e of turn t (see track_kernel).
+template <int kBlock, int kPPT, bool kDump>
+__device__ __forceinline__ void after_element(const TrackArgs &a, const ElemHeader &h, long base, int t, int e,
+                                              Particle (&p)[kPPT], PtCache (&c)[kPPT], bool (&alive)[kPPT],
+                                              int &nalive) {
+#pragma unroll
+  for (int k = 0; k < kPPT; k++) {
+    if (!alive[k]) continue;
+    const long i = base + (long)k * kBlock;
+    if (kDump) {
+      double *d = a.dump + (((size_t)i * a.nturn + t) * a.nelem + e) * 6;
+      d[0] = p[k].x; d[1] = p[k].px; d[2] = p[k].y; d[3] = p[k].py; d[4] = p[k].z; d[5] = p[k].pt;
+    }
+    if (needs_loss_check(h) && is_lost(p[k], h.apx, h.apy, a.r2)) {
+      store_particle(a, i, p[k]);
+      a.lost_turn[i] = a.turn0 + t;
+      a.lost_elem[i] = e;
+      alive[k] = false;
+      nalive--;
+      p[k] = Particle{0., 0., 0., 0., 0., 0.};
+      pt_refresh(a.ref, 0.0, c[k]);
+    }
+  }
+}
+
+// The segmented form of track_kernel (kSeg).  Step s of this CTA's sequence
+// tracks segment s % nseg from buffer s & 1; buffer b's mbarrier completes
+// once per staging, so its parity alternates with every use.
+template <int kBlock, int kPPT, bool kDump>
+__device__ void track_segmented(const TrackArgs &a, unsigned char *smem, uint64_t *sbar) {
+  const long chunk = (long)kBlock * kPPT;
+  const long stride = (long)gridDim.x * chunk;
+  const long first = (long)blockIdx.x * chunk;
+  const long my_chunks = first < a.n ? (a.n - first + stride - 1) / stride : 0;
+  const int nseg = a.nseg;
+  const long total = my_chunks * (long)a.nturn * nseg;
+  if (total == 0) return;
+  unsigned char *buf[2] = {smem, smem + a.seg_bytes};
+  if (threadIdx.x == 0) {
+    for (int b = 0; b < 2; b++) {
+      const uint32_t ba = (uint32_t)__cvta_generic_to_shared(&sbar[b]);
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(ba) : "memory");
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    issue_segment(a, a.segs[0], buf[0], &sbar[0]);
+    if (total > 1) issue_segment(a, a.segs[1 % nseg], buf[1], &sbar[1]);
+  }
+  uint32_t phase[2] = {0u, 0u};
+  long step = 0;
+  const RefConsts &R = a.ref;
+  for (long base = first + threadIdx.x; step < total; base += stride) {
+    Particle p[kPPT];
+    PtCache c[kPPT];
+    bool alive[kPPT];
+    int nalive = load_particles<kBlock, kPPT>(a, base, p, c, alive);
+    for (int t = 0; t < a.nturn; t++) {
+      for (int k = 0; k < nseg; k++, step++) {
+        const int b = (int)(step & 1);
+        const bool ok = wait_phase(&sbar[b], phase[b]);
+        phase[b] ^= 1u;
+        if (!__syncthreads_and((int)ok)) {
+          // give the copies in flight a bounded time to land before the CTA exits
+          if (threadIdx.x == 0) {
+            atomicExch(a.status, STB_ETIMEOUT);
+            wait_phase(&sbar[b ^ 1], phase[b ^ 1]);
+          }
+          __syncthreads();
+          return;
+        }
+        const SegDesc sg = a.segs[k];
+        const ElemHeader *hs = reinterpret_cast<const ElemHeader *>(buf[b]);
+        const double *ps = reinterpret_cast<const double *>(buf[b] + (size_t)sg.ne * sizeof(ElemHeader));
+        if (nalive > 0) {
+          for (int j = 0; j < sg.ne; j++) {
+            const ElemHeader h = hs[j];
+            apply_element<kPPT>(h, ps + (h.poff - sg.pool_lo), p, c, R);
+            after_element<kBlock, kPPT, kDump>(a, h, base, t, sg.e0 + j, p, c, alive, nalive);
+            if (nalive == 0) break;
+          }
+        }
+        __syncthreads();  // every thread is done with buffer b
+        if (threadIdx.x == 0 && step + 2 < total) issue_segment(a, a.segs[(step + 2) % nseg], buf[b], &sbar[b]);
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < kPPT; k++)
+      if (alive[k]) store_particle(a, base + (long)k * kBlock, p[k]);
+  }
+}
+
 // kPPT particles per thread: particle base + k*kBlock for k < kPPT, so every
 // load and store of a warp stays coalesced.  A particle that is lost has its
 // coordinates and loss record stored at once; its slot is then reset to the
 // reference orbit so the remaining particles of the thread keep running on
 // benign operands.
-template <bool kSmem, int kBlock, int kMinBlocks, int kPPT, bool kDump, bool kPF = false>
+//
+// kSeg (with kSmem): the table is staged segment by segment into two
+// shared-memory buffers, the next segment's bulk copy running while the
+// current one is tracked.  The whole CTA walks the same sequence of
+// (particle chunk, turn, segment) steps in lockstep: a barrier after every
+// segment frees its buffer for the copy two steps ahead.  Threads whose
+// particles are lost (or that have none) keep taking part in the barriers.
+template <bool kSmem, int kBlock, int kMinBlocks, int kPPT, bool kDump, bool kPF = false, bool kSeg = false>
 __global__ void __launch_bounds__(kBlock, kMinBlocks) track_kernel(const __grid_constant__ TrackArgs a) {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ __align__(8) uint64_t bar;
+  __shared__ __align__(8) uint64_t sbar[2];
   const ElemHeader *hdr = a.hdr;
   const double *pool = a.pool;
+  if (kSeg) {
+    track_segmented<kBlock, kPPT, kDump>(a, smem, sbar);
+    return;
+  }
   if (kSmem) {
     if (!stage_table(a, smem, &bar)) {
       if (threadIdx.x == 0) atomicExch(a.status, STB_ETIMEOUT);

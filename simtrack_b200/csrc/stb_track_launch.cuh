@@ -14,9 +14,9 @@ namespace {
 
 // Persistent grid: as many CTAs as fit on the device at once (never more
 // than the particles need); each CTA strides over the particle range.
-template <bool kSmem, int kBlock, int kMinBlocks, int kPPT, bool kDump, bool kPF = false>
+template <bool kSmem, int kBlock, int kMinBlocks, int kPPT, bool kDump, bool kPF = false, bool kSeg = false>
 cudaError_t launch_variant(const TrackArgs &a, int num_sms, size_t smem, cudaStream_t stream) {
-  auto kern = track_kernel<kSmem, kBlock, kMinBlocks, kPPT, kDump, kPF>;
+  auto kern = track_kernel<kSmem, kBlock, kMinBlocks, kPPT, kDump, kPF, kSeg>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   int per_sm = 0;
@@ -33,8 +33,14 @@ cudaError_t launch_variant(const TrackArgs &a, int num_sms, size_t smem, cudaStr
 
 cudaError_t launch_track_variants(const TrackArgs &a, int num_sms, int variant, cudaStream_t stream) {
   const size_t sm = track_smem_bytes(a.nelem, a.npool_padded);
+  const size_t sg = 2 * (size_t)a.seg_bytes;  // two segment buffers
+  const bool seg_ok = a.segs != nullptr && a.nseg > 0 && a.seg_bytes > 0;
+  if (kVariants[variant < 0 || variant >= kNumTrackVariants ? 0 : variant].seg && !seg_ok)
+    return cudaErrorInvalidValue;
   if (a.dump) {
-    // Per-element probe (diagnostics and parity tests): small particle counts only.
+    // Per-element probe (diagnostics and parity tests): small particle counts
+    // only; through the segment buffers when the table is tracked that way.
+    if (seg_ok && kVariants[variant].seg) return launch_variant<true, 256, 1, 1, true, false, true>(a, num_sms, sg, stream);
     return launch_variant<false, 256, 1, 1, true>(a, num_sms, 0, stream);
   }
   switch (variant) {
@@ -49,6 +55,9 @@ cudaError_t launch_track_variants(const TrackArgs &a, int num_sms, int variant, 
     case 8: return launch_variant<false, 128, 3, 2, false>(a, num_sms, 0, stream);
     case 9: return launch_variant<true, 1024, 1, 1, false, true>(a, num_sms, sm, stream);
     case 10: return launch_variant<true, 768, 1, 1, false, true>(a, num_sms, sm, stream);
+    case 11: return launch_variant<true, 1024, 1, 1, false, false, true>(a, num_sms, sg, stream);
+    case 12: return launch_variant<true, 768, 1, 1, false, false, true>(a, num_sms, sg, stream);
+    case 13: return launch_variant<true, 512, 1, 1, false, false, true>(a, num_sms, sg, stream);
     default: return cudaErrorInvalidValue;
   }
 }

@@ -6,7 +6,7 @@ reference source in place).  For each fixture lattice it records, per
 particle, Track()'s loss outputs and the six coordinates after every element
 for a few sampled turns, as produced by the reference's own element Pass
 functions.  The fixtures let the C restatement be pinned on machines where
-the reference cannot be built.  It also copies the reference's Example2 HSR
+the reference cannot be built.  It also copies the reference's Example1 RHIC lattice and its Example2 HSR
 lattice table and its printed closed orbit (compressed) and records the
 reference's closed orbit for that table.
 
@@ -72,6 +72,10 @@ TUNE_WINDOWS = [(0.2, 0.45, False), (0.0, 0.5, False), (0.0, 1.0, True)]
 # closed orbit the reference printed for it (Print_Orbit after Cal_Optics).
 _REF = oracle_bridge.ref_source_dir()
 EXAMPLE2 = _REF / "Example2" if _REF else Path("/nonexistent")
+# The reference's Example1 RHIC lattice (MAD-X TFS, 6,858 elements), the
+# table too large for one shared-memory copy that the segmented-staging tests
+# track on the GPU.
+EXAMPLE1 = _REF / "Example1" if _REF else Path("/nonexistent")
 HSR_ENERGY = (275000. / 938.27201, 938.27201, 1.0, 1.0)  # Set_RefPartEnergy, Example2/DA_cal.cpp:613
 
 
@@ -110,9 +114,19 @@ def hsr_fixtures(ref) -> None:
     print("wrote hsr fixtures")
 
 
+def rhic_example1_fixture() -> None:
+    import lzma
+    (HERE / "rhic_example1.tfs.xz").write_bytes(lzma.compress((EXAMPLE1 / "parameters_input").read_bytes(), preset=9))
+    print("wrote rhic_example1.tfs.xz")
+
+
 def main():
     from oracle_bridge import RefOracle
+    if len(sys.argv) > 1 and sys.argv[1] == "rhic_example1":
+        rhic_example1_fixture()
+        return
     ref = RefOracle()
+    rhic_example1_fixture()
     hsr_fixtures(ref)
     xs, pxs = tune_signals()
     tunes = np.array([[ref.fine_tune(x, px if w else None, lo, hi) for lo, hi, w in TUNE_WINDOWS]
