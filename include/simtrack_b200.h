@@ -454,6 +454,13 @@ int stb_math_eval(int fn, const double *in, double *out, long n, int device);
  * FMA chains per thread on every SM; the roofline denominator of the tracking kernel). */
 int stb_fp64_peak(int device, double *tflops);
 
+/* Diagnostics: the drift's square root, reciprocal and quotients as the
+ * tracking kernels compute them (from the cached reciprocal of 1+delta, no
+ * IEEE division or sqrt sequence) against IEEE sqrt and division, over n
+ * random drift arguments drawn from `seed`, on GPU `device` or on the host
+ * (device < 0).  mismatch4 receives the counts for pz, 1/pz, betaz, L/betaz. */
+int stb_check_drift_quotients(long n, unsigned long long seed, int device, unsigned long long *mismatch4);
+
 #ifdef __cplusplus
 }
 #endif

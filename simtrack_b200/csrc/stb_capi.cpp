@@ -1105,6 +1105,19 @@ int stb_fp64_peak(int device, double *tflops) {
   });
 }
 
+int stb_check_drift_quotients(long n, unsigned long long seed, int device, unsigned long long *mismatch4) {
+  return guarded([&] {
+    if (!mismatch4 || n < 0) throw Error(STB_EINVAL, "bad arguments");
+    if (device >= 0) {
+      DeviceGuard g(device);
+      cuda_check(drift_quotient_check(n, seed, device, mismatch4), "drift quotient check");
+    } else {
+      cuda_check(drift_quotient_check(n, seed, -1, mismatch4), "drift quotient check");
+    }
+    return STB_OK;
+  });
+}
+
 int stb_math_eval(int fn, const double *in, double *out, long n, int device) {
   return guarded([&] {
     if (!math_fn_valid(fn)) throw Error(STB_EINVAL, "unknown function code");

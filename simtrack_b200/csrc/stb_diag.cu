@@ -52,7 +52,75 @@ __global__ void dfma_peak_kernel(double *out, int iters, double a, double b) {
   if (s == 12345.678) out[blockIdx.x] = s;
 }
 
+// splitmix64: the i-th draw of a seeded stream, the same on host and device.
+__host__ __device__ inline uint64_t mix64(uint64_t z) {
+  z += 0x9e3779b97f4a7c15ull;
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+  return z ^ (z >> 31);
+}
+__host__ __device__ inline double unif(uint64_t seed, uint64_t i, int k) {
+  return (double)(mix64(seed ^ (i * 8 + (uint64_t)k) * 0x2545f4914f6cdd1dull) >> 11) * (1.0 / 9007199254740992.0);
+}
+
+// Random drift arguments (a proton beam at gamma 106.6: pt up to 2e-3, slopes
+// up to 7e-3 with a logarithmic spread down to 7e-7 and every 64th sample up
+// to 0.05, lengths 0.01-6 m) and the number of drift quotients
+// (drift_quotients) that differ from the IEEE results: pz, 1/pz, betaz,
+// L/betaz.
+__host__ __device__ inline void drift_check_one(uint64_t seed, uint64_t i, unsigned long long *bad) {
+  const double beta = 0.99995598, gamma = 106.58, sg = sqrt(gamma * gamma - 1.);
+  const double pt = (2 * unif(seed, i, 0) - 1) * 2e-3 * pow(10.0, -3 * unif(seed, i, 1));
+  const double smax = (i % 64 == 63) ? 0.05 : kSeedSlope;
+  const double px = (2 * unif(seed, i, 2) - 1) * smax * pow(10.0, -4 * unif(seed, i, 3));
+  const double py = (2 * unif(seed, i, 4) - 1) * smax * pow(10.0, -4 * unif(seed, i, 5));
+  const double L = 0.01 + 6 * unif(seed, i, 6);
+  const double delta1 = sqrt(1.0 + 2 * pt / beta + pt * pt) - 1.0;
+  const double gamma1 = gamma + sg * pt;
+  const double beta1 = sqrt(1.0 - 1.0 / gamma1 / gamma1);
+  const double opd = 1.0 + delta1, opd2 = opd * opd, iopd = 1.0 / opd, ibeta1 = 1.0 / beta1;
+  double pz, ipz, betaz, lb;
+  drift_quotients(opd, opd2, beta1, iopd, ibeta1, px, py, L, pz, ipz, betaz, lb);
+  const double rpz = sqrt(opd2 - px * px - py * py);
+  const double ripz = 1.0 / rpz;
+  const double rbetaz = mul_rn(rpz, beta1) / opd;
+  const double rlb = L / rbetaz;
+  if (pz != rpz) bad[0]++;
+  if (ipz != ripz) bad[1]++;
+  if (betaz != rbetaz) bad[2]++;
+  if (lb != rlb) bad[3]++;
+}
+
+__global__ void drift_check_kernel(uint64_t seed, long n, unsigned long long *bad) {
+  unsigned long long loc[4] = {0, 0, 0, 0};
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+    drift_check_one(seed, (uint64_t)i, loc);
+  for (int k = 0; k < 4; k++)
+    if (loc[k]) atomicAdd(bad + k, loc[k]);
+}
+
 }  // namespace
+
+// Mismatch counts of the drift quotients against IEEE sqrt and division over
+// n random drift arguments, on `device` (or the host for device < 0).
+cudaError_t drift_quotient_check(long n, unsigned long long seed, int device, unsigned long long *bad4) {
+  for (int k = 0; k < 4; k++) bad4[k] = 0;
+  if (device < 0) {
+    for (long i = 0; i < n; i++) drift_check_one(seed, (uint64_t)i, bad4);
+    return cudaSuccess;
+  }
+  unsigned long long *d = nullptr;
+  cudaError_t e = cudaMalloc(&d, 4 * sizeof(unsigned long long));
+  if (e != cudaSuccess) return e;
+  cudaMemset(d, 0, 4 * sizeof(unsigned long long));
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  drift_check_kernel<<<sms * 8, 256>>>(seed, n, d);
+  e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpy(bad4, d, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  return e;
+}
 
 // Measured FP64 FMA peak of `device` in TFLOP/s (2 flops per FMA).
 cudaError_t fp64_peak_probe(int device, double *tflops) {

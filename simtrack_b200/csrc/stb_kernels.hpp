@@ -81,6 +81,7 @@ bool math_fn_valid(int fn);
 cudaError_t math_eval_device(int fn, const double *d_in, double *d_out, long n, cudaStream_t s);
 void math_eval_host(int fn, const double *in, double *out, long n);
 cudaError_t fp64_peak_probe(int device, double *tflops);
+cudaError_t drift_quotient_check(long n, unsigned long long seed, int device, unsigned long long *bad4);
 
 size_t track_smem_bytes(int nelem, int npool_padded);
 // Consecutive segments of at most `budget` bytes of staged table (headers plus

@@ -62,16 +62,87 @@ __device__ __forceinline__ void pt_refresh(const RefConsts &R, double pt, PtCach
   c.ibeta1 = 1.0 / c.beta1;
 }
 
+// Square root and reciprocal of a drift from the cached seed.  With
+// v = (1+delta1)^2 - px^2 - py^2 and y0 = RN(1/(1+delta1)), y0 is within
+// (px^2 + py^2) / (2 (1+delta1)^2) <= 5e-5 relative of 1/sqrt(v) when |px|
+// and |py| are below kSeedSlope.  Two Newton steps for the reciprocal square
+// root in FMA form, y <- y + (y/2)(1 - v y^2), bring y within about an ulp;
+// the square root s = RN(v y) is then corrected once with its exact remainder,
+// s + (v - s^2) y/2 (Markstein's square-root step, IBM J. Res. Dev. 34 (1990)
+// 111), and the reciprocal once with its remainder, y + y (1 - s y).  Both
+// are the correctly rounded values unless the exact one lies within about
+// 2^-50 ulp of a rounding midpoint (the same order as qdiv above); they are
+// checked against IEEE sqrt and division on random drift arguments on the
+// host and on the GPU.  Steeper slopes return false: the caller then takes
+// IEEE sqrt and division.  14 FP64 operations and no MUFU, where sqrt and a
+// reciprocal cost two MUFU seeds and two Newton sequences with range checks.
+constexpr double kSeedSlope = 7e-3;
+
+__host__ __device__ __forceinline__ double mul_rn(double a, double b) {
+#ifdef __CUDA_ARCH__
+  return __dmul_rn(a, b);  // never contracted into an FMA, whatever the unit's flags
+#else
+  return a * b;
+#endif
+}
+
+__host__ __device__ __forceinline__ bool seeded_sqrt_recip(double v, double y0, double px, double py, double &s,
+                                                           double &is) {
+  if (!(fabs(px) < kSeedSlope && fabs(py) < kSeedSlope)) return false;
+  double y = y0;
+#pragma unroll
+  for (int k = 0; k < 2; k++) {
+    const double t = mul_rn(v, y);
+    const double e = fma(-t, y, 1.0);
+    y = fma(mul_rn(0.5, y), e, y);
+  }
+  const double s0 = mul_rn(v, y);
+  const double d = fma(-s0, s0, v);
+  s = fma(d, mul_rn(0.5, y), s0);
+  is = fma(y, fma(-s, y, 1.0), y);
+  return true;
+}
+
+// a / b with y within a few ulp of 1/b (here a product of correctly rounded
+// reciprocals): q0 = RN(a y) and one correction with the exact remainder,
+// correctly rounded unless a/b lies within about 2^-48 ulp of a rounding
+// midpoint.
+__host__ __device__ __forceinline__ double qdiv_near(double a, double b, double y) {
+  const double q0 = mul_rn(a, y);
+  const double r = fma(-q0, b, a);
+  return fma(r, y, q0);
+}
+
+// The divisions and square root of DRIFT_Pass's exact branch: pz =
+// sqrt((1+delta1)^2 - px^2 - py^2), 1/pz, betaz = pz*beta1/(1+delta1) and
+// L/betaz.  The reciprocal of betaz is (1+delta1) * (1/pz) * (1/beta1) from
+// the cached reciprocals, within ~2.5 ulp.
+__host__ __device__ __forceinline__ void drift_quotients(double opd, double opd2, double beta1, double iopd,
+                                                         double ibeta1, double px, double py, double L, double &pz,
+                                                         double &ipz, double &betaz, double &L_betaz) {
+  const double v = opd2 - px * px - py * py;
+  if (seeded_sqrt_recip(v, iopd, px, py, pz, ipz)) {
+    const double t = mul_rn(pz, beta1);
+    betaz = qdiv_near(t, opd, iopd);
+    L_betaz = qdiv_near(L, betaz, mul_rn(mul_rn(opd, ipz), ibeta1));
+  } else {
+    pz = sqrt(v);
+    ipz = 1.0 / pz;
+    const double t = mul_rn(pz, beta1);
+    betaz = qdiv_near(t, opd, iopd);
+    L_betaz = L / betaz;
+  }
+}
+
 // DRIFT_Pass exact branch, simtrack.cpp:3759-3764.  L and Lb = L/GP.beta.
 // The two quotients by pz share one reciprocal; (pz*beta1)/(1+delta1) uses
 // the cached reciprocal of 1+delta1.
 __device__ __forceinline__ void drift(Particle &p, const PtCache &c, double L, double Lb) {
-  const double pz = sqrt(c.opd2 - p.px * p.px - p.py * p.py);
-  const double ipz = 1.0 / pz;
-  const double betaz = qdiv(pz * c.beta1, c.opd, c.iopd);
+  double pz, ipz, betaz, L_betaz;
+  drift_quotients(c.opd, c.opd2, c.beta1, c.iopd, c.ibeta1, p.px, p.py, L, pz, ipz, betaz, L_betaz);
   p.x = p.x + qdiv(p.px * L, pz, ipz);
   p.y = p.y + qdiv(p.py * L, pz, ipz);
-  p.z = p.z - (L / betaz - Lb);
+  p.z = p.z - (L_betaz - Lb);
 }
 
 // sbend_exact_pass, simtrack.cpp:3833-3858.  B = [L, L/beta, href, 1/href, cosA, sinA].

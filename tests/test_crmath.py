@@ -185,3 +185,25 @@ def test_shared_reciprocal_quotient_equals_ieee_division(native_lib):
     q = ev(native_lib, 5, ab, 0)
     assert np.array_equal(q, a / b)
     assert np.array_equal(ev(native_lib, 15, ab, 0), a / b)
+
+
+def _drift_check(native_lib, n, seed, device):
+    from ctypes import c_ulonglong
+    bad = (c_ulonglong * 4)()
+    assert native_lib.stb_check_drift_quotients(n, seed, device, bad) == 0
+    return list(bad)
+
+
+def test_drift_quotients_equal_ieee_on_the_host(native_lib):
+    """The drift's seeded square root and reciprocal and its quotients
+    (stb_physics.cuh drift_quotients), built for the host, against IEEE sqrt
+    and division on 4e6 random drift arguments."""
+    assert _drift_check(native_lib, 4_000_000, 2024, -1) == [0, 0, 0, 0]
+
+
+@pytest.mark.gpu
+def test_drift_quotients_equal_ieee_on_the_gpu(native_lib):
+    """The same on the GPU over 2e9 random drift arguments (device code,
+    -fmad=false unit)."""
+    for seed in (1, 2):
+        assert _drift_check(native_lib, 1_000_000_000, seed, 0) == [0, 0, 0, 0]
