@@ -156,8 +156,11 @@ __device__ __forceinline__ void bend_exact(Particle &p, const PtCache &c, const 
   const double pz1 = sqrt(c.opd2 - npx * npx - py0 * py0);
   const double der = (-px0) * sinA * href + (pz0 - 1. - x0 * href) * cosA * href;
   p.x = qdiv(pz1, href, invh) - qdiv(qdiv(der, href, invh), href, invh) - invh;
-  const double temp = sqrt(c.opd2 - py0 * py0);
-  const double itemp = 1.0 / temp;
+  double temp, itemp;
+  if (!seeded_sqrt_recip(c.opd2 - py0 * py0, c.iopd, 0.0, py0, temp, itemp)) {
+    temp = sqrt(c.opd2 - py0 * py0);
+    itemp = 1.0 / temp;
+  }
   const double as1 = cr_asin(qdiv(px0, temp, itemp));
   const double as2 = cr_asin(qdiv(npx, temp, itemp));
   const double das = as1 - as2;

@@ -44,12 +44,24 @@ __device__ __noinline__ void spin_rotate(const Particle &x0, const PtCache &c, c
   if (!(B0 * B0 + B1 * B1 + B2 * B2 != 0.)) return;
   const double gamma1 = R.gamma + R.sqrt_g2m1 * x0.pt;
   const double Gr = R.G * gamma1;
-  double temp = sqrt(c.opd2 - x0.px * x0.px - x0.py * x0.py);
-  double u0 = x0.px / temp, u1 = x0.py / temp, u2 = 1.0;
-  temp = sqrt(u0 * u0 + u1 * u1 + u2 * u2);
-  u0 = u0 / temp;
-  u1 = u1 / temp;
-  u2 = u2 / temp;
+  // Quotients by a shared divisor use its reciprocal and the one-FMA
+  // correction (qdiv); the square roots and their reciprocals come from
+  // seeds close to them (1/(1+delta) for the longitudinal momentum, 1 for
+  // the norm of (px/pz, py/pz, 1)), IEEE sqrt and division for steep slopes.
+  double temp, itemp;
+  if (!seeded_sqrt_recip(c.opd2 - x0.px * x0.px - x0.py * x0.py, c.iopd, x0.px, x0.py, temp, itemp)) {
+    temp = sqrt(c.opd2 - x0.px * x0.px - x0.py * x0.py);
+    itemp = 1.0 / temp;
+  }
+  double u0 = qdiv(x0.px, temp, itemp), u1 = qdiv(x0.py, temp, itemp), u2 = 1.0;
+  double itemp2;
+  if (!seeded_sqrt_recip(u0 * u0 + u1 * u1 + u2 * u2, 1.0, u0, u1, temp, itemp2)) {
+    temp = sqrt(u0 * u0 + u1 * u1 + u2 * u2);
+    itemp2 = 1.0 / temp;
+  }
+  u0 = qdiv(u0, temp, itemp2);
+  u1 = qdiv(u1, temp, itemp2);
+  u2 = qdiv(u2, temp, itemp2);
   temp = (1 + href * x0.x) * temp;
   const double udotB = u0 * B0 + u1 * B1 + u2 * B2;
   const double g1 = 1 + Gr, g2 = R.G * (1 - gamma1);
@@ -61,7 +73,8 @@ __device__ __noinline__ void spin_rotate(const Particle &x0, const PtCache &c, c
   F2 = qdiv(F2 * temp, c.opd, c.iopd);
   F1 = F1 - angle;
   const double Fabs = sqrt(F0 * F0 + F1 * F1 + F2 * F2);
-  const double a0 = F0 / Fabs, a1 = F1 / Fabs, a2 = F2 / Fabs;
+  const double iFabs = 1.0 / Fabs;
+  const double a0 = qdiv(F0, Fabs, iFabs), a1 = qdiv(F1, Fabs, iFabs), a2 = qdiv(F2, Fabs, iFabs);
   const double theta = -Fabs;
   double st, ct;
   cr_sincos(theta, st, ct);
