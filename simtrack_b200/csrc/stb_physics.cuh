@@ -205,8 +205,9 @@ __device__ __forceinline__ void quad_kick(Particle &p, double kl, double ksl) {
 __device__ __forceinline__ void sext_kick(Particle &p, double kl, double ksl) {
   const double pr = p.x * p.x - p.y * p.y;
   const double pi = 2. * p.x * p.y;
-  const double Bx = (ksl * pr + kl * pi) / 2.;
-  const double By = (kl * pr - ksl * pi) / 2.;
+  // x / 2. and x * 0.5 are the same exact scaling (also for subnormal results)
+  const double Bx = (ksl * pr + kl * pi) * 0.5;
+  const double By = (kl * pr - ksl * pi) * 0.5;
   p.px = p.px - By;
   p.py = p.py + Bx;
 }
@@ -359,7 +360,7 @@ __device__ __forceinline__ void bb4d(double x, double y, double c4, double sigma
     Dpy = temp1 * y * temp2;
   } else if (sigmax > sigmay) {
     const double temp1 = c4 * sqrt(PI / 2. / (sigmax * sigmax - sigmay * sigmay));
-    const double temp2 = cr_exp(-x * x / 2. / sigmax / sigmax - y * y / 2. / sigmay / sigmay);
+    const double temp2 = cr_exp(-x * x * 0.5 / sigmax / sigmax - y * y * 0.5 / sigmay / sigmay);
     const double temp3 = sqrt(2. * (sigmax * sigmax - sigmay * sigmay));
     double w1r, w1i, w2r, w2i;
     const double x1 = fabs(x) / temp3, y1 = fabs(y) / temp3;
@@ -396,7 +397,7 @@ static __device__ __noinline__ void bb6d(Particle &p, const double *P, int nslic
   const double *zs = P + 13;
   for (int i = 0; i < nslice; i++) {
     const Particle q = p;
-    const double S = (q.z - zs[i]) / 2.0;
+    const double S = (q.z - zs[i]) * 0.5;
     const double betax = betax_s + 2 * S * alfx_s + S * S * gx;
     const double betay = betay_s + 2 * S * alfy_s + S * S * gy;
     const double sigmax = sqrt(emitx * betax);
@@ -409,7 +410,7 @@ static __device__ __noinline__ void bb6d(Particle &p, const double *P, int nslic
     bb4d(X, Y, c4, sigmax, sigmay, Dpx, Dpy);
     const double temp1 = 1.0 / 2. / (sigmax * sigmax - sigmay * sigmay);
     const double temp2 = X * Dpx + Y * Dpy;
-    const double temp4 = cr_exp(-X * X / 2. / sigmax / sigmax - Y * Y / 2. / sigmay / sigmay);
+    const double temp4 = cr_exp(-X * X * 0.5 / sigmax / sigmax - Y * Y * 0.5 / sigmay / sigmay);
     p.x = q.x - S * Dpx * bbscale;
     p.px = q.px + Dpx * bbscale;
     p.y = q.y - S * Dpy * bbscale;
