@@ -220,8 +220,8 @@ class Line:
             pass
 
 
-NUM_VARIANTS = 14
-NUM_SCAN_VARIANTS = 7
+NUM_VARIANTS = 16
+NUM_SCAN_VARIANTS = 9
 
 
 def _check_device_arrays(coords, lost_turn, lost_elem, n: int, device: int, ncoord: int = 6) -> None:
@@ -658,8 +658,8 @@ class Scan:
     def autotune(self, nturn: int = 16) -> dict:
         """Picks the fastest tracking-kernel variant on a snapshot of the current state."""
         ch = c_int()
-        t = (c_double * 8)()
-        check(lib().stb_scan_autotune(self._h, nturn, byref(ch), t, 8))
+        t = (c_double * 16)()
+        check(lib().stb_scan_autotune(self._h, nturn, byref(ch), t, 16))
         return {"chosen": ch.value, "ms": [t[i] for i in range(NUM_SCAN_VARIANTS)]}
 
     def run(self, nturn: int, turns_per_block: int = 256, use_graph: bool = True) -> None:

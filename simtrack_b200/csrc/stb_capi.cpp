@@ -217,9 +217,13 @@ int autotune(stb_table *t, const double *const *in, int nc, long n, int nturn, d
   const size_t seg_full = (size_t)track_smem_limit(t->device) / 2 & ~size_t(15);
   const size_t seg_budgets[2] = {seg_full, seg_full / 2 & ~size_t(15)};
   size_t best_seg = (size_t)t->seg_bytes;
-  for (int vv = 0; vv < nvar + (t->nseg > 0 ? 3 : 0); vv++) {
+  int seg_list[kNumTrackVariants], nseg_v = 0;
+  if (!t->host.spin && t->nseg > 0)
+    for (int v = 0; v < kNumTrackVariants; v++)
+      if (kVariants[v].seg) seg_list[nseg_v++] = v;
+  for (int vv = 0; vv < nvar + nseg_v; vv++) {
     // vv >= nvar: the seg_* variants again with the smaller segment budget
-    const int v = vv < nvar ? vv : kNumTrackVariants - 3 + (vv - nvar);
+    const int v = vv < nvar ? vv : seg_list[vv - nvar];
     const bool seg_v = !t->host.spin && kVariants[v].seg;
     if (seg_v) set_segments(t, seg_budgets[vv < nvar ? 0 : 1]);
     float ms = -1.f;

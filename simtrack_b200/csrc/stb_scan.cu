@@ -305,7 +305,7 @@ cudaError_t prepare_scan_variant(int num_sms, size_t smem, int *grid) {
 const ScanVariant kScanVariants[kNumScanVariants] = {
     {true, 1024, 1, "smem_b1024_r64"}, {true, 512, 1, "smem_b512_r128"}, {false, 256, 4, "l1_b256_r64"},
     {false, 256, 3, "l1_b256_r80"},    {false, 128, 8, "l1_b128_r64"},    {false, 256, 2, "l1_b256_r128"},
-    {false, 128, 2, "l1_b128_r255"},
+    {false, 128, 2, "l1_b128_r255"},   {true, 256, 1, "smem_b256_r255"},  {true, 128, 1, "smem_b128_r255"},
 };
 
 cudaError_t prepare_scan(int variant, int num_sms, size_t smem, int *grid) {
@@ -317,6 +317,8 @@ cudaError_t prepare_scan(int variant, int num_sms, size_t smem, int *grid) {
     case 4: return prepare_scan_variant<false, 128, 8>(num_sms, 0, grid);
     case 5: return prepare_scan_variant<false, 256, 2>(num_sms, 0, grid);
     case 6: return prepare_scan_variant<false, 128, 2>(num_sms, 0, grid);
+    case 7: return prepare_scan_variant<true, 256, 1>(num_sms, smem, grid);
+    case 8: return prepare_scan_variant<true, 128, 1>(num_sms, smem, grid);
     default: return cudaErrorInvalidValue;
   }
 }
@@ -334,6 +336,8 @@ cudaError_t launch_scan_block(const ScanArgs &a, int variant, int grid, size_t s
     case 4: scan_track_kernel<false, 128, 8><<<grid, 128, 0, st>>>(a); break;
     case 5: scan_track_kernel<false, 256, 2><<<grid, 256, 0, st>>>(a); break;
     case 6: scan_track_kernel<false, 128, 2><<<grid, 128, 0, st>>>(a); break;
+    case 7: scan_track_kernel<true, 256, 1><<<grid, 256, smem, st>>>(a); break;
+    case 8: scan_track_kernel<true, 128, 1><<<grid, 128, smem, st>>>(a); break;
     default: return cudaErrorInvalidValue;
   }
   e = cudaGetLastError();

@@ -61,7 +61,7 @@ struct ScanVariant {
   int min_blocks;
   const char *name;
 };
-constexpr int kNumScanVariants = 7;
+constexpr int kNumScanVariants = 9;
 extern const ScanVariant kScanVariants[kNumScanVariants];
 
 // Sets the kernel attributes of a variant and returns its persistent grid size

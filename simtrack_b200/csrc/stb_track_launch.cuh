@@ -58,6 +58,8 @@ cudaError_t launch_track_variants(const TrackArgs &a, int num_sms, int variant, 
     case 11: return launch_variant<true, 1024, 1, 1, false, false, true>(a, num_sms, sg, stream);
     case 12: return launch_variant<true, 768, 1, 1, false, false, true>(a, num_sms, sg, stream);
     case 13: return launch_variant<true, 512, 1, 1, false, false, true>(a, num_sms, sg, stream);
+    case 14: return launch_variant<true, 256, 1, 1, false>(a, num_sms, sm, stream);
+    case 15: return launch_variant<true, 128, 1, 1, false>(a, num_sms, sm, stream);
     default: return cudaErrorInvalidValue;
   }
 }

@@ -7,7 +7,7 @@ import pytest
 
 from simtrack_b200 import lattices as lt
 from simtrack_b200._native import STB_EABORTED, STB_ETIMEOUT, SimTrackError
-from simtrack_b200.api import Scan, Table
+from simtrack_b200.api import NUM_SCAN_VARIANTS, Scan, Table
 
 pytestmark = pytest.mark.gpu
 
@@ -50,7 +50,7 @@ def test_scan_matches_single_table_tracking(use_graph):
 def test_scan_variants_agree():
     tabs, xs, lats = seed_setup(2, namp=12, nang=3)
     ref = None
-    for v in range(5):
+    for v in range(NUM_SCAN_VARIANTS):
         sc = Scan(tabs, xs, aperture_radius=0.03)
         try:
             sc.configure(variant=v, chunk=128)
