@@ -207,62 +207,127 @@ __device__ __forceinline__ void write_output(const ScanArgs &a, long slot, int l
   x[5] = a.pt[slot];
 }
 
-// One CTA per seed: stable in-place compaction of [off, off + live).  Each
-// pass reads one CTA-sized window into registers, ranks the live particles
-// with warp ballots and a block prefix sum, synchronises, then writes; a
-// destination never exceeds its source, and all reads of a window precede
-// its writes, so the in-place moves are safe.
-__global__ void __launch_bounds__(kCompactBlock) scan_compact_kernel(ScanArgs a) {
-  constexpr int kWarps = kCompactBlock / 32;
-  __shared__ int warp_off[kWarps];
-  __shared__ int window_total;
-  const int s = blockIdx.x;
+// Stable compaction of every seed's live slots [off, off + live) in three
+// passes over windows of kCompactWindow slots, one CTA per (window, seed), so
+// that it runs on every SM whatever the number of seeds:
+//   1. count:   the survivors of each window (a block-wide count); particles
+//               lost in this block get their outputs (indexed by original id);
+//   2. gather:  each window's survivors, ranked by warp ballots and a block
+//               prefix over warps, go to the staging arrays at the seed offset
+//               plus the survivors of the windows before it;
+//   3. back:    the seed's first `survivors` slots are copied back from the
+//               staging arrays and marked alive; the live count and the turn
+//               counter are updated.
+// Order within a seed is kept, so results equal those of tracking each seed
+// alone.
+__global__ void __launch_bounds__(kCompactBlock) compact_count_kernel(ScanArgs a) {
+  const int s = blockIdx.y, w = blockIdx.x;
   const ScanSeed sd = a.seeds[s];
   const int live = a.live[s];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  int base = 0;
-  for (int w0 = 0; w0 < live; w0 += kCompactBlock) {
-    const int j = w0 + threadIdx.x;
-    const bool in = j < live;
+  const int j = w * kCompactWindow + threadIdx.x;
+  bool keep = false;
+  if (j < live) {
     const long src = sd.off + j;
-    int lt = -1, idv = 0;
-    double v[6] = {0, 0, 0, 0, 0, 0};
-    if (in) {
-      lt = a.lost_turn[src];
-      idv = a.id[src];
-      v[0] = a.x[src]; v[1] = a.px[src]; v[2] = a.y[src];
-      v[3] = a.py[src]; v[4] = a.z[src]; v[5] = a.pt[src];
-      if (lt >= 0) write_output(a, src, lt, a.lost_elem[src]);
-    }
-    const bool keep = in && lt < 0;
-    const unsigned m = __ballot_sync(0xffffffffu, keep);
-    if (lane == 0) warp_off[warp] = __popc(m);
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      int acc = 0;
-      for (int w = 0; w < kWarps; w++) {
-        const int c = warp_off[w];
-        warp_off[w] = acc;
-        acc += c;
-      }
-      window_total = acc;
-    }
-    __syncthreads();
-    if (keep) {
-      const long dst = sd.off + base + warp_off[warp] + __popc(m & ((1u << lane) - 1u));
-      a.x[dst] = v[0]; a.px[dst] = v[1]; a.y[dst] = v[2];
-      a.py[dst] = v[3]; a.z[dst] = v[4]; a.pt[dst] = v[5];
-      a.id[dst] = idv;
-      a.lost_turn[dst] = -1;
-      a.lost_elem[dst] = 0;
-    }
-    base += window_total;
-    __syncthreads();
+    const int lt = a.lost_turn[src];
+    if (lt >= 0) write_output(a, src, lt, a.lost_elem[src]);
+    keep = lt < 0;
   }
+  const int c = __syncthreads_count(keep);
+  if (threadIdx.x == 0) a.win_count[s * a.nwin + w] = w * kCompactWindow < live ? c : 0;
+}
+
+// Sum of win_count[s][0, upto) by the whole block.
+__device__ __forceinline__ int windows_before(const ScanArgs &a, int s, int upto, int *red) {
+  int acc = 0;
+  for (int k = threadIdx.x; k < upto; k += kCompactBlock) acc += a.win_count[s * a.nwin + k];
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  int tot = 0;
+  for (int k = 0; k < kCompactBlock / 32; k++) tot += red[k];
+  __syncthreads();
+  return tot;
+}
+
+__global__ void __launch_bounds__(kCompactBlock) compact_gather_kernel(ScanArgs a) {
+  constexpr int kWarps = kCompactBlock / 32;
+  __shared__ int red[kWarps];
+  __shared__ int warp_off[kWarps];
+  const int s = blockIdx.y, w = blockIdx.x;
+  const ScanSeed sd = a.seeds[s];
+  const int live = a.live[s];
+  if (w * kCompactWindow >= live) return;
+  const int base = windows_before(a, s, w, red);
+  const int j = w * kCompactWindow + threadIdx.x;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const long src = sd.off + j;
+  const bool keep = j < live && a.lost_turn[src] < 0;
+  const unsigned m = __ballot_sync(0xffffffffu, keep);
+  if (lane == 0) warp_off[warp] = __popc(m);
+  __syncthreads();
   if (threadIdx.x == 0) {
-    a.live[s] = base;
+    int acc = 0;
+    for (int k = 0; k < kWarps; k++) {
+      const int c = warp_off[k];
+      warp_off[k] = acc;
+      acc += c;
+    }
+  }
+  __syncthreads();
+  if (keep) {
+    const long dst = sd.off + base + warp_off[warp] + __popc(m & ((1u << lane) - 1u));
+    const long n = a.ntot;
+    a.stage[dst] = a.x[src];
+    a.stage[n + dst] = a.px[src];
+    a.stage[2 * n + dst] = a.y[src];
+    a.stage[3 * n + dst] = a.py[src];
+    a.stage[4 * n + dst] = a.z[src];
+    a.stage[5 * n + dst] = a.pt[src];
+    a.stage_id[dst] = a.id[src];
+  }
+}
+
+__global__ void __launch_bounds__(kCompactBlock) compact_back_kernel(ScanArgs a) {
+  __shared__ int red[kCompactBlock / 32];
+  const int s = blockIdx.y, w = blockIdx.x;
+  const ScanSeed sd = a.seeds[s];
+  const int live = a.live[s];
+  if (w * kCompactWindow >= live) return;  // every block of this seed sees the old live count
+  const int total = windows_before(a, s, a.nwin, red);
+  const int j = w * kCompactWindow + threadIdx.x;
+  if (j < total) {
+    const long i = sd.off + j;
+    const long n = a.ntot;
+    a.x[i] = a.stage[i];
+    a.px[i] = a.stage[n + i];
+    a.y[i] = a.stage[2 * n + i];
+    a.py[i] = a.stage[3 * n + i];
+    a.z[i] = a.stage[4 * n + i];
+    a.pt[i] = a.stage[5 * n + i];
+    a.id[i] = a.stage_id[i];
+    a.lost_turn[i] = -1;
+    a.lost_elem[i] = 0;
+  }
+}
+
+// Live counts and the turn counter, after every window of every seed is back.
+__global__ void compact_finish_kernel(ScanArgs a) {
+  __shared__ int red[kCompactBlock / 32];
+  const int s = blockIdx.x;
+  const int total = windows_before(a, s, a.nwin, red);
+  if (threadIdx.x == 0) {
+    a.live[s] = total;
     if (s == 0 && *a.block_skipped == 0) *a.turn0 += a.nturn;
   }
+}
+
+cudaError_t launch_compaction(const ScanArgs &a, cudaStream_t st) {
+  const dim3 grid((unsigned)a.nwin, (unsigned)a.nseed);
+  compact_count_kernel<<<grid, kCompactBlock, 0, st>>>(a);
+  compact_gather_kernel<<<grid, kCompactBlock, 0, st>>>(a);
+  compact_back_kernel<<<grid, kCompactBlock, 0, st>>>(a);
+  compact_finish_kernel<<<a.nseed, kCompactBlock, 0, st>>>(a);
+  return cudaGetLastError();
 }
 
 __global__ void scan_retire_kernel(ScanArgs a, const uint8_t *mask) {
@@ -342,14 +407,10 @@ cudaError_t launch_scan_block(const ScanArgs &a, int variant, int grid, size_t s
   }
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  scan_compact_kernel<<<a.nseed, kCompactBlock, 0, st>>>(a);
-  return cudaGetLastError();
+  return launch_compaction(a, st);
 }
 
-cudaError_t launch_scan_compact_only(const ScanArgs &a, cudaStream_t st) {
-  scan_compact_kernel<<<a.nseed, kCompactBlock, 0, st>>>(a);
-  return cudaGetLastError();
-}
+cudaError_t launch_scan_compact_only(const ScanArgs &a, cudaStream_t st) { return launch_compaction(a, st); }
 
 cudaError_t launch_scan_track_only(const ScanArgs &a, int variant, int grid, size_t smem, cudaStream_t st) {
   scan_worklist_kernel<<<1, 1024, 0, st>>>(a);

@@ -50,7 +50,17 @@ struct ScanArgs {
   // device flag recording that the current block was skipped.
   const volatile int32_t *abort;
   int32_t *block_skipped;
+  // Compaction across many CTAs: windows of kCompactWindow slots per seed
+  // (nwin per seed), their live counts, and a staging copy of the slots
+  // (six coordinates, then the ids) the survivors are gathered into.
+  int nwin;
+  int32_t *win_count;  // [nseed * nwin]
+  double *stage;       // [6 * ntot]
+  int32_t *stage_id;   // [ntot]
 };
+
+// Slots per compaction window (one CTA each).
+constexpr int kCompactWindow = 1024;
 
 // Loss code written for particles removed by stb_scan_retire (never a turn).
 constexpr int32_t kRetiredCode = 0x40000000;

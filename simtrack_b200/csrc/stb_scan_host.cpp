@@ -47,6 +47,8 @@ struct stb_scan {
   double device_ms = 0.0;
   long blocks_run = 0;
   int32_t *h_abort = nullptr;  // mapped host flag read by every turn block (stb_scan_set_abort)
+  int32_t *d_win = nullptr;    // compaction: survivors per window
+  double *d_stage = nullptr;   // compaction: staging copy of the slots (6 coordinates + ids)
   double budget_s = 0.0;       // wall-clock budget of one stb_scan_run call (0: none)
 };
 
@@ -65,7 +67,7 @@ void scan_destroy(stb_scan *s) {
   if (s->stream) cudaStreamDestroy(s->stream);
   if (s->h_abort) cudaFreeHost(s->h_abort);
   for (void *p : {(void *)s->d_seeds, (void *)s->d_coords, (void *)s->d_i32, (void *)s->d_live, (void *)s->d_items,
-                  (void *)s->d_ctr, (void *)s->d_out_x, (void *)s->d_status})
+                  (void *)s->d_ctr, (void *)s->d_out_x, (void *)s->d_status, (void *)s->d_win, (void *)s->d_stage})
     if (p) cudaFree(p);
   if (prev >= 0) cudaSetDevice(prev);
   delete s;
@@ -125,6 +127,9 @@ stb_scan *scan_build(stb_table **tables, int nseed, const double *x0, const long
   cuda_check(cudaHostGetDevicePointer((void **)&d_abort, s->h_abort, 0), "abort flag mapping");
   cuda_check(cudaMalloc(&s->d_out_x, sizeof(double) * 6 * n), "cudaMalloc(outputs)");
   cuda_check(cudaMalloc(&s->d_status, sizeof(int)), "cudaMalloc(status)");
+  const int nwin = (int)std::max<long>(1, (s->max_per_seed + kCompactWindow - 1) / kCompactWindow);
+  cuda_check(cudaMalloc(&s->d_win, sizeof(int32_t) * (size_t)nseed * nwin), "cudaMalloc(compaction windows)");
+  cuda_check(cudaMalloc(&s->d_stage, (sizeof(double) * 6 + sizeof(int32_t)) * (size_t)n), "cudaMalloc(compaction staging)");
   // initial state: AoS host -> SoA device; id = original index; all alive
   std::vector<double> soa((size_t)6 * n);
   for (long i = 0; i < n; i++)
@@ -170,6 +175,10 @@ stb_scan *scan_build(stb_table **tables, int nseed, const double *x0, const long
   a.item_chunk = s->d_ctr + 3;
   a.block_skipped = s->d_ctr + 4;
   a.abort = d_abort;
+  a.nwin = nwin;
+  a.win_count = s->d_win;
+  a.stage = s->d_stage;
+  a.stage_id = reinterpret_cast<int32_t *>(s->d_stage + 6 * n);
   a.r2 = radius > 0.0 ? radius * radius : INFINITY;
   a.status = s->d_status;
   a.tbt = nullptr;
