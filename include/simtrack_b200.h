@@ -350,6 +350,13 @@ int stb_scan_retire(stb_scan *s, const uint8_t *mask);
  * intact.  While the flag is set every stb_scan_run returns STB_EABORTED at
  * once; stb_scan_set_abort(s, 0) re-arms the scan. */
 int stb_scan_set_abort(stb_scan *s, int value);
+/* Work-item packing (no reference counterpart): 0 spreads the live particles
+ * over every resident CTA in items down to one warp; 1 keeps every item at
+ * the full chunk, so a small population runs on few SMs with many warps each.
+ * stb_scan_autotune tries both with every launch variant and keeps the
+ * faster; stb_scan_packing reports the current choice. */
+int stb_scan_set_packing(stb_scan *s, int pack);
+int stb_scan_packing(const stb_scan *s, int *pack);
 /* Wall-clock budget of each stb_scan_run call in seconds (0: none), checked
  * between groups of turn blocks; when it is spent the call returns
  * STB_ETIMEOUT at a turn-block boundary with the state intact. */

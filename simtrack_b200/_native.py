@@ -122,6 +122,8 @@ SIGNATURES = [
                                  c_void_p]),
     ("stb_scan_retire", c_int, [c_void_p, c_void_p]),
     ("stb_scan_set_abort", c_int, [c_void_p, c_int]),
+    ("stb_scan_set_packing", c_int, [c_void_p, c_int]),
+    ("stb_scan_packing", c_int, [c_void_p, POINTER(c_int)]),
     ("stb_table_set_contraction", c_int, [c_void_p, c_int]),
     ("stb_table_set_segment_bytes", c_int, [c_void_p, c_long]),
     ("stb_table_segments", c_int, [c_void_p, POINTER(c_int), POINTER(c_int)]),

@@ -660,7 +660,7 @@ class Scan:
         ch = c_int()
         t = (c_double * 16)()
         check(lib().stb_scan_autotune(self._h, nturn, byref(ch), t, 16))
-        return {"chosen": ch.value, "ms": [t[i] for i in range(NUM_SCAN_VARIANTS)]}
+        return {"chosen": ch.value, "packed": self.packing(), "ms": [t[i] for i in range(NUM_SCAN_VARIANTS)]}
 
     def run(self, nturn: int, turns_per_block: int = 256, use_graph: bool = True) -> None:
         check(lib().stb_scan_run(self._h, nturn, turns_per_block, int(use_graph)))
@@ -692,6 +692,14 @@ class Scan:
         if m.size != self.n:
             raise SimTrackError(-1, "mask must have one entry per particle")
         check(lib().stb_scan_retire(self._h, c_void_p(m.ctypes.data)))
+
+    def set_packing(self, pack: bool) -> None:
+        check(lib().stb_scan_set_packing(self._h, int(bool(pack))))
+
+    def packing(self) -> bool:
+        v = c_int()
+        check(lib().stb_scan_packing(self._h, byref(v)))
+        return bool(v.value)
 
     def set_abort(self, value: bool = True) -> None:
         """Asks a run in progress (in another thread) to stop at the next turn

@@ -37,7 +37,10 @@ constexpr int kCompactBlock = 1024;
 
 // Work-item size adapts to the live population: with few survivors the items
 // shrink (down to one warp) so that they still spread over every resident
-// CTA; with many they grow up to the configured chunk.
+// CTA; with many they grow up to the configured chunk.  In packed mode the
+// items keep the full chunk, so a small population occupies few SMs with many
+// warps each: latency-bound tails run faster that way when warps that walk
+// the same element sequence share their SM's instruction fetches.
 __global__ void scan_worklist_kernel(ScanArgs a) {
   __shared__ int pre[kMaxScanSeeds + 1];
   __shared__ int chunk_s;
@@ -73,7 +76,7 @@ __global__ void scan_worklist_kernel(ScanArgs a) {
     long c = (total + a.grid - 1) / (a.grid > 0 ? a.grid : 1);
     c = ((c + 31) / 32) * 32;
     if (c < 32) c = 32;
-    if (c > a.chunk) c = a.chunk;
+    if (c > a.chunk || a.pack) c = a.chunk;
     chunk_s = (int)c;
   }
   __syncthreads();

@@ -25,6 +25,7 @@ struct ScanArgs {
   const ScanSeed *seeds;
   int nseed;
   int chunk;  // largest work item (particles); the work list may use smaller ones
+  int pack;   // nonzero: items always hold `chunk` particles (few CTAs busy, many warps each)
   int grid;   // resident CTAs of the tracking kernel
   RefConsts ref;
   double *x, *px, *y, *py, *z, *pt;  // flat slot arrays

@@ -31,6 +31,7 @@ struct stb_scan {
   int variant = 2;
   int grid = 0;  // persistent grid of the current variant
   int chunk = 1024;
+  int pack = 0;  // packed work items (see scan_worklist_kernel), chosen by the autotuner
   stb::ScanArgs args{};
   // device buffers
   stb::ScanSeed *d_seeds = nullptr;
@@ -42,7 +43,7 @@ struct stb_scan {
   long max_items = 0;
   cudaStream_t stream = nullptr;
   cudaGraphExec_t graph = nullptr;
-  int graph_blocks = 0, graph_tpb = 0, graph_variant = -1, graph_chunk = -1;
+  int graph_blocks = 0, graph_tpb = 0, graph_variant = -1, graph_chunk = -1, graph_pack = -1;
   int turns_done = 0;
   double device_ms = 0.0;
   long blocks_run = 0;
@@ -216,7 +217,7 @@ void run_blocks_direct(stb_scan *s, int nblocks, int tpb) {
 
 void ensure_graph(stb_scan *s, int blocks, int tpb) {
   if (s->graph && s->graph_blocks == blocks && s->graph_tpb == tpb && s->graph_variant == s->variant &&
-      s->graph_chunk == s->chunk)
+      s->graph_chunk == s->chunk && s->graph_pack == s->pack)
     return;
   if (s->graph) {
     cudaGraphExecDestroy(s->graph);
@@ -238,6 +239,7 @@ void ensure_graph(stb_scan *s, int blocks, int tpb) {
   s->graph_tpb = tpb;
   s->graph_variant = s->variant;
   s->graph_chunk = s->chunk;
+  s->graph_pack = s->pack;
 }
 
 int32_t device_turn(stb_scan *s) {
@@ -442,9 +444,11 @@ int scan_autotune(stb_scan *s, int nturn, double *timings, int ntimings) {
   cuda_check(cudaEventCreate(&e0), "event");
   cuda_check(cudaEventCreate(&e1), "event");
   const int saved_v = s->variant, saved_grid = s->grid;
-  int best = -1;
+  int best = -1, best_pack = 0;
   float best_ms = 0.f;
-  for (int v = 0; v < kNumScanVariants; v++) {
+  for (int vv = 0; vv < 2 * kNumScanVariants; vv++) {
+    // every variant with spread and with packed work items
+    const int v = vv >> 1, pack = vv & 1;
     float ms = -1.f;
     int grid = 0;
     if ((!kScanVariants[v].smem || s->smem_ok) && prepare_scan(v, s->num_sms, s->smem, &grid) == cudaSuccess) {
@@ -452,6 +456,7 @@ int scan_autotune(stb_scan *s, int nturn, double *timings, int ntimings) {
       a.nturn = nturn;
       a.grid = grid;
       a.chunk = kScanVariants[v].block;
+      a.pack = pack;
       cuda_check(cudaEventRecord(e0, s->stream), "event");
       cudaError_t le = launch_scan_block(a, v, grid, s->smem, s->stream);
       cuda_check(cudaEventRecord(e1, s->stream), "event");
@@ -463,9 +468,11 @@ int scan_autotune(stb_scan *s, int nturn, double *timings, int ntimings) {
     } else {
       cudaGetLastError();
     }
-    if (timings && v < ntimings) timings[v] = ms;
+    if (timings && v < ntimings && ms > 0.f && (timings[v] <= 0.0 || pack == 0 || ms < timings[v])) timings[v] = ms;
+    if (timings && v < ntimings && pack == 0 && ms <= 0.f) timings[v] = ms;
     if (ms > 0.f && (best < 0 || ms < best_ms)) {
       best = v;
+      best_pack = pack;
       best_ms = ms;
     }
   }
@@ -478,6 +485,8 @@ int scan_autotune(stb_scan *s, int nturn, double *timings, int ntimings) {
     s->variant = best;
     cuda_check(prepare_scan(best, s->num_sms, s->smem, &s->grid), "scan kernel setup");
     set_chunk(s, kScanVariants[best].block);
+    s->pack = best_pack;
+    s->args.pack = best_pack;
   }
   s->args.grid = s->grid;
   return s->variant;
@@ -587,6 +596,27 @@ int stb_scan_retire(stb_scan *s, const uint8_t *mask) {
     cuda_check(stb::launch_scan_compact_only(a, s->stream), "compaction");
     cuda_check(launch_scan_finalize(s->args, s->max_per_seed, s->stream), "finalize");
     cuda_check(cudaStreamSynchronize(s->stream), "retire");
+    return STB_OK;
+  });
+}
+
+int stb_scan_set_packing(stb_scan *s, int pack) {
+  return guarded([&] {
+    if (!s) throw Error(STB_EINVAL, "NULL scan");
+    s->pack = pack != 0;
+    s->args.pack = s->pack;
+    if (s->graph) {  // captured launches embed the old arguments
+      cudaGraphExecDestroy(s->graph);
+      s->graph = nullptr;
+    }
+    return STB_OK;
+  });
+}
+
+int stb_scan_packing(const stb_scan *s, int *pack) {
+  return guarded([&] {
+    if (!s || !pack) throw Error(STB_EINVAL, "NULL argument");
+    *pack = s->pack;
     return STB_OK;
   });
 }

@@ -196,3 +196,18 @@ def test_wall_clock_budget_stops_and_resumes():
     sc.run(256 - done, turns_per_block=16)
     for a, b in zip(whole.results(), sc.results()):
         assert np.array_equal(a, b)
+
+
+def test_packed_work_items_agree():
+    """Packed and spread work items give the same bits."""
+    tabs, xs, lats = seed_setup(2, namp=12, nang=3)
+    res = []
+    for pack in (False, True):
+        sc = Scan(tabs, xs, aperture_radius=0.03)
+        sc.configure(variant=2, chunk=128)
+        sc.set_packing(pack)
+        assert sc.packing() == pack
+        sc.run(200, turns_per_block=50)
+        res.append(sc.results())
+    for a, b in zip(*res):
+        assert np.array_equal(a, b)
