@@ -71,7 +71,7 @@ __host__ __device__ inline double unif(uint64_t seed, uint64_t i, int k) {
 __host__ __device__ inline void drift_check_one(uint64_t seed, uint64_t i, unsigned long long *bad) {
   const double beta = 0.99995598, gamma = 106.58, sg = sqrt(gamma * gamma - 1.);
   const double pt = (2 * unif(seed, i, 0) - 1) * 2e-3 * pow(10.0, -3 * unif(seed, i, 1));
-  const double smax = (i % 64 == 63) ? 0.05 : kSeedSlope;
+  const double smax = (i % 64 == 63) ? 0.05 : kSeedSlope2;
   const double px = (2 * unif(seed, i, 2) - 1) * smax * pow(10.0, -4 * unif(seed, i, 3));
   const double py = (2 * unif(seed, i, 4) - 1) * smax * pow(10.0, -4 * unif(seed, i, 5));
   const double L = 0.01 + 6 * unif(seed, i, 6);
@@ -80,7 +80,7 @@ __host__ __device__ inline void drift_check_one(uint64_t seed, uint64_t i, unsig
   const double beta1 = sqrt(1.0 - 1.0 / gamma1 / gamma1);
   const double opd = 1.0 + delta1, opd2 = opd * opd, iopd = 1.0 / opd, ibeta1 = 1.0 / beta1;
   double pz, ipz, betaz, lb;
-  drift_quotients(opd, opd2, beta1, iopd, ibeta1, px, py, L, pz, ipz, betaz, lb);
+  drift_quotients(opd, opd2, beta1, iopd, mul_rn(opd, ibeta1), px, py, L, pz, ipz, betaz, lb);
   const double rpz = sqrt(opd2 - px * px - py * py);
   const double ripz = 1.0 / rpz;
   const double rbetaz = mul_rn(rpz, beta1) / opd;

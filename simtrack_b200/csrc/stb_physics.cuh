@@ -42,7 +42,17 @@ struct PtCache {
   double beta1;   // particle velocity / c
   double iopd;    // RN(1 / opd)
   double ibeta1;  // RN(1 / beta1)
+  double opd_ibeta1;  // RN(opd * ibeta1), for 1/betaz in the drift
 };
+
+// RN(a * b), a product that no contraction policy fuses into an FMA.
+__host__ __device__ __forceinline__ double mul_rn(double a, double b) {
+#ifdef __CUDA_ARCH__
+  return __dmul_rn(a, b);  // never contracted into an FMA, whatever the unit's flags
+#else
+  return a * b;
+#endif
+}
 
 // a / b given y = RN(1/b) (see the division note above).
 __device__ __forceinline__ double qdiv(double a, double b, double y) {
@@ -60,38 +70,40 @@ __device__ __forceinline__ void pt_refresh(const RefConsts &R, double pt, PtCach
   c.opd2 = c.opd * c.opd;
   c.iopd = 1.0 / c.opd;
   c.ibeta1 = 1.0 / c.beta1;
+  c.opd_ibeta1 = mul_rn(c.opd, c.ibeta1);
 }
 
 // Square root and reciprocal of a drift from the cached seed.  With
 // v = (1+delta1)^2 - px^2 - py^2 and y0 = RN(1/(1+delta1)), y0 is within
-// (px^2 + py^2) / (2 (1+delta1)^2) <= 5e-5 relative of 1/sqrt(v) when |px|
-// and |py| are below kSeedSlope.  Two Newton steps for the reciprocal square
-// root in FMA form, y <- y + (y/2)(1 - v y^2), bring y within about an ulp;
-// the square root s = RN(v y) is then corrected once with its exact remainder,
-// s + (v - s^2) y/2 (Markstein's square-root step, IBM J. Res. Dev. 34 (1990)
-// 111), and the reciprocal once with its remainder, y + y (1 - s y).  Both
-// are the correctly rounded values unless the exact one lies within about
-// 2^-50 ulp of a rounding midpoint (the same order as qdiv above); they are
-// checked against IEEE sqrt and division on random drift arguments on the
-// host and on the GPU.  Steeper slopes return false: the caller then takes
-// IEEE sqrt and division.  14 FP64 operations and no MUFU, where sqrt and a
-// reciprocal cost two MUFU seeds and two Newton sequences with range checks.
-constexpr double kSeedSlope = 7e-3;
-
-__host__ __device__ __forceinline__ double mul_rn(double a, double b) {
-#ifdef __CUDA_ARCH__
-  return __dmul_rn(a, b);  // never contracted into an FMA, whatever the unit's flags
-#else
-  return a * b;
-#endif
-}
+// e0 = (px^2 + py^2) / (2 (1+delta1)^2) relative of 1/sqrt(v).  Newton steps
+// for the reciprocal square root in FMA form, y <- y + (y/2)(1 - v y^2),
+// square the error (times 3/2): one step suffices when |px| and |py| are below
+// kSeedSlope1 (e0 <= 6.4e-7, then 2^-40), a second one up to kSeedSlope2
+// (e0 <= 5e-5).  The square root s = RN(v y) is then corrected once with its
+// exact remainder, s + (v - s^2) y/2 (Markstein's square-root step, IBM J.
+// Res. Dev. 34 (1990) 111), and the reciprocal once with its remainder,
+// y + y (1 - s y).  Both are the correctly rounded values unless the exact
+// one lies within about 2^-50 ulp of a rounding midpoint (the same order as
+// qdiv above); they are checked against IEEE sqrt and division on random
+// drift arguments on the host and on the GPU.  Steeper slopes return false:
+// the caller then takes IEEE sqrt and division.  10 or 14 FP64 operations and
+// no MUFU, where sqrt and a reciprocal cost two MUFU seeds and two Newton
+// sequences with range checks.  The step count is chosen per lane; the lanes
+// of a warp usually agree, so the branch rarely diverges.
+constexpr double kSeedSlope1 = 8e-4;
+constexpr double kSeedSlope2 = 7e-3;
 
 __host__ __device__ __forceinline__ bool seeded_sqrt_recip(double v, double y0, double px, double py, double &s,
                                                            double &is) {
-  if (!(fabs(px) < kSeedSlope && fabs(py) < kSeedSlope)) return false;
+  const double apx = fabs(px), apy = fabs(py);
+  if (!(apx < kSeedSlope2 && apy < kSeedSlope2)) return false;
   double y = y0;
-#pragma unroll
-  for (int k = 0; k < 2; k++) {
+  {
+    const double t = mul_rn(v, y);
+    const double e = fma(-t, y, 1.0);
+    y = fma(mul_rn(0.5, y), e, y);
+  }
+  if (!(apx < kSeedSlope1 && apy < kSeedSlope1)) {
     const double t = mul_rn(v, y);
     const double e = fma(-t, y, 1.0);
     y = fma(mul_rn(0.5, y), e, y);
@@ -115,16 +127,16 @@ __host__ __device__ __forceinline__ double qdiv_near(double a, double b, double 
 
 // The divisions and square root of DRIFT_Pass's exact branch: pz =
 // sqrt((1+delta1)^2 - px^2 - py^2), 1/pz, betaz = pz*beta1/(1+delta1) and
-// L/betaz.  The reciprocal of betaz is (1+delta1) * (1/pz) * (1/beta1) from
-// the cached reciprocals, within ~2.5 ulp.
+// L/betaz.  The reciprocal of betaz is ((1+delta1)/beta1) * (1/pz) from the
+// cached RN((1+delta1) * RN(1/beta1)), within ~2.5 ulp.
 __host__ __device__ __forceinline__ void drift_quotients(double opd, double opd2, double beta1, double iopd,
-                                                         double ibeta1, double px, double py, double L, double &pz,
-                                                         double &ipz, double &betaz, double &L_betaz) {
+                                                         double opd_ibeta1, double px, double py, double L,
+                                                         double &pz, double &ipz, double &betaz, double &L_betaz) {
   const double v = opd2 - px * px - py * py;
   if (seeded_sqrt_recip(v, iopd, px, py, pz, ipz)) {
     const double t = mul_rn(pz, beta1);
     betaz = qdiv_near(t, opd, iopd);
-    L_betaz = qdiv_near(L, betaz, mul_rn(mul_rn(opd, ipz), ibeta1));
+    L_betaz = qdiv_near(L, betaz, mul_rn(opd_ibeta1, ipz));
   } else {
     pz = sqrt(v);
     ipz = 1.0 / pz;
@@ -139,7 +151,7 @@ __host__ __device__ __forceinline__ void drift_quotients(double opd, double opd2
 // the cached reciprocal of 1+delta1.
 __device__ __forceinline__ void drift(Particle &p, const PtCache &c, double L, double Lb) {
   double pz, ipz, betaz, L_betaz;
-  drift_quotients(c.opd, c.opd2, c.beta1, c.iopd, c.ibeta1, p.px, p.py, L, pz, ipz, betaz, L_betaz);
+  drift_quotients(c.opd, c.opd2, c.beta1, c.iopd, c.opd_ibeta1, p.px, p.py, L, pz, ipz, betaz, L_betaz);
   p.x = p.x + qdiv(p.px * L, pz, ipz);
   p.y = p.y + qdiv(p.py * L, pz, ipz);
   p.z = p.z - (L_betaz - Lb);
