@@ -220,7 +220,7 @@ class Line:
             pass
 
 
-NUM_VARIANTS = 16
+NUM_VARIANTS = 18
 NUM_SCAN_VARIANTS = 9
 
 
@@ -287,10 +287,10 @@ class Table:
         """Times every kernel launch variant on a copy of `coords` (6 CUDA float64
         tensors, not modified) and keeps the fastest; returns {name: ms}."""
         chosen = c_int()
-        t = (c_double * 16)()
+        t = (c_double * 32)()
         n = coords[0].numel()
         check(lib().stb_table_autotune(self._h, *[c_void_p(c.data_ptr()) for c in coords], n, nturn,
-                                       aperture_radius, byref(chosen), t, 16))
+                                       aperture_radius, byref(chosen), t, 32))
         return {"chosen": variant_name(chosen.value),
                 "ms": {variant_name(v): t[v] for v in range(NUM_VARIANTS)}}
 

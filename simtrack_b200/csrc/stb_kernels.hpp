@@ -21,7 +21,7 @@ struct TrackVariant {
   const char *name;
   bool prefetch;   // next element header loaded while the current element runs
 };
-constexpr int kNumTrackVariants = 16;
+constexpr int kNumTrackVariants = 18;
 extern const TrackVariant kVariants[kNumTrackVariants];
 
 struct TrackArgs {

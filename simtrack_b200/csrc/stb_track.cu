@@ -47,6 +47,7 @@ const TrackVariant kVariants[kNumTrackVariants] = {
     {true, false, 768, 1, 1, "smem_b768_r85_pf", true},     {true, true, 1024, 1, 1, "seg_b1024_r64", false},
     {true, true, 768, 1, 1, "seg_b768_r85", false},         {true, true, 512, 1, 1, "seg_b512_r128", false},
     {true, false, 256, 1, 1, "smem_b256_r255", false},      {true, false, 128, 1, 1, "smem_b128_r255", false},
+    {true, false, 896, 1, 1, "smem_b896_r72", false},       {true, false, 640, 1, 1, "smem_b640_r96", false},
 };
 
 // Segments of at most `budget` bytes each (headers plus the 16-byte aligned

@@ -60,6 +60,8 @@ cudaError_t launch_track_variants(const TrackArgs &a, int num_sms, int variant, 
     case 13: return launch_variant<true, 512, 1, 1, false, false, true>(a, num_sms, sg, stream);
     case 14: return launch_variant<true, 256, 1, 1, false>(a, num_sms, sm, stream);
     case 15: return launch_variant<true, 128, 1, 1, false>(a, num_sms, sm, stream);
+    case 16: return launch_variant<true, 896, 1, 1, false>(a, num_sms, sm, stream);
+    case 17: return launch_variant<true, 640, 1, 1, false>(a, num_sms, sm, stream);
     default: return cudaErrorInvalidValue;
   }
 }
