@@ -286,7 +286,7 @@ __device__ __forceinline__ void call_out_of_line(const ElemHeader &h, const doub
 // loss.  For the hot element types the per-particle maps are issued back to
 // back, so their independent FP64 dependency chains interleave in the
 // instruction stream (latency hiding without more resident warps).
-template <int kPPT>
+template <int kPPT, bool kLoopSlices = false>
 __device__ __forceinline__ void apply_element(const ElemHeader &h, const double *P, Particle (&p)[kPPT],
                                               PtCache (&c)[kPPT], const RefConsts &R) {
   const double *M = P;
@@ -323,22 +323,41 @@ __device__ __forceinline__ void apply_element(const ElemHeader &h, const double 
       const volatile double *V = P;
       if (h.flags & EF_FRINGE)
         for (int k = 0; k < kPPT; k++) quad_fringe(p[k], P[8], true);
+      if (kLoopSlices) {
+        // one copy of the drift code: smaller instruction footprint, better
+        // for many resident warps; the unrolled form has the shorter latency
 #pragma unroll 1
-      for (int s = 0; s < h.nint; s++) {
+        for (int s = 0; s < h.nint; s++) {
+#pragma unroll 1
+          for (int q = 0; q < 4; q++) {
+            const int dofs = (q == 0 || q == 3) ? 0 : 2;
 #pragma unroll
-        for (int k = 0; k < kPPT; k++) drift(p[k], c[k], V[0], V[1]);
+            for (int k = 0; k < kPPT; k++) drift(p[k], c[k], V[dofs], V[dofs + 1]);
+            if (q < 3) {
+              const int kofs = (q == 1) ? 6 : 4;
 #pragma unroll
-        for (int k = 0; k < kPPT; k++) quad_kick(p[k], V[4], V[5]);
+              for (int k = 0; k < kPPT; k++) quad_kick(p[k], V[kofs], V[kofs + 1]);
+            }
+          }
+        }
+      } else {
+#pragma unroll 1
+        for (int s = 0; s < h.nint; s++) {
 #pragma unroll
-        for (int k = 0; k < kPPT; k++) drift(p[k], c[k], V[2], V[3]);
+          for (int k = 0; k < kPPT; k++) drift(p[k], c[k], V[0], V[1]);
 #pragma unroll
-        for (int k = 0; k < kPPT; k++) quad_kick(p[k], V[6], V[7]);
+          for (int k = 0; k < kPPT; k++) quad_kick(p[k], V[4], V[5]);
 #pragma unroll
-        for (int k = 0; k < kPPT; k++) drift(p[k], c[k], V[2], V[3]);
+          for (int k = 0; k < kPPT; k++) drift(p[k], c[k], V[2], V[3]);
 #pragma unroll
-        for (int k = 0; k < kPPT; k++) quad_kick(p[k], V[4], V[5]);
+          for (int k = 0; k < kPPT; k++) quad_kick(p[k], V[6], V[7]);
 #pragma unroll
-        for (int k = 0; k < kPPT; k++) drift(p[k], c[k], V[0], V[1]);
+          for (int k = 0; k < kPPT; k++) drift(p[k], c[k], V[2], V[3]);
+#pragma unroll
+          for (int k = 0; k < kPPT; k++) quad_kick(p[k], V[4], V[5]);
+#pragma unroll
+          for (int k = 0; k < kPPT; k++) drift(p[k], c[k], V[0], V[1]);
+        }
       }
       if (h.flags & EF_FRINGE)
         for (int k = 0; k < kPPT; k++) quad_fringe(p[k], P[8], false);
@@ -491,7 +510,7 @@ __device__ void track_segmented(const TrackArgs &a, unsigned char *smem, uint64_
         if (nalive > 0) {
           for (int j = 0; j < sg.ne; j++) {
             const ElemHeader h = hs[j];
-            apply_element<kPPT>(h, ps + (h.poff - sg.pool_lo), p, c, R);
+            apply_element<kPPT, (kBlock >= 512)>(h, ps + (h.poff - sg.pool_lo), p, c, R);
             after_element<kBlock, kPPT, kDump>(a, h, base, t, sg.e0 + j, p, c, alive, nalive);
             if (nalive == 0) break;
           }
@@ -580,7 +599,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) track_kernel(const __grid_
         } else {
           h = hdr[e];
         }
-        apply_element<kPPT>(h, pool + h.poff, p, c, R);
+        apply_element<kPPT, (kBlock >= 512)>(h, pool + h.poff, p, c, R);
 #pragma unroll
         for (int k = 0; k < kPPT; k++) {
           if (!alive[k]) continue;
