@@ -250,7 +250,7 @@ def _check_device_arrays(coords, lost_turn, lost_elem, n: int, device: int, ncoo
     ok(lost_elem, torch.int32, "lost_elem")
 
 
-NUM_SPIN_VARIANTS = 9
+NUM_SPIN_VARIANTS = 12
 
 
 def spin_variant_name(v: int) -> str:

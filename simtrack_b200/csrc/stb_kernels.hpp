@@ -62,7 +62,7 @@ struct SpinVariant {
   int min_blocks;
   const char *name;
 };
-constexpr int kNumSpinVariants = 9;
+constexpr int kNumSpinVariants = 12;
 extern const SpinVariant kSpinVariants[kNumSpinVariants];
 cudaError_t launch_spin(const SpinArgs &a, int num_sms, int variant, cudaStream_t stream);
 

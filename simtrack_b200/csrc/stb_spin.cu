@@ -39,8 +39,8 @@ struct Spin {
 // (direction of motion, pt, horizontal offset); c: the pt cache of x0;
 // angle, href: the reference orbit's bend angle and curvature over the step;
 // B: the integrated field over (B rho)_0.  Rotates s in place.
-__device__ __noinline__ void spin_rotate(const Particle &x0, const PtCache &c, const RefConsts &R, double angle,
-                                         double href, double B0, double B1, double B2, Spin &s) {
+__device__ __forceinline__ void spin_rotate(const Particle &x0, const PtCache &c, const RefConsts &R, double angle,
+                                            double href, double B0, double B1, double B2, Spin &s) {
   if (!(B0 * B0 + B1 * B1 + B2 * B2 != 0.)) return;
   const double gamma1 = R.gamma + R.sqrt_g2m1 * x0.pt;
   const double Gr = R.G * gamma1;
@@ -162,8 +162,8 @@ __device__ __forceinline__ void mpole_field(int order, bool thick, double x1, do
 }
 
 // One spin-opcode element (after the misalignment entrance transform).
-__device__ __noinline__ void spin_element(const ElemHeader &h, const double *P, Particle &p, Spin &s, PtCache &c,
-                                          const RefConsts &R) {
+__device__ __forceinline__ void spin_element(const ElemHeader &h, const double *P, Particle &p, Spin &s, PtCache &c,
+                                             const RefConsts &R) {
   switch (h.op) {
     case OP_S_SBEND: {
       p.px = p.px + P[0] * p.x;
@@ -339,12 +339,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) spin_track_kernel(const __
             gtol1(p[0], M, h.flags);
             P += kMisalignParams;
           }
-          Particle q = p[0];
-          Spin ss = s;
-          PtCache cc = c[0];
-          spin_element(h, P, q, ss, cc, R);
-          p[0] = q;
-          s = ss;
+          spin_element(h, P, p[0], s, c[0], R);
           if (mis) ltog1(p[0], M, h.flags);
         } else {
           apply_element<1>(h, P, p, c, R);
@@ -405,6 +400,7 @@ const SpinVariant kSpinVariants[kNumSpinVariants] = {
     {true, 512, 1, "smem_b512_r128"}, {true, 1024, 1, "smem_b1024_r64"}, {true, 768, 1, "smem_b768_r85"},
     {false, 256, 2, "l1_b256_r128"},  {false, 256, 3, "l1_b256_r80"},    {false, 256, 4, "l1_b256_r64"},
     {false, 128, 4, "l1_b128_r128"},  {false, 64, 8, "l1_b64_r128"},     {false, 64, 12, "l1_b64_r85"},
+    {false, 64, 4, "l1_b64_r255"},    {false, 128, 2, "l1_b128_r255"},   {true, 256, 1, "smem_b256_r255"},
 };
 
 cudaError_t launch_spin(const SpinArgs &a, int num_sms, int variant, cudaStream_t stream) {
@@ -421,6 +417,9 @@ cudaError_t launch_spin(const SpinArgs &a, int num_sms, int variant, cudaStream_
     case 6: return launch_spin_variant<false, 128, 4, false>(a, num_sms, 0, stream);
     case 7: return launch_spin_variant<false, 64, 8, false>(a, num_sms, 0, stream);
     case 8: return launch_spin_variant<false, 64, 12, false>(a, num_sms, 0, stream);
+    case 9: return launch_spin_variant<false, 64, 4, false>(a, num_sms, 0, stream);
+    case 10: return launch_spin_variant<false, 128, 2, false>(a, num_sms, 0, stream);
+    case 11: return launch_spin_variant<true, 256, 1, false>(a, num_sms, sm, stream);
     default: return cudaErrorInvalidValue;
   }
 }
