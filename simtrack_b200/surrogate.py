@@ -89,6 +89,7 @@ def early_phase(tables, grids, radius: float, twiss6, cfg: SurrogateConfig, devi
     dev = torch.device("cuda", device)
     t0 = time.perf_counter()
     sc = Scan(tables, grids, aperture_radius=radius, device=device)
+    sc.autotune(nturn=16)
     n = sc.n
     tbt = torch.empty((cfg.nrec, 4, n), dtype=torch.float64, device=dev)
     sc.set_tbt(tbt, cfg.nrec)
@@ -263,8 +264,12 @@ def da_of(survive: np.ndarray, nseed: int, nd: int, nang: int, namp: int, amax: 
 
 
 def plain_scan(tables, grids, radius, cfg: SurrogateConfig, device: int = 0):
+    """Every particle to its loss or the full turn count, one persistent scan;
+    the launch variant (and work-item packing) tuned on the first turns, as the
+    pruned scan tunes its own phases."""
     t0 = time.perf_counter()
     sc = Scan(tables, grids, aperture_radius=radius, device=device)
+    sc.autotune(nturn=16)
     sc.run(cfg.nturn, cfg.turns_per_block)
     lt, _, _ = sc.results()
     wall = time.perf_counter() - t0
