@@ -5,7 +5,10 @@ the GPU) of the EIC-like ring: `nseed` error seeds x `n` particles each, all
 seeds' launches issued on their own CUDA streams and timed together with CUDA
 events; prints one JSON line.  `python -m simtrack_b200.measure radial` does
 the same for Track_Radial on the RHIC-like ring.  `python -m
-simtrack_b200.measure contraction --turns 1000` compares the FMA-contracted
+simtrack_b200.measure launch --case quad --variant 1 --particles 1048576
+--turns 1` runs exactly two launches of the tracking kernel (a warm-up and
+the timed one) on one single-type lattice or the ring, the form the ncu
+summaries capture.  `python -m simtrack_b200.measure contraction --turns 1000` compares the FMA-contracted
 kernel with the strict one on the RHIC-like ring's DA grid (divergence, DA,
 loss turns, throughput).  `python -m simtrack_b200.measure elements` times
 the tracking kernel on single-type
@@ -87,6 +90,70 @@ def run(kind: str = "spin", nseed: int = 16, n: int = 2048, nturn: int = 200, wa
             "variants": sorted(set(chosen))}
     print(json.dumps(line))
     return line
+
+
+def _single_type_lattice(name: str):
+    """The single-type lattices of element_costs (name: drift, quad, sbend,
+    sext, mult, bb6d, rfcav), or the RHIC-like ring with seed-1 errors (rhic)."""
+    from .lattices import ElementSpec as S, Lattice, mult_args
+    if name == "rhic":
+        return lattices.rhic_like_ring(seed=1)
+    gamma = 100000.0 / lattices.PROTON_MASS_MEV
+    err = [0.0, 0.29] + [1e-4 * (-1) ** k * math.factorial(k) / 0.031 ** (k - 1) * 0.29 for k in range(2, 10)] + [0.0]
+    cases = {
+        "drift": ([("DRIFT", (1.0,))], 400),
+        "quad": ([("QUAD", (1.1, 0.1, 0.0), {"Nint": 4}), ("QUAD", (1.1, -0.1, 0.0), {"Nint": 4})], 200),
+        "sbend": ([("SBEND", (5.8, 0.0145, 0.0, 0.0))], 400),
+        "sext": ([("SEXT", (0.0, 0.6, 0.0))], 400),
+        "mult": ([("MULT", mult_args(2.0, err, [0.0] * 11), {"Nint": 8}),
+                  ("MULT", mult_args(2.0, [-e for e in err], [0.0] * 11), {"Nint": 8})], 20),
+        "bb6d": ([("BEAMBEAM", (6, 2e11, 1.0, 0.3, 5, 2.4e-8, 0.6, 0.0, 2.4e-8, 0.6, 0.0))], 100),
+        "rfcav": ([("RFCAV", (0.0, 3.0, 197e6, 0.0))], 200),
+    }
+    specs, reps = cases[name]
+    els = [S(sp[0], f"e{r}_{i}", sp[1], sp[2] if len(sp) > 2 else {}) for r in range(reps) for i, sp in enumerate(specs)]
+    return Lattice("mb_" + name, els, gamma)
+
+
+def one_launch(case: str = "rhic", n: int = 1 << 20, variant: int = 1, nturn: int = 1, device: int = 0) -> dict:
+    """Exactly two launches of the tracking kernel with a fixed launch variant
+    (a warm-up turn, then `nturn` turns timed with CUDA events) on one lattice
+    of _single_type_lattice: the form profilers capture (skip one launch,
+    capture one).  Gaussian beam for the ring, small offsets for the
+    single-type lattices.  Prints one JSON line."""
+    import torch
+    from .api import variant_name
+    lat = _single_type_lattice(case)
+    if case == "rhic":
+        X = lattices.gaussian_beam(lattices.rhic_like_ring(seed=None, bb=False), n, seed=7)
+    else:
+        rng = np.random.default_rng(1)
+        X = np.zeros((n, 6))
+        X[:, 0] = rng.normal(0, 1e-4, n)
+        X[:, 2] = rng.normal(0, 1e-4, n)
+        X[:, 5] = rng.normal(0, 1e-4, n)
+    tab = Table(lattices.build_line(lat), device)
+    tab.set_variant(variant)
+    dev = torch.device("cuda", device)
+    c = [torch.tensor(np.ascontiguousarray(X[:, k]), device=dev) for k in range(6)]
+    lt = torch.full((n,), -1, dtype=torch.int32, device=dev)
+    le = torch.zeros(n, dtype=torch.int32, device=dev)
+    r = lat.aperture_radius
+    tab.track_device(c, lt, le, 0, 1, r)
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    tab.track_device(c, lt, le, 1, nturn, r)
+    e1.record()
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1) / nturn
+    info = tab.info()
+    out = {"case": case, "particles": n, "variant": variant_name(variant), "ms_per_turn": ms,
+           "elements": info["elements"], "flops_per_turn": info["flops_per_turn"],
+           "tflops": info["flops_per_turn"] * n / (ms * 1e-3) / 1e12,
+           "ps_per_element_particle": ms * 1e9 / (n * info["elements"]), "alive": int((lt < 0).sum())}
+    print(json.dumps(out))
+    return out
 
 
 def element_costs(n: int = 1 << 20, device: int = 0) -> dict:
@@ -227,7 +294,9 @@ def contraction(nturn: int = 1000, every: int = 10, n_rate: int = 1 << 20, rate_
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("kind", choices=["spin", "radial", "elements", "contraction"])
+    ap.add_argument("kind", choices=["spin", "radial", "elements", "contraction", "launch"])
+    ap.add_argument("--case", default="rhic")
+    ap.add_argument("--variant", type=int, default=1)
     ap.add_argument("--seeds", type=int, default=16)
     ap.add_argument("--particles", type=int, default=2048)
     ap.add_argument("--turns", type=int, default=200)
@@ -236,6 +305,8 @@ def main(argv=None):
         element_costs()
     elif a.kind == "contraction":
         contraction(nturn=a.turns)
+    elif a.kind == "launch":
+        one_launch(a.case, a.particles, a.variant, a.turns)
     else:
         run(a.kind, a.seeds, a.particles, a.turns)
 
