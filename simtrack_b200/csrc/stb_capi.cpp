@@ -123,6 +123,9 @@ stb_table *table_build(const Line &line, int device, bool spin = false) {
   std::unique_ptr<stb_table, void (*)(stb_table *)> t(new stb_table(), table_destroy);
   t->device = device;
   t->host = spin ? flatten_spin(line) : flatten(line);
+  t->min_ap2 = INFINITY;
+  for (const ElemHeader &h : t->host.hdr)
+    if ((h.flags & EF_NO_LOSS_CHECK) == 0) t->min_ap2 = std::fmin(t->min_ap2, std::fmin(h.apx * h.apx, h.apy * h.apy));
   if (t->host.hdr.empty()) throw Error(STB_EINVAL, "line has no elements");
   DeviceGuard g(device);
   std::vector<double> pool = t->host.pool;
@@ -178,6 +181,7 @@ int track_device(stb_table *t, double *x, double *px, double *y, double *py, dou
   a.turn0 = turn0;
   a.nturn = nturn;
   a.r2 = radius > 0.0 ? radius * radius : INFINITY;
+  a.loss_mode = loss_mode_for(a.r2, t->min_ap2);
   a.lost_turn = lost_turn;
   a.lost_elem = lost_elem;
   a.dump = dump;
@@ -238,6 +242,7 @@ int autotune(stb_table *t, const double *const *in, int nc, long n, int nturn, d
         TrackArgs a = make_args(t);
         a.x = buf; a.px = buf + m; a.y = buf + 2 * m; a.py = buf + 3 * m; a.z = buf + 4 * m; a.pt = buf + 5 * m;
         a.n = m; a.turn0 = 1; a.nturn = nturn; a.r2 = radius > 0 ? radius * radius : INFINITY;
+        a.loss_mode = loss_mode_for(a.r2, t->min_ap2);
         a.lost_turn = lost; a.lost_elem = lost + m; a.dump = nullptr;
         cuda_check(cudaEventRecord(e0), "event");
         cudaError_t le;
@@ -388,6 +393,7 @@ int radial_device(stb_table *t, double *x, double *px, double *y, double *py, do
   a.turn0 = turn0;
   a.nturn = nturn;
   a.r2 = radius > 0.0 ? radius * radius : INFINITY;
+  a.loss_mode = loss_mode_for(a.r2, t->min_ap2);
   a.lost_turn = lost_turn;
   a.lost_elem = lost_elem;
   a.dump = dump;
@@ -466,6 +472,7 @@ int spin_device(stb_table *t, double *const xs[9], long n, int turn0, int nturn,
   a.t.turn0 = turn0;
   a.t.nturn = nturn;
   a.t.r2 = radius > 0.0 ? radius * radius : INFINITY;
+  a.t.loss_mode = loss_mode_for(a.t.r2, t->min_ap2);
   a.t.lost_turn = lost_turn;
   a.t.lost_elem = lost_elem;
   a.dump = dump;

@@ -35,6 +35,7 @@ struct TrackArgs {
   int turn0;   // global index of the first turn of this block
   int nturn;   // turns in this block
   double r2;   // circular aperture radius squared; +inf when there is none
+  int loss_mode;  // which terms of the loss test can fire (is_lost), set by loss_mode_for
   int32_t *lost_turn;  // < 0 while alive
   int32_t *lost_elem;
   int *status;  // device status word (STB_OK or an error code)
@@ -84,6 +85,12 @@ cudaError_t fp64_peak_probe(int device, double *tflops);
 cudaError_t drift_quotient_check(long n, unsigned long long seed, int device, unsigned long long *bad4);
 
 size_t track_smem_bytes(int nelem, int npool_padded);
+// The loss-test mode of a launch with circular aperture r2 (+inf: none) on a
+// table whose loss-checked elements have min(RN(APx^2), RN(APy^2)) >= min_ap2.
+inline int loss_mode_for(double r2, double min_ap2) {
+  if (!(r2 < 1e300)) return 2;      // no circle
+  return r2 < min_ap2 ? 1 : 0;      // circle strictly inside every rectangle
+}
 // Consecutive segments of at most `budget` bytes of staged table (headers plus
 // 16-byte aligned pool slice); empty if one element alone exceeds the budget.
 std::vector<SegDesc> plan_segments(const ElemHeader *hdr, int nelem, int npool_padded, size_t budget);

@@ -89,7 +89,7 @@ __global__ void __launch_bounds__(kBlock, 1) radial_track_kernel(const __grid_co
           double *d = a.dump + (((size_t)i * a.nturn + t) * a.nelem + e) * 6;
           d[0] = p[0].x; d[1] = p[0].px; d[2] = p[0].y; d[3] = p[0].py; d[4] = p[0].z; d[5] = p[0].pt;
         }
-        if (needs_loss_check(h) && is_lost(p[0], h.apx, h.apy, a.r2)) {
+        if (needs_loss_check(h) && is_lost(p[0], h.apx, h.apy, a.r2, a.loss_mode)) {
           lt = a.turn0 + t;
           le = e;
           break;

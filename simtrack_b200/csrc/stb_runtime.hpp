@@ -20,6 +20,7 @@ struct stb_table {
   bool use_smem = false;  // the table fits the shared-memory variants
   int variant = 2;        // launch variant (stb::kVariants), set by the autotuner
   bool fast = false;      // FMA-contracted kernel (stb_table_set_contraction) instead of the strict one
+  double min_ap2 = 0.;    // min over loss-checked elements of RN(APx^2), RN(APy^2) (loss_mode_for)
   // Segment plan for tables that do not fit shared memory whole (seg_*
   // launch variants): segments of at most seg_bytes bytes each.
   stb::SegDesc *d_segs = nullptr;

@@ -167,7 +167,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) scan_track_kernel(const __
         for (int e = 0; e < sd.nelem; e++) {
           const ElemHeader h = hdr[e];
           apply_element<1, (kBlock >= 512)>(h, pool + h.poff, p, c, R);
-          if (needs_loss_check(h) && is_lost(p[0], h.apx, h.apy, a.r2)) {
+          if (needs_loss_check(h) && is_lost(p[0], h.apx, h.apy, a.r2, a.loss_mode)) {
             lt = turn0 + t;
             le = e;
             break;

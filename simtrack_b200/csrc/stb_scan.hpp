@@ -37,6 +37,7 @@ struct ScanArgs {
   int32_t *turn0;                    // device turn counter
   int nturn;                         // turns per block
   double r2;
+  int loss_mode;  // see is_lost / loss_mode_for
   int *status;
   int32_t *out_lost_turn, *out_lost_elem;  // by original index
   double *out_x;                           // AoS by original index

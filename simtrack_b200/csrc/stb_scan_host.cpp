@@ -181,6 +181,9 @@ stb_scan *scan_build(stb_table **tables, int nseed, const double *x0, const long
   a.stage = s->d_stage;
   a.stage_id = reinterpret_cast<int32_t *>(s->d_stage + 6 * n);
   a.r2 = radius > 0.0 ? radius * radius : INFINITY;
+  double min_ap2 = INFINITY;
+  for (int i = 0; i < nseed; i++) min_ap2 = std::fmin(min_ap2, tables[i]->min_ap2);
+  a.loss_mode = loss_mode_for(a.r2, min_ap2);
   a.status = s->d_status;
   a.tbt = nullptr;
   a.tbt_turns = 0;

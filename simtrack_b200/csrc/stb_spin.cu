@@ -349,7 +349,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) spin_track_kernel(const __
           d[0] = p[0].x; d[1] = p[0].px; d[2] = p[0].y; d[3] = p[0].py; d[4] = p[0].z; d[5] = p[0].pt;
           d[6] = s.x; d[7] = s.y; d[8] = s.z;
         }
-        if (needs_loss_check(h) && is_lost(p[0], h.apx, h.apy, a.r2)) {
+        if (needs_loss_check(h) && is_lost(p[0], h.apx, h.apy, a.r2, a.loss_mode)) {
           lt = a.turn0 + t;
           le = e;
           break;

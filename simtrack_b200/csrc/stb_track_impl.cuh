@@ -109,7 +109,17 @@ __device__ __forceinline__ bool wait_phase(uint64_t *bar, uint32_t phase) {
 // Track()'s loss test (simtrack.cpp:20802): |x| > APx, |y| > APy or NaN;
 // !(|x| <= APx) is true for NaN as well.  r2 is the circular aperture radius
 // squared, +inf when there is none.
-__device__ __forceinline__ bool is_lost(const Particle &p, double apx, double apy, double r2) {
+//
+// loss_mode (uniform per launch, chosen on the host) drops the terms that
+// cannot change the outcome: kLossCircle when the circle lies strictly inside
+// every element's rectangle in rounded arithmetic (r2 < RN(APx^2), RN(APy^2):
+// a point outside a rectangle is then outside the circle, and a NaN fails
+// x^2 + y^2 <= r2), kLossRect when there is no circle (r2 = +inf, whose test
+// never fires).
+constexpr int kLossFull = 0, kLossCircle = 1, kLossRect = 2;
+__device__ __forceinline__ bool is_lost(const Particle &p, double apx, double apy, double r2, int mode = kLossFull) {
+  if (mode == kLossCircle) return !(p.x * p.x + p.y * p.y <= r2);
+  if (mode == kLossRect) return !(fabs(p.x) <= apx) || !(fabs(p.y) <= apy);
   return !(fabs(p.x) <= apx) || !(fabs(p.y) <= apy) || p.x * p.x + p.y * p.y > r2;
 }
 
@@ -445,7 +455,7 @@ __device__ __forceinline__ void after_element(const TrackArgs &a, const ElemHead
       double *d = a.dump + (((size_t)i * a.nturn + t) * a.nelem + e) * 6;
       d[0] = p[k].x; d[1] = p[k].px; d[2] = p[k].y; d[3] = p[k].py; d[4] = p[k].z; d[5] = p[k].pt;
     }
-    if (needs_loss_check(h) && is_lost(p[k], h.apx, h.apy, a.r2)) {
+    if (needs_loss_check(h) && is_lost(p[k], h.apx, h.apy, a.r2, a.loss_mode)) {
       store_particle(a, i, p[k]);
       a.lost_turn[i] = a.turn0 + t;
       a.lost_elem[i] = e;
@@ -608,7 +618,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) track_kernel(const __grid_
             double *d = a.dump + (((size_t)i * a.nturn + t) * a.nelem + e) * 6;
             d[0] = p[k].x; d[1] = p[k].px; d[2] = p[k].y; d[3] = p[k].py; d[4] = p[k].z; d[5] = p[k].pt;
           }
-          if (needs_loss_check(h) && is_lost(p[k], h.apx, h.apy, a.r2)) {
+          if (needs_loss_check(h) && is_lost(p[k], h.apx, h.apy, a.r2, a.loss_mode)) {
             store_particle(a, i, p[k]);
             a.lost_turn[i] = a.turn0 + t;
             a.lost_elem[i] = e;
@@ -618,7 +628,8 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) track_kernel(const __grid_
             pt_refresh(R, 0.0, c[k]);
           }
         }
-        if (nalive == 0) break;
+        // a thread whose particles are all lost finishes the turn on benign
+        // operands and stops at the turn boundary (no per-element test)
       }
     }
 #pragma unroll

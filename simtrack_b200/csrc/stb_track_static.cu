@@ -155,6 +155,9 @@ int track_seeds_static(stb_table *const *tables, int nseed, const long *n_per_se
   a.item_chunk = sc->ctr + 3;
   a.nturn = nturn;
   a.r2 = radius > 0.0 ? radius * radius : INFINITY;
+  double min_ap2 = INFINITY;
+  for (int i = 0; i < nseed; i++) min_ap2 = std::fmin(min_ap2, tables[i]->min_ap2);
+  a.loss_mode = loss_mode_for(a.r2, min_ap2);
   a.status = &sc->status;
   a.ntot = total;
   a.abort = nullptr;
