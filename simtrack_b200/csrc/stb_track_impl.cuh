@@ -328,9 +328,11 @@ __device__ __forceinline__ void apply_element(const ElemHeader &h, const double 
       }
       break;
     case OP_QUAD_THICK: {
-      // Slice constants are re-read from the table at each use (volatile view)
-      // instead of being hoisted into eight live register pairs.
-      const volatile double *V = P;
+      // Wide CTAs (few registers) re-read the slice constants from the table at
+      // each use (volatile view) instead of holding eight register pairs; the
+      // latency variants (up to 255 registers) keep them in registers.
+      const double *V = P;
+      const volatile double *VV = P;
       if (h.flags & EF_FRINGE)
         for (int k = 0; k < kPPT; k++) quad_fringe(p[k], P[8], true);
       if (kLoopSlices) {
@@ -342,11 +344,11 @@ __device__ __forceinline__ void apply_element(const ElemHeader &h, const double 
           for (int q = 0; q < 4; q++) {
             const int dofs = (q == 0 || q == 3) ? 0 : 2;
 #pragma unroll
-            for (int k = 0; k < kPPT; k++) drift(p[k], c[k], V[dofs], V[dofs + 1]);
+            for (int k = 0; k < kPPT; k++) drift(p[k], c[k], VV[dofs], VV[dofs + 1]);
             if (q < 3) {
               const int kofs = (q == 1) ? 6 : 4;
 #pragma unroll
-              for (int k = 0; k < kPPT; k++) quad_kick(p[k], V[kofs], V[kofs + 1]);
+              for (int k = 0; k < kPPT; k++) quad_kick(p[k], VV[kofs], VV[kofs + 1]);
             }
           }
         }
