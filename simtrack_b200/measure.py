@@ -156,6 +156,25 @@ def one_launch(case: str = "rhic", n: int = 1 << 20, variant: int = 1, nturn: in
     return out
 
 
+def compaction(nseed: int = 64, n: int = 16384, device: int = 0) -> dict:
+    """Two turn blocks of one turn each of a batched scan with nseed seeds x n
+    Gaussian particles (spread work items of 256, the L1 variant), every
+    particle alive: the form the compaction kernels are profiled in (each
+    block ends with the four compaction passes over all live particles).
+    Prints one JSON line."""
+    from .api import Scan
+    lats = [lattices.rhic_like_ring(seed=s + 1) for s in range(nseed)]
+    tabs = [Table(lattices.build_line(lat), device) for lat in lats]
+    base = lattices.rhic_like_ring(seed=None, bb=False)
+    xs = [lattices.gaussian_beam(base, n, seed=100 + s) for s in range(nseed)]
+    sc = Scan(tabs, xs, aperture_radius=lats[0].aperture_radius, device=device)
+    sc.configure(variant=2, chunk=256)
+    sc.run(2, turns_per_block=1, use_graph=False)
+    out = {"measure": "scan compaction", "seeds": nseed, "particles": sc.n, "stats": sc.stats()}
+    print(json.dumps(out))
+    return out
+
+
 def element_costs(n: int = 1 << 20, device: int = 0) -> dict:
     """Picoseconds per element-particle of the autotuned tracking kernel on
     single-type lattices (one JSON line per type)."""
@@ -294,7 +313,7 @@ def contraction(nturn: int = 1000, every: int = 10, n_rate: int = 1 << 20, rate_
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("kind", choices=["spin", "radial", "elements", "contraction", "launch"])
+    ap.add_argument("kind", choices=["spin", "radial", "elements", "contraction", "launch", "compaction"])
     ap.add_argument("--case", default="rhic")
     ap.add_argument("--variant", type=int, default=1)
     ap.add_argument("--seeds", type=int, default=16)
@@ -307,6 +326,8 @@ def main(argv=None):
         contraction(nturn=a.turns)
     elif a.kind == "launch":
         one_launch(a.case, a.particles, a.variant, a.turns)
+    elif a.kind == "compaction":
+        compaction(a.seeds, a.particles)
     else:
         run(a.kind, a.seeds, a.particles, a.turns)
 
