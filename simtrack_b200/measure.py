@@ -156,6 +156,38 @@ def one_launch(case: str = "rhic", n: int = 1 << 20, variant: int = 1, nturn: in
     return out
 
 
+def spin_launch(n: int = 2048, variant: int = 10, nturn: int = 3, seed: int = 1, device: int = 0) -> dict:
+    """Exactly two launches of the spin kernel with a fixed launch variant on
+    one seed of the EIC-like ring (a warm-up turn, then `nturn` turns timed
+    with CUDA events): the form the spin kernel's profile captures.  Prints
+    one JSON line."""
+    import torch
+    from .api import spin_variant_name
+    lat = lattices.eic_like_ring(seed=seed)
+    tab = SpinTable(lattices.build_line(lat), device)
+    tab.set_variant(variant)
+    X = _beam(lat, n, 1000 + seed, True)
+    dev = torch.device("cuda", device)
+    c = [torch.tensor(np.ascontiguousarray(X[:, k]), device=dev) for k in range(9)]
+    lt = torch.full((n,), -1, dtype=torch.int32, device=dev)
+    le = torch.zeros(n, dtype=torch.int32, device=dev)
+    r = lat.aperture_radius
+    tab.track_device(c, lt, le, 0, 1, r)
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    tab.track_device(c, lt, le, 1, nturn, r)
+    e1.record()
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1) / nturn
+    f = tab.info()["flops_per_turn"]
+    out = {"case": "eic_spin", "particles": n, "variant": spin_variant_name(variant), "ms_per_turn": ms,
+           "particle_turns_per_s": n / (ms * 1e-3), "tflops": f * n / (ms * 1e-3) / 1e12,
+           "alive": int((lt < 0).sum())}
+    print(json.dumps(out))
+    return out
+
+
 def compaction(nseed: int = 64, n: int = 16384, device: int = 0) -> dict:
     """Two turn blocks of one turn each of a batched scan with nseed seeds x n
     Gaussian particles (spread work items of 256, the L1 variant), every
@@ -313,7 +345,8 @@ def contraction(nturn: int = 1000, every: int = 10, n_rate: int = 1 << 20, rate_
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("kind", choices=["spin", "radial", "elements", "contraction", "launch", "compaction"])
+    ap.add_argument("kind", choices=["spin", "radial", "elements", "contraction", "launch", "compaction",
+                                     "spin_launch"])
     ap.add_argument("--case", default="rhic")
     ap.add_argument("--variant", type=int, default=1)
     ap.add_argument("--seeds", type=int, default=16)
@@ -328,6 +361,8 @@ def main(argv=None):
         one_launch(a.case, a.particles, a.variant, a.turns)
     elif a.kind == "compaction":
         compaction(a.seeds, a.particles)
+    elif a.kind == "spin_launch":
+        spin_launch(a.particles, a.variant, a.turns)
     else:
         run(a.kind, a.seeds, a.particles, a.turns)
 
