@@ -468,6 +468,15 @@ int stb_fp64_peak(int device, double *tflops);
  * (device < 0).  mismatch4 receives the counts for pz, 1/pz, betaz, L/betaz. */
 int stb_check_drift_quotients(long n, unsigned long long seed, int device, unsigned long long *mismatch4);
 
+/* Diagnostics: the table-driven fast path of the tracking maps' correctly
+ * rounded sin and cos against their double-double series, over n random
+ * arguments drawn from `seed` (|x| < 800: log-uniform magnitudes, spin
+ * rotation angles, and small offsets from multiples of pi/128), on GPU
+ * `device` or on the host (device < 0).  count4 receives: sin results that
+ * differ, cos results that differ, arguments left to the series among the
+ * generic classes, and among the offsets from multiples of pi/128. */
+int stb_check_sincos(long n, unsigned long long seed, int device, unsigned long long *count4);
+
 #ifdef __cplusplus
 }
 #endif

@@ -147,6 +147,7 @@ SIGNATURES = [
     ("stb_mlp_gemm_test", c_int, [c_void_p, c_int, c_void_p, c_int, c_int, c_int, c_int, c_void_p, c_int, c_int]),
     ("stb_fp64_peak", c_int, [c_int, POINTER(c_double)]),
     ("stb_check_drift_quotients", c_int, [c_long, c_ulonglong, c_int, POINTER(c_ulonglong)]),
+    ("stb_check_sincos", c_int, [c_long, c_ulonglong, c_int, POINTER(c_ulonglong)]),
     ("stb_math_eval", c_int, [c_int, POINTER(c_double), POINTER(c_double), c_long, c_int]),
     ("stb_track_probe", c_int, [c_void_p, POINTER(c_double), c_long, c_int, c_double, POINTER(c_double),
                                 POINTER(c_int), POINTER(c_int), POINTER(c_int)]),

@@ -1129,6 +1129,19 @@ int stb_check_drift_quotients(long n, unsigned long long seed, int device, unsig
   });
 }
 
+int stb_check_sincos(long n, unsigned long long seed, int device, unsigned long long *count4) {
+  return guarded([&] {
+    if (!count4 || n < 0) throw Error(STB_EINVAL, "bad arguments");
+    if (device >= 0) {
+      DeviceGuard g(device);
+      cuda_check(sincos_fast_check(n, seed, device, count4), "sin/cos check");
+    } else {
+      cuda_check(sincos_fast_check(n, seed, -1, count4), "sin/cos check");
+    }
+    return STB_OK;
+  });
+}
+
 int stb_math_eval(int fn, const double *in, double *out, long n, int device) {
   return guarded([&] {
     if (!math_fn_valid(fn)) throw Error(STB_EINVAL, "unknown function code");

@@ -16,8 +16,18 @@
 // asin outside it; cr_exp covers results in the normal range; cr_sin/cr_cos
 // reduce |x| < 2^20.  Outside those domains the CUDA library functions are
 // used (error <= 2 ulp).
+//
+// sin and cos first try a two-step scheme (Ziv's strategy, as in the
+// correctly rounded libraries CRlibm and CORE-MATH): a table-driven
+// approximation with a proven error bound is accepted when that bound
+// decides the rounding, which it does for all but about 2^-15 of the
+// arguments; the others take the double-double series.
 #pragma once
 #include <cmath>
+#include <cstdint>
+#include <cstring>
+
+#include "stb_sincos_table.cuh"
 
 namespace stb {
 
@@ -225,7 +235,118 @@ static __host__ __device__ __noinline__ void cr_sincos_reduced(double x, dd &sr,
   quad = ((int)fmod(k, 4.0) + 4) & 3;
 }
 
+// Table of the fast sin/cos path, [sin(i pi/128) hi, lo, cos(i pi/128) hi,
+// lo] for i = 0..63: one copy in device memory (read through the read-only
+// cache), one for host builds of the same functions.
+__device__ const double kSinCosTabDev[256] = STB_SINCOS_TABLE_INIT;
+static const double kSinCosTabHost[256] = STB_SINCOS_TABLE_INIT;
+
+__host__ __device__ __forceinline__ uint64_t dbl_bits(double v) {
+#ifdef __CUDA_ARCH__
+  return (uint64_t)__double_as_longlong(v);
+#else
+  uint64_t u;
+  memcpy(&u, &v, sizeof u);
+  return u;
+#endif
+}
+__host__ __device__ __forceinline__ double bits_dbl(uint64_t u) {
+#ifdef __CUDA_ARCH__
+  return __longlong_as_double((long long)u);
+#else
+  double v;
+  memcpy(&v, &u, sizeof v);
+  return v;
+#endif
+}
+
+// True when every real number within 2^-70 |y.hi| of y.hi + y.lo rounds to
+// y.hi (y normalised: y.hi = RN(y.hi + y.lo)).  Half the gap to the next
+// double is 2^(e-53) for y.hi in [2^e, 2^(e+1)), half of that below a power
+// of two.  Tiny, zero and non-finite values are left to the slow path.
+__host__ __device__ __forceinline__ bool rounding_decided(dd y) {
+  const uint64_t u = dbl_bits(y.hi);
+  const int e = (int)((u >> 52) & 0x7ff);
+  if (e < 60 || e == 0x7ff) return false;
+  double half = bits_dbl((uint64_t)(e - 53) << 52);
+  if ((u & 0xfffffffffffffull) == 0) half *= 0.5;
+  return fabs(y.lo) + fabs(y.hi) * 0x1p-70 < half;
+}
+
+// Fast path of sin and cos, |x| < 800.  x = k pi/128 + r with the constant
+// in three parts (x - k A is exact, k B is exact, k C is rounded once):
+// |r| <= pi/256 (1 + 2^-30) and r is a double-double with absolute error
+// below 2^-112, i.e. 2^-78 relative when |r| >= 2^-34 (smaller r with
+// k != 0 go to the slow path).  With j = k mod 256, q = j / 64 (the
+// quadrant) and a = (j mod 64) pi/128:
+//   sin(a + r) = S cos r + C sin r,   cos(a + r) = C cos r - S sin r,
+// S, C from the table; cos r - 1 and sin r - r from their Taylor series
+// through r^10 and r^11 (truncation below 2^-100 relative), the leading
+// terms r^2/2 and r^3/6 in double-double, the rest in double (relative error
+// of those tails below 2^-50, i.e. 2^-80 of cos r and sin r).  For a >= pi/128
+// both results are >= sin(pi/256), so the sums do not cancel; for a = 0 the
+// expressions reduce exactly to sin r and cos r.  Each double-double result
+// is within 2^-77 relative of the exact value; rounding_decided() allows
+// 2^-70.  False when it does not decide either rounding.
+__host__ __device__ __forceinline__ bool sincos_fast(double x, double &sn, double &cs) {
+  if (!(fabs(x) < 800.0)) return false;
+  const double k = rint(x * kPi128Inv);
+  dd r = dd_two_sum(fma(-k, kPi128A, x), -k * kPi128B);
+  if (k != 0.0 && !(fabs(r.hi) >= 0x1p-34)) return false;
+  r = dd_fast_two_sum(r.hi, fma(-k, kPi128C, r.lo));
+  const int j = (int)k & 255, i = j & 63;
+#ifdef __CUDA_ARCH__
+  const double *T = kSinCosTabDev + 4 * i;
+  const double Sh = __ldg(T), Sl = __ldg(T + 1), Ch = __ldg(T + 2), Cl = __ldg(T + 3);
+#else
+  const double *T = kSinCosTabHost + 4 * i;
+  const double Sh = T[0], Sl = T[1], Ch = T[2], Cl = T[3];
+#endif
+  // r^2 = t.hi + t.lo
+  dd t = dd_two_prod(r.hi, r.hi);
+  t.lo = fma(r.hi + r.hi, r.lo, t.lo);
+  const double th = t.hi;
+  // cos r = 1 - r^2/2 + r^4 (1/24 - r^2/720 + r^4/40320 - r^6/3628800)
+  const double qc = fma(th, fma(th, fma(th, -1.0 / 3628800.0, 1.0 / 40320.0), -1.0 / 720.0), 1.0 / 24.0);
+  dd cr = dd_fast_two_sum(1.0, -0.5 * th);
+  cr.lo = cr.lo + fma(th * th, qc, -0.5 * t.lo);
+  // sin r = r + r^3 (-1/6 + r^2/120 - r^4/5040 + r^6/362880 - r^8/39916800)
+  const double c1h = -0.16666666666666666, c1l = -9.25185853854297e-18;  // -1/6 = c1h + c1l
+  const double pl =
+      c1l + th * fma(th, fma(th, fma(th, -1.0 / 39916800.0, 1.0 / 362880.0), -1.0 / 5040.0), 1.0 / 120.0);
+  dd rt = dd_two_prod(r.hi, th);  // r^3
+  rt.lo = rt.lo + fma(r.hi, t.lo, r.lo * th);
+  dd sm = dd_two_prod(rt.hi, c1h);
+  sm.lo = sm.lo + fma(rt.hi, pl, rt.lo * c1h);
+  dd sr = dd_fast_two_sum(r.hi, sm.hi);
+  sr.lo = sr.lo + (r.lo + sm.lo);
+  // S cos r + C sin r
+  dd a = dd_two_prod(Sh, cr.hi);
+  a.lo = a.lo + fma(Sh, cr.lo, Sl * cr.hi);
+  dd b = dd_two_prod(Ch, sr.hi);
+  b.lo = b.lo + fma(Ch, sr.lo, Cl * sr.hi);
+  dd s = dd_two_sum(a.hi, b.hi);
+  s = dd_fast_two_sum(s.hi, s.lo + (a.lo + b.lo));
+  // C cos r - S sin r
+  dd c = dd_two_prod(Ch, cr.hi);
+  c.lo = c.lo + fma(Ch, cr.lo, Cl * cr.hi);
+  dd d = dd_two_prod(Sh, sr.hi);
+  d.lo = d.lo + fma(Sh, sr.lo, Sl * sr.hi);
+  dd e = dd_two_sum(c.hi, -d.hi);
+  e = dd_fast_two_sum(e.hi, e.lo + (c.lo - d.lo));
+  if (!(rounding_decided(s) && rounding_decided(e))) return false;
+  const int q = j >> 6;
+  const double sv = s.hi, cv = e.hi;
+  if (q == 0) { sn = sv; cs = cv; }
+  else if (q == 1) { sn = cv; cs = -sv; }
+  else if (q == 2) { sn = -sv; cs = -cv; }
+  else { sn = -cv; cs = sv; }
+  return true;
+}
+
 __host__ __device__ inline double cr_sin(double x) {
+  double fs, fc;
+  if (sincos_fast(x, fs, fc)) return fs;
   if (!(fabs(x) < 1048576.0)) return sin(x);
   dd s, c;
   int q;
@@ -236,8 +357,9 @@ __host__ __device__ inline double cr_sin(double x) {
   return -(c.hi + c.lo);
 }
 
-// sin and cos of the same argument from one reduction.
-__host__ __device__ inline void cr_sincos(double x, double &sn, double &cs) {
+// sin and cos of the same argument from one reduction, by the double-double
+// series alone.
+__host__ __device__ inline void cr_sincos_series(double x, double &sn, double &cs) {
   if (!(fabs(x) < 1048576.0)) {
     sn = sin(x);
     cs = cos(x);
@@ -253,7 +375,14 @@ __host__ __device__ inline void cr_sincos(double x, double &sn, double &cs) {
   else { sn = -cv; cs = sv; }
 }
 
+__host__ __device__ inline void cr_sincos(double x, double &sn, double &cs) {
+  if (sincos_fast(x, sn, cs)) return;
+  cr_sincos_series(x, sn, cs);
+}
+
 __host__ __device__ inline double cr_cos(double x) {
+  double fs, fc;
+  if (sincos_fast(x, fs, fc)) return fc;
   if (!(fabs(x) < 1048576.0)) return cos(x);
   dd s, c;
   int q;

@@ -99,14 +99,56 @@ __global__ void drift_check_kernel(uint64_t seed, long n, unsigned long long *ba
     if (loc[k]) atomicAdd(bad + k, loc[k]);
 }
 
-}  // namespace
+// Random sin/cos arguments: log-uniform magnitudes in [2^-40, 800]; uniform
+// in [-pi, pi] (spin rotation angles); uniform in [-pi/256, pi/256] (the
+// table's first interval); and multiples k pi/128 (|k| <= 32000) offset by a
+// log-uniform amount in [2^-40, 2^-6] (small reduced arguments).  Counts:
+// sin and cos of the fast path that differ from the double-double series,
+// arguments the fast path leaves to the series among the first three
+// classes, and among the last.
+__host__ __device__ inline void sincos_check_one(uint64_t seed, uint64_t i, unsigned long long *cnt) {
+  const double u = unif(seed, i, 0), sgn = unif(seed, i, 1) < 0.5 ? -1.0 : 1.0;
+  double x;
+  int cls;
+  if (u < 0.4) {
+    x = sgn * exp2(-40.0 + (40.0 + 9.64) * unif(seed, i, 2));
+    cls = 0;
+  } else if (u < 0.7) {
+    x = sgn * 3.141592653589793 * unif(seed, i, 2);
+    cls = 0;
+  } else if (u < 0.8) {
+    x = sgn * 0.01227184630308513 * unif(seed, i, 2);
+    cls = 0;
+  } else {
+    const double k = floor(32001.0 * unif(seed, i, 2));
+    x = sgn * (k * 0.02454369260617026 + exp2(-40.0 + 34.0 * unif(seed, i, 3)) * (unif(seed, i, 4) - 0.5));
+    cls = 1;
+  }
+  if (!(fabs(x) < 800.0)) x = 799.0 * sgn;
+  double fs, fc, ss, sc;
+  cr_sincos_series(x, ss, sc);
+  if (sincos_fast(x, fs, fc)) {
+    if (fs != ss) cnt[0]++;
+    if (fc != sc) cnt[1]++;
+  } else {
+    cnt[2 + cls]++;
+  }
+}
 
-// Mismatch counts of the drift quotients against IEEE sqrt and division over
-// n random drift arguments, on `device` (or the host for device < 0).
-cudaError_t drift_quotient_check(long n, unsigned long long seed, int device, unsigned long long *bad4) {
-  for (int k = 0; k < 4; k++) bad4[k] = 0;
+__global__ void sincos_check_kernel(uint64_t seed, long n, unsigned long long *cnt) {
+  unsigned long long loc[4] = {0, 0, 0, 0};
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+    sincos_check_one(seed, (uint64_t)i, loc);
+  for (int k = 0; k < 4; k++)
+    if (loc[k]) atomicAdd(cnt + k, loc[k]);
+}
+
+template <class One>
+cudaError_t run_check(long n, unsigned long long seed, int device, unsigned long long *cnt4, One one,
+                      void (*kern)(uint64_t, long, unsigned long long *)) {
+  for (int k = 0; k < 4; k++) cnt4[k] = 0;
   if (device < 0) {
-    for (long i = 0; i < n; i++) drift_check_one(seed, (uint64_t)i, bad4);
+    for (long i = 0; i < n; i++) one(seed, (uint64_t)i, cnt4);
     return cudaSuccess;
   }
   unsigned long long *d = nullptr;
@@ -115,11 +157,28 @@ cudaError_t drift_quotient_check(long n, unsigned long long seed, int device, un
   cudaMemset(d, 0, 4 * sizeof(unsigned long long));
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-  drift_check_kernel<<<sms * 8, 256>>>(seed, n, d);
+  kern<<<sms * 8, 256>>>(seed, n, d);
   e = cudaGetLastError();
-  if (e == cudaSuccess) e = cudaMemcpy(bad4, d, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(cnt4, d, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost);
   cudaFree(d);
   return e;
+}
+
+}  // namespace
+
+// Fast sin/cos path against the double-double series over n random
+// arguments, on `device` (or the host for device < 0); counts as in
+// sincos_check_one.
+cudaError_t sincos_fast_check(long n, unsigned long long seed, int device, unsigned long long *cnt4) {
+  return run_check(n, seed, device, cnt4, [](uint64_t s, uint64_t i, unsigned long long *c) { sincos_check_one(s, i, c); },
+                   sincos_check_kernel);
+}
+
+// Mismatch counts of the drift quotients against IEEE sqrt and division over
+// n random drift arguments, on `device` (or the host for device < 0).
+cudaError_t drift_quotient_check(long n, unsigned long long seed, int device, unsigned long long *bad4) {
+  return run_check(n, seed, device, bad4, [](uint64_t s, uint64_t i, unsigned long long *c) { drift_check_one(s, i, c); },
+                   drift_check_kernel);
 }
 
 // Measured FP64 FMA peak of `device` in TFLOP/s (2 flops per FMA).

@@ -83,6 +83,7 @@ cudaError_t math_eval_device(int fn, const double *d_in, double *d_out, long n, 
 void math_eval_host(int fn, const double *in, double *out, long n);
 cudaError_t fp64_peak_probe(int device, double *tflops);
 cudaError_t drift_quotient_check(long n, unsigned long long seed, int device, unsigned long long *bad4);
+cudaError_t sincos_fast_check(long n, unsigned long long seed, int device, unsigned long long *cnt4);
 
 size_t track_smem_bytes(int nelem, int npool_padded);
 // The loss-test mode of a launch with circular aperture r2 (+inf: none) on a

@@ -207,3 +207,42 @@ def test_drift_quotients_equal_ieee_on_the_gpu(native_lib):
     -fmad=false unit)."""
     for seed in (1, 2):
         assert _drift_check(native_lib, 1_000_000_000, seed, 0) == [0, 0, 0, 0]
+
+
+def _sincos_check(native_lib, n, seed, device):
+    from ctypes import c_ulonglong
+    cnt = (c_ulonglong * 4)()
+    assert native_lib.stb_check_sincos(n, seed, device, cnt) == 0
+    return list(cnt)
+
+
+def test_sincos_fast_path_equals_series_on_the_host(native_lib):
+    """The table-driven fast path of sin/cos (rounding decided by a proven
+    error bound) returns the double-double series' values whenever it
+    answers, and leaves few arguments to the series (host build)."""
+    n = 2_000_000
+    ds, dc, slow, slow_near = _sincos_check(native_lib, n, 7, -1)
+    assert (ds, dc) == (0, 0)
+    assert slow < 1e-3 * n  # expected about 2^-15 of the generic arguments
+    assert slow_near < 0.1 * n  # offsets below 2^-34 from k pi/128 always take the series
+
+
+def test_sincos_table_header_is_current():
+    """stb_sincos_table.cuh is what its generator writes (mpmath constants)."""
+    import importlib.util
+    from pathlib import Path
+    csrc = Path(__file__).resolve().parents[1] / "simtrack_b200" / "csrc"
+    spec = importlib.util.spec_from_file_location("gen_sincos_table", csrc / "gen_sincos_table.py")
+    gen = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(gen)
+    assert (csrc / "stb_sincos_table.cuh").read_text() == gen.text()
+
+
+@pytest.mark.gpu
+def test_sincos_fast_path_equals_series_on_the_gpu(native_lib):
+    """The same on the GPU over 1e9 arguments (device code, -fmad=false unit)."""
+    n = 500_000_000
+    for seed in (1, 2):
+        ds, dc, slow, slow_near = _sincos_check(native_lib, n, seed, 0)
+        assert (ds, dc) == (0, 0)
+        assert slow < 1e-3 * n
