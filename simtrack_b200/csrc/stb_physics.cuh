@@ -184,7 +184,7 @@ __device__ __forceinline__ void bend_exact(Particle &p, const PtCache &c, const 
 
 // general_sbend_exact_pass, simtrack.cpp:3974-4010.
 // G = [L, L/beta, rhoc, b0, b0*rhoc, cosA, sinA, 1/rhoc, 1/b0]
-static __device__ __noinline__ void gbend_exact(Particle &p, const PtCache &c, const double *G) {
+static __device__ __forceinline__ void gbend_exact(Particle &p, const PtCache &c, const double *G) {
   const double L = G[0], Lb = G[1], rhoc = G[2], b0 = G[3], b0r = G[4], cosA = G[5], sinA = G[6];
   const double irhoc = G[7], ib0 = G[8];
   const double x0 = p.x, px0 = p.px, py0 = p.py;
@@ -256,7 +256,7 @@ __device__ __forceinline__ void mult_kick(Particle &p, int norder, const double 
 }
 
 // Hard-edge quadrupole fringe maps, simtrack.cpp:4906-4920 (entry) and 4948-4956 (exit).
-static __device__ __noinline__ void quad_fringe(Particle &p, double k, bool entry) {
+static __device__ __forceinline__ void quad_fringe(Particle &p, double k, bool entry) {
   const double x0 = p.x, px0 = p.px, y0 = p.y, py0 = p.py, z0 = p.z, d0 = p.pt;
   const double a = k * (x0 * x0 * x0 + 3 * x0 * y0 * y0) / 12 / (1 + d0);
   const double b = k * ((x0 * x0 + y0 * y0) * px0 - 2 * x0 * y0 * py0) / 4 / (1 + d0);
@@ -305,7 +305,7 @@ __device__ __forceinline__ void ltog1(Particle &p, const double *M, int flags) {
 // rx[n], ry[n] for n = nu..1 and then consumes them for n = nc..1 with
 // nc < nu; both loops run downwards, so the two are fused here and the
 // arrays are not materialised.  Values are unchanged.
-static __device__ __noinline__ void cerrf_dev(double xx, double yy, double &wx, double &wy) {
+static __device__ __forceinline__ void cerrf_dev(double xx, double yy, double &wx, double &wy) {
   const double cc = 1.12837916709551, xlim = 5.33, ylim = 4.29, fac1 = 3.2, fac2 = 23, fac3 = 21;
   const double x = fabs(xx), y = fabs(yy);
   if (y < ylim && x < xlim) {
@@ -402,7 +402,7 @@ __device__ __forceinline__ void bb4d(double x, double y, double c4, double sigma
 // BB6D, simtrack.cpp:6622-6677 (slice loop).  P layout (built by the flattener):
 // [bbscale, emitx, emity, betax*, alfx*, betay*, alfy*, gx*, gy*, 2*emitx, 2*emity,
 //  temp3, c4, z_star[0..N-1]]
-static __device__ __noinline__ void bb6d(Particle &p, const double *P, int nslice) {
+static __device__ __forceinline__ void bb6d(Particle &p, const double *P, int nslice) {
   const double bbscale = P[0], emitx = P[1], emity = P[2];
   const double betax_s = P[3], alfx_s = P[4], betay_s = P[5], alfy_s = P[6];
   const double gx = P[7], gy = P[8], e2x = P[9], e2y = P[10], t3 = P[11], c4 = P[12];
@@ -440,7 +440,7 @@ static __device__ __noinline__ void bb6d(Particle &p, const double *P, int nslic
 }
 
 // LBT_Pass, simtrack.cpp:6069-6093.  P = [sin, cos, tan]
-static __device__ __noinline__ void lbt(Particle &p, const double *P) {
+static __device__ __forceinline__ void lbt(Particle &p, const double *P) {
   const double st = P[0], ct = P[1], tt = P[2];
   const double x0 = p.x, px0 = p.px, y0 = p.y, py0 = p.py, z0 = p.z, pz0 = p.pt;
   const double ps0 = sqrt((1 + pz0) * (1 + pz0) - px0 * px0 - py0 * py0);
@@ -459,7 +459,7 @@ static __device__ __noinline__ void lbt(Particle &p, const double *P) {
 }
 
 // ILBT_Pass, simtrack.cpp:6095-6123.  P = [sin, cos]
-static __device__ __noinline__ void ilbt(Particle &p, const double *P) {
+static __device__ __forceinline__ void ilbt(Particle &p, const double *P) {
   const double st = P[0], ct = P[1];
   const double xs = p.x, pxs = p.px, ys = p.y, pys = p.py, zs = p.z, pzs = p.pt;
   const double pss = sqrt((1 + pzs) * (1 + pzs) - pxs * pxs - pys * pys);
@@ -476,7 +476,7 @@ static __device__ __noinline__ void ilbt(Particle &p, const double *P) {
 
 // CCMULT_Pass kick part, simtrack.cpp:6037-6064.
 // P = [kf, PHASE0, scale, brho, B2, A2, B3, A3, B4, A4, B5, A5]
-static __device__ __noinline__ void ccmult_kick(Particle &p, const double *P) {
+static __device__ __forceinline__ void ccmult_kick(Particle &p, const double *P) {
   const double kf = P[0], PHASE0 = P[1], scale = P[2], brho = P[3];
   const double B2 = P[4], A2 = P[5], B3 = P[6], A3 = P[7], B4 = P[8], A4 = P[9], B5 = P[10], A5 = P[11];
   const double arg = kf * p.z / 2.99792458e8 + PHASE0;
