@@ -179,13 +179,12 @@ int stb_track_host(stb_table *t, double *x, long n, int nturn, double aperture_r
  * STB_EINVAL): for callers whose device memory belongs to another allocator's
  * pool, or which must not call cudaMalloc/cudaFree (they synchronise the
  * device) between their own kernels.  Each call rewrites the whole scratch
- * before use.  The first call on a device looks the scratch up
- * (cudaGetSymbolAddress); make it before any stream capture begins on that
- * device.  Calls that overlap in time on one device race on the shared
- * scratch.  Every call reads its status word back and waits for `stream`
- * before returning.  The looked-up address lives as long as the CUDA
- * context: after cudaDeviceReset no handle of this library (tables, scans,
- * this scratch) may be used again. */
+ * before use; every call looks the scratch up (cudaGetSymbolAddress,
+ * no allocation).  Never call it while `stream` or its device is being
+ * captured into a CUDA graph: it copies its status word back and waits for
+ * `stream` before returning.  Calls that overlap in time on one device race
+ * on the shared scratch.  Tables are handles of one CUDA context: after
+ * cudaDeviceReset they may not be used again. */
 #define STB_STATIC_MAX_SEEDS 64
 #define STB_STATIC_MAX_PARTICLES 1048576
 int stb_track_seeds_static(stb_table *const *tables, int nseed, const long *n_per_seed, double *x, double *px,

@@ -8,8 +8,9 @@
 // table, per-seed particle counts, the work list, its counters and the status
 // word sit in g_static_scratch; the particles stay in the caller's buffers.
 //
-// The first call on a device looks up the scratch address
-// (cudaGetSymbolAddress); later calls reuse it.  The scratch is shared by all
+// Every call looks up the scratch address (cudaGetSymbolAddress, which
+// allocates nothing), so the entry point stays valid after a
+// cudaDeviceReset reloads the module.  The scratch is shared by all
 // calls on a device, so calls that overlap in time on one device (several
 // host threads, or several streams without ordering between them) race on it.
 // Each call waits for its stream before returning, so sequential calls from
@@ -19,7 +20,6 @@
 #include <algorithm>
 #include <cstdint>
 #include <cstring>
-#include <mutex>
 #include <string>
 
 #include "stb_runtime.hpp"
@@ -73,17 +73,11 @@ __global__ void static_init_kernel(const __grid_constant__ StaticInit in, Static
   }
 }
 
-std::mutex g_mu;
-StaticScratch *g_scratch[kMaxDevices] = {};
-
-StaticScratch *scratch_for(int device) {
-  std::lock_guard<std::mutex> lk(g_mu);
-  if (!g_scratch[device]) {
-    void *p = nullptr;
-    cuda_check(cudaGetSymbolAddress(&p, g_static_scratch), "cudaGetSymbolAddress(scratch)");
-    g_scratch[device] = static_cast<StaticScratch *>(p);
-  }
-  return g_scratch[device];
+// The scratch of the current device.
+StaticScratch *scratch_for() {
+  void *p = nullptr;
+  cuda_check(cudaGetSymbolAddress(&p, g_static_scratch), "cudaGetSymbolAddress(scratch)");
+  return static_cast<StaticScratch *>(p);
 }
 
 int track_seeds_static(stb_table *const *tables, int nseed, const long *n_per_seed, double *x, double *px,
@@ -125,7 +119,7 @@ int track_seeds_static(stb_table *const *tables, int nseed, const long *n_per_se
   in.nseed = nseed;
   in.turn0 = turn0;
   DeviceGuard g(device);
-  StaticScratch *sc = scratch_for(device);
+  StaticScratch *sc = scratch_for();
   const int variant = smem_ok ? 0 : 2;
   // Raise (never lower) the kernel's shared-memory limit to the device maximum,
   // so that handles prepared with other table sizes keep working.
