@@ -45,8 +45,22 @@ int stb_version(void);
 int stb_set_ref_energy(double gamma, double E0, double Q, double A);
 /* Set_Spin_G(g)  simtrack.cpp:110-115 */
 int stb_set_spin_g(double g);
-/* GP.H_expand, GP.quad_fringe  simtrack.h:62-66 (GP.radiate is not supported) */
+/* GP.H_expand, GP.quad_fringe  simtrack.h:62-66 (GP.radiate: stb_set_radiation) */
 int stb_set_flags(int h_expand, int quad_fringe);
+
+/* GP.radiate (simtrack.h:57): synchrotron radiation in the sector bends
+ * (SBEND_Pass's radiating branch, simtrack.cpp:4740-4748: radiate1 with
+ * quantum excitation after each of the Nint slices) and in GMULT/SBENDMULT
+ * (5312-5338, 5437-5463: radiate after each slice), for tables created after
+ * the call.  The reference draws the quantum-excitation deviates from GSL's
+ * sequential stream (gsl_ran_gaussian on gsl_r2, seeded 1324 in
+ * Init_GSL_Seeds, 317-329); here the k-th deviate of particle i (its index in
+ * the arrays of the Track call, k counting its radiating slices from turn 0)
+ * is a function of (seed, i, k): Philox4x32-10 and Box-Muller, the same on
+ * every launch shape.  Radiating tables are tracked by the stb_track_* entry
+ * points (not the scan, Track_Radial, spin or static ones); GSBEND's photon
+ * Monte Carlo (radiate2) is not implemented (STB_EUNSUPPORTED). */
+int stb_set_radiation(int radiate, unsigned long long seed);
 /* out[0..7] = GP.gamma, GP.beta, GP.energy, GP.brho, GP.Q, GP.energy0, GP.G, GP.p */
 int stb_get_ref(double *out8);
 
@@ -475,6 +489,16 @@ int stb_check_drift_quotients(long n, unsigned long long seed, int device, unsig
  * differ, cos results that differ, arguments left to the series among the
  * generic classes, and among the offsets from multiples of pi/128. */
 int stb_check_sincos(long n, unsigned long long seed, int device, unsigned long long *count4);
+
+/* Diagnostics: deviates k0 .. k0+n-1 of particle `id`'s quantum-excitation
+ * stream under `seed` (see stb_set_radiation), evaluated on GPU `device` or
+ * on the host (device < 0); out is host memory. */
+int stb_rad_normals(unsigned long long seed, unsigned long long id, unsigned long long k0, long n, double *out,
+                    int device);
+
+/* Diagnostics: one Philox4x32-10 block (the stream's generator), for its
+ * published known-answer vectors. */
+int stb_philox4x32_10(const unsigned int ctr[4], const unsigned int key[2], unsigned int out[4]);
 
 #ifdef __cplusplus
 }

@@ -16,6 +16,8 @@
 //   ref_track_dump  -> the Track() loop that also records all six
 //                      coordinates after every element (the per-element
 //                      parity probe).
+//   ref_set_radiation -> GP.radiate, with the deviates radiate1 draws from
+//                      GSL supplied by the stream below.
 // Nothing in the product links or loads this file.
 #include "simtrack.h"
 
@@ -23,6 +25,7 @@
 #include <cstring>
 #include <vector>
 #include <cmath>
+#include <cstdint>
 
 extern GlobalVariables GP;
 extern double tune_low, tune_high;
@@ -81,7 +84,71 @@ inline bool circ_lost(const double *x, double r2) {
   return r2 > 0.0 && x[0] * x[0] + x[2] * x[2] > r2;
 }
 
+// Normal deviates for the reference's radiate1 (gsl_ran_gaussian, reached
+// through the GSL shim).  GSL is absent, so the stream is the tracker's
+// definition, restated here independently: the k-th deviate of particle id
+// under seed is Philox4x32-10 (Salmon et al., SC'11; counter (k, id), key
+// seed) -> two 53-bit uniforms in (0, 1] -> Box-Muller with a natural log
+// made of basic operations (ln m = 2 atanh((m-1)/(m+1)), series through the
+// 23rd power) and the library cos (correctly rounded in libsimtrack_ref_cr).
+// k counts the particle's calls from the start of its tracking.
+unsigned long long g_rng_seed = 1324;
+long g_rng_base = 0, g_rng_id = 0;
+unsigned long long g_rng_k = 0;
+
+void rng_particle(long id) {
+  g_rng_id = id;
+  g_rng_k = 0;
+}
+
+void philox10(uint32_t ctr[4], uint32_t key0, uint32_t key1) {
+  for (int round = 0; round < 10; round++) {
+    if (round) {
+      key0 += 0x9E3779B9u;
+      key1 += 0xBB67AE85u;
+    }
+    const uint64_t m0 = (uint64_t)ctr[0] * 0xD2511F53u;
+    const uint64_t m1 = (uint64_t)ctr[2] * 0xCD9E8D57u;
+    const uint32_t n0 = (uint32_t)(m1 >> 32) ^ ctr[1] ^ key0;
+    const uint32_t n2 = (uint32_t)(m0 >> 32) ^ ctr[3] ^ key1;
+    ctr[0] = n0;
+    ctr[1] = (uint32_t)m1;
+    ctr[2] = n2;
+    ctr[3] = (uint32_t)m0;
+  }
+}
+
+double series_log(double x) {
+  uint64_t bits;
+  std::memcpy(&bits, &x, 8);
+  int ex = (int)((bits >> 52) & 0x7ff) - 1023;
+  bits = (bits & 0x000fffffffffffffull) | 0x3ff0000000000000ull;
+  double m;
+  std::memcpy(&m, &bits, 8);
+  if (m > 1.4142135623730951) {
+    m = m * 0.5;
+    ex = ex + 1;
+  }
+  const double s = (m - 1.0) / (m + 1.0);
+  const double s2 = s * s;
+  double acc = 1.0 / 23.0;
+  for (int odd = 21; odd >= 3; odd -= 2) acc = acc * s2 + 1.0 / (double)odd;
+  const double lnm = 2.0 * s + 2.0 * s * (s2 * acc);
+  return (double)ex * 0.6931471805599453094 + ((double)ex * 2.319046813846299558e-17 + lnm);
+}
+
+double stream_gaussian(unsigned long long seed, unsigned long long id, unsigned long long k) {
+  uint32_t c[4] = {(uint32_t)k, (uint32_t)(k >> 32), (uint32_t)id, (uint32_t)(id >> 32)};
+  philox10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+  const uint64_t w1 = ((uint64_t)c[0] << 32) | c[1], w2 = ((uint64_t)c[2] << 32) | c[3];
+  const double u1 = (double)((w1 >> 11) + 1) * (1.0 / 9007199254740992.0);
+  const double u2 = (double)((w2 >> 11) + 1) * (1.0 / 9007199254740992.0);
+  return std::sqrt(-2.0 * series_log(u1)) * std::cos(6.283185307179586 * u2);
+}
+
 }  // namespace
+
+extern "C" double ref_rng_gaussian(void) { return stream_gaussian(g_rng_seed, (unsigned long long)g_rng_id, g_rng_k++); }
 
 extern "C" {
 
@@ -95,6 +162,19 @@ void ref_set_flags(int h_expand, int quad_fringe) {
   GP.H_expand = h_expand != 0;
   GP.quad_fringe = quad_fringe != 0;
   GP.radiate = false;
+}
+
+// GP.radiate and the seed of the deviate stream (ref_set_flags clears
+// GP.radiate).  Particle i of a ref_track / ref_track_circ call, and the one
+// particle of ref_track_dump, draws as stream id base + i.
+void ref_set_radiation(int radiate, unsigned long long seed) {
+  GP.radiate = radiate != 0;
+  g_rng_seed = seed;
+}
+void ref_rng_id_base(long base) { g_rng_base = base; }
+// Deviate k of stream `id` under `seed` (the stream's own check).
+double ref_rng_stream(unsigned long long seed, unsigned long long id, unsigned long long k) {
+  return stream_gaussian(seed, id, k);
 }
 
 // gamma, beta, energy, brho, Q, energy0, G
@@ -225,6 +305,7 @@ void ref_track(void *line, double *x, long n, int nturn, int *stable, int *lost_
   Line &l = *static_cast<Line *>(line);
   for (long i = 0; i < n; i++) {
     int st = stable[i], lt = 0, lp = 0;
+    rng_particle(g_rng_base + i);
     Track(l, x + 6 * i, nturn, st, lt, lp);
     stable[i] = st; lost_turn[i] = lt; lost_post[i] = lp;
   }
@@ -305,6 +386,7 @@ void ref_track_circ(void *line, double *x, long n, int nturn, double radius, int
   for (long i = 0; i < n; i++) {
     double *xi = x + 6 * i;
     stable[i] = 1; lost_turn[i] = 0; lost_post[i] = 0;
+    rng_particle(g_rng_base + i);
     if (std::abs(xi[0]) > 0.1 || std::abs(xi[2]) > 0.1) { stable[i] = 0; continue; }
     bool lost = false;
     for (GP.turn = 0; GP.turn < nturn && !lost; GP.turn++) {
@@ -327,6 +409,7 @@ void ref_track_dump(void *line, double *x, int nturn, double radius, double *dum
   Line &l = *static_cast<Line *>(line);
   const double r2 = radius > 0.0 ? radius * radius : 0.0;
   *stable = 1; *lost_turn = 0; *lost_post = 0;
+  rng_particle(g_rng_base);
   if (std::abs(x[0]) > 0.1 || std::abs(x[2]) > 0.1) { *stable = 0; return; }
   for (GP.turn = 0; GP.turn < nturn; GP.turn++) {
     for (long j = 0; j < l.Ncell; j++) {

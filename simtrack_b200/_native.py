@@ -37,6 +37,7 @@ SIGNATURES = [
     ("stb_set_ref_energy", c_int, [c_double, c_double, c_double, c_double]),
     ("stb_set_spin_g", c_int, [c_double]),
     ("stb_set_flags", c_int, [c_int, c_int]),
+    ("stb_set_radiation", c_int, [c_int, c_ulonglong]),
     ("stb_get_ref", c_int, [POINTER(c_double)]),
     ("stb_element_new", c_int, [c_char_p, c_char_p, POINTER(c_double), c_int, POINTER(c_void_p)]),
     ("stb_element_free", c_int, [c_void_p]),
@@ -148,6 +149,8 @@ SIGNATURES = [
     ("stb_fp64_peak", c_int, [c_int, POINTER(c_double)]),
     ("stb_check_drift_quotients", c_int, [c_long, c_ulonglong, c_int, POINTER(c_ulonglong)]),
     ("stb_check_sincos", c_int, [c_long, c_ulonglong, c_int, POINTER(c_ulonglong)]),
+    ("stb_rad_normals", c_int, [c_ulonglong, c_ulonglong, c_ulonglong, c_long, POINTER(c_double), c_int]),
+    ("stb_philox4x32_10", c_int, [POINTER(ctypes.c_uint), POINTER(ctypes.c_uint), POINTER(ctypes.c_uint)]),
     ("stb_math_eval", c_int, [c_int, POINTER(c_double), POINTER(c_double), c_long, c_int]),
     ("stb_track_probe", c_int, [c_void_p, POINTER(c_double), c_long, c_int, c_double, POINTER(c_double),
                                 POINTER(c_int), POINTER(c_int), POINTER(c_int)]),

@@ -39,6 +39,14 @@ def Set_Flags(h_expand: bool = False, quad_fringe: bool = False) -> None:
     check(lib().stb_set_flags(int(h_expand), int(quad_fringe)))
 
 
+def Set_Radiation(radiate: bool = False, seed: int = 1324) -> None:
+    """GP.radiate (simtrack.h:57) for tables created afterwards: radiation in
+    the sector bends (radiate1, with quantum excitation) and GMULT/SBENDMULT
+    (radiate).  `seed` keys the quantum-excitation deviates (the reference
+    seeds its GSL stream with 1324, simtrack.cpp:328)."""
+    check(lib().stb_set_radiation(int(radiate), int(seed)))
+
+
 def GP() -> dict:
     """Snapshot of the reference-particle globals."""
     out = (c_double * 8)()

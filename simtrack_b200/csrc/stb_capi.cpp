@@ -371,6 +371,8 @@ int radial_device(stb_table *t, double *x, double *px, double *y, double *py, do
                   double *dump = nullptr) {
   if (!t) throw Error(STB_EINVAL, "table is NULL");
   if (t->host.spin) throw Error(STB_EINVAL, "table is flattened for spin tracking");
+  if (t->host.radiate)
+    throw Error(STB_EUNSUPPORTED, "Track_Radial of a table flattened with GP.radiate is not implemented");
   if (n < 0 || nturn < 0 || turn0 < 0) throw Error(STB_EINVAL, "negative particle count or turn");
   if (n == 0 || nturn == 0) return STB_OK;
   if (!x || !px || !y || !py || !z || !pt || !lost_turn || !lost_elem)
@@ -655,6 +657,13 @@ int stb_set_flags(int h_expand, int quad_fringe) {
   return guarded([&] {
     GP.H_expand = h_expand != 0;
     GP.quad_fringe = quad_fringe != 0;
+    return STB_OK;
+  });
+}
+int stb_set_radiation(int radiate, unsigned long long seed) {
+  return guarded([&] {
+    GP.radiate = radiate != 0;
+    set_radiation_seed(seed);
     return STB_OK;
   });
 }
@@ -1138,6 +1147,32 @@ int stb_check_sincos(long n, unsigned long long seed, int device, unsigned long 
     } else {
       cuda_check(sincos_fast_check(n, seed, -1, count4), "sin/cos check");
     }
+    return STB_OK;
+  });
+}
+
+int stb_rad_normals(unsigned long long seed, unsigned long long id, unsigned long long k0, long n, double *out,
+                    int device) {
+  return guarded([&] {
+    if (n < 0 || (n > 0 && !out)) throw Error(STB_EINVAL, "bad buffers");
+    if (device >= 0) {
+      DeviceGuard g(device);
+      double *d = nullptr;
+      cuda_check(cudaMalloc(&d, sizeof(double) * (size_t)(n > 0 ? n : 1)), "cudaMalloc(deviates)");
+      DevFree f{d};
+      cuda_check(rad_normals(seed, id, k0, n, d, device), "deviate kernel");
+      cuda_check(cudaMemcpy(out, d, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost), "download deviates");
+    } else {
+      cuda_check(rad_normals(seed, id, k0, n, out, -1), "deviates");
+    }
+    return STB_OK;
+  });
+}
+
+int stb_philox4x32_10(const unsigned int ctr[4], const unsigned int key[2], unsigned int out[4]) {
+  return guarded([&] {
+    if (!ctr || !key || !out) throw Error(STB_EINVAL, "NULL argument");
+    philox_block(ctr, key, out);
     return STB_OK;
   });
 }

@@ -7,6 +7,7 @@
 #include "stb_crmath.cuh"
 #include "stb_kernels.hpp"
 #include "stb_physics.cuh"
+#include "stb_rng.cuh"
 
 namespace stb {
 
@@ -164,7 +165,32 @@ cudaError_t run_check(long n, unsigned long long seed, int device, unsigned long
   return e;
 }
 
+__global__ void rad_normals_kernel(uint64_t seed, uint64_t id, uint64_t k0, long n, double *out) {
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+    out[i] = rad_gaussian(seed, id, k0 + (uint64_t)i);
+}
+
 }  // namespace
+
+// Deviates k0 .. k0+n-1 of particle `id`'s quantum-excitation stream, on
+// `device` (out in device memory) or on the host (device < 0).
+cudaError_t rad_normals(unsigned long long seed, unsigned long long id, unsigned long long k0, long n, double *out,
+                        int device) {
+  if (device < 0) {
+    for (long i = 0; i < n; i++) out[i] = rad_gaussian(seed, id, k0 + (uint64_t)i);
+    return cudaSuccess;
+  }
+  if (n <= 0) return cudaSuccess;
+  long grid = (n + 255) / 256;
+  if (grid > 4096) grid = 4096;
+  rad_normals_kernel<<<(unsigned)grid, 256>>>(seed, id, k0, n, out);
+  return cudaGetLastError();
+}
+
+void philox_block(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]) {
+  const Philox4 r = philox4x32_10(Philox4{{ctr[0], ctr[1], ctr[2], ctr[3]}}, key[0], key[1]);
+  for (int i = 0; i < 4; i++) out[i] = r.v[i];
+}
 
 // Fast sin/cos path against the double-double series over n random
 // arguments, on `device` (or the host for device < 0); counts as in

@@ -147,6 +147,12 @@ const double kFlSpin = 110;
 
 // One solenoid slice with its entry and exit conversions (SOLEN_Pass).
 const double kFlSolen = 76;
+// radiate(): pz, the direction cosines, the cross product, the pt update,
+// delta2 and the momentum rescaling, plus the pt-cache refresh it forces;
+// radiate1() adds the fluctuation term and its normal deviate (ln and cos
+// counted 1 each).
+const double kFlRadiate = 50 + kFlPtRefresh;
+const double kFlQuantum = 25;
 
 // Parameters of SOLEN_Pass / SOLEN_sPass for KS != 0 (simtrack.cpp:5804-5857,
 // 8118-8183): Bz is KS*brho in Pass and KS*brho/L in sPass.  The solenoid's
@@ -338,9 +344,12 @@ bool spin_form(Builder &B, const Element &E, ElemHeader &h, double &fl) {
   return false;
 }
 
+unsigned long long g_radiation_seed = 1324;
+
 HostTable flatten_impl(const Line &line, bool spin) {
   if (GP.H_expand) throw Error(STB_EUNSUPPORTED, "GP.H_expand == true is not implemented on the GPU path");
-  if (GP.radiate) throw Error(STB_EUNSUPPORTED, "GP.radiate == true is not implemented on the GPU path");
+  if (GP.radiate && spin)
+    throw Error(STB_EUNSUPPORTED, "GP.radiate == true is not implemented for spin tracking on the GPU path");
   Builder B;
   HostTable &t = B.t;
   t.ref.gamma = GP.gamma;
@@ -351,6 +360,13 @@ HostTable flatten_impl(const Line &line, bool spin) {
   t.ref.G = GP.G;
   t.ref.ibeta = 1.0 / GP.beta;
   t.ref.ienergy = 1.0 / GP.energy;
+  t.ref.rad_seed = radiation_seed();
+  t.ref.rad_slices = 0;
+  t.radiate = GP.radiate;
+  // radiate()/radiate1() constants: pow(GP.energy/1000., 3) (simtrack.cpp:4224)
+  // and Cf (simtrack.cpp:26), with the reference's expressions
+  const double rad_E3 = std::pow(GP.energy / 1000., 3);
+  const double rad_Cf = (55. / 24. / std::sqrt(3.)) * 2.8179403e-15 * 1.054572e-34 / 9.1093822e-31;
   t.flops_per_turn = kFlPtRefresh;  // turn-start evaluation of the pt cache
   t.spin = spin;
   const Yoshida &Y = B.y;
@@ -431,6 +447,28 @@ HostTable flatten_impl(const Line &line, bool spin) {
       const double L = E.L, Angle = E.GetP("ANGLE"), E1 = E.GetP("E1"), E2 = E.GetP("E2");
       if (Angle == 0.) {
         as_drift(L);
+      } else if (GP.radiate) {
+        // radiating exact branch, simtrack.cpp:4740-4748
+        const int Nint = (int)E.GetP("Nint");
+        if (Nint <= 0) throw Error(STB_EINVAL, "element " + E.NAME + ": Nint must be positive");
+        const double href = Angle / L, Lint = L / Nint, an = Angle / Nint;
+        h.op = OP_SBEND_RAD;
+        h.nint = Nint;
+        h.flags |= EF_CHANGES_PT;
+        B.push(std::tan(E1) * href);
+        B.push(std::tan(E2) * href);
+        B.bend_params(Lint, an, std::cos(an), std::sin(an));
+        B.push(Lint);
+        B.push(href);
+        B.push(an);
+        B.push(rad_E3);
+        B.push(rad_Cf);
+        B.push((double)t.ref.rad_slices);
+        t.ref.rad_slices += Nint;
+        if (E1 != 0.) { h.flags |= EF_EDGE1; fl += kFlEdge; }
+        if (E2 != 0.) { h.flags |= EF_EDGE2; fl += kFlEdge; }
+        fl += Nint * (kFlBend + kFlRadiate + kFlQuantum);
+        t.pt_refreshes += Nint;
       } else {
         const double href = Angle / L;
         h.op = OP_SBEND;
@@ -447,6 +485,9 @@ HostTable flatten_impl(const Line &line, bool spin) {
       const double E1 = E.GetP("E1"), E2 = E.GetP("E2");
       if (Angle == 0.) {
         as_drift(L);
+      } else if (GP.radiate) {
+        throw Error(STB_EUNSUPPORTED, "element " + E.NAME +
+                                          ": GSBEND with GP.radiate (radiate2, photon Monte Carlo) is not implemented");
       } else {
         const double hreal = K0L / L;
         const double rhoc = L / Angle, b0 = K0L / L;
@@ -562,6 +603,19 @@ HostTable flatten_impl(const Line &line, bool spin) {
         B.mult_block(Norder, k1, s1);
         B.mult_block(Norder, k2, s2);
         fl += 2 * kFlEdge + Nint * (4 * kFlBend + 2 * mult_kick_flops(Norder, k1, s1) + mult_kick_flops(Norder, k2, s2));
+        if (GP.radiate) {
+          // radiating exact branch, GMULT_Pass 5312-5338 / SBENDMULT_Pass 5437-5463
+          h.op = OP_BENDMULT_RAD;
+          h.flags |= EF_CHANGES_PT;
+          B.mult_block(Norder, knl, knsl);
+          B.push(Angle);
+          B.push((double)Nint);
+          B.push(Lint);
+          B.push(href);
+          B.push(rad_E3);
+          fl += Nint * (mult_kick_flops(Norder, knl, knsl) + 11 + kFlRadiate);
+          t.pt_refreshes += Nint;
+        }
       }
     } else if (T == "KICKER" || T == "HKICKER" || T == "VKICKER") {
       // KICK_Pass, simtrack.cpp:5887-5893
@@ -727,6 +781,9 @@ HostTable flatten_impl(const Line &line, bool spin) {
 }
 
 }  // namespace
+
+unsigned long long radiation_seed() { return g_radiation_seed; }
+void set_radiation_seed(unsigned long long seed) { g_radiation_seed = seed; }
 
 HostTable flatten(const Line &line) { return flatten_impl(line, false); }
 HostTable flatten_spin(const Line &line) { return flatten_impl(line, true); }

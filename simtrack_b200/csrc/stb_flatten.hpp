@@ -19,11 +19,21 @@ struct HostTable {
   int pt_refreshes = 0;
   // Flattened for spin tracking (Element::sPass semantics).
   bool spin = false;
+  // Flattened with GP.radiate: radiating bends (OP_SBEND_RAD, OP_BENDMULT_RAD),
+  // tracked by the plain Track() entry points only.
+  bool radiate = false;
 };
+
+// Seed of the quantum-excitation normal deviates (stb_rng.cuh), read at
+// flatten time; the default is the seed the reference gives its GSL stream
+// (Init_GSL_Seeds, simtrack.cpp:328).
+unsigned long long radiation_seed();
+void set_radiation_seed(unsigned long long seed);
 
 // Flatten `line` against the current reference-particle state GP.
 // Throws stb::Error(STB_EUNSUPPORTED) for element types or settings that
-// the GPU kernel does not implement (radiation, H_expand, pitch/yaw).
+// the GPU kernel does not implement (H_expand, pitch/yaw, GSBEND's photon
+// Monte Carlo under GP.radiate).
 HostTable flatten(const Line &line);
 // Flatten for Track_Spin (simtrack.cpp:21766-21789): the orbit maps of
 // Element::sPass plus the Thomas-BMT rotation of spin() after every slice.

@@ -84,6 +84,9 @@ void math_eval_host(int fn, const double *in, double *out, long n);
 cudaError_t fp64_peak_probe(int device, double *tflops);
 cudaError_t drift_quotient_check(long n, unsigned long long seed, int device, unsigned long long *bad4);
 cudaError_t sincos_fast_check(long n, unsigned long long seed, int device, unsigned long long *cnt4);
+cudaError_t rad_normals(unsigned long long seed, unsigned long long id, unsigned long long k0, long n, double *out,
+                        int device);
+void philox_block(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
 
 size_t track_smem_bytes(int nelem, int npool_padded);
 // The loss-test mode of a launch with circular aperture r2 (+inf: none) on a

@@ -255,6 +255,72 @@ __device__ __forceinline__ void mult_kick(Particle &p, int norder, const double 
   p.py = p.py + Bx;
 }
 
+// Field sum of cal_Bfield (simtrack.cpp:4169-4196) at (x, y) for the
+// multipole block K = [KNL0, KNSL0, (KNLi, KNSLi, 1/i!) i = 1..norder] of the
+// element's own strengths: By + i Bx, the divisions by i! exact IEEE ones as
+// in the reference (an integer factorial converted to double).
+__device__ __forceinline__ void bfield_sum(double x, double y, int norder, const double *K, double &By, double &Bx) {
+  double Xn = 1., Yn = 0.;
+  By = K[0];
+  Bx = K[1];
+  double fac = 1.;
+#pragma unroll 1
+  for (int i = 1; i <= norder; i++) {
+    const double Xn0 = Xn, Yn0 = Yn;
+    Xn = Xn0 * x - Yn0 * y;
+    Yn = Xn0 * y + Yn0 * x;
+    fac = fac * (double)i;
+    const double kn = K[3 * i - 1], ks = K[3 * i];
+    if (kn != 0. || ks != 0.) {
+      By = By + (kn * Xn - ks * Yn) / fac;
+      Bx = Bx + (kn * Yn + ks * Xn) / fac;
+    }
+  }
+}
+
+// Synchrotron radiation over one integration step: radiate()
+// (simtrack.cpp:4198-4234) and, with `quantum`, radiate1() (4236-4288),
+// whose fluctuation term takes the normal deviate `gauss`.  L: the step's
+// length on the reference orbit; href: the reference orbit's curvature;
+// (B0, B1, B2): the field integrated over the step over (B rho)_0; E3 =
+// pow(GP.energy/1000, 3) and Cf (simtrack.cpp:26) from the host.  Every
+// operation is the reference's, in its order, with IEEE division and square
+// root; the pt cache is refreshed for the new pt.
+constexpr double kCr = 8.84627632682e-5;          // simtrack.cpp:25
+constexpr double kRadPI = 3.14159265358979323;    // PI, simtrack.cpp:23
+constexpr double kSpeedLight = 299792458.;        // speed_light, simtrack.cpp:24
+__device__ __forceinline__ void radiate_step(Particle &p, PtCache &c, const RefConsts &R, double L, double href,
+                                             double B0, double B1, double B2, double E3, bool quantum, double Cf,
+                                             double gauss) {
+  const double px0 = p.px, py0 = p.py, pt0 = p.pt;
+  const double pz = sqrt(c.opd2 - p.px * p.px - p.py * p.py);
+  const double xp = (1 + p.x * href) * p.px / pz;
+  const double yp = (1 + p.x * href) * p.py / pz;
+  const double temp1 = sqrt((1 + p.x * href) * (1 + p.x * href) + xp * xp + yp * yp);
+  const double u0 = xp / temp1, u1 = yp / temp1, u2 = (1 + p.x * href) / temp1;
+  // vector_cross_product(BLbrho, u, BLper), simtrack.cpp:1639-1644
+  const double b0 = B1 * u2 - B2 * u1;
+  const double b1 = -1.0 * B0 * u2 + B2 * u0;
+  const double b2 = B0 * u1 - B1 * u0;
+  const double bper2 = b0 * b0 + b1 * b1 + b2 * b2;
+  const double temp2 = kCr * c.opd * c.opd * E3 / 2 / kRadPI;
+  if (quantum) {
+    const double ptloss = temp2 * bper2 * temp1 / L;
+    const double gamma1 = R.gamma + R.sqrt_g2m1 * pt0;
+    const double dtdl = temp1 / c.beta1 / kSpeedLight;
+    const double g1 = sqrt(bper2 / L / L) / c.opd;
+    const double ptfluct = sqrt(Cf * gamma1 * gamma1 * gamma1 * gamma1 * gamma1 * g1 * g1 * g1 * dtdl * L) * gauss;
+    p.pt = p.pt - ptloss + ptfluct;
+  } else {
+    p.pt = p.pt - temp2 * bper2 * temp1 / L;
+  }
+  const double delta2 = sqrt(1.0 + 2 * p.pt / R.beta + p.pt * p.pt) - 1.0;
+  const double ratio = (1 + delta2) / c.opd;
+  p.px = px0 * ratio;
+  p.py = py0 * ratio;
+  pt_refresh(R, p.pt, c);
+}
+
 // Hard-edge quadrupole fringe maps, simtrack.cpp:4906-4920 (entry) and 4948-4956 (exit).
 static __device__ __forceinline__ void quad_fringe(Particle &p, double k, bool entry) {
   const double x0 = p.x, px0 = p.px, y0 = p.y, py0 = p.py, z0 = p.z, d0 = p.pt;

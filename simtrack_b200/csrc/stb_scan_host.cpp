@@ -99,6 +99,8 @@ stb_scan *scan_build(stb_table **tables, int nseed, const double *x0, const long
     if (!t) throw Error(STB_EINVAL, "NULL table");
     if (t->device != device) throw Error(STB_EINVAL, "all tables must live on the scan's device");
     if (t->host.spin) throw Error(STB_EINVAL, "spin tables cannot be scanned");
+    if (t->host.radiate)
+      throw Error(STB_EUNSUPPORTED, "tables flattened with GP.radiate cannot be scanned (Track() entry points only)");
     if (std::memcmp(&t->host.ref, &tables[0]->host.ref, sizeof(RefConsts)) != 0)
       throw Error(STB_EINVAL, "all tables must be flattened for the same reference particle");
     if (n_per_seed[i] < 0 || n_per_seed[i] > (1L << 30)) throw Error(STB_EINVAL, "bad particle count");

@@ -332,7 +332,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) spin_track_kernel(const __
       for (int e = 0; e < a.nelem; e++) {
         const ElemHeader h = hdr[e];
         const double *P = pool + h.poff;
-        if (h.op >= OP_S_FIRST) {
+        if (h.op >= OP_S_FIRST && h.op <= OP_S_LAST) {
           const double *M = P;
           const bool mis = (h.flags & (EF_MISALIGN_OFFSET | EF_MISALIGN_ROLL)) != 0;
           if (mis) {

@@ -49,9 +49,13 @@ enum Op : int32_t {
   OP_S_BENDMULT_KICK = 29,  // SBENDMULT_sPass L == 0
   OP_S_KICK = 30,           // KICK_sPass                        8193-8208
   OP_S_SOLEN = 31,          // SOLEN_sPass, KS != 0              8118-8183
-  OP_COUNT = 32
+  // Radiating forms (GP.radiate == true), orbit tables only.
+  OP_SBEND_RAD = 32,     // SBEND_Pass exact radiating branch: Nint slices + radiate1   4740-4748
+  OP_BENDMULT_RAD = 33,  // GMULT/SBENDMULT exact radiating branch: + radiate           5312-5338, 5437-5463
+  OP_COUNT = 34
 };
 constexpr int16_t OP_S_FIRST = OP_S_SBEND;
+constexpr int16_t OP_S_LAST = OP_S_SOLEN;
 
 // Header flag bits (ElemHeader::flags).
 enum : int16_t {
@@ -93,6 +97,11 @@ struct RefConsts {
   double G;          // spin G
   double ibeta;      // RN(1/GP.beta)
   double ienergy;    // RN(1/GP.energy)
+  // Quantum excitation (OP_SBEND_RAD): the normal-deviate stream's seed and
+  // the number of radiating bend slices per turn (the k-th draw of a
+  // particle is its (turn * rad_slices + slice index in the turn)-th).
+  uint64_t rad_seed;
+  int64_t rad_slices;
 };
 
 // Misalignment parameters sit in front of the element parameters when an

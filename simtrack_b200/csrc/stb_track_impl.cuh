@@ -8,6 +8,7 @@
 
 #include "stb_kernels.hpp"
 #include "stb_physics.cuh"
+#include "stb_rng.cuh"
 
 namespace stb {
 namespace {
@@ -197,6 +198,70 @@ __device__ __forceinline__ void op_bendmult(const ElemHeader &h, const double *P
   p.py = p.py - P[1] * p.y;
 }
 
+// Which particles a thread carries, for the normal-deviate streams of the
+// radiating bends: particle k of the thread has id id0 + k * id_stride (its
+// index in the caller's arrays); `turn` is the global turn.  Kernels that
+// never see a radiating table pass the default.
+struct RadKey {
+  long id0 = 0, id_stride = 0;
+  long turn = 0;
+};
+
+// SBEND_Pass, exact radiating branch (simtrack.cpp:4740-4748): Nint slices
+// of sbend_exact_pass over Lint and Angle/Nint, each followed by radiate1
+// with the field {0, Angle/Nint, 0}.  P = [tan(E1)h, tan(E2)h, slice bend
+// (6), Lint, href, Angle/Nint, E3, Cf, first slice index within the turn].
+__device__ __forceinline__ void op_sbend_rad(const ElemHeader &h, const double *P, Particle &p, PtCache &c,
+                                             const RefConsts &R, long id, long turn) {
+  if (h.flags & EF_EDGE1) {
+    p.px = p.px + P[0] * p.x;
+    p.py = p.py - P[0] * p.y;
+  }
+  const double Lint = P[8], href = P[9], an = P[10], E3 = P[11], Cf = P[12];
+  const uint64_t k0 = (uint64_t)turn * (uint64_t)R.rad_slices + (uint64_t)P[13];
+#pragma unroll 1
+  for (int s = 0; s < h.nint; s++) {
+    bend_exact(p, c, P + 2);
+    const double g = rad_gaussian(R.rad_seed, (uint64_t)id, k0 + (uint64_t)s);
+    radiate_step(p, c, R, Lint, href, 0., an, 0., E3, true, Cf, g);
+  }
+  if (h.flags & EF_EDGE2) {
+    p.px = p.px + P[1] * p.x;
+    p.py = p.py - P[1] * p.y;
+  }
+}
+
+// GMULT_Pass / SBENDMULT_Pass, exact radiating branch (simtrack.cpp:
+// 5312-5338, 5437-5463): each slice as in op_bendmult, then radiate() with
+// the field of the element's own strengths at the slice's midpoint
+// (cal_Bfield, 4169-4196).  P as OP_BENDMULT, then [block(KNL), Angle, Nint,
+// Lint, href, E3].
+__device__ __forceinline__ void op_bendmult_rad(const ElemHeader &h, const double *P, Particle &p, PtCache &c,
+                                                const RefConsts &R) {
+  const int no = h.aux, bs = 2 + 3 * no;
+  const double *B1 = P + 2, *B2 = P + 8;
+  const double *K1 = P + 14, *K2 = K1 + bs, *KR = K2 + bs;
+  const double Angle = KR[bs], nd = KR[bs + 1], Lint = KR[bs + 2], href = KR[bs + 3], E3 = KR[bs + 4];
+  p.px = p.px + P[0] * p.x;
+  p.py = p.py - P[0] * p.y;
+#pragma unroll 1
+  for (int s = 0; s < h.nint; s++) {
+    const Particle x1 = p;
+    bend_exact(p, c, B1);
+    mult_kick(p, no, K1);
+    bend_exact(p, c, B2);
+    mult_kick(p, no, K2);
+    bend_exact(p, c, B2);
+    mult_kick(p, no, K1);
+    bend_exact(p, c, B1);
+    double By, Bx;
+    bfield_sum((p.x + x1.x) / 2., (p.y + x1.y) / 2., no, KR, By, Bx);
+    radiate_step(p, c, R, Lint, href, Bx / nd, (Angle + By) / nd, 0., E3, false, 0., 0.);
+  }
+  p.px = p.px + P[1] * p.x;
+  p.py = p.py - P[1] * p.y;
+}
+
 __device__ __forceinline__ void op_misc(const ElemHeader &h, const double *P, Particle &p, PtCache &c,
                                      const RefConsts &R) {
   switch (h.op) {
@@ -274,7 +339,7 @@ __device__ __forceinline__ void op_misc(const ElemHeader &h, const double *P, Pa
 // instruction stream (latency hiding without more resident warps).
 template <int kPPT, bool kLoopSlices = false>
 __device__ __forceinline__ void apply_element(const ElemHeader &h, const double *P, Particle (&p)[kPPT],
-                                              PtCache (&c)[kPPT], const RefConsts &R) {
+                                              PtCache (&c)[kPPT], const RefConsts &R, const RadKey &rk = RadKey{}) {
   const double *M = P;
   const bool mis = (h.flags & (EF_MISALIGN_OFFSET | EF_MISALIGN_ROLL)) != 0;
   if (mis) {
@@ -373,6 +438,12 @@ __device__ __forceinline__ void apply_element(const ElemHeader &h, const double 
       break;
     case OP_BENDMULT:
       for (int k = 0; k < kPPT; k++) op_bendmult(h, P, p[k], c[k]);
+      break;
+    case OP_SBEND_RAD:
+      for (int k = 0; k < kPPT; k++) op_sbend_rad(h, P, p[k], c[k], R, rk.id0 + (long)k * rk.id_stride, rk.turn);
+      break;
+    case OP_BENDMULT_RAD:
+      for (int k = 0; k < kPPT; k++) op_bendmult_rad(h, P, p[k], c[k], R);
       break;
     default:
       for (int k = 0; k < kPPT; k++) op_misc(h, P, p[k], c[k], R);
@@ -498,7 +569,8 @@ __device__ void track_segmented(const TrackArgs &a, unsigned char *smem, uint64_
         if (nalive > 0) {
           for (int j = 0; j < sg.ne; j++) {
             const ElemHeader h = hs[j];
-            apply_element<kPPT, (kBlock >= 512)>(h, ps + (h.poff - sg.pool_lo), p, c, R);
+            apply_element<kPPT, (kBlock >= 512)>(h, ps + (h.poff - sg.pool_lo), p, c, R,
+                                                 RadKey{base, kBlock, (long)a.turn0 + t});
             after_element<kBlock, kPPT, kDump>(a, h, base, t, sg.e0 + j, p, c, alive, nalive);
             if (nalive == 0) break;
           }
@@ -587,7 +659,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) track_kernel(const __grid_
         } else {
           h = hdr[e];
         }
-        apply_element<kPPT, (kBlock >= 512)>(h, pool + h.poff, p, c, R);
+        apply_element<kPPT, (kBlock >= 512)>(h, pool + h.poff, p, c, R, RadKey{base, kBlock, (long)a.turn0 + t});
 #pragma unroll
         for (int k = 0; k < kPPT; k++) {
           if (!alive[k]) continue;

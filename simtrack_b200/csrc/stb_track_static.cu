@@ -109,6 +109,8 @@ int track_seeds_static(stb_table *const *tables, int nseed, const long *n_per_se
     if (!t) throw Error(STB_EINVAL, "NULL table");
     if (t->device != device) throw Error(STB_EINVAL, "all tables must live on one device");
     if (t->host.spin) throw Error(STB_EINVAL, "spin tables need the stb_track_spin_* entry points");
+    if (t->host.radiate)
+      throw Error(STB_EUNSUPPORTED, "tables flattened with GP.radiate need the stb_track_* entry points");
     if (std::memcmp(&t->host.ref, &tables[0]->host.ref, sizeof(RefConsts)) != 0)
       throw Error(STB_EINVAL, "all tables must be flattened for the same reference particle");
     in.seeds[i] = ScanSeed{t->d_hdr, t->d_pool, (int)t->host.hdr.size(), t->npool_padded, off, (int)n_per_seed[i], 0};

@@ -38,10 +38,13 @@ class Lattice:
     quad_fringe: bool = False
     aperture_radius: float = 0.0
     meta: dict = field(default_factory=dict)
+    radiate: bool = False  # GP.radiate
+    radiation_seed: int = 1324
 
     def set_reference(self) -> None:
         api.Set_RefPartEnergy(self.gamma, self.E0, self.Q, self.A)
         api.Set_Flags(False, self.quad_fringe)
+        api.Set_Radiation(self.radiate, self.radiation_seed)
 
     @property
     def circumference(self) -> float:
@@ -114,6 +117,50 @@ def fodo_ring(ncell: int = 100, gamma: Optional[float] = None, nint: int = 4, k1
     frf = harmonic * beta * 299792458.0 / C
     els.append(ElementSpec("RFCAV", "rf", (0.0, vrf_mv, frf, 0.0)))
     lat.meta.update({"harmonic": harmonic, "frf": frf, "emit_norm": 2.5e-6})
+    return lat
+
+
+ELECTRON_MASS_MEV = 0.51099895
+
+
+def electron_ring(ncell: int = 40, energy_gev: float = 3.0, nint: int = 5, k1: float = 0.25, k2l: float = 0.3,
+                  vrf_mv: float = 2.0, harmonic: int = 400, radiate: bool = True, seed: int = 1324) -> Lattice:
+    """An electron storage ring with synchrotron radiation (GP.radiate): `ncell`
+    FODO cells, each with a thick sector dipole (L = 2 m, `nint` slices, each
+    followed by radiation with quantum excitation) and a combined-function
+    SBENDMULT (L = 1.5 m, `nint` slices with a small sextupole and skew
+    quadrupole component, radiation after each slice), thick quadrupoles
+    (K1 = +/-`k1` m^-2), thin sextupoles and one thin RF cavity.  Electrons
+    (Q = -1) at `energy_gev` total energy; the two dipoles of a cell bend by
+    2 pi / ncell together."""
+    gamma = energy_gev * 1000.0 / ELECTRON_MASS_MEV
+    ang = 2 * math.pi / ncell
+    a1, a2 = 0.6 * ang, 0.4 * ang
+    els: List[ElementSpec] = []
+    for c in range(ncell):
+        knl = [0.0, 0.0, 0.02 * (1 if c % 2 == 0 else -1)] + [0.0] * 8
+        knsl = [0.0, 1e-4] + [0.0] * 9
+        els += [
+            ElementSpec("QUAD", f"qf{c}", (0.5, k1 * 0.5, 0.0), {"Nint": 4}),
+            ElementSpec("DRIFT", f"d1_{c}", (0.4,)),
+            ElementSpec("SEXT", f"sf{c}", (0.0, k2l, 0.0)),
+            ElementSpec("DRIFT", f"d2_{c}", (0.4,)),
+            ElementSpec("SBEND", f"b{c}", (2.0, a1, 0.0, 0.0), {"Nint": nint}),
+            ElementSpec("DRIFT", f"d3_{c}", (0.4,)),
+            ElementSpec("QUAD", f"qd{c}", (0.5, -k1 * 0.5, 0.0), {"Nint": 4}),
+            ElementSpec("DRIFT", f"d4_{c}", (0.4,)),
+            ElementSpec("SEXT", f"sd{c}", (0.0, -k2l, 0.0)),
+            ElementSpec("DRIFT", f"d5_{c}", (0.4,)),
+            ElementSpec("SBENDMULT", f"bm{c}", (1.5, a2, 0.0, 0.0, *knl, *knsl), {"Nint": nint}),
+            ElementSpec("DRIFT", f"d6_{c}", (0.4,)),
+        ]
+    lat = Lattice("electron_ring", els, gamma, E0=ELECTRON_MASS_MEV, Q=-1.0, A=1.0, radiate=radiate,
+                  radiation_seed=seed)
+    C = lat.circumference
+    beta = math.sqrt(1.0 - 1.0 / gamma / gamma)
+    frf = harmonic * beta * 299792458.0 / C
+    els.append(ElementSpec("RFCAV", "rf", (0.0, vrf_mv, frf, 0.0)))
+    lat.meta.update({"harmonic": harmonic, "frf": frf})
     return lat
 
 

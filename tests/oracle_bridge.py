@@ -107,6 +107,10 @@ class RefOracle:
         L.ref_set_spin_g.argtypes = [c_double]
         L.ref_fine_tune.argtypes = [c_int, POINTER(c_double), POINTER(c_double), c_double, c_double]
         L.ref_fine_tune.restype = c_double
+        L.ref_set_radiation.argtypes = [c_int, ctypes.c_ulonglong]
+        L.ref_rng_id_base.argtypes = [c_long]
+        L.ref_rng_stream.argtypes = [ctypes.c_ulonglong] * 3
+        L.ref_rng_stream.restype = c_double
         self.L = L
         self.line = None
         self.nelem = 0
@@ -115,6 +119,9 @@ class RefOracle:
         L = self.L
         L.ref_set_ref_energy(lat.gamma, lat.E0, lat.Q, lat.A)
         L.ref_set_flags(0, int(lat.quad_fringe))
+        if getattr(lat, "radiate", False):
+            L.ref_set_radiation(1, int(lat.radiation_seed))
+        L.ref_rng_id_base(0)
         if self.line:
             L.ref_line_free(self.line)
         self.line = L.ref_line_new()
@@ -402,9 +409,10 @@ class PortOracle:
 
 
 def _ref_track_worker(args):
-    lat, x, nturn, cr, spin = args
+    lat, x, nturn, cr, spin, first = args
     o = RefOracle(cr=cr)
     o.build(lat)
+    o.L.ref_rng_id_base(int(first))  # particle ids of the radiation deviate streams
     return o.track_spin(x, nturn) if spin else o.track(x, nturn)
 
 
@@ -419,6 +427,7 @@ def ref_track_parallel(lat: Lattice, x: np.ndarray, nturn: int, cr: bool = False
     procs = procs or os.cpu_count() or 1
     procs = max(1, min(procs, len(x)))
     chunks = np.array_split(np.ascontiguousarray(x, dtype=np.float64), procs)
+    firsts = np.cumsum([0] + [len(c) for c in chunks[:-1]])
     with mp.get_context("spawn").Pool(procs) as pool:
-        res = pool.map(_ref_track_worker, [(lat, c, nturn, cr, spin) for c in chunks])
+        res = pool.map(_ref_track_worker, [(lat, c, nturn, cr, spin, f) for c, f in zip(chunks, firsts)])
     return tuple(np.concatenate([r[k] for r in res]) for k in range(4))

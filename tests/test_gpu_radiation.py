@@ -1,0 +1,139 @@
+"""Synchrotron radiation on the GPU (GP.radiate) against the compiled
+reference (needs a B200).
+
+Ring: `lattices.electron_ring` (3 GeV electrons, 40 cells of sector dipoles
+with 5 radiating slices each (SBEND_Pass's radiating branch,
+simtrack.cpp:4740-4748: radiate1 with quantum excitation) and combined-
+function SBENDMULTs (5437-5463: radiate with the midpoint field of
+cal_Bfield), thick quadrupoles, sextupoles, RF).  The reference's radiate1
+takes its deviates from GSL, which is absent; both sides use the
+per-particle counter-based stream (tests/test_radiation.py pins it).  The
+reference is the correctly rounded build (its cos matches the tracker's).
+
+Tolerance as in test_gpu_parity: 1e-12 relative with the per-coordinate rms
+floor; loss turn and element exact.
+"""
+import numpy as np
+import pytest
+
+import oracle_bridge
+from simtrack_b200 import api
+from simtrack_b200 import lattices as lt
+from simtrack_b200._native import SimTrackError
+from simtrack_b200.api import Table
+from test_gpu_parity import assert_close_traj
+from test_radiation import normals
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(autouse=True)
+def radiation_off_afterwards():
+    yield
+    api.Set_Radiation(False)
+
+
+@pytest.fixture(scope="module")
+def ring():
+    lat = lt.electron_ring()
+    tab = Table(lt.build_line(lat))
+    api.Set_Radiation(False)
+    return lat, tab
+
+
+def _need_ref():
+    if not oracle_bridge.ref_available(cr=True):
+        pytest.skip("compiled reference oracle (oracle/_ref) not built here")
+
+
+def _particles(n, seed=3):
+    rng = np.random.default_rng(seed)
+    X = np.zeros((n, 6))
+    X[:, 0] = rng.normal(0, 1e-3, n)
+    X[:, 1] = rng.normal(0, 1e-4, n)
+    X[:, 2] = rng.normal(0, 1e-3, n)
+    X[:, 3] = rng.normal(0, 1e-4, n)
+    X[:, 5] = rng.normal(0, 5e-4, n)
+    return X
+
+
+def test_device_stream_equals_host(native_lib):
+    for seed, pid, k0 in ((1324, 0, 0), (99, 12345, 2**34 + 7)):
+        assert np.array_equal(normals(native_lib, seed, pid, k0, 500_000, 0),
+                              normals(native_lib, seed, pid, k0, 500_000, -1))
+
+
+def test_every_element_vs_reference(ring):
+    _need_ref()
+    lat, tab = ring
+    ref = oracle_bridge.RefOracle(cr=True)
+    ref.build(lat)
+    X = _particles(4)
+    nt = 200
+    xg, st, ltn, lp, dump = tab.track_probe(X.copy(), nt)
+    for i, x0 in enumerate(X):
+        ref.L.ref_rng_id_base(i)  # the probe's particle i draws from stream i
+        xo, so, lo, po, do = ref.track_dump(x0, nt, 0.0)
+        assert (st[i], ltn[i], lp[i]) == (so, lo, po), f"particle {i}"
+        assert_close_traj(dump[i], do, f"particle {i}")
+    # radiation is on: the momentum deviation differs from the tracking without it
+    plain = lt.electron_ring(radiate=False)
+    ref.build(plain)
+    xp = ref.track_dump(X[0], nt, 0.0)[0]
+    assert abs(xp[5] - xg[0, 5]) > 1e-7
+
+
+def test_grid_vs_reference(ring):
+    _need_ref()
+    lat, tab = ring
+    import dataclasses
+    X = _particles(256, seed=11)
+    X[::16, 0] *= 8.0  # some particles start near the 10 mm aperture
+    nt = 400
+    xg, sg, lg, pg = tab.track_host(X.copy(), nt, 0.01)
+    xo, so, lo, po = oracle_bridge.ref_track_parallel(dataclasses.replace(lat, aperture_radius=0.01), X, nt, cr=True)
+    assert np.array_equal(sg, so)
+    lost = so == 0
+    assert lost.any() and not lost.all()
+    assert np.array_equal(lg[lost], lo[lost]) and np.array_equal(pg[lost], po[lost])
+    assert_close_traj(xg[~lost], xo[~lost], "survivors")
+
+
+def test_launch_shape_and_turn_blocks_do_not_change_the_stream(ring):
+    import torch
+    lat, tab = ring
+    X = _particles(3000, seed=5)
+    nt = 60
+    results = []
+    for v in (0, 1, 3, 7, 15):  # 7: two particles per thread
+        tab.set_variant(v)
+        results.append(tab.track_host(X.copy(), nt))
+    for r in results[1:]:
+        for a, b in zip(results[0], r):
+            assert np.array_equal(a, b)
+    tab.set_variant(1)
+    dev = torch.device("cuda", 0)
+    c = [torch.tensor(np.ascontiguousarray(X[:, k]), device=dev) for k in range(6)]
+    lt_ = torch.full((len(X),), -1, dtype=torch.int32, device=dev)
+    le_ = torch.zeros(len(X), dtype=torch.int32, device=dev)
+    tab.track_device(c, lt_, le_, 0, nt // 2)
+    tab.track_device(c, lt_, le_, nt // 2, nt - nt // 2)
+    torch.cuda.synchronize()
+    xs = np.stack([t.cpu().numpy() for t in c], 1)
+    alive = lt_.cpu().numpy() < 0
+    assert np.array_equal(alive, results[0][1] == 1)
+    assert np.array_equal(xs[alive], results[0][0][alive])
+
+
+def test_unsupported_uses_are_rejected(ring):
+    lat, tab = ring
+    with pytest.raises(SimTrackError):
+        tab.track_radial_host(_particles(4), 2)
+    with pytest.raises(SimTrackError):
+        api.Scan([tab], [_particles(64)])
+    with pytest.raises(SimTrackError):
+        api.SpinTable(lt.build_line(lat))
+    gs = lt.Lattice("gsbend_rad", [lt.ElementSpec("GSBEND", "g", (2.0, 0.01, 0.0101, 0.0, 0.0))],
+                    lat.gamma, E0=lat.E0, Q=-1.0, radiate=True)
+    with pytest.raises(SimTrackError):
+        Table(lt.build_line(gs))
