@@ -146,15 +146,35 @@ __host__ __device__ __forceinline__ void drift_quotients(double opd, double opd2
   }
 }
 
+// The increments of one drift: x += dx, y += dy, z -= dz.
+struct DriftStep {
+  double dx, dy, dz;
+};
+
+// A drift's increments depend on px, py, pt and L only, none of which the
+// drift changes: a second drift of the same length with no kick between
+// (the last drift of a Yoshida slice and the first of the next one) adds the
+// very same three values, so it can reuse them (drift_again) and round
+// exactly as the reference's recomputation does.
+__device__ __forceinline__ DriftStep drift_step(const Particle &p, const PtCache &c, double L, double Lb) {
+  double pz, ipz, betaz, L_betaz;
+  drift_quotients(c.opd, c.opd2, c.beta1, c.iopd, c.opd_ibeta1, p.px, p.py, L, pz, ipz, betaz, L_betaz);
+  return DriftStep{qdiv(p.px * L, pz, ipz), qdiv(p.py * L, pz, ipz), L_betaz - Lb};
+}
+
+__device__ __forceinline__ void drift_again(Particle &p, const DriftStep &d) {
+  p.x = p.x + d.dx;
+  p.y = p.y + d.dy;
+  p.z = p.z - d.dz;
+}
+
 // DRIFT_Pass exact branch, simtrack.cpp:3759-3764.  L and Lb = L/GP.beta.
 // The two quotients by pz share one reciprocal; (pz*beta1)/(1+delta1) uses
 // the cached reciprocal of 1+delta1.
-__device__ __forceinline__ void drift(Particle &p, const PtCache &c, double L, double Lb) {
-  double pz, ipz, betaz, L_betaz;
-  drift_quotients(c.opd, c.opd2, c.beta1, c.iopd, c.opd_ibeta1, p.px, p.py, L, pz, ipz, betaz, L_betaz);
-  p.x = p.x + qdiv(p.px * L, pz, ipz);
-  p.y = p.y + qdiv(p.py * L, pz, ipz);
-  p.z = p.z - (L_betaz - Lb);
+__device__ __forceinline__ DriftStep drift(Particle &p, const PtCache &c, double L, double Lb) {
+  const DriftStep d = drift_step(p, c, L, Lb);
+  drift_again(p, d);
+  return d;
 }
 
 // sbend_exact_pass, simtrack.cpp:3833-3858.  B = [L, L/beta, href, 1/href, cosA, sinA].

@@ -148,15 +148,16 @@ template <int kOrder>
 __device__ __forceinline__ void op_thick_sext_oct(const ElemHeader &h, const double *P, Particle &p, const PtCache &c) {
   const double d1 = P[0], d1b = P[1], d2 = P[2], d2b = P[3];
   const double a1 = P[4], s1 = P[5], a2 = P[6], s2 = P[7];
+  DriftStep last = drift(p, c, d1, d1b);  // slice 0's opening drift
 #pragma unroll 1
   for (int s = 0; s < h.nint; s++) {
-    drift(p, c, d1, d1b);
+    if (s > 0) drift_again(p, last);  // the same increments as the drift before it
     if (kOrder == 2) sext_kick(p, a1, s1); else oct_kick(p, a1, s1);
     drift(p, c, d2, d2b);
     if (kOrder == 2) sext_kick(p, a2, s2); else oct_kick(p, a2, s2);
     drift(p, c, d2, d2b);
     if (kOrder == 2) sext_kick(p, a1, s1); else oct_kick(p, a1, s1);
-    drift(p, c, d1, d1b);
+    last = drift(p, c, d1, d1b);
   }
 }
 
@@ -165,15 +166,16 @@ __device__ __forceinline__ void op_mult_thick(const ElemHeader &h, const double 
   const int no = h.aux;
   const double *K1 = P + 4;
   const double *K2 = K1 + 2 + 3 * no;
+  DriftStep last = drift(p, c, V[0], V[1]);  // slice 0's opening drift
 #pragma unroll 1
   for (int s = 0; s < h.nint; s++) {
-    drift(p, c, V[0], V[1]);
+    if (s > 0) drift_again(p, last);  // the same increments as the drift before it
     mult_kick(p, no, K1);
     drift(p, c, V[2], V[3]);
     mult_kick(p, no, K2);
     drift(p, c, V[2], V[3]);
     mult_kick(p, no, K1);
-    drift(p, c, V[0], V[1]);
+    last = drift(p, c, V[0], V[1]);
   }
 }
 
@@ -376,28 +378,35 @@ __device__ __forceinline__ void apply_element(const ElemHeader &h, const double 
       const volatile double *VV = P;
       if (h.flags & EF_FRINGE)
         for (int k = 0; k < kPPT; k++) quad_fringe(p[k], P[8], true);
+      // Slice s is d1 k1 d2 k2 d2 k1 d1.  The closing d1 of slice s and the
+      // opening d1 of slice s+1 meet with no kick between them, so the second
+      // adds the first one's increments again (drift_again), bit for bit what
+      // recomputing them gives.
+      DriftStep d1[kPPT];
+#pragma unroll
+      for (int k = 0; k < kPPT; k++) d1[k] = drift(p[k], c[k], V[0], V[1]);
       if (kLoopSlices) {
         // one copy of the drift code: smaller instruction footprint, better
         // for many resident warps; the unrolled form has the shorter latency
 #pragma unroll 1
         for (int s = 0; s < h.nint; s++) {
 #pragma unroll 1
-          for (int q = 0; q < 4; q++) {
-            const int dofs = (q == 0 || q == 3) ? 0 : 2;
+          for (int q = 0; q < 3; q++) {
+            const int kofs = (q == 1) ? 6 : 4;
+            const int dofs = (q == 2) ? 0 : 2;
 #pragma unroll
-            for (int k = 0; k < kPPT; k++) drift(p[k], c[k], VV[dofs], VV[dofs + 1]);
-            if (q < 3) {
-              const int kofs = (q == 1) ? 6 : 4;
+            for (int k = 0; k < kPPT; k++) quad_kick(p[k], VV[kofs], VV[kofs + 1]);
 #pragma unroll
-              for (int k = 0; k < kPPT; k++) quad_kick(p[k], VV[kofs], VV[kofs + 1]);
-            }
+            for (int k = 0; k < kPPT; k++) d1[k] = drift(p[k], c[k], VV[dofs], VV[dofs + 1]);
+          }
+          if (s + 1 < h.nint) {
+#pragma unroll
+            for (int k = 0; k < kPPT; k++) drift_again(p[k], d1[k]);
           }
         }
       } else {
 #pragma unroll 1
         for (int s = 0; s < h.nint; s++) {
-#pragma unroll
-          for (int k = 0; k < kPPT; k++) drift(p[k], c[k], V[0], V[1]);
 #pragma unroll
           for (int k = 0; k < kPPT; k++) quad_kick(p[k], V[4], V[5]);
 #pragma unroll
@@ -409,7 +418,11 @@ __device__ __forceinline__ void apply_element(const ElemHeader &h, const double 
 #pragma unroll
           for (int k = 0; k < kPPT; k++) quad_kick(p[k], V[4], V[5]);
 #pragma unroll
-          for (int k = 0; k < kPPT; k++) drift(p[k], c[k], V[0], V[1]);
+          for (int k = 0; k < kPPT; k++) d1[k] = drift(p[k], c[k], V[0], V[1]);
+          if (s + 1 < h.nint) {
+#pragma unroll
+            for (int k = 0; k < kPPT; k++) drift_again(p[k], d1[k]);
+          }
         }
       }
       if (h.flags & EF_FRINGE)
