@@ -490,6 +490,20 @@ int stb_check_drift_quotients(long n, unsigned long long seed, int device, unsig
  * generic classes, and among the offsets from multiples of pi/128. */
 int stb_check_sincos(long n, unsigned long long seed, int device, unsigned long long *count4);
 
+/* Strong-strong beam-beam, soft-Gaussian 4D: BeamBeam4D_SoftGaussian(Np1,
+ * Npart_1, PartDist_1, Np2, Npart_2, PartDist_2, gamma1, gamma2, bbscale1,
+ * bbscale2), simtrack.cpp:22846-22872 (simtrack.h:1403).  Each beam's
+ * transverse centroid and rms size (Cal_Mean_RMS, 724-743, its running sums
+ * in particle order) kick the other beam's macro-particles through BB4D;
+ * px and py of both AoS beams x1[6*n1], x2[6*n2] are updated in place.  The
+ * _device form takes device arrays and is asynchronous on `stream` (one
+ * collision at a time per device: the moments live in one static device
+ * buffer); the _host form takes host arrays and returns when done. */
+int stb_bb4d_soft_gaussian_device(double Np1, long n1, double *x1, double Np2, long n2, double *x2, double gamma1,
+                                  double gamma2, double bbscale1, double bbscale2, int device, void *stream);
+int stb_bb4d_soft_gaussian_host(double Np1, long n1, double *x1, double Np2, long n2, double *x2, double gamma1,
+                                double gamma2, double bbscale1, double bbscale2, int device);
+
 /* Diagnostics: deviates k0 .. k0+n-1 of particle `id`'s quantum-excitation
  * stream under `seed` (see stb_set_radiation), evaluated on GPU `device` or
  * on the host (device < 0); out is host memory. */

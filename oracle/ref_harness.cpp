@@ -426,6 +426,12 @@ void ref_track_dump(void *line, double *x, int nturn, double radius, double *dum
 
 double ref_pinv(double p) { return gsl_cdf_ugaussian_Pinv(p); }
 
+// The reference's strong-strong soft-Gaussian collision, called as is.
+void ref_bb4d_soft_gaussian(double Np1, int n1, double *x1, double Np2, int n2, double *x2, double gamma1,
+                            double gamma2, double bbscale1, double bbscale2) {
+  BeamBeam4D_SoftGaussian(Np1, n1, x1, Np2, n2, x2, gamma1, gamma2, bbscale1, bbscale2);
+}
+
 // FineTuneFinder, both overloads (simtrack.cpp:2288, 2321).
 double ref_fine_tune(int n, const double *x, const double *px, double lo, double hi) {
   std::vector<double> a(x, x + n);

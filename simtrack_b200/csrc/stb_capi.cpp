@@ -1151,6 +1151,57 @@ int stb_check_sincos(long n, unsigned long long seed, int device, unsigned long 
   });
 }
 
+namespace {
+// BeamBeam4D_SoftGaussian's arguments: BB4D's constant 2 N rp / gamma for
+// each beam (kicked by the other beam's N), in the reference's order.
+void soft_gaussian_args(double Np1, long n1, double Np2, long n2, double gamma1, double gamma2, double &c4_1,
+                        double &c4_2) {
+  if (n1 < 1 || n2 < 1) throw Error(STB_EINVAL, "each beam needs at least one macro-particle");
+  if (!(gamma1 > 0) || !(gamma2 > 0)) throw Error(STB_EINVAL, "gamma must be positive");
+  const double rp = 1.53469826769e-18;  // BB4D, simtrack.cpp:6328
+  c4_1 = 2 * Np2 * rp / gamma1;
+  c4_2 = 2 * Np1 * rp / gamma2;
+}
+}  // namespace
+
+int stb_bb4d_soft_gaussian_device(double Np1, long n1, double *x1, double Np2, long n2, double *x2, double gamma1,
+                                  double gamma2, double bbscale1, double bbscale2, int device, void *stream) {
+  return guarded([&] {
+    if (!x1 || !x2) throw Error(STB_EINVAL, "NULL beam");
+    double c4_1, c4_2;
+    soft_gaussian_args(Np1, n1, Np2, n2, gamma1, gamma2, c4_1, c4_2);
+    DeviceGuard g(device);
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    cuda_check(soft_gaussian_4d(x1, n1, x2, n2, c4_1, c4_2, bbscale1, bbscale2, sms, (cudaStream_t)stream),
+               "soft-Gaussian beam-beam");
+    return STB_OK;
+  });
+}
+
+int stb_bb4d_soft_gaussian_host(double Np1, long n1, double *x1, double Np2, long n2, double *x2, double gamma1,
+                                double gamma2, double bbscale1, double bbscale2, int device) {
+  return guarded([&] {
+    if (!x1 || !x2) throw Error(STB_EINVAL, "NULL beam");
+    double c4_1, c4_2;
+    soft_gaussian_args(Np1, n1, Np2, n2, gamma1, gamma2, c4_1, c4_2);
+    DeviceGuard g(device);
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    double *d = nullptr;
+    const size_t b1 = sizeof(double) * 6 * (size_t)n1, b2 = sizeof(double) * 6 * (size_t)n2;
+    cuda_check(cudaMalloc(&d, b1 + b2), "cudaMalloc(beams)");
+    DevFree f{d};
+    cuda_check(cudaMemcpy(d, x1, b1, cudaMemcpyHostToDevice), "upload beam 1");
+    cuda_check(cudaMemcpy(d + 6 * n1, x2, b2, cudaMemcpyHostToDevice), "upload beam 2");
+    cuda_check(soft_gaussian_4d(d, n1, d + 6 * n1, n2, c4_1, c4_2, bbscale1, bbscale2, sms, 0),
+               "soft-Gaussian beam-beam");
+    cuda_check(cudaMemcpy(x1, d, b1, cudaMemcpyDeviceToHost), "download beam 1");
+    cuda_check(cudaMemcpy(x2, d + 6 * n1, b2, cudaMemcpyDeviceToHost), "download beam 2");
+    return STB_OK;
+  });
+}
+
 int stb_rad_normals(unsigned long long seed, unsigned long long id, unsigned long long k0, long n, double *out,
                     int device) {
   return guarded([&] {

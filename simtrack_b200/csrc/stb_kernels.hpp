@@ -87,6 +87,9 @@ cudaError_t sincos_fast_check(long n, unsigned long long seed, int device, unsig
 cudaError_t rad_normals(unsigned long long seed, unsigned long long id, unsigned long long k0, long n, double *out,
                         int device);
 void philox_block(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
+// BeamBeam4D_SoftGaussian on device AoS beams (stb_ssbb.cu); c4_k = 2 N_other rp / gamma_k.
+cudaError_t soft_gaussian_4d(double *x1, long n1, double *x2, long n2, double c4_1, double c4_2, double bbscale1,
+                             double bbscale2, int num_sms, cudaStream_t s);
 
 size_t track_smem_bytes(int nelem, int npool_padded);
 // The loss-test mode of a launch with circular aperture r2 (+inf: none) on a

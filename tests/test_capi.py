@@ -99,3 +99,16 @@ def test_flatten_rejects_unsupported_settings(native_lib):
     with pytest.raises(st.SimTrackError) as ei:
         st.Table(line)
     assert ei.value.code in (-6, -3)
+
+
+def test_soft_gaussian_collision_rejects_empty_beams(native_lib):
+    """BeamBeam4D_SoftGaussian's entry points check their beams before any
+    device work (an empty beam has no moments)."""
+    from ctypes import POINTER, c_double
+    from simtrack_b200 import _native
+    b = (c_double * 6)()
+    L = native_lib
+    assert L.stb_bb4d_soft_gaussian_host(1e11, 0, b, 1e11, 1, b, 100.0, 100.0, 1.0, 1.0, 0) == _native.STB_EINVAL
+    assert L.stb_bb4d_soft_gaussian_host(1e11, 1, None, 1e11, 1, b, 100.0, 100.0, 1.0, 1.0, 0) == _native.STB_EINVAL
+    assert L.stb_bb4d_soft_gaussian_device(1e11, 1, None, 1e11, 1, None, 100.0, 100.0, 1.0, 1.0, 0, None) \
+        == _native.STB_EINVAL
