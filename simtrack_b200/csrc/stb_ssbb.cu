@@ -9,11 +9,11 @@
 // the tracking kernels, bb4d in stb_physics.cuh).
 //
 // The moments are the reference's running sums in the reference's order:
-// one warp loads 32 particles at a time and its lane 0 adds them one by one,
-// so the sums round exactly as the reference's loop does (a tree reduction
-// would round differently and the kicks would differ in the last bits).
-// That pass is a dependent chain of n additions (about 1 ms per 1e5
-// particles); the kicks are one thread per particle.
+// one CTA stages the particles in shared memory and one thread adds them one
+// by one, so the sums round exactly as the reference's loop does (a tree
+// reduction would round differently and the kicks would differ in the last
+// bits).  That pass is a dependent chain of n additions; the kicks are one
+// thread per particle.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -24,25 +24,33 @@
 namespace stb {
 namespace {
 
-// mean[0..1], rms[0..1] of x and y of n particles, AoS x[6 n].
-__global__ void soft_gaussian_moments_kernel(const double *x, long n, double *out4) {
-  const int lane = threadIdx.x & 31;
+// mean[0..1], rms[0..1] of x and y of n particles, AoS x[6 n].  The CTA
+// stages kMomentChunk particles' x and y in shared memory; thread 0 adds them
+// in particle order (the loads of the next chunk do not wait on its sums).
+constexpr int kMomentBlock = 256, kMomentChunk = 2048;
+__global__ void __launch_bounds__(kMomentBlock) soft_gaussian_moments_kernel(const double *x, long n, double *out4) {
+  __shared__ double cx[kMomentChunk], cy[kMomentChunk];
   double sx = 0, sy = 0, sx2 = 0, sy2 = 0;
-  for (long base = 0; base < n; base += 32) {
-    const long i = base + lane;
-    const double tx = i < n ? x[6 * i] : 0.0;
-    const double ty = i < n ? x[6 * i + 2] : 0.0;
-    const int m = (int)(n - base < 32 ? n - base : 32);
-    for (int j = 0; j < m; j++) {
-      const double a = __shfl_sync(0xffffffffu, tx, j);
-      const double b = __shfl_sync(0xffffffffu, ty, j);
-      sx = sx + a;
-      sy = sy + b;
-      sx2 = sx2 + a * a;
-      sy2 = sy2 + b * b;
+  for (long base = 0; base < n; base += kMomentChunk) {
+    const int m = (int)(n - base < kMomentChunk ? n - base : kMomentChunk);
+    for (int k = threadIdx.x; k < m; k += kMomentBlock) {
+      cx[k] = x[6 * (base + k)];
+      cy[k] = x[6 * (base + k) + 2];
     }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll 8
+      for (int j = 0; j < m; j++) {
+        const double a = cx[j], b = cy[j];
+        sx = sx + a;
+        sy = sy + b;
+        sx2 = sx2 + a * a;
+        sy2 = sy2 + b * b;
+      }
+    }
+    __syncthreads();
   }
-  if (lane == 0) {
+  if (threadIdx.x == 0) {
     const double N = (double)n;
     const double mx = sx / N, my = sy / N;
     out4[0] = mx;
@@ -78,8 +86,8 @@ cudaError_t soft_gaussian_4d(double *x1, long n1, double *x2, long n2, double c4
   double *d_m8 = nullptr;
   cudaError_t e = cudaGetSymbolAddress((void **)&d_m8, g_soft_gaussian_moments);
   if (e != cudaSuccess) return e;
-  soft_gaussian_moments_kernel<<<1, 32, 0, s>>>(x1, n1, d_m8);
-  soft_gaussian_moments_kernel<<<1, 32, 0, s>>>(x2, n2, d_m8 + 4);
+  soft_gaussian_moments_kernel<<<1, kMomentBlock, 0, s>>>(x1, n1, d_m8);
+  soft_gaussian_moments_kernel<<<1, kMomentBlock, 0, s>>>(x2, n2, d_m8 + 4);
   const int block = 256;
   auto grid = [&](long n) {
     long g = (n + block - 1) / block;
