@@ -182,16 +182,20 @@ __device__ __forceinline__ void spin_element(const ElemHeader &h, const double *
     case OP_S_MPOLE_THICK: {
       const int order = h.aux;
       const double kl = P[8], ksl = P[9], nd = P[10];
+      DriftStep last{};
 #pragma unroll 1
       for (int i = 0; i < h.nint; i++) {
         const Particle x0 = p;
-        drift(p, c, P[0], P[1]);
+        // the rotation changes no orbit coordinate: this drift repeats the
+        // previous slice's closing one, so its increments are added again
+        if (i > 0) drift_again(p, last);
+        else drift(p, c, P[0], P[1]);
         mpole_kick(p, order, P[4], P[5]);
         drift(p, c, P[2], P[3]);
         mpole_kick(p, order, P[6], P[7]);
         drift(p, c, P[2], P[3]);
         mpole_kick(p, order, P[4], P[5]);
-        drift(p, c, P[0], P[1]);
+        last = drift(p, c, P[0], P[1]);
         const double x1 = (p.x + x0.x) / 2., y1 = (p.y + x0.y) / 2.;
         double B0, B1;
         mpole_field(order, true, x1, y1, kl, ksl, nd, B0, B1);
@@ -219,16 +223,18 @@ __device__ __forceinline__ void spin_element(const ElemHeader &h, const double *
       const int no = h.aux, bs = 2 + 3 * no;
       const double *K1 = P + 4, *K2 = K1 + bs, *KR = K2 + bs;
       const double nd = KR[bs];
+      DriftStep last{};
 #pragma unroll 1
       for (int i = 0; i < h.nint; i++) {
         const Particle x0 = p;
-        drift(p, c, P[0], P[1]);
+        if (i > 0) drift_again(p, last);  // repeats the previous slice's closing drift
+        else drift(p, c, P[0], P[1]);
         mult_kick(p, no, K1);
         drift(p, c, P[2], P[3]);
         mult_kick(p, no, K2);
         drift(p, c, P[2], P[3]);
         mult_kick(p, no, K1);
-        drift(p, c, P[0], P[1]);
+        last = drift(p, c, P[0], P[1]);
         const double x1 = (p.x + x0.x) / 2., y1 = (p.y + x0.y) / 2.;
         double By, Bx;
         mult_field(x1, y1, no, KR, By, Bx);
