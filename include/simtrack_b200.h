@@ -57,9 +57,11 @@ int stb_set_flags(int h_expand, int quad_fringe);
  * Init_GSL_Seeds, 317-329); here the k-th deviate of particle i (its index in
  * the arrays of the Track call, k counting its radiating slices from turn 0)
  * is a function of (seed, i, k): Philox4x32-10 and Box-Muller, the same on
- * every launch shape.  Radiating tables are tracked by the stb_track_* entry
- * points (not the scan, Track_Radial, spin or static ones); GSBEND's photon
- * Monte Carlo (radiate2) is not implemented (STB_EUNSUPPORTED). */
+ * every launch shape.  Radiating tables are tracked by the stb_track_* and
+ * stb_track_spin_* entry points (spin tables: radiate after each slice's spin
+ * rotation of SBEND and SBENDMULT, 7519-7529, 7887-7918), not by the scan,
+ * Track_Radial or static ones; GSBEND's photon Monte Carlo (radiate2) is not
+ * implemented (STB_EUNSUPPORTED). */
 int stb_set_radiation(int radiate, unsigned long long seed);
 /* out[0..7] = GP.gamma, GP.beta, GP.energy, GP.brho, GP.Q, GP.energy0, GP.G, GP.p */
 int stb_get_ref(double *out8);

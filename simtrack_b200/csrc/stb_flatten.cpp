@@ -204,6 +204,12 @@ bool spin_form(Builder &B, const Element &E, ElemHeader &h, double &fl) {
     B.push(an);
     B.push(href);
     fl += 2 * kFlEdge + Nint * (kFlBend + kFlSpin);
+    if (GP.radiate) {  // radiate() after each slice's rotation, 7529
+      h.flags |= EF_RADIATE | EF_CHANGES_PT;
+      B.push(std::pow(GP.energy / 1000., 3));
+      fl += Nint * kFlRadiate;
+      B.t.pt_refreshes += Nint;
+    }
     return true;
   }
   if (T == "QUAD" || T == "SKEWQ" || T == "SEXT" || T == "OCT") {
@@ -316,6 +322,13 @@ bool spin_form(Builder &B, const Element &E, ElemHeader &h, double &fl) {
       fl += 2 * kFlEdge + Nint * (4 * kFlBend + 2 * mult_kick_flops(Norder, k1, s1) +
                                   mult_kick_flops(Norder, k2, s2) + mult_kick_flops(Norder, knl, knsl) + 8 +
                                   kFlSpin);
+      if (GP.radiate) {  // radiate() after each slice's rotation, 7918
+        h.flags |= EF_RADIATE | EF_CHANGES_PT;
+        B.push(Lint);
+        B.push(std::pow(GP.energy / 1000., 3));
+        fl += Nint * kFlRadiate;
+        B.t.pt_refreshes += Nint;
+      }
     }
     return true;
   }
@@ -348,8 +361,6 @@ unsigned long long g_radiation_seed = 1324;
 
 HostTable flatten_impl(const Line &line, bool spin) {
   if (GP.H_expand) throw Error(STB_EUNSUPPORTED, "GP.H_expand == true is not implemented on the GPU path");
-  if (GP.radiate && spin)
-    throw Error(STB_EUNSUPPORTED, "GP.radiate == true is not implemented for spin tracking on the GPU path");
   Builder B;
   HostTable &t = B.t;
   t.ref.gamma = GP.gamma;

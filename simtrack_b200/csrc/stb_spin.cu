@@ -11,13 +11,13 @@
 //
 // Parameter layouts of the spin opcodes (after the optional misalignment
 // block [dx, dy, cos(dpsi), sin(dpsi)]), as stb_flatten.cpp writes them:
-//   OP_S_SBEND          [tan(E1)h, tan(E2)h, sub-bend(6), Angle/Nint, Angle/L]
+//   OP_S_SBEND          [tan(E1)h, tan(E2)h, sub-bend(6), Angle/Nint, Angle/L (, E3 with EF_RADIATE)]
 //   OP_S_MPOLE_THICK    [d1, d1/b, d2, d2/b, k1 kick pair, k2 kick pair, KL, KSL, Nint]   aux = order
 //   OP_S_MPOLE_KICK     [KL, KSL, Nint]                                                 aux = order
 //   OP_S_MULT_THICK     [d1, d1/b, d2, d2/b, block(k1), block(k2), block(KNL), Nint]     aux = Norder
 //   OP_S_MULT_KICK      [block(KNL)]                                                    aux = Norder
 //   OP_S_BENDMULT       [tan(E1)h, tan(E2)h, bend(d1), bend(d2), block(k1), block(k2), block(KNL),
-//                        Angle/Nint, Angle/L, Angle, Nint]                              aux = Norder
+//                        Angle/Nint, Angle/L, Angle, Nint (, Lint, E3 with EF_RADIATE)]  aux = Norder
 //   OP_S_BENDMULT_KICK  [block(KNL), Angle]                                             aux = Norder
 //   OP_S_KICK           [L/2, L/2/b, HKICK, VKICK]
 //   OP_S_SOLEN          [q*Bz/2, L, Nint, L/Nint, L/beta/c, m0, p0, Bz*(L/Nint)/brho]  (Bz = KS*brho/L)
@@ -174,6 +174,7 @@ __device__ __forceinline__ void spin_element(const ElemHeader &h, const double *
         const Particle x0 = p;
         bend_exact(p, c, P + 2);
         spin_rotate(x0, c, R, an, href, 0., an, 0., s);
+        if (h.flags & EF_RADIATE) radiate_step(p, c, R, P[2], href, 0., an, 0., P[10], false, 0., 0.);
       }
       p.px = p.px + P[1] * p.x;
       p.py = p.py - P[1] * p.y;
@@ -262,7 +263,9 @@ __device__ __forceinline__ void spin_element(const ElemHeader &h, const double *
         const double x1 = (p.x + x0.x) / 2., y1 = (p.y + x0.y) / 2.;
         double By, Bx;
         mult_field(x1, y1, no, KR, By, Bx);
-        spin_rotate(x0, c, R, an, href, Bx / nd, (Angle + By) / nd, 0., s);
+        const double B0 = Bx / nd, B1 = (Angle + By) / nd;
+        spin_rotate(x0, c, R, an, href, B0, B1, 0., s);
+        if (h.flags & EF_RADIATE) radiate_step(p, c, R, KR[bs + 4], href, B0, B1, 0., KR[bs + 5], false, 0., 0.);
       }
       p.px = p.px + P[1] * p.x;
       p.py = p.py - P[1] * p.y;

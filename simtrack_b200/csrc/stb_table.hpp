@@ -69,6 +69,10 @@ enum : int16_t {
   // previous one: a kick that leaves x and y untouched, no misalignment, an
   // aperture no tighter than the previous element's.
   EF_NO_LOSS_CHECK = 64,
+  // GP.radiate in a spin table: radiate() after each slice's spin rotation
+  // (SBEND_sPass 7519-7529, SBENDMULT_sPass 7887-7918); the element's
+  // parameters end with [Lint, E3] (OP_S_BENDMULT) or [E3] (OP_S_SBEND).
+  EF_RADIATE = 128,
 };
 
 struct ElemHeader {

@@ -131,9 +131,38 @@ def test_unsupported_uses_are_rejected(ring):
         tab.track_radial_host(_particles(4), 2)
     with pytest.raises(SimTrackError):
         api.Scan([tab], [_particles(64)])
-    with pytest.raises(SimTrackError):
-        api.SpinTable(lt.build_line(lat))
     gs = lt.Lattice("gsbend_rad", [lt.ElementSpec("GSBEND", "g", (2.0, 0.01, 0.0101, 0.0, 0.0))],
                     lat.gamma, E0=lat.E0, Q=-1.0, radiate=True)
     with pytest.raises(SimTrackError):
         Table(lt.build_line(gs))
+
+
+def test_spin_tracking_with_radiation_vs_reference():
+    """Track_Spin with GP.radiate: SBEND_sPass and SBENDMULT_sPass apply
+    radiate() after each slice's spin rotation (simtrack.cpp:7529, 7918; no
+    quantum excitation in the spin passes).  Electron G; every element for 50
+    turns against the correctly rounded reference."""
+    from test_gpu_spin import assert_close9
+    _need_ref()
+    g_e = 0.00115965218
+    lat = lt.electron_ring()
+    ref = oracle_bridge.RefOracle(cr=True)
+    api.Set_Spin_G(g_e)
+    try:
+        tab = api.SpinTable(lt.build_line(lat))
+        ref.build(lat)
+        ref.L.ref_set_spin_g(g_e)
+        X = np.zeros((4, 9))
+        X[:, :6] = _particles(4, seed=8)
+        X[:, 7] = 1.0  # spin along y
+        X[1, 6:9] = [0.6, 0.8, 0.0]
+        nt = 50
+        xg, st, ltn, lp, dump = tab.track_probe(X.copy(), nt)
+        for i, x0 in enumerate(X):
+            xo, so, lo, po, do = ref.track_spin_dump(x0, nt)
+            assert (st[i], ltn[i], lp[i]) == (so, lo, po), f"particle {i}"
+            assert_close9(dump[i], do, f"particle {i}")
+        assert np.abs(xg[:, 5] - X[:, 5]).max() > 1e-6  # radiation moved the momentum deviation
+    finally:
+        api.Set_Spin_G(1.7928474)
+        ref.L.ref_set_spin_g(1.7928474)
