@@ -50,9 +50,9 @@ int stb_set_flags(int h_expand, int quad_fringe);
 
 /* GP.radiate (simtrack.h:57): synchrotron radiation in the sector bends
  * (SBEND_Pass's radiating branch, simtrack.cpp:4740-4748: radiate1 with
- * quantum excitation after each of the Nint slices) and in GMULT/SBENDMULT
- * (5312-5338, 5437-5463: radiate after each slice), for tables created after
- * the call.  The reference draws the quantum-excitation deviates from GSL's
+ * quantum excitation after each of the Nint slices), in GMULT/SBENDMULT
+ * (5312-5338, 5437-5463: radiate after each slice) and in GSBEND (4866-4873:
+ * radiate2), for tables created after the call.  The reference draws the quantum-excitation deviates from GSL's
  * sequential stream (gsl_ran_gaussian on gsl_r2, seeded 1324 in
  * Init_GSL_Seeds, 317-329); here the k-th deviate of particle i (its index in
  * the arrays of the Track call, k counting its radiating slices from turn 0)
@@ -60,8 +60,9 @@ int stb_set_flags(int h_expand, int quad_fringe);
  * every launch shape.  Radiating tables are tracked by the stb_track_* and
  * stb_track_spin_* entry points (spin tables: radiate after each slice's spin
  * rotation of SBEND and SBENDMULT, 7519-7529, 7887-7918), not by the scan,
- * Track_Radial or static ones; GSBEND's photon Monte Carlo (radiate2) is not
- * implemented (STB_EUNSUPPORTED). */
+ * Track_Radial or static ones.  GSBEND radiates by photon Monte Carlo
+ * (radiate2, 4290-4372), its Poisson photon count and photon uniforms drawn
+ * from the same per-particle generator. */
 int stb_set_radiation(int radiate, unsigned long long seed);
 /* out[0..7] = GP.gamma, GP.beta, GP.energy, GP.brho, GP.Q, GP.energy0, GP.G, GP.p */
 int stb_get_ref(double *out8);

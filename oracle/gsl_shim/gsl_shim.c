@@ -121,10 +121,14 @@ int gsl_eigen_nonsymmv_sort(gsl_vector_complex *eval, gsl_matrix_complex *evec, 
 void gsl_rng_env_setup(void) { not_in_shim("gsl_rng_env_setup"); }
 gsl_rng *gsl_rng_alloc(const gsl_rng_type *T) { (void)T; not_in_shim("gsl_rng_alloc"); return NULL; }
 void gsl_rng_set(const gsl_rng *r, unsigned long s) { (void)r; (void)s; not_in_shim("gsl_rng_set"); }
-double gsl_rng_uniform(const gsl_rng *r) { (void)r; not_in_shim("gsl_rng_uniform"); return 0.0; }
+/* radiate2's photon draws (simtrack.cpp:4345, 4349): the harness's streams
+   (ref_harness.cpp, ref_rng_poisson / ref_rng_uniform) in place of GSL's. */
+double ref_rng_uniform(void);
+unsigned int ref_rng_poisson(double mu);
+double gsl_rng_uniform(const gsl_rng *r) { (void)r; return ref_rng_uniform(); }
 /* radiate1's quantum-excitation deviate (simtrack.cpp:4275): GSL's own
    stream does not exist here, so the harness supplies the tracker's
    per-particle counter-based stream (ref_harness.cpp, ref_rng_gaussian). */
 double ref_rng_gaussian(void);
 double gsl_ran_gaussian(const gsl_rng *r, double sigma) { (void)r; return sigma * ref_rng_gaussian(); }
-unsigned int gsl_ran_poisson(const gsl_rng *r, double mu) { (void)r; (void)mu; not_in_shim("gsl_ran_poisson"); return 0; }
+unsigned int gsl_ran_poisson(const gsl_rng *r, double mu) { (void)r; return ref_rng_poisson(mu); }

@@ -146,9 +146,41 @@ double stream_gaussian(unsigned long long seed, unsigned long long id, unsigned 
   return std::sqrt(-2.0 * series_log(u1)) * std::cos(6.283185307179586 * u2);
 }
 
+// radiate2's photon draws: for the particle's k-th radiating slice, draw 0
+// gives the photon count (Poisson by inversion from exp(-mu), at most 1000)
+// and draws 1, 2, ... the photons' uniforms; Philox counter (k, 2^31 | j,
+// id), key seed.
+unsigned long long g_photon_k = 0;
+uint32_t g_photon_j = 0;
+
+double stream_uniform(unsigned long long seed, unsigned long long id, unsigned long long k, uint32_t j) {
+  uint32_t c[4] = {(uint32_t)k, 0x80000000u | j, (uint32_t)id, (uint32_t)(id >> 32)};
+  philox10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+  const uint64_t w = ((uint64_t)c[0] << 32) | c[1];
+  return (double)((w >> 11) + 1) * (1.0 / 9007199254740992.0);
+}
+
 }  // namespace
 
 extern "C" double ref_rng_gaussian(void) { return stream_gaussian(g_rng_seed, (unsigned long long)g_rng_id, g_rng_k++); }
+
+extern "C" unsigned int ref_rng_poisson(double mu) {
+  g_photon_k = g_rng_k++;
+  g_photon_j = 0;
+  const double u = stream_uniform(g_rng_seed, (unsigned long long)g_rng_id, g_photon_k, 0);
+  double term = std::exp(-mu), cdf = term;
+  unsigned int count = 0;
+  while (u > cdf && count < 1000) {
+    count = count + 1;
+    term = term * mu / (double)count;
+    cdf = cdf + term;
+  }
+  return count;
+}
+
+extern "C" double ref_rng_uniform(void) {
+  return stream_uniform(g_rng_seed, (unsigned long long)g_rng_id, g_photon_k, ++g_photon_j);
+}
 
 extern "C" {
 

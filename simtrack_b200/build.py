@@ -28,7 +28,7 @@ CUDA_SOURCES = ["stb_track.cu", "stb_track_fast.cu", "stb_scan.cu", "stb_track_s
 CXX_SOURCES = ["stb_elements.cpp", "stb_flatten.cpp", "stb_capi.cpp", "stb_scan_host.cpp", "stb_mlp_host.cpp",
                "stb_tune_host.cpp", "stb_readers.cpp", "stb_da.cpp",
                "stb_orbit.cpp", "stb_tbt.cpp"]
-HEADERS = ["stb_table.hpp", "stb_physics.cuh", "stb_crmath.cuh", "stb_sincos_table.cuh", "stb_rng.cuh", "stb_kernels.hpp", "stb_status.hpp", "stb_flatten.hpp",
+HEADERS = ["stb_table.hpp", "stb_physics.cuh", "stb_crmath.cuh", "stb_sincos_table.cuh", "stb_rng.cuh", "stb_photon_spectrum.cuh", "stb_kernels.hpp", "stb_status.hpp", "stb_flatten.hpp",
            "stb_track_impl.cuh", "stb_track_launch.cuh", "stb_scan.hpp", "stb_runtime.hpp", "stb_mlp.hpp", "stb_tune.hpp"]
 
 # Units compiled with FMA contraction: the fast tracking kernel only.

@@ -497,8 +497,37 @@ HostTable flatten_impl(const Line &line, bool spin) {
       if (Angle == 0.) {
         as_drift(L);
       } else if (GP.radiate) {
-        throw Error(STB_EUNSUPPORTED, "element " + E.NAME +
-                                          ": GSBEND with GP.radiate (radiate2, photon Monte Carlo) is not implemented");
+        // radiating exact branch, simtrack.cpp:4866-4873: Nint slices of
+        // general_sbend_exact_pass(Lint, Angle/Nint, K0L/Nint), radiate2 after each
+        const int Nint = (int)E.GetP("Nint");
+        if (Nint <= 0) throw Error(STB_EINVAL, "element " + E.NAME + ": Nint must be positive");
+        const double href = Angle / L, hreal = K0L / L, Lint = L / Nint;
+        const double an = Angle / Nint, kn = K0L / Nint;
+        const double rhoc = Lint / an, b0 = kn / Lint;
+        h.op = OP_GSBEND_RAD;
+        h.nint = Nint;
+        h.flags |= EF_CHANGES_PT;
+        B.push(std::tan(E1) * hreal);
+        B.push(std::tan(E2) * hreal);
+        B.push(Lint);
+        B.push(Lint / GP.beta);
+        B.push(rhoc);
+        B.push(b0);
+        B.push(b0 * rhoc);
+        B.push(std::cos(an));
+        B.push(std::sin(an));
+        B.push(1.0 / rhoc);
+        B.push(1.0 / b0);
+        B.push(href);
+        B.push(kn);
+        // facg of radiate2, simtrack.cpp:4316
+        B.push(12. * std::sqrt(3.) / (std::pow(2., 1.0 / 3.0) * 5.0 * 2.6789385347077475));
+        B.push((double)t.ref.rad_slices);
+        t.ref.rad_slices += Nint;
+        if (E1 != 0.) { h.flags |= EF_EDGE1; fl += kFlEdge; }
+        if (E2 != 0.) { h.flags |= EF_EDGE2; fl += kFlEdge; }
+        fl += Nint * (kFlBend + 4 + kFlRadiate + kFlQuantum);
+        t.pt_refreshes += Nint;
       } else {
         const double hreal = K0L / L;
         const double rhoc = L / Angle, b0 = K0L / L;

@@ -28,6 +28,7 @@
 #include <cstdint>
 
 #include "stb_crmath.cuh"
+#include "stb_rng.cuh"
 #include "stb_table.hpp"
 
 namespace stb {
@@ -334,6 +335,62 @@ __device__ __forceinline__ void radiate_step(Particle &p, PtCache &c, const RefC
   } else {
     p.pt = p.pt - temp2 * bper2 * temp1 / L;
   }
+  const double delta2 = sqrt(1.0 + 2 * p.pt / R.beta + p.pt * p.pt) - 1.0;
+  const double ratio = (1 + delta2) / c.opd;
+  p.px = px0 * ratio;
+  p.py = py0 * ratio;
+  pt_refresh(R, p.pt, c);
+}
+
+// splint (simtrack.cpp:333-358): linear interpolation in a table by bisection.
+__device__ __forceinline__ double splint_dev(const double *XA, const double *YA, int N, double X) {
+  int klo = 0, khi = N - 1;
+  while (khi - klo > 1) {
+    const int k = (khi + klo) / 2;
+    if (XA[k] > X) khi = k;
+    else klo = k;
+  }
+  const double H = XA[khi] - XA[klo];
+  const double A = (XA[khi] - X) / H;
+  const double B = (X - XA[klo]) / H;
+  return A * YA[klo] + B * YA[khi];
+}
+
+// radiate2 (simtrack.cpp:4290-4372): photon emission over one step by Monte
+// Carlo, for the field (0, B1, 0): the critical energy Ec and mean photon
+// count Nr of the step, Ng photons drawn with mean Nr, each photon's energy
+// from the spectrum table (or (u/facg)^3 below u = 0.26).  `draws(j)` returns
+// the step's j-th uniform (j = 0: the photon count).  As in the reference,
+// the vertical slope uses x[1] (px) in place of x[3] (simtrack.cpp:4328).
+template <class Draws>
+__device__ __forceinline__ void radiate2_step(Particle &p, PtCache &c, const RefConsts &R, double L, double href,
+                                              double B1, double facg, const double *XA, const double *YA, int N,
+                                              Draws draws) {
+  const double px0 = p.px, py0 = p.py;
+  const double alpha = 1.0 / 137.0359997;
+  const double gamma1 = R.gamma + R.sqrt_g2m1 * p.pt;
+  const double pz = sqrt(c.opd2 - p.px * p.px - p.py * p.py);
+  const double xp = (1 + p.x * href) * p.px / pz;
+  const double yp = (1 + p.x * href) * p.px / pz;
+  const double temp1 = sqrt((1 + p.x * href) * (1 + p.x * href) + xp * xp + yp * yp);
+  const double u0 = xp / temp1, u1 = yp / temp1, u2 = (1 + p.x * href) / temp1;
+  const double B0 = 0., B2 = 0.;
+  const double b0 = B1 * u2 - B2 * u1;
+  const double b1 = -1.0 * B0 * u2 + B2 * u0;
+  const double b2 = B0 * u1 - B1 * u0;
+  const double bper2 = b0 * b0 + b1 * b1 + b2 * b2;
+  const double rho1 = (1 + p.pt) / sqrt(bper2) * L;
+  const double Ec = 1.5 * 6.582119e-16 * 2.99792458e8 * gamma1 * gamma1 * gamma1 / rho1 / 1.0e6;
+  const double Nr = 5. * alpha * gamma1 / 2. / sqrt(3.) / rho1 * L * temp1 / c.beta1;
+  const int Ng = rad_poisson(draws(0u), Nr);
+  double Etot = 0.;
+  for (int i = 0; i < Ng; i++) {
+    const double rtemp = draws((uint32_t)i + 1u);
+    const double Etemp = rtemp < 0.26 ? cr_pown(rtemp / facg, 3) : splint_dev(XA, YA, N, rtemp);
+    Etot = Etot + Etemp;
+  }
+  Etot = Etot * Ec;
+  p.pt = p.pt - Etot / R.energy;
   const double delta2 = sqrt(1.0 + 2 * p.pt / R.beta + p.pt * p.pt) - 1.0;
   const double ratio = (1 + delta2) / c.opd;
   p.px = px0 * ratio;

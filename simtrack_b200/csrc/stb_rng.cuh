@@ -82,4 +82,31 @@ __host__ __device__ __forceinline__ double rad_gaussian(uint64_t seed, uint64_t 
   return sqrt(-2.0 * det_log(u1)) * cr_cos(6.283185307179586 * u2);
 }
 
+// The photon-emission draws of radiate2 (simtrack.cpp:4290-4372), which the
+// reference takes from GSL (gsl_ran_poisson on gsl_r1, gsl_rng_uniform on
+// gsl_r2): for radiating slice k of particle id, draw j = 0 is the uniform
+// behind the photon count and draws j = 1, 2, ... the photons' uniforms.  The
+// counter's second word has its top bit set, so these never coincide with
+// the normal deviates above (whose second word is k's high half, below 2^31).
+__host__ __device__ __forceinline__ double rad_uniform(uint64_t seed, uint64_t id, uint64_t k, uint32_t j) {
+  const Philox4 r = philox4x32_10(Philox4{{(uint32_t)k, 0x80000000u | j, (uint32_t)id, (uint32_t)(id >> 32)}},
+                                  (uint32_t)seed, (uint32_t)(seed >> 32));
+  const uint64_t a = ((uint64_t)r.v[0] << 32) | r.v[1];
+  return (double)((a >> 11) + 1) * 0x1p-53;  // (0, 1]
+}
+
+// Photon count with mean mu: inversion of the Poisson distribution
+// (D. E. Knuth, TAOCP vol. 2, 3.4.1), the smallest n with u <= F(n),
+// F summed term by term from exp(-mu); at most 1000.
+__host__ __device__ __forceinline__ int rad_poisson(double u, double mu) {
+  double term = cr_exp(-mu), cdf = term;
+  int n = 0;
+  while (u > cdf && n < 1000) {
+    n = n + 1;
+    term = term * mu / (double)n;
+    cdf = cdf + term;
+  }
+  return n;
+}
+
 }  // namespace stb

@@ -52,7 +52,8 @@ enum Op : int32_t {
   // Radiating forms (GP.radiate == true), orbit tables only.
   OP_SBEND_RAD = 32,     // SBEND_Pass exact radiating branch: Nint slices + radiate1   4740-4748
   OP_BENDMULT_RAD = 33,  // GMULT/SBENDMULT exact radiating branch: + radiate           5312-5338, 5437-5463
-  OP_COUNT = 34
+  OP_GSBEND_RAD = 34,    // GSBEND_Pass exact radiating branch: Nint slices + radiate2    4866-4873
+  OP_COUNT = 35
 };
 constexpr int16_t OP_S_FIRST = OP_S_SBEND;
 constexpr int16_t OP_S_LAST = OP_S_SOLEN;

@@ -8,6 +8,7 @@
 
 #include "stb_kernels.hpp"
 #include "stb_physics.cuh"
+#include "stb_photon_spectrum.cuh"
 #include "stb_rng.cuh"
 
 namespace stb {
@@ -226,6 +227,32 @@ __device__ __forceinline__ void op_sbend_rad(const ElemHeader &h, const double *
     bend_exact(p, c, P + 2);
     const double g = rad_gaussian(R.rad_seed, (uint64_t)id, k0 + (uint64_t)s);
     radiate_step(p, c, R, Lint, href, 0., an, 0., E3, true, Cf, g);
+  }
+  if (h.flags & EF_EDGE2) {
+    p.px = p.px + P[1] * p.x;
+    p.py = p.py - P[1] * p.y;
+  }
+}
+
+// GSBEND_Pass, exact radiating branch (simtrack.cpp:4866-4873): Nint slices
+// of general_sbend_exact_pass over (Lint, Angle/Nint, K0L/Nint), each
+// followed by radiate2 with the field {0, K0L/Nint, 0}.  P = [tan(E1)hreal,
+// tan(E2)hreal, slice bend (9, as OP_GSBEND), href, K0L/Nint, facg, first
+// slice index within the turn].
+__device__ __forceinline__ void op_gsbend_rad(const ElemHeader &h, const double *P, Particle &p, PtCache &c,
+                                              const RefConsts &R, long id, long turn) {
+  if (h.flags & EF_EDGE1) {
+    p.px = p.px + P[0] * p.x;
+    p.py = p.py - P[0] * p.y;
+  }
+  const double Lint = P[2], href = P[11], kn = P[12], facg = P[13];
+  const uint64_t k0 = (uint64_t)turn * (uint64_t)R.rad_slices + (uint64_t)P[14];
+#pragma unroll 1
+  for (int s = 0; s < h.nint; s++) {
+    gbend_exact(p, c, P + 2);
+    const uint64_t k = k0 + (uint64_t)s;
+    radiate2_step(p, c, R, Lint, href, kn, facg, kPhotonU, kPhotonE, kPhotonTable,
+                  [&](uint32_t j) { return rad_uniform(R.rad_seed, (uint64_t)id, k, j); });
   }
   if (h.flags & EF_EDGE2) {
     p.px = p.px + P[1] * p.x;
@@ -457,6 +484,9 @@ __device__ __forceinline__ void apply_element(const ElemHeader &h, const double 
       break;
     case OP_BENDMULT_RAD:
       for (int k = 0; k < kPPT; k++) op_bendmult_rad(h, P, p[k], c[k], R);
+      break;
+    case OP_GSBEND_RAD:
+      for (int k = 0; k < kPPT; k++) op_gsbend_rad(h, P, p[k], c[k], R, rk.id0 + (long)k * rk.id_stride, rk.turn);
       break;
     default:
       for (int k = 0; k < kPPT; k++) op_misc(h, P, p[k], c[k], R);

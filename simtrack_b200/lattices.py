@@ -124,7 +124,8 @@ ELECTRON_MASS_MEV = 0.51099895
 
 
 def electron_ring(ncell: int = 40, energy_gev: float = 3.0, nint: int = 5, k1: float = 0.25, k2l: float = 0.3,
-                  vrf_mv: float = 2.0, harmonic: int = 400, radiate: bool = True, seed: int = 1324) -> Lattice:
+                  vrf_mv: float = 2.0, harmonic: int = 400, radiate: bool = True, seed: int = 1324,
+                  gsbend: bool = False) -> Lattice:
     """An electron storage ring with synchrotron radiation (GP.radiate): `ncell`
     FODO cells, each with a thick sector dipole (L = 2 m, `nint` slices, each
     followed by radiation with quantum excitation) and a combined-function
@@ -132,7 +133,9 @@ def electron_ring(ncell: int = 40, energy_gev: float = 3.0, nint: int = 5, k1: f
     quadrupole component, radiation after each slice), thick quadrupoles
     (K1 = +/-`k1` m^-2), thin sextupoles and one thin RF cavity.  Electrons
     (Q = -1) at `energy_gev` total energy; the two dipoles of a cell bend by
-    2 pi / ncell together."""
+    2 pi / ncell together.  gsbend=True makes the sector dipoles GSBENDs whose
+    field is 0.2 % above the frame's curvature (radiation by photon Monte
+    Carlo, radiate2)."""
     gamma = energy_gev * 1000.0 / ELECTRON_MASS_MEV
     ang = 2 * math.pi / ncell
     a1, a2 = 0.6 * ang, 0.4 * ang
@@ -145,7 +148,8 @@ def electron_ring(ncell: int = 40, energy_gev: float = 3.0, nint: int = 5, k1: f
             ElementSpec("DRIFT", f"d1_{c}", (0.4,)),
             ElementSpec("SEXT", f"sf{c}", (0.0, k2l, 0.0)),
             ElementSpec("DRIFT", f"d2_{c}", (0.4,)),
-            ElementSpec("SBEND", f"b{c}", (2.0, a1, 0.0, 0.0), {"Nint": nint}),
+            (ElementSpec("GSBEND", f"b{c}", (2.0, a1, a1 * 1.002, 0.0, 0.0), {"Nint": nint}) if gsbend else
+             ElementSpec("SBEND", f"b{c}", (2.0, a1, 0.0, 0.0), {"Nint": nint})),
             ElementSpec("DRIFT", f"d3_{c}", (0.4,)),
             ElementSpec("QUAD", f"qd{c}", (0.5, -k1 * 0.5, 0.0), {"Nint": 4}),
             ElementSpec("DRIFT", f"d4_{c}", (0.4,)),

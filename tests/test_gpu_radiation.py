@@ -131,10 +131,6 @@ def test_unsupported_uses_are_rejected(ring):
         tab.track_radial_host(_particles(4), 2)
     with pytest.raises(SimTrackError):
         api.Scan([tab], [_particles(64)])
-    gs = lt.Lattice("gsbend_rad", [lt.ElementSpec("GSBEND", "g", (2.0, 0.01, 0.0101, 0.0, 0.0))],
-                    lat.gamma, E0=lat.E0, Q=-1.0, radiate=True)
-    with pytest.raises(SimTrackError):
-        Table(lt.build_line(gs))
 
 
 def test_spin_tracking_with_radiation_vs_reference():
@@ -166,3 +162,36 @@ def test_spin_tracking_with_radiation_vs_reference():
     finally:
         api.Set_Spin_G(1.7928474)
         ref.L.ref_set_spin_g(1.7928474)
+
+
+def test_gsbend_photon_emission_vs_reference():
+    """GSBEND_Pass's radiating branch (simtrack.cpp:4866-4873): radiate2's
+    photon Monte Carlo (Poisson photon count, energies from the spectrum
+    table) after each slice, the draws from the per-particle streams on both
+    sides.  Every element for 100 turns and a 128-particle grid over 200 turns
+    against the correctly rounded reference."""
+    import dataclasses
+    _need_ref()
+    lat = lt.electron_ring(gsbend=True)
+    tab = Table(lt.build_line(lat))
+    ref = oracle_bridge.RefOracle(cr=True)
+    ref.build(lat)
+    X = _particles(4, seed=21)
+    nt = 100
+    xg, st, ltn, lp, dump = tab.track_probe(X.copy(), nt)
+    for i, x0 in enumerate(X):
+        ref.L.ref_rng_id_base(i)
+        xo, so, lo, po, do = ref.track_dump(x0, nt, 0.0)
+        assert (st[i], ltn[i], lp[i]) == (so, lo, po), f"particle {i}"
+        assert_close_traj(dump[i], do, f"particle {i}")
+    plain = lt.electron_ring(gsbend=True, radiate=False)
+    ref.build(plain)
+    assert abs(ref.track_dump(X[0], nt, 0.0)[0][5] - xg[0, 5]) > 1e-7  # photons were emitted
+    Y = _particles(128, seed=22)
+    xg2, sg2, lg2, pg2 = tab.track_host(Y.copy(), 200, 0.01)
+    xo2, so2, lo2, po2 = oracle_bridge.ref_track_parallel(dataclasses.replace(lat, aperture_radius=0.01), Y, 200,
+                                                          cr=True)
+    assert np.array_equal(sg2, so2)
+    lost = so2 == 0
+    assert np.array_equal(lg2[lost], lo2[lost]) and np.array_equal(pg2[lost], po2[lost])
+    assert_close_traj(xg2[~lost], xo2[~lost], "survivors")
