@@ -507,6 +507,24 @@ int stb_bb4d_soft_gaussian_device(double Np1, long n1, double *x1, double Np2, l
 int stb_bb4d_soft_gaussian_host(double Np1, long n1, double *x1, double Np2, long n2, double *x2, double gamma1,
                                 double gamma2, double bbscale1, double bbscale2, int device);
 
+/* Strong-strong beam-beam, sliced soft-Gaussian 6D: BeamBeam6D_SoftGaussian(
+ * Np1, Mp1, x1, Np2, Mp2, x2, gamma1, gamma2, bbscale1, bbscale2, Nslice1,
+ * Nslice2), simtrack.cpp:22874-23132 (simtrack.h:1406).  Both AoS bunches are
+ * reordered in place by z, largest first (equal z keep their order), cut
+ * into Nslice slices of Mp/Nslice particles (the remainder is not collided);
+ * the slice pairs collide in the reference's order, each drifting to its
+ * collision point, kicking as soft Gaussians (BB4D with N/Nslice) and
+ * drifting back.  Unlike the reference, no slice-centroid files are written.
+ * Every slice needs at least two particles.  The _device form synchronises
+ * `stream` (the pair order is decided on the host from the slice centroids);
+ * one collision at a time per device. */
+int stb_bb6d_soft_gaussian_device(double Np1, long Mp1, double *x1, double Np2, long Mp2, double *x2, double gamma1,
+                                  double gamma2, double bbscale1, double bbscale2, int nslice1, int nslice2,
+                                  int device, void *stream);
+int stb_bb6d_soft_gaussian_host(double Np1, long Mp1, double *x1, double Np2, long Mp2, double *x2, double gamma1,
+                                double gamma2, double bbscale1, double bbscale2, int nslice1, int nslice2,
+                                int device);
+
 /* Diagnostics: deviates k0 .. k0+n-1 of particle `id`'s quantum-excitation
  * stream under `seed` (see stb_set_radiation), evaluated on GPU `device` or
  * on the host (device < 0); out is host memory. */

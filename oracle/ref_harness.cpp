@@ -458,6 +458,13 @@ void ref_track_dump(void *line, double *x, int nturn, double radius, double *dum
 
 double ref_pinv(double p) { return gsl_cdf_ugaussian_Pinv(p); }
 
+// The reference's sliced 6D soft-Gaussian collision, called as is (it also
+// writes ./bunch1_Z.dat and ./bunch2_Z.dat in the working directory).
+void ref_bb6d_soft_gaussian(double Np1, int Mp1, double *x1, double Np2, int Mp2, double *x2, double gamma1,
+                            double gamma2, double bbscale1, double bbscale2, int ns1, int ns2) {
+  BeamBeam6D_SoftGaussian(Np1, Mp1, x1, Np2, Mp2, x2, gamma1, gamma2, bbscale1, bbscale2, ns1, ns2);
+}
+
 // The reference's strong-strong soft-Gaussian collision, called as is.
 void ref_bb4d_soft_gaussian(double Np1, int n1, double *x1, double Np2, int n2, double *x2, double gamma1,
                             double gamma2, double bbscale1, double bbscale2) {

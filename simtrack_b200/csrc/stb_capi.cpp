@@ -1202,6 +1202,55 @@ int stb_bb4d_soft_gaussian_host(double Np1, long n1, double *x1, double Np2, lon
   });
 }
 
+namespace {
+void soft_gaussian_6d_args(long Mp1, long Mp2, double gamma1, double gamma2, int ns1, int ns2) {
+  if (ns1 < 1 || ns2 < 1 || (long)ns1 * ns2 > 4096) throw Error(STB_EINVAL, "slice counts must be 1..4096 pairs");
+  if (Mp1 / ns1 < 2 || Mp2 / ns2 < 2) throw Error(STB_EINVAL, "every slice needs at least two macro-particles");
+  if (Mp1 > 0x7fffffffL || Mp2 > 0x7fffffffL) throw Error(STB_EINVAL, "too many macro-particles");
+  if (!(gamma1 > 0) || !(gamma2 > 0)) throw Error(STB_EINVAL, "gamma must be positive");
+}
+}  // namespace
+
+int stb_bb6d_soft_gaussian_device(double Np1, long Mp1, double *x1, double Np2, long Mp2, double *x2, double gamma1,
+                                  double gamma2, double bbscale1, double bbscale2, int nslice1, int nslice2,
+                                  int device, void *stream) {
+  return guarded([&] {
+    if (!x1 || !x2) throw Error(STB_EINVAL, "NULL bunch");
+    soft_gaussian_6d_args(Mp1, Mp2, gamma1, gamma2, nslice1, nslice2);
+    DeviceGuard g(device);
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    cuda_check(soft_gaussian_6d(Np1, Mp1, x1, Np2, Mp2, x2, gamma1, gamma2, bbscale1, bbscale2, nslice1, nslice2,
+                                sms, (cudaStream_t)stream),
+               "sliced soft-Gaussian beam-beam");
+    return STB_OK;
+  });
+}
+
+int stb_bb6d_soft_gaussian_host(double Np1, long Mp1, double *x1, double Np2, long Mp2, double *x2, double gamma1,
+                                double gamma2, double bbscale1, double bbscale2, int nslice1, int nslice2,
+                                int device) {
+  return guarded([&] {
+    if (!x1 || !x2) throw Error(STB_EINVAL, "NULL bunch");
+    soft_gaussian_6d_args(Mp1, Mp2, gamma1, gamma2, nslice1, nslice2);
+    DeviceGuard g(device);
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    double *d = nullptr;
+    const size_t b1 = sizeof(double) * 6 * (size_t)Mp1, b2 = sizeof(double) * 6 * (size_t)Mp2;
+    cuda_check(cudaMalloc(&d, b1 + b2), "cudaMalloc(bunches)");
+    DevFree f{d};
+    cuda_check(cudaMemcpy(d, x1, b1, cudaMemcpyHostToDevice), "upload bunch 1");
+    cuda_check(cudaMemcpy(d + 6 * Mp1, x2, b2, cudaMemcpyHostToDevice), "upload bunch 2");
+    cuda_check(soft_gaussian_6d(Np1, Mp1, d, Np2, Mp2, d + 6 * Mp1, gamma1, gamma2, bbscale1, bbscale2, nslice1,
+                                nslice2, sms, 0),
+               "sliced soft-Gaussian beam-beam");
+    cuda_check(cudaMemcpy(x1, d, b1, cudaMemcpyDeviceToHost), "download bunch 1");
+    cuda_check(cudaMemcpy(x2, d + 6 * Mp1, b2, cudaMemcpyDeviceToHost), "download bunch 2");
+    return STB_OK;
+  });
+}
+
 int stb_rad_normals(unsigned long long seed, unsigned long long id, unsigned long long k0, long n, double *out,
                     int device) {
   return guarded([&] {

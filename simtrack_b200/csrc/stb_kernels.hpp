@@ -90,6 +90,14 @@ void philox_block(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4])
 // BeamBeam4D_SoftGaussian on device AoS beams (stb_ssbb.cu); c4_k = 2 N_other rp / gamma_k.
 cudaError_t soft_gaussian_4d(double *x1, long n1, double *x2, long n2, double c4_1, double c4_2, double bbscale1,
                              double bbscale2, int num_sms, cudaStream_t s);
+cudaError_t sort_bunch_by_z(double *x, long n, double *scratch, int32_t *order, cudaStream_t s);
+cudaError_t slice_mean_z(const double *x, int nslice, long m, double *z, cudaStream_t s);
+cudaError_t slice_pair_collision(double *x1, long m1, double *x2, long m2, double S, double c4_1, double c4_2,
+                                 double bbscale1, double bbscale2, int num_sms, cudaStream_t s);
+// BeamBeam6D_SoftGaussian on device AoS bunches (synchronises `s`).
+cudaError_t soft_gaussian_6d(double Np1, long Mp1, double *x1, double Np2, long Mp2, double *x2, double gamma1,
+                             double gamma2, double bbscale1, double bbscale2, int Nslice1, int Nslice2, int num_sms,
+                             cudaStream_t s);
 
 size_t track_smem_bytes(int nelem, int npool_padded);
 // The loss-test mode of a launch with circular aperture r2 (+inf: none) on a

@@ -17,6 +17,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <vector>
 
 #include "stb_kernels.hpp"
 #include "stb_physics.cuh"
@@ -79,7 +80,90 @@ __global__ void soft_gaussian_kick_kernel(double *x, long n, const double *m4, d
 // device).
 __device__ double g_soft_gaussian_moments[8];
 
+// Rank of particle i when the bunch is ordered by z, largest first (the
+// order of BeamBeam6D_SoftGaussian's exchange sort, simtrack.cpp:22897-22916,
+// for distinct z; equal z keep their input order): order[rank] = i.
+constexpr int kRankBlock = 256;
+__global__ void __launch_bounds__(kRankBlock) z_rank_kernel(const double *x, long n, int32_t *order) {
+  __shared__ double zt[kRankBlock];
+  const long i = (long)blockIdx.x * kRankBlock + threadIdx.x;
+  const double zi = i < n ? x[6 * i + 4] : 0.0;
+  long rank = 0;
+  for (long t0 = 0; t0 < n; t0 += kRankBlock) {
+    const long j = t0 + threadIdx.x;
+    zt[threadIdx.x] = j < n ? x[6 * j + 4] : 0.0;
+    __syncthreads();
+    const int m = (int)(n - t0 < kRankBlock ? n - t0 : kRankBlock);
+    for (int k = 0; k < m; k++) {
+      const double zj = zt[k];
+      rank += (zj > zi || (zj == zi && t0 + k < i)) ? 1 : 0;
+    }
+    __syncthreads();
+  }
+  if (i < n) order[rank] = (int32_t)i;
+}
+
+__global__ void gather_particles_kernel(const double *src, const int32_t *order, long n, double *dst) {
+  for (long r = (long)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (long)gridDim.x * blockDim.x) {
+    const long i = order[r];
+    for (int k = 0; k < 6; k++) dst[6 * r + k] = src[6 * i + k];
+  }
+}
+
+// Mean z of each slice of m consecutive particles (the reference's running
+// sum, 22986-23004): one thread per slice.
+__global__ void slice_mean_z_kernel(const double *x, int nslice, long m, double *z) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nslice) return;
+  double t = 0;
+  for (long j = (long)s * m; j < (long)(s + 1) * m; j++) t = t + x[6 * j + 4];
+  z[s] = t / (double)m;
+}
+
+// x += sign * px * S, y += sign * py * S over n particles (the drift to and
+// from the slices' collision point, 23059-23066, 23096-23103).
+__global__ void slice_drift_kernel(double *x, long n, double S, bool forward) {
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    double *p = x + 6 * i;
+    if (forward) {
+      p[0] = p[0] + p[1] * S;
+      p[2] = p[2] + p[3] * S;
+    } else {
+      p[0] = p[0] - p[1] * S;
+      p[2] = p[2] - p[3] * S;
+    }
+  }
+}
+
 }  // namespace
+
+cudaError_t sort_bunch_by_z(double *x, long n, double *scratch, int32_t *order, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  z_rank_kernel<<<(unsigned)((n + kRankBlock - 1) / kRankBlock), kRankBlock, 0, s>>>(x, n, order);
+  gather_particles_kernel<<<(unsigned)((n + 255) / 256 < 4096 ? (n + 255) / 256 : 4096), 256, 0, s>>>(x, order, n,
+                                                                                                    scratch);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  return cudaMemcpyAsync(x, scratch, sizeof(double) * 6 * (size_t)n, cudaMemcpyDeviceToDevice, s);
+}
+
+cudaError_t slice_mean_z(const double *x, int nslice, long m, double *z, cudaStream_t s) {
+  slice_mean_z_kernel<<<(nslice + 63) / 64, 64, 0, s>>>(x, nslice, m, z);
+  return cudaGetLastError();
+}
+
+cudaError_t slice_pair_collision(double *x1, long m1, double *x2, long m2, double S, double c4_1, double c4_2,
+                                 double bbscale1, double bbscale2, int num_sms, cudaStream_t s) {
+  const unsigned g1 = (unsigned)((m1 + 255) / 256 < num_sms * 8 ? (m1 + 255) / 256 : num_sms * 8);
+  const unsigned g2 = (unsigned)((m2 + 255) / 256 < num_sms * 8 ? (m2 + 255) / 256 : num_sms * 8);
+  slice_drift_kernel<<<g1 < 1 ? 1 : g1, 256, 0, s>>>(x1, m1, S, true);
+  slice_drift_kernel<<<g2 < 1 ? 1 : g2, 256, 0, s>>>(x2, m2, -S, true);
+  cudaError_t e = soft_gaussian_4d(x1, m1, x2, m2, c4_1, c4_2, bbscale1, bbscale2, num_sms, s);
+  if (e != cudaSuccess) return e;
+  slice_drift_kernel<<<g1 < 1 ? 1 : g1, 256, 0, s>>>(x1, m1, S, false);
+  slice_drift_kernel<<<g2 < 1 ? 1 : g2, 256, 0, s>>>(x2, m2, -S, false);
+  return cudaGetLastError();
+}
 
 cudaError_t soft_gaussian_4d(double *x1, long n1, double *x2, long n2, double c4_1, double c4_2, double bbscale1,
                              double bbscale2, int num_sms, cudaStream_t s) {
@@ -97,6 +181,66 @@ cudaError_t soft_gaussian_4d(double *x1, long n1, double *x2, long n2, double c4
   if (n1 > 0) soft_gaussian_kick_kernel<<<grid(n1), block, 0, s>>>(x1, n1, d_m8 + 4, c4_1, bbscale1);
   if (n2 > 0) soft_gaussian_kick_kernel<<<grid(n2), block, 0, s>>>(x2, n2, d_m8, c4_2, bbscale2);
   return cudaGetLastError();
+}
+
+// BeamBeam6D_SoftGaussian (simtrack.cpp:22874-23132) on device AoS bunches:
+// both bunches ordered by z (largest first) in place; each cut into Nslice
+// slices of Mp/Nslice consecutive particles (the remainder is not
+// collided); slice pairs (i, j) taken in increasing order of
+// -(Z1[i] + Z2[j])/2 by the reference's own exchange sort; for each pair
+// both slices drift to the collision point (S = (Z1[i] - Z2[j])/2), kick
+// each other as soft Gaussians (strength N/Nslice) and drift back.  The
+// reference also writes its slice centroids to ./bunch1_Z.dat and
+// ./bunch2_Z.dat on every call; nothing is written here.
+cudaError_t soft_gaussian_6d(double Np1, long Mp1, double *x1, double Np2, long Mp2, double *x2, double gamma1,
+                             double gamma2, double bbscale1, double bbscale2, int Nslice1, int Nslice2, int num_sms,
+                             cudaStream_t s) {
+  const long nmax = Mp1 > Mp2 ? Mp1 : Mp2;
+  double *scratch = nullptr;
+  cudaError_t e = cudaMalloc(&scratch, sizeof(double) * (6 * (size_t)nmax + (size_t)Nslice1 + (size_t)Nslice2) +
+                                           sizeof(int32_t) * (size_t)nmax);
+  if (e != cudaSuccess) return e;
+  double *dz = scratch + 6 * nmax;
+  int32_t *order = reinterpret_cast<int32_t *>(dz + Nslice1 + Nslice2);
+  const long m1 = Mp1 / Nslice1, m2 = Mp2 / Nslice2;
+  std::vector<double> Z1(Nslice1), Z2(Nslice2);
+  if ((e = sort_bunch_by_z(x1, Mp1, scratch, order, s)) == cudaSuccess &&
+      (e = sort_bunch_by_z(x2, Mp2, scratch, order, s)) == cudaSuccess &&
+      (e = slice_mean_z(x1, Nslice1, m1, dz, s)) == cudaSuccess &&
+      (e = slice_mean_z(x2, Nslice2, m2, dz + Nslice1, s)) == cudaSuccess &&
+      (e = cudaMemcpyAsync(Z1.data(), dz, sizeof(double) * Nslice1, cudaMemcpyDeviceToHost, s)) == cudaSuccess &&
+      (e = cudaMemcpyAsync(Z2.data(), dz + Nslice1, sizeof(double) * Nslice2, cudaMemcpyDeviceToHost, s)) ==
+          cudaSuccess &&
+      (e = cudaStreamSynchronize(s)) == cudaSuccess) {
+    // collision order, simtrack.cpp:23022-23042 (the same exchange sort)
+    const int np = Nslice1 * Nslice2;
+    std::vector<int> I1(np), I2(np);
+    std::vector<double> S(np), Z10(np);
+    for (int i = 0; i < Nslice1; i++)
+      for (int j = 0; j < Nslice2; j++) {
+        I1[i * Nslice2 + j] = i;
+        I2[i * Nslice2 + j] = j;
+        S[i * Nslice2 + j] = (Z1[i] - Z2[j]) / 2.;
+        Z10[i * Nslice2 + j] = -(Z1[i] + Z2[j]) / 2.;
+      }
+    for (int i = 0; i < np; i++)
+      for (int j = i + 1; j < np; j++)
+        if (Z10[j] < Z10[i]) {
+          std::swap(Z10[i], Z10[j]);
+          std::swap(S[i], S[j]);
+          std::swap(I1[i], I1[j]);
+          std::swap(I2[i], I2[j]);
+        }
+    const double rp = 1.53469826769e-18;  // BB4D, simtrack.cpp:6328
+    const double N2s = Np2 / Nslice2, N1s = Np1 / Nslice1;
+    const double c4_1 = 2 * N2s * rp / gamma1, c4_2 = 2 * N1s * rp / gamma2;
+    for (int i = 0; i < np && e == cudaSuccess; i++)
+      e = slice_pair_collision(x1 + 6 * (long)I1[i] * m1, m1, x2 + 6 * (long)I2[i] * m2, m2, S[i], c4_1, c4_2,
+                               bbscale1, bbscale2, num_sms, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  }
+  cudaFree(scratch);
+  return e;
 }
 
 }  // namespace stb
