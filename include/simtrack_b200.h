@@ -525,6 +525,18 @@ int stb_bb6d_soft_gaussian_host(double Np1, long Mp1, double *x1, double Np2, lo
                                 double gamma2, double bbscale1, double bbscale2, int nslice1, int nslice2,
                                 int device);
 
+/* The overload with slice boundaries, BeamBeam6D_SoftGaussian(..., Nslice1,
+ * Nslice2, zb1, zb2), simtrack.cpp:23134-23283 (simtrack.h:1409): slice s of
+ * a bunch holds its particles with zb[s+1] <= z < zb[s] (zb: nslice + 1
+ * decreasing host values); particles keep their places; each slice pair
+ * collides as the 4D soft-Gaussian form with N scaled by the slice's share
+ * of its bunch.  Defined (as in the reference) for Nslice1 == Nslice2 and
+ * slices of 2 .. 2*Mp/Nslice particles; otherwise STB_EINVAL and the bunches
+ * are unchanged.  Host AoS bunches, updated in place. */
+int stb_bb6d_soft_gaussian_zb_host(double Np1, long Mp1, double *x1, double Np2, long Mp2, double *x2,
+                                   double gamma1, double gamma2, double bbscale1, double bbscale2, int nslice1,
+                                   int nslice2, const double *zb1, const double *zb2, int device);
+
 /* Diagnostics: deviates k0 .. k0+n-1 of particle `id`'s quantum-excitation
  * stream under `seed` (see stb_set_radiation), evaluated on GPU `device` or
  * on the host (device < 0); out is host memory. */

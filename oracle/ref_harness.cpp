@@ -465,6 +465,13 @@ void ref_bb6d_soft_gaussian(double Np1, int Mp1, double *x1, double Np2, int Mp2
   BeamBeam6D_SoftGaussian(Np1, Mp1, x1, Np2, Mp2, x2, gamma1, gamma2, bbscale1, bbscale2, ns1, ns2);
 }
 
+// Its overload with slice boundaries zb1, zb2, called as is.
+void ref_bb6d_soft_gaussian_zb(double Np1, int Mp1, double *x1, double Np2, int Mp2, double *x2, double gamma1,
+                               double gamma2, double bbscale1, double bbscale2, int ns1, int ns2, double *zb1,
+                               double *zb2) {
+  BeamBeam6D_SoftGaussian(Np1, Mp1, x1, Np2, Mp2, x2, gamma1, gamma2, bbscale1, bbscale2, ns1, ns2, zb1, zb2);
+}
+
 // The reference's strong-strong soft-Gaussian collision, called as is.
 void ref_bb4d_soft_gaussian(double Np1, int n1, double *x1, double Np2, int n2, double *x2, double gamma1,
                             double gamma2, double bbscale1, double bbscale2) {

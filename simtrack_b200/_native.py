@@ -157,6 +157,9 @@ SIGNATURES = [
                                               c_double, c_double, c_double, c_int, c_int, c_int, c_void_p]),
     ("stb_bb6d_soft_gaussian_host", c_int, [c_double, c_long, POINTER(c_double), c_double, c_long, POINTER(c_double),
                                             c_double, c_double, c_double, c_double, c_int, c_int, c_int]),
+    ("stb_bb6d_soft_gaussian_zb_host", c_int, [c_double, c_long, POINTER(c_double), c_double, c_long,
+                                               POINTER(c_double), c_double, c_double, c_double, c_double, c_int, c_int,
+                                               POINTER(c_double), POINTER(c_double), c_int]),
     ("stb_rad_normals", c_int, [c_ulonglong, c_ulonglong, c_ulonglong, c_long, POINTER(c_double), c_int]),
     ("stb_philox4x32_10", c_int, [POINTER(ctypes.c_uint), POINTER(ctypes.c_uint), POINTER(ctypes.c_uint)]),
     ("stb_math_eval", c_int, [c_int, POINTER(c_double), POINTER(c_double), c_long, c_int]),

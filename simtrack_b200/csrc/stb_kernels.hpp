@@ -94,6 +94,11 @@ cudaError_t sort_bunch_by_z(double *x, long n, double *scratch, int32_t *order, 
 cudaError_t slice_mean_z(const double *x, int nslice, long m, double *z, cudaStream_t s);
 cudaError_t slice_pair_collision(double *x1, long m1, double *x2, long m2, double S, double c4_1, double c4_2,
                                  double bbscale1, double bbscale2, int num_sms, cudaStream_t s);
+// BeamBeam6D_SoftGaussian with slice boundaries zb1, zb2 (host arrays of
+// nslice + 1, decreasing), on device AoS bunches (synchronises `s`).
+cudaError_t soft_gaussian_6d_zb(double Np1, long Mp1, double *x1, double Np2, long Mp2, double *x2, double gamma1,
+                                double gamma2, double bbscale1, double bbscale2, int nslice, const double *zb1,
+                                const double *zb2, int num_sms, cudaStream_t s);
 // BeamBeam6D_SoftGaussian on device AoS bunches (synchronises `s`).
 cudaError_t soft_gaussian_6d(double Np1, long Mp1, double *x1, double Np2, long Mp2, double *x2, double gamma1,
                              double gamma2, double bbscale1, double bbscale2, int Nslice1, int Nslice2, int num_sms,

@@ -120,6 +120,38 @@ __global__ void slice_mean_z_kernel(const double *x, int nslice, long m, double 
   z[s] = t / (double)m;
 }
 
+// Members of each z slice [zb[s+1], zb[s]) in particle order (one thread per
+// slice, the reference's running sum of their z, 23172-23191): idx[s * cap
+// + r] for r < cap, count[s] (beyond cap only counted).
+__global__ void zb_slice_members_kernel(const double *x, long n, const double *zb, int nslice, long cap,
+                                        int32_t *idx, long *count, double *zsum) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nslice) return;
+  const double hi = zb[s], lo = zb[s + 1];
+  double t = 0;
+  long c = 0;
+  for (long j = 0; j < n; j++) {
+    const double z = x[6 * j + 4];
+    if (z < hi && z >= lo) {
+      t = t + z;
+      if (c < cap) idx[(long)s * cap + c] = (int32_t)j;
+      c++;
+    }
+  }
+  count[s] = c;
+  zsum[s] = t;
+}
+
+__global__ void gather_members_kernel(const double *x, const int32_t *idx, long m, double *xc) {
+  for (long r = (long)blockIdx.x * blockDim.x + threadIdx.x; r < m; r += (long)gridDim.x * blockDim.x)
+    for (int k = 0; k < 6; k++) xc[6 * r + k] = x[6 * (long)idx[r] + k];
+}
+
+__global__ void scatter_members_kernel(double *x, const int32_t *idx, long m, const double *xc) {
+  for (long r = (long)blockIdx.x * blockDim.x + threadIdx.x; r < m; r += (long)gridDim.x * blockDim.x)
+    for (int k = 0; k < 6; k++) x[6 * (long)idx[r] + k] = xc[6 * r + k];
+}
+
 // x += sign * px * S, y += sign * py * S over n particles (the drift to and
 // from the slices' collision point, 23059-23066, 23096-23103).
 __global__ void slice_drift_kernel(double *x, long n, double S, bool forward) {
@@ -240,6 +272,96 @@ cudaError_t soft_gaussian_6d(double Np1, long Mp1, double *x1, double Np2, long 
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   }
   cudaFree(scratch);
+  return e;
+}
+
+// BeamBeam6D_SoftGaussian with slice boundaries (simtrack.cpp:23134-23283):
+// slice s of a bunch holds its particles with zb[s+1] <= z < zb[s], in
+// place (no reordering); slice centroids from the running sums of z over
+// the members; the slice pairs in the same collision order as above; each
+// pair's members are gathered in particle order, drift, collide as the 4D
+// soft-Gaussian form with N scaled by the slice's share of the bunch
+// (Np Mp_coll / Mp), drift back and are scattered to their places.  The
+// reference copies each slice into a buffer of 2 Mp/Nslice particles and
+// initialises its per-slice counters for Nslice1 entries of both bunches, so
+// it is defined only for Nslice1 == Nslice2 and slices of at most that
+// size, and a slice of fewer than two particles has no rms size: all are
+// checked before any particle moves.  Returns cudaErrorInvalidValue when a
+// slice is too full or too thin.
+cudaError_t soft_gaussian_6d_zb(double Np1, long Mp1, double *x1, double Np2, long Mp2, double *x2, double gamma1,
+                                double gamma2, double bbscale1, double bbscale2, int nslice, const double *zb1,
+                                const double *zb2, int num_sms, cudaStream_t s) {
+  const long cap1 = 2 * Mp1 / nslice, cap2 = 2 * Mp2 / nslice;
+  const size_t nidx = (size_t)nslice * (size_t)(cap1 + cap2);
+  const size_t bytes = sizeof(double) * (6 * (size_t)(cap1 + cap2) + 2 * (size_t)(nslice + 1) + 2 * (size_t)nslice) +
+                       sizeof(long) * 2 * (size_t)nslice + sizeof(int32_t) * nidx;
+  unsigned char *buf = nullptr;
+  cudaError_t e = cudaMalloc(&buf, bytes);
+  if (e != cudaSuccess) return e;
+  double *xc1 = reinterpret_cast<double *>(buf), *xc2 = xc1 + 6 * cap1;
+  double *dzb1 = xc2 + 6 * cap2, *dzb2 = dzb1 + (nslice + 1);
+  double *zs = dzb2 + (nslice + 1);
+  long *cnt = reinterpret_cast<long *>(zs + 2 * nslice);
+  int32_t *idx1 = reinterpret_cast<int32_t *>(cnt + 2 * nslice), *idx2 = idx1 + (size_t)nslice * cap1;
+  std::vector<long> c(2 * nslice);
+  std::vector<double> z(2 * nslice);
+  if ((e = cudaMemcpyAsync(dzb1, zb1, sizeof(double) * (nslice + 1), cudaMemcpyHostToDevice, s)) == cudaSuccess &&
+      (e = cudaMemcpyAsync(dzb2, zb2, sizeof(double) * (nslice + 1), cudaMemcpyHostToDevice, s)) == cudaSuccess) {
+    zb_slice_members_kernel<<<(nslice + 63) / 64, 64, 0, s>>>(x1, Mp1, dzb1, nslice, cap1, idx1, cnt, zs);
+    zb_slice_members_kernel<<<(nslice + 63) / 64, 64, 0, s>>>(x2, Mp2, dzb2, nslice, cap2, idx2, cnt + nslice,
+                                                              zs + nslice);
+    if ((e = cudaGetLastError()) == cudaSuccess &&
+        (e = cudaMemcpyAsync(c.data(), cnt, sizeof(long) * 2 * nslice, cudaMemcpyDeviceToHost, s)) == cudaSuccess &&
+        (e = cudaMemcpyAsync(z.data(), zs, sizeof(double) * 2 * nslice, cudaMemcpyDeviceToHost, s)) ==
+            cudaSuccess &&
+        (e = cudaStreamSynchronize(s)) == cudaSuccess) {
+      for (int i = 0; i < nslice; i++)
+        if (c[i] > cap1 || c[nslice + i] > cap2 || c[i] < 2 || c[nslice + i] < 2) e = cudaErrorInvalidValue;
+    }
+  }
+  if (e == cudaSuccess) {
+    const int np = nslice * nslice;
+    std::vector<int> I1(np), I2(np);
+    std::vector<double> S(np), Z10(np), Z1(nslice), Z2(nslice);
+    for (int i = 0; i < nslice; i++) {
+      Z1[i] = z[i] / (double)(int)c[i];
+      Z2[i] = z[nslice + i] / (double)(int)c[nslice + i];
+    }
+    for (int i = 0; i < nslice; i++)
+      for (int j = 0; j < nslice; j++) {
+        I1[i * nslice + j] = i;
+        I2[i * nslice + j] = j;
+        S[i * nslice + j] = (Z1[i] - Z2[j]) / 2.;
+        Z10[i * nslice + j] = -(Z1[i] + Z2[j]) / 2.;
+      }
+    for (int i = 0; i < np; i++)
+      for (int j = i + 1; j < np; j++)
+        if (Z10[j] < Z10[i]) {
+          std::swap(Z10[i], Z10[j]);
+          std::swap(S[i], S[j]);
+          std::swap(I1[i], I1[j]);
+          std::swap(I2[i], I2[j]);
+        }
+    const double rp = 1.53469826769e-18;  // BB4D, simtrack.cpp:6328
+    const unsigned cap = (unsigned)num_sms * 8;
+    for (int i = 0; i < np && e == cudaSuccess; i++) {
+      const long m1 = c[I1[i]], m2 = c[nslice + I2[i]];
+      const int32_t *j1 = idx1 + (size_t)I1[i] * cap1, *j2 = idx2 + (size_t)I2[i] * cap2;
+      // BeamBeam4D_SoftGaussian(Np1*Mp1_coll/Mp1, ..., Np2*Mp2_coll/Mp2, ...), 23245
+      const double N1c = Np1 * (int)m1 / (int)Mp1, N2c = Np2 * (int)m2 / (int)Mp2;
+      const double c4_1 = 2 * N2c * rp / gamma1, c4_2 = 2 * N1c * rp / gamma2;
+      const unsigned g1 = (unsigned)((m1 + 255) / 256 < cap ? (m1 + 255) / 256 : cap);
+      const unsigned g2 = (unsigned)((m2 + 255) / 256 < cap ? (m2 + 255) / 256 : cap);
+      if (m1 > 0) gather_members_kernel<<<g1, 256, 0, s>>>(x1, j1, m1, xc1);
+      if (m2 > 0) gather_members_kernel<<<g2, 256, 0, s>>>(x2, j2, m2, xc2);
+      e = slice_pair_collision(xc1, m1, xc2, m2, S[i], c4_1, c4_2, bbscale1, bbscale2, num_sms, s);
+      if (m1 > 0) scatter_members_kernel<<<g1, 256, 0, s>>>(x1, j1, m1, xc1);
+      if (m2 > 0) scatter_members_kernel<<<g2, 256, 0, s>>>(x2, j2, m2, xc2);
+      if (e == cudaSuccess) e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  }
+  cudaFree(buf);
   return e;
 }
 

@@ -111,6 +111,9 @@ class RefOracle:
                                              c_double, c_double, c_double, c_double]
         L.ref_bb6d_soft_gaussian.argtypes = [c_double, c_int, POINTER(c_double), c_double, c_int, POINTER(c_double),
                                              c_double, c_double, c_double, c_double, c_int, c_int]
+        L.ref_bb6d_soft_gaussian_zb.argtypes = [c_double, c_int, POINTER(c_double), c_double, c_int,
+                                                POINTER(c_double), c_double, c_double, c_double, c_double, c_int,
+                                                c_int, POINTER(c_double), POINTER(c_double)]
         L.ref_set_radiation.argtypes = [c_int, ctypes.c_ulonglong]
         L.ref_rng_id_base.argtypes = [c_long]
         L.ref_rng_stream.argtypes = [ctypes.c_ulonglong] * 3

@@ -130,3 +130,36 @@ def test_sliced_collision_rejects_thin_slices(native_lib):
     from simtrack_b200 import _native
     assert native_lib.stb_bb6d_soft_gaussian_host(1e11, 6, P(b), 1e11, 6, P(b.copy()), GAMMA, GAMMA, 1.0, 1.0, 4, 2,
                                                   0) == _native.STB_EINVAL
+
+
+def test_slice_boundary_form_vs_reference(native_lib):
+    """The overload with slice boundaries (simtrack.cpp:23134-23283): slices
+    by z ranges, particles in place, N scaled by each slice's population;
+    against the reference's own function."""
+    if not oracle_bridge.ref_available(cr=True):
+        pytest.skip("compiled reference oracle (oracle/_ref) not built here")
+    Mp1, Mp2, ns = 4000, 4500, 5
+    b1 = _beam(Mp1, 1.2e-4, 1.0e-4, 2e-6, 0.0, 7)
+    b2 = _beam(Mp2, 1.1e-4, 1.2e-4, 0.0, -1e-6, 8)
+    zb1 = np.array([1.0, 0.1, 0.03, -0.03, -0.1, -1.0])
+    zb2 = np.array([1.0, 0.12, 0.02, -0.04, -0.11, -1.0])
+    g1, g2 = b1.copy(), b2.copy()
+    P = lambda a: a.ctypes.data_as(POINTER(c_double))
+    assert native_lib.stb_bb6d_soft_gaussian_zb_host(2e11, Mp1, P(g1), 1.8e11, Mp2, P(g2), GAMMA, GAMMA, 1.0, 1.0,
+                                                     ns, ns, P(zb1), P(zb2), 0) == 0
+    ref = oracle_bridge.RefOracle(cr=True)
+    r1, r2 = b1.copy(), b2.copy()
+    ref.L.ref_bb6d_soft_gaussian_zb(2e11, Mp1, P(r1), 1.8e11, Mp2, P(r2), GAMMA, GAMMA, 1.0, 1.0, ns, ns, P(zb1),
+                                    P(zb2))
+    assert np.array_equal(g1, r1) and np.array_equal(g2, r2)
+    assert np.array_equal(g1[:, 4], b1[:, 4])  # particles keep their places
+    assert not np.array_equal(g1[:, 1], b1[:, 1])
+    # undefined in the reference: unequal slice counts, an overfull slice
+    from simtrack_b200 import _native
+    assert native_lib.stb_bb6d_soft_gaussian_zb_host(2e11, Mp1, P(g1), 1.8e11, Mp2, P(g2), GAMMA, GAMMA, 1.0, 1.0,
+                                                     ns, ns - 1, P(zb1), P(zb2), 0) == _native.STB_EINVAL
+    wide = np.array([1.0, 0.9, 0.8, 0.7, -0.9, -1.0])
+    keep = g1.copy()
+    assert native_lib.stb_bb6d_soft_gaussian_zb_host(2e11, Mp1, P(g1), 1.8e11, Mp2, P(g2), GAMMA, GAMMA, 1.0, 1.0,
+                                                     ns, ns, P(wide), P(wide), 0) == _native.STB_EINVAL
+    assert np.array_equal(g1, keep)
