@@ -162,6 +162,7 @@ TrackArgs make_args(stb_table *t) {
   a.segs = t->d_segs;
   a.nseg = t->nseg;
   a.seg_bytes = t->seg_bytes;
+  a.radiate = (t->host.radiate && !t->host.spin) ? 1 : 0;
   return a;
 }
 
@@ -251,6 +252,7 @@ int autotune(stb_table *t, const double *const *in, int nc, long n, int nturn, d
           sa.t = a;
           sa.sx = buf + 6 * m; sa.sy = buf + 7 * m; sa.sz = buf + 8 * m;
           sa.dump = nullptr;
+          sa.radiate = t->host.radiate ? 1 : 0;
           le = launch_spin(sa, t->num_sms, v, 0);
         } else {
           le = (t->fast ? launch_track_fast : launch_track)(a, t->num_sms, v, 0);
@@ -470,6 +472,7 @@ int spin_device(stb_table *t, double *const xs[9], long n, int turn0, int nturn,
   a.t = make_args(t);
   a.t.x = xs[0]; a.t.px = xs[1]; a.t.y = xs[2]; a.t.py = xs[3]; a.t.z = xs[4]; a.t.pt = xs[5];
   a.sx = xs[6]; a.sy = xs[7]; a.sz = xs[8];
+  a.radiate = t->host.radiate ? 1 : 0;
   a.t.n = n;
   a.t.turn0 = turn0;
   a.t.nturn = nturn;

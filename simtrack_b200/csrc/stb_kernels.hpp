@@ -47,6 +47,9 @@ struct TrackArgs {
   const SegDesc *segs;
   int nseg;
   int seg_bytes;
+  // The table has radiating elements (GP.radiate): launched on the one
+  // kernel instantiation that carries the radiating maps.
+  int radiate;
 };
 
 // Spin tracking (stb_spin.cu): the orbit arguments plus the spin unit vector
@@ -54,6 +57,7 @@ struct TrackArgs {
 struct SpinArgs {
   TrackArgs t;  // t.dump is unused
   double *sx, *sy, *sz;
+  int radiate;  // the table was flattened with GP.radiate
   // Optional per-element probe: dump[((i * nturn + t) * nelem + e) * 9 + k].
   double *dump;
 };

@@ -162,6 +162,9 @@ __device__ __forceinline__ void mpole_field(int order, bool thick, double x1, do
 }
 
 // One spin-opcode element (after the misalignment entrance transform).
+// kRad: compile radiate() after the slice rotations of the bends (tables
+// flattened with GP.radiate run the one kernel instantiation that has it).
+template <bool kRad>
 __device__ __forceinline__ void spin_element(const ElemHeader &h, const double *P, Particle &p, Spin &s, PtCache &c,
                                              const RefConsts &R) {
   switch (h.op) {
@@ -174,7 +177,7 @@ __device__ __forceinline__ void spin_element(const ElemHeader &h, const double *
         const Particle x0 = p;
         bend_exact(p, c, P + 2);
         spin_rotate(x0, c, R, an, href, 0., an, 0., s);
-        if (h.flags & EF_RADIATE) radiate_step(p, c, R, P[2], href, 0., an, 0., P[10], false, 0., 0.);
+        if (kRad && (h.flags & EF_RADIATE)) radiate_step(p, c, R, P[2], href, 0., an, 0., P[10], false, 0., 0.);
       }
       p.px = p.px + P[1] * p.x;
       p.py = p.py - P[1] * p.y;
@@ -183,20 +186,16 @@ __device__ __forceinline__ void spin_element(const ElemHeader &h, const double *
     case OP_S_MPOLE_THICK: {
       const int order = h.aux;
       const double kl = P[8], ksl = P[9], nd = P[10];
-      DriftStep last{};
 #pragma unroll 1
       for (int i = 0; i < h.nint; i++) {
         const Particle x0 = p;
-        // the rotation changes no orbit coordinate: this drift repeats the
-        // previous slice's closing one, so its increments are added again
-        if (i > 0) drift_again(p, last);
-        else drift(p, c, P[0], P[1]);
+        drift(p, c, P[0], P[1]);
         mpole_kick(p, order, P[4], P[5]);
         drift(p, c, P[2], P[3]);
         mpole_kick(p, order, P[6], P[7]);
         drift(p, c, P[2], P[3]);
         mpole_kick(p, order, P[4], P[5]);
-        last = drift(p, c, P[0], P[1]);
+        drift(p, c, P[0], P[1]);
         const double x1 = (p.x + x0.x) / 2., y1 = (p.y + x0.y) / 2.;
         double B0, B1;
         mpole_field(order, true, x1, y1, kl, ksl, nd, B0, B1);
@@ -224,18 +223,16 @@ __device__ __forceinline__ void spin_element(const ElemHeader &h, const double *
       const int no = h.aux, bs = 2 + 3 * no;
       const double *K1 = P + 4, *K2 = K1 + bs, *KR = K2 + bs;
       const double nd = KR[bs];
-      DriftStep last{};
 #pragma unroll 1
       for (int i = 0; i < h.nint; i++) {
         const Particle x0 = p;
-        if (i > 0) drift_again(p, last);  // repeats the previous slice's closing drift
-        else drift(p, c, P[0], P[1]);
+        drift(p, c, P[0], P[1]);
         mult_kick(p, no, K1);
         drift(p, c, P[2], P[3]);
         mult_kick(p, no, K2);
         drift(p, c, P[2], P[3]);
         mult_kick(p, no, K1);
-        last = drift(p, c, P[0], P[1]);
+        drift(p, c, P[0], P[1]);
         const double x1 = (p.x + x0.x) / 2., y1 = (p.y + x0.y) / 2.;
         double By, Bx;
         mult_field(x1, y1, no, KR, By, Bx);
@@ -265,7 +262,8 @@ __device__ __forceinline__ void spin_element(const ElemHeader &h, const double *
         mult_field(x1, y1, no, KR, By, Bx);
         const double B0 = Bx / nd, B1 = (Angle + By) / nd;
         spin_rotate(x0, c, R, an, href, B0, B1, 0., s);
-        if (h.flags & EF_RADIATE) radiate_step(p, c, R, KR[bs + 4], href, B0, B1, 0., KR[bs + 5], false, 0., 0.);
+        if (kRad && (h.flags & EF_RADIATE))
+          radiate_step(p, c, R, KR[bs + 4], href, B0, B1, 0., KR[bs + 5], false, 0., 0.);
       }
       p.px = p.px + P[1] * p.x;
       p.py = p.py - P[1] * p.y;
@@ -307,7 +305,7 @@ __device__ __forceinline__ void spin_element(const ElemHeader &h, const double *
   }
 }
 
-template <bool kSmem, int kBlock, int kMinBlocks, bool kDump>
+template <bool kSmem, int kBlock, int kMinBlocks, bool kDump, bool kRad = false>
 __global__ void __launch_bounds__(kBlock, kMinBlocks) spin_track_kernel(const __grid_constant__ SpinArgs sa) {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ __align__(8) uint64_t bar;
@@ -348,7 +346,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) spin_track_kernel(const __
             gtol1(p[0], M, h.flags);
             P += kMisalignParams;
           }
-          spin_element(h, P, p[0], s, c[0], R);
+          spin_element<kRad>(h, P, p[0], s, c[0], R);
           if (mis) ltog1(p[0], M, h.flags);
         } else {
           apply_element<1>(h, P, p, c, R);
@@ -381,9 +379,9 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) spin_track_kernel(const __
   }
 }
 
-template <bool kSmem, int kBlock, int kMinBlocks, bool kDump>
+template <bool kSmem, int kBlock, int kMinBlocks, bool kDump, bool kRad = false>
 cudaError_t launch_spin_variant(const SpinArgs &a, int num_sms, size_t smem, cudaStream_t stream) {
-  auto kern = spin_track_kernel<kSmem, kBlock, kMinBlocks, kDump>;
+  auto kern = spin_track_kernel<kSmem, kBlock, kMinBlocks, kDump, kRad>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   int per_sm = 0;
@@ -414,7 +412,10 @@ const SpinVariant kSpinVariants[kNumSpinVariants] = {
 
 cudaError_t launch_spin(const SpinArgs &a, int num_sms, int variant, cudaStream_t stream) {
   if (a.t.n <= 0 || a.t.nturn <= 0) return cudaSuccess;
-  if (a.dump) return launch_spin_variant<false, 128, 1, true>(a, num_sms, 0, stream);
+  if (a.dump) return launch_spin_variant<false, 128, 1, true, true>(a, num_sms, 0, stream);
+  // tables flattened with GP.radiate: the instantiation with radiate() (the
+  // shape of l1_b128_r255), whatever the variant
+  if (a.radiate) return launch_spin_variant<false, 128, 2, false, true>(a, num_sms, 0, stream);
   const size_t sm = track_smem_bytes(a.t.nelem, a.t.npool_padded);
   switch (variant) {
     case 0: return launch_spin_variant<true, 512, 1, false>(a, num_sms, sm, stream);

@@ -366,7 +366,10 @@ __device__ __forceinline__ void op_misc(const ElemHeader &h, const double *P, Pa
 // loss.  For the hot element types the per-particle maps are issued back to
 // back, so their independent FP64 dependency chains interleave in the
 // instruction stream (latency hiding without more resident warps).
-template <int kPPT, bool kLoopSlices = false>
+// kRad: compile the radiating maps (GP.radiate tables); only the tracking
+// kernel instantiation that such tables launch carries them, so the code of
+// every other kernel stays as small as without radiation.
+template <int kPPT, bool kLoopSlices = false, bool kRad = false>
 __device__ __forceinline__ void apply_element(const ElemHeader &h, const double *P, Particle (&p)[kPPT],
                                               PtCache (&c)[kPPT], const RefConsts &R, const RadKey &rk = RadKey{}) {
   const double *M = P;
@@ -480,13 +483,16 @@ __device__ __forceinline__ void apply_element(const ElemHeader &h, const double 
       for (int k = 0; k < kPPT; k++) op_bendmult(h, P, p[k], c[k]);
       break;
     case OP_SBEND_RAD:
-      for (int k = 0; k < kPPT; k++) op_sbend_rad(h, P, p[k], c[k], R, rk.id0 + (long)k * rk.id_stride, rk.turn);
+      if (kRad)
+        for (int k = 0; k < kPPT; k++) op_sbend_rad(h, P, p[k], c[k], R, rk.id0 + (long)k * rk.id_stride, rk.turn);
       break;
     case OP_BENDMULT_RAD:
-      for (int k = 0; k < kPPT; k++) op_bendmult_rad(h, P, p[k], c[k], R);
+      if (kRad)
+        for (int k = 0; k < kPPT; k++) op_bendmult_rad(h, P, p[k], c[k], R);
       break;
     case OP_GSBEND_RAD:
-      for (int k = 0; k < kPPT; k++) op_gsbend_rad(h, P, p[k], c[k], R, rk.id0 + (long)k * rk.id_stride, rk.turn);
+      if (kRad)
+        for (int k = 0; k < kPPT; k++) op_gsbend_rad(h, P, p[k], c[k], R, rk.id0 + (long)k * rk.id_stride, rk.turn);
       break;
     default:
       for (int k = 0; k < kPPT; k++) op_misc(h, P, p[k], c[k], R);
@@ -562,7 +568,7 @@ __device__ __forceinline__ void after_element(const TrackArgs &a, const ElemHead
 // The segmented form of track_kernel (kSeg).  Step s of this CTA's sequence
 // tracks segment s % nseg from buffer s & 1; buffer b's mbarrier completes
 // once per staging, so its parity alternates with every use.
-template <int kBlock, int kPPT, bool kDump>
+template <int kBlock, int kPPT, bool kDump, bool kRad>
 __device__ void track_segmented(const TrackArgs &a, unsigned char *smem, uint64_t *sbar) {
   const long chunk = (long)kBlock * kPPT;
   const long stride = (long)gridDim.x * chunk;
@@ -612,7 +618,7 @@ __device__ void track_segmented(const TrackArgs &a, unsigned char *smem, uint64_
         if (nalive > 0) {
           for (int j = 0; j < sg.ne; j++) {
             const ElemHeader h = hs[j];
-            apply_element<kPPT, (kBlock >= 512)>(h, ps + (h.poff - sg.pool_lo), p, c, R,
+            apply_element<kPPT, (kBlock >= 512), kRad>(h, ps + (h.poff - sg.pool_lo), p, c, R,
                                                  RadKey{base, kBlock, (long)a.turn0 + t});
             after_element<kBlock, kPPT, kDump>(a, h, base, t, sg.e0 + j, p, c, alive, nalive);
             if (nalive == 0) break;
@@ -640,7 +646,8 @@ __device__ void track_segmented(const TrackArgs &a, unsigned char *smem, uint64_
 // (particle chunk, turn, segment) steps in lockstep: a barrier after every
 // segment frees its buffer for the copy two steps ahead.  Threads whose
 // particles are lost (or that have none) keep taking part in the barriers.
-template <bool kSmem, int kBlock, int kMinBlocks, int kPPT, bool kDump, bool kPF = false, bool kSeg = false>
+template <bool kSmem, int kBlock, int kMinBlocks, int kPPT, bool kDump, bool kPF = false, bool kSeg = false,
+          bool kRad = false>
 __global__ void __launch_bounds__(kBlock, kMinBlocks) track_kernel(const __grid_constant__ TrackArgs a) {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ __align__(8) uint64_t bar;
@@ -648,7 +655,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) track_kernel(const __grid_
   const ElemHeader *hdr = a.hdr;
   const double *pool = a.pool;
   if (kSeg) {
-    track_segmented<kBlock, kPPT, kDump>(a, smem, sbar);
+    track_segmented<kBlock, kPPT, kDump, kRad>(a, smem, sbar);
     return;
   }
   if (kSmem) {
@@ -702,7 +709,8 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) track_kernel(const __grid_
         } else {
           h = hdr[e];
         }
-        apply_element<kPPT, (kBlock >= 512)>(h, pool + h.poff, p, c, R, RadKey{base, kBlock, (long)a.turn0 + t});
+        apply_element<kPPT, (kBlock >= 512), kRad>(h, pool + h.poff, p, c, R,
+                                                   RadKey{base, kBlock, (long)a.turn0 + t});
 #pragma unroll
         for (int k = 0; k < kPPT; k++) {
           if (!alive[k]) continue;

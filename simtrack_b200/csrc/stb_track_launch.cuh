@@ -14,9 +14,10 @@ namespace {
 
 // Persistent grid: as many CTAs as fit on the device at once (never more
 // than the particles need); each CTA strides over the particle range.
-template <bool kSmem, int kBlock, int kMinBlocks, int kPPT, bool kDump, bool kPF = false, bool kSeg = false>
+template <bool kSmem, int kBlock, int kMinBlocks, int kPPT, bool kDump, bool kPF = false, bool kSeg = false,
+          bool kRad = false>
 cudaError_t launch_variant(const TrackArgs &a, int num_sms, size_t smem, cudaStream_t stream) {
-  auto kern = track_kernel<kSmem, kBlock, kMinBlocks, kPPT, kDump, kPF, kSeg>;
+  auto kern = track_kernel<kSmem, kBlock, kMinBlocks, kPPT, kDump, kPF, kSeg, kRad>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   int per_sm = 0;
@@ -40,9 +41,13 @@ cudaError_t launch_track_variants(const TrackArgs &a, int num_sms, int variant, 
   if (a.dump) {
     // Per-element probe (diagnostics and parity tests): small particle counts
     // only; through the segment buffers when the table is tracked that way.
-    if (seg_ok && kVariants[variant].seg) return launch_variant<true, 256, 1, 1, true, false, true>(a, num_sms, sg, stream);
-    return launch_variant<false, 256, 1, 1, true>(a, num_sms, 0, stream);
+    if (seg_ok && kVariants[variant].seg)
+      return launch_variant<true, 256, 1, 1, true, false, true, true>(a, num_sms, sg, stream);
+    return launch_variant<false, 256, 1, 1, true, false, false, true>(a, num_sms, 0, stream);
   }
+  // Tables with radiating elements run the one instantiation that carries the
+  // radiating maps (the shape of l1_b256_r128), whatever the variant.
+  if (a.radiate) return launch_variant<false, 256, 2, 1, false, false, false, true>(a, num_sms, 0, stream);
   switch (variant) {
     case 0: return launch_variant<true, 512, 1, 1, false>(a, num_sms, sm, stream);
     case 1: return launch_variant<true, 1024, 1, 1, false>(a, num_sms, sm, stream);
