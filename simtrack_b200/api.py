@@ -21,6 +21,7 @@ __all__ = [
     "Set_RefPartEnergy", "Set_Spin_G", "Set_Flags", "GP", "Element", "Line", "Table", "Track", "Track_Batch",
     "DRIFT", "MARKER", "SBEND", "GSBEND", "QUAD", "SKEWQ", "SEXT", "OCT", "MULT", "GMULT", "SBENDMULT",
     "KICKER", "HKICKER", "VKICKER", "RFCAV", "CRABRF", "CCMULT", "LBT", "ILBT", "BEAMBEAM",
+    "Set_Radiation", "BeamBeam4D_SoftGaussian", "BeamBeam6D_SoftGaussian",
 ]
 
 
@@ -45,6 +46,45 @@ def Set_Radiation(radiate: bool = False, seed: int = 1324) -> None:
     (radiate).  `seed` keys the quantum-excitation deviates (the reference
     seeds its GSL stream with 1324, simtrack.cpp:328)."""
     check(lib().stb_set_radiation(int(radiate), int(seed)))
+
+
+def _bunch(x) -> np.ndarray:
+    b = np.asarray(x)
+    if b.dtype != np.float64 or not b.flags.c_contiguous or b.ndim != 2 or b.shape[1] != 6:
+        raise ValueError("a bunch is a C-contiguous float64 array of shape (n, 6), updated in place")
+    return b
+
+
+def BeamBeam4D_SoftGaussian(Np1: float, x1: np.ndarray, Np2: float, x2: np.ndarray, gamma1: float, gamma2: float,
+                            bbscale1: float, bbscale2: float, device: int = 0) -> None:
+    """BeamBeam4D_SoftGaussian (simtrack.cpp:22846-22872) on the GPU: the two
+    macro-particle bunches (numpy (n, 6) float64, updated in place) kick each
+    other as soft Gaussians."""
+    b1, b2 = _bunch(x1), _bunch(x2)
+    P = lambda a: a.ctypes.data_as(POINTER(c_double))
+    check(lib().stb_bb4d_soft_gaussian_host(Np1, len(b1), P(b1), Np2, len(b2), P(b2), gamma1, gamma2, bbscale1,
+                                            bbscale2, device))
+
+
+def BeamBeam6D_SoftGaussian(Np1: float, x1: np.ndarray, Np2: float, x2: np.ndarray, gamma1: float, gamma2: float,
+                            bbscale1: float, bbscale2: float, Nslice1: int, Nslice2: int, zb1=None, zb2=None,
+                            device: int = 0) -> None:
+    """BeamBeam6D_SoftGaussian on the GPU: without zb1/zb2 the sorted-slice
+    form (simtrack.cpp:22874-23132; both bunches come back ordered by z,
+    largest first), with them the slice-boundary form (23134-23283, zb of
+    Nslice + 1 decreasing values).  Bunches: numpy (n, 6) float64, in place."""
+    b1, b2 = _bunch(x1), _bunch(x2)
+    P = lambda a: a.ctypes.data_as(POINTER(c_double))
+    if zb1 is None and zb2 is None:
+        check(lib().stb_bb6d_soft_gaussian_host(Np1, len(b1), P(b1), Np2, len(b2), P(b2), gamma1, gamma2, bbscale1,
+                                                bbscale2, Nslice1, Nslice2, device))
+        return
+    z1 = np.ascontiguousarray(zb1, dtype=np.float64)
+    z2 = np.ascontiguousarray(zb2, dtype=np.float64)
+    if z1.shape != (Nslice1 + 1,) or z2.shape != (Nslice2 + 1,):
+        raise ValueError("zb1 and zb2 need Nslice + 1 boundaries each")
+    check(lib().stb_bb6d_soft_gaussian_zb_host(Np1, len(b1), P(b1), Np2, len(b2), P(b2), gamma1, gamma2, bbscale1,
+                                               bbscale2, Nslice1, Nslice2, P(z1), P(z2), device))
 
 
 def GP() -> dict:

@@ -163,3 +163,29 @@ def test_slice_boundary_form_vs_reference(native_lib):
     assert native_lib.stb_bb6d_soft_gaussian_zb_host(2e11, Mp1, P(g1), 1.8e11, Mp2, P(g2), GAMMA, GAMMA, 1.0, 1.0,
                                                      ns, ns, P(wide), P(wide), 0) == _native.STB_EINVAL
     assert np.array_equal(g1, keep)
+
+
+def test_python_wrappers_vs_reference(tmp_path, monkeypatch):
+    """simtrack_b200.api's BeamBeam4D_SoftGaussian / BeamBeam6D_SoftGaussian
+    (both forms) against the reference's functions."""
+    from simtrack_b200 import api
+    if not oracle_bridge.ref_available(cr=True):
+        pytest.skip("compiled reference oracle (oracle/_ref) not built here")
+    monkeypatch.chdir(tmp_path)
+    ref = oracle_bridge.RefOracle(cr=True)
+    P = lambda a: a.ctypes.data_as(POINTER(c_double))
+    b1, b2 = _beam(2000, 1.2e-4, 1.1e-4, 0.0, 0.0, 9), _beam(2400, 1.1e-4, 1.2e-4, 0.0, 0.0, 10)
+    g1, g2, r1, r2 = b1.copy(), b2.copy(), b1.copy(), b2.copy()
+    api.BeamBeam4D_SoftGaussian(2e11, g1, 2e11, g2, GAMMA, GAMMA, 1.0, 1.0)
+    ref.L.ref_bb4d_soft_gaussian(2e11, 2000, P(r1), 2e11, 2400, P(r2), GAMMA, GAMMA, 1.0, 1.0)
+    assert np.array_equal(g1, r1) and np.array_equal(g2, r2)
+    g1, g2, r1, r2 = b1.copy(), b2.copy(), b1.copy(), b2.copy()
+    api.BeamBeam6D_SoftGaussian(2e11, g1, 2e11, g2, GAMMA, GAMMA, 1.0, 1.0, 4, 4)
+    ref.L.ref_bb6d_soft_gaussian(2e11, 2000, P(r1), 2e11, 2400, P(r2), GAMMA, GAMMA, 1.0, 1.0, 4, 4)
+    assert np.array_equal(g1, r1) and np.array_equal(g2, r2)
+    zb = np.array([1.0, 0.08, 0.0, -0.08, -1.0])
+    g1, g2, r1, r2 = b1.copy(), b2.copy(), b1.copy(), b2.copy()
+    api.BeamBeam6D_SoftGaussian(2e11, g1, 2e11, g2, GAMMA, GAMMA, 1.0, 1.0, 4, 4, zb, zb)
+    ref.L.ref_bb6d_soft_gaussian_zb(2e11, 2000, P(r1), 2e11, 2400, P(r2), GAMMA, GAMMA, 1.0, 1.0, 4, 4, P(zb.copy()),
+                                    P(zb.copy()))
+    assert np.array_equal(g1, r1) and np.array_equal(g2, r2)
