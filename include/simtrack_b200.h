@@ -64,6 +64,15 @@ int stb_set_flags(int h_expand, int quad_fringe);
  * (radiate2, 4290-4372), its Poisson photon count and photon uniforms drawn
  * from the same per-particle generator. */
 int stb_set_radiation(int radiate, unsigned long long seed);
+
+/* Cal_SRLoss_U0rad (track_form 0) / Cal_SRLoss_U0rad_Track (track_form 1),
+ * simtrack.cpp:20691-20766: the reference particle's synchrotron-radiation
+ * loss per turn in MeV (also kept as GP.U0rad), 0 unless GP.radiate.  GSBENDs
+ * (and, in the track form, every sector bend) take their path on the orbit
+ * stored in the element before them (stb_cal_orbit fills it; zero before);
+ * a bend as the line's first element is rejected (the reference would read
+ * before the line).  Host computation, no GPU. */
+int stb_cal_srloss_u0rad(stb_line *line, int track_form, double *u0rad_mev);
 /* out[0..7] = GP.gamma, GP.beta, GP.energy, GP.brho, GP.Q, GP.energy0, GP.G, GP.p */
 int stb_get_ref(double *out8);
 

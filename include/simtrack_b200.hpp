@@ -36,8 +36,18 @@ struct GlobalVariables {
   double gamma = 106., beta = 0.999955, brho = 331.738;
   double G = 1.7928474, Gr = 191.079706193;
   bool H_expand = false, radiate = false, quad_fringe = false;
+  double U0rad = 0.;  // reference particle's radiation loss per turn, MeV (Cal_SRLoss_U0rad)
 };
 extern GlobalVariables GP;
+
+// Cal_SRLoss_U0rad / Cal_SRLoss_U0rad_Track (simtrack.cpp:20691-20766): the
+// reference particle's synchrotron-radiation loss per turn in MeV, into
+// GP.U0rad (0 unless GP.radiate); the track form takes every bend's path on
+// the orbit stored in the element before it (Cal_Orbit_Num fills X).
+class Line;
+double Cal_SRLoss_U0rad(Line &line, bool track_form = false);
+// Cal_gsbend_l_angle (simtrack.cpp:4006-4044).
+void Cal_gsbend_l_angle(double x[6], double L, double Angle, double K0L, double &actual_l, double &actual_angle);
 
 // Set_RefPartEnergy (simtrack.cpp:87-108) and Set_Spin_G (simtrack.cpp:110-115).
 void Set_RefPartEnergy(double gamma, double E0, double Q, double A);

@@ -204,6 +204,13 @@ void ref_set_radiation(int radiate, unsigned long long seed) {
   g_rng_seed = seed;
 }
 void ref_rng_id_base(long base) { g_rng_base = base; }
+
+// Cal_SRLoss_U0rad / Cal_SRLoss_U0rad_Track, called as is; returns GP.U0rad.
+double ref_cal_srloss(void *line, int track_form) {
+  if (track_form) Cal_SRLoss_U0rad_Track(*static_cast<Line *>(line));
+  else Cal_SRLoss_U0rad(*static_cast<Line *>(line));
+  return GP.U0rad;
+}
 // Deviate k of stream `id` under `seed` (the stream's own check).
 double ref_rng_stream(unsigned long long seed, unsigned long long id, unsigned long long k) {
   return stream_gaussian(seed, id, k);

@@ -736,6 +736,14 @@ int stb_element_geometry(const stb_element *e, double *out10) {
     return STB_OK;
   });
 }
+int stb_cal_srloss_u0rad(stb_line *l, int track_form, double *u0rad_mev) {
+  return guarded([&] {
+    if (!l || !u0rad_mev) throw Error(STB_EINVAL, "NULL argument");
+    *u0rad_mev = Cal_SRLoss_U0rad(*Lp(l), track_form != 0);
+    return STB_OK;
+  });
+}
+
 int stb_cal_orbit(stb_line *l, double deltap, double *orbit6, int device) {
   return guarded([&] {
     if (!l) throw Error(STB_EINVAL, "NULL line");

@@ -64,3 +64,30 @@ def test_stream_moments(native_lib):
     a, b = normals(native_lib, 1324, 5, 0, 100000), normals(native_lib, 1324, 6, 0, 100000)
     assert abs(np.corrcoef(a, b)[0, 1]) < 0.02
     assert abs(np.corrcoef(a[:-1], a[1:])[0, 1]) < 0.02
+
+
+@pytest.mark.parametrize("gsbend", [False, True])
+@pytest.mark.parametrize("track_form", [0, 1])
+def test_srloss_u0rad_vs_reference(native_lib, gsbend, track_form):
+    """Cal_SRLoss_U0rad / Cal_SRLoss_U0rad_Track (simtrack.cpp:20691-20766):
+    the reference particle's radiation loss per turn, host computation,
+    against the reference's own functions on the electron ring (sector
+    dipoles or GSBENDs; the bends' paths on the stored orbit, zero here)."""
+    from ctypes import byref, c_double
+    from simtrack_b200 import api
+    from simtrack_b200 import lattices as lt
+    if not oracle_bridge.ref_available():
+        pytest.skip("compiled reference oracle (oracle/_ref) not built here")
+    lat = lt.electron_ring(gsbend=gsbend)
+    try:
+        line = lt.build_line(lat)
+        u = c_double()
+        assert native_lib.stb_cal_srloss_u0rad(line._h, track_form, byref(u)) == 0
+        ref = oracle_bridge.RefOracle()
+        ref.build(lat)
+        assert u.value == ref.L.ref_cal_srloss(ref.line, track_form)
+        assert u.value > 0.1  # MeV per turn for 3 GeV electrons in a 276 m ring
+        api.Set_Radiation(False)
+        assert native_lib.stb_cal_srloss_u0rad(line._h, track_form, byref(u)) == 0 and u.value == 0.0
+    finally:
+        api.Set_Radiation(False)
