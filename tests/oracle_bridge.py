@@ -45,6 +45,17 @@ def ref_available(cr: bool = False) -> bool:
     return (REF_CR_SO if cr else REF_SO).exists()
 
 
+def reference_radiation_off() -> None:
+    """Turn GP.radiate off in both compiled references loaded in this process
+    (their globals outlive one test; a reference line built afterwards
+    without RefOracle.build would otherwise track with radiation)."""
+    for cr in (False, True):
+        if ref_available(cr=cr):
+            L = ctypes.CDLL(str(REF_CR_SO if cr else REF_SO))
+            L.ref_set_radiation.argtypes = [c_int, ctypes.c_ulonglong]
+            L.ref_set_radiation(0, 1324)
+
+
 def port_available() -> bool:
     return PORT_SO.exists()
 

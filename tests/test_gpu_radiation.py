@@ -31,6 +31,7 @@ pytestmark = pytest.mark.gpu
 def radiation_off_afterwards():
     yield
     api.Set_Radiation(False)
+    oracle_bridge.reference_radiation_off()
 
 
 @pytest.fixture(scope="module")

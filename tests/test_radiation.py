@@ -91,3 +91,4 @@ def test_srloss_u0rad_vs_reference(native_lib, gsbend, track_form):
         assert native_lib.stb_cal_srloss_u0rad(line._h, track_form, byref(u)) == 0 and u.value == 0.0
     finally:
         api.Set_Radiation(False)
+        oracle_bridge.reference_radiation_off()
