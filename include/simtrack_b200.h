@@ -73,6 +73,14 @@ int stb_set_radiation(int radiate, unsigned long long seed);
  * a bend as the line's first element is rejected (the reference would read
  * before the line).  Host computation, no GPU. */
 int stb_cal_srloss_u0rad(stb_line *line, int track_form, double *u0rad_mev);
+/* Cal_SRLoss_Particle, simtrack.cpp:20768-20781: x6 passed once through
+ * every element of the line but the RF cavities, on `device`, and updated in
+ * place; *loss_mev = (pt - pt0) * GP.beta * GP.energy.  Radiating bends draw
+ * from particle 0's deviate stream at turn 0.  The reference passes without
+ * loss tests; a particle that Track()'s tests would stop (|x| or |y| > 0.1 at
+ * entry, outside an element's aperture, NaN) is rejected with STB_EINVAL and
+ * x6 unchanged. */
+int stb_cal_srloss_particle(stb_line *line, double *x6, double *loss_mev, int device);
 /* out[0..7] = GP.gamma, GP.beta, GP.energy, GP.brho, GP.Q, GP.energy0, GP.G, GP.p */
 int stb_get_ref(double *out8);
 

@@ -46,6 +46,12 @@ extern GlobalVariables GP;
 // the orbit stored in the element before it (Cal_Orbit_Num fills X).
 class Line;
 double Cal_SRLoss_U0rad(Line &line, bool track_form = false);
+// Cal_SRLoss_Particle (simtrack.cpp:20768-20781): x[6] passed once through
+// every element but the RF cavities on the GPU (radiating bends radiate, with
+// the particle-0 deviate stream), loss = (pt - pt0) GP.beta GP.energy (MeV,
+// negative for a loss).  A particle that Track()'s loss tests would stop is
+// rejected (stb::Error, STB_EINVAL) with x unchanged.
+void Cal_SRLoss_Particle(Line &line, double x[], double &loss, int device = 0);
 // Cal_gsbend_l_angle (simtrack.cpp:4006-4044).
 void Cal_gsbend_l_angle(double x[6], double L, double Angle, double K0L, double &actual_l, double &actual_angle);
 

@@ -211,6 +211,14 @@ double ref_cal_srloss(void *line, int track_form) {
   else Cal_SRLoss_U0rad(*static_cast<Line *>(line));
   return GP.U0rad;
 }
+// The reference's Cal_SRLoss_Particle (simtrack.cpp:20768), the pass drawing
+// from particle g_rng_base's stream; x6 updated in place.
+double ref_cal_srloss_particle(void *line, double *x6) {
+  double loss = 0;
+  rng_particle(g_rng_base);
+  Cal_SRLoss_Particle(*static_cast<Line *>(line), x6, loss);
+  return loss;
+}
 // Deviate k of stream `id` under `seed` (the stream's own check).
 double ref_rng_stream(unsigned long long seed, unsigned long long id, unsigned long long k) {
   return stream_gaussian(seed, id, k);

@@ -39,6 +39,7 @@ SIGNATURES = [
     ("stb_set_flags", c_int, [c_int, c_int]),
     ("stb_set_radiation", c_int, [c_int, c_ulonglong]),
     ("stb_cal_srloss_u0rad", c_int, [c_void_p, c_int, POINTER(c_double)]),
+    ("stb_cal_srloss_particle", c_int, [c_void_p, POINTER(c_double), POINTER(c_double), c_int]),
     ("stb_get_ref", c_int, [POINTER(c_double)]),
     ("stb_element_new", c_int, [c_char_p, c_char_p, POINTER(c_double), c_int, POINTER(c_void_p)]),
     ("stb_element_free", c_int, [c_void_p]),

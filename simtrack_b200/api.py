@@ -513,6 +513,27 @@ def Cal_Orbit_Num(line: Line, deltap: float = 0.0, device: int = 0) -> np.ndarra
     return out
 
 
+def Cal_SRLoss_U0rad(line: Line, track_form: bool = False) -> float:
+    """Cal_SRLoss_U0rad / Cal_SRLoss_U0rad_Track (simtrack.cpp:20691-20766):
+    the reference particle's synchrotron-radiation loss per turn, MeV (0
+    unless radiation is on; host computation)."""
+    u = c_double()
+    check(lib().stb_cal_srloss_u0rad(line._h, int(track_form), byref(u)))
+    return u.value
+
+
+def Cal_SRLoss_Particle(line: Line, x, device: int = 0) -> float:
+    """Cal_SRLoss_Particle (simtrack.cpp:20768-20781): x (6 float64, updated
+    in place) passed once through every element but the RF cavities on the
+    GPU; returns (pt - pt0) * beta * energy in MeV (negative for a loss)."""
+    v = np.asarray(x)
+    if v.dtype != np.float64 or v.shape != (6,) or not v.flags.c_contiguous:
+        raise ValueError("x is a C-contiguous float64 array of 6 coordinates, updated in place")
+    loss = c_double()
+    check(lib().stb_cal_srloss_particle(line._h, v.ctypes.data_as(POINTER(c_double)), byref(loss), device))
+    return loss.value
+
+
 DA_DRIVERS = {"Track_DA1": 1, "Track_DA2": 2, "Track_DA3": 3, "Track_DA_Radial": 4, "Track_DA_Uniform": 5,
               "Track_DA_Radial_Uniform": 6}
 

@@ -119,10 +119,10 @@ bool variant_allowed(const stb_table *t, int v) {
   return !kVariants[v].smem || t->use_smem;
 }
 
-stb_table *table_build(const Line &line, int device, bool spin = false) {
+stb_table *table_build_from(HostTable host, int device, bool spin) {
   std::unique_ptr<stb_table, void (*)(stb_table *)> t(new stb_table(), table_destroy);
   t->device = device;
-  t->host = spin ? flatten_spin(line) : flatten(line);
+  t->host = std::move(host);
   t->min_ap2 = INFINITY;
   for (const ElemHeader &h : t->host.hdr)
     if ((h.flags & EF_NO_LOSS_CHECK) == 0) t->min_ap2 = std::fmin(t->min_ap2, std::fmin(h.apx * h.apx, h.apy * h.apy));
@@ -149,6 +149,10 @@ stb_table *table_build(const Line &line, int device, bool spin = false) {
   // segment (two buffers of half the shared memory each) by the seg_* variants
   if (!t->use_smem && !spin) set_segments(t.get(), (size_t)track_smem_limit(device) / 2 & ~size_t(15));
   return t.release();
+}
+
+stb_table *table_build(const Line &line, int device, bool spin = false) {
+  return table_build_from(spin ? flatten_spin(line) : flatten(line), device, spin);
 }
 
 TrackArgs make_args(stb_table *t) {
@@ -567,6 +571,27 @@ void Track(Line &line, double x[], int nturn, int &stable, int &lost_turn, int &
   Track_Batch(line, x, 1, nturn, &stable, &lost_turn, &lost_post);
 }
 
+// Cal_SRLoss_Particle (simtrack.cpp:20768-20781): one pass of x through
+// every element but the RF cavities, loss = (pt - pt0) GP.beta GP.energy.
+// The reference passes without loss tests; a particle that Track()'s tests
+// would stop (|x| or |y| > 0.1 at entry, outside an aperture, NaN) is
+// rejected here instead of tracked on.
+void Cal_SRLoss_Particle(Line &line, double x[], double &loss, int device) {
+  std::unique_ptr<stb_table, void (*)(stb_table *)> t(table_build_from(flatten(line, true), device, false),
+                                                      table_destroy);
+  const double pt0 = x[5];
+  double y[6];
+  for (int i = 0; i < 6; i++) y[i] = x[i];
+  int stable = 1, lost_turn = 0, lost_post = 0;
+  int rc = track_host(t.get(), y, 1, 1, 0.0, &stable, &lost_turn, &lost_post);
+  if (rc != STB_OK) throw Error(rc, last_error());
+  if (!stable)
+    throw Error(STB_EINVAL, "the particle fails Track()'s loss test (entry check or element " +
+                                std::to_string(lost_post) + "'s aperture); the reference's pass has none");
+  for (int i = 0; i < 6; i++) x[i] = y[i];
+  loss = (x[5] - pt0) * GP.beta * GP.energy;
+}
+
 void Track_Radial(Line &line, double x[], int nturn, int &stable, int &lost_turn, int &lost_post) {
   std::unique_ptr<stb_table, void (*)(stb_table *)> t(table_build(line, 0), table_destroy);
   int rc = radial_host(t.get(), x, 1, nturn, 0.0, &stable, &lost_turn, &lost_post);
@@ -740,6 +765,14 @@ int stb_cal_srloss_u0rad(stb_line *l, int track_form, double *u0rad_mev) {
   return guarded([&] {
     if (!l || !u0rad_mev) throw Error(STB_EINVAL, "NULL argument");
     *u0rad_mev = Cal_SRLoss_U0rad(*Lp(l), track_form != 0);
+    return STB_OK;
+  });
+}
+
+int stb_cal_srloss_particle(stb_line *l, double *x6, double *loss_mev, int device) {
+  return guarded([&] {
+    if (!l || !x6 || !loss_mev) throw Error(STB_EINVAL, "NULL argument");
+    Cal_SRLoss_Particle(*Lp(l), x6, *loss_mev, device);
     return STB_OK;
   });
 }

@@ -359,7 +359,7 @@ bool spin_form(Builder &B, const Element &E, ElemHeader &h, double &fl) {
 
 unsigned long long g_radiation_seed = 1324;
 
-HostTable flatten_impl(const Line &line, bool spin) {
+HostTable flatten_impl(const Line &line, bool spin, bool skip_rfcav) {
   if (GP.H_expand) throw Error(STB_EUNSUPPORTED, "GP.H_expand == true is not implemented on the GPU path");
   Builder B;
   HostTable &t = B.t;
@@ -389,6 +389,14 @@ HostTable flatten_impl(const Line &line, bool spin) {
     h.apx = E.APx;
     h.apy = E.APy;
     double fl = 0;
+    if (skip_rfcav && T == "RFCAV") {
+      // Cal_SRLoss_Particle (simtrack.cpp:20768-20781) passes every element
+      // but the cavities: no map, no misalignment.
+      h.op = OP_IDENTITY;
+      h.poff = B.here();
+      t.hdr.push_back(h);
+      continue;
+    }
 
     // GtoL dispatch (simtrack.cpp:3701-3741).  DRIFT and MARKER never call it,
     // nor do LBT::sPass and ILBT::sPass (11004, 11053) in spin tracking.
@@ -825,7 +833,7 @@ HostTable flatten_impl(const Line &line, bool spin) {
 unsigned long long radiation_seed() { return g_radiation_seed; }
 void set_radiation_seed(unsigned long long seed) { g_radiation_seed = seed; }
 
-HostTable flatten(const Line &line) { return flatten_impl(line, false); }
-HostTable flatten_spin(const Line &line) { return flatten_impl(line, true); }
+HostTable flatten(const Line &line, bool skip_rfcav) { return flatten_impl(line, false, skip_rfcav); }
+HostTable flatten_spin(const Line &line) { return flatten_impl(line, true, false); }
 
 }  // namespace stb

@@ -34,7 +34,8 @@ void set_radiation_seed(unsigned long long seed);
 // Throws stb::Error(STB_EUNSUPPORTED) for element types or settings that
 // the GPU kernel does not implement (H_expand, pitch/yaw, GSBEND's photon
 // Monte Carlo under GP.radiate).
-HostTable flatten(const Line &line);
+// skip_rfcav: every RFCAV becomes a no-op (Cal_SRLoss_Particle's pass).
+HostTable flatten(const Line &line, bool skip_rfcav = false);
 // Flatten for Track_Spin (simtrack.cpp:21766-21789): the orbit maps of
 // Element::sPass plus the Thomas-BMT rotation of spin() after every slice.
 // GSBEND and GMULT are not available in this form (STB_EUNSUPPORTED).

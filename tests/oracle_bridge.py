@@ -128,6 +128,8 @@ class RefOracle:
         L.ref_set_radiation.argtypes = [c_int, ctypes.c_ulonglong]
         L.ref_cal_srloss.argtypes = [c_void_p, c_int]
         L.ref_cal_srloss.restype = c_double
+        L.ref_cal_srloss_particle.argtypes = [c_void_p, c_void_p]
+        L.ref_cal_srloss_particle.restype = c_double
         L.ref_rng_id_base.argtypes = [c_long]
         L.ref_rng_stream.argtypes = [ctypes.c_ulonglong] * 3
         L.ref_rng_stream.restype = c_double

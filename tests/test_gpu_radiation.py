@@ -196,3 +196,33 @@ def test_gsbend_photon_emission_vs_reference():
     lost = so2 == 0
     assert np.array_equal(lg2[lost], lo2[lost]) and np.array_equal(pg2[lost], po2[lost])
     assert_close_traj(xg2[~lost], xo2[~lost], "survivors")
+
+
+@pytest.mark.parametrize("gsbend", [False, True])
+def test_srloss_particle_vs_reference(gsbend):
+    """Cal_SRLoss_Particle (simtrack.cpp:20768-20781): one pass through
+    every element but the RF cavities, radiating (radiate1 in the sector
+    bends or radiate2's photons in the GSBENDs, radiate in the combined-
+    function bends), from particle 0's stream on both sides; exit coordinates
+    within the parity tolerance and the loss within 1e-10 relative.  Without
+    radiation nothing but the cavities changes pt: the loss is exactly 0."""
+    _need_ref()
+    lat = lt.electron_ring(gsbend=gsbend)
+    line = lt.build_line(lat)
+    ref = oracle_bridge.RefOracle(cr=True)
+    ref.build(lat)
+    ref.L.ref_rng_id_base(0)
+    for x0 in (np.zeros(6), np.array([1e-3, 1e-4, -5e-4, 2e-5, 0.0, 3e-4])):
+        xg, xo = x0.copy(), x0.copy()
+        lg = api.Cal_SRLoss_Particle(line, xg)
+        lo = ref.L.ref_cal_srloss_particle(ref.line, xo.ctypes.data)
+        assert_close_traj(xg[None], xo[None], "exit")
+        assert lo < -0.2 and abs(lg - lo) <= 1e-10 * abs(lo), (lg, lo)
+    x = np.array([0.2, 0, 0, 0, 0, 0.0])  # Track()'s entry test would stop it
+    with pytest.raises(SimTrackError):
+        api.Cal_SRLoss_Particle(line, x)
+    assert x[0] == 0.2 and not x[1:].any()
+    api.Set_Radiation(False)
+    plain = lt.build_line(lt.electron_ring(gsbend=gsbend, radiate=False))
+    x = np.array([1e-3, 1e-4, -5e-4, 2e-5, 0.0, 3e-4])
+    assert api.Cal_SRLoss_Particle(plain, x) == 0.0 and x[5] == 3e-4
