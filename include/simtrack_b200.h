@@ -524,6 +524,25 @@ int stb_bb4d_soft_gaussian_device(double Np1, long n1, double *x1, double Np2, l
 int stb_bb4d_soft_gaussian_host(double Np1, long n1, double *x1, double Np2, long n2, double *x2, double gamma1,
                                 double gamma2, double bbscale1, double bbscale2, int device);
 
+/* Strong-strong beam-beam by particle-in-cell, 4D: BeamBeam4D_PIC(Np1, Mp1,
+ * xc1, Np2, Mp2, xc2, gamma1, gamma2, bbscale1, bbscale2),
+ * simtrack.cpp:23286-23378 (simtrack.h:1407).  Each beam's charge, deposited
+ * on a 64 x 64 grid 15 rms sizes wide around its centroid (the smaller rms
+ * size of the two beams per plane), gives the potential through the
+ * integrated Green function and FFT convolution on the doubled grid; the
+ * field kicks the other beam's macro-particles within 29 cells of their own
+ * centroid.  px and py of both AoS beams x1[6*n1], x2[6*n2] are updated in
+ * place, equal to the reference's bit for bit.  Each beam needs at least two
+ * macro-particles (an rms size), at most INT32_MAX / 9; a particle that
+ * would fall outside the grid (non-finite coordinates or rms size) gives
+ * STB_EINVAL.  Both forms return when done (the Green function is tabulated
+ * on the host between the moments and the deposition); the _device form
+ * works on device arrays on `stream`. */
+int stb_bb4d_pic_device(double Np1, long n1, double *x1, double Np2, long n2, double *x2, double gamma1,
+                        double gamma2, double bbscale1, double bbscale2, int device, void *stream);
+int stb_bb4d_pic_host(double Np1, long n1, double *x1, double Np2, long n2, double *x2, double gamma1, double gamma2,
+                      double bbscale1, double bbscale2, int device);
+
 /* Strong-strong beam-beam, sliced soft-Gaussian 6D: BeamBeam6D_SoftGaussian(
  * Np1, Mp1, x1, Np2, Mp2, x2, gamma1, gamma2, bbscale1, bbscale2, Nslice1,
  * Nslice2), simtrack.cpp:22874-23132 (simtrack.h:1406).  Both AoS bunches are

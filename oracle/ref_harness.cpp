@@ -493,6 +493,12 @@ void ref_bb4d_soft_gaussian(double Np1, int n1, double *x1, double Np2, int n2, 
   BeamBeam4D_SoftGaussian(Np1, n1, x1, Np2, n2, x2, gamma1, gamma2, bbscale1, bbscale2);
 }
 
+// BeamBeam4D_PIC (simtrack.cpp:23286).
+void ref_bb4d_pic(double Np1, int n1, double *x1, double Np2, int n2, double *x2, double gamma1, double gamma2,
+                  double bbscale1, double bbscale2) {
+  BeamBeam4D_PIC(Np1, n1, x1, Np2, n2, x2, gamma1, gamma2, bbscale1, bbscale2);
+}
+
 // FineTuneFinder, both overloads (simtrack.cpp:2288, 2321).
 double ref_fine_tune(int n, const double *x, const double *px, double lo, double hi) {
   std::vector<double> a(x, x + n);

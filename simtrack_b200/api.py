@@ -66,6 +66,18 @@ def BeamBeam4D_SoftGaussian(Np1: float, x1: np.ndarray, Np2: float, x2: np.ndarr
                                             bbscale2, device))
 
 
+def BeamBeam4D_PIC(Np1: float, x1: np.ndarray, Np2: float, x2: np.ndarray, gamma1: float, gamma2: float,
+                   bbscale1: float, bbscale2: float, device: int = 0) -> None:
+    """BeamBeam4D_PIC (simtrack.cpp:23286-23378) on the GPU: each bunch's
+    charge on a 64 x 64 grid, the potential by FFT convolution with the
+    integrated Green function, the field kicking the other bunch (numpy
+    (n, 6) float64, updated in place)."""
+    b1, b2 = _bunch(x1), _bunch(x2)
+    P = lambda a: a.ctypes.data_as(POINTER(c_double))
+    check(lib().stb_bb4d_pic_host(Np1, len(b1), P(b1), Np2, len(b2), P(b2), gamma1, gamma2, bbscale1, bbscale2,
+                                  device))
+
+
 def BeamBeam6D_SoftGaussian(Np1: float, x1: np.ndarray, Np2: float, x2: np.ndarray, gamma1: float, gamma2: float,
                             bbscale1: float, bbscale2: float, Nslice1: int, Nslice2: int, zb1=None, zb2=None,
                             device: int = 0) -> None:

@@ -24,7 +24,7 @@ CSRC = PKG / "csrc"
 LIBDIR = PKG / "_lib"
 LIB = LIBDIR / "libsimtrack_b200.so"
 
-CUDA_SOURCES = ["stb_track.cu", "stb_track_fast.cu", "stb_scan.cu", "stb_track_static.cu", "stb_tune.cu", "stb_spin.cu", "stb_radial.cu", "stb_diag.cu", "stb_mlp.cu", "stb_mlp_ops.cu", "stb_ssbb.cu"]
+CUDA_SOURCES = ["stb_track.cu", "stb_track_fast.cu", "stb_scan.cu", "stb_track_static.cu", "stb_tune.cu", "stb_spin.cu", "stb_radial.cu", "stb_diag.cu", "stb_mlp.cu", "stb_mlp_ops.cu", "stb_ssbb.cu", "stb_pic.cu"]
 CXX_SOURCES = ["stb_elements.cpp", "stb_srloss.cpp", "stb_flatten.cpp", "stb_capi.cpp", "stb_scan_host.cpp", "stb_mlp_host.cpp",
                "stb_tune_host.cpp", "stb_readers.cpp", "stb_da.cpp",
                "stb_orbit.cpp", "stb_tbt.cpp"]

@@ -1206,7 +1206,53 @@ void soft_gaussian_args(double Np1, long n1, double Np2, long n2, double gamma1,
   c4_1 = 2 * Np2 * rp / gamma1;
   c4_2 = 2 * Np1 * rp / gamma2;
 }
+void pic_args(long n1, long n2, double gamma1, double gamma2) {
+  // the reference keeps Mp in an int and the sort keys 9 Mp items in one
+  if (n1 < 2 || n2 < 2) throw Error(STB_EINVAL, "each beam needs at least two macro-particles (an rms size)");
+  if (n1 > INT32_MAX / 9 || n2 > INT32_MAX / 9) throw Error(STB_EINVAL, "too many macro-particles");
+  if (!(gamma1 > 0) || !(gamma2 > 0)) throw Error(STB_EINVAL, "gamma must be positive");
+}
+
+void pic_run(double Np1, long n1, double *x1, double Np2, long n2, double *x2, double gamma1, double gamma2,
+             double bbscale1, double bbscale2, int device, cudaStream_t s) {
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  const cudaError_t e = pic_4d(Np1, n1, x1, Np2, n2, x2, gamma1, gamma2, bbscale1, bbscale2, sms, s);
+  if (e == cudaErrorInvalidValue)
+    throw Error(STB_EINVAL, "a macro-particle maps outside the 64 x 64 grid (non-finite rms size or coordinates)");
+  cuda_check(e, "particle-in-cell beam-beam");
+}
 }  // namespace
+
+int stb_bb4d_pic_device(double Np1, long n1, double *x1, double Np2, long n2, double *x2, double gamma1,
+                        double gamma2, double bbscale1, double bbscale2, int device, void *stream) {
+  return guarded([&] {
+    if (!x1 || !x2) throw Error(STB_EINVAL, "NULL beam");
+    pic_args(n1, n2, gamma1, gamma2);
+    DeviceGuard g(device);
+    pic_run(Np1, n1, x1, Np2, n2, x2, gamma1, gamma2, bbscale1, bbscale2, device, (cudaStream_t)stream);
+    return STB_OK;
+  });
+}
+
+int stb_bb4d_pic_host(double Np1, long n1, double *x1, double Np2, long n2, double *x2, double gamma1, double gamma2,
+                      double bbscale1, double bbscale2, int device) {
+  return guarded([&] {
+    if (!x1 || !x2) throw Error(STB_EINVAL, "NULL beam");
+    pic_args(n1, n2, gamma1, gamma2);
+    DeviceGuard g(device);
+    double *d = nullptr;
+    const size_t b1 = sizeof(double) * 6 * (size_t)n1, b2 = sizeof(double) * 6 * (size_t)n2;
+    cuda_check(cudaMalloc(&d, b1 + b2), "cudaMalloc(beams)");
+    DevFree f{d};
+    cuda_check(cudaMemcpy(d, x1, b1, cudaMemcpyHostToDevice), "upload beam 1");
+    cuda_check(cudaMemcpy(d + 6 * n1, x2, b2, cudaMemcpyHostToDevice), "upload beam 2");
+    pic_run(Np1, n1, d, Np2, n2, d + 6 * n1, gamma1, gamma2, bbscale1, bbscale2, device, 0);
+    cuda_check(cudaMemcpy(x1, d, b1, cudaMemcpyDeviceToHost), "download beam 1");
+    cuda_check(cudaMemcpy(x2, d + 6 * n1, b2, cudaMemcpyDeviceToHost), "download beam 2");
+    return STB_OK;
+  });
+}
 
 int stb_bb4d_soft_gaussian_device(double Np1, long n1, double *x1, double Np2, long n2, double *x2, double gamma1,
                                   double gamma2, double bbscale1, double bbscale2, int device, void *stream) {

@@ -108,6 +108,16 @@ cudaError_t soft_gaussian_6d(double Np1, long Mp1, double *x1, double Np2, long 
                              double gamma2, double bbscale1, double bbscale2, int Nslice1, int Nslice2, int num_sms,
                              cudaStream_t s);
 
+// Cal_Mean_RMS of x and y (simtrack.cpp:724-743) of two device AoS beams,
+// out8 = mean x, mean y, rms x, rms y of beam 1, then of beam 2, the
+// reference's running sums.
+cudaError_t beam_pair_mean_rms(const double *x1, long n1, const double *x2, long n2, double *out8, cudaStream_t s);
+// BeamBeam4D_PIC (simtrack.cpp:23286-23378) on device AoS beams
+// (stb_pic.cu; synchronises `s`).  cudaErrorInvalidValue if a particle maps
+// outside the 64 x 64 grid.
+cudaError_t pic_4d(double Np1, long Mp1, double *x1, double Np2, long Mp2, double *x2, double gamma1, double gamma2,
+                   double bbscale1, double bbscale2, int num_sms, cudaStream_t s);
+
 size_t track_smem_bytes(int nelem, int npool_padded);
 // The loss-test mode of a launch with circular aperture r2 (+inf: none) on a
 // table whose loss-checked elements have min(RN(APx^2), RN(APy^2)) >= min_ap2.

@@ -1,0 +1,452 @@
+// Strong-strong beam-beam by particle-in-cell, 4D: BeamBeam4D_PIC
+// (simtrack.cpp:23286-23378) on the GPU.
+//
+// Each beam's charge is deposited on a 64 x 64 grid (triangular-shaped
+// cloud, Cal_Grid_Weight 2747-2791, Charge2Grid 2793-2806), the potential
+// is the convolution of the charge with the integrated Green function of the
+// 2D Poisson equation on the doubled 128 x 128 grid (Cal_Effective_Green_
+// Function 2881-2921, Cal_Potential_Convolution 2955-2989, both through the
+// reference's radix-2 FFT2D, 2583-2695), the field its 3 x 3-stencil
+// gradient (Cal_Electric_Field 2998-3019), interpolated back to the other
+// beam's particles with the same weights (Interpolate_Electric_Field
+// 3021-3045), which take the kick.
+//
+// Every result equals the reference's bit for bit, so each step keeps the
+// reference's operations and their order:
+//   * deposition: the reference adds each particle's nine weights to the grid
+//     in particle order.  Here every particle emits its nine (cell, weight)
+//     items, a stable radix sort on the cell brings each cell's items
+//     together in particle order, and one thread per cell adds them from
+//     zero, so each cell's sum is the reference's chain of additions;
+//   * FFT: the reference's in-place radix-2 transform (bit reversal, then
+//     log2 n butterfly stages whose twiddles follow a recurrence).  The
+//     twiddles do not depend on the data: the host runs the recurrence once
+//     and the butterflies of a stage, independent of each other, run one per
+//     thread with the reference's expressions;
+//   * the Green function takes atan and log per cell: it is tabulated on the
+//     host with the C library the reference calls (both directions' tables
+//     at once, rows split across host threads), then transformed on the GPU.
+#include <cuda_runtime.h>
+
+#include <cub/device/device_radix_sort.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <thread>
+#include <vector>
+
+#include "stb_kernels.hpp"
+
+namespace stb {
+namespace {
+
+constexpr int kNx = 64, kNy = 64;           // grid (Nx, Ny in the reference)
+constexpr int kNsigma = 15;                 // grid width in rms sizes
+constexpr int kN2 = 2 * kNx;                // doubled grid, 128 x 128
+constexpr int kLog2N2 = 7;
+constexpr int kCells = kNx * kNy;
+constexpr uint32_t kNoCell = kCells;        // key of a particle outside the cut
+constexpr int kKeyBits = 13;                // keys 0 .. kCells
+constexpr double kEps0 = 8.854187817e-12;
+
+static_assert(kNx == kNy, "the reference indexes its grids with Nx as the row length of both axes");
+
+// Cal_Grid_Weight (simtrack.cpp:2747-2791): the three mesh lines nearest the
+// point and their weights along one axis.
+__device__ __forceinline__ void grid_weight_1d(double d, double h, int m[3], double w[3]) {
+  const double f = d / h;
+  const int i = (int)f;
+  double r;
+  if ((f - i) <= 0.5) {
+    m[0] = i;
+    m[1] = i + 1;
+    m[2] = i - 1;
+    r = f - i;
+  } else {
+    m[0] = i + 1;
+    m[1] = i;
+    m[2] = i + 2;
+    r = (i + 1) - f;
+  }
+  const double r2 = r * r;
+  w[0] = 0.75 - r2;
+  w[1] = 0.5 * (0.25 + r + r2);
+  w[2] = 0.5 * (0.25 - r + r2);
+}
+
+__device__ __forceinline__ bool mesh_ok(const int m[3], int n) {
+  return m[0] >= 0 && m[0] < n && m[1] >= 0 && m[1] < n && m[2] >= 0 && m[2] < n;
+}
+
+// The cut of Charge2Grid's and the kick's callers: |x - mean| < (Nx/2 - 3) hx.
+__device__ __forceinline__ bool in_cut(double xp, double yp, double mx, double my, double hx, double hy) {
+  return fabs(xp - mx) < (kNx / 2 - 3) * hx && fabs(yp - my) < (kNy / 2 - 3) * hy;
+}
+
+struct GridFrame {
+  double mx, my;  // mean of the beam whose particles pass the cut
+  double x0, y0;  // grid origin
+  double hx, hy;
+};
+
+// Nine (cell, weight) items per particle of the depositing beam, in the
+// reference's (i, j) order; a particle outside the cut emits kNoCell.
+__global__ void deposit_items_kernel(const double *x, long n, GridFrame g, uint32_t *keys, double *vals,
+                                     int *err) {
+  for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long)gridDim.x * blockDim.x) {
+    const double xp = x[6 * p], yp = x[6 * p + 2];
+    uint32_t *k = keys + 9 * p;
+    double *v = vals + 9 * p;
+    int xm[3], ym[3];
+    double xw[3], yw[3];
+    bool ok = in_cut(xp, yp, g.mx, g.my, g.hx, g.hy);
+    if (ok) {
+      grid_weight_1d(xp - g.x0, g.hx, xm, xw);
+      grid_weight_1d(yp - g.y0, g.hy, ym, yw);
+      if (!mesh_ok(xm, kNx) || !mesh_ok(ym, kNy)) {
+        atomicExch(err, 1);
+        ok = false;
+      }
+    }
+    for (int i = 0; i < 3; i++)
+      for (int j = 0; j < 3; j++) {
+        k[3 * i + j] = ok ? (uint32_t)(xm[i] * kNx + ym[j]) : kNoCell;
+        v[3 * i + j] = ok ? xw[i] * yw[j] : 0.0;
+      }
+  }
+}
+
+// First and one-past-last item of every cell in the sorted keys.
+__global__ void cell_bounds_kernel(const uint32_t *keys, long m, int *start, int *end) {
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (long)gridDim.x * blockDim.x) {
+    const uint32_t k = keys[i];
+    if (k >= kNoCell) continue;
+    if (i == 0 || keys[i - 1] != k) start[k] = (int)i;
+    if (i == m - 1 || keys[i + 1] != k) end[k] = (int)(i + 1);
+  }
+}
+
+// src[c] = 0 + w_1 + w_2 + ... over the cell's items in particle order,
+// written straight into the zero-padded real part of the doubled grid
+// (Cal_Potential_Convolution's src_c_r); the rest of both parts is zero.
+__global__ void cell_sum_pad_kernel(const double *vals, const int *start, const int *end, double *re, double *im) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= kN2 * kN2) return;
+  const int i = t / kN2, j = t % kN2;
+  double s = 0.;
+  if (i < kNx && j < kNy) {
+    const int c = i * kNx + j;
+    for (int q = start[c]; q < end[c]; q++) s = s + vals[q];
+  }
+  re[t] = s;
+  im[t] = 0.;
+}
+
+// One FFT1D (simtrack.cpp:2583-2647) per block over n = 128 points: line b
+// holds the elements base + t * es, base = b * ls.  tw holds the butterfly
+// twiddles (u1, u2) of every stage, stage l's l1 = 2^l values from offset
+// l1 - 1, as the reference's recurrence produces them for this direction.
+// dir == 1 divides by n, as the reference's forward transform does.
+__global__ void __launch_bounds__(kN2 / 2) fft_lines_kernel(double *re, double *im, int ls, int es,
+                                                           const double2 *tw, int dir) {
+  __shared__ double sr[kN2], si[kN2];
+  const int base = blockIdx.x * ls;
+  for (int t = threadIdx.x; t < kN2; t += blockDim.x) {
+    const int r = (int)(__brev((unsigned)t) >> (32 - kLog2N2));
+    sr[r] = re[base + t * es];
+    si[r] = im[base + t * es];
+  }
+  const int b = threadIdx.x;
+  for (int l = 0; l < kLog2N2; l++) {
+    __syncthreads();
+    const int l1 = 1 << l;
+    const int j = b & (l1 - 1);
+    const int i = ((b >> l) << (l + 1)) + j, i1 = i + l1;
+    const double2 u = tw[l1 - 1 + j];
+    const double t1 = u.x * sr[i1] - u.y * si[i1];
+    const double t2 = u.x * si[i1] + u.y * sr[i1];
+    sr[i1] = sr[i] - t1;
+    si[i1] = si[i] - t2;
+    sr[i] += t1;
+    si[i] += t2;
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < kN2; t += blockDim.x) {
+    double a = sr[t], c = si[t];
+    if (dir == 1) {
+      a /= (double)kN2;
+      c /= (double)kN2;
+    }
+    re[base + t * es] = a;
+    im[base + t * es] = c;
+  }
+}
+
+// FFT2D (simtrack.cpp:2649-2695): the columns x[i*n + j] over i, then the rows.
+void fft2d(double *re, double *im, const double2 *tw, int dir, cudaStream_t s) {
+  fft_lines_kernel<<<kN2, kN2 / 2, 0, s>>>(re, im, 1, kN2, tw, dir);
+  fft_lines_kernel<<<kN2, kN2 / 2, 0, s>>>(re, im, kN2, 1, tw, dir);
+}
+
+// The spectrum product of Cal_Potential_Convolution, in place into (re, im).
+__global__ void spectrum_product_kernel(double *re, double *im, const double *gr, const double *gi) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= kN2 * kN2) return;
+  const double a = re[t], b = im[t], c = gr[t], d = gi[t];
+  re[t] = a * c - b * d;
+  im[t] = a * d + b * c;
+}
+
+// phi from the inverse transform, then Cal_Electric_Field's stencil
+// (zero on the grid's border).  One thread per cell; phi is re-derived by
+// each neighbour with the same expression, so every value is the reference's.
+__device__ __forceinline__ double phi_at(const double *re, int i, int j) {
+  return re[i * kN2 + j] * 2 * kNx * 2 * kNy / 2 / 3.14159265 / kEps0;
+}
+
+__global__ void field_kernel(const double *re, double hx, double hy, double *Ex, double *Ey) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= kCells) return;
+  const int i = t / kNx, j = t % kNx;
+  double ex = 0., ey = 0.;
+  if (i >= 1 && i < kNx - 1 && j >= 1 && j < kNy - 1) {
+    ex = -((phi_at(re, i + 1, j + 1) - phi_at(re, i - 1, j + 1)) + 4 * (phi_at(re, i + 1, j) - phi_at(re, i - 1, j)) +
+           (phi_at(re, i + 1, j - 1) - phi_at(re, i - 1, j - 1))) /
+         12. / hx;
+    ey = -((phi_at(re, i + 1, j + 1) - phi_at(re, i + 1, j - 1)) + 4 * (phi_at(re, i, j + 1) - phi_at(re, i, j - 1)) +
+           (phi_at(re, i - 1, j + 1) - phi_at(re, i - 1, j - 1))) /
+         12. / hy;
+  }
+  Ex[t] = ex;
+  Ey[t] = ey;
+}
+
+// The kicked beam: particles inside the cut (around their own mean) take
+// the field interpolated at (x - xoffset, y - yoffset) on the other beam's
+// grid; px += ex e bbscale / (gamma m_p c^2 / e) (Np_other / Mp_other).
+__global__ void pic_kick_kernel(double *x, long n, GridFrame g, double xoffset, double yoffset, const double *Ex,
+                                const double *Ey, double bbscale, double gamma, double np_per_mp, int *err) {
+  for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long)gridDim.x * blockDim.x) {
+    double *q = x + 6 * p;
+    const double xp = q[0], yp = q[2];
+    if (!in_cut(xp, yp, g.mx, g.my, g.hx, g.hy)) continue;
+    const double xs = xp - xoffset, ys = yp - yoffset;
+    int xm[3], ym[3];
+    double xw[3], yw[3];
+    grid_weight_1d(xs - g.x0, g.hx, xm, xw);
+    grid_weight_1d(ys - g.y0, g.hy, ym, yw);
+    if (!mesh_ok(xm, kNx) || !mesh_ok(ym, kNy)) {
+      atomicExch(err, 1);
+      continue;
+    }
+    double ex = 0., ey = 0.;
+    for (int i = 0; i < 3; i++)
+      for (int j = 0; j < 3; j++) {
+        ex = ex + Ex[xm[i] * kNx + ym[j]] * xw[i] * yw[j];
+        ey = ey + Ey[xm[i] * kNx + ym[j]] * xw[i] * yw[j];
+      }
+    q[1] = q[1] + ex * 1.60217662e-19 * bbscale / (gamma * 938.27201e6) * np_per_mp;
+    q[3] = q[3] + ey * 1.60217662e-19 * bbscale / (gamma * 938.27201e6) * np_per_mp;
+  }
+}
+
+// The butterfly twiddles of FFT1D for n = 2^m in direction dir, from the
+// reference's recurrence (u advanced by (c1, c2) within a stage; c1, c2
+// halved in angle between stages).
+std::vector<double2> fft_twiddles(int m, int dir) {
+  std::vector<double2> tw;
+  double c1 = -1.0, c2 = 0.0;
+  long l2 = 1;
+  for (int l = 0; l < m; l++) {
+    const long l1 = l2;
+    l2 <<= 1;
+    double u1 = 1.0, u2 = 0.0;
+    for (long j = 0; j < l1; j++) {
+      tw.push_back(make_double2(u1, u2));
+      const double z = u1 * c1 - u2 * c2;
+      u2 = u1 * c2 + u2 * c1;
+      u1 = z;
+    }
+    c2 = std::sqrt((1.0 - c1) / 2.0);
+    if (dir == 1) c2 = -c2;
+    c1 = std::sqrt((1.0 + c1) / 2.0);
+  }
+  return tw;
+}
+
+// int_green and calc_egreen (simtrack.cpp:2808-2879): the Green function
+// of the 2D Poisson equation integrated over the cell [x1, x2] x [y1, y2].
+double int_green(double x, double y) {
+  if (0 == x || 0 == y) return 0;
+  const double x2 = x * x, y2 = y * y;
+  return -3 * x * y + x2 * std::atan(y / x) + y2 * std::atan(x / y) + x * y * std::log(x2 + y2);
+}
+
+double calc_egreen(double x1, double x2, double y1, double y2, double hx, double hy) {
+  if (x1 * x2 * y1 * y2 != 0.) {
+    int s11 = 1, s12 = 1, s21 = 1, s22 = 1;
+    if (x1 > 0) {
+      s11 *= -1;
+      s12 *= -1;
+    } else if (x1 < 0 && x2 < 0) {
+      s21 *= -1;
+      s22 *= -1;
+    }
+    if (y1 > 0) {
+      s11 *= -1;
+      s21 *= -1;
+    } else if (y1 < 0 && y2 < 0) {
+      s12 *= -1;
+      s22 *= -1;
+    }
+    x1 = std::fabs(x1);
+    x2 = std::fabs(x2);
+    y1 = std::fabs(y1);
+    y2 = std::fabs(y2);
+    const double v11 = int_green(x1, y1), v12 = int_green(x1, y2);
+    const double v21 = int_green(x2, y1), v22 = int_green(x2, y2);
+    const double r = s11 * v11 + s12 * v12 + s21 * v21 + s22 * v22;
+    return -1.0 * r / hx / hy / 2;
+  }
+  double r = 0.;
+  for (int i = 0; i < 20; i++)
+    for (int j = 0; j < 20; j++) {
+      const double tx = x1 + (i - 1) * hx / 20 + hx / 40;
+      const double ty = y1 + (j - 1) * hy / 20 + hy / 40;
+      if (tx != 0. && ty != 0.) r = r - 0.5 * std::log(tx * tx + ty * ty);
+    }
+  return r / 400.;
+}
+
+// Cal_Effective_Green_Function's tables before their transform (2881-2918)
+// for both directions: g[d][i * 2Nx + j] over the four quadrants of the
+// doubled grid, offsets (xoff[d], yoff[d]); the 2 x 128 rows are split across
+// host threads.
+void green_tables(const double xoff[2], const double yoff[2], double hx, double hy, double *const g[2]) {
+  auto rows = [&](int r0, int r1) {
+    for (int r = r0; r < r1; r++) {
+      const int d = r / kN2, i = r % kN2;
+      for (int j = 0; j < kN2; j++) {
+        double x1, y1;
+        if (i <= kNx - 1) x1 = xoff[d] + i * hx - 0.5 * hx;
+        else x1 = xoff[d] - (2 * kNx - i) * hx - 0.5 * hx;
+        if (j <= kNy - 1) y1 = yoff[d] + j * hy - 0.5 * hy;
+        else y1 = yoff[d] - (2 * kNy - j) * hy - 0.5 * hy;
+        g[d][i * kN2 + j] = calc_egreen(x1, x1 + hx, y1, y1 + hy, hx, hy);
+      }
+    }
+  };
+  const int nrows = 2 * kN2;
+  const int nt = (int)std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+  std::vector<std::thread> th;
+  const int per = (nrows + nt - 1) / nt;
+  for (int t = 0; t < nt; t++) {
+    const int a = t * per, b = std::min(nrows, a + per);
+    if (a < b) th.emplace_back(rows, a, b);
+  }
+  for (auto &t : th) t.join();
+}
+
+}  // namespace
+
+cudaError_t pic_4d(double Np1, long Mp1, double *x1, double Np2, long Mp2, double *x2, double gamma1, double gamma2,
+                   double bbscale1, double bbscale2, int num_sms, cudaStream_t s) {
+  const long nmax = std::max(Mp1, Mp2), nitem = 9 * nmax;
+  const size_t grid2 = (size_t)kN2 * kN2;
+  size_t sort_bytes = 0;
+  cudaError_t e = cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, (const uint32_t *)nullptr, (uint32_t *)nullptr,
+                                                  (const double *)nullptr, (double *)nullptr, (int)nitem, 0, kKeyBits,
+                                                  s);
+  if (e != cudaSuccess) return e;
+  // doubles: green (re, im) per direction, work (re, im), Ex, Ey, moments,
+  // twiddles (2 directions of the transform), items; then keys, cell bounds,
+  // the error flag and the sort's scratch
+  const int ntw = kN2 - 1;
+  const size_t nd = 6 * grid2 + 2 * kCells + 8 + 4 * (size_t)ntw + 2 * (size_t)nitem;
+  const size_t bytes = sizeof(double) * nd + sizeof(uint32_t) * 2 * (size_t)nitem + sizeof(int) * (2 * kCells + 2) +
+                       sort_bytes + 256;
+  unsigned char *buf = nullptr;
+  if ((e = cudaMalloc(&buf, bytes)) != cudaSuccess) return e;
+  double *g_re[2], *g_im[2];
+  g_re[0] = reinterpret_cast<double *>(buf);
+  g_im[0] = g_re[0] + grid2;
+  g_re[1] = g_im[0] + grid2;
+  g_im[1] = g_re[1] + grid2;
+  double *wr = g_im[1] + grid2, *wi = wr + grid2;
+  double *Ex = wi + grid2, *Ey = Ex + kCells, *m8 = Ey + kCells;
+  double2 *tw_fwd = reinterpret_cast<double2 *>(m8 + 8), *tw_inv = tw_fwd + ntw;
+  double *vals_in = reinterpret_cast<double *>(tw_inv + ntw), *vals_out = vals_in + nitem;
+  uint32_t *keys_in = reinterpret_cast<uint32_t *>(vals_out + nitem), *keys_out = keys_in + nitem;
+  int *cstart = reinterpret_cast<int *>(keys_out + nitem), *cend = cstart + kCells, *err = cend + kCells;
+  void *sort_tmp = reinterpret_cast<void *>(((uintptr_t)(err + 2) + 255) & ~(uintptr_t)255);
+
+  const std::vector<double2> twf = fft_twiddles(kLog2N2, 1), twi = fft_twiddles(kLog2N2, -1);
+  std::vector<double> h_m8(8), h_green(2 * grid2);
+  auto grid_of = [&](long n) {
+    const long g = (n + 255) / 256, cap = (long)num_sms * 8;
+    return (unsigned)(g < 1 ? 1 : g > cap ? cap : g);
+  };
+  int h_err = 0;
+  do {
+    if ((e = cudaMemcpyAsync(tw_fwd, twf.data(), sizeof(double2) * ntw, cudaMemcpyHostToDevice, s)) != cudaSuccess)
+      break;
+    if ((e = cudaMemcpyAsync(tw_inv, twi.data(), sizeof(double2) * ntw, cudaMemcpyHostToDevice, s)) != cudaSuccess)
+      break;
+    if ((e = cudaMemsetAsync(err, 0, sizeof(int), s)) != cudaSuccess) break;
+    if ((e = beam_pair_mean_rms(x1, Mp1, x2, Mp2, m8, s)) != cudaSuccess) break;
+    if ((e = cudaMemcpyAsync(h_m8.data(), m8, sizeof(double) * 8, cudaMemcpyDeviceToHost, s)) != cudaSuccess) break;
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) break;
+    const double mean1[2] = {h_m8[0], h_m8[1]}, rms1[2] = {h_m8[2], h_m8[3]};
+    const double mean2[2] = {h_m8[4], h_m8[5]}, rms2[2] = {h_m8[6], h_m8[7]};
+    const double rmsx = rms1[0] > rms2[0] ? rms2[0] : rms1[0];
+    const double rmsy = rms1[1] > rms2[1] ? rms2[1] : rms1[1];
+    const double hx = kNsigma * rmsx / kNx, hy = kNsigma * rmsy / kNy;
+    // direction 0: beam 1 deposits, beam 2 is kicked; direction 1 the reverse
+    const double xoff[2] = {mean2[0] - mean1[0], mean1[0] - mean2[0]};
+    const double yoff[2] = {mean2[1] - mean1[1], mean1[1] - mean2[1]};
+    double *const hg[2] = {h_green.data(), h_green.data() + grid2};
+    green_tables(xoff, yoff, hx, hy, hg);
+    for (int d = 0; d < 2 && e == cudaSuccess; d++) {
+      if ((e = cudaMemcpyAsync(g_re[d], hg[d], sizeof(double) * grid2, cudaMemcpyHostToDevice, s)) != cudaSuccess ||
+          (e = cudaMemsetAsync(g_im[d], 0, sizeof(double) * grid2, s)) != cudaSuccess)
+        break;
+      fft2d(g_re[d], g_im[d], tw_fwd, 1, s);
+    }
+    for (int d = 0; d < 2 && e == cudaSuccess; d++) {
+      const double *ms = d == 0 ? mean1 : mean2, *mt = d == 0 ? mean2 : mean1;
+      const double *xs = d == 0 ? x1 : x2;
+      double *xt = d == 0 ? x2 : x1;
+      const long ns = d == 0 ? Mp1 : Mp2, nt = d == 0 ? Mp2 : Mp1;
+      const double np_per_mp = (d == 0 ? Np1 : Np2) / (double)(int)ns;
+      const GridFrame gs{ms[0], ms[1], ms[0] - kNx * hx / 2, ms[1] - kNy * hy / 2, hx, hy};
+      deposit_items_kernel<<<grid_of(ns), 256, 0, s>>>(xs, ns, gs, keys_in, vals_in, err);
+      if ((e = cub::DeviceRadixSort::SortPairs(sort_tmp, sort_bytes, keys_in, keys_out, vals_in, vals_out,
+                                               (int)(9 * ns), 0, kKeyBits, s)) != cudaSuccess)
+        break;
+      if ((e = cudaMemsetAsync(cstart, 0, sizeof(int) * 2 * kCells, s)) != cudaSuccess) break;
+      cell_bounds_kernel<<<grid_of(9 * ns), 256, 0, s>>>(keys_out, 9 * ns, cstart, cend);
+      cell_sum_pad_kernel<<<(int)(grid2 / 128), 128, 0, s>>>(vals_out, cstart, cend, wr, wi);
+      fft2d(wr, wi, tw_fwd, 1, s);
+      spectrum_product_kernel<<<(int)(grid2 / 256), 256, 0, s>>>(wr, wi, g_re[d], g_im[d]);
+      fft2d(wr, wi, tw_inv, -1, s);
+      field_kernel<<<kCells / 128, 128, 0, s>>>(wr, hx, hy, Ex, Ey);
+      GridFrame gt = gs;
+      gt.mx = mt[0];
+      gt.my = mt[1];
+      pic_kick_kernel<<<grid_of(nt), 256, 0, s>>>(xt, nt, gt, xoff[d], yoff[d], Ex, Ey,
+                                                   d == 0 ? bbscale2 : bbscale1, d == 0 ? gamma2 : gamma1,
+                                                   np_per_mp, err);
+      e = cudaGetLastError();
+    }
+    if (e != cudaSuccess) break;
+    if ((e = cudaMemcpyAsync(&h_err, err, sizeof(int), cudaMemcpyDeviceToHost, s)) != cudaSuccess) break;
+    e = cudaStreamSynchronize(s);
+  } while (false);
+  cudaStreamSynchronize(s);
+  cudaFree(buf);
+  if (e == cudaSuccess && h_err) e = cudaErrorInvalidValue;
+  return e;
+}
+
+}  // namespace stb

@@ -9,11 +9,11 @@
 // the tracking kernels, bb4d in stb_physics.cuh).
 //
 // The moments are the reference's running sums in the reference's order:
-// one CTA stages the particles in shared memory and one thread adds them one
-// by one, so the sums round exactly as the reference's loop does (a tree
-// reduction would round differently and the kicks would differ in the last
-// bits).  That pass is a dependent chain of n additions; the kicks are one
-// thread per particle.
+// a CTA per beam stages the particles in shared memory and one thread per
+// sum adds them one by one, so the sums round exactly as the reference's
+// loop does (a tree reduction would round differently and the kicks would
+// differ in the last bits).  Each sum is a dependent chain of n additions;
+// the kicks are one thread per particle.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -25,39 +25,58 @@
 namespace stb {
 namespace {
 
-// mean[0..1], rms[0..1] of x and y of n particles, AoS x[6 n].  The CTA
-// stages kMomentChunk particles' x and y in shared memory; thread 0 adds them
-// in particle order (the loads of the next chunk do not wait on its sums).
-constexpr int kMomentBlock = 256, kMomentChunk = 2048;
-__global__ void __launch_bounds__(kMomentBlock) soft_gaussian_moments_kernel(const double *x, long n, double *out4) {
-  __shared__ double cx[kMomentChunk], cy[kMomentChunk];
-  double sx = 0, sy = 0, sx2 = 0, sy2 = 0;
-  for (long base = 0; base < n; base += kMomentChunk) {
+// mean[0..1], rms[0..1] of x and y of n particles, AoS x[6 n]; CTA b
+// (0 or 1) takes beam b of the pair and writes out8[4b .. 4b+3].  The four
+// running sums are independent chains: lane 0 of warps 0-3 each keeps one
+// (sum x, sum y, sum x^2, sum y^2), adding the staged particles in order,
+// while warps 4-7 stage the next kMomentChunk particles' x and y in the other
+// shared-memory buffer.  Each chain is a dependent sequence of n additions,
+// which no parallel split would round the same way.
+constexpr int kMomentBlock = 256, kMomentChunk = 1024;
+__global__ void __launch_bounds__(kMomentBlock) moments_pair_kernel(const double *xa, long na, const double *xb,
+                                                                    long nb, double *out8) {
+  __shared__ double cx[2][kMomentChunk], cy[2][kMomentChunk];
+  __shared__ double sums[4];
+  const double *x = blockIdx.x == 0 ? xa : xb;
+  const long n = blockIdx.x == 0 ? na : nb;
+  double *out4 = out8 + 4 * blockIdx.x;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  auto stage = [&](long base, int buf, int t0, int nt) {
     const int m = (int)(n - base < kMomentChunk ? n - base : kMomentChunk);
-    for (int k = threadIdx.x; k < m; k += kMomentBlock) {
-      cx[k] = x[6 * (base + k)];
-      cy[k] = x[6 * (base + k) + 2];
+    for (int k = t0; k < m; k += nt) {
+      cx[buf][k] = x[6 * (base + k)];
+      cy[buf][k] = x[6 * (base + k) + 2];
     }
-    __syncthreads();
-    if (threadIdx.x == 0) {
+  };
+  if (n > 0) stage(0, 0, threadIdx.x, kMomentBlock);
+  __syncthreads();
+  double acc = 0;
+  for (long base = 0, c = 0; base < n; base += kMomentChunk, c++) {
+    const int buf = (int)(c & 1);
+    if (warp >= 4) {
+      if (base + kMomentChunk < n) stage(base + kMomentChunk, buf ^ 1, threadIdx.x - 128, kMomentBlock - 128);
+    } else if (lane == 0) {
+      const int m = (int)(n - base < kMomentChunk ? n - base : kMomentChunk);
+      const double *v = (warp & 1) ? cy[buf] : cx[buf];
+      if (warp < 2) {
 #pragma unroll 8
-      for (int j = 0; j < m; j++) {
-        const double a = cx[j], b = cy[j];
-        sx = sx + a;
-        sy = sy + b;
-        sx2 = sx2 + a * a;
-        sy2 = sy2 + b * b;
+        for (int j = 0; j < m; j++) acc = acc + v[j];
+      } else {
+#pragma unroll 8
+        for (int j = 0; j < m; j++) acc = acc + v[j] * v[j];
       }
     }
     __syncthreads();
   }
+  if (warp < 4 && lane == 0) sums[warp] = acc;
+  __syncthreads();
   if (threadIdx.x == 0) {
     const double N = (double)n;
-    const double mx = sx / N, my = sy / N;
+    const double mx = sums[0] / N, my = sums[1] / N;
     out4[0] = mx;
     out4[1] = my;
-    out4[2] = sqrt(sx2 / N - mx * mx);
-    out4[3] = sqrt(sy2 / N - my * my);
+    out4[2] = sqrt(sums[2] / N - mx * mx);
+    out4[3] = sqrt(sums[3] / N - my * my);
   }
 }
 
@@ -197,13 +216,17 @@ cudaError_t slice_pair_collision(double *x1, long m1, double *x2, long m2, doubl
   return cudaGetLastError();
 }
 
+cudaError_t beam_pair_mean_rms(const double *x1, long n1, const double *x2, long n2, double *out8, cudaStream_t s) {
+  moments_pair_kernel<<<2, kMomentBlock, 0, s>>>(x1, n1, x2, n2, out8);
+  return cudaGetLastError();
+}
+
 cudaError_t soft_gaussian_4d(double *x1, long n1, double *x2, long n2, double c4_1, double c4_2, double bbscale1,
                              double bbscale2, int num_sms, cudaStream_t s) {
   double *d_m8 = nullptr;
   cudaError_t e = cudaGetSymbolAddress((void **)&d_m8, g_soft_gaussian_moments);
   if (e != cudaSuccess) return e;
-  soft_gaussian_moments_kernel<<<1, kMomentBlock, 0, s>>>(x1, n1, d_m8);
-  soft_gaussian_moments_kernel<<<1, kMomentBlock, 0, s>>>(x2, n2, d_m8 + 4);
+  moments_pair_kernel<<<2, kMomentBlock, 0, s>>>(x1, n1, x2, n2, d_m8);
   const int block = 256;
   auto grid = [&](long n) {
     long g = (n + block - 1) / block;
