@@ -543,6 +543,19 @@ int stb_bb4d_pic_device(double Np1, long n1, double *x1, double Np2, long n2, do
 int stb_bb4d_pic_host(double Np1, long n1, double *x1, double Np2, long n2, double *x2, double gamma1, double gamma2,
                       double bbscale1, double bbscale2, int device);
 
+/* Lumi_Cal_PIC_4D(Np1, Mp1, Np2, Mp2, x1, x2, Ncoll, freq),
+ * simtrack.cpp:23617-23701: both beams' charge on one 64 x 64 grid spanning
+ * their joint x-y extent widened by 4 cells per side, *lumi = Ncoll *
+ * sum(src1 src2) (Np1/Mp1) (Np2/Mp2) freq / hx / hy / 1e4, equal to the
+ * reference's bit for bit.  Beams that span no area, or hold non-finite x or
+ * y (for which the reference's grid indices are undefined), give
+ * STB_EINVAL.  Both forms return when done; the _device form reads device
+ * arrays on `stream`. */
+int stb_lumi_pic_4d_device(double Np1, long Mp1, double Np2, long Mp2, const double *x1, const double *x2, int Ncoll,
+                           double freq, int device, void *stream, double *lumi);
+int stb_lumi_pic_4d_host(double Np1, long Mp1, double Np2, long Mp2, const double *x1, const double *x2, int Ncoll,
+                         double freq, int device, double *lumi);
+
 /* Strong-strong beam-beam, sliced soft-Gaussian 6D: BeamBeam6D_SoftGaussian(
  * Np1, Mp1, x1, Np2, Mp2, x2, gamma1, gamma2, bbscale1, bbscale2, Nslice1,
  * Nslice2), simtrack.cpp:22874-23132 (simtrack.h:1406).  Both AoS bunches are

@@ -499,6 +499,11 @@ void ref_bb4d_pic(double Np1, int n1, double *x1, double Np2, int n2, double *x2
   BeamBeam4D_PIC(Np1, n1, x1, Np2, n2, x2, gamma1, gamma2, bbscale1, bbscale2);
 }
 
+// Lumi_Cal_PIC_4D (simtrack.cpp:23617).
+double ref_lumi_pic_4d(double Np1, int n1, double Np2, int n2, double *x1, double *x2, int ncoll, double freq) {
+  return Lumi_Cal_PIC_4D(Np1, n1, Np2, n2, x1, x2, ncoll, freq);
+}
+
 // FineTuneFinder, both overloads (simtrack.cpp:2288, 2321).
 double ref_fine_tune(int n, const double *x, const double *px, double lo, double hi) {
   std::vector<double> a(x, x + n);

@@ -78,6 +78,18 @@ def BeamBeam4D_PIC(Np1: float, x1: np.ndarray, Np2: float, x2: np.ndarray, gamma
                                   device))
 
 
+def Lumi_Cal_PIC_4D(Np1: float, x1: np.ndarray, Np2: float, x2: np.ndarray, Ncoll: int, freq: float,
+                    device: int = 0) -> float:
+    """Lumi_Cal_PIC_4D (simtrack.cpp:23617-23701) on the GPU: the two
+    bunches' (numpy (n, 6) float64) charge overlap on one 64 x 64 grid,
+    Ncoll collisions per turn at revolution frequency freq (cm^-2 s^-1)."""
+    b1, b2 = _bunch(x1), _bunch(x2)
+    P = lambda a: a.ctypes.data_as(POINTER(c_double))
+    out = c_double()
+    check(lib().stb_lumi_pic_4d_host(Np1, len(b1), Np2, len(b2), P(b1), P(b2), int(Ncoll), freq, device, byref(out)))
+    return out.value
+
+
 def BeamBeam6D_SoftGaussian(Np1: float, x1: np.ndarray, Np2: float, x2: np.ndarray, gamma1: float, gamma2: float,
                             bbscale1: float, bbscale2: float, Nslice1: int, Nslice2: int, zb1=None, zb2=None,
                             device: int = 0) -> None:

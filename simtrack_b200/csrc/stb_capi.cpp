@@ -1254,6 +1254,42 @@ int stb_bb4d_pic_host(double Np1, long n1, double *x1, double Np2, long n2, doub
   });
 }
 
+int stb_lumi_pic_4d_device(double Np1, long Mp1, double Np2, long Mp2, const double *x1, const double *x2, int Ncoll,
+                           double freq, int device, void *stream, double *lumi) {
+  return guarded([&] {
+    if (!x1 || !x2 || !lumi) throw Error(STB_EINVAL, "NULL argument");
+    if (Mp1 < 1 || Mp2 < 1 || Mp1 > INT32_MAX / 9 || Mp2 > INT32_MAX / 9)
+      throw Error(STB_EINVAL, "macro-particle counts must be 1 .. INT32_MAX / 9");
+    DeviceGuard g(device);
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    const cudaError_t e = lumi_pic_4d(Np1, Mp1, Np2, Mp2, x1, x2, Ncoll, freq, sms, (cudaStream_t)stream, lumi);
+    if (e == cudaErrorInvalidValue)
+      throw Error(STB_EINVAL, "the beams span no area (zero or non-finite extent) or hold non-finite coordinates");
+    cuda_check(e, "PIC luminosity");
+    return STB_OK;
+  });
+}
+
+int stb_lumi_pic_4d_host(double Np1, long Mp1, double Np2, long Mp2, const double *x1, const double *x2, int Ncoll,
+                         double freq, int device, double *lumi) {
+  return guarded([&] {
+    if (!x1 || !x2 || !lumi) throw Error(STB_EINVAL, "NULL argument");
+    if (Mp1 < 1 || Mp2 < 1 || Mp1 > INT32_MAX / 9 || Mp2 > INT32_MAX / 9)
+      throw Error(STB_EINVAL, "macro-particle counts must be 1 .. INT32_MAX / 9");
+    DeviceGuard g(device);
+    double *d = nullptr;
+    const size_t b1 = sizeof(double) * 6 * (size_t)Mp1, b2 = sizeof(double) * 6 * (size_t)Mp2;
+    cuda_check(cudaMalloc(&d, b1 + b2), "cudaMalloc(beams)");
+    DevFree f{d};
+    cuda_check(cudaMemcpy(d, x1, b1, cudaMemcpyHostToDevice), "upload beam 1");
+    cuda_check(cudaMemcpy(d + 6 * Mp1, x2, b2, cudaMemcpyHostToDevice), "upload beam 2");
+    int rc = stb_lumi_pic_4d_device(Np1, Mp1, Np2, Mp2, d, d + 6 * Mp1, Ncoll, freq, device, nullptr, lumi);
+    if (rc != STB_OK) throw Error(rc, last_error());
+    return STB_OK;
+  });
+}
+
 int stb_bb4d_soft_gaussian_device(double Np1, long n1, double *x1, double Np2, long n2, double *x2, double gamma1,
                                   double gamma2, double bbscale1, double bbscale2, int device, void *stream) {
   return guarded([&] {

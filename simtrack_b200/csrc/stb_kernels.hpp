@@ -118,6 +118,12 @@ cudaError_t beam_pair_mean_rms(const double *x1, long n1, const double *x2, long
 cudaError_t pic_4d(double Np1, long Mp1, double *x1, double Np2, long Mp2, double *x2, double gamma1, double gamma2,
                    double bbscale1, double bbscale2, int num_sms, cudaStream_t s);
 
+// Lumi_Cal_PIC_4D (simtrack.cpp:23617-23701) of two device AoS beams
+// (synchronises `s`).  cudaErrorInvalidValue for a grid of zero or
+// non-finite width.
+cudaError_t lumi_pic_4d(double Np1, long Mp1, double Np2, long Mp2, const double *x1, const double *x2, int Ncoll,
+                        double freq, int num_sms, cudaStream_t s, double *lumi_out);
+
 size_t track_smem_bytes(int nelem, int npool_padded);
 // The loss-test mode of a launch with circular aperture r2 (+inf: none) on a
 // table whose loss-checked elements have min(RN(APx^2), RN(APy^2)) >= min_ap2.

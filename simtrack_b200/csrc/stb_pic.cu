@@ -91,8 +91,9 @@ struct GridFrame {
 };
 
 // Nine (cell, weight) items per particle of the depositing beam, in the
-// reference's (i, j) order; a particle outside the cut emits kNoCell.
-__global__ void deposit_items_kernel(const double *x, long n, GridFrame g, uint32_t *keys, double *vals,
+// reference's (i, j) order; with `cut`, a particle outside the cut emits
+// kNoCell.
+__global__ void deposit_items_kernel(const double *x, long n, GridFrame g, bool cut, uint32_t *keys, double *vals,
                                      int *err) {
   for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long)gridDim.x * blockDim.x) {
     const double xp = x[6 * p], yp = x[6 * p + 2];
@@ -100,7 +101,11 @@ __global__ void deposit_items_kernel(const double *x, long n, GridFrame g, uint3
     double *v = vals + 9 * p;
     int xm[3], ym[3];
     double xw[3], yw[3];
-    bool ok = in_cut(xp, yp, g.mx, g.my, g.hx, g.hy);
+    bool ok = !cut || in_cut(xp, yp, g.mx, g.my, g.hx, g.hy);
+    if (ok && !cut && !(isfinite(xp) && isfinite(yp))) {  // no cut to exclude it: no cell either
+      atomicExch(err, 1);
+      ok = false;
+    }
     if (ok) {
       grid_weight_1d(xp - g.x0, g.hx, xm, xw);
       grid_weight_1d(yp - g.y0, g.hy, ym, yw);
@@ -249,6 +254,67 @@ __global__ void pic_kick_kernel(double *x, long n, GridFrame g, double xoffset, 
     q[1] = q[1] + ex * 1.60217662e-19 * bbscale / (gamma * 938.27201e6) * np_per_mp;
     q[3] = q[3] + ey * 1.60217662e-19 * bbscale / (gamma * 938.27201e6) * np_per_mp;
   }
+}
+
+// src[c] = 0 + w_1 + w_2 + ... for the 64 x 64 grid alone (Charge2Grid's
+// array).
+__global__ void cell_sum_kernel(const double *vals, const int *start, const int *end, double *src) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= kCells) return;
+  double s = 0.;
+  for (int q = start[c]; q < end[c]; q++) s = s + vals[q];
+  src[c] = s;
+}
+
+// Lumi_Cal_PIC_4D's grid extent (simtrack.cpp:23639-23652): min and max of
+// x and y over both beams, starting from 1000 and -1000 as the reference
+// does.  Exact in any order; one CTA, out4 = xmin, xmax, ymin, ymax.
+constexpr int kExtentBlock = 1024;
+__global__ void __launch_bounds__(kExtentBlock) extent_kernel(const double *x1, long n1, const double *x2, long n2,
+                                                              double *out4) {
+  __shared__ double red[4][kExtentBlock / 32];
+  double v[4] = {1000., -1000., 1000., -1000.};
+  for (int b = 0; b < 2; b++) {
+    const double *x = b == 0 ? x1 : x2;
+    const long n = b == 0 ? n1 : n2;
+    for (long i = threadIdx.x; i < n; i += kExtentBlock) {
+      const double a = x[6 * i], c = x[6 * i + 2];
+      if (a < v[0]) v[0] = a;
+      if (a > v[1]) v[1] = a;
+      if (c < v[2]) v[2] = c;
+      if (c > v[3]) v[3] = c;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    const double a0 = __shfl_down_sync(0xffffffffu, v[0], o), a1 = __shfl_down_sync(0xffffffffu, v[1], o);
+    const double a2 = __shfl_down_sync(0xffffffffu, v[2], o), a3 = __shfl_down_sync(0xffffffffu, v[3], o);
+    if (a0 < v[0]) v[0] = a0;
+    if (a1 > v[1]) v[1] = a1;
+    if (a2 < v[2]) v[2] = a2;
+    if (a3 > v[3]) v[3] = a3;
+  }
+  const int w = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0)
+    for (int k = 0; k < 4; k++) red[k][w] = v[k];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < 4; k++) v[k] = red[k][0];
+    for (int q = 1; q < kExtentBlock / 32; q++) {
+      if (red[0][q] < v[0]) v[0] = red[0][q];
+      if (red[1][q] > v[1]) v[1] = red[1][q];
+      if (red[2][q] < v[2]) v[2] = red[2][q];
+      if (red[3][q] > v[3]) v[3] = red[3][q];
+    }
+    for (int k = 0; k < 4; k++) out4[k] = v[k];
+  }
+}
+
+// The overlap sum of Lumi_Cal_PIC_4D (23680-23683), in cell order.
+__global__ void overlap_sum_kernel(const double *src1, const double *src2, double *out) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double l = 0;
+  for (int i = 0; i < kCells; i++) l = l + src1[i] * src2[i];
+  *out = l;
 }
 
 // The butterfly twiddles of FFT1D for n = 2^m in direction dir, from the
@@ -420,7 +486,7 @@ cudaError_t pic_4d(double Np1, long Mp1, double *x1, double Np2, long Mp2, doubl
       const long ns = d == 0 ? Mp1 : Mp2, nt = d == 0 ? Mp2 : Mp1;
       const double np_per_mp = (d == 0 ? Np1 : Np2) / (double)(int)ns;
       const GridFrame gs{ms[0], ms[1], ms[0] - kNx * hx / 2, ms[1] - kNy * hy / 2, hx, hy};
-      deposit_items_kernel<<<grid_of(ns), 256, 0, s>>>(xs, ns, gs, keys_in, vals_in, err);
+      deposit_items_kernel<<<grid_of(ns), 256, 0, s>>>(xs, ns, gs, true, keys_in, vals_in, err);
       if ((e = cub::DeviceRadixSort::SortPairs(sort_tmp, sort_bytes, keys_in, keys_out, vals_in, vals_out,
                                                (int)(9 * ns), 0, kKeyBits, s)) != cudaSuccess)
         break;
@@ -446,6 +512,73 @@ cudaError_t pic_4d(double Np1, long Mp1, double *x1, double Np2, long Mp2, doubl
   cudaStreamSynchronize(s);
   cudaFree(buf);
   if (e == cudaSuccess && h_err) e = cudaErrorInvalidValue;
+  return e;
+}
+
+cudaError_t lumi_pic_4d(double Np1, long Mp1, double Np2, long Mp2, const double *x1, const double *x2, int Ncoll,
+                        double freq, int num_sms, cudaStream_t s, double *lumi_out) {
+  const long nmax = std::max(Mp1, Mp2), nitem = 9 * nmax;
+  size_t sort_bytes = 0;
+  cudaError_t e = cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, (const uint32_t *)nullptr, (uint32_t *)nullptr,
+                                                  (const double *)nullptr, (double *)nullptr, (int)nitem, 0, kKeyBits,
+                                                  s);
+  if (e != cudaSuccess) return e;
+  // doubles: src1, src2, extent, overlap, items; then keys, bounds, flag, sort scratch
+  const size_t nd = 2 * kCells + 8 + 2 * (size_t)nitem;
+  const size_t bytes = sizeof(double) * nd + sizeof(uint32_t) * 2 * (size_t)nitem + sizeof(int) * (2 * kCells + 2) +
+                       sort_bytes + 256;
+  unsigned char *buf = nullptr;
+  if ((e = cudaMalloc(&buf, bytes)) != cudaSuccess) return e;
+  double *src1 = reinterpret_cast<double *>(buf), *src2 = src1 + kCells, *ext = src2 + kCells, *ov = ext + 4;
+  double *vals_in = ext + 8, *vals_out = vals_in + nitem;
+  uint32_t *keys_in = reinterpret_cast<uint32_t *>(vals_out + nitem), *keys_out = keys_in + nitem;
+  int *cstart = reinterpret_cast<int *>(keys_out + nitem), *cend = cstart + kCells, *err = cend + kCells;
+  void *sort_tmp = reinterpret_cast<void *>(((uintptr_t)(err + 2) + 255) & ~(uintptr_t)255);
+  auto grid_of = [&](long n) {
+    const long g = (n + 255) / 256, cap = (long)num_sms * 8;
+    return (unsigned)(g < 1 ? 1 : g > cap ? cap : g);
+  };
+  double h_ext[4] = {0, 0, 0, 0}, h_ov = 0;
+  int h_err = 0;
+  bool degenerate = false;
+  do {
+    if ((e = cudaMemsetAsync(err, 0, sizeof(int), s)) != cudaSuccess) break;
+    extent_kernel<<<1, kExtentBlock, 0, s>>>(x1, Mp1, x2, Mp2, ext);
+    if ((e = cudaMemcpyAsync(h_ext, ext, sizeof(h_ext), cudaMemcpyDeviceToHost, s)) != cudaSuccess) break;
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) break;
+    const double xmin = h_ext[0], xmax = h_ext[1], ymin = h_ext[2], ymax = h_ext[3];
+    // the reference's grid: 64 cells over the extent, widened by 4 of them on each side
+    double hx = (xmax - xmin) / kNx, hy = (ymax - ymin) / kNy;
+    const double x0 = xmin - 4 * hx, y0 = ymin - 4 * hy;
+    hx = (xmax - xmin + 8 * hx) / kNx;
+    hy = (ymax - ymin + 8 * hy) / kNy;
+    if (!(hx > 0) || !(hy > 0) || !std::isfinite(hx) || !std::isfinite(hy)) {
+      degenerate = true;
+      break;
+    }
+    const GridFrame g{0., 0., x0, y0, hx, hy};
+    for (int b = 0; b < 2 && e == cudaSuccess; b++) {
+      const double *x = b == 0 ? x1 : x2;
+      const long n = b == 0 ? Mp1 : Mp2;
+      deposit_items_kernel<<<grid_of(n), 256, 0, s>>>(x, n, g, false, keys_in, vals_in, err);
+      if ((e = cub::DeviceRadixSort::SortPairs(sort_tmp, sort_bytes, keys_in, keys_out, vals_in, vals_out,
+                                               (int)(9 * n), 0, kKeyBits, s)) != cudaSuccess)
+        break;
+      if ((e = cudaMemsetAsync(cstart, 0, sizeof(int) * 2 * kCells, s)) != cudaSuccess) break;
+      cell_bounds_kernel<<<grid_of(9 * n), 256, 0, s>>>(keys_out, 9 * n, cstart, cend);
+      cell_sum_kernel<<<kCells / 128, 128, 0, s>>>(vals_out, cstart, cend, b == 0 ? src1 : src2);
+      e = cudaGetLastError();
+    }
+    if (e != cudaSuccess) break;
+    overlap_sum_kernel<<<1, 32, 0, s>>>(src1, src2, ov);
+    if ((e = cudaMemcpyAsync(&h_ov, ov, sizeof(double), cudaMemcpyDeviceToHost, s)) != cudaSuccess) break;
+    if ((e = cudaMemcpyAsync(&h_err, err, sizeof(int), cudaMemcpyDeviceToHost, s)) != cudaSuccess) break;
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) break;
+    *lumi_out = Ncoll * h_ov * (Np1 / (int)Mp1) * (Np2 / (int)Mp2) * freq / hx / hy / 10000;
+  } while (false);
+  cudaStreamSynchronize(s);
+  cudaFree(buf);
+  if (e == cudaSuccess && (h_err || degenerate)) e = cudaErrorInvalidValue;
   return e;
 }
 

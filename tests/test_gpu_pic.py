@@ -96,3 +96,41 @@ def test_rejected_inputs():
     o1 = bad.copy()
     api.BeamBeam4D_PIC(1e11, o1, 1e11, o2, GAMMA, GAMMA, 1.0, 1.0)
     assert np.array_equal(o1, bad, equal_nan=True) and np.array_equal(o2, b2)
+
+
+LUMI_CASES = [
+    # (n1, sx1, sy1, n2, sx2, sy2, offset, Ncoll)
+    (4000, 1.2e-4, 1.2e-4, 5000, 1.2e-4, 1.2e-4, (0.0, 0.0), 1),
+    (3000, 9.5e-5, 8.5e-6, 3500, 9.5e-5, 8.5e-6, (2e-5, 1e-6), 2),
+    (1, 1.0e-4, 1.0e-4, 2000, 1.0e-4, 5.0e-5, (0.0, 0.0), 1),
+    (150_000, 1.0e-4, 6.0e-5, 200_000, 1.1e-4, 5.5e-5, (3e-6, -2e-6), 3),
+]
+
+
+@pytest.mark.parametrize("case", LUMI_CASES)
+def test_lumi_pic_4d_vs_reference(case):
+    """Lumi_Cal_PIC_4D (simtrack.cpp:23617-23701): the charge overlap on the
+    beams' joint grid, bit for bit (halo particles widen the grid)."""
+    _need_ref()
+    n1, sx1, sy1, n2, sx2, sy2, (dx, dy), ncoll = case
+    b1 = _beam(n1, sx1, sy1, 0.0, 0.0, 3)
+    b2 = _beam(n2, sx2, sy2, dx, dy, 4)
+    if n2 > 100:
+        b2[5, 0] += 12 * sx2
+    P = lambda a: a.ctypes.data_as(POINTER(c_double))
+    ours = api.Lumi_Cal_PIC_4D(1.1e11, b1, 1.2e11, b2, ncoll, 78196.0)
+    ref = oracle_bridge.RefOracle()
+    theirs = ref.L.ref_lumi_pic_4d(1.1e11, n1, 1.2e11, n2, P(b1.copy()), P(b2.copy()), ncoll, 78196.0)
+    assert ours == theirs and ours > 0
+
+
+def test_lumi_rejected_inputs():
+    b = _beam(100, 1e-4, 1e-4, 0, 0, 1)
+    flat = b.copy()
+    flat[:, 2] = 0.0
+    with pytest.raises(SimTrackError):  # no extent in y
+        api.Lumi_Cal_PIC_4D(1e11, flat, 1e11, flat.copy(), 1, 1e4)
+    bad = b.copy()
+    bad[4, 2] = np.inf
+    with pytest.raises(SimTrackError):
+        api.Lumi_Cal_PIC_4D(1e11, bad, 1e11, b, 1, 1e4)
