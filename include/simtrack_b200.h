@@ -543,6 +543,31 @@ int stb_bb4d_pic_device(double Np1, long n1, double *x1, double Np2, long n2, do
 int stb_bb4d_pic_host(double Np1, long n1, double *x1, double Np2, long n2, double *x2, double gamma1, double gamma2,
                       double bbscale1, double bbscale2, int device);
 
+/* Cal_Effective_Green_Function(xoffset, yoffset, Nx, Ny, hx, hy, grn_c_r,
+ * grn_c_i), simtrack.cpp:2881-2921: the integrated Green function of the 2D
+ * Poisson equation on the doubled 2Nx x 2Ny grid, transformed by the
+ * reference's FFT2D, into host arrays of 4 Nx Ny doubles, bit for bit.  The
+ * grid must be square with Nx a power of two from 8 to 512 (STB_EINVAL
+ * otherwise; the reference's FFT2D assumes both).  Tabulated on the host,
+ * transformed on `device`. */
+int stb_pic_green_function(double xoffset, double yoffset, int Nx, int Ny, double hx, double hy, double *grn_c_r,
+                           double *grn_c_i, int device);
+
+/* BeamBeam4D_PIC_NonOffset(Np1, Mp1, xc1, Np2, Mp2, xc2, gamma1, gamma2,
+ * bbscale1, bbscale2, Nx, Ny, hx, hy, grn_c_r, grn_c_i),
+ * simtrack.cpp:24226-24280: the PIC collision on the caller's grid centred on
+ * the origin (spacing hx, hy; Green spectrum grn_c_r/grn_c_i of 4 Nx Ny from
+ * stb_pic_green_function(0, 0, ...)), particles within Nx/2 - 3 cells of the
+ * origin depositing and kicked; bit for bit.  Grids as for
+ * stb_pic_green_function.  The _host form takes host beams and Green arrays,
+ * the _device form device ones, on `stream`; both return when done. */
+int stb_bb4d_pic_nonoffset_device(double Np1, long Mp1, double *x1, double Np2, long Mp2, double *x2, double gamma1,
+                                  double gamma2, double bbscale1, double bbscale2, int Nx, int Ny, double hx,
+                                  double hy, const double *grn_c_r, const double *grn_c_i, int device, void *stream);
+int stb_bb4d_pic_nonoffset_host(double Np1, long Mp1, double *x1, double Np2, long Mp2, double *x2, double gamma1,
+                                double gamma2, double bbscale1, double bbscale2, int Nx, int Ny, double hx, double hy,
+                                const double *grn_c_r, const double *grn_c_i, int device);
+
 /* Lumi_Cal_PIC_4D(Np1, Mp1, Np2, Mp2, x1, x2, Ncoll, freq),
  * simtrack.cpp:23617-23701: both beams' charge on one 64 x 64 grid spanning
  * their joint x-y extent widened by 4 cells per side, *lumi = Ncoll *

@@ -499,6 +499,17 @@ void ref_bb4d_pic(double Np1, int n1, double *x1, double Np2, int n2, double *x2
   BeamBeam4D_PIC(Np1, n1, x1, Np2, n2, x2, gamma1, gamma2, bbscale1, bbscale2);
 }
 
+// Cal_Effective_Green_Function (simtrack.cpp:2881) and
+// BeamBeam4D_PIC_NonOffset (simtrack.cpp:24226).
+void ref_green_function(double xoffset, double yoffset, int nx, int ny, double hx, double hy, double *gr, double *gi) {
+  Cal_Effective_Green_Function(xoffset, yoffset, nx, ny, hx, hy, gr, gi);
+}
+void ref_bb4d_pic_nonoffset(double Np1, int n1, double *x1, double Np2, int n2, double *x2, double gamma1,
+                            double gamma2, double bbscale1, double bbscale2, int nx, int ny, double hx, double hy,
+                            double *gr, double *gi) {
+  BeamBeam4D_PIC_NonOffset(Np1, n1, x1, Np2, n2, x2, gamma1, gamma2, bbscale1, bbscale2, nx, ny, hx, hy, gr, gi);
+}
+
 // Lumi_Cal_PIC_4D (simtrack.cpp:23617).
 double ref_lumi_pic_4d(double Np1, int n1, double Np2, int n2, double *x1, double *x2, int ncoll, double freq) {
   return Lumi_Cal_PIC_4D(Np1, n1, Np2, n2, x1, x2, ncoll, freq);

@@ -1254,6 +1254,66 @@ int stb_bb4d_pic_host(double Np1, long n1, double *x1, double Np2, long n2, doub
   });
 }
 
+int stb_pic_green_function(double xoffset, double yoffset, int Nx, int Ny, double hx, double hy, double *grn_c_r,
+                           double *grn_c_i, int device) {
+  return guarded([&] {
+    if (!grn_c_r || !grn_c_i) throw Error(STB_EINVAL, "NULL argument");
+    if (!pic_grid_valid(Nx, Ny)) throw Error(STB_EINVAL, "the grid must be square, Nx a power of two from 8 to 512");
+    DeviceGuard g(device);
+    cuda_check(pic_green_function(xoffset, yoffset, Nx, hx, hy, grn_c_r, grn_c_i, 0), "Green function");
+    return STB_OK;
+  });
+}
+
+int stb_bb4d_pic_nonoffset_device(double Np1, long Mp1, double *x1, double Np2, long Mp2, double *x2, double gamma1,
+                                  double gamma2, double bbscale1, double bbscale2, int Nx, int Ny, double hx,
+                                  double hy, const double *grn_c_r, const double *grn_c_i, int device,
+                                  void *stream) {
+  return guarded([&] {
+    if (!x1 || !x2 || !grn_c_r || !grn_c_i) throw Error(STB_EINVAL, "NULL argument");
+    if (!pic_grid_valid(Nx, Ny)) throw Error(STB_EINVAL, "the grid must be square, Nx a power of two from 8 to 512");
+    if (Mp1 < 1 || Mp2 < 1 || Mp1 > INT32_MAX / 9 || Mp2 > INT32_MAX / 9)
+      throw Error(STB_EINVAL, "macro-particle counts must be 1 .. INT32_MAX / 9");
+    if (!(gamma1 > 0) || !(gamma2 > 0)) throw Error(STB_EINVAL, "gamma must be positive");
+    DeviceGuard g(device);
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    const cudaError_t e = pic_4d_nonoffset(Np1, Mp1, x1, Np2, Mp2, x2, gamma1, gamma2, bbscale1, bbscale2, Nx, hx,
+                                           hy, grn_c_r, grn_c_i, sms, (cudaStream_t)stream);
+    if (e == cudaErrorInvalidValue) throw Error(STB_EINVAL, "a macro-particle maps outside the grid");
+    cuda_check(e, "particle-in-cell beam-beam");
+    return STB_OK;
+  });
+}
+
+int stb_bb4d_pic_nonoffset_host(double Np1, long Mp1, double *x1, double Np2, long Mp2, double *x2, double gamma1,
+                                double gamma2, double bbscale1, double bbscale2, int Nx, int Ny, double hx, double hy,
+                                const double *grn_c_r, const double *grn_c_i, int device) {
+  return guarded([&] {
+    if (!x1 || !x2 || !grn_c_r || !grn_c_i) throw Error(STB_EINVAL, "NULL argument");
+    if (!pic_grid_valid(Nx, Ny)) throw Error(STB_EINVAL, "the grid must be square, Nx a power of two from 8 to 512");
+    if (Mp1 < 1 || Mp2 < 1 || Mp1 > INT32_MAX / 9 || Mp2 > INT32_MAX / 9)
+      throw Error(STB_EINVAL, "macro-particle counts must be 1 .. INT32_MAX / 9");
+    DeviceGuard g(device);
+    const size_t b1 = sizeof(double) * 6 * (size_t)Mp1, b2 = sizeof(double) * 6 * (size_t)Mp2;
+    const size_t bg = sizeof(double) * 4 * (size_t)Nx * Ny;
+    double *d = nullptr;
+    cuda_check(cudaMalloc(&d, b1 + b2 + 2 * bg), "cudaMalloc(beams)");
+    DevFree f{d};
+    double *d2 = d + 6 * Mp1, *gr = d2 + 6 * Mp2, *gi = gr + 4 * (size_t)Nx * Ny;
+    cuda_check(cudaMemcpy(d, x1, b1, cudaMemcpyHostToDevice), "upload beam 1");
+    cuda_check(cudaMemcpy(d2, x2, b2, cudaMemcpyHostToDevice), "upload beam 2");
+    cuda_check(cudaMemcpy(gr, grn_c_r, bg, cudaMemcpyHostToDevice), "upload Green function");
+    cuda_check(cudaMemcpy(gi, grn_c_i, bg, cudaMemcpyHostToDevice), "upload Green function");
+    int rc = stb_bb4d_pic_nonoffset_device(Np1, Mp1, d, Np2, Mp2, d2, gamma1, gamma2, bbscale1, bbscale2, Nx, Ny,
+                                           hx, hy, gr, gi, device, nullptr);
+    if (rc != STB_OK) throw Error(rc, last_error());
+    cuda_check(cudaMemcpy(x1, d, b1, cudaMemcpyDeviceToHost), "download beam 1");
+    cuda_check(cudaMemcpy(x2, d2, b2, cudaMemcpyDeviceToHost), "download beam 2");
+    return STB_OK;
+  });
+}
+
 int stb_lumi_pic_4d_device(double Np1, long Mp1, double Np2, long Mp2, const double *x1, const double *x2, int Ncoll,
                            double freq, int device, void *stream, double *lumi) {
   return guarded([&] {

@@ -118,6 +118,18 @@ cudaError_t beam_pair_mean_rms(const double *x1, long n1, const double *x2, long
 cudaError_t pic_4d(double Np1, long Mp1, double *x1, double Np2, long Mp2, double *x2, double gamma1, double gamma2,
                    double bbscale1, double bbscale2, int num_sms, cudaStream_t s);
 
+// A grid the PIC functions take: nx == ny, a power of two from 8 to 512.
+bool pic_grid_valid(int nx, int ny);
+// BeamBeam4D_PIC_NonOffset (simtrack.cpp:24226-24280) on device AoS beams
+// with the caller's nx x nx grid (nx a power of two, 8 .. 512), spacing and
+// Green spectrum (device arrays of 4 nx^2); synchronises `s`.
+cudaError_t pic_4d_nonoffset(double Np1, long Mp1, double *x1, double Np2, long Mp2, double *x2, double gamma1,
+                             double gamma2, double bbscale1, double bbscale2, int nx, double hx, double hy,
+                             const double *grn_re, const double *grn_im, int num_sms, cudaStream_t s);
+// Cal_Effective_Green_Function (simtrack.cpp:2881-2921) into host arrays of
+// 4 nx^2 (nx a power of two, 8 .. 512); synchronises `s`.
+cudaError_t pic_green_function(double xoffset, double yoffset, int nx, double hx, double hy, double *grn_re,
+                               double *grn_im, cudaStream_t s);
 // Lumi_Cal_PIC_4D (simtrack.cpp:23617-23701) of two device AoS beams
 // (synchronises `s`).  cudaErrorInvalidValue for a grid of zero or
 // non-finite width.

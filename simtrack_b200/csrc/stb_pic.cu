@@ -41,16 +41,21 @@
 namespace stb {
 namespace {
 
-constexpr int kNx = 64, kNy = 64;           // grid (Nx, Ny in the reference)
-constexpr int kNsigma = 15;                 // grid width in rms sizes
-constexpr int kN2 = 2 * kNx;                // doubled grid, 128 x 128
-constexpr int kLog2N2 = 7;
-constexpr int kCells = kNx * kNy;
-constexpr uint32_t kNoCell = kCells;        // key of a particle outside the cut
-constexpr int kKeyBits = 13;                // keys 0 .. kCells
+// Grids are square, nx x nx cells with nx a power of two (the reference
+// indexes both axes with Nx as the row length, and its FFT2D takes powers of
+// two); the doubled grid of the convolution is 2nx x 2nx.  BeamBeam4D_PIC and
+// Lumi_Cal_PIC_4D use nx = 64 (Nx = Ny = 64 in the reference).
+constexpr int kPicNx = 64;
+constexpr int kMinLog2N2 = 4, kMaxLog2N2 = 10;  // nx from 8 to 512
+constexpr int kNsigma = 15;                     // grid width in rms sizes
 constexpr double kEps0 = 8.854187817e-12;
 
-static_assert(kNx == kNy, "the reference indexes its grids with Nx as the row length of both axes");
+// Radix-sort key bits for the cell keys 0 .. ncell (ncell: outside the cut).
+int key_bits(int ncell) {
+  int b = 1;
+  while ((1u << b) <= (unsigned)ncell) b++;
+  return b;
+}
 
 // Cal_Grid_Weight (simtrack.cpp:2747-2791): the three mesh lines nearest the
 // point and their weights along one axis.
@@ -79,20 +84,21 @@ __device__ __forceinline__ bool mesh_ok(const int m[3], int n) {
   return m[0] >= 0 && m[0] < n && m[1] >= 0 && m[1] < n && m[2] >= 0 && m[2] < n;
 }
 
-// The cut of Charge2Grid's and the kick's callers: |x - mean| < (Nx/2 - 3) hx.
-__device__ __forceinline__ bool in_cut(double xp, double yp, double mx, double my, double hx, double hy) {
-  return fabs(xp - mx) < (kNx / 2 - 3) * hx && fabs(yp - my) < (kNy / 2 - 3) * hy;
-}
-
 struct GridFrame {
-  double mx, my;  // mean of the beam whose particles pass the cut
+  double mx, my;  // centre of the cut (the beam's mean, or 0)
   double x0, y0;  // grid origin
   double hx, hy;
+  int nx;         // cells per side
 };
+
+// The cut of Charge2Grid's and the kick's callers: |x - mx| < (Nx/2 - 3) hx.
+__device__ __forceinline__ bool in_cut(double xp, double yp, const GridFrame &g) {
+  return fabs(xp - g.mx) < (g.nx / 2 - 3) * g.hx && fabs(yp - g.my) < (g.nx / 2 - 3) * g.hy;
+}
 
 // Nine (cell, weight) items per particle of the depositing beam, in the
 // reference's (i, j) order; with `cut`, a particle outside the cut emits
-// kNoCell.
+// the key nx * nx (after every cell).
 __global__ void deposit_items_kernel(const double *x, long n, GridFrame g, bool cut, uint32_t *keys, double *vals,
                                      int *err) {
   for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long)gridDim.x * blockDim.x) {
@@ -101,7 +107,7 @@ __global__ void deposit_items_kernel(const double *x, long n, GridFrame g, bool 
     double *v = vals + 9 * p;
     int xm[3], ym[3];
     double xw[3], yw[3];
-    bool ok = !cut || in_cut(xp, yp, g.mx, g.my, g.hx, g.hy);
+    bool ok = !cut || in_cut(xp, yp, g);
     if (ok && !cut && !(isfinite(xp) && isfinite(yp))) {  // no cut to exclude it: no cell either
       atomicExch(err, 1);
       ok = false;
@@ -109,24 +115,24 @@ __global__ void deposit_items_kernel(const double *x, long n, GridFrame g, bool 
     if (ok) {
       grid_weight_1d(xp - g.x0, g.hx, xm, xw);
       grid_weight_1d(yp - g.y0, g.hy, ym, yw);
-      if (!mesh_ok(xm, kNx) || !mesh_ok(ym, kNy)) {
+      if (!mesh_ok(xm, g.nx) || !mesh_ok(ym, g.nx)) {
         atomicExch(err, 1);
         ok = false;
       }
     }
     for (int i = 0; i < 3; i++)
       for (int j = 0; j < 3; j++) {
-        k[3 * i + j] = ok ? (uint32_t)(xm[i] * kNx + ym[j]) : kNoCell;
+        k[3 * i + j] = ok ? (uint32_t)(xm[i] * g.nx + ym[j]) : (uint32_t)(g.nx * g.nx);
         v[3 * i + j] = ok ? xw[i] * yw[j] : 0.0;
       }
   }
 }
 
 // First and one-past-last item of every cell in the sorted keys.
-__global__ void cell_bounds_kernel(const uint32_t *keys, long m, int *start, int *end) {
+__global__ void cell_bounds_kernel(const uint32_t *keys, long m, int ncell, int *start, int *end) {
   for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (long)gridDim.x * blockDim.x) {
     const uint32_t k = keys[i];
-    if (k >= kNoCell) continue;
+    if (k >= (uint32_t)ncell) continue;
     if (i == 0 || keys[i - 1] != k) start[k] = (int)i;
     if (i == m - 1 || keys[i + 1] != k) end[k] = (int)(i + 1);
   }
@@ -135,35 +141,39 @@ __global__ void cell_bounds_kernel(const uint32_t *keys, long m, int *start, int
 // src[c] = 0 + w_1 + w_2 + ... over the cell's items in particle order,
 // written straight into the zero-padded real part of the doubled grid
 // (Cal_Potential_Convolution's src_c_r); the rest of both parts is zero.
-__global__ void cell_sum_pad_kernel(const double *vals, const int *start, const int *end, double *re, double *im) {
+__global__ void cell_sum_pad_kernel(const double *vals, const int *start, const int *end, double *re, double *im,
+                                    int nx) {
+  const int n2 = 2 * nx;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= kN2 * kN2) return;
-  const int i = t / kN2, j = t % kN2;
+  if (t >= n2 * n2) return;
+  const int i = t / n2, j = t % n2;
   double s = 0.;
-  if (i < kNx && j < kNy) {
-    const int c = i * kNx + j;
+  if (i < nx && j < nx) {
+    const int c = i * nx + j;
     for (int q = start[c]; q < end[c]; q++) s = s + vals[q];
   }
   re[t] = s;
   im[t] = 0.;
 }
 
-// One FFT1D (simtrack.cpp:2583-2647) per block over n = 128 points: line b
+// One FFT1D (simtrack.cpp:2583-2647) per block over n = 2^LOG2N points: line b
 // holds the elements base + t * es, base = b * ls.  tw holds the butterfly
 // twiddles (u1, u2) of every stage, stage l's l1 = 2^l values from offset
 // l1 - 1, as the reference's recurrence produces them for this direction.
 // dir == 1 divides by n, as the reference's forward transform does.
-__global__ void __launch_bounds__(kN2 / 2) fft_lines_kernel(double *re, double *im, int ls, int es,
-                                                           const double2 *tw, int dir) {
-  __shared__ double sr[kN2], si[kN2];
+template <int LOG2N>
+__global__ void __launch_bounds__((1 << LOG2N) / 2) fft_lines_kernel(double *re, double *im, int ls, int es,
+                                                                    const double2 *tw, int dir) {
+  constexpr int N = 1 << LOG2N;
+  __shared__ double sr[N], si[N];
   const int base = blockIdx.x * ls;
-  for (int t = threadIdx.x; t < kN2; t += blockDim.x) {
-    const int r = (int)(__brev((unsigned)t) >> (32 - kLog2N2));
+  for (int t = threadIdx.x; t < N; t += blockDim.x) {
+    const int r = (int)(__brev((unsigned)t) >> (32 - LOG2N));
     sr[r] = re[base + t * es];
     si[r] = im[base + t * es];
   }
   const int b = threadIdx.x;
-  for (int l = 0; l < kLog2N2; l++) {
+  for (int l = 0; l < LOG2N; l++) {
     __syncthreads();
     const int l1 = 1 << l;
     const int j = b & (l1 - 1);
@@ -177,27 +187,41 @@ __global__ void __launch_bounds__(kN2 / 2) fft_lines_kernel(double *re, double *
     si[i] += t2;
   }
   __syncthreads();
-  for (int t = threadIdx.x; t < kN2; t += blockDim.x) {
+  for (int t = threadIdx.x; t < N; t += blockDim.x) {
     double a = sr[t], c = si[t];
     if (dir == 1) {
-      a /= (double)kN2;
-      c /= (double)kN2;
+      a /= (double)N;
+      c /= (double)N;
     }
     re[base + t * es] = a;
     im[base + t * es] = c;
   }
 }
 
-// FFT2D (simtrack.cpp:2649-2695): the columns x[i*n + j] over i, then the rows.
-void fft2d(double *re, double *im, const double2 *tw, int dir, cudaStream_t s) {
-  fft_lines_kernel<<<kN2, kN2 / 2, 0, s>>>(re, im, 1, kN2, tw, dir);
-  fft_lines_kernel<<<kN2, kN2 / 2, 0, s>>>(re, im, kN2, 1, tw, dir);
+// FFT2D (simtrack.cpp:2649-2695) of an n x n array, n = 2^log2n: the
+// columns x[i*n + j] over i, then the rows.
+template <int LOG2N>
+void fft2d_n(double *re, double *im, const double2 *tw, int dir, cudaStream_t s) {
+  constexpr int N = 1 << LOG2N;
+  fft_lines_kernel<LOG2N><<<N, N / 2, 0, s>>>(re, im, 1, N, tw, dir);
+  fft_lines_kernel<LOG2N><<<N, N / 2, 0, s>>>(re, im, N, 1, tw, dir);
+}
+void fft2d(double *re, double *im, const double2 *tw, int dir, int log2n, cudaStream_t s) {
+  switch (log2n) {
+    case 4: return fft2d_n<4>(re, im, tw, dir, s);
+    case 5: return fft2d_n<5>(re, im, tw, dir, s);
+    case 6: return fft2d_n<6>(re, im, tw, dir, s);
+    case 7: return fft2d_n<7>(re, im, tw, dir, s);
+    case 8: return fft2d_n<8>(re, im, tw, dir, s);
+    case 9: return fft2d_n<9>(re, im, tw, dir, s);
+    default: return fft2d_n<10>(re, im, tw, dir, s);
+  }
 }
 
 // The spectrum product of Cal_Potential_Convolution, in place into (re, im).
-__global__ void spectrum_product_kernel(double *re, double *im, const double *gr, const double *gi) {
+__global__ void spectrum_product_kernel(double *re, double *im, const double *gr, const double *gi, int total) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= kN2 * kN2) return;
+  if (t >= total) return;
   const double a = re[t], b = im[t], c = gr[t], d = gi[t];
   re[t] = a * c - b * d;
   im[t] = a * d + b * c;
@@ -206,21 +230,26 @@ __global__ void spectrum_product_kernel(double *re, double *im, const double *gr
 // phi from the inverse transform, then Cal_Electric_Field's stencil
 // (zero on the grid's border).  One thread per cell; phi is re-derived by
 // each neighbour with the same expression, so every value is the reference's.
-__device__ __forceinline__ double phi_at(const double *re, int i, int j) {
-  return re[i * kN2 + j] * 2 * kNx * 2 * kNy / 2 / 3.14159265 / kEps0;
+__device__ __forceinline__ double phi_at(const double *re, int i, int j, int nx) {
+  return re[i * 2 * nx + j] * 2 * nx * 2 * nx / 2 / 3.14159265 / kEps0;
 }
 
-__global__ void field_kernel(const double *re, double hx, double hy, double *Ex, double *Ey) {
+// Interpolate_Electric_Field_1Potential (3047-3094) differences the same
+// potential values with the same stencil around the particle, so this field
+// serves both interpolations bit for bit.
+__global__ void field_kernel(const double *re, double hx, double hy, double *Ex, double *Ey, int nx) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= kCells) return;
-  const int i = t / kNx, j = t % kNx;
+  if (t >= nx * nx) return;
+  const int i = t / nx, j = t % nx;
   double ex = 0., ey = 0.;
-  if (i >= 1 && i < kNx - 1 && j >= 1 && j < kNy - 1) {
-    ex = -((phi_at(re, i + 1, j + 1) - phi_at(re, i - 1, j + 1)) + 4 * (phi_at(re, i + 1, j) - phi_at(re, i - 1, j)) +
-           (phi_at(re, i + 1, j - 1) - phi_at(re, i - 1, j - 1))) /
+  if (i >= 1 && i < nx - 1 && j >= 1 && j < nx - 1) {
+    ex = -((phi_at(re, i + 1, j + 1, nx) - phi_at(re, i - 1, j + 1, nx)) +
+           4 * (phi_at(re, i + 1, j, nx) - phi_at(re, i - 1, j, nx)) +
+           (phi_at(re, i + 1, j - 1, nx) - phi_at(re, i - 1, j - 1, nx))) /
          12. / hx;
-    ey = -((phi_at(re, i + 1, j + 1) - phi_at(re, i + 1, j - 1)) + 4 * (phi_at(re, i, j + 1) - phi_at(re, i, j - 1)) +
-           (phi_at(re, i - 1, j + 1) - phi_at(re, i - 1, j - 1))) /
+    ey = -((phi_at(re, i + 1, j + 1, nx) - phi_at(re, i + 1, j - 1, nx)) +
+           4 * (phi_at(re, i, j + 1, nx) - phi_at(re, i, j - 1, nx)) +
+           (phi_at(re, i - 1, j + 1, nx) - phi_at(re, i - 1, j - 1, nx))) /
          12. / hy;
   }
   Ex[t] = ex;
@@ -235,21 +264,21 @@ __global__ void pic_kick_kernel(double *x, long n, GridFrame g, double xoffset, 
   for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long)gridDim.x * blockDim.x) {
     double *q = x + 6 * p;
     const double xp = q[0], yp = q[2];
-    if (!in_cut(xp, yp, g.mx, g.my, g.hx, g.hy)) continue;
+    if (!in_cut(xp, yp, g)) continue;
     const double xs = xp - xoffset, ys = yp - yoffset;
     int xm[3], ym[3];
     double xw[3], yw[3];
     grid_weight_1d(xs - g.x0, g.hx, xm, xw);
     grid_weight_1d(ys - g.y0, g.hy, ym, yw);
-    if (!mesh_ok(xm, kNx) || !mesh_ok(ym, kNy)) {
+    if (!mesh_ok(xm, g.nx) || !mesh_ok(ym, g.nx)) {
       atomicExch(err, 1);
       continue;
     }
     double ex = 0., ey = 0.;
     for (int i = 0; i < 3; i++)
       for (int j = 0; j < 3; j++) {
-        ex = ex + Ex[xm[i] * kNx + ym[j]] * xw[i] * yw[j];
-        ey = ey + Ey[xm[i] * kNx + ym[j]] * xw[i] * yw[j];
+        ex = ex + Ex[xm[i] * g.nx + ym[j]] * xw[i] * yw[j];
+        ey = ey + Ey[xm[i] * g.nx + ym[j]] * xw[i] * yw[j];
       }
     q[1] = q[1] + ex * 1.60217662e-19 * bbscale / (gamma * 938.27201e6) * np_per_mp;
     q[3] = q[3] + ey * 1.60217662e-19 * bbscale / (gamma * 938.27201e6) * np_per_mp;
@@ -258,9 +287,9 @@ __global__ void pic_kick_kernel(double *x, long n, GridFrame g, double xoffset, 
 
 // src[c] = 0 + w_1 + w_2 + ... for the 64 x 64 grid alone (Charge2Grid's
 // array).
-__global__ void cell_sum_kernel(const double *vals, const int *start, const int *end, double *src) {
+__global__ void cell_sum_kernel(const double *vals, const int *start, const int *end, double *src, int ncell) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= kCells) return;
+  if (c >= ncell) return;
   double s = 0.;
   for (int q = start[c]; q < end[c]; q++) s = s + vals[q];
   src[c] = s;
@@ -310,10 +339,10 @@ __global__ void __launch_bounds__(kExtentBlock) extent_kernel(const double *x1, 
 }
 
 // The overlap sum of Lumi_Cal_PIC_4D (23680-23683), in cell order.
-__global__ void overlap_sum_kernel(const double *src1, const double *src2, double *out) {
+__global__ void overlap_sum_kernel(const double *src1, const double *src2, double *out, int ncell) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   double l = 0;
-  for (int i = 0; i < kCells; i++) l = l + src1[i] * src2[i];
+  for (int i = 0; i < ncell; i++) l = l + src1[i] * src2[i];
   *out = l;
 }
 
@@ -386,24 +415,25 @@ double calc_egreen(double x1, double x2, double y1, double y2, double hx, double
 }
 
 // Cal_Effective_Green_Function's tables before their transform (2881-2918)
-// for both directions: g[d][i * 2Nx + j] over the four quadrants of the
-// doubled grid, offsets (xoff[d], yoff[d]); the 2 x 128 rows are split across
-// host threads.
-void green_tables(const double xoff[2], const double yoff[2], double hx, double hy, double *const g[2]) {
+// for nd directions: g[d][i * 2nx + j] over the four quadrants of the
+// doubled grid, offsets (xoff[d], yoff[d]); the rows are split across host
+// threads.
+void green_tables(int nd, const double *xoff, const double *yoff, double hx, double hy, int nx, double *const *g) {
+  const int n2 = 2 * nx;
   auto rows = [&](int r0, int r1) {
     for (int r = r0; r < r1; r++) {
-      const int d = r / kN2, i = r % kN2;
-      for (int j = 0; j < kN2; j++) {
+      const int d = r / n2, i = r % n2;
+      for (int j = 0; j < n2; j++) {
         double x1, y1;
-        if (i <= kNx - 1) x1 = xoff[d] + i * hx - 0.5 * hx;
-        else x1 = xoff[d] - (2 * kNx - i) * hx - 0.5 * hx;
-        if (j <= kNy - 1) y1 = yoff[d] + j * hy - 0.5 * hy;
-        else y1 = yoff[d] - (2 * kNy - j) * hy - 0.5 * hy;
-        g[d][i * kN2 + j] = calc_egreen(x1, x1 + hx, y1, y1 + hy, hx, hy);
+        if (i <= nx - 1) x1 = xoff[d] + i * hx - 0.5 * hx;
+        else x1 = xoff[d] - (2 * nx - i) * hx - 0.5 * hx;
+        if (j <= nx - 1) y1 = yoff[d] + j * hy - 0.5 * hy;
+        else y1 = yoff[d] - (2 * nx - j) * hy - 0.5 * hy;
+        g[d][i * n2 + j] = calc_egreen(x1, x1 + hx, y1, y1 + hy, hx, hy);
       }
     }
   };
-  const int nrows = 2 * kN2;
+  const int nrows = nd * n2;
   const int nt = (int)std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
   std::vector<std::thread> th;
   const int per = (nrows + nt - 1) / nt;
@@ -414,171 +444,249 @@ void green_tables(const double xoff[2], const double yoff[2], double hx, double 
   for (auto &t : th) t.join();
 }
 
+int log2_of(int n) {
+  int l = 0;
+  while ((1 << l) < n) l++;
+  return l;
+}
+
+// Device scratch of one collision on an nx x nx grid with at most nmax
+// particles per beam: two Green spectra, the work grid, the field, the
+// moments, the twiddles of both directions, the (cell, weight) items, the
+// cell bounds, the error flag and the radix sort's scratch.
+struct PicScratch {
+  unsigned char *buf = nullptr;
+  int nx = 0, n2 = 0, log2n2 = 0, ncell = 0, kbits = 0;
+  size_t grid2 = 0, sort_bytes = 0;
+  long nitem = 0;
+  double *g_re[2] = {nullptr, nullptr}, *g_im[2] = {nullptr, nullptr};
+  double *wr = nullptr, *wi = nullptr, *Ex = nullptr, *Ey = nullptr, *m8 = nullptr;
+  double2 *tw_fwd = nullptr, *tw_inv = nullptr;
+  double *vals_in = nullptr, *vals_out = nullptr;
+  uint32_t *keys_in = nullptr, *keys_out = nullptr;
+  int *cstart = nullptr, *cend = nullptr, *err = nullptr;
+  void *sort_tmp = nullptr;
+  std::vector<double2> twf, twi;
+
+  ~PicScratch() {
+    if (buf) cudaFree(buf);
+  }
+  cudaError_t init(int nx_, long nmax, cudaStream_t s) {
+    nx = nx_;
+    n2 = 2 * nx;
+    log2n2 = log2_of(n2);
+    ncell = nx * nx;
+    kbits = key_bits(ncell);
+    grid2 = (size_t)n2 * n2;
+    nitem = 9 * nmax;
+    cudaError_t e = cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, (const uint32_t *)nullptr,
+                                                    (uint32_t *)nullptr, (const double *)nullptr, (double *)nullptr,
+                                                    (int)nitem, 0, kbits, s);
+    if (e != cudaSuccess) return e;
+    const int ntw = n2 - 1;
+    const size_t nd = 6 * grid2 + 2 * (size_t)ncell + 8 + 4 * (size_t)ntw + 2 * (size_t)nitem;
+    const size_t bytes = sizeof(double) * nd + sizeof(uint32_t) * 2 * (size_t)nitem +
+                         sizeof(int) * (2 * (size_t)ncell + 2) + sort_bytes + 256;
+    if ((e = cudaMalloc(&buf, bytes)) != cudaSuccess) return e;
+    g_re[0] = reinterpret_cast<double *>(buf);
+    g_im[0] = g_re[0] + grid2;
+    g_re[1] = g_im[0] + grid2;
+    g_im[1] = g_re[1] + grid2;
+    wr = g_im[1] + grid2;
+    wi = wr + grid2;
+    Ex = wi + grid2;
+    Ey = Ex + ncell;
+    m8 = Ey + ncell;
+    tw_fwd = reinterpret_cast<double2 *>(m8 + 8);
+    tw_inv = tw_fwd + ntw;
+    vals_in = reinterpret_cast<double *>(tw_inv + ntw);
+    vals_out = vals_in + nitem;
+    keys_in = reinterpret_cast<uint32_t *>(vals_out + nitem);
+    keys_out = keys_in + nitem;
+    cstart = reinterpret_cast<int *>(keys_out + nitem);
+    cend = cstart + ncell;
+    err = cend + ncell;
+    sort_tmp = reinterpret_cast<void *>(((uintptr_t)(err + 2) + 255) & ~(uintptr_t)255);
+    twf = fft_twiddles(log2n2, 1);
+    twi = fft_twiddles(log2n2, -1);
+    if ((e = cudaMemcpyAsync(tw_fwd, twf.data(), sizeof(double2) * ntw, cudaMemcpyHostToDevice, s)) != cudaSuccess)
+      return e;
+    if ((e = cudaMemcpyAsync(tw_inv, twi.data(), sizeof(double2) * ntw, cudaMemcpyHostToDevice, s)) != cudaSuccess)
+      return e;
+    return cudaMemsetAsync(err, 0, sizeof(int), s);
+  }
+};
+
+unsigned grid_of(long n, int num_sms) {
+  const long g = (n + 255) / 256, cap = (long)num_sms * 8;
+  return (unsigned)(g < 1 ? 1 : g > cap ? cap : g);
+}
+
+// Charge2Grid over the n particles of x (with or without the cut), the
+// per-cell ordered sums into `src` (nx x nx), or, when `pad`, into the real
+// part of the zero-padded doubled grid (wr, wi).
+cudaError_t deposit(PicScratch &S, const double *x, long n, const GridFrame &g, bool cut, bool pad, double *src,
+                    int num_sms, cudaStream_t s) {
+  deposit_items_kernel<<<grid_of(n, num_sms), 256, 0, s>>>(x, n, g, cut, S.keys_in, S.vals_in, S.err);
+  cudaError_t e = cub::DeviceRadixSort::SortPairs(S.sort_tmp, S.sort_bytes, S.keys_in, S.keys_out, S.vals_in,
+                                                  S.vals_out, (int)(9 * n), 0, S.kbits, s);
+  if (e != cudaSuccess) return e;
+  if ((e = cudaMemsetAsync(S.cstart, 0, sizeof(int) * 2 * (size_t)S.ncell, s)) != cudaSuccess) return e;
+  cell_bounds_kernel<<<grid_of(9 * n, num_sms), 256, 0, s>>>(S.keys_out, 9 * n, S.ncell, S.cstart, S.cend);
+  if (pad)
+    cell_sum_pad_kernel<<<(int)((S.grid2 + 127) / 128), 128, 0, s>>>(S.vals_out, S.cstart, S.cend, S.wr, S.wi,
+                                                                      S.nx);
+  else
+    cell_sum_kernel<<<(S.ncell + 127) / 128, 128, 0, s>>>(S.vals_out, S.cstart, S.cend, src, S.ncell);
+  return cudaGetLastError();
+}
+
+// Cal_Potential_Convolution and Cal_Electric_Field on the deposited charge
+// (wr, wi) with the Green spectrum (gre, gim): Ex, Ey.
+cudaError_t potential_field(PicScratch &S, const double *gre, const double *gim, double hx, double hy,
+                            cudaStream_t s) {
+  fft2d(S.wr, S.wi, S.tw_fwd, 1, S.log2n2, s);
+  spectrum_product_kernel<<<(int)((S.grid2 + 255) / 256), 256, 0, s>>>(S.wr, S.wi, gre, gim, (int)S.grid2);
+  fft2d(S.wr, S.wi, S.tw_inv, -1, S.log2n2, s);
+  field_kernel<<<(S.ncell + 127) / 128, 128, 0, s>>>(S.wr, hx, hy, S.Ex, S.Ey, S.nx);
+  return cudaGetLastError();
+}
+
+cudaError_t finish(PicScratch &S, cudaError_t e, cudaStream_t s) {
+  int h_err = 0;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&h_err, S.err, sizeof(int), cudaMemcpyDeviceToHost, s);
+  const cudaError_t e2 = cudaStreamSynchronize(s);
+  if (e == cudaSuccess) e = e2;
+  if (e == cudaSuccess && h_err) e = cudaErrorInvalidValue;
+  return e;
+}
+
 }  // namespace
+
+bool pic_grid_valid(int nx, int ny) {
+  if (nx != ny || nx < 1 || (nx & (nx - 1)) != 0) return false;
+  const int l = log2_of(2 * nx);
+  return l >= kMinLog2N2 && l <= kMaxLog2N2;
+}
 
 cudaError_t pic_4d(double Np1, long Mp1, double *x1, double Np2, long Mp2, double *x2, double gamma1, double gamma2,
                    double bbscale1, double bbscale2, int num_sms, cudaStream_t s) {
-  const long nmax = std::max(Mp1, Mp2), nitem = 9 * nmax;
-  const size_t grid2 = (size_t)kN2 * kN2;
-  size_t sort_bytes = 0;
-  cudaError_t e = cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, (const uint32_t *)nullptr, (uint32_t *)nullptr,
-                                                  (const double *)nullptr, (double *)nullptr, (int)nitem, 0, kKeyBits,
-                                                  s);
-  if (e != cudaSuccess) return e;
-  // doubles: green (re, im) per direction, work (re, im), Ex, Ey, moments,
-  // twiddles (2 directions of the transform), items; then keys, cell bounds,
-  // the error flag and the sort's scratch
-  const int ntw = kN2 - 1;
-  const size_t nd = 6 * grid2 + 2 * kCells + 8 + 4 * (size_t)ntw + 2 * (size_t)nitem;
-  const size_t bytes = sizeof(double) * nd + sizeof(uint32_t) * 2 * (size_t)nitem + sizeof(int) * (2 * kCells + 2) +
-                       sort_bytes + 256;
-  unsigned char *buf = nullptr;
-  if ((e = cudaMalloc(&buf, bytes)) != cudaSuccess) return e;
-  double *g_re[2], *g_im[2];
-  g_re[0] = reinterpret_cast<double *>(buf);
-  g_im[0] = g_re[0] + grid2;
-  g_re[1] = g_im[0] + grid2;
-  g_im[1] = g_re[1] + grid2;
-  double *wr = g_im[1] + grid2, *wi = wr + grid2;
-  double *Ex = wi + grid2, *Ey = Ex + kCells, *m8 = Ey + kCells;
-  double2 *tw_fwd = reinterpret_cast<double2 *>(m8 + 8), *tw_inv = tw_fwd + ntw;
-  double *vals_in = reinterpret_cast<double *>(tw_inv + ntw), *vals_out = vals_in + nitem;
-  uint32_t *keys_in = reinterpret_cast<uint32_t *>(vals_out + nitem), *keys_out = keys_in + nitem;
-  int *cstart = reinterpret_cast<int *>(keys_out + nitem), *cend = cstart + kCells, *err = cend + kCells;
-  void *sort_tmp = reinterpret_cast<void *>(((uintptr_t)(err + 2) + 255) & ~(uintptr_t)255);
-
-  const std::vector<double2> twf = fft_twiddles(kLog2N2, 1), twi = fft_twiddles(kLog2N2, -1);
-  std::vector<double> h_m8(8), h_green(2 * grid2);
-  auto grid_of = [&](long n) {
-    const long g = (n + 255) / 256, cap = (long)num_sms * 8;
-    return (unsigned)(g < 1 ? 1 : g > cap ? cap : g);
-  };
-  int h_err = 0;
+  PicScratch S;
+  cudaError_t e = S.init(kPicNx, std::max(Mp1, Mp2), s);
+  std::vector<double> h_m8(8), h_green(2 * S.grid2);
   do {
-    if ((e = cudaMemcpyAsync(tw_fwd, twf.data(), sizeof(double2) * ntw, cudaMemcpyHostToDevice, s)) != cudaSuccess)
-      break;
-    if ((e = cudaMemcpyAsync(tw_inv, twi.data(), sizeof(double2) * ntw, cudaMemcpyHostToDevice, s)) != cudaSuccess)
-      break;
-    if ((e = cudaMemsetAsync(err, 0, sizeof(int), s)) != cudaSuccess) break;
-    if ((e = beam_pair_mean_rms(x1, Mp1, x2, Mp2, m8, s)) != cudaSuccess) break;
-    if ((e = cudaMemcpyAsync(h_m8.data(), m8, sizeof(double) * 8, cudaMemcpyDeviceToHost, s)) != cudaSuccess) break;
+    if (e != cudaSuccess) break;
+    if ((e = beam_pair_mean_rms(x1, Mp1, x2, Mp2, S.m8, s)) != cudaSuccess) break;
+    if ((e = cudaMemcpyAsync(h_m8.data(), S.m8, sizeof(double) * 8, cudaMemcpyDeviceToHost, s)) != cudaSuccess) break;
     if ((e = cudaStreamSynchronize(s)) != cudaSuccess) break;
     const double mean1[2] = {h_m8[0], h_m8[1]}, rms1[2] = {h_m8[2], h_m8[3]};
     const double mean2[2] = {h_m8[4], h_m8[5]}, rms2[2] = {h_m8[6], h_m8[7]};
     const double rmsx = rms1[0] > rms2[0] ? rms2[0] : rms1[0];
     const double rmsy = rms1[1] > rms2[1] ? rms2[1] : rms1[1];
-    const double hx = kNsigma * rmsx / kNx, hy = kNsigma * rmsy / kNy;
+    const double hx = kNsigma * rmsx / kPicNx, hy = kNsigma * rmsy / kPicNx;
     // direction 0: beam 1 deposits, beam 2 is kicked; direction 1 the reverse
     const double xoff[2] = {mean2[0] - mean1[0], mean1[0] - mean2[0]};
     const double yoff[2] = {mean2[1] - mean1[1], mean1[1] - mean2[1]};
-    double *const hg[2] = {h_green.data(), h_green.data() + grid2};
-    green_tables(xoff, yoff, hx, hy, hg);
+    double *const hg[2] = {h_green.data(), h_green.data() + S.grid2};
+    green_tables(2, xoff, yoff, hx, hy, kPicNx, hg);
     for (int d = 0; d < 2 && e == cudaSuccess; d++) {
-      if ((e = cudaMemcpyAsync(g_re[d], hg[d], sizeof(double) * grid2, cudaMemcpyHostToDevice, s)) != cudaSuccess ||
-          (e = cudaMemsetAsync(g_im[d], 0, sizeof(double) * grid2, s)) != cudaSuccess)
+      if ((e = cudaMemcpyAsync(S.g_re[d], hg[d], sizeof(double) * S.grid2, cudaMemcpyHostToDevice, s)) !=
+              cudaSuccess ||
+          (e = cudaMemsetAsync(S.g_im[d], 0, sizeof(double) * S.grid2, s)) != cudaSuccess)
         break;
-      fft2d(g_re[d], g_im[d], tw_fwd, 1, s);
+      fft2d(S.g_re[d], S.g_im[d], S.tw_fwd, 1, S.log2n2, s);
     }
     for (int d = 0; d < 2 && e == cudaSuccess; d++) {
       const double *ms = d == 0 ? mean1 : mean2, *mt = d == 0 ? mean2 : mean1;
-      const double *xs = d == 0 ? x1 : x2;
-      double *xt = d == 0 ? x2 : x1;
       const long ns = d == 0 ? Mp1 : Mp2, nt = d == 0 ? Mp2 : Mp1;
-      const double np_per_mp = (d == 0 ? Np1 : Np2) / (double)(int)ns;
-      const GridFrame gs{ms[0], ms[1], ms[0] - kNx * hx / 2, ms[1] - kNy * hy / 2, hx, hy};
-      deposit_items_kernel<<<grid_of(ns), 256, 0, s>>>(xs, ns, gs, true, keys_in, vals_in, err);
-      if ((e = cub::DeviceRadixSort::SortPairs(sort_tmp, sort_bytes, keys_in, keys_out, vals_in, vals_out,
-                                               (int)(9 * ns), 0, kKeyBits, s)) != cudaSuccess)
-        break;
-      if ((e = cudaMemsetAsync(cstart, 0, sizeof(int) * 2 * kCells, s)) != cudaSuccess) break;
-      cell_bounds_kernel<<<grid_of(9 * ns), 256, 0, s>>>(keys_out, 9 * ns, cstart, cend);
-      cell_sum_pad_kernel<<<(int)(grid2 / 128), 128, 0, s>>>(vals_out, cstart, cend, wr, wi);
-      fft2d(wr, wi, tw_fwd, 1, s);
-      spectrum_product_kernel<<<(int)(grid2 / 256), 256, 0, s>>>(wr, wi, g_re[d], g_im[d]);
-      fft2d(wr, wi, tw_inv, -1, s);
-      field_kernel<<<kCells / 128, 128, 0, s>>>(wr, hx, hy, Ex, Ey);
+      const GridFrame gs{ms[0], ms[1], ms[0] - kPicNx * hx / 2, ms[1] - kPicNx * hy / 2, hx, hy, kPicNx};
+      if ((e = deposit(S, d == 0 ? x1 : x2, ns, gs, true, true, nullptr, num_sms, s)) != cudaSuccess) break;
+      if ((e = potential_field(S, S.g_re[d], S.g_im[d], hx, hy, s)) != cudaSuccess) break;
       GridFrame gt = gs;
       gt.mx = mt[0];
       gt.my = mt[1];
-      pic_kick_kernel<<<grid_of(nt), 256, 0, s>>>(xt, nt, gt, xoff[d], yoff[d], Ex, Ey,
-                                                   d == 0 ? bbscale2 : bbscale1, d == 0 ? gamma2 : gamma1,
-                                                   np_per_mp, err);
+      pic_kick_kernel<<<grid_of(nt, num_sms), 256, 0, s>>>(d == 0 ? x2 : x1, nt, gt, xoff[d], yoff[d], S.Ex, S.Ey,
+                                                            d == 0 ? bbscale2 : bbscale1, d == 0 ? gamma2 : gamma1,
+                                                            (d == 0 ? Np1 : Np2) / (double)(int)ns, S.err);
       e = cudaGetLastError();
     }
-    if (e != cudaSuccess) break;
-    if ((e = cudaMemcpyAsync(&h_err, err, sizeof(int), cudaMemcpyDeviceToHost, s)) != cudaSuccess) break;
-    e = cudaStreamSynchronize(s);
   } while (false);
-  cudaStreamSynchronize(s);
-  cudaFree(buf);
-  if (e == cudaSuccess && h_err) e = cudaErrorInvalidValue;
-  return e;
+  return finish(S, e, s);
+}
+
+cudaError_t pic_4d_nonoffset(double Np1, long Mp1, double *x1, double Np2, long Mp2, double *x2, double gamma1,
+                             double gamma2, double bbscale1, double bbscale2, int nx, double hx, double hy,
+                             const double *grn_re, const double *grn_im, int num_sms, cudaStream_t s) {
+  PicScratch S;
+  cudaError_t e = S.init(nx, std::max(Mp1, Mp2), s);
+  // the grid is centred on the origin: x0 = -Nx hx / 2, no offset, the cut around 0
+  const GridFrame g{0., 0., -nx * hx / 2, -nx * hy / 2, hx, hy, nx};
+  for (int d = 0; d < 2 && e == cudaSuccess; d++) {
+    const long ns = d == 0 ? Mp1 : Mp2, nt = d == 0 ? Mp2 : Mp1;
+    if ((e = deposit(S, d == 0 ? x1 : x2, ns, g, true, true, nullptr, num_sms, s)) != cudaSuccess) break;
+    if ((e = potential_field(S, grn_re, grn_im, hx, hy, s)) != cudaSuccess) break;
+    pic_kick_kernel<<<grid_of(nt, num_sms), 256, 0, s>>>(d == 0 ? x2 : x1, nt, g, 0., 0., S.Ex, S.Ey,
+                                                          d == 0 ? bbscale2 : bbscale1, d == 0 ? gamma2 : gamma1,
+                                                          (d == 0 ? Np1 : Np2) / (double)(int)ns, S.err);
+    e = cudaGetLastError();
+  }
+  return finish(S, e, s);
+}
+
+cudaError_t pic_green_function(double xoffset, double yoffset, int nx, double hx, double hy, double *grn_re,
+                               double *grn_im, cudaStream_t s) {
+  PicScratch S;
+  cudaError_t e = S.init(nx, 1, s);
+  std::vector<double> h(S.grid2);
+  do {
+    if (e != cudaSuccess) break;
+    double *const hg[1] = {h.data()};
+    green_tables(1, &xoffset, &yoffset, hx, hy, nx, hg);
+    if ((e = cudaMemcpyAsync(S.g_re[0], h.data(), sizeof(double) * S.grid2, cudaMemcpyHostToDevice, s)) !=
+            cudaSuccess ||
+        (e = cudaMemsetAsync(S.g_im[0], 0, sizeof(double) * S.grid2, s)) != cudaSuccess)
+      break;
+    fft2d(S.g_re[0], S.g_im[0], S.tw_fwd, 1, S.log2n2, s);
+    if ((e = cudaMemcpyAsync(grn_re, S.g_re[0], sizeof(double) * S.grid2, cudaMemcpyDeviceToHost, s)) !=
+            cudaSuccess ||
+        (e = cudaMemcpyAsync(grn_im, S.g_im[0], sizeof(double) * S.grid2, cudaMemcpyDeviceToHost, s)) != cudaSuccess)
+      break;
+  } while (false);
+  return finish(S, e, s);
 }
 
 cudaError_t lumi_pic_4d(double Np1, long Mp1, double Np2, long Mp2, const double *x1, const double *x2, int Ncoll,
                         double freq, int num_sms, cudaStream_t s, double *lumi_out) {
-  const long nmax = std::max(Mp1, Mp2), nitem = 9 * nmax;
-  size_t sort_bytes = 0;
-  cudaError_t e = cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, (const uint32_t *)nullptr, (uint32_t *)nullptr,
-                                                  (const double *)nullptr, (double *)nullptr, (int)nitem, 0, kKeyBits,
-                                                  s);
-  if (e != cudaSuccess) return e;
-  // doubles: src1, src2, extent, overlap, items; then keys, bounds, flag, sort scratch
-  const size_t nd = 2 * kCells + 8 + 2 * (size_t)nitem;
-  const size_t bytes = sizeof(double) * nd + sizeof(uint32_t) * 2 * (size_t)nitem + sizeof(int) * (2 * kCells + 2) +
-                       sort_bytes + 256;
-  unsigned char *buf = nullptr;
-  if ((e = cudaMalloc(&buf, bytes)) != cudaSuccess) return e;
-  double *src1 = reinterpret_cast<double *>(buf), *src2 = src1 + kCells, *ext = src2 + kCells, *ov = ext + 4;
-  double *vals_in = ext + 8, *vals_out = vals_in + nitem;
-  uint32_t *keys_in = reinterpret_cast<uint32_t *>(vals_out + nitem), *keys_out = keys_in + nitem;
-  int *cstart = reinterpret_cast<int *>(keys_out + nitem), *cend = cstart + kCells, *err = cend + kCells;
-  void *sort_tmp = reinterpret_cast<void *>(((uintptr_t)(err + 2) + 255) & ~(uintptr_t)255);
-  auto grid_of = [&](long n) {
-    const long g = (n + 255) / 256, cap = (long)num_sms * 8;
-    return (unsigned)(g < 1 ? 1 : g > cap ? cap : g);
-  };
+  PicScratch S;
+  cudaError_t e = S.init(kPicNx, std::max(Mp1, Mp2), s);
   double h_ext[4] = {0, 0, 0, 0}, h_ov = 0;
-  int h_err = 0;
   bool degenerate = false;
+  double hx = 0, hy = 0;
   do {
-    if ((e = cudaMemsetAsync(err, 0, sizeof(int), s)) != cudaSuccess) break;
-    extent_kernel<<<1, kExtentBlock, 0, s>>>(x1, Mp1, x2, Mp2, ext);
-    if ((e = cudaMemcpyAsync(h_ext, ext, sizeof(h_ext), cudaMemcpyDeviceToHost, s)) != cudaSuccess) break;
+    if (e != cudaSuccess) break;
+    extent_kernel<<<1, kExtentBlock, 0, s>>>(x1, Mp1, x2, Mp2, S.m8);
+    if ((e = cudaMemcpyAsync(h_ext, S.m8, sizeof(h_ext), cudaMemcpyDeviceToHost, s)) != cudaSuccess) break;
     if ((e = cudaStreamSynchronize(s)) != cudaSuccess) break;
     const double xmin = h_ext[0], xmax = h_ext[1], ymin = h_ext[2], ymax = h_ext[3];
     // the reference's grid: 64 cells over the extent, widened by 4 of them on each side
-    double hx = (xmax - xmin) / kNx, hy = (ymax - ymin) / kNy;
+    hx = (xmax - xmin) / kPicNx;
+    hy = (ymax - ymin) / kPicNx;
     const double x0 = xmin - 4 * hx, y0 = ymin - 4 * hy;
-    hx = (xmax - xmin + 8 * hx) / kNx;
-    hy = (ymax - ymin + 8 * hy) / kNy;
+    hx = (xmax - xmin + 8 * hx) / kPicNx;
+    hy = (ymax - ymin + 8 * hy) / kPicNx;
     if (!(hx > 0) || !(hy > 0) || !std::isfinite(hx) || !std::isfinite(hy)) {
       degenerate = true;
       break;
     }
-    const GridFrame g{0., 0., x0, y0, hx, hy};
-    for (int b = 0; b < 2 && e == cudaSuccess; b++) {
-      const double *x = b == 0 ? x1 : x2;
-      const long n = b == 0 ? Mp1 : Mp2;
-      deposit_items_kernel<<<grid_of(n), 256, 0, s>>>(x, n, g, false, keys_in, vals_in, err);
-      if ((e = cub::DeviceRadixSort::SortPairs(sort_tmp, sort_bytes, keys_in, keys_out, vals_in, vals_out,
-                                               (int)(9 * n), 0, kKeyBits, s)) != cudaSuccess)
-        break;
-      if ((e = cudaMemsetAsync(cstart, 0, sizeof(int) * 2 * kCells, s)) != cudaSuccess) break;
-      cell_bounds_kernel<<<grid_of(9 * n), 256, 0, s>>>(keys_out, 9 * n, cstart, cend);
-      cell_sum_kernel<<<kCells / 128, 128, 0, s>>>(vals_out, cstart, cend, b == 0 ? src1 : src2);
-      e = cudaGetLastError();
-    }
-    if (e != cudaSuccess) break;
-    overlap_sum_kernel<<<1, 32, 0, s>>>(src1, src2, ov);
-    if ((e = cudaMemcpyAsync(&h_ov, ov, sizeof(double), cudaMemcpyDeviceToHost, s)) != cudaSuccess) break;
-    if ((e = cudaMemcpyAsync(&h_err, err, sizeof(int), cudaMemcpyDeviceToHost, s)) != cudaSuccess) break;
-    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) break;
-    *lumi_out = Ncoll * h_ov * (Np1 / (int)Mp1) * (Np2 / (int)Mp2) * freq / hx / hy / 10000;
+    const GridFrame g{0., 0., x0, y0, hx, hy, kPicNx};
+    if ((e = deposit(S, x1, Mp1, g, false, false, S.wr, num_sms, s)) != cudaSuccess) break;
+    if ((e = deposit(S, x2, Mp2, g, false, false, S.wi, num_sms, s)) != cudaSuccess) break;
+    overlap_sum_kernel<<<1, 32, 0, s>>>(S.wr, S.wi, S.m8 + 4, S.ncell);
+    if ((e = cudaMemcpyAsync(&h_ov, S.m8 + 4, sizeof(double), cudaMemcpyDeviceToHost, s)) != cudaSuccess) break;
   } while (false);
-  cudaStreamSynchronize(s);
-  cudaFree(buf);
-  if (e == cudaSuccess && (h_err || degenerate)) e = cudaErrorInvalidValue;
+  e = finish(S, e, s);
+  if (e == cudaSuccess && degenerate) e = cudaErrorInvalidValue;
+  if (e == cudaSuccess) *lumi_out = Ncoll * h_ov * (Np1 / (int)Mp1) * (Np2 / (int)Mp2) * freq / hx / hy / 10000;
   return e;
 }
 

@@ -125,6 +125,11 @@ class RefOracle:
         L.ref_lumi_pic_4d.argtypes = [c_double, c_int, c_double, c_int, POINTER(c_double), POINTER(c_double), c_int,
                                       c_double]
         L.ref_lumi_pic_4d.restype = c_double
+        L.ref_green_function.argtypes = [c_double, c_double, c_int, c_int, c_double, c_double, POINTER(c_double),
+                                         POINTER(c_double)]
+        L.ref_bb4d_pic_nonoffset.argtypes = [c_double, c_int, POINTER(c_double), c_double, c_int, POINTER(c_double),
+                                             c_double, c_double, c_double, c_double, c_int, c_int, c_double, c_double,
+                                             POINTER(c_double), POINTER(c_double)]
         L.ref_bb6d_soft_gaussian.argtypes = [c_double, c_int, POINTER(c_double), c_double, c_int, POINTER(c_double),
                                              c_double, c_double, c_double, c_double, c_int, c_int]
         L.ref_bb6d_soft_gaussian_zb.argtypes = [c_double, c_int, POINTER(c_double), c_double, c_int,

@@ -134,3 +134,59 @@ def test_lumi_rejected_inputs():
     bad[4, 2] = np.inf
     with pytest.raises(SimTrackError):
         api.Lumi_Cal_PIC_4D(1e11, bad, 1e11, b, 1, 1e4)
+
+
+def _green(nx, hx, hy, xoff=0.0, yoff=0.0, ours=True):
+    gr, gi = np.empty(4 * nx * nx), np.empty(4 * nx * nx)
+    P = lambda a: a.ctypes.data_as(POINTER(c_double))
+    if ours:
+        from simtrack_b200._native import lib
+        assert lib().stb_pic_green_function(xoff, yoff, nx, nx, hx, hy, P(gr), P(gi), 0) == 0
+    else:
+        oracle_bridge.RefOracle().L.ref_green_function(xoff, yoff, nx, nx, hx, hy, P(gr), P(gi))
+    return gr, gi
+
+
+@pytest.mark.parametrize("nx,xoff,yoff", [(8, 0.0, 0.0), (32, 1e-5, -2e-5), (64, 0.0, 0.0), (128, -3e-6, 4e-6)])
+def test_green_function_vs_reference(nx, xoff, yoff):
+    """Cal_Effective_Green_Function (simtrack.cpp:2881-2921): the host table
+    and the GPU transform equal the reference's, bit for bit."""
+    _need_ref()
+    hx, hy = 15 * 1e-4 / nx, 15 * 6e-5 / nx
+    ours = _green(nx, hx, hy, xoff, yoff)
+    theirs = _green(nx, hx, hy, xoff, yoff, ours=False)
+    assert np.array_equal(ours[0], theirs[0]) and np.array_equal(ours[1], theirs[1])
+
+
+@pytest.mark.parametrize("nx,n1,n2", [(64, 4000, 5000), (128, 30_000, 20_000), (32, 2, 3000)])
+def test_pic_nonoffset_vs_reference(nx, n1, n2):
+    """BeamBeam4D_PIC_NonOffset (simtrack.cpp:24226-24280) with the
+    reference's own Green spectrum on the caller's grid, bit for bit."""
+    _need_ref()
+    hx, hy = 15 * 1e-4 / nx, 15 * 6e-5 / nx
+    gr, gi = _green(nx, hx, hy, ours=False)
+    b1 = _beam(n1, 1e-4, 6e-5, 0.0, 0.0, 7)
+    b2 = _beam(n2, 1.1e-4, 5.5e-5, 2e-6, -1e-6, 8)
+    if n2 > 100:
+        b2[9, 0] = 0.6 * nx * hx  # outside the cut
+    P = lambda a: a.ctypes.data_as(POINTER(c_double))
+    o1, o2 = b1.copy(), b2.copy()
+    from simtrack_b200._native import lib
+    assert lib().stb_bb4d_pic_nonoffset_host(1.5e11, n1, P(o1), 1.3e11, n2, P(o2), GAMMA, GAMMA, 1.0, -1.0, nx, nx,
+                                             hx, hy, P(gr), P(gi), 0) == 0
+    r1, r2 = b1.copy(), b2.copy()
+    oracle_bridge.RefOracle().L.ref_bb4d_pic_nonoffset(1.5e11, n1, P(r1), 1.3e11, n2, P(r2), GAMMA, GAMMA, 1.0, -1.0,
+                                                       nx, nx, hx, hy, P(gr), P(gi))
+    assert np.array_equal(o1, r1) and np.array_equal(o2, r2)
+    assert (o2[:, 1] != b2[:, 1]).sum() > 0.9 * n2
+    if n2 > 100:
+        assert o2[9, 1] == b2[9, 1]
+
+
+def test_pic_grid_rejections():
+    from simtrack_b200._native import lib
+    gr, gi = np.empty(4 * 48 * 48), np.empty(4 * 48 * 48)
+    P = lambda a: a.ctypes.data_as(POINTER(c_double))
+    assert lib().stb_pic_green_function(0.0, 0.0, 48, 48, 1e-5, 1e-5, P(gr), P(gi), 0) != 0  # not a power of two
+    assert lib().stb_pic_green_function(0.0, 0.0, 32, 64, 1e-5, 1e-5, P(gr), P(gi), 0) != 0  # not square
+    assert lib().stb_pic_green_function(0.0, 0.0, 1024, 1024, 1e-5, 1e-5, P(gr), P(gi), 0) != 0  # above 512
