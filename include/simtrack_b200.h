@@ -543,6 +543,21 @@ int stb_bb4d_pic_device(double Np1, long n1, double *x1, double Np2, long n2, do
 int stb_bb4d_pic_host(double Np1, long n1, double *x1, double Np2, long n2, double *x2, double gamma1, double gamma2,
                       double bbscale1, double bbscale2, int device);
 
+/* BeamBeam6D_PIC(Np1, Mp1, x1, Np2, Mp2, x2, gamma1, gamma2, bbscale1,
+ * bbscale2, Nslice1, Nslice2), simtrack.cpp:23380-23615: the sliced 6D
+ * collision of stb_bb6d_soft_gaussian_* (bunches reordered in place by z,
+ * largest first; slices of Mp/Nslice particles; slice pairs in the
+ * reference's collision order, each drifted to its collision point) with
+ * each slice pair colliding as stb_bb4d_pic_* with N/Nslice; bit for bit.
+ * Arguments as for stb_bb6d_soft_gaussian_*.  The reference also writes
+ * every bunch and slice to ./bunch*.dat on each call; this build writes
+ * nothing.  Both forms return when done. */
+int stb_bb6d_pic_device(double Np1, long Mp1, double *x1, double Np2, long Mp2, double *x2, double gamma1,
+                        double gamma2, double bbscale1, double bbscale2, int nslice1, int nslice2, int device,
+                        void *stream);
+int stb_bb6d_pic_host(double Np1, long Mp1, double *x1, double Np2, long Mp2, double *x2, double gamma1,
+                      double gamma2, double bbscale1, double bbscale2, int nslice1, int nslice2, int device);
+
 /* Cal_Effective_Green_Function(xoffset, yoffset, Nx, Ny, hx, hy, grn_c_r,
  * grn_c_i), simtrack.cpp:2881-2921: the integrated Green function of the 2D
  * Poisson equation on the doubled 2Nx x 2Ny grid, transformed by the

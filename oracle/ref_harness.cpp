@@ -510,6 +510,13 @@ void ref_bb4d_pic_nonoffset(double Np1, int n1, double *x1, double Np2, int n2, 
   BeamBeam4D_PIC_NonOffset(Np1, n1, x1, Np2, n2, x2, gamma1, gamma2, bbscale1, bbscale2, nx, ny, hx, hy, gr, gi);
 }
 
+// BeamBeam6D_PIC (simtrack.cpp:23380); it writes bunch and slice files
+// into the working directory.
+void ref_bb6d_pic(double Np1, int n1, double *x1, double Np2, int n2, double *x2, double gamma1, double gamma2,
+                  double bbscale1, double bbscale2, int ns1, int ns2) {
+  BeamBeam6D_PIC(Np1, n1, x1, Np2, n2, x2, gamma1, gamma2, bbscale1, bbscale2, ns1, ns2);
+}
+
 // Lumi_Cal_PIC_4D (simtrack.cpp:23617).
 double ref_lumi_pic_4d(double Np1, int n1, double Np2, int n2, double *x1, double *x2, int ncoll, double freq) {
   return Lumi_Cal_PIC_4D(Np1, n1, Np2, n2, x1, x2, ncoll, freq);

@@ -78,6 +78,17 @@ def BeamBeam4D_PIC(Np1: float, x1: np.ndarray, Np2: float, x2: np.ndarray, gamma
                                   device))
 
 
+def BeamBeam6D_PIC(Np1: float, x1: np.ndarray, Np2: float, x2: np.ndarray, gamma1: float, gamma2: float,
+                   bbscale1: float, bbscale2: float, Nslice1: int, Nslice2: int, device: int = 0) -> None:
+    """BeamBeam6D_PIC (simtrack.cpp:23380-23615) on the GPU: both bunches
+    (numpy (n, 6) float64, updated in place and reordered by z as in the
+    reference) sliced, each slice pair colliding as BeamBeam4D_PIC."""
+    b1, b2 = _bunch(x1), _bunch(x2)
+    P = lambda a: a.ctypes.data_as(POINTER(c_double))
+    check(lib().stb_bb6d_pic_host(Np1, len(b1), P(b1), Np2, len(b2), P(b2), gamma1, gamma2, bbscale1, bbscale2,
+                                  int(Nslice1), int(Nslice2), device))
+
+
 def Lumi_Cal_PIC_4D(Np1: float, x1: np.ndarray, Np2: float, x2: np.ndarray, Ncoll: int, freq: float,
                     device: int = 0) -> float:
     """Lumi_Cal_PIC_4D (simtrack.cpp:23617-23701) on the GPU: the two

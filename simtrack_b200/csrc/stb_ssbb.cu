@@ -247,9 +247,16 @@ cudaError_t soft_gaussian_4d(double *x1, long n1, double *x2, long n2, double c4
 // each other as soft Gaussians (strength N/Nslice) and drift back.  The
 // reference also writes its slice centroids to ./bunch1_Z.dat and
 // ./bunch2_Z.dat on every call; nothing is written here.
-cudaError_t soft_gaussian_6d(double Np1, long Mp1, double *x1, double Np2, long Mp2, double *x2, double gamma1,
-                             double gamma2, double bbscale1, double bbscale2, int Nslice1, int Nslice2, int num_sms,
-                             cudaStream_t s) {
+namespace {
+// The sliced 6D collision of BeamBeam6D_SoftGaussian (simtrack.cpp:
+// 22874-23132) and BeamBeam6D_PIC (23380-23615), which differ only in the
+// collision of a slice pair: both bunches sorted by z (largest first), cut
+// into Nslice slices of Mp/Nslice consecutive particles, the slice pairs put
+// in the reference's collision order, and `collide(slice1, m1, slice2, m2,
+// S)` called for each pair in that order.
+template <class Collide>
+cudaError_t sliced_6d(long Mp1, double *x1, long Mp2, double *x2, int Nslice1, int Nslice2, cudaStream_t s,
+                      Collide collide) {
   const long nmax = Mp1 > Mp2 ? Mp1 : Mp2;
   double *scratch = nullptr;
   cudaError_t e = cudaMalloc(&scratch, sizeof(double) * (6 * (size_t)nmax + (size_t)Nslice1 + (size_t)Nslice2) +
@@ -286,16 +293,45 @@ cudaError_t soft_gaussian_6d(double Np1, long Mp1, double *x1, double Np2, long 
           std::swap(I1[i], I1[j]);
           std::swap(I2[i], I2[j]);
         }
-    const double rp = 1.53469826769e-18;  // BB4D, simtrack.cpp:6328
-    const double N2s = Np2 / Nslice2, N1s = Np1 / Nslice1;
-    const double c4_1 = 2 * N2s * rp / gamma1, c4_2 = 2 * N1s * rp / gamma2;
     for (int i = 0; i < np && e == cudaSuccess; i++)
-      e = slice_pair_collision(x1 + 6 * (long)I1[i] * m1, m1, x2 + 6 * (long)I2[i] * m2, m2, S[i], c4_1, c4_2,
-                               bbscale1, bbscale2, num_sms, s);
+      e = collide(x1 + 6 * (long)I1[i] * m1, m1, x2 + 6 * (long)I2[i] * m2, m2, S[i]);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   }
   cudaFree(scratch);
   return e;
+}
+}  // namespace
+
+cudaError_t soft_gaussian_6d(double Np1, long Mp1, double *x1, double Np2, long Mp2, double *x2, double gamma1,
+                             double gamma2, double bbscale1, double bbscale2, int Nslice1, int Nslice2, int num_sms,
+                             cudaStream_t s) {
+  const double rp = 1.53469826769e-18;  // BB4D, simtrack.cpp:6328
+  const double N2s = Np2 / Nslice2, N1s = Np1 / Nslice1;
+  const double c4_1 = 2 * N2s * rp / gamma1, c4_2 = 2 * N1s * rp / gamma2;
+  return sliced_6d(Mp1, x1, Mp2, x2, Nslice1, Nslice2, s, [&](double *a, long m1, double *b, long m2, double S) {
+    return slice_pair_collision(a, m1, b, m2, S, c4_1, c4_2, bbscale1, bbscale2, num_sms, s);
+  });
+}
+
+// BeamBeam6D_PIC (simtrack.cpp:23380-23615): each slice pair drifts to its
+// collision point, collides as BeamBeam4D_PIC with N/Nslice, drifts back.
+// The reference also writes every bunch and slice to ./bunch*.dat files on
+// each call; this build writes nothing.
+cudaError_t pic_6d(double Np1, long Mp1, double *x1, double Np2, long Mp2, double *x2, double gamma1, double gamma2,
+                   double bbscale1, double bbscale2, int Nslice1, int Nslice2, int num_sms, cudaStream_t s) {
+  return sliced_6d(Mp1, x1, Mp2, x2, Nslice1, Nslice2, s, [&](double *a, long m1, double *b, long m2, double S) {
+    const unsigned g1 = (unsigned)((m1 + 255) / 256 < num_sms * 8 ? (m1 + 255) / 256 : num_sms * 8);
+    const unsigned g2 = (unsigned)((m2 + 255) / 256 < num_sms * 8 ? (m2 + 255) / 256 : num_sms * 8);
+    slice_drift_kernel<<<g1 < 1 ? 1 : g1, 256, 0, s>>>(a, m1, S, true);
+    slice_drift_kernel<<<g2 < 1 ? 1 : g2, 256, 0, s>>>(b, m2, -S, true);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess)
+      e = pic_4d(Np1 / Nslice1, m1, a, Np2 / Nslice2, m2, b, gamma1, gamma2, bbscale1, bbscale2, num_sms, s);
+    if (e != cudaSuccess) return e;
+    slice_drift_kernel<<<g1 < 1 ? 1 : g1, 256, 0, s>>>(a, m1, S, false);
+    slice_drift_kernel<<<g2 < 1 ? 1 : g2, 256, 0, s>>>(b, m2, -S, false);
+    return cudaGetLastError();
+  });
 }
 
 // BeamBeam6D_SoftGaussian with slice boundaries (simtrack.cpp:23134-23283):

@@ -130,6 +130,8 @@ class RefOracle:
         L.ref_bb4d_pic_nonoffset.argtypes = [c_double, c_int, POINTER(c_double), c_double, c_int, POINTER(c_double),
                                              c_double, c_double, c_double, c_double, c_int, c_int, c_double, c_double,
                                              POINTER(c_double), POINTER(c_double)]
+        L.ref_bb6d_pic.argtypes = [c_double, c_int, POINTER(c_double), c_double, c_int, POINTER(c_double),
+                                   c_double, c_double, c_double, c_double, c_int, c_int]
         L.ref_bb6d_soft_gaussian.argtypes = [c_double, c_int, POINTER(c_double), c_double, c_int, POINTER(c_double),
                                              c_double, c_double, c_double, c_double, c_int, c_int]
         L.ref_bb6d_soft_gaussian_zb.argtypes = [c_double, c_int, POINTER(c_double), c_double, c_int,
