@@ -558,6 +558,22 @@ int stb_bb6d_pic_device(double Np1, long Mp1, double *x1, double Np2, long Mp2, 
 int stb_bb6d_pic_host(double Np1, long Mp1, double *x1, double Np2, long Mp2, double *x2, double gamma1,
                       double gamma2, double bbscale1, double bbscale2, int nslice1, int nslice2, int device);
 
+/* Lumi_Cal_PIC_6D(Np1, Mp1, Np2, Mp2, Nslice1, Nslice2, x1, x2, gamma1,
+ * gamma2, bbscale1, bbscale2, Ncoll, freq), simtrack.cpp:23703-23944: the
+ * sliced driver of stb_bb6d_pic_* (bunches reordered by z in place, slice
+ * pairs in collision order, drifted to their collision points); per pair the
+ * luminosity of stb_lumi_pic_4d_* with N/Nslice is summed into *lumi, then
+ * the pair collides as soft Gaussians (BB4D, N/Nslice) and drifts back, so
+ * px and py change too; bit for bit.  Slice arguments as for
+ * stb_bb6d_soft_gaussian_*.  The reference also writes the collision order
+ * to ./collide_order.dat; this build writes nothing. */
+int stb_lumi_pic_6d_device(double Np1, long Mp1, double Np2, long Mp2, int nslice1, int nslice2, double *x1,
+                           double *x2, double gamma1, double gamma2, double bbscale1, double bbscale2, int Ncoll,
+                           double freq, int device, void *stream, double *lumi);
+int stb_lumi_pic_6d_host(double Np1, long Mp1, double Np2, long Mp2, int nslice1, int nslice2, double *x1,
+                         double *x2, double gamma1, double gamma2, double bbscale1, double bbscale2, int Ncoll,
+                         double freq, int device, double *lumi);
+
 /* Cal_Effective_Green_Function(xoffset, yoffset, Nx, Ny, hx, hy, grn_c_r,
  * grn_c_i), simtrack.cpp:2881-2921: the integrated Green function of the 2D
  * Poisson equation on the doubled 2Nx x 2Ny grid, transformed by the

@@ -517,6 +517,12 @@ void ref_bb6d_pic(double Np1, int n1, double *x1, double Np2, int n2, double *x2
   BeamBeam6D_PIC(Np1, n1, x1, Np2, n2, x2, gamma1, gamma2, bbscale1, bbscale2, ns1, ns2);
 }
 
+// Lumi_Cal_PIC_6D (simtrack.cpp:23703); it writes ./collide_order.dat.
+double ref_lumi_pic_6d(double Np1, int n1, double Np2, int n2, int ns1, int ns2, double *x1, double *x2,
+                       double gamma1, double gamma2, double bbscale1, double bbscale2, int ncoll, double freq) {
+  return Lumi_Cal_PIC_6D(Np1, n1, Np2, n2, ns1, ns2, x1, x2, gamma1, gamma2, bbscale1, bbscale2, ncoll, freq);
+}
+
 // Lumi_Cal_PIC_4D (simtrack.cpp:23617).
 double ref_lumi_pic_4d(double Np1, int n1, double Np2, int n2, double *x1, double *x2, int ncoll, double freq) {
   return Lumi_Cal_PIC_4D(Np1, n1, Np2, n2, x1, x2, ncoll, freq);

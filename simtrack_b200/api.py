@@ -101,6 +101,21 @@ def Lumi_Cal_PIC_4D(Np1: float, x1: np.ndarray, Np2: float, x2: np.ndarray, Ncol
     return out.value
 
 
+def Lumi_Cal_PIC_6D(Np1: float, x1: np.ndarray, Np2: float, x2: np.ndarray, Nslice1: int, Nslice2: int,
+                    gamma1: float, gamma2: float, bbscale1: float, bbscale2: float, Ncoll: int, freq: float,
+                    device: int = 0) -> float:
+    """Lumi_Cal_PIC_6D (simtrack.cpp:23703-23944) on the GPU: the sliced
+    luminosity, the slice pairs colliding as soft Gaussians as they pass
+    (both bunches, numpy (n, 6) float64, updated in place and reordered by z
+    as in the reference)."""
+    b1, b2 = _bunch(x1), _bunch(x2)
+    P = lambda a: a.ctypes.data_as(POINTER(c_double))
+    out = c_double()
+    check(lib().stb_lumi_pic_6d_host(Np1, len(b1), Np2, len(b2), int(Nslice1), int(Nslice2), P(b1), P(b2), gamma1,
+                                     gamma2, bbscale1, bbscale2, int(Ncoll), freq, device, byref(out)))
+    return out.value
+
+
 def BeamBeam6D_SoftGaussian(Np1: float, x1: np.ndarray, Np2: float, x2: np.ndarray, gamma1: float, gamma2: float,
                             bbscale1: float, bbscale2: float, Nslice1: int, Nslice2: int, zb1=None, zb2=None,
                             device: int = 0) -> None:

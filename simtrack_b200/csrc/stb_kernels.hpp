@@ -140,6 +140,11 @@ cudaError_t lumi_pic_4d(double Np1, long Mp1, double Np2, long Mp2, const double
 cudaError_t pic_6d(double Np1, long Mp1, double *x1, double Np2, long Mp2, double *x2, double gamma1, double gamma2,
                    double bbscale1, double bbscale2, int Nslice1, int Nslice2, int num_sms, cudaStream_t s);
 
+// Lumi_Cal_PIC_6D on device AoS bunches (stb_ssbb.cu; synchronises `s`).
+cudaError_t lumi_pic_6d(double Np1, long Mp1, double *x1, double Np2, long Mp2, double *x2, double gamma1,
+                        double gamma2, double bbscale1, double bbscale2, int Nslice1, int Nslice2, int Ncoll,
+                        double freq, int num_sms, cudaStream_t s, double *lumi_out);
+
 size_t track_smem_bytes(int nelem, int npool_padded);
 // The loss-test mode of a launch with circular aperture r2 (+inf: none) on a
 // table whose loss-checked elements have min(RN(APx^2), RN(APy^2)) >= min_ap2.

@@ -209,3 +209,22 @@ def test_pic_6d_vs_reference(case, tmp_path, monkeypatch):
     oracle_bridge.RefOracle().L.ref_bb6d_pic(2e11, Mp1, P(r1), 1.8e11, Mp2, P(r2), GAMMA, GAMMA, s1, s2, ns1, ns2)
     assert np.array_equal(o1, r1) and np.array_equal(o2, r2)
     assert (np.sort(o1[:, 4]) == np.sort(b1[:, 4])).all() and (o1[:-1, 4] >= o1[1:, 4]).all()
+
+
+@pytest.mark.parametrize("case", [(3000, 2600, 4, 3, 1.0, 1.0, 2), (2001, 2003, 3, 3, -1.0, 0.5, 1)])
+def test_lumi_pic_6d_vs_reference(case, tmp_path, monkeypatch):
+    """Lumi_Cal_PIC_6D (simtrack.cpp:23703-23944): the summed slice-pair
+    luminosities and the bunches after the soft-Gaussian passes, bit for bit."""
+    _need_ref()
+    monkeypatch.chdir(tmp_path)  # the reference writes ./collide_order.dat
+    Mp1, Mp2, ns1, ns2, s1, s2, ncoll = case
+    b1 = _beam(Mp1, 1.2e-4, 1.0e-4, 0.0, 0.0, 13)
+    b2 = _beam(Mp2, 1.1e-4, 1.1e-4, 1e-5, -5e-6, 14)
+    o1, o2 = b1.copy(), b2.copy()
+    ours = api.Lumi_Cal_PIC_6D(2e11, o1, 1.8e11, o2, ns1, ns2, GAMMA, GAMMA, s1, s2, ncoll, 78196.0)
+    P = lambda a: a.ctypes.data_as(POINTER(c_double))
+    r1, r2 = b1.copy(), b2.copy()
+    theirs = oracle_bridge.RefOracle(cr=True).L.ref_lumi_pic_6d(2e11, Mp1, 1.8e11, Mp2, ns1, ns2, P(r1), P(r2),
+                                                                GAMMA, GAMMA, s1, s2, ncoll, 78196.0)
+    assert ours == theirs and ours > 0
+    assert np.array_equal(o1, r1) and np.array_equal(o2, r2)
