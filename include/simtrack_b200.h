@@ -558,6 +558,18 @@ int stb_bb6d_pic_device(double Np1, long Mp1, double *x1, double Np2, long Mp2, 
 int stb_bb6d_pic_host(double Np1, long Mp1, double *x1, double Np2, long Mp2, double *x2, double gamma1,
                       double gamma2, double bbscale1, double bbscale2, int nslice1, int nslice2, int device);
 
+/* BeamBeam6D_PIC_NonOffset(Np1, Mp1, x1, Np2, Mp2, x2, gamma1, gamma2,
+ * bbscale1, bbscale2, Nslice1, Nslice2, zb1, zb2, Nx, Ny, hx, hy, grn_c_r,
+ * grn_c_i), simtrack.cpp:24282-24432: the slice-boundary driver of
+ * stb_bb6d_soft_gaussian_zb_host (slices zb[s+1] <= z < zb[s], particles
+ * kept in place, the same checks) with each slice pair colliding as
+ * stb_bb4d_pic_nonoffset_* with N scaled by the slice's share; bit for bit.
+ * Grid and Green spectrum (host arrays) as for stb_bb4d_pic_nonoffset_host. */
+int stb_bb6d_pic_nonoffset_host(double Np1, long Mp1, double *x1, double Np2, long Mp2, double *x2, double gamma1,
+                                double gamma2, double bbscale1, double bbscale2, int nslice1, int nslice2,
+                                const double *zb1, const double *zb2, int Nx, int Ny, double hx, double hy,
+                                const double *grn_c_r, const double *grn_c_i, int device);
+
 /* Lumi_Cal_PIC_6D(Np1, Mp1, Np2, Mp2, Nslice1, Nslice2, x1, x2, gamma1,
  * gamma2, bbscale1, bbscale2, Ncoll, freq), simtrack.cpp:23703-23944: the
  * sliced driver of stb_bb6d_pic_* (bunches reordered by z in place, slice

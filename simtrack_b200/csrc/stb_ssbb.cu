@@ -380,9 +380,10 @@ cudaError_t lumi_pic_6d(double Np1, long Mp1, double *x1, double Np2, long Mp2, 
 // size, and a slice of fewer than two particles has no rms size: all are
 // checked before any particle moves.  Returns cudaErrorInvalidValue when a
 // slice is too full or too thin.
-cudaError_t soft_gaussian_6d_zb(double Np1, long Mp1, double *x1, double Np2, long Mp2, double *x2, double gamma1,
-                                double gamma2, double bbscale1, double bbscale2, int nslice, const double *zb1,
-                                const double *zb2, int num_sms, cudaStream_t s) {
+namespace {
+template <class Collide>
+cudaError_t sliced_6d_zb(double Np1, long Mp1, double *x1, double Np2, long Mp2, double *x2, int nslice,
+                         const double *zb1, const double *zb2, int num_sms, cudaStream_t s, Collide collide) {
   const long cap1 = 2 * Mp1 / nslice, cap2 = 2 * Mp2 / nslice;
   const size_t nidx = (size_t)nslice * (size_t)(cap1 + cap2);
   const size_t bytes = sizeof(double) * (6 * (size_t)(cap1 + cap2) + 2 * (size_t)(nslice + 1) + 2 * (size_t)nslice) +
@@ -434,19 +435,17 @@ cudaError_t soft_gaussian_6d_zb(double Np1, long Mp1, double *x1, double Np2, lo
           std::swap(I1[i], I1[j]);
           std::swap(I2[i], I2[j]);
         }
-    const double rp = 1.53469826769e-18;  // BB4D, simtrack.cpp:6328
     const unsigned cap = (unsigned)num_sms * 8;
     for (int i = 0; i < np && e == cudaSuccess; i++) {
       const long m1 = c[I1[i]], m2 = c[nslice + I2[i]];
       const int32_t *j1 = idx1 + (size_t)I1[i] * cap1, *j2 = idx2 + (size_t)I2[i] * cap2;
-      // BeamBeam4D_SoftGaussian(Np1*Mp1_coll/Mp1, ..., Np2*Mp2_coll/Mp2, ...), 23245
+      // the pair collides with Np1*Mp1_coll/Mp1 and Np2*Mp2_coll/Mp2 (23245, 24400)
       const double N1c = Np1 * (int)m1 / (int)Mp1, N2c = Np2 * (int)m2 / (int)Mp2;
-      const double c4_1 = 2 * N2c * rp / gamma1, c4_2 = 2 * N1c * rp / gamma2;
       const unsigned g1 = (unsigned)((m1 + 255) / 256 < cap ? (m1 + 255) / 256 : cap);
       const unsigned g2 = (unsigned)((m2 + 255) / 256 < cap ? (m2 + 255) / 256 : cap);
       if (m1 > 0) gather_members_kernel<<<g1, 256, 0, s>>>(x1, j1, m1, xc1);
       if (m2 > 0) gather_members_kernel<<<g2, 256, 0, s>>>(x2, j2, m2, xc2);
-      e = slice_pair_collision(xc1, m1, xc2, m2, S[i], c4_1, c4_2, bbscale1, bbscale2, num_sms, s);
+      e = collide(xc1, m1, xc2, m2, S[i], N1c, N2c);
       if (m1 > 0) scatter_members_kernel<<<g1, 256, 0, s>>>(x1, j1, m1, xc1);
       if (m2 > 0) scatter_members_kernel<<<g2, 256, 0, s>>>(x2, j2, m2, xc2);
       if (e == cudaSuccess) e = cudaGetLastError();
@@ -455,6 +454,43 @@ cudaError_t soft_gaussian_6d_zb(double Np1, long Mp1, double *x1, double Np2, lo
   }
   cudaFree(buf);
   return e;
+}
+
+}  // namespace
+
+cudaError_t soft_gaussian_6d_zb(double Np1, long Mp1, double *x1, double Np2, long Mp2, double *x2, double gamma1,
+                                double gamma2, double bbscale1, double bbscale2, int nslice, const double *zb1,
+                                const double *zb2, int num_sms, cudaStream_t s) {
+  const double rp = 1.53469826769e-18;  // BB4D, simtrack.cpp:6328
+  return sliced_6d_zb(Np1, Mp1, x1, Np2, Mp2, x2, nslice, zb1, zb2, num_sms, s,
+                      [&](double *a, long m1, double *b, long m2, double S, double N1c, double N2c) {
+                        const double c4_1 = 2 * N2c * rp / gamma1, c4_2 = 2 * N1c * rp / gamma2;
+                        return slice_pair_collision(a, m1, b, m2, S, c4_1, c4_2, bbscale1, bbscale2, num_sms, s);
+                      });
+}
+
+// BeamBeam6D_PIC_NonOffset (simtrack.cpp:24282-24432): the slice-boundary
+// driver above with each slice pair colliding as BeamBeam4D_PIC_NonOffset on
+// the caller's grid and Green spectrum (device arrays).
+cudaError_t pic_6d_nonoffset(double Np1, long Mp1, double *x1, double Np2, long Mp2, double *x2, double gamma1,
+                             double gamma2, double bbscale1, double bbscale2, int nslice, const double *zb1,
+                             const double *zb2, int nx, double hx, double hy, const double *grn_re,
+                             const double *grn_im, int num_sms, cudaStream_t s) {
+  return sliced_6d_zb(Np1, Mp1, x1, Np2, Mp2, x2, nslice, zb1, zb2, num_sms, s,
+                      [&](double *a, long m1, double *b, long m2, double S, double N1c, double N2c) {
+                        const unsigned g1 = (unsigned)((m1 + 255) / 256 < num_sms * 8 ? (m1 + 255) / 256 : num_sms * 8);
+                        const unsigned g2 = (unsigned)((m2 + 255) / 256 < num_sms * 8 ? (m2 + 255) / 256 : num_sms * 8);
+                        slice_drift_kernel<<<g1 < 1 ? 1 : g1, 256, 0, s>>>(a, m1, S, true);
+                        slice_drift_kernel<<<g2 < 1 ? 1 : g2, 256, 0, s>>>(b, m2, -S, true);
+                        cudaError_t r = cudaGetLastError();
+                        if (r == cudaSuccess)
+                          r = pic_4d_nonoffset(N1c, m1, a, N2c, m2, b, gamma1, gamma2, bbscale1, bbscale2, nx, hx, hy,
+                                               grn_re, grn_im, num_sms, s);
+                        if (r != cudaSuccess) return r;
+                        slice_drift_kernel<<<g1 < 1 ? 1 : g1, 256, 0, s>>>(a, m1, S, false);
+                        slice_drift_kernel<<<g2 < 1 ? 1 : g2, 256, 0, s>>>(b, m2, -S, false);
+                        return cudaGetLastError();
+                      });
 }
 
 }  // namespace stb
