@@ -558,6 +558,17 @@ int stb_bb6d_pic_device(double Np1, long Mp1, double *x1, double Np2, long Mp2, 
 int stb_bb6d_pic_host(double Np1, long Mp1, double *x1, double Np2, long Mp2, double *x2, double gamma1,
                       double gamma2, double bbscale1, double bbscale2, int nslice1, int nslice2, int device);
 
+/* Lumi_Cal_PIC_6D_Angle(Np1, Mp1, Np2, Mp2, theta, Nslice1, Nslice2, x1, x2,
+ * gamma1, gamma2, bbscale1, bbscale2, Ncoll, freq), simtrack.cpp:
+ * 23946-24224: both bunches boosted to the head-on frame of half crossing
+ * angle theta (Lorentz_Transfer, 6790-6815; they are returned boosted, as
+ * the reference leaves them), then stb_lumi_pic_6d_host; bit for bit.
+ * |theta| < 1.5.  The reference's bunch, slice and collision-order files are
+ * not written. */
+int stb_lumi_pic_6d_angle_host(double Np1, long Mp1, double Np2, long Mp2, double theta, int nslice1, int nslice2,
+                               double *x1, double *x2, double gamma1, double gamma2, double bbscale1,
+                               double bbscale2, int Ncoll, double freq, int device, double *lumi);
+
 /* BeamBeam6D_PIC_NonOffset(Np1, Mp1, x1, Np2, Mp2, x2, gamma1, gamma2,
  * bbscale1, bbscale2, Nslice1, Nslice2, zb1, zb2, Nx, Ny, hx, hy, grn_c_r,
  * grn_c_i), simtrack.cpp:24282-24432: the slice-boundary driver of

@@ -525,6 +525,15 @@ void ref_bb6d_pic_nonoffset(double Np1, int n1, double *x1, double Np2, int n2, 
                            hx, hy, gr, gi);
 }
 
+// Lumi_Cal_PIC_6D_Angle (simtrack.cpp:23946); it writes bunch, slice and
+// collision-order files into the working directory.
+double ref_lumi_pic_6d_angle(double Np1, int n1, double Np2, int n2, double theta, int ns1, int ns2, double *x1,
+                             double *x2, double gamma1, double gamma2, double bbscale1, double bbscale2, int ncoll,
+                             double freq) {
+  return Lumi_Cal_PIC_6D_Angle(Np1, n1, Np2, n2, theta, ns1, ns2, x1, x2, gamma1, gamma2, bbscale1, bbscale2, ncoll,
+                               freq);
+}
+
 // Lumi_Cal_PIC_6D (simtrack.cpp:23703); it writes ./collide_order.dat.
 double ref_lumi_pic_6d(double Np1, int n1, double Np2, int n2, int ns1, int ns2, double *x1, double *x2,
                        double gamma1, double gamma2, double bbscale1, double bbscale2, int ncoll, double freq) {

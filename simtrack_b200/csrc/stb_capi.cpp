@@ -1517,6 +1517,34 @@ int stb_lumi_pic_6d_host(double Np1, long Mp1, double Np2, long Mp2, int nslice1
   });
 }
 
+int stb_lumi_pic_6d_angle_host(double Np1, long Mp1, double Np2, long Mp2, double theta, int nslice1, int nslice2,
+                               double *x1, double *x2, double gamma1, double gamma2, double bbscale1,
+                               double bbscale2, int Ncoll, double freq, int device, double *lumi) {
+  return guarded([&] {
+    if (!x1 || !x2 || !lumi) throw Error(STB_EINVAL, "NULL argument");
+    soft_gaussian_6d_args(Mp1, Mp2, gamma1, gamma2, nslice1, nslice2);
+    if (Mp1 / nslice1 > INT32_MAX / 9 || Mp2 / nslice2 > INT32_MAX / 9) throw Error(STB_EINVAL, "slices too large");
+    if (!(std::fabs(theta) < 1.5)) throw Error(STB_EINVAL, "half crossing angle out of range");
+    DeviceGuard g(device);
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    double *d = nullptr;
+    const size_t b1 = sizeof(double) * 6 * (size_t)Mp1, b2 = sizeof(double) * 6 * (size_t)Mp2;
+    cuda_check(cudaMalloc(&d, b1 + b2), "cudaMalloc(bunches)");
+    DevFree f{d};
+    cuda_check(cudaMemcpy(d, x1, b1, cudaMemcpyHostToDevice), "upload bunch 1");
+    cuda_check(cudaMemcpy(d + 6 * Mp1, x2, b2, cudaMemcpyHostToDevice), "upload bunch 2");
+    const cudaError_t e = lumi_pic_6d_angle(Np1, Mp1, d, Np2, Mp2, d + 6 * Mp1, theta, gamma1, gamma2, bbscale1,
+                                            bbscale2, nslice1, nslice2, Ncoll, freq, sms, 0, lumi);
+    if (e == cudaErrorInvalidValue)
+      throw Error(STB_EINVAL, "a slice pair spans no area (zero or non-finite extent) or holds non-finite coordinates");
+    cuda_check(e, "sliced PIC luminosity with crossing angle");
+    cuda_check(cudaMemcpy(x1, d, b1, cudaMemcpyDeviceToHost), "download bunch 1");
+    cuda_check(cudaMemcpy(x2, d + 6 * Mp1, b2, cudaMemcpyDeviceToHost), "download bunch 2");
+    return STB_OK;
+  });
+}
+
 int stb_bb6d_soft_gaussian_zb_host(double Np1, long Mp1, double *x1, double Np2, long Mp2, double *x2,
                                    double gamma1, double gamma2, double bbscale1, double bbscale2, int nslice1,
                                    int nslice2, const double *zb1, const double *zb2, int device) {

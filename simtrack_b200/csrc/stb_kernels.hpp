@@ -147,6 +147,11 @@ cudaError_t pic_6d_nonoffset(double Np1, long Mp1, double *x1, double Np2, long 
                              double gamma2, double bbscale1, double bbscale2, int nslice, const double *zb1,
                              const double *zb2, int nx, double hx, double hy, const double *grn_re,
                              const double *grn_im, int num_sms, cudaStream_t s);
+// Lumi_Cal_PIC_6D_Angle: the bunches boosted by half crossing angle theta,
+// then Lumi_Cal_PIC_6D (stb_ssbb.cu; synchronises `s`).
+cudaError_t lumi_pic_6d_angle(double Np1, long Mp1, double *x1, double Np2, long Mp2, double *x2, double theta,
+                              double gamma1, double gamma2, double bbscale1, double bbscale2, int Nslice1,
+                              int Nslice2, int Ncoll, double freq, int num_sms, cudaStream_t s, double *lumi_out);
 // Lumi_Cal_PIC_6D on device AoS bunches (stb_ssbb.cu; synchronises `s`).
 cudaError_t lumi_pic_6d(double Np1, long Mp1, double *x1, double Np2, long Mp2, double *x2, double gamma1,
                         double gamma2, double bbscale1, double bbscale2, int Nslice1, int Nslice2, int Ncoll,

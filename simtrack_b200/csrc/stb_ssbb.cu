@@ -186,6 +186,29 @@ __global__ void slice_drift_kernel(double *x, long n, double S, bool forward) {
   }
 }
 
+// Lorentz_Transfer (simtrack.cpp:6790-6815): the boost of one particle to
+// the head-on frame of a collision with half crossing angle theta; sn, cs,
+// tn = sin, cos, tan(theta) as the reference forms them on the host.
+__global__ void lorentz_boost_kernel(double *x, long n, double sn, double cs, double tn) {
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    double *q = x + 6 * i;
+    const double x0 = q[0], px0 = q[1], y0 = q[2], py0 = q[3], z0 = q[4], pz0 = q[5];
+    const double ps0 = sqrt((1 + pz0) * (1 + pz0) - px0 * px0 - py0 * py0);
+    const double h0 = (1 + pz0) - ps0;
+    const double px_s = (px0 - tn * h0) / cs;
+    const double py_s = py0 / cs;
+    const double pz_s = pz0 - tn * px0 + tn * tn * h0;
+    const double ps_s = sqrt((1 + pz_s) * (1 + pz_s) - px_s * px_s - py_s * py_s);
+    const double h_s = (1 + pz_s) - ps_s;
+    q[0] = tn * z0 + (1 + (px_s / ps_s) * sn) * x0;
+    q[1] = px_s;
+    q[2] = y0 + sn * (py_s / ps_s) * x0;
+    q[3] = py_s;
+    q[4] = z0 / cs + (-h_s / ps_s) * sn * x0;
+    q[5] = pz_s;
+  }
+}
+
 }  // namespace
 
 cudaError_t sort_bunch_by_z(double *x, long n, double *scratch, int32_t *order, cudaStream_t s) {
@@ -365,6 +388,28 @@ cudaError_t lumi_pic_6d(double Np1, long Mp1, double *x1, double Np2, long Mp2, 
       });
   if (e == cudaSuccess) *lumi_out = lumi;
   return e;
+}
+
+// Lumi_Cal_PIC_6D_Angle (simtrack.cpp:23946-24224): every particle of
+// both bunches boosted to the head-on frame (Lorentz_Transfer; the bunches
+// stay boosted, as in the reference), then Lumi_Cal_PIC_6D.  The reference's
+// bunch, slice and collision-order files are not written.
+cudaError_t lumi_pic_6d_angle(double Np1, long Mp1, double *x1, double Np2, long Mp2, double *x2, double theta,
+                              double gamma1, double gamma2, double bbscale1, double bbscale2, int Nslice1,
+                              int Nslice2, int Ncoll, double freq, int num_sms, cudaStream_t s, double *lumi_out) {
+  // sin(theta), cos(theta) (correctly rounded) and their quotient, as
+  // Lorentz_Transfer forms them (its second cos(theta) is the same value)
+  const double sn = cr_sin(theta), cs = cr_cos(theta), tn = sn / cs;
+  const unsigned cap = (unsigned)num_sms * 8;
+  for (int b = 0; b < 2; b++) {
+    const long n = b == 0 ? Mp1 : Mp2;
+    const unsigned g = (unsigned)((n + 255) / 256 < cap ? (n + 255) / 256 : cap);
+    if (n > 0) lorentz_boost_kernel<<<g < 1 ? 1 : g, 256, 0, s>>>(b == 0 ? x1 : x2, n, sn, cs, tn);
+  }
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  return lumi_pic_6d(Np1, Mp1, x1, Np2, Mp2, x2, gamma1, gamma2, bbscale1, bbscale2, Nslice1, Nslice2, Ncoll, freq,
+                     num_sms, s, lumi_out);
 }
 
 // BeamBeam6D_SoftGaussian with slice boundaries (simtrack.cpp:23134-23283):

@@ -139,6 +139,10 @@ class RefOracle:
                                              c_double, c_double, c_double, c_double, c_int, c_int, POINTER(c_double),
                                              POINTER(c_double), c_int, c_int, c_double, c_double, POINTER(c_double),
                                              POINTER(c_double)]
+        L.ref_lumi_pic_6d_angle.argtypes = [c_double, c_int, c_double, c_int, c_double, c_int, c_int,
+                                            POINTER(c_double), POINTER(c_double), c_double, c_double, c_double,
+                                            c_double, c_int, c_double]
+        L.ref_lumi_pic_6d_angle.restype = c_double
         L.ref_bb6d_soft_gaussian.argtypes = [c_double, c_int, POINTER(c_double), c_double, c_int, POINTER(c_double),
                                              c_double, c_double, c_double, c_double, c_int, c_int]
         L.ref_bb6d_soft_gaussian_zb.argtypes = [c_double, c_int, POINTER(c_double), c_double, c_int,

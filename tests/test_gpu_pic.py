@@ -255,3 +255,27 @@ def test_pic_6d_nonoffset_vs_reference():
     assert np.array_equal(o1, r1) and np.array_equal(o2, r2)
     assert np.array_equal(o1[:, 4], b1[:, 4])  # particles stay in place
     assert (o1[:, 1] != b1[:, 1]).sum() > 0.9 * Mp1
+
+
+@pytest.mark.parametrize("theta", [0.0, 0.0125])
+def test_lumi_pic_6d_angle_vs_reference(theta, tmp_path, monkeypatch):
+    """Lumi_Cal_PIC_6D_Angle (simtrack.cpp:23946-24224): the Lorentz boost
+    of both bunches to the head-on frame, then the sliced luminosity; the
+    luminosity and the (boosted) bunches bit for bit."""
+    _need_ref()
+    monkeypatch.chdir(tmp_path)  # the reference writes its bunches, slices and collision order
+    Mp1, Mp2, ns1, ns2 = 2400, 2000, 3, 4
+    b1 = _beam(Mp1, 1.2e-4, 1.0e-4, 0.0, 0.0, 31)
+    b2 = _beam(Mp2, 1.1e-4, 1.1e-4, 1e-5, -5e-6, 32)
+    P = lambda a: a.ctypes.data_as(POINTER(c_double))
+    from ctypes import byref
+    from simtrack_b200._native import lib
+    o1, o2 = b1.copy(), b2.copy()
+    lumi = c_double()
+    assert lib().stb_lumi_pic_6d_angle_host(2e11, Mp1, 1.8e11, Mp2, theta, ns1, ns2, P(o1), P(o2), GAMMA, GAMMA, 1.0,
+                                            1.0, 1, 78196.0, 0, byref(lumi)) == 0
+    r1, r2 = b1.copy(), b2.copy()
+    theirs = oracle_bridge.RefOracle(cr=True).L.ref_lumi_pic_6d_angle(2e11, Mp1, 1.8e11, Mp2, theta, ns1, ns2, P(r1),
+                                                                      P(r2), GAMMA, GAMMA, 1.0, 1.0, 1, 78196.0)
+    assert lumi.value == theirs and theirs > 0
+    assert np.array_equal(o1, r1) and np.array_equal(o2, r2)
