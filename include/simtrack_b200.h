@@ -273,7 +273,11 @@ int stb_cal_tunes_track(stb_line *l, double *x6, int nturn, double tune_lower, d
 int stb_cal_tunes_track_orbit(stb_line *l, double deltap0, double tune_lower, double tune_upper, double *tunes2,
                               int device);
 /* Cal_Chrom_Track (simtrack.cpp:21027-21051): chroms4 = Chromx1, Chromy1,
- * Chromx2, Chromy2 from the tracked tunes at deltap = +3e-4, -3e-4, 0. */
+ * Chromx2, Chromy2 from the tracked tunes at deltap = +3e-4, -3e-4, 0.
+ * stb_cal_tunes_track, stb_cal_tunes_track_orbit and stb_cal_chrom_track set
+ * the process-wide tune window (the reference's globals tune_low, tune_high)
+ * for the length of the call: do not call them from two host threads at
+ * once. */
 int stb_cal_chrom_track(stb_line *l, double tune_lower, double tune_upper, double *chroms4, int device);
 
 /* ---- Track_Radial (simtrack.cpp:21641-21680) ----
