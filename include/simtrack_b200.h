@@ -585,6 +585,20 @@ int stb_bb6d_pic_nonoffset_host(double Np1, long Mp1, double *x1, double Np2, lo
                                 const double *zb1, const double *zb2, int Nx, int Ny, double hx, double hy,
                                 const double *grn_c_r, const double *grn_c_i, int device);
 
+/* BeamBeam6D_PIC_Interpolation(Np1, Mp1, x1, Np2, Mp2, x2, gamma1, gamma2,
+ * bbscale1, bbscale2, Nslice1, Nslice2, zb1, zb2, Nx, Ny, hx, hy, grn_c_r,
+ * grn_c_i), simtrack.cpp:24434-24700: slices and checks as for
+ * stb_bb6d_pic_nonoffset_host; in each slice pair each slice in turn
+ * deposits its charge drifted to the front and the back of the other slice
+ * (two potentials), and the other slice's particles, each drifted to its
+ * own collision point, take the field of the potential interpolated between
+ * the two (Interpolate_Electric_Field_2Potential, 3096-3152), with N/Mp of
+ * the whole depositing bunch; bit for bit. */
+int stb_bb6d_pic_interpolation_host(double Np1, long Mp1, double *x1, double Np2, long Mp2, double *x2,
+                                    double gamma1, double gamma2, double bbscale1, double bbscale2, int nslice1,
+                                    int nslice2, const double *zb1, const double *zb2, int Nx, int Ny, double hx,
+                                    double hy, const double *grn_c_r, const double *grn_c_i, int device);
+
 /* Lumi_Cal_PIC_6D(Np1, Mp1, Np2, Mp2, Nslice1, Nslice2, x1, x2, gamma1,
  * gamma2, bbscale1, bbscale2, Ncoll, freq), simtrack.cpp:23703-23944: the
  * sliced driver of stb_bb6d_pic_* (bunches reordered by z in place, slice

@@ -534,6 +534,14 @@ double ref_lumi_pic_6d_angle(double Np1, int n1, double Np2, int n2, double thet
                                freq);
 }
 
+// BeamBeam6D_PIC_Interpolation (simtrack.cpp:24434).
+void ref_bb6d_pic_interpolation(double Np1, int n1, double *x1, double Np2, int n2, double *x2, double gamma1,
+                                double gamma2, double bbscale1, double bbscale2, int ns1, int ns2, double *zb1,
+                                double *zb2, int nx, int ny, double hx, double hy, double *gr, double *gi) {
+  BeamBeam6D_PIC_Interpolation(Np1, n1, x1, Np2, n2, x2, gamma1, gamma2, bbscale1, bbscale2, ns1, ns2, zb1, zb2, nx,
+                               ny, hx, hy, gr, gi);
+}
+
 // Lumi_Cal_PIC_6D (simtrack.cpp:23703); it writes ./collide_order.dat.
 double ref_lumi_pic_6d(double Np1, int n1, double Np2, int n2, int ns1, int ns2, double *x1, double *x2,
                        double gamma1, double gamma2, double bbscale1, double bbscale2, int ncoll, double freq) {

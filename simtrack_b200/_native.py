@@ -188,6 +188,10 @@ SIGNATURES = [
     ("stb_lumi_pic_6d_angle_host", c_int, [c_double, c_long, c_double, c_long, c_double, c_int, c_int,
                                            POINTER(c_double), POINTER(c_double), c_double, c_double, c_double,
                                            c_double, c_int, c_double, c_int, POINTER(c_double)]),
+    ("stb_bb6d_pic_interpolation_host", c_int, [c_double, c_long, POINTER(c_double), c_double, c_long,
+                                                POINTER(c_double), c_double, c_double, c_double, c_double, c_int,
+                                                c_int, POINTER(c_double), POINTER(c_double), c_int, c_int, c_double,
+                                                c_double, POINTER(c_double), POINTER(c_double), c_int]),
     ("stb_bb6d_soft_gaussian_device", c_int, [c_double, c_long, c_void_p, c_double, c_long, c_void_p, c_double,
                                               c_double, c_double, c_double, c_int, c_int, c_int, c_void_p]),
     ("stb_bb6d_soft_gaussian_host", c_int, [c_double, c_long, POINTER(c_double), c_double, c_long, POINTER(c_double),

@@ -1612,6 +1612,43 @@ int stb_bb6d_pic_nonoffset_host(double Np1, long Mp1, double *x1, double Np2, lo
   });
 }
 
+int stb_bb6d_pic_interpolation_host(double Np1, long Mp1, double *x1, double Np2, long Mp2, double *x2, double gamma1,
+                                double gamma2, double bbscale1, double bbscale2, int nslice1, int nslice2,
+                                const double *zb1, const double *zb2, int Nx, int Ny, double hx, double hy,
+                                const double *grn_c_r, const double *grn_c_i, int device) {
+  return guarded([&] {
+    if (!x1 || !x2 || !zb1 || !zb2 || !grn_c_r || !grn_c_i) throw Error(STB_EINVAL, "NULL argument");
+    if (nslice1 != nslice2)
+      throw Error(STB_EINVAL, "the reference's slice-boundary form is defined for equal slice counts only");
+    if (nslice1 < 1 || nslice1 > 64) throw Error(STB_EINVAL, "slice count must be 1..64");
+    if (Mp1 < 2 || Mp2 < 2 || Mp1 > INT32_MAX / 9 || Mp2 > INT32_MAX / 9) throw Error(STB_EINVAL, "bad bunch size");
+    if (!(gamma1 > 0) || !(gamma2 > 0)) throw Error(STB_EINVAL, "gamma must be positive");
+    if (!pic_grid_valid(Nx, Ny)) throw Error(STB_EINVAL, "the grid must be square, Nx a power of two from 8 to 512");
+    DeviceGuard g(device);
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    const size_t b1 = sizeof(double) * 6 * (size_t)Mp1, b2 = sizeof(double) * 6 * (size_t)Mp2;
+    const size_t bg = sizeof(double) * 4 * (size_t)Nx * Ny;
+    double *d = nullptr;
+    cuda_check(cudaMalloc(&d, b1 + b2 + 2 * bg), "cudaMalloc(bunches)");
+    DevFree f{d};
+    double *d2 = d + 6 * Mp1, *gr = d2 + 6 * Mp2, *gi = gr + 4 * (size_t)Nx * Ny;
+    cuda_check(cudaMemcpy(d, x1, b1, cudaMemcpyHostToDevice), "upload bunch 1");
+    cuda_check(cudaMemcpy(d2, x2, b2, cudaMemcpyHostToDevice), "upload bunch 2");
+    cuda_check(cudaMemcpy(gr, grn_c_r, bg, cudaMemcpyHostToDevice), "upload Green function");
+    cuda_check(cudaMemcpy(gi, grn_c_i, bg, cudaMemcpyHostToDevice), "upload Green function");
+    const cudaError_t e = pic_6d_interpolation(Np1, Mp1, d, Np2, Mp2, d2, gamma1, gamma2, bbscale1, bbscale2,
+                                               nslice1, zb1, zb2, Nx, hx, hy, gr, gi, sms, 0);
+    if (e == cudaErrorInvalidValue)
+      throw Error(STB_EINVAL,
+                  "a slice holds fewer than 2 or more than 2*Mp/Nslice particles, or a particle maps outside the grid");
+    cuda_check(e, "sliced particle-in-cell beam-beam (interpolated potentials)");
+    cuda_check(cudaMemcpy(x1, d, b1, cudaMemcpyDeviceToHost), "download bunch 1");
+    cuda_check(cudaMemcpy(x2, d2, b2, cudaMemcpyDeviceToHost), "download bunch 2");
+    return STB_OK;
+  });
+}
+
 int stb_rad_normals(unsigned long long seed, unsigned long long id, unsigned long long k0, long n, double *out,
                     int device) {
   return guarded([&] {

@@ -147,6 +147,18 @@ cudaError_t pic_6d_nonoffset(double Np1, long Mp1, double *x1, double Np2, long 
                              double gamma2, double bbscale1, double bbscale2, int nslice, const double *zb1,
                              const double *zb2, int nx, double hx, double hy, const double *grn_re,
                              const double *grn_im, int num_sms, cudaStream_t s);
+// One slice pair of BeamBeam6D_PIC_Interpolation (stb_pic.cu; synchronises
+// `s`): slice centres z1c, z2c, kick factors Np/Mp of the whole bunches.
+cudaError_t pic_interpolation_pair(double *x1, long m1, double *x2, long m2, double z1c, double z2c,
+                                   double np1_per_mp1, double np2_per_mp2, double gamma1, double gamma2,
+                                   double bbscale1, double bbscale2, int nx, double hx, double hy,
+                                   const double *grn_re, const double *grn_im, int num_sms, cudaStream_t s);
+// BeamBeam6D_PIC_Interpolation with slice boundaries zb1, zb2 (host arrays)
+// and the caller's grid and Green spectrum (device arrays); stb_ssbb.cu.
+cudaError_t pic_6d_interpolation(double Np1, long Mp1, double *x1, double Np2, long Mp2, double *x2, double gamma1,
+                                 double gamma2, double bbscale1, double bbscale2, int nslice, const double *zb1,
+                                 const double *zb2, int nx, double hx, double hy, const double *grn_re,
+                                 const double *grn_im, int num_sms, cudaStream_t s);
 // Lumi_Cal_PIC_6D_Angle: the bunches boosted by half crossing angle theta,
 // then Lumi_Cal_PIC_6D (stb_ssbb.cu; synchronises `s`).
 cudaError_t lumi_pic_6d_angle(double Np1, long Mp1, double *x1, double Np2, long Mp2, double *x2, double theta,

@@ -285,6 +285,123 @@ __global__ void pic_kick_kernel(double *x, long n, GridFrame g, double xoffset, 
   }
 }
 
+// The potential of Cal_Potential_Convolution, phi[i*nx + j], from the
+// inverse transform.
+__global__ void potential_kernel(const double *re, double *phi, int nx) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nx * nx) return;
+  phi[t] = phi_at(re, t / nx, t % nx, nx);
+}
+
+// x -= px S (plus = false) or x += px S, and the same for y.
+__global__ void drift_xy_kernel(double *x, long n, double S, bool plus) {
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    double *q = x + 6 * i;
+    if (plus) {
+      q[0] = q[0] + q[1] * S;
+      q[2] = q[2] + q[3] * S;
+    } else {
+      q[0] = q[0] - q[1] * S;
+      q[2] = q[2] - q[3] * S;
+    }
+  }
+}
+
+// The z range of a slice, from -100 and 100 as the reference starts
+// (exact in any order): out2 = zfront (largest), zback (smallest).
+__global__ void __launch_bounds__(1024) zrange_kernel(const double *x, long n, double *out2) {
+  __shared__ double red[2][32];
+  double zf = -100, zb = 100;
+  for (long i = threadIdx.x; i < n; i += 1024) {
+    const double z = x[6 * i + 4];
+    if (z > zf) zf = z;
+    if (z < zb) zb = z;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    const double a = __shfl_down_sync(0xffffffffu, zf, o), c = __shfl_down_sync(0xffffffffu, zb, o);
+    if (a > zf) zf = a;
+    if (c < zb) zb = c;
+  }
+  if ((threadIdx.x & 31) == 0) {
+    red[0][threadIdx.x >> 5] = zf;
+    red[1][threadIdx.x >> 5] = zb;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    zf = red[0][0];
+    zb = red[1][0];
+    for (int w = 1; w < 32; w++) {
+      if (red[0][w] > zf) zf = red[0][w];
+      if (red[1][w] < zb) zb = red[1][w];
+    }
+    out2[0] = zf;
+    out2[1] = zb;
+  }
+}
+
+// The kicked slice of BeamBeam6D_PIC_Interpolation (simtrack.cpp:24600-24615
+// and its mirror): each particle drifts by sp = (z - zc) / 2, takes the
+// field of Interpolate_Electric_Field_2Potential (3096-3152: a 5 x 5 patch of
+// the potential interpolated in s between phi1 at sfront and phi2 at sback,
+// differenced with the field stencil at the 3 x 3 mesh lines, weighted) if
+// inside the cut around the origin, and drifts back with the kicked momenta.
+__global__ void interp2_kick_kernel(double *x, long n, double zc, GridFrame g, double sfront, double sback,
+                                    const double *phi1, const double *phi2, double bbscale, double gamma,
+                                    double np_per_mp, int *err) {
+  for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long)gridDim.x * blockDim.x) {
+    double *q = x + 6 * p;
+    const double sp = (q[4] - zc) / 2;
+    q[0] = q[0] + q[1] * sp;
+    q[2] = q[2] + q[3] * sp;
+    const double xp = q[0], yp = q[2];
+    if (in_cut(xp, yp, g)) {
+      int xm[3], ym[3];
+      double xw[3], yw[3];
+      grid_weight_1d(xp - g.x0, g.hx, xm, xw);
+      grid_weight_1d(yp - g.y0, g.hy, ym, yw);
+      int i0 = 10000, j0 = 10000;
+      for (int k = 0; k < 3; k++) {
+        if (xm[k] < i0) i0 = xm[k];
+        if (ym[k] < j0) j0 = ym[k];
+      }
+      if (i0 < 1 || j0 < 1 || i0 + 3 >= g.nx || j0 + 3 >= g.nx) {
+        atomicExch(err, 1);
+      } else {
+        double ph[25];
+        for (int a = 0; a < 5; a++)
+          for (int b = 0; b < 5; b++) {
+            const int c = g.nx * (i0 - 1 + a) + (j0 - 1 + b);
+            if (sfront == sback) {
+              ph[5 * a + b] = phi1[c];
+            } else {
+              const double pf = phi1[c], pb = phi2[c];
+              ph[5 * a + b] = pb + (pf - pb) * (sp - sback) / (sfront - sback);
+            }
+          }
+        double ex = 0., ey = 0.;
+        for (int i = 0; i < 3; i++)
+          for (int j = 0; j < 3; j++) {
+            const int a = xm[i] - i0 + 1, b = ym[j] - j0 + 1;
+            const double fx = -((ph[(a + 1) * 5 + b + 1] - ph[(a - 1) * 5 + b + 1]) +
+                                4 * (ph[(a + 1) * 5 + b] - ph[(a - 1) * 5 + b]) +
+                                (ph[(a + 1) * 5 + b - 1] - ph[(a - 1) * 5 + b - 1])) /
+                              12. / g.hx;
+            const double fy = -((ph[(a + 1) * 5 + b + 1] - ph[(a + 1) * 5 + b - 1]) +
+                                4 * (ph[a * 5 + b + 1] - ph[a * 5 + b - 1]) +
+                                (ph[(a - 1) * 5 + b + 1] - ph[(a - 1) * 5 + b - 1])) /
+                              12. / g.hy;
+            ex = ex + fx * xw[i] * yw[j];
+            ey = ey + fy * xw[i] * yw[j];
+          }
+        q[1] = q[1] + ex * 1.60217662e-19 * bbscale / (gamma * 938.27201e6) * np_per_mp;
+        q[3] = q[3] + ey * 1.60217662e-19 * bbscale / (gamma * 938.27201e6) * np_per_mp;
+      }
+    }
+    q[0] = q[0] - q[1] * sp;
+    q[2] = q[2] - q[3] * sp;
+  }
+}
+
 // src[c] = 0 + w_1 + w_2 + ... for the 64 x 64 grid alone (Charge2Grid's
 // array).
 __global__ void cell_sum_kernel(const double *vals, const int *start, const int *end, double *src, int ncell) {
@@ -552,6 +669,16 @@ cudaError_t potential_field(PicScratch &S, const double *gre, const double *gim,
   return cudaGetLastError();
 }
 
+// Cal_Potential_Convolution alone: the potential of the deposited charge
+// (wr, wi) with the Green spectrum (gre, gim) into phi (nx x nx).
+cudaError_t potential(PicScratch &S, const double *gre, const double *gim, double *phi, cudaStream_t s) {
+  fft2d(S.wr, S.wi, S.tw_fwd, 1, S.log2n2, s);
+  spectrum_product_kernel<<<(int)((S.grid2 + 255) / 256), 256, 0, s>>>(S.wr, S.wi, gre, gim, (int)S.grid2);
+  fft2d(S.wr, S.wi, S.tw_inv, -1, S.log2n2, s);
+  potential_kernel<<<(S.ncell + 127) / 128, 128, 0, s>>>(S.wr, phi, S.nx);
+  return cudaGetLastError();
+}
+
 cudaError_t finish(PicScratch &S, cudaError_t e, cudaStream_t s) {
   int h_err = 0;
   if (e == cudaSuccess) e = cudaMemcpyAsync(&h_err, S.err, sizeof(int), cudaMemcpyDeviceToHost, s);
@@ -628,6 +755,42 @@ cudaError_t pic_4d_nonoffset(double Np1, long Mp1, double *x1, double Np2, long 
     pic_kick_kernel<<<grid_of(nt, num_sms), 256, 0, s>>>(d == 0 ? x2 : x1, nt, g, 0., 0., S.Ex, S.Ey,
                                                           d == 0 ? bbscale2 : bbscale1, d == 0 ? gamma2 : gamma1,
                                                           (d == 0 ? Np1 : Np2) / (double)(int)ns, S.err);
+    e = cudaGetLastError();
+  }
+  return finish(S, e, s);
+}
+
+cudaError_t pic_interpolation_pair(double *x1, long m1, double *x2, long m2, double z1c, double z2c,
+                                   double np1_per_mp1, double np2_per_mp2, double gamma1, double gamma2,
+                                   double bbscale1, double bbscale2, int nx, double hx, double hy,
+                                   const double *grn_re, const double *grn_im, int num_sms, cudaStream_t s) {
+  PicScratch S;
+  cudaError_t e = S.init(nx, std::max(m1, m2), s);
+  const GridFrame g{0., 0., -nx * hx / 2, -nx * hy / 2, hx, hy, nx};
+  double zr[2] = {0, 0};
+  // direction 0: slice 1 deposits at the front and back of slice 2, slice 2
+  // is kicked; direction 1 the reverse, with slice 2's kicked momenta
+  for (int d = 0; d < 2 && e == cudaSuccess; d++) {
+    double *xs = d == 0 ? x1 : x2, *xt = d == 0 ? x2 : x1;
+    const long ms = d == 0 ? m1 : m2, mt = d == 0 ? m2 : m1;
+    const double zc = d == 0 ? z1c : z2c;
+    zrange_kernel<<<1, 1024, 0, s>>>(xt, mt, S.m8);
+    if ((e = cudaMemcpyAsync(zr, S.m8, sizeof(zr), cudaMemcpyDeviceToHost, s)) != cudaSuccess) break;
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) break;
+    const double sfront = (zr[0] - zc) / 2, sback = (zr[1] - zc) / 2;
+    const double sd[2] = {sfront, sback};
+    double *phi[2] = {S.Ex, S.Ey};
+    for (int k = 0; k < 2 && e == cudaSuccess; k++) {
+      drift_xy_kernel<<<grid_of(ms, num_sms), 256, 0, s>>>(xs, ms, sd[k], false);
+      if ((e = deposit(S, xs, ms, g, true, true, nullptr, num_sms, s)) != cudaSuccess) break;
+      if ((e = potential(S, grn_re, grn_im, phi[k], s)) != cudaSuccess) break;
+      drift_xy_kernel<<<grid_of(ms, num_sms), 256, 0, s>>>(xs, ms, sd[k], true);
+      e = cudaGetLastError();
+    }
+    if (e != cudaSuccess) break;
+    interp2_kick_kernel<<<grid_of(mt, num_sms), 256, 0, s>>>(xt, mt, zc, g, sfront, sback, S.Ex, S.Ey,
+                                                              d == 0 ? bbscale2 : bbscale1, d == 0 ? gamma2 : gamma1,
+                                                              d == 0 ? np1_per_mp1 : np2_per_mp2, S.err);
     e = cudaGetLastError();
   }
   return finish(S, e, s);

@@ -490,7 +490,7 @@ cudaError_t sliced_6d_zb(double Np1, long Mp1, double *x1, double Np2, long Mp2,
       const unsigned g2 = (unsigned)((m2 + 255) / 256 < cap ? (m2 + 255) / 256 : cap);
       if (m1 > 0) gather_members_kernel<<<g1, 256, 0, s>>>(x1, j1, m1, xc1);
       if (m2 > 0) gather_members_kernel<<<g2, 256, 0, s>>>(x2, j2, m2, xc2);
-      e = collide(xc1, m1, xc2, m2, S[i], N1c, N2c);
+      e = collide(xc1, m1, xc2, m2, S[i], N1c, N2c, Z1[I1[i]], Z2[I2[i]]);
       if (m1 > 0) scatter_members_kernel<<<g1, 256, 0, s>>>(x1, j1, m1, xc1);
       if (m2 > 0) scatter_members_kernel<<<g2, 256, 0, s>>>(x2, j2, m2, xc2);
       if (e == cudaSuccess) e = cudaGetLastError();
@@ -508,7 +508,7 @@ cudaError_t soft_gaussian_6d_zb(double Np1, long Mp1, double *x1, double Np2, lo
                                 const double *zb2, int num_sms, cudaStream_t s) {
   const double rp = 1.53469826769e-18;  // BB4D, simtrack.cpp:6328
   return sliced_6d_zb(Np1, Mp1, x1, Np2, Mp2, x2, nslice, zb1, zb2, num_sms, s,
-                      [&](double *a, long m1, double *b, long m2, double S, double N1c, double N2c) {
+                      [&](double *a, long m1, double *b, long m2, double S, double N1c, double N2c, double, double) {
                         const double c4_1 = 2 * N2c * rp / gamma1, c4_2 = 2 * N1c * rp / gamma2;
                         return slice_pair_collision(a, m1, b, m2, S, c4_1, c4_2, bbscale1, bbscale2, num_sms, s);
                       });
@@ -522,7 +522,7 @@ cudaError_t pic_6d_nonoffset(double Np1, long Mp1, double *x1, double Np2, long 
                              const double *zb2, int nx, double hx, double hy, const double *grn_re,
                              const double *grn_im, int num_sms, cudaStream_t s) {
   return sliced_6d_zb(Np1, Mp1, x1, Np2, Mp2, x2, nslice, zb1, zb2, num_sms, s,
-                      [&](double *a, long m1, double *b, long m2, double S, double N1c, double N2c) {
+                      [&](double *a, long m1, double *b, long m2, double S, double N1c, double N2c, double, double) {
                         const unsigned g1 = (unsigned)((m1 + 255) / 256 < num_sms * 8 ? (m1 + 255) / 256 : num_sms * 8);
                         const unsigned g2 = (unsigned)((m2 + 255) / 256 < num_sms * 8 ? (m2 + 255) / 256 : num_sms * 8);
                         slice_drift_kernel<<<g1 < 1 ? 1 : g1, 256, 0, s>>>(a, m1, S, true);
@@ -535,6 +535,25 @@ cudaError_t pic_6d_nonoffset(double Np1, long Mp1, double *x1, double Np2, long 
                         slice_drift_kernel<<<g1 < 1 ? 1 : g1, 256, 0, s>>>(a, m1, S, false);
                         slice_drift_kernel<<<g2 < 1 ? 1 : g2, 256, 0, s>>>(b, m2, -S, false);
                         return cudaGetLastError();
+                      });
+}
+
+// BeamBeam6D_PIC_Interpolation (simtrack.cpp:24434-24700): the
+// slice-boundary driver above; in each slice pair, each slice in turn
+// deposits its charge drifted to the front and the back of the other slice
+// (two potentials on the caller's grid and Green spectrum), and the other
+// slice's particles, each drifted to its own collision point, take the field
+// of the potential interpolated between the two, with N/Mp of the whole
+// depositing bunch.
+cudaError_t pic_6d_interpolation(double Np1, long Mp1, double *x1, double Np2, long Mp2, double *x2, double gamma1,
+                                 double gamma2, double bbscale1, double bbscale2, int nslice, const double *zb1,
+                                 const double *zb2, int nx, double hx, double hy, const double *grn_re,
+                                 const double *grn_im, int num_sms, cudaStream_t s) {
+  const double q1 = Np1 / (int)Mp1, q2 = Np2 / (int)Mp2;
+  return sliced_6d_zb(Np1, Mp1, x1, Np2, Mp2, x2, nslice, zb1, zb2, num_sms, s,
+                      [&](double *a, long m1, double *b, long m2, double, double, double, double z1c, double z2c) {
+                        return pic_interpolation_pair(a, m1, b, m2, z1c, z2c, q1, q2, gamma1, gamma2, bbscale1,
+                                                      bbscale2, nx, hx, hy, grn_re, grn_im, num_sms, s);
                       });
 }
 

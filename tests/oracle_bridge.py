@@ -143,6 +143,7 @@ class RefOracle:
                                             POINTER(c_double), POINTER(c_double), c_double, c_double, c_double,
                                             c_double, c_int, c_double]
         L.ref_lumi_pic_6d_angle.restype = c_double
+        L.ref_bb6d_pic_interpolation.argtypes = L.ref_bb6d_pic_nonoffset.argtypes
         L.ref_bb6d_soft_gaussian.argtypes = [c_double, c_int, POINTER(c_double), c_double, c_int, POINTER(c_double),
                                              c_double, c_double, c_double, c_double, c_int, c_int]
         L.ref_bb6d_soft_gaussian_zb.argtypes = [c_double, c_int, POINTER(c_double), c_double, c_int,

@@ -279,3 +279,29 @@ def test_lumi_pic_6d_angle_vs_reference(theta, tmp_path, monkeypatch):
                                                                       P(r2), GAMMA, GAMMA, 1.0, 1.0, 1, 78196.0)
     assert lumi.value == theirs and theirs > 0
     assert np.array_equal(o1, r1) and np.array_equal(o2, r2)
+
+
+def test_pic_6d_interpolation_vs_reference():
+    """BeamBeam6D_PIC_Interpolation (simtrack.cpp:24434-24700): per slice
+    pair, two potentials at the front and back of the other slice, the field
+    interpolated in s at each particle's own collision point; bit for bit with
+    the reference's own Green spectrum."""
+    _need_ref()
+    Mp1, Mp2, ns, nx = 4000, 3600, 5, 64
+    b1 = _beam(Mp1, 1.2e-4, 1.0e-4, 0.0, 0.0, 41)
+    b2 = _beam(Mp2, 1.1e-4, 1.1e-4, 1e-5, -5e-6, 42)
+    zb1 = np.array([1.0, 0.1, 0.03, -0.03, -0.1, -1.0])
+    zb2 = np.array([1.0, 0.12, 0.02, -0.04, -0.11, -1.0])
+    hx, hy = 15 * 1.1e-4 / nx, 15 * 1.0e-4 / nx
+    gr, gi = _green(nx, hx, hy, ours=False)
+    P = lambda a: a.ctypes.data_as(POINTER(c_double))
+    from simtrack_b200._native import lib
+    o1, o2 = b1.copy(), b2.copy()
+    assert lib().stb_bb6d_pic_interpolation_host(2e11, Mp1, P(o1), 1.8e11, Mp2, P(o2), GAMMA, GAMMA, 1.0, 1.0, ns,
+                                                 ns, P(zb1), P(zb2), nx, nx, hx, hy, P(gr), P(gi), 0) == 0
+    r1, r2 = b1.copy(), b2.copy()
+    oracle_bridge.RefOracle().L.ref_bb6d_pic_interpolation(2e11, Mp1, P(r1), 1.8e11, Mp2, P(r2), GAMMA, GAMMA, 1.0,
+                                                           1.0, ns, ns, P(zb1.copy()), P(zb2.copy()), nx, nx, hx, hy,
+                                                           P(gr), P(gi))
+    assert np.array_equal(o1, r1) and np.array_equal(o2, r2)
+    assert (o1[:, 1] != b1[:, 1]).sum() > 0.9 * Mp1
