@@ -112,3 +112,34 @@ def test_soft_gaussian_collision_rejects_empty_beams(native_lib):
     assert L.stb_bb4d_soft_gaussian_host(1e11, 1, None, 1e11, 1, b, 100.0, 100.0, 1.0, 1.0, 0) == _native.STB_EINVAL
     assert L.stb_bb4d_soft_gaussian_device(1e11, 1, None, 1e11, 1, None, 100.0, 100.0, 1.0, 1.0, 0, None) \
         == _native.STB_EINVAL
+
+
+def test_pic_and_luminosity_entry_points_check_arguments_first(native_lib):
+    """The particle-in-cell and luminosity entry points reject bad beams,
+    grids and slice counts before any device work (no GPU needed)."""
+    from ctypes import byref, c_double
+    from simtrack_b200 import _native
+    L, E = native_lib, _native.STB_EINVAL
+    b = (c_double * 60)()
+    g = (c_double * (4 * 48 * 48))()
+    out = c_double()
+    # BeamBeam4D_PIC: at least two macro-particles per beam, positive gamma
+    assert L.stb_bb4d_pic_host(1e11, 1, b, 1e11, 10, b, 100.0, 100.0, 1.0, 1.0, 0) == E
+    assert L.stb_bb4d_pic_host(1e11, 10, b, 1e11, 10, b, -1.0, 100.0, 1.0, 1.0, 0) == E
+    assert L.stb_bb4d_pic_device(1e11, 10, None, 1e11, 10, None, 100.0, 100.0, 1.0, 1.0, 0, None) == E
+    # grids: square, a power of two from 8 to 512
+    for nx, ny in ((48, 48), (32, 64), (4, 4), (1024, 1024)):
+        assert L.stb_pic_green_function(0.0, 0.0, nx, ny, 1e-5, 1e-5, g, g, 0) == E
+        assert L.stb_bb4d_pic_nonoffset_host(1e11, 10, b, 1e11, 10, b, 100.0, 100.0, 1.0, 1.0, nx, ny, 1e-5, 1e-5, g,
+                                             g, 0) == E
+    # luminosities: non-empty beams; sliced forms: slice counts and populations
+    assert L.stb_lumi_pic_4d_host(1e11, 0, 1e11, 10, b, b, 1, 1e4, 0, byref(out)) == E
+    assert L.stb_lumi_pic_6d_host(1e11, 10, 1e11, 10, 0, 1, b, b, 100.0, 100.0, 1.0, 1.0, 1, 1e4, 0, byref(out)) == E
+    assert L.stb_lumi_pic_6d_angle_host(1e11, 10, 1e11, 10, 2.0, 1, 1, b, b, 100.0, 100.0, 1.0, 1.0, 1, 1e4, 0,
+                                        byref(out)) == E
+    assert L.stb_bb6d_pic_host(1e11, 10, b, 1e11, 10, b, 100.0, 100.0, 1.0, 1.0, 6, 1, 0) == E  # slices of 1
+    zb = (c_double * 3)(1.0, 0.0, -1.0)
+    assert L.stb_bb6d_pic_interpolation_host(1e11, 10, b, 1e11, 10, b, 100.0, 100.0, 1.0, 1.0, 2, 1, zb, zb, 64, 64,
+                                             1e-5, 1e-5, g, g, 0) == E  # unequal slice counts
+    # Cal_SRLoss_Particle: NULL arguments
+    assert L.stb_cal_srloss_particle(None, None, None, 0) == E
